@@ -1,0 +1,315 @@
+"""ctypes binding of libclb.so (include/clb.h), the C-ABI of the B200 reactive-transport step.
+
+This module is what a Python caller (and this repository's tests and benchmark) uses; a C++
+host links the same library directly. There is no fallback: if libclb.so is missing or no CUDA
+device is present, every call fails with an exception naming the cause.
+
+Arrays follow the library's layout: x slowest, z fastest, index (x*ny + y)*nz + z; population
+arrays are [q][N] in Palabos' velocity order, shifted by the weights.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libclb.so")
+
+F64, F32, F16S = 0, 1, 2
+DIRICHLET, NEUMANN, CLOSED = 0, 1, 2
+LAW_NONE, LAW_DECAY, LAW_MONOD, LAW_DUAL_MONOD = 0, 1, 2, 3
+FIELD_MATERIAL, FIELD_FLOW_VELOCITY, FIELD_FLOW_POPULATIONS = 0, 1, 2
+FIELD_CONCENTRATION, FIELD_ADE_POPULATIONS, FIELD_BIOMASS, FIELD_ADE_VELOCITY = 3, 4, 5, 6
+
+STATUS = {0: "OK", 1: "INVALID_ARG", 2: "NOT_CONVERGED", 3: "NONFINITE", 4: "PERCOLATION_LOST",
+          5: "CUDA_ERROR", 6: "TIMEOUT", 7: "NOT_INITIALIZED", 8: "OUT_OF_MEMORY"}
+
+MAX_MICROBES, MAX_PORE_CODES, MAX_SPECIES = 8, 8, 16
+
+
+class DomainDesc(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("flow_precision", C.c_int32), ("ade_precision", C.c_int32),
+                ("solid_code", C.c_int32), ("bounce_back_code", C.c_int32),
+                ("n_pore_codes", C.c_int32), ("pore_codes", C.c_int32 * MAX_PORE_CODES),
+                ("n_microbes", C.c_int32), ("bio_codes", C.c_int32 * MAX_MICROBES),
+                ("perm_ratio", C.c_double * MAX_MICROBES), ("tau", C.c_double)]
+
+
+class SpeciesDesc(C.Structure):
+    _fields_ = [("omega_pore", C.c_double), ("omega_biofilm", C.c_double), ("mobile", C.c_int32),
+                ("left_type", C.c_int32), ("right_type", C.c_int32),
+                ("left_bc", C.c_double), ("right_bc", C.c_double), ("c0", C.c_double)]
+
+
+class FlowStats(C.Structure):
+    _fields_ = [("pore_mean_u", C.c_double), ("pore_max_ux", C.c_double), ("darcy_outlet_ux", C.c_double),
+                ("permeability", C.c_double), ("energy", C.c_double), ("iterations", C.c_int64),
+                ("bgk_nodes", C.c_int64), ("active_nodes", C.c_int64)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("total", C.c_double * MAX_SPECIES), ("content", C.c_double * MAX_SPECIES),
+                ("biomass", C.c_double * MAX_MICROBES), ("min_c", C.c_double * MAX_SPECIES),
+                ("max_c", C.c_double * MAX_SPECIES), ("open_voxels", C.c_int64),
+                ("nonfinite", C.c_int64), ("ade_iterations", C.c_int64)]
+
+
+class GeomOptions(C.Structure):
+    _fields_ = [("kind", C.c_char_p), ("porosity", C.c_double), ("radius", C.c_double),
+                ("aperture", C.c_double), ("roughness", C.c_double), ("count", C.c_int32),
+                ("layers", C.c_int32), ("seed", C.c_uint64), ("walls", C.c_char_p)]
+
+
+class Inspection(C.Structure):
+    _fields_ = [("porosity", C.c_double), ("open_voxels", C.c_int64), ("isolated_voxels", C.c_int64),
+                ("clusters", C.c_int32), ("spanning_clusters", C.c_int32), ("percolates", C.c_int32),
+                ("quasi_2d", C.c_int32)]
+
+
+# every symbol include/clb.h declares, with its argument types
+SIGNATURES = {
+    "clb_set_device": [C.c_int],
+    "clb_create": [C.POINTER(DomainDesc), C.c_void_p, C.POINTER(C.c_void_p)],
+    "clb_destroy": [C.c_void_p],
+    "clb_last_error": [C.c_void_p],
+    "clb_global_error": [],
+    "clb_synchronize": [C.c_void_p],
+    "clb_set_stream": [C.c_void_p, C.c_void_p],
+    "clb_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
+    "clb_flow_init": [C.c_void_p, C.c_double],
+    "clb_flow_step": [C.c_void_p, C.c_int],
+    "clb_flow_solve": [C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_int)],
+    "clb_flow_stats_get": [C.c_void_p, C.c_double, C.POINTER(FlowStats)],
+    "clb_flow_solve_peclet": [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
+                              C.POINTER(C.c_double), C.POINTER(C.c_int)],
+    "clb_ade_init": [C.c_void_p, C.POINTER(SpeciesDesc), C.c_int],
+    "clb_couple_velocity": [C.c_void_p],
+    "clb_set_kinetics": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double],
+    "clb_set_biomass": [C.c_void_p, C.c_int, C.c_void_p],
+    "clb_ade_step": [C.c_void_p, C.c_int],
+    "clb_reduce": [C.c_void_p, C.POINTER(Stats)],
+    "clb_get_field": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int],
+    "clb_set_field": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int],
+    "clb_geom_generate": [C.POINTER(GeomOptions), C.c_int, C.c_int, C.c_int, C.c_void_p],
+    "clb_geom_sphere_pack": [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                             C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p],
+    "clb_geom_read_dat": [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p],
+    "clb_geom_inspect": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(Inspection)],
+}
+
+_lib = None
+
+
+def lib():
+    """Load libclb.so once; raise if it is missing (no silent fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libclb.so not built at {LIB_PATH}; run __graft_entry__.build()")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_char_p if name in ("clb_last_error", "clb_global_error") else C.c_int
+        _lib = L
+    return _lib
+
+
+class ClbError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _check_global(st):
+    if st != 0:
+        raise ClbError(st, lib().clb_global_error().decode())
+
+
+# ------------------------------------------------------------------------------ geometry
+def geom_generate(kind, nx, ny, nz, porosity=0.4, radius=6.0, aperture=6.0, roughness=2.0, count=20,
+                  layers=4, seed=1, walls="y"):
+    out = np.empty(nx * ny * nz, dtype=np.int8)
+    o = GeomOptions(kind.encode(), porosity, radius, aperture, roughness, count, layers, seed, walls.encode())
+    _check_global(lib().clb_geom_generate(C.byref(o), nx, ny, nz, _ptr(out)))
+    return out
+
+
+def sphere_pack(nx, ny, nz, porosity, rmin, rmax, seed, walls="yz", grain=1, wall=1, pore=2):
+    out = np.empty(nx * ny * nz, dtype=np.int8)
+    _check_global(lib().clb_geom_sphere_pack(nx, ny, nz, porosity, rmin, rmax, seed, walls.encode(),
+                                             grain, wall, pore, _ptr(out)))
+    return out
+
+
+def read_dat(path, nx_inner, ny, nz):
+    out = np.empty((nx_inner + 2) * ny * nz, dtype=np.int8)
+    _check_global(lib().clb_geom_read_dat(path.encode(), nx_inner, ny, nz, _ptr(out)))
+    return out
+
+
+def inspect(mat, nx, ny, nz):
+    r = Inspection()
+    m = np.ascontiguousarray(mat, dtype=np.int8)
+    _check_global(lib().clb_geom_inspect(_ptr(m), nx, ny, nz, C.byref(r)))
+    return {k: getattr(r, k) for k, _ in Inspection._fields_}
+
+
+# ------------------------------------------------------------------------------ domain
+class Domain:
+    """One handle of the library (a domain with its flow and species lattices)."""
+
+    def __init__(self, material, nx, ny, nz, tau, flow_precision=F32, ade_precision=F32,
+                 solid_code=0, bounce_back_code=1, pore_codes=(2,), bio_codes=(), perm_ratio=(), device=None):
+        L = lib()
+        if device is not None:
+            _check_global(L.clb_set_device(int(device)))
+        d = DomainDesc()
+        d.nx, d.ny, d.nz = nx, ny, nz
+        d.flow_precision, d.ade_precision = flow_precision, ade_precision
+        d.solid_code, d.bounce_back_code = solid_code, bounce_back_code
+        d.n_pore_codes = len(pore_codes)
+        for k, c in enumerate(pore_codes):
+            d.pore_codes[k] = c
+        d.n_microbes = len(bio_codes)
+        for k, c in enumerate(bio_codes):
+            d.bio_codes[k] = c
+            d.perm_ratio[k] = perm_ratio[k] if k < len(perm_ratio) else 1.0
+        d.tau = tau
+        self.desc = d
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.N = nx * ny * nz
+        self.S = 0
+        m = np.ascontiguousarray(material, dtype=np.int8)
+        assert m.size == self.N
+        h = C.c_void_p()
+        _check_global(L.clb_create(C.byref(d), _ptr(m), C.byref(h)))
+        self.h = h
+
+    def _check(self, st):
+        if st != 0:
+            raise ClbError(st, lib().clb_last_error(self.h).decode())
+        return st
+
+    def close(self):
+        if self.h:
+            lib().clb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        self._check(lib().clb_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def stream(self):
+        p = C.c_void_p()
+        self._check(lib().clb_get_stream(self.h, C.byref(p)))
+        return p.value
+
+    def sync(self):
+        self._check(lib().clb_synchronize(self.h))
+
+    # ---- flow
+    def flow_init(self, delta_p):
+        self._check(lib().clb_flow_init(self.h, delta_p))
+
+    def flow_step(self, n=1):
+        self._check(lib().clb_flow_step(self.h, n))
+
+    def flow_solve(self, max_it, eps, allow_unconverged=False):
+        it = C.c_int(0)
+        st = lib().clb_flow_solve(self.h, max_it, eps, C.byref(it))
+        if not (st == 0 or (allow_unconverged and st == 2)):
+            self._check(st)
+        return it.value, st == 0
+
+    def flow_solve_peclet(self, peclet, char_length, tau_ade_fixed, max_it, eps):
+        dp = C.c_double(0)
+        it = C.c_int(0)
+        st = lib().clb_flow_solve_peclet(self.h, peclet, char_length, tau_ade_fixed, max_it, eps,
+                                         C.byref(dp), C.byref(it))
+        if st not in (0, 2):
+            self._check(st)
+        return dp.value, it.value, st == 0
+
+    def flow_stats(self, char_length=1.0):
+        s = FlowStats()
+        self._check(lib().clb_flow_stats_get(self.h, char_length, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in FlowStats._fields_}
+
+    def velocity(self):
+        u = np.empty(3 * self.N, dtype=np.float64)
+        self._check(lib().clb_get_field(self.h, FIELD_FLOW_VELOCITY, 0, _ptr(u), 0))
+        return u.reshape(3, self.N)
+
+    def flow_populations(self):
+        f = np.empty(19 * self.N, dtype=np.float64)
+        self._check(lib().clb_get_field(self.h, FIELD_FLOW_POPULATIONS, 0, _ptr(f), 0))
+        return f.reshape(19, self.N)
+
+    def set_flow_populations(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        self._check(lib().clb_set_field(self.h, FIELD_FLOW_POPULATIONS, 0, _ptr(f), 0))
+
+    # ---- transport
+    def ade_init(self, species):
+        arr = (SpeciesDesc * len(species))()
+        for k, s in enumerate(species):
+            arr[k] = SpeciesDesc(s["omega_pore"], s.get("omega_biofilm", s["omega_pore"]), s.get("mobile", 1),
+                                 s.get("left_type", NEUMANN), s.get("right_type", NEUMANN),
+                                 s.get("left_bc", 0.0), s.get("right_bc", 0.0), s.get("c0", 0.0))
+        self.S = len(species)
+        self._check(lib().clb_ade_init(self.h, arr, len(species)))
+
+    def couple_velocity(self):
+        self._check(lib().clb_couple_velocity(self.h))
+
+    def set_velocity(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self._check(lib().clb_set_field(self.h, FIELD_ADE_VELOCITY, 0, _ptr(u), 0))
+
+    def set_kinetics(self, law, params, dt):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        self._check(lib().clb_set_kinetics(self.h, law, _ptr(p), p.size, dt))
+
+    def set_biomass(self, b):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        M = b.size // self.N
+        self._check(lib().clb_set_biomass(self.h, M, _ptr(b)))
+
+    def ade_step(self, n=1):
+        self._check(lib().clb_ade_step(self.h, n))
+
+    def concentration(self, s):
+        c = np.empty(self.N, dtype=np.float64)
+        self._check(lib().clb_get_field(self.h, FIELD_CONCENTRATION, s, _ptr(c), 0))
+        return c
+
+    def ade_populations(self, s):
+        g = np.empty(7 * self.N, dtype=np.float64)
+        self._check(lib().clb_get_field(self.h, FIELD_ADE_POPULATIONS, s, _ptr(g), 0))
+        return g.reshape(7, self.N)
+
+    def biomass(self, m):
+        b = np.empty(self.N, dtype=np.float64)
+        self._check(lib().clb_get_field(self.h, FIELD_BIOMASS, m, _ptr(b), 0))
+        return b
+
+    def reduce(self):
+        s = Stats()
+        self._check(lib().clb_reduce(self.h, C.byref(s)))
+        S = self.S
+        return {"total": np.array(s.total[:S]), "content": np.array(s.content[:S]),
+                "biomass": np.array(s.biomass[:]), "min": np.array(s.min_c[:S]), "max": np.array(s.max_c[:S]),
+                "open_voxels": s.open_voxels, "nonfinite": s.nonfinite, "ade_iterations": s.ade_iterations}

@@ -1,0 +1,282 @@
+// api.cu -- the extern "C" surface: handle lifetime, status reporting, field transfer.
+#include "clb_internal.cuh"
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+// Every entry point that uses a handle runs on the handle's device, whatever the calling
+// thread has current.
+#define CLB_ON_DEVICE(h) cudaSetDevice((h)->device)
+
+namespace clb {
+
+static thread_local std::string g_global_err;
+
+clb_status fail(clb_handle* h, clb_status s, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_global_err = msg;
+    return s;
+}
+
+clb_status cuda_check(clb_handle* h, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CLB_OK;
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(h, e == cudaErrorMemoryAllocation ? CLB_OUT_OF_MEMORY : CLB_CUDA_ERROR, m);
+}
+
+// Compacted list of nodes whose class (by material code) is nonzero, in lexicographic order.
+std::vector<int32_t> build_list(const clb_handle* h, const int8_t* cls_by_code) {
+    std::vector<int32_t> list;
+    list.reserve((size_t)h->g.N / 2);
+    for (int64_t n = 0; n < h->g.N; ++n)
+        if (cls_by_code[(uint8_t)h->h_mat[n] & 127]) list.push_back((int32_t)n);
+    return list;
+}
+
+}  // namespace clb
+
+using namespace clb;
+
+extern "C" {
+
+const char* clb_last_error(const clb_handle* h) { return h ? h->err.c_str() : g_global_err.c_str(); }
+const char* clb_global_error(void) { return g_global_err.c_str(); }
+
+clb_status clb_set_device(int device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, CLB_CUDA_ERROR, std::string("set device: ") + cudaGetErrorString(e));
+    return CLB_OK;
+}
+
+clb_status clb_create(const clb_domain_desc* desc, const int8_t* material, clb_handle** out) {
+    if (!desc || !material || !out) return fail(nullptr, CLB_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (desc->nx < 3 || desc->ny < 1 || desc->nz < 1) return fail(nullptr, CLB_INVALID_ARG, "domain too small");
+    const int64_t N = (int64_t)desc->nx * desc->ny * desc->nz;
+    if (N > (int64_t)INT32_MAX / 2) return fail(nullptr, CLB_INVALID_ARG, "domain exceeds 2^30 voxels");
+    if (!(desc->tau > 0.5)) return fail(nullptr, CLB_INVALID_ARG, "tau must exceed 1/2");
+    if (desc->n_microbes < 0 || desc->n_microbes > CLB_MAX_MICROBES)
+        return fail(nullptr, CLB_INVALID_ARG, "microbe count out of range");
+    for (int64_t n = 0; n < N; ++n)
+        if (material[n] < 0) return fail(nullptr, CLB_INVALID_ARG, "negative material code");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(nullptr, CLB_CUDA_ERROR, "no CUDA device");
+    clb_handle* h = new (std::nothrow) clb_handle_s();
+    if (!h) return fail(nullptr, CLB_OUT_OF_MEMORY, "host allocation");
+    h->d = *desc;
+    h->device = dev;
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    h->g.nx = desc->nx;
+    h->g.ny = desc->ny;
+    h->g.nz = desc->nz;
+    h->g.N = N;
+    h->g.plane = desc->ny * desc->nz;
+    h->h_mat.assign(material, material + N);
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_mat, N);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_mat, material, N, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        std::string m = std::string("create: ") + cudaGetErrorString(e);
+        if (h->d_mat) cudaFree(h->d_mat);
+        if (h->stream) cudaStreamDestroy(h->stream);
+        delete h;
+        return fail(nullptr, CLB_CUDA_ERROR, m);
+    }
+    *out = h;
+    return CLB_OK;
+}
+
+clb_status clb_destroy(clb_handle* h) {
+    if (!h) return CLB_OK;
+    cudaStreamSynchronize(h->stream);
+    flow_free(h);
+    ade_free(h);
+    cudaFree(h->d_mat);
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return CLB_OK;
+}
+
+clb_status clb_synchronize(clb_handle* h) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    return cuda_check(h, cudaStreamSynchronize(h->stream), "synchronize");
+}
+
+clb_status clb_set_stream(clb_handle* h, void* stream) {
+    if (!h || !stream) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_check(h, e, "set stream");
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->stream = (cudaStream_t)stream;
+    h->own_stream = false;
+    return CLB_OK;
+}
+
+clb_status clb_get_stream(clb_handle* h, void** stream) {
+    if (!h || !stream) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    *stream = (void*)h->stream;
+    return CLB_OK;
+}
+
+clb_status clb_flow_init(clb_handle* h, double delta_p) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    if (!std::isfinite(delta_p)) return fail(h, CLB_INVALID_ARG, "delta_p not finite");
+    return flow_init(h, delta_p);
+}
+
+clb_status clb_flow_step(clb_handle* h, int n) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
+    if (n < 0) return fail(h, CLB_INVALID_ARG, "negative step count");
+    return flow_step(h, n, false, 0.0);
+}
+
+clb_status clb_flow_solve(clb_handle* h, int max_it, double eps, int* iterations) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
+    if (max_it < 0 || !(eps > 0)) return fail(h, CLB_INVALID_ARG, "bad solve arguments");
+    clb_status s = flow_solve(h, max_it, eps, iterations);
+    if (s == CLB_NOT_CONVERGED) h->err = "flow did not converge within the iteration cap";
+    return s;
+}
+
+clb_status clb_flow_stats_get(clb_handle* h, double char_length, clb_flow_stats* out) {
+    if (!h || !out) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
+    return flow_stats(h, char_length, out);
+}
+
+clb_status clb_flow_solve_peclet(clb_handle* h, double peclet, double char_length, double tau_ade_fixed, int max_it,
+                                 double eps, double* delta_p_out, int* iterations) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
+    int it1 = 0, it2 = 0;
+    clb_status s = flow_solve(h, max_it, eps, &it1);
+    if (s != CLB_OK && s != CLB_NOT_CONVERGED) return s;
+    clb_flow_stats st;
+    clb_status s2 = flow_stats(h, char_length, &st);
+    if (s2 != CLB_OK) return s2;
+    const double nu = (h->d.tau - 0.5) / 3.0;
+    const double d_fixed = 0.25 * (tau_ade_fixed - 0.5);
+    const double u_target = peclet * d_fixed / char_length;
+    if (!(st.permeability > 0)) return fail(h, CLB_PERCOLATION_LOST, "zero permeability: no flow path");
+    const double dp_new = u_target * nu * char_length / st.permeability;
+    if (std::fabs(dp_new - h->delta_p) / h->delta_p > 0.01) {
+        s2 = flow_init(h, dp_new);
+        if (s2 != CLB_OK) return s2;
+        s = flow_solve(h, max_it, eps, &it2);
+        if (s != CLB_OK && s != CLB_NOT_CONVERGED) return s;
+    }
+    if (delta_p_out) *delta_p_out = h->delta_p;
+    if (iterations) *iterations = it1 + it2;
+    if (s == CLB_NOT_CONVERGED) h->err = "flow did not converge within the iteration cap";
+    return s;
+}
+
+clb_status clb_ade_init(clb_handle* h, const clb_species_desc* species, int n_species) {
+    if (!h || !species) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    for (int s = 0; s < n_species; ++s) {
+        const clb_species_desc& sp = species[s];
+        if (sp.mobile && (!(sp.omega_pore > 0 && sp.omega_pore < 2) || !(sp.omega_biofilm > 0 && sp.omega_biofilm < 2)))
+            return fail(h, CLB_INVALID_ARG, "species omega outside (0, 2)");
+        if (sp.left_type < 0 || sp.left_type > 2 || sp.right_type < 0 || sp.right_type > 2)
+            return fail(h, CLB_INVALID_ARG, "unknown face type");
+    }
+    return ade_init(h, species, n_species);
+}
+
+clb_status clb_couple_velocity(clb_handle* h) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    return ade_couple(h);
+}
+
+clb_status clb_set_kinetics(clb_handle* h, int law, const double* params, int n_params, double dt) {
+    if (!h || (n_params > 0 && !params)) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return ade_set_kinetics(h, law, params, n_params, dt);
+}
+
+clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass) {
+    if (!h || (n_microbes > 0 && !biomass)) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return ade_set_biomass(h, n_microbes, biomass);
+}
+
+clb_status clb_ade_step(clb_handle* h, int n) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    if (n < 0) return fail(h, CLB_INVALID_ARG, "negative step count");
+    return ade_step(h, n);
+}
+
+clb_status clb_reduce(clb_handle* h, clb_stats* out) {
+    if (!h || !out) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return ade_reduce(h, out);
+}
+
+clb_status clb_get_field(clb_handle* h, int field, int index, void* host, int dtype) {
+    if (!h || !host) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    const size_t N = (size_t)h->g.N;
+    if (field == CLB_FIELD_MATERIAL) {
+        if (dtype != 2) return fail(h, CLB_INVALID_ARG, "material is int8");
+        std::memcpy(host, h->h_mat.data(), N);
+        return CLB_OK;
+    }
+    if (dtype != 0) return fail(h, CLB_INVALID_ARG, "fields are read as float64");
+    switch (field) {
+        case CLB_FIELD_FLOW_VELOCITY:
+            if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
+            return flow_velocity(h, host, 0, true);
+        case CLB_FIELD_FLOW_POPULATIONS:
+            if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
+            return flow_populations(h, (double*)host);
+        case CLB_FIELD_CONCENTRATION: return ade_density(h, index, (double*)host);
+        case CLB_FIELD_ADE_POPULATIONS: return ade_populations(h, index, (double*)host);
+        case CLB_FIELD_BIOMASS: return ade_biomass(h, index, (double*)host);
+        case CLB_FIELD_ADE_VELOCITY: return ade_velocity(h, (double*)host);
+        default: return fail(h, CLB_INVALID_ARG, "unknown field");
+    }
+}
+
+clb_status clb_set_field(clb_handle* h, int field, int index, const void* host, int dtype) {
+    if (!h || !host) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    if (dtype != 0) return fail(h, CLB_INVALID_ARG, "fields are written as float64");
+    switch (field) {
+        case CLB_FIELD_FLOW_POPULATIONS:
+            if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
+            return flow_set_populations(h, (const double*)host);
+        case CLB_FIELD_ADE_POPULATIONS: return ade_set_populations(h, index, (const double*)host);
+        case CLB_FIELD_ADE_VELOCITY: {
+            if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+            const size_t N = (size_t)h->g.N;
+            const double* src = (const double*)host;
+            if (h->ade_prec == CLB_F64)
+                return cuda_check(h, cudaMemcpy(h->d_u, src, 8 * 3 * N, cudaMemcpyHostToDevice), "u");
+            std::vector<float> tmp(3 * N);
+            for (size_t k = 0; k < 3 * N; ++k) tmp[k] = (float)src[k];
+            return cuda_check(h, cudaMemcpy(h->d_u, tmp.data(), 4 * 3 * N, cudaMemcpyHostToDevice), "u");
+        }
+        case CLB_FIELD_BIOMASS: {
+            if (!h->ade_ready || index < 0 || index >= h->M) return fail(h, CLB_INVALID_ARG, "no such biomass field");
+            return cuda_check(h, cudaMemcpy(h->d_bio + (size_t)index * h->g.N, host, 8 * (size_t)h->g.N,
+                                            cudaMemcpyHostToDevice), "biomass");
+        }
+        default: return fail(h, CLB_INVALID_ARG, "field is read-only");
+    }
+}
+
+}  // extern "C"

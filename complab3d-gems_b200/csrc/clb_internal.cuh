@@ -1,0 +1,193 @@
+// clb_internal.cuh -- shared declarations of the library's translation units.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/clb.h"
+
+namespace clb {
+
+// ------------------------------------------------------------------ lattice constants
+// D3Q19 in Palabos' order: 0 rest, 1..9 the "negative" half, i+9 the opposite of i.
+__host__ __device__ constexpr int q19cx(int i) {
+    return (i == 1 || i == 4 || i == 5 || i == 6 || i == 7) ? -1
+         : (i == 10 || i == 13 || i == 14 || i == 15 || i == 16) ? 1 : 0;
+}
+__host__ __device__ constexpr int q19cy(int i) {
+    return (i == 2 || i == 4 || i == 8 || i == 9 || i == 14) ? -1
+         : (i == 5 || i == 11 || i == 13 || i == 17 || i == 18) ? 1 : 0;
+}
+__host__ __device__ constexpr int q19cz(int i) {
+    return (i == 3 || i == 6 || i == 8 || i == 16 || i == 18) ? -1
+         : (i == 7 || i == 9 || i == 12 || i == 15 || i == 17) ? 1 : 0;
+}
+__host__ __device__ constexpr double q19w(int i) {
+    return i == 0 ? 1.0 / 3.0 : ((i == 1 || i == 2 || i == 3 || i == 10 || i == 11 || i == 12) ? 1.0 / 18.0 : 1.0 / 36.0);
+}
+__host__ __device__ constexpr int q19opp(int i) { return i == 0 ? 0 : (i <= 9 ? i + 9 : i - 9); }
+
+// D3Q7 in Palabos' order: 0 rest, 1..3 = -x,-y,-z, 4..6 = +x,+y,+z.
+__host__ __device__ constexpr int q7cx(int i) { return i == 1 ? -1 : (i == 4 ? 1 : 0); }
+__host__ __device__ constexpr int q7cy(int i) { return i == 2 ? -1 : (i == 5 ? 1 : 0); }
+__host__ __device__ constexpr int q7cz(int i) { return i == 3 ? -1 : (i == 6 ? 1 : 0); }
+__host__ __device__ constexpr double q7w(int i) { return i == 0 ? 0.25 : 0.125; }
+__host__ __device__ constexpr int q7opp(int i) { return i == 0 ? 0 : (i <= 3 ? i + 3 : i - 3); }
+
+// Dynamics classes per material code.
+enum : int8_t { DYN_BB = 0, DYN_NONE = 1, DYN_BGK = 2 };
+enum : int8_t { ADE_BB = 0, ADE_NONE = 1, ADE_PORE = 2, ADE_BIO = 3 };
+
+constexpr int MAX_CODES = 128;  // material codes 0..127 (int8, non-negative)
+constexpr double THRD = 1e-12;  // complab3d_processors.hh:60
+
+// ------------------------------------------------------------------ storage conversion
+template <typename TS, typename TC>
+__device__ __forceinline__ TC ld(const TS* p) { return (TC)(*p); }
+template <>
+__device__ __forceinline__ float ld<__half, float>(const __half* p) { return __half2float(*p); }
+template <typename TS, typename TC>
+__device__ __forceinline__ void st(TS* p, TC v) { *p = (TS)v; }
+template <>
+__device__ __forceinline__ void st<__half, float>(__half* p, float v) { *p = __float2half_rn(v); }
+
+// ------------------------------------------------------------------ geometry of a domain
+struct Geom {
+    int nx, ny, nz;
+    int64_t N;    // nx*ny*nz
+    int plane;    // ny*nz
+};
+
+__device__ __forceinline__ void decode(const Geom& g, int64_t n, int& x, int& y, int& z) {
+    x = (int)(n / g.plane);
+    int r = (int)(n - (int64_t)x * g.plane);
+    y = r / g.nz;
+    z = r - y * g.nz;
+}
+
+// ------------------------------------------------------------------ convergence tracer
+// util::ValueTracer<T>(1, 1000, eps) held on the device so a captured sequence of steps can
+// stop itself: the last block of every step pushes the stored average energy and evaluates
+// the criterion; later steps of the same batch see `converged` and do nothing.
+constexpr int TRACER_WINDOW = 500;
+struct Tracer {
+    double ring[TRACER_WINDOW];
+    double eps;
+    double energy;          // last stored average energy
+    int64_t iterations;     // collide-and-stream calls made
+    int32_t count;          // values in the window
+    int32_t head;           // next slot
+    int32_t enabled;        // 1 while a solve runs
+    int32_t converged;      // set once the criterion holds
+    uint32_t done_blocks;   // completion counter of the running step
+    int32_t pad;
+};
+
+// ------------------------------------------------------------------ flow parameters
+struct FlowParams {
+    Geom g;
+    double omega[MAX_CODES];
+    int8_t dyn[MAX_CODES];
+    double rho_w, rho_e;    // pressure planes
+    int64_t n_bgk;          // nodes that take statistics
+};
+
+// ------------------------------------------------------------------ ADE parameters
+struct AdeParams {
+    Geom g;
+    int S;                  // species
+    int M;                  // microbes with biomass fields
+    int law;
+    double dt;
+    double prm[4 * CLB_MAX_SPECIES];
+    int8_t dyn[MAX_CODES];
+    int8_t react[MAX_CODES];
+    int mobile[CLB_MAX_SPECIES];
+    int slot[CLB_MAX_SPECIES];    // index of a mobile species among the mobile ones, -1 immobile
+    int ltype[CLB_MAX_SPECIES], rtype[CLB_MAX_SPECIES];
+    double lbc[CLB_MAX_SPECIES], rbc[CLB_MAX_SPECIES];
+    double wpore[CLB_MAX_SPECIES], wbio[CLB_MAX_SPECIES];
+    double c0[CLB_MAX_SPECIES];
+};
+
+}  // namespace clb
+
+// ------------------------------------------------------------------ the handle
+struct clb_handle_s {
+    clb_domain_desc d;
+    clb::Geom g;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+    int device = 0;
+    int num_sms = 148;
+    std::string err;
+    std::vector<int8_t> h_mat;
+    int8_t* d_mat = nullptr;
+
+    // flow
+    bool flow_ready = false;
+    int flow_prec = CLB_F32;
+    void* d_f = nullptr;              // [19][N] storage type
+    int32_t* d_flow_list = nullptr;   // active (collide or stream) nodes, lexicographic
+    int64_t n_flow_list = 0;
+    clb::FlowParams fp;
+    clb::Tracer* d_tracer = nullptr;
+    double* d_partials = nullptr;     // per-block partial sums (scratch)
+    int partial_cap = 0;
+    int flow_grid = 0;
+    int64_t flow_iters = 0;           // host mirror of the device iteration count
+    double delta_p = 0;
+
+    // transport
+    bool ade_ready = false;
+    int ade_prec = CLB_F32;
+    int S = 0, n_mobile = 0, M = 0;
+    std::vector<clb_species_desc> species;
+    void* d_g = nullptr;              // [n_mobile][7][N] storage type
+    double* d_imm = nullptr;          // [S][N] immobile concentrations (unused rows stay empty)
+    double* d_bio = nullptr;          // [M][N] biomass
+    float* d_u = nullptr;             // [3][N] advection velocity
+    int32_t* d_ade_list = nullptr;
+    int64_t n_ade_list = 0;
+    double* d_neu = nullptr;          // [S][2][ny*nz] stored boundary densities
+    clb::AdeParams ap;
+    int64_t ade_iters = 0;
+    int ade_grid = 0;
+};
+
+namespace clb {
+// error helpers (api.cu)
+clb_status fail(clb_handle* h, clb_status s, const std::string& msg);
+clb_status cuda_check(clb_handle* h, cudaError_t e, const char* what);
+
+// flow.cu
+clb_status flow_init(clb_handle* h, double delta_p);
+clb_status flow_step(clb_handle* h, int n, bool trace, double eps);
+clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations);
+clb_status flow_stats(clb_handle* h, double char_length, clb_flow_stats* out);
+clb_status flow_velocity(clb_handle* h, void* dst, int dtype_device, bool to_host);
+clb_status flow_populations(clb_handle* h, double* host);
+clb_status flow_set_populations(clb_handle* h, const double* host);
+void flow_free(clb_handle* h);
+
+// ade.cu
+clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S);
+clb_status ade_step(clb_handle* h, int n);
+clb_status ade_couple(clb_handle* h);
+clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm, double dt);
+clb_status ade_set_biomass(clb_handle* h, int M, const double* b);
+clb_status ade_density(clb_handle* h, int s, double* host);
+clb_status ade_populations(clb_handle* h, int s, double* host);
+clb_status ade_set_populations(clb_handle* h, int s, const double* host);
+clb_status ade_biomass(clb_handle* h, int m, double* host);
+clb_status ade_velocity(clb_handle* h, double* host);
+clb_status ade_reduce(clb_handle* h, clb_stats* out);
+void ade_free(clb_handle* h);
+
+// list building (api.cu)
+std::vector<int32_t> build_list(const clb_handle* h, const int8_t* cls_by_code);
+}  // namespace clb

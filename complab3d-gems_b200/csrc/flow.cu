@@ -1,0 +1,607 @@
+// flow.cu -- D3Q19 incompressible BGK flow lattice on the AA in-place pattern.
+//
+// Reference behaviour (Palabos dynamics installed by NSdomainSetup,
+// complab_functions.hh:296-345, driven by complab.cpp:1095-1206):
+//   IncBGK collision with per-material omega (pore, biofilm: omega_bio =
+//   1/(permRatio (1/omega - 1/2) + 1/2), :323), BounceBack walls (full-way: populations are
+//   held one step in the wall node), NoDynamics solids (no collision, populations stream
+//   through), Palabos' local regularized density boundary on the planes x = 0 (rho = 1) and
+//   x = nx-1 (rho = 1 - 3 dP), reflection of populations whose source lies outside the box.
+//
+// Layout: populations direction-major f[19][N] (N = nx*ny*nz, x slowest, z fastest) of the
+// storage type; one array, updated in place with the AA pattern:
+//   even step: node x reads f[i][x], collides, writes outgoing i to f[opp(i)][x];
+//   odd step:  node x reads incoming i from f[opp(i)][x - c_i], collides, writes outgoing
+//              i to f[i][x + c_i].
+// Each slot is read and written by exactly one node per step, so a step needs no second
+// array and no synchronisation. A bounce-back node is a no-op in both steps (its swap is the
+// identity on its AA slots), so only collide-or-stream nodes are launched: a compacted list
+// of them, in lexicographic order. A source or destination outside the box maps to the node's
+// own opposite slot, which is Palabos' reflection at the block edge.
+//
+// Algorithmic bytes per node update: 2 * 19 * sizeof(storage) (+1 byte material, +4 bytes
+// list index that count against the roofline fraction).
+#include "clb_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace clb {
+
+constexpr int FLOW_THREADS = 256;
+
+template <typename TC>
+__device__ __forceinline__ TC feq19(int i, TC rb, TC jx, TC jy, TC jz, TC jsq) {
+    TC cj = (TC)q19cx(i) * jx + (TC)q19cy(i) * jy + (TC)q19cz(i) * jz;
+    return (TC)q19w(i) * (rb + (TC)3 * cj + (TC)1.5 * ((TC)3 * cj * cj - jsq));
+}
+
+// Palabos' regularized density boundary on the x planes (direction 0, orientation o):
+// j_x = o (rb_0 + 2 rb_n - rb), j_y = j_z = 0, Pi_neq from the known populations with the
+// off-equilibrium parts of the normal ones counted twice, then f_i = feq_i + fneq_i(Pi).
+template <typename TC>
+__device__ __forceinline__ void regularize19(TC (&g)[19], int orient, TC rb) {
+    TC r0 = 0, rn = 0;
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        if (q19cx(i) == 0) r0 += g[i];
+        else if (q19cx(i) == orient) rn += g[i];
+    }
+    const TC jx = (TC)orient * (r0 + (TC)2 * rn - rb);
+    const TC jsq = jx * jx;
+    TC pxx = 0, pxy = 0, pxz = 0, pyy = 0, pyz = 0, pzz = 0;
+#pragma unroll
+    for (int i = 1; i < 19; ++i) {
+        const int cx = q19cx(i);
+        if (cx == -orient) continue;
+        const TC fac = (cx == 0) ? (TC)1 : (TC)2;
+        const TC fneq = fac * (g[i] - feq19<TC>(i, rb, jx, (TC)0, (TC)0, jsq));
+        pxx += (TC)(q19cx(i) * q19cx(i)) * fneq;
+        pxy += (TC)(q19cx(i) * q19cy(i)) * fneq;
+        pxz += (TC)(q19cx(i) * q19cz(i)) * fneq;
+        pyy += (TC)(q19cy(i) * q19cy(i)) * fneq;
+        pyz += (TC)(q19cy(i) * q19cz(i)) * fneq;
+        pzz += (TC)(q19cz(i) * q19cz(i)) * fneq;
+    }
+    const TC third = (TC)1 / (TC)3;
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        const TC cx = q19cx(i), cy = q19cy(i), cz = q19cz(i);
+        TC s = (cx * cx - third) * pxx + (cy * cy - third) * pyy + (cz * cz - third) * pzz +
+               (TC)2 * (cx * cy * pxy + cx * cz * pxz + cy * cz * pyz);
+        g[i] = feq19<TC>(i, rb, jx, (TC)0, (TC)0, jsq) + (TC)q19w(i) * (TC)4.5 * s;
+    }
+}
+
+template <typename TS, typename TC, bool ODD>
+__device__ __forceinline__ void load19(const TS* __restrict__ f, int64_t N, const Geom& G, int64_t n, int x, int y,
+                                       int z, TC (&g)[19]) {
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        if (!ODD || i == 0) {
+            g[i] = ld<TS, TC>(f + (int64_t)i * N + n);
+        } else {
+            const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i);
+            const bool in = (cx == 0 || ((unsigned)(x - cx) < (unsigned)G.nx)) &&
+                            (cy == 0 || ((unsigned)(y - cy) < (unsigned)G.ny)) &&
+                            (cz == 0 || ((unsigned)(z - cz) < (unsigned)G.nz));
+            const int64_t off = (int64_t)cx * G.plane + cy * G.nz + cz;
+            g[i] = in ? ld<TS, TC>(f + (int64_t)q19opp(i) * N + n - off) : ld<TS, TC>(f + (int64_t)i * N + n);
+        }
+    }
+}
+
+template <typename TS, typename TC, bool ODD>
+__device__ __forceinline__ void store19(TS* __restrict__ f, int64_t N, const Geom& G, int64_t n, int x, int y, int z,
+                                        const TC (&o)[19]) {
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        if (!ODD || i == 0) {
+            st<TS, TC>(f + (int64_t)q19opp(i) * N + n, o[i]);
+        } else {
+            const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i);
+            const bool in = (cx == 0 || ((unsigned)(x + cx) < (unsigned)G.nx)) &&
+                            (cy == 0 || ((unsigned)(y + cy) < (unsigned)G.ny)) &&
+                            (cz == 0 || ((unsigned)(z + cz) < (unsigned)G.nz));
+            const int64_t off = (int64_t)cx * G.plane + cy * G.nz + cz;
+            if (in) st<TS, TC>(f + (int64_t)i * N + n + off, o[i]);
+            else st<TS, TC>(f + (int64_t)q19opp(i) * N + n, o[i]);
+        }
+    }
+}
+
+// Block-wide FP64 sum; result valid in thread 0.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += sh[k];
+    __syncthreads();
+    return r;
+}
+
+// The last block of a step turns the partial sums into the stored average energy and runs
+// the tracer. Deterministic: fixed grid, fixed reduction order.
+__device__ void finish_step(Tracer* tr, double* partials, double block_total, int64_t n_bgk, int trace) {
+    __shared__ bool s_last;
+    __shared__ double sh[32];
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = block_total;
+        __threadfence();
+        unsigned t = atomicAdd(&tr->done_blocks, 1u);
+        s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double v = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) v += ((volatile double*)partials)[k];
+    double tot = block_sum(v, sh);
+    __shared__ double s_energy, s_mean;
+    __shared__ int s_count;
+    if (threadIdx.x == 0) {
+        double e = n_bgk > 0 ? 0.5 * tot / (double)n_bgk : 0.0;
+        tr->energy = e;
+        tr->iterations += 1;
+        tr->done_blocks = 0;
+        s_energy = e;
+        s_count = 0;
+        if (trace) {
+            tr->ring[tr->head] = e;
+            tr->head = (tr->head + 1) % TRACER_WINDOW;
+            if (tr->count < TRACER_WINDOW) tr->count += 1;
+            s_count = tr->count;
+        }
+    }
+    __syncthreads();
+    if (!trace || s_count < TRACER_WINDOW) return;
+    v = 0;
+    for (int k = threadIdx.x; k < TRACER_WINDOW; k += blockDim.x) v += tr->ring[k];
+    double sum = block_sum(v, sh);
+    if (threadIdx.x == 0) s_mean = sum / (double)TRACER_WINDOW;
+    __syncthreads();
+    v = 0;
+    for (int k = threadIdx.x; k < TRACER_WINDOW; k += blockDim.x) {
+        double d = tr->ring[k] - s_mean;
+        v += d * d;
+    }
+    double sq = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        double sd = sqrt(sq / (double)(TRACER_WINDOW - 1));
+        double r = sd / s_mean;
+        if (isnan(r) || fabs(r) < tr->eps) tr->converged = 1;
+    }
+    (void)s_energy;
+}
+
+template <typename TS, typename TC, bool ODD>
+__global__ void __launch_bounds__(FLOW_THREADS)
+    k_flow_aa(TS* __restrict__ f, const int32_t* __restrict__ list, int64_t nlist, const int8_t* __restrict__ mat,
+              const FlowParams P, Tracer* __restrict__ tr, double* __restrict__ partials, int trace) {
+    if (trace && tr->converged) return;  // a batch continues past convergence as no-ops
+    const Geom G = P.g;
+    const int64_t N = G.N;
+    double esum = 0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nlist; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n = list[k];
+        int x, y, z;
+        decode(G, n, x, y, z);
+        const int code = mat[n];
+        TC g[19];
+        load19<TS, TC, ODD>(f, N, G, n, x, y, z, g);
+        if (P.dyn[code] == DYN_BGK) {
+            if (x == 0) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
+            else if (x == G.nx - 1) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
+            TC rb = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                rb += g[i];
+                jx += (TC)q19cx(i) * g[i];
+                jy += (TC)q19cy(i) * g[i];
+                jz += (TC)q19cz(i) * g[i];
+            }
+            const TC jsq = jx * jx + jy * jy + jz * jz;
+            const TC w = (TC)P.omega[code];
+            const TC omw = (TC)1 - w;
+#pragma unroll
+            for (int i = 0; i < 19; ++i) g[i] = g[i] * omw + w * feq19<TC>(i, rb, jx, jy, jz, jsq);
+            esum += (double)jsq;
+        }
+        store19<TS, TC, ODD>(f, N, G, n, x, y, z, g);
+    }
+    __shared__ double sh[32];
+    double bt = block_sum(esum, sh);
+    finish_step(tr, partials, bt, P.n_bgk, trace);
+}
+
+// PressureGradient equilibrium (complab_functions.hh:82-94): BGK nodes t_i (rho(x) - 1),
+// every other node zero (BounceBack / NoDynamics equilibria are zero).
+template <typename TS>
+__global__ void k_flow_init(TS* __restrict__ f, const int8_t* __restrict__ mat, const FlowParams P, double delta_p) {
+    const Geom G = P.g;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(n / G.plane);
+        const double rho = 1.0 - delta_p * 3.0 / (double)(G.nx - 1) * (double)x;
+        const bool bgk = P.dyn[mat[n]] == DYN_BGK;
+#pragma unroll
+        for (int i = 0; i < 19; ++i) {
+            double v = bgk ? q19w(i) * (rho - 1.0) : 0.0;
+            if constexpr (std::is_same<TS, __half>::value) f[(int64_t)i * G.N + n] = __double2half(v);
+            else f[(int64_t)i * G.N + n] = (TS)v;
+        }
+    }
+}
+
+// computeVelocity of every node: BGK u = j; pressure-plane BGK nodes (j_x from the known
+// populations, 0, 0); others 0. The incoming populations are gathered with the parity rule,
+// which holds for unlaunched bounce-back nodes too.
+template <typename TS, typename TC, typename TO>
+__global__ void k_flow_velocity(const TS* __restrict__ f, const int8_t* __restrict__ mat, const FlowParams P, int odd,
+                                TO* __restrict__ u) {
+    const Geom G = P.g;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, z;
+        decode(G, n, x, y, z);
+        TC g[19];
+        if (odd) load19<TS, TC, true>(f, G.N, G, n, x, y, z, g);
+        else load19<TS, TC, false>(f, G.N, G, n, x, y, z, g);
+        TC jx = 0, jy = 0, jz = 0;
+        if (P.dyn[mat[n]] == DYN_BGK) {
+            if (x == 0 || x == G.nx - 1) {
+                const int o = (x == 0) ? -1 : 1;
+                const TC rb = (TC)((x == 0 ? P.rho_w : P.rho_e) - 1.0);
+                TC r0 = 0, rn = 0;
+#pragma unroll
+                for (int i = 0; i < 19; ++i) {
+                    if (q19cx(i) == 0) r0 += g[i];
+                    else if (q19cx(i) == o) rn += g[i];
+                }
+                jx = (TC)o * (r0 + (TC)2 * rn - rb);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 19; ++i) {
+                    jx += (TC)q19cx(i) * g[i];
+                    jy += (TC)q19cy(i) * g[i];
+                    jz += (TC)q19cz(i) * g[i];
+                }
+            }
+        }
+        u[n] = (TO)jx;
+        u[G.N + n] = (TO)jy;
+        u[2 * G.N + n] = (TO)jz;
+    }
+}
+
+// Incoming populations in natural layout, or back from it (scatter through the parity rule).
+template <typename TS>
+__global__ void k_flow_get_pops(const TS* __restrict__ f, const FlowParams P, int odd, double* __restrict__ out) {
+    const Geom G = P.g;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, z;
+        decode(G, n, x, y, z);
+        double g[19];
+        if constexpr (std::is_same<TS, double>::value) {
+            if (odd) load19<TS, double, true>(f, G.N, G, n, x, y, z, g);
+            else load19<TS, double, false>(f, G.N, G, n, x, y, z, g);
+        } else {
+            float h[19];
+            if (odd) load19<TS, float, true>(f, G.N, G, n, x, y, z, h);
+            else load19<TS, float, false>(f, G.N, G, n, x, y, z, h);
+            for (int i = 0; i < 19; ++i) g[i] = h[i];
+        }
+        for (int i = 0; i < 19; ++i) out[(int64_t)i * G.N + n] = g[i];
+    }
+}
+
+template <typename TS>
+__global__ void k_flow_set_pops(TS* __restrict__ f, const FlowParams P, int odd, const double* __restrict__ in) {
+    const Geom G = P.g;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, z;
+        decode(G, n, x, y, z);
+        for (int i = 0; i < 19; ++i) {
+            int64_t slot = (int64_t)i * G.N + n;
+            if (odd && i != 0) {
+                const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i);
+                const bool inb = ((unsigned)(x - cx) < (unsigned)G.nx) && ((unsigned)(y - cy) < (unsigned)G.ny) &&
+                                 ((unsigned)(z - cz) < (unsigned)G.nz);
+                const int64_t off = (int64_t)cx * G.plane + cy * G.nz + cz;
+                if (inb) slot = (int64_t)q19opp(i) * G.N + n - off;
+            }
+            double v = in[(int64_t)i * G.N + n];
+            if constexpr (std::is_same<TS, __half>::value) f[slot] = __double2half(v);
+            else f[slot] = (TS)v;
+        }
+    }
+}
+
+// FP64 plane / volume statistics of the velocity field (complab.cpp:1136-1160).
+__global__ void k_flow_vstats(const double* __restrict__ u, const Geom G, double* __restrict__ acc) {
+    // acc[0] sum |u| over x=1..nx-2, acc[1] max u_x (as ordered bits), acc[2] sum u_x on x=nx-2
+    __shared__ double sh[32];
+    double s_norm = 0, s_out = 0, m = -1e300;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(n / G.plane);
+        if (x < 1 || x > G.nx - 2) continue;
+        const double ux = u[n], uy = u[G.N + n], uz = u[2 * G.N + n];
+        s_norm += sqrt(ux * ux + uy * uy + uz * uz);
+        m = fmax(m, ux);
+        if (x == G.nx - 2) s_out += ux;
+    }
+    double a = block_sum(s_norm, sh);
+    double b = block_sum(s_out, sh);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    __shared__ double smax[32];
+    if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mm = -1e300;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) mm = fmax(mm, smax[k]);
+        atomicAdd(&acc[0], a);
+        atomicAdd(&acc[2], b);
+        // max of doubles via the ordered-integer trick
+        long long bits = __double_as_longlong(mm);
+        long long key = bits >= 0 ? bits : (bits ^ 0x7fffffffffffffffLL);
+        atomicMax((long long*)&acc[1], key);
+    }
+}
+
+// ------------------------------------------------------------------ host side
+
+static size_t storage_size(int prec) { return prec == CLB_F64 ? 8 : (prec == CLB_F32 ? 4 : 2); }
+
+template <typename F>
+static int grid_for(clb_handle* h, F kernel, int threads) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    if (per_sm < 1) per_sm = 1;
+    return h->num_sms * per_sm;
+}
+
+void flow_free(clb_handle* h) {
+    cudaFree(h->d_f); h->d_f = nullptr;
+    cudaFree(h->d_flow_list); h->d_flow_list = nullptr;
+    cudaFree(h->d_tracer); h->d_tracer = nullptr;
+    cudaFree(h->d_partials); h->d_partials = nullptr;
+    h->flow_ready = false;
+}
+
+clb_status flow_init(clb_handle* h, double delta_p) {
+    const clb_domain_desc& d = h->d;
+    FlowParams& P = h->fp;
+    std::memset(&P, 0, sizeof(P));
+    P.g = h->g;
+    const double omega = 1.0 / d.tau;
+    // NSdomainSetup: IncBGK(omega) everywhere, pore codes IncBGK, bounce-back, no-dynamics,
+    // biofilm IncBGK(omega_bio) or BounceBack when impermeable.
+    for (int c = 0; c < MAX_CODES; ++c) { P.dyn[c] = DYN_BGK; P.omega[c] = omega; }
+    if (d.bounce_back_code >= 0 && d.bounce_back_code < MAX_CODES) P.dyn[d.bounce_back_code] = DYN_BB;
+    if (d.solid_code >= 0 && d.solid_code < MAX_CODES) P.dyn[d.solid_code] = DYN_NONE;
+    for (int m = 0; m < d.n_microbes; ++m) {
+        int c = d.bio_codes[m];
+        if (c < 0 || c >= MAX_CODES) continue;
+        if (d.perm_ratio[m] > 1e-14) {
+            P.dyn[c] = DYN_BGK;
+            P.omega[c] = 1.0 / (d.perm_ratio[m] * (1.0 / omega - 0.5) + 0.5);
+        } else {
+            P.dyn[c] = DYN_BB;
+        }
+    }
+    P.rho_w = 1.0;
+    P.rho_e = 1.0 - delta_p * 3.0;
+    h->delta_p = delta_p;
+    int64_t nbgk = 0;
+    for (int64_t n = 0; n < h->g.N; ++n) nbgk += (P.dyn[(uint8_t)h->h_mat[n]] == DYN_BGK);
+    P.n_bgk = nbgk;
+
+    int8_t cls[MAX_CODES];
+    for (int c = 0; c < MAX_CODES; ++c) cls[c] = (P.dyn[c] != DYN_BB);
+    std::vector<int32_t> list = build_list(h, cls);
+
+    flow_free(h);
+    h->flow_prec = d.flow_precision;
+    const size_t es = storage_size(h->flow_prec);
+    cudaError_t e;
+    if ((e = cudaMalloc(&h->d_f, es * 19 * (size_t)h->g.N)) != cudaSuccess) return cuda_check(h, e, "flow populations");
+    if ((e = cudaMalloc(&h->d_flow_list, sizeof(int32_t) * std::max<size_t>(1, list.size()))) != cudaSuccess)
+        return cuda_check(h, e, "flow list");
+    if ((e = cudaMalloc(&h->d_tracer, sizeof(Tracer))) != cudaSuccess) return cuda_check(h, e, "tracer");
+    h->n_flow_list = (int64_t)list.size();
+    if (!list.empty())
+        cudaMemcpyAsync(h->d_flow_list, list.data(), sizeof(int32_t) * list.size(), cudaMemcpyHostToDevice, h->stream);
+    cudaMemsetAsync(h->d_tracer, 0, sizeof(Tracer), h->stream);
+
+    int grid = 0;
+    switch (h->flow_prec) {
+        case CLB_F64: grid = grid_for(h, k_flow_aa<double, double, false>, FLOW_THREADS); break;
+        case CLB_F32: grid = grid_for(h, k_flow_aa<float, float, false>, FLOW_THREADS); break;
+        default: grid = grid_for(h, k_flow_aa<__half, float, false>, FLOW_THREADS); break;
+    }
+    h->flow_grid = grid;
+    if ((e = cudaMalloc(&h->d_partials, sizeof(double) * grid)) != cudaSuccess) return cuda_check(h, e, "partials");
+    h->partial_cap = grid;
+
+    const int ig = h->num_sms * 8;
+    switch (h->flow_prec) {
+        case CLB_F64: k_flow_init<double><<<ig, 256, 0, h->stream>>>((double*)h->d_f, h->d_mat, P, delta_p); break;
+        case CLB_F32: k_flow_init<float><<<ig, 256, 0, h->stream>>>((float*)h->d_f, h->d_mat, P, delta_p); break;
+        default: k_flow_init<__half><<<ig, 256, 0, h->stream>>>((__half*)h->d_f, h->d_mat, P, delta_p); break;
+    }
+    h->flow_iters = 0;
+    h->flow_ready = true;
+    return cuda_check(h, cudaGetLastError(), "flow init");
+}
+
+static void launch_flow(clb_handle* h, bool odd, int trace) {
+    const FlowParams& P = h->fp;
+    const int grid = h->flow_grid;
+#define CLB_LAUNCH(TS, TC)                                                                                        \
+    if (odd)                                                                                                      \
+        k_flow_aa<TS, TC, true><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, h->d_flow_list, h->n_flow_list, \
+                                                                       h->d_mat, P, h->d_tracer, h->d_partials, trace); \
+    else                                                                                                          \
+        k_flow_aa<TS, TC, false><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, h->d_flow_list, h->n_flow_list, \
+                                                                        h->d_mat, P, h->d_tracer, h->d_partials, trace);
+    switch (h->flow_prec) {
+        case CLB_F64: CLB_LAUNCH(double, double); break;
+        case CLB_F32: CLB_LAUNCH(float, float); break;
+        default: CLB_LAUNCH(__half, float); break;
+    }
+#undef CLB_LAUNCH
+}
+
+clb_status flow_step(clb_handle* h, int n, bool trace, double eps) {
+    (void)eps;
+    for (int k = 0; k < n; ++k) {
+        launch_flow(h, (h->flow_iters & 1) != 0, trace ? 1 : 0);
+        h->flow_iters += 1;
+    }
+    return cuda_check(h, cudaGetLastError(), "flow step");
+}
+
+clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations) {
+    // a fresh util::ValueTracer: empty window, new epsilon
+    Tracer t0;
+    std::memset(&t0, 0, sizeof(t0));
+    Tracer cur;
+    cudaError_t e = cudaMemcpyAsync(&cur, h->d_tracer, sizeof(Tracer), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_check(h, e, "tracer read");
+    t0.eps = eps;
+    t0.iterations = cur.iterations;
+    t0.energy = cur.energy;
+    cudaMemcpyAsync(h->d_tracer, &t0, sizeof(Tracer), cudaMemcpyHostToDevice, h->stream);
+    const int64_t start = cur.iterations;
+    int done = 0;
+    int chunk = 64;
+    bool conv = false;
+    while (done < max_it) {
+        int k = std::min(chunk, max_it - done);
+        clb_status s = flow_step(h, k, true, eps);
+        if (s != CLB_OK) return s;
+        done += k;
+        e = cudaMemcpyAsync(&cur, h->d_tracer, sizeof(Tracer), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return cuda_check(h, e, "tracer read");
+        if (cur.converged) { conv = true; break; }
+        if (chunk < 1024) chunk *= 2;
+    }
+    h->flow_iters = cur.iterations;  // steps after convergence were no-ops
+    if (iterations) *iterations = (int)(cur.iterations - start);
+    // leave the tracer disabled for plain steps
+    int zero = 0;
+    cudaMemcpyAsync(&h->d_tracer->converged, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+    return conv ? CLB_OK : CLB_NOT_CONVERGED;
+}
+
+clb_status flow_velocity(clb_handle* h, void* dst, int dtype_device, bool to_host) {
+    const FlowParams& P = h->fp;
+    const int odd = (int)(h->flow_iters & 1);
+    void* out = dst;
+    const size_t es = dtype_device == 0 ? 8 : 4;
+    if (to_host) {
+        cudaError_t e = cudaMalloc(&out, es * 3 * (size_t)h->g.N);
+        if (e != cudaSuccess) return cuda_check(h, e, "velocity buffer");
+    }
+    const int grid = h->num_sms * 8;
+#define CLB_VEL(TS, TC)                                                                                           \
+    if (dtype_device == 0) k_flow_velocity<TS, TC, double><<<grid, 256, 0, h->stream>>>((const TS*)h->d_f, h->d_mat, P, odd, (double*)out); \
+    else k_flow_velocity<TS, TC, float><<<grid, 256, 0, h->stream>>>((const TS*)h->d_f, h->d_mat, P, odd, (float*)out);
+    switch (h->flow_prec) {
+        case CLB_F64: CLB_VEL(double, double); break;
+        case CLB_F32: CLB_VEL(float, float); break;
+        default: CLB_VEL(__half, float); break;
+    }
+#undef CLB_VEL
+    if (to_host) {
+        cudaError_t e = cudaMemcpyAsync(dst, out, es * 3 * (size_t)h->g.N, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        cudaFree(out);
+        if (e != cudaSuccess) return cuda_check(h, e, "velocity copy");
+    }
+    return cuda_check(h, cudaGetLastError(), "flow velocity");
+}
+
+clb_status flow_populations(clb_handle* h, double* host) {
+    double* buf = nullptr;
+    cudaError_t e = cudaMalloc(&buf, sizeof(double) * 19 * (size_t)h->g.N);
+    if (e != cudaSuccess) return cuda_check(h, e, "population buffer");
+    const int odd = (int)(h->flow_iters & 1);
+    const int grid = h->num_sms * 8;
+    switch (h->flow_prec) {
+        case CLB_F64: k_flow_get_pops<double><<<grid, 256, 0, h->stream>>>((const double*)h->d_f, h->fp, odd, buf); break;
+        case CLB_F32: k_flow_get_pops<float><<<grid, 256, 0, h->stream>>>((const float*)h->d_f, h->fp, odd, buf); break;
+        default: k_flow_get_pops<__half><<<grid, 256, 0, h->stream>>>((const __half*)h->d_f, h->fp, odd, buf); break;
+    }
+    e = cudaMemcpyAsync(host, buf, sizeof(double) * 19 * (size_t)h->g.N, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(buf);
+    return cuda_check(h, e, "population copy");
+}
+
+clb_status flow_set_populations(clb_handle* h, const double* host) {
+    double* buf = nullptr;
+    cudaError_t e = cudaMalloc(&buf, sizeof(double) * 19 * (size_t)h->g.N);
+    if (e != cudaSuccess) return cuda_check(h, e, "population buffer");
+    e = cudaMemcpyAsync(buf, host, sizeof(double) * 19 * (size_t)h->g.N, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) { cudaFree(buf); return cuda_check(h, e, "population copy"); }
+    const int odd = (int)(h->flow_iters & 1);
+    const int grid = h->num_sms * 8;
+    switch (h->flow_prec) {
+        case CLB_F64: k_flow_set_pops<double><<<grid, 256, 0, h->stream>>>((double*)h->d_f, h->fp, odd, buf); break;
+        case CLB_F32: k_flow_set_pops<float><<<grid, 256, 0, h->stream>>>((float*)h->d_f, h->fp, odd, buf); break;
+        default: k_flow_set_pops<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_f, h->fp, odd, buf); break;
+    }
+    e = cudaStreamSynchronize(h->stream);
+    cudaFree(buf);
+    return cuda_check(h, e, "set populations");
+}
+
+clb_status flow_stats(clb_handle* h, double char_length, clb_flow_stats* out) {
+    double* u = nullptr;
+    double* acc = nullptr;
+    cudaError_t e = cudaMalloc(&u, sizeof(double) * 3 * (size_t)h->g.N);
+    if (e != cudaSuccess) return cuda_check(h, e, "stats buffer");
+    e = cudaMalloc(&acc, sizeof(double) * 3);
+    if (e != cudaSuccess) { cudaFree(u); return cuda_check(h, e, "stats buffer"); }
+    clb_status s = flow_velocity(h, u, 0, false);
+    if (s != CLB_OK) { cudaFree(u); cudaFree(acc); return s; }
+    double init[3] = {0.0, 0.0, 0.0};
+    long long neg = (long long)0x8000000000000000ULL;  // below every ordered key
+    std::memcpy(&init[1], &neg, sizeof(double));
+    cudaMemcpyAsync(acc, init, sizeof(init), cudaMemcpyHostToDevice, h->stream);
+    k_flow_vstats<<<h->num_sms * 4, 256, 0, h->stream>>>(u, h->g, acc);
+    double r[3];
+    Tracer t;
+    cudaMemcpyAsync(r, acc, sizeof(r), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(&t, h->d_tracer, sizeof(Tracer), cudaMemcpyDeviceToHost, h->stream);
+    e = cudaStreamSynchronize(h->stream);
+    cudaFree(u);
+    cudaFree(acc);
+    if (e != cudaSuccess) return cuda_check(h, e, "stats");
+    long long key;
+    std::memcpy(&key, &r[1], sizeof(key));
+    long long bits = key >= 0 ? key : (key ^ 0x7fffffffffffffffLL);
+    double mx;
+    std::memcpy(&mx, &bits, sizeof(mx));
+    const int64_t inner = (int64_t)(h->g.nx - 2) * h->g.plane;
+    out->pore_mean_u = r[0] / (double)inner;
+    out->pore_max_ux = mx;
+    out->darcy_outlet_ux = r[2] / (double)h->g.plane;
+    const double nu = (h->d.tau - 0.5) / 3.0;
+    out->permeability = h->delta_p != 0 ? out->darcy_outlet_ux * nu * char_length / h->delta_p : 0.0;
+    out->energy = t.energy;
+    out->iterations = t.iterations;
+    out->bgk_nodes = h->fp.n_bgk;
+    out->active_nodes = h->n_flow_list;
+    return CLB_OK;
+}
+
+}  // namespace clb

@@ -1,0 +1,245 @@
+/* clb.h -- C ABI of the B200-native CompLaB3D reactive-transport step.
+ *
+ * One opaque handle owns every device buffer of one domain. Host buffers passed in are
+ * copied; no pointer is retained across calls. Calls enqueue on the handle's CUDA stream
+ * and return a clb_status; clb_last_error() gives the message of the last failure. No call
+ * aborts the process or throws across the ABI.
+ *
+ * Layouts. Every per-voxel array is lexicographic with x slowest and z fastest:
+ * index(x,y,z) = (x*ny + y)*nz + z -- the order of the reference's serial processor loops
+ * (iX outer, iZ inner). nx counts the two ghost x-planes that the reference adds when it
+ * reads a geometry (complab_functions.hh:999, readGeometry :178-207). Population arrays are
+ * direction-major [q][N] in Palabos' velocity order, shifted by the lattice weights
+ * (f_i - t_i), as Palabos stores them.
+ *
+ * Each entry point names the reference interface it replaces (paths inside the
+ * CompLaB3D-GEMS project).
+ */
+#ifndef CLB_H
+#define CLB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum clb_status {
+    CLB_OK = 0,
+    CLB_INVALID_ARG = 1,
+    CLB_NOT_CONVERGED = 2,
+    CLB_NONFINITE = 3,
+    CLB_PERCOLATION_LOST = 4,
+    CLB_CUDA_ERROR = 5,
+    CLB_TIMEOUT = 6,
+    CLB_NOT_INITIALIZED = 7,
+    CLB_OUT_OF_MEMORY = 8
+} clb_status;
+
+/* Storage precision of lattice populations. Arithmetic is FP64 for CLB_F64 and FP32 for
+ * the two others. CLB_F16S stores the Palabos shifted populations f - t_i in IEEE half. */
+typedef enum clb_precision { CLB_F64 = 0, CLB_F32 = 1, CLB_F16S = 2 } clb_precision;
+
+/* x-face boundary kinds of an advection-diffusion species (complab_functions.hh:404-438). */
+typedef enum clb_face { CLB_DIRICHLET = 0, CLB_NEUMANN = 1, CLB_CLOSED = 2 } clb_face;
+
+/* Rate laws compiled into the library (the reference compiles defineRxnKinetics /
+ * defineAbioticRxnKinetics from config/kinetics/ into its binary). */
+typedef enum clb_law {
+    CLB_LAW_NONE = 0,
+    CLB_LAW_DECAY = 1,      /* params k[S]:          R_s = -k_s C_s                        */
+    CLB_LAW_MONOD = 2,      /* params k[S], Ks[S]:   R_s = -k_s C_s / (Ks_s + C_s)           */
+    CLB_LAW_DUAL_MONOD = 3  /* params mu_max, Ks, Y, kd; microbe m grows on species 0 (donor)
+                               and species 1+m (acceptor):
+                               growth = mu_max C0/(Ks+C0) Ca/(Ks+Ca) B_m,
+                               R_B = growth - kd B_m, R_0 -= growth/Y, R_a -= growth/Y     */
+} clb_law;
+
+#define CLB_MAX_MICROBES 8
+#define CLB_MAX_PORE_CODES 8
+#define CLB_MAX_SPECIES 16
+
+/* The material-number surface of CompLaB.xml <material_numbers> plus the flow relaxation
+ * (complab_functions.hh:1213-1285, NSdomainSetup :296-345). */
+typedef struct clb_domain_desc {
+    int32_t nx, ny, nz;           /* lattice size, ghost x-planes included                  */
+    int32_t flow_precision;       /* clb_precision of the D3Q19 lattice                      */
+    int32_t ade_precision;        /* clb_precision of the D3Q7 lattices                      */
+    int32_t solid_code;           /* <solid>: NoDynamics on the flow lattice; -1 if none     */
+    int32_t bounce_back_code;     /* <bounce_back>: inert wall; -1 if none                   */
+    int32_t n_pore_codes;
+    int32_t pore_codes[CLB_MAX_PORE_CODES];
+    int32_t n_microbes;           /* biofilm material numbers, one per microbe               */
+    int32_t bio_codes[CLB_MAX_MICROBES];
+    double perm_ratio[CLB_MAX_MICROBES]; /* biofilm omega = 1/(r (1/omega - 1/2) + 1/2);
+                                            r <= 1e-14 makes that biofilm bounce-back      */
+    double tau;                   /* flow relaxation time                                    */
+} clb_domain_desc;
+
+/* One advection-diffusion species (soluteDomainSetup, complab_functions.hh:347-442;
+ * relaxation rates as complab.cpp:1230-1253 derives them). */
+typedef struct clb_species_desc {
+    double omega_pore;
+    double omega_biofilm;
+    int32_t mobile;               /* 0: immobile -- never collides or streams               */
+    int32_t left_type, right_type;/* clb_face                                                */
+    double left_bc, right_bc;     /* Dirichlet values                                        */
+    double c0;                    /* initial and background concentration                    */
+} clb_species_desc;
+
+typedef struct clb_flow_stats {
+    double pore_mean_u;           /* mean |u| over x = 1..nx-2 (complab.cpp:1150)            */
+    double pore_max_ux;           /* max u_x over x = 1..nx-2                                */
+    double darcy_outlet_ux;       /* mean u_x over the plane x = nx-2                        */
+    double permeability;          /* darcy_outlet_ux * nu * L / dP (complab.cpp:1160)        */
+    double energy;                /* last stored average energy (half the mean |u|^2)       */
+    int64_t iterations;           /* collide-and-stream calls made so far                    */
+    int64_t bgk_nodes;            /* nodes that collide (pore + permeable biofilm)           */
+    int64_t active_nodes;         /* nodes the step launches (BGK + no-dynamics)             */
+} clb_flow_stats;
+
+typedef struct clb_stats {
+    double total[CLB_MAX_SPECIES];   /* sum of concentration over x=1..nx-2, open voxels     */
+    double content[CLB_MAX_SPECIES]; /* sum over every node of (sum of populations + 1)      */
+    double biomass[CLB_MAX_MICROBES];/* sum of biomass over x=1..nx-2                        */
+    double min_c[CLB_MAX_SPECIES], max_c[CLB_MAX_SPECIES];
+    int64_t open_voxels;             /* pore + biofilm voxels in x=1..nx-2                   */
+    int64_t nonfinite;               /* non-finite concentrations found                      */
+    int64_t ade_iterations;
+} clb_stats;
+
+/* Field identifiers for clb_get_field / clb_set_field. dtype: 0 = float64, 1 = float32,
+ * 2 = int8. */
+typedef enum clb_field {
+    CLB_FIELD_MATERIAL = 0,       /* int8 [N]                                                */
+    CLB_FIELD_FLOW_VELOCITY = 1,  /* [3][N]  computeVelocity of the flow lattice            */
+    CLB_FIELD_FLOW_POPULATIONS = 2, /* [19][N] incoming (post-stream) populations            */
+    CLB_FIELD_CONCENTRATION = 3,  /* [N] of species `index`: computeDensity                  */
+    CLB_FIELD_ADE_POPULATIONS = 4,/* [7][N] of species `index`                               */
+    CLB_FIELD_BIOMASS = 5,        /* [N] of microbe `index`                                  */
+    CLB_FIELD_ADE_VELOCITY = 6    /* [3][N] the advection velocity the species see          */
+} clb_field;
+
+typedef struct clb_handle_s clb_handle;
+
+/* ---------------------------------------------------------------- lifetime */
+
+/* Selects the CUDA device that later clb_create calls on this thread allocate on (the library
+ * carries its own CUDA runtime, so a device chosen through another runtime is not seen). */
+clb_status clb_set_device(int device);
+
+/* Allocates the domain on the current CUDA device and uploads the material map.
+ * Replaces: MultiScalarField3D<int> geometry + readGeometry (complab.cpp:1051-1052). */
+clb_status clb_create(const clb_domain_desc* desc, const int8_t* material, clb_handle** out);
+clb_status clb_destroy(clb_handle* h);
+const char* clb_last_error(const clb_handle* h);
+/* Message of the last failure of a call that had no handle to record it in. */
+const char* clb_global_error(void);
+clb_status clb_synchronize(clb_handle* h);
+
+/* Every call of the handle enqueues on this stream (a cudaStream_t). By default the handle
+ * owns a non-blocking stream; a caller that times or orders work with its own stream passes it
+ * here (the handle then never destroys it). */
+clb_status clb_set_stream(clb_handle* h, void* stream);
+clb_status clb_get_stream(clb_handle* h, void** stream);
+
+/* ---------------------------------------------------------------- flow (D3Q19) */
+
+/* Dynamics from the material map, pressure planes at x=0 (rho=1) and x=nx-1
+ * (rho=1-3 dP), PressureGradient equilibrium initial state.
+ * Replaces: NSdomainSetup (complab_functions.hh:296-345). */
+clb_status clb_flow_init(clb_handle* h, double delta_p);
+
+/* n x nsLattice.collideAndStream() (complab.cpp:1120-1124 loop body). */
+clb_status clb_flow_step(clb_handle* h, int n);
+
+/* Runs collideAndStream until util::ValueTracer(1,1000,eps) on the stored average energy
+ * converges or max_it calls are made (complab.cpp:1113-1124). *iterations receives the
+ * number of collideAndStream calls made. Returns CLB_NOT_CONVERGED at the cap. */
+clb_status clb_flow_solve(clb_handle* h, int max_it, double eps, int* iterations);
+
+/* Velocity statistics and permeability (complab.cpp:1136-1160). */
+clb_status clb_flow_stats_get(clb_handle* h, double char_length, clb_flow_stats* out);
+
+/* The Peclet rescale of complab.cpp:1156-1179: permeability from the solved field, the
+ * pressure drop that gives u = Pe D / L with D = (tau_ade_fixed - 1/2)/4, and a re-solve
+ * from a fresh initial state when that drop differs by more than 1 %. *delta_p_out
+ * receives the drop in use afterwards. */
+clb_status clb_flow_solve_peclet(clb_handle* h, double peclet, double char_length,
+                                 double tau_ade_fixed, int max_it, double eps,
+                                 double* delta_p_out, int* iterations);
+
+/* ---------------------------------------------------------------- transport (D3Q7) */
+
+/* Species lattices at equilibrium at c0, wall/solid nodes seeded at c0, x faces as
+ * described. Replaces: soluteDomainSetup (complab_functions.hh:347-442) and the wall
+ * seeding of complab.cpp:1506-1656. */
+clb_status clb_ade_init(clb_handle* h, const clb_species_desc* species, int n_species);
+
+/* Copies the flow velocity into the species' advection field.
+ * Replaces: latticeToPassiveAdvDiff (complab.cpp:2014, 3119). */
+clb_status clb_couple_velocity(clb_handle* h);
+
+/* Selects the compiled rate law and the time step used for dC = R dt.
+ * Replaces: run_kinetics + update_rxnLattices (complab3d_processors_part1.hh:85-187,
+ * 406-497) with the clamp dC = max(R dt, -C). */
+clb_status clb_set_kinetics(clb_handle* h, int law, const double* params, int n_params, double dt);
+
+/* Biomass fields of the CA microbes, [n_microbes][N] float64. */
+clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass);
+
+/* n transport iterations: collide every mobile species, kinetics, deposit, stream, Neumann
+ * planes (complab.cpp:2307-2315, 2340-2452, 3251-3259), fused in one pass per step. */
+clb_status clb_ade_step(clb_handle* h, int n);
+
+/* FP64 reductions over the live fields (complab3d_processors_part3.hh:387-600). */
+clb_status clb_reduce(clb_handle* h, clb_stats* out);
+
+/* ---------------------------------------------------------------- fields */
+
+clb_status clb_get_field(clb_handle* h, int field, int index, void* host, int dtype);
+clb_status clb_set_field(clb_handle* h, int field, int index, const void* host, int dtype);
+
+/* ---------------------------------------------------------------- geometry (host) */
+
+/* complab_geom::GenOptions (complab3d_geometry.hh:111-120). */
+typedef struct clb_geom_options {
+    const char* kind;             /* channel, spheres, cylinders, random, fracture, layered  */
+    double porosity, radius, aperture, roughness;
+    int32_t count, layers;
+    uint64_t seed;
+    const char* walls;            /* "y", "yz", "none", ...                                  */
+} clb_geom_options;
+
+/* complab_geom::generate (complab3d_geometry.hh:138-200): the same voxels for the same
+ * options. Output in this library's layout (x slowest) of an nx*ny*nz grid. */
+clb_status clb_geom_generate(const clb_geom_options* opt, int nx, int ny, int nz, int8_t* out);
+
+/* Porosity-targeted sphere pack: spheres with radius uniform in [rmin, rmax] and centres
+ * uniform in the box, drawn from the reference's xorshift64* stream, are carved as `grain`
+ * until the open fraction reaches `porosity`; then walls (code `wall`) on the listed axes. */
+clb_status clb_geom_sphere_pack(int nx, int ny, int nz, double porosity, double rmin, double rmax,
+                                uint64_t seed, const char* walls, int grain, int wall, int pore,
+                                int8_t* out);
+
+/* readGeometry (complab_functions.hh:178-207): a .dat file of nx_inner slices (x slowest,
+ * z fastest) into an (nx_inner+2)*ny*nz map whose ghost planes duplicate slices 1 and
+ * nx_inner. */
+clb_status clb_geom_read_dat(const char* path, int nx_inner, int ny, int nz, int8_t* out);
+
+typedef struct clb_inspection {
+    double porosity;
+    int64_t open_voxels, isolated_voxels;
+    int32_t clusters, spanning_clusters, percolates, quasi_2d;
+} clb_inspection;
+
+/* complab_geom::inspect (complab3d_geometry.hh:287-355) on a map in this library's layout:
+ * open = code >= 2, 6-connected clusters, spanning = touches x=0 and x=nx-1. */
+clb_status clb_geom_inspect(const int8_t* map, int nx, int ny, int nz, clb_inspection* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLB_H */

@@ -1,0 +1,633 @@
+/* lbm_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+ *
+ * An FP64 CPU restatement of CompLaB3D's coupled reactive-transport step (flow lattice,
+ * per-species advection-diffusion lattices, kinetics increments), used only as the parity
+ * checker by tests/, by __graft_entry__.smoke(), and as the timed CPU baseline by bench.py.
+ * It is never linked into, called by, or shipped with the product library.
+ *
+ * The LBM arithmetic itself lives in Palabos 2.3.0 (not vendored with the reference). What
+ * is restated here follows the reference's call sites and the published Palabos algorithms:
+ *
+ *   flow lattice  (complab_functions.hh:296-345 NSdomainSetup)
+ *     - IncBGKdynamics: f_i <- (1-w) f_i + w t_i (rb + 3 c.j + 4.5 (c.j)^2 - 1.5 j^2),
+ *       populations stored shifted by t_i, u = j (incompressible, rho0 = 1).
+ *     - BounceBack: the collision swaps opposite populations (full-way bounce-back;
+ *       populations are held one step inside the wall node).
+ *     - NoDynamics: no collision; populations still stream.
+ *     - pressure planes x=0 (rho=1) and x=nx-1 (rho=1-3 dP): Palabos' local regularized
+ *       density boundary (createLocalBoundaryCondition3D + addPressureBoundary0N/0P):
+ *       j_x = orient (rb_0 + 2 rb_n - rb), j_y = j_z = 0, Pi_neq from the known
+ *       populations with bounce-back of off-equilibrium parts, f_i = feq_i + fneq_i(Pi),
+ *       then the wrapped IncBGK collision.  Wrapping a bounce-back or no-dynamics node is a
+ *       no-op in Palabos (their equilibrium is zero and regularize() does nothing), so the
+ *       boundary acts on BGK nodes only.
+ *     - edges of the box along y and z: Palabos' swap streaming leaves a population whose
+ *       source lies outside the block in the node's own opposite slot (reflection).
+ *     - PressureGradient initial state (complab_functions.hh:82-94).
+ *     - statistics: the mean of |u|^2 over BGK nodes gathered during the collision;
+ *       getStoredAverageEnergy returns half that mean.
+ *     - util::ValueTracer(u=1, L=1000, eps): window deltaT = L/u/2 = 500 values,
+ *       converged when the window is full and stddev/mean < eps (sample stddev, n-1).
+ *       Driven exactly as complab.cpp:1120-1124 does.
+ *
+ *   advection-diffusion lattices  (complab_functions.hh:347-442 soluteDomainSetup,
+ *   complab.cpp:1380-1393, 1506-1656)
+ *     - AdvectionDiffusionBGKdynamics (D3Q7, t0=1/4, ti=1/8, cs2=1/4):
+ *       g_i <- (1-w) g_i + w t_i (rb + 4 c_i.(rho u)), u the external (flow) velocity.
+ *     - per-voxel omega: pore vs biofilm (complab.cpp:1244-1253).
+ *     - solid and wall voxels of a mobile species are BounceBack seeded at c0
+ *       (complab.cpp:1589-1656, stabilizeADElattice3D part3.hh:261-311).
+ *     - x faces: 0 Dirichlet, 1 Neumann, 2 closed (complab_functions.hh:404-438).
+ *       Dirichlet/Neumann: the single unknown population is completed so the node's
+ *       density equals the stored value (Palabos AdvectionDiffusionBoundaryDynamics);
+ *       Neumann stores the inner neighbour's density after every stream
+ *       (FlatAdiabaticBoundaryFunctional3D, an integrated processor run by stream()).
+ *       Closed: the whole plane becomes BounceBack after initialisation.
+ *     - step order (complab.cpp:2307-2315, 2340-2452, 3251-3259): collide all mobile
+ *       species, kinetics on the post-collision densities, deposit dC*t_i, stream.
+ *     - kinetics (part1.hh:85-187, 406-497): x in 1..nx-2, mask not solid/wall;
+ *       C < 1e-12 is read as 0; dC = R dt; clamp dC = max(R dt, -C)
+ *       (complab3d_processors_symbolic.hh:165-180); applied only if |dC| > 1e-12;
+ *       biomass never negative (ibid. :193).
+ */
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ---------------------------------------------------------------- D3Q19 (Palabos order)
+const int Q19 = 19;
+const int C19[19][3] = {
+    {0, 0, 0},
+    {-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {-1, -1, 0}, {-1, 1, 0}, {-1, 0, -1},
+    {-1, 0, 1}, {0, -1, -1}, {0, -1, 1},
+    {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {1, -1, 0}, {1, 0, 1},
+    {1, 0, -1}, {0, 1, 1}, {0, 1, -1}};
+const double T19[19] = {
+    1.0 / 3,
+    1.0 / 18, 1.0 / 18, 1.0 / 18, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36,
+    1.0 / 18, 1.0 / 18, 1.0 / 18, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36};
+inline int opp19(int i) { return i == 0 ? 0 : (i <= 9 ? i + 9 : i - 9); }
+
+// ---------------------------------------------------------------- D3Q7 (Palabos order)
+const int Q7 = 7;
+const int C7[7][3] = {{0, 0, 0}, {-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+const double T7[7] = {0.25, 0.125, 0.125, 0.125, 0.125, 0.125, 0.125};
+inline int opp7(int i) { return i == 0 ? 0 : (i <= 3 ? i + 3 : i - 3); }
+
+const double THRD = 1e-12;  // complab3d_processors.hh:60
+
+enum { DYN_BB = 0, DYN_NONE = 1, DYN_BGK = 2 };
+
+inline double feq19(int i, double rb, const double j[3], double jsq) {
+    double cj = C19[i][0] * j[0] + C19[i][1] * j[1] + C19[i][2] * j[2];
+    return T19[i] * (rb + 3.0 * cj + 1.5 * (3.0 * cj * cj - jsq));
+}
+
+int g_threads = 1;
+
+struct Tracer {  // util::ValueTracer<T>(1, 1000, eps)
+    int deltaT = 500;
+    double eps = 1e-6;
+    std::vector<double> v;
+    void take(double x) {
+        v.push_back(x);
+        if ((int)v.size() > deltaT) v.erase(v.begin());
+    }
+    bool converged() const {
+        if ((int)v.size() < deltaT) return false;
+        double s = 0;
+        for (double x : v) s += x;
+        double avg = s / (double)v.size();
+        double sq = 0;
+        for (double x : v) sq += (x - avg) * (x - avg);
+        double sd = std::sqrt(sq / (double)(v.size() - 1));
+        double r = sd / avg;
+        if (std::isnan(r)) return true;  // "simulation diverged" also ends the loop
+        return std::fabs(r) < eps;
+    }
+};
+
+}  // namespace
+
+// =====================================================================================
+//                                   FLOW LATTICE
+// =====================================================================================
+struct OrcFlow {
+    int nx, ny, nz;
+    size_t N;
+    std::vector<double> f, fp;  // [N][19]
+    std::vector<int8_t> mat;
+    int dyn[256];
+    double omega[256];
+    double rho_w, rho_e;
+    double energy = 0;
+    long iters = 0;
+    Tracer tr;
+    size_t id(int x, int y, int z) const { return ((size_t)x * ny + y) * nz + z; }
+};
+
+extern "C" {
+
+void orc_set_threads(int n) {
+    g_threads = n > 0 ? n : 1;
+#ifdef _OPENMP
+    omp_set_num_threads(g_threads);
+#endif
+}
+
+int orc_max_threads() {
+#ifdef _OPENMP
+    return omp_get_num_procs();
+#else
+    return 1;
+#endif
+}
+
+OrcFlow* orc_flow_create(int nx, int ny, int nz, const int8_t* mat, const int32_t* dyn_by_code,
+                         const double* omega_by_code, double delta_p) {
+    OrcFlow* F = new OrcFlow();
+    F->nx = nx; F->ny = ny; F->nz = nz;
+    F->N = (size_t)nx * ny * nz;
+    F->mat.assign(mat, mat + F->N);
+    for (int k = 0; k < 256; ++k) { F->dyn[k] = dyn_by_code[k]; F->omega[k] = omega_by_code[k]; }
+    F->rho_w = 1.0;
+    F->rho_e = 1.0 - delta_p * 3.0;
+    F->f.assign(F->N * Q19, 0.0);
+    F->fp.assign(F->N * Q19, 0.0);
+    // initializeAtEquilibrium(PressureGradient): rho(x) = 1 - dP*invCs2/(nx-1)*x, u = 0.
+    // BounceBack / NoDynamics return a zero equilibrium, i.e. shifted populations 0.
+    for (int x = 0; x < nx; ++x) {
+        double rho = 1.0 - delta_p * 3.0 / (double)(nx - 1) * (double)x;
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = F->id(x, y, z);
+                if (F->dyn[(uint8_t)F->mat[n]] != DYN_BGK) continue;
+                for (int i = 0; i < Q19; ++i) F->f[n * Q19 + i] = T19[i] * (rho - 1.0);
+            }
+    }
+    return F;
+}
+
+void orc_flow_destroy(OrcFlow* F) { delete F; }
+
+static void flow_collide_stream(OrcFlow* F) {
+    const int nx = F->nx, ny = F->ny, nz = F->nz;
+    double esum = 0;
+    long ecnt = 0;
+    // ---- collision (all nodes)
+#pragma omp parallel for reduction(+ : esum, ecnt) schedule(static)
+    for (int x = 0; x < nx; ++x) {
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = F->id(x, y, z);
+                double* c = &F->f[n * Q19];
+                double* o = &F->fp[n * Q19];
+                int d = F->dyn[(uint8_t)F->mat[n]];
+                if (d == DYN_NONE) {
+                    for (int i = 0; i < Q19; ++i) o[i] = c[i];
+                    continue;
+                }
+                if (d == DYN_BB) {
+                    for (int i = 0; i < Q19; ++i) o[i] = c[opp19(i)];
+                    continue;
+                }
+                double w = F->omega[(uint8_t)F->mat[n]];
+                double g[19];
+                for (int i = 0; i < Q19; ++i) g[i] = c[i];
+                if (x == 0 || x == nx - 1) {
+                    // regularized density boundary, direction 0, orientation -1 (west) / +1 (east)
+                    int orient = (x == 0) ? -1 : 1;
+                    double rb = ((x == 0) ? F->rho_w : F->rho_e) - 1.0;
+                    double r0 = 0, rn = 0;
+                    for (int i = 0; i < Q19; ++i) {
+                        if (C19[i][0] == 0) r0 += g[i];
+                        else if (C19[i][0] == orient) rn += g[i];
+                    }
+                    double j[3] = {orient * (r0 + 2.0 * rn - rb), 0.0, 0.0};
+                    double jsq = j[0] * j[0];
+                    double pi[6] = {0, 0, 0, 0, 0, 0};  // xx xy xz yy yz zz
+                    for (int i = 0; i < Q19; ++i) {
+                        double fac;
+                        if (C19[i][0] == 0) fac = 1.0;
+                        else if (C19[i][0] == orient) fac = 2.0;
+                        else continue;
+                        double fneq = (i == 0 && C19[i][0] == orient) ? 0.0 : g[i] - feq19(i, rb, j, jsq);
+                        int p = 0;
+                        for (int a = 0; a < 3; ++a)
+                            for (int b = a; b < 3; ++b) pi[p++] += fac * C19[i][a] * C19[i][b] * fneq;
+                    }
+                    for (int i = 0; i < Q19; ++i) {
+                        double s = 0;
+                        int p = 0;
+                        for (int a = 0; a < 3; ++a)
+                            for (int b = a; b < 3; ++b) {
+                                double q = C19[i][a] * C19[i][b];
+                                if (a == b) q -= 1.0 / 3.0;
+                                else q *= 2.0;
+                                s += q * pi[p++];
+                            }
+                        g[i] = feq19(i, rb, j, jsq) + T19[i] * 9.0 / 2.0 * s;
+                    }
+                }
+                double rb = 0, j[3] = {0, 0, 0};
+                for (int i = 0; i < Q19; ++i) {
+                    rb += g[i];
+                    j[0] += C19[i][0] * g[i];
+                    j[1] += C19[i][1] * g[i];
+                    j[2] += C19[i][2] * g[i];
+                }
+                double jsq = j[0] * j[0] + j[1] * j[1] + j[2] * j[2];
+                for (int i = 0; i < Q19; ++i) o[i] = g[i] * (1.0 - w) + w * feq19(i, rb, j, jsq);
+                esum += jsq;
+                ecnt += 1;
+            }
+    }
+    // ---- streaming (pull form of Palabos' swap streaming; out-of-block sources reflect)
+#pragma omp parallel for schedule(static)
+    for (int x = 0; x < nx; ++x) {
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = F->id(x, y, z);
+                double* dst = &F->f[n * Q19];
+                dst[0] = F->fp[n * Q19];
+                for (int i = 1; i < Q19; ++i) {
+                    int sx = x - C19[i][0], sy = y - C19[i][1], sz = z - C19[i][2];
+                    if (sx < 0 || sy < 0 || sz < 0 || sx >= nx || sy >= ny || sz >= nz)
+                        dst[i] = F->fp[n * Q19 + opp19(i)];
+                    else
+                        dst[i] = F->fp[F->id(sx, sy, sz) * Q19 + i];
+                }
+            }
+    }
+    F->energy = ecnt > 0 ? 0.5 * esum / (double)ecnt : 0.0;
+    F->iters += 1;
+}
+
+void orc_flow_step(OrcFlow* F, int n) {
+    for (int k = 0; k < n; ++k) flow_collide_stream(F);
+}
+
+double orc_flow_energy(OrcFlow* F) { return F->energy; }
+long orc_flow_iterations(OrcFlow* F) { return F->iters; }
+
+/* complab.cpp:1120-1124: for (; iT < max; ++iT) { collideAndStream(); takeValue(energy);
+ * if (hasConverged()) break; }.  Returns the number of collideAndStream calls made. */
+int orc_flow_solve(OrcFlow* F, int max_it, double eps) {
+    F->tr = Tracer();
+    F->tr.eps = eps;
+    int k = 0;
+    for (; k < max_it;) {
+        flow_collide_stream(F);
+        ++k;
+        F->tr.take(F->energy);
+        if (F->tr.converged()) break;
+    }
+    return k;
+}
+
+/* computeVelocity: BGK nodes u = j; density-boundary nodes u = (j_x from the known
+ * populations, 0, 0); BounceBack and NoDynamics nodes report zero. */
+void orc_flow_velocity(OrcFlow* F, double* u) {
+    const int nx = F->nx, ny = F->ny, nz = F->nz;
+    const size_t N = F->N;
+#pragma omp parallel for schedule(static)
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = F->id(x, y, z);
+                const double* g = &F->f[n * Q19];
+                double j[3] = {0, 0, 0};
+                if (F->dyn[(uint8_t)F->mat[n]] == DYN_BGK) {
+                    if (x == 0 || x == nx - 1) {
+                        int orient = (x == 0) ? -1 : 1;
+                        double rb = ((x == 0) ? F->rho_w : F->rho_e) - 1.0;
+                        double r0 = 0, rn = 0;
+                        for (int i = 0; i < Q19; ++i) {
+                            if (C19[i][0] == 0) r0 += g[i];
+                            else if (C19[i][0] == orient) rn += g[i];
+                        }
+                        j[0] = orient * (r0 + 2.0 * rn - rb);
+                    } else {
+                        for (int i = 0; i < Q19; ++i)
+                            for (int a = 0; a < 3; ++a) j[a] += C19[i][a] * g[i];
+                    }
+                }
+                u[n] = j[0];
+                u[N + n] = j[1];
+                u[2 * N + n] = j[2];
+            }
+}
+
+/* Palabos populations as stored (shifted by t_i), direction-major [19][N]. */
+void orc_flow_populations(OrcFlow* F, double* out) {
+    for (size_t n = 0; n < F->N; ++n)
+        for (int i = 0; i < Q19; ++i) out[(size_t)i * F->N + n] = F->f[n * Q19 + i];
+}
+
+void orc_flow_set_populations(OrcFlow* F, const double* in) {
+    for (size_t n = 0; n < F->N; ++n)
+        for (int i = 0; i < Q19; ++i) F->f[n * Q19 + i] = in[(size_t)i * F->N + n];
+}
+
+}  // extern "C"
+
+// =====================================================================================
+//                           ADVECTION-DIFFUSION LATTICES
+// =====================================================================================
+enum { ADE_BB = 0, ADE_NONE = 1, ADE_PORE = 2, ADE_BIO = 3 };
+enum { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_CLOSED = 2 };
+enum { LAW_NONE = 0, LAW_DECAY = 1, LAW_MONOD = 2, LAW_DUAL_MONOD = 3 };
+
+struct OrcAde {
+    int nx, ny, nz, S, M;
+    size_t N;
+    std::vector<int8_t> mat;
+    int dyn[256];       // ADE_* per material code (mobile species)
+    int react[256];     // 1 where kinetics runs (mask not solid / wall)
+    std::vector<double> wpore, wbio, c0, lbc, rbc;
+    std::vector<int> mobile, ltype, rtype;
+    std::vector<double> u;                 // [3][N]
+    std::vector<std::vector<double>> g, gp;  // per species [N][7]
+    std::vector<std::vector<double>> imm;   // immobile species: concentration [N]
+    std::vector<double> bio;                // biomass [M][N]
+    std::vector<double> lstore, rstore;     // stored boundary densities [S][ny*nz]
+    int law = LAW_NONE;
+    std::vector<double> prm;
+    double dt = 1.0;
+    long iters = 0;
+    size_t id(int x, int y, int z) const { return ((size_t)x * ny + y) * nz + z; }
+    // the lattice dynamics of species s at node n
+    int node_dyn(int s, int x, size_t n) const {
+        if ((x == 0 && ltype[s] == BC_CLOSED) || (x == nx - 1 && rtype[s] == BC_CLOSED)) return ADE_BB;
+        return dyn[(uint8_t)mat[n]];
+    }
+};
+
+extern "C" {
+
+OrcAde* orc_ade_create(int nx, int ny, int nz, const int8_t* mat, int S, const int32_t* dyn_by_code,
+                       const int32_t* react_by_code, const double* omega_pore, const double* omega_bio,
+                       const int32_t* mobile, const int32_t* left_type, const int32_t* right_type,
+                       const double* left_bc, const double* right_bc, const double* c0, const double* u) {
+    OrcAde* A = new OrcAde();
+    A->nx = nx; A->ny = ny; A->nz = nz; A->S = S; A->M = 0;
+    A->N = (size_t)nx * ny * nz;
+    A->mat.assign(mat, mat + A->N);
+    for (int k = 0; k < 256; ++k) { A->dyn[k] = dyn_by_code[k]; A->react[k] = react_by_code[k]; }
+    A->wpore.assign(omega_pore, omega_pore + S);
+    A->wbio.assign(omega_bio, omega_bio + S);
+    A->mobile.assign(mobile, mobile + S);
+    A->ltype.assign(left_type, left_type + S);
+    A->rtype.assign(right_type, right_type + S);
+    A->lbc.assign(left_bc, left_bc + S);
+    A->rbc.assign(right_bc, right_bc + S);
+    A->c0.assign(c0, c0 + S);
+    A->u.assign(u, u + 3 * A->N);
+    A->g.resize(S);
+    A->gp.resize(S);
+    A->imm.resize(S);
+    const size_t P = (size_t)ny * nz;
+    A->lstore.assign((size_t)S * P, 0.0);
+    A->rstore.assign((size_t)S * P, 0.0);
+    for (int s = 0; s < S; ++s) {
+        double c = c0[s];
+        if (c < THRD && c > -THRD) c = 0;  // stabilizeADElattice3D
+        if (!mobile[s]) {
+            A->imm[s].assign(A->N, c0[s]);
+            continue;
+        }
+        // every node at equilibrium at c0 with u = 0 (initializeAtEquilibrium for BGK nodes,
+        // stabilizeADElattice3D for wall and solid nodes); closed planes keep these values.
+        A->g[s].assign(A->N * Q7, 0.0);
+        A->gp[s].assign(A->N * Q7, 0.0);
+        for (size_t n = 0; n < A->N; ++n)
+            for (int i = 0; i < Q7; ++i) A->g[s][n * Q7 + i] = T7[i] * (c - 1.0);
+        for (size_t p = 0; p < P; ++p) {
+            A->lstore[(size_t)s * P + p] = left_type[s] == BC_DIRICHLET ? left_bc[s] : c0[s];
+            A->rstore[(size_t)s * P + p] = right_type[s] == BC_DIRICHLET ? right_bc[s] : c0[s];
+        }
+    }
+    return A;
+}
+
+void orc_ade_destroy(OrcAde* A) { delete A; }
+
+/* law parameters:
+ *   LAW_DECAY:      k[S]                      R_s = -k_s C_s
+ *   LAW_MONOD:      k[S], Ks[S]               R_s = -k_s C_s / (Ks_s + C_s)
+ *   LAW_DUAL_MONOD: mu_max, Ks, Y, kd         per microbe m (biomass field m):
+ *                   growth = mu_max * C0/(Ks+C0) * Ca/(Ks+Ca) * B_m,  a = 1 + m
+ *                   R_B = growth - kd B_m;  R_0 -= growth / Y;  R_a -= growth / Y */
+void orc_ade_set_kinetics(OrcAde* A, int law, const double* prm, int nprm, double dt) {
+    A->law = law;
+    A->prm.assign(prm, prm + nprm);
+    A->dt = dt;
+}
+
+void orc_ade_set_biomass(OrcAde* A, int M, const double* b) {
+    A->M = M;
+    A->bio.assign(b, b + (size_t)M * A->N);
+}
+
+static void rates(const OrcAde* A, const double* C, const double* B, double* R, double* RB) {
+    const int S = A->S;
+    for (int s = 0; s < S; ++s) R[s] = 0;
+    for (int m = 0; m < A->M; ++m) RB[m] = 0;
+    switch (A->law) {
+        case LAW_DECAY:
+            for (int s = 0; s < S; ++s) R[s] = -A->prm[s] * C[s];
+            break;
+        case LAW_MONOD:
+            for (int s = 0; s < S; ++s) R[s] = -A->prm[s] * C[s] / (A->prm[S + s] + C[s]);
+            break;
+        case LAW_DUAL_MONOD: {
+            double mu = A->prm[0], ks = A->prm[1], Y = A->prm[2], kd = A->prm[3];
+            for (int m = 0; m < A->M; ++m) {
+                int a = 1 + m;
+                if (a >= S) break;
+                double Bm = B[m];
+                if (Bm <= 0.0) continue;
+                double growth = mu * (C[0] / (ks + C[0])) * (C[a] / (ks + C[a])) * Bm;
+                RB[m] += growth - kd * Bm;
+                R[0] -= growth / Y;
+                R[a] -= growth / Y;
+            }
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+static void ade_step(OrcAde* A) {
+    const int nx = A->nx, ny = A->ny, nz = A->nz, S = A->S;
+    const size_t N = A->N, P = (size_t)ny * nz;
+    // ---- 1. collide every mobile species
+    for (int s = 0; s < S; ++s) {
+        if (!A->mobile[s]) continue;
+        std::vector<double>& G = A->g[s];
+        std::vector<double>& GP = A->gp[s];
+#pragma omp parallel for schedule(static)
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    size_t n = A->id(x, y, z);
+                    const double* c = &G[n * Q7];
+                    double* o = &GP[n * Q7];
+                    int d = A->node_dyn(s, x, n);
+                    if (d == ADE_NONE) { for (int i = 0; i < Q7; ++i) o[i] = c[i]; continue; }
+                    if (d == ADE_BB) { for (int i = 0; i < Q7; ++i) o[i] = c[opp7(i)]; continue; }
+                    double w = (d == ADE_BIO) ? A->wbio[s] : A->wpore[s];
+                    double gg[7];
+                    for (int i = 0; i < Q7; ++i) gg[i] = c[i];
+                    if (x == 0 || x == nx - 1) {
+                        // AdvectionDiffusionBoundaryDynamics: complete the inward population
+                        double rs = (x == 0 ? A->lstore[(size_t)s * P + (size_t)y * nz + z]
+                                            : A->rstore[(size_t)s * P + (size_t)y * nz + z]) - 1.0;
+                        int miss = (x == 0) ? 4 : 1;
+                        double sum = 0;
+                        for (int i = 0; i < Q7; ++i) if (i != miss) sum += gg[i];
+                        gg[miss] = rs - sum;
+                    }
+                    double rb = 0;
+                    for (int i = 0; i < Q7; ++i) rb += gg[i];
+                    double rho = rb + 1.0;
+                    double je[3] = {rho * A->u[n], rho * A->u[N + n], rho * A->u[2 * N + n]};
+                    for (int i = 0; i < Q7; ++i) {
+                        double cj = C7[i][0] * je[0] + C7[i][1] * je[1] + C7[i][2] * je[2];
+                        o[i] = gg[i] * (1.0 - w) + w * (T7[i] * (rb + 4.0 * cj));
+                    }
+                }
+    }
+    // ---- 2. kinetics on post-collision densities, deposit t_i dC (update_rxnLattices)
+    if (A->law != LAW_NONE) {
+#pragma omp parallel for schedule(static)
+        for (int x = 1; x < nx - 1; ++x) {
+            std::vector<double> C(S), R(S), B(A->M + 1), RB(A->M + 1);
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    size_t n = A->id(x, y, z);
+                    if (!A->react[(uint8_t)A->mat[n]]) continue;
+                    for (int s = 0; s < S; ++s) {
+                        double c;
+                        if (A->mobile[s]) {
+                            c = 0;
+                            for (int i = 0; i < Q7; ++i) c += A->gp[s][n * Q7 + i];
+                            c += 1.0;
+                        } else {
+                            c = A->imm[s][n];
+                        }
+                        if (c < THRD) c = 0;
+                        C[s] = c;
+                    }
+                    for (int m = 0; m < A->M; ++m) {
+                        double b = A->bio[(size_t)m * N + n];
+                        if (b < THRD) b = 0;
+                        B[m] = b;
+                    }
+                    rates(A, C.data(), B.data(), R.data(), RB.data());
+                    for (int s = 0; s < S; ++s) {
+                        double dC = R[s] * A->dt;
+                        if (!(dC > THRD || dC < -THRD)) continue;
+                        if (dC + C[s] < 0.0) dC = -C[s];
+                        if (!(dC > THRD || dC < -THRD)) continue;
+                        if (A->mobile[s]) {
+                            for (int i = 0; i < Q7; ++i) A->gp[s][n * Q7 + i] += dC * T7[i];
+                        } else {
+                            A->imm[s][n] += dC;
+                        }
+                    }
+                    for (int m = 0; m < A->M; ++m) {
+                        double dB = RB[m] * A->dt;
+                        if (!(dB > THRD || dB < -THRD)) continue;
+                        if (dB + B[m] < 0.0) dB = -B[m];
+                        A->bio[(size_t)m * N + n] += dB;
+                    }
+                }
+        }
+    }
+    // ---- 3. stream, then the Neumann planes take the inner neighbour's density
+    for (int s = 0; s < S; ++s) {
+        if (!A->mobile[s]) continue;
+        std::vector<double>& G = A->g[s];
+        std::vector<double>& GP = A->gp[s];
+#pragma omp parallel for schedule(static)
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    size_t n = A->id(x, y, z);
+                    G[n * Q7] = GP[n * Q7];
+                    for (int i = 1; i < Q7; ++i) {
+                        int sx = x - C7[i][0], sy = y - C7[i][1], sz = z - C7[i][2];
+                        if (sx < 0 || sy < 0 || sz < 0 || sx >= nx || sy >= ny || sz >= nz)
+                            G[n * Q7 + i] = GP[n * Q7 + opp7(i)];
+                        else
+                            G[n * Q7 + i] = GP[A->id(sx, sy, sz) * Q7 + i];
+                    }
+                }
+        for (int side = 0; side < 2; ++side) {
+            int bt = side == 0 ? A->ltype[s] : A->rtype[s];
+            if (bt != BC_NEUMANN) continue;
+            int xb = side == 0 ? 0 : nx - 1, xi = side == 0 ? 1 : nx - 2;
+            std::vector<double>& st = side == 0 ? A->lstore : A->rstore;
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    size_t nb = A->id(xb, y, z), ni = A->id(xi, y, z);
+                    int db = A->node_dyn(s, xb, nb), di = A->node_dyn(s, xi, ni);
+                    if (db != ADE_PORE && db != ADE_BIO) continue;
+                    if (di != ADE_PORE && di != ADE_BIO) continue;  // keep the previous value
+                    double r = 1.0;
+                    for (int i = 0; i < Q7; ++i) r += G[ni * Q7 + i];
+                    st[(size_t)s * P + (size_t)y * nz + z] = r;
+                }
+        }
+    }
+    A->iters += 1;
+}
+
+void orc_ade_step(OrcAde* A, int n) {
+    for (int k = 0; k < n; ++k) ade_step(A);
+}
+
+/* computeDensity of species s at every node: BGK nodes sum + 1; boundary nodes of a
+ * Dirichlet / Neumann plane report their stored value; bounce-back nodes report the sum
+ * of their populations + 1 (the "held" content the reference's diagnostics track). */
+void orc_ade_density(OrcAde* A, int s, double* out) {
+    const size_t N = A->N, P = (size_t)A->ny * A->nz;
+    if (!A->mobile[s]) {
+        for (size_t n = 0; n < N; ++n) out[n] = A->imm[s][n];
+        return;
+    }
+    for (int x = 0; x < A->nx; ++x)
+        for (int y = 0; y < A->ny; ++y)
+            for (int z = 0; z < A->nz; ++z) {
+                size_t n = A->id(x, y, z);
+                int d = A->node_dyn(s, x, n);
+                bool bgk = (d == ADE_PORE || d == ADE_BIO);
+                if (bgk && x == 0) { out[n] = A->lstore[(size_t)s * P + (size_t)y * A->nz + z]; continue; }
+                if (bgk && x == A->nx - 1) { out[n] = A->rstore[(size_t)s * P + (size_t)y * A->nz + z]; continue; }
+                double r = 1.0;
+                for (int i = 0; i < Q7; ++i) r += A->g[s][n * Q7 + i];
+                out[n] = r;
+            }
+}
+
+void orc_ade_populations(OrcAde* A, int s, double* out) {
+    for (size_t n = 0; n < A->N; ++n)
+        for (int i = 0; i < Q7; ++i) out[(size_t)i * A->N + n] = A->g[s][n * Q7 + i];
+}
+
+void orc_ade_biomass(OrcAde* A, double* out) {
+    std::copy(A->bio.begin(), A->bio.end(), out);
+}
+
+void orc_ade_set_velocity(OrcAde* A, const double* u) { A->u.assign(u, u + 3 * A->N); }
+
+}  // extern "C"

@@ -1,0 +1,183 @@
+"""ctypes front end of the FP64 CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by bench.py's CPU
+baseline leg, never by the product. The per-material dynamics tables are derived here from the
+reference's setup rules, independently of the product's own table code:
+
+  flow lattice (complab_functions.hh:296-345): every code IncBGK(omega) by default; the
+  bounce-back code BounceBack; the solid code NoDynamics; each microbe's code IncBGK(omega_bio)
+  with omega_bio = 1/(r (1/omega - 1/2) + 1/2), or BounceBack when r <= 1e-14.
+
+  species lattices (complab_functions.hh:347-442, complab.cpp:1589-1656): pore BGK, biofilm
+  BGK with the biofilm omega, wall and solid BounceBack for a mobile species; kinetics where
+  the mask is neither solid nor wall (complab3d_processors_part1.hh:96-99).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+DYN_BB, DYN_NONE, DYN_BGK = 0, 1, 2
+ADE_BB, ADE_NONE, ADE_PORE, ADE_BIO = 0, 1, 2, 3
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        vp, dp, ip = C.c_void_p, C.c_double, C.c_int
+        sig = {
+            "orc_set_threads": ([ip], None), "orc_max_threads": ([], ip),
+            "orc_flow_create": ([ip, ip, ip, vp, vp, vp, dp], vp), "orc_flow_destroy": ([vp], None),
+            "orc_flow_step": ([vp, ip], None), "orc_flow_solve": ([vp, ip, dp], ip),
+            "orc_flow_energy": ([vp], dp), "orc_flow_iterations": ([vp], C.c_long),
+            "orc_flow_velocity": ([vp, vp], None), "orc_flow_populations": ([vp, vp], None),
+            "orc_flow_set_populations": ([vp, vp], None),
+            "orc_ade_create": ([ip, ip, ip, vp, ip, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], vp),
+            "orc_ade_destroy": ([vp], None), "orc_ade_set_kinetics": ([vp, ip, vp, ip, dp], None),
+            "orc_ade_set_biomass": ([vp, ip, vp], None), "orc_ade_step": ([vp, ip], None),
+            "orc_ade_density": ([vp, ip, vp], None), "orc_ade_populations": ([vp, ip, vp], None),
+            "orc_ade_biomass": ([vp, vp], None), "orc_ade_set_velocity": ([vp, vp], None),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+def max_threads():
+    return lib().orc_max_threads()
+
+
+class OracleFlow:
+    def __init__(self, mat, nx, ny, nz, tau, delta_p, solid_code=0, bounce_back_code=1, bio_codes=(),
+                 perm_ratio=()):
+        omega = 1.0 / tau
+        dyn = np.full(256, DYN_BGK, dtype=np.int32)
+        om = np.full(256, omega, dtype=np.float64)
+        if bounce_back_code >= 0:
+            dyn[bounce_back_code] = DYN_BB
+        if solid_code >= 0:
+            dyn[solid_code] = DYN_NONE
+        for c, r in zip(bio_codes, perm_ratio):
+            if r > 1e-14:
+                dyn[c] = DYN_BGK
+                om[c] = 1.0 / (r * (1.0 / omega - 0.5) + 0.5)
+            else:
+                dyn[c] = DYN_BB
+        self.N = nx * ny * nz
+        self.shape = (nx, ny, nz)
+        self._mat = np.ascontiguousarray(mat, dtype=np.int8)
+        self.h = lib().orc_flow_create(nx, ny, nz, _p(self._mat), _p(dyn), _p(om), delta_p)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_flow_destroy(self.h)
+            self.h = None
+
+    def step(self, n=1):
+        lib().orc_flow_step(self.h, n)
+
+    def solve(self, max_it, eps):
+        return lib().orc_flow_solve(self.h, max_it, eps)
+
+    @property
+    def energy(self):
+        return lib().orc_flow_energy(self.h)
+
+    def velocity(self):
+        u = np.empty(3 * self.N)
+        lib().orc_flow_velocity(self.h, _p(u))
+        return u.reshape(3, self.N)
+
+    def populations(self):
+        f = np.empty(19 * self.N)
+        lib().orc_flow_populations(self.h, _p(f))
+        return f.reshape(19, self.N)
+
+    def set_populations(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        lib().orc_flow_set_populations(self.h, _p(f))
+
+
+class OracleAde:
+    def __init__(self, mat, nx, ny, nz, species, u, solid_code=0, bounce_back_code=1, bio_codes=()):
+        dyn = np.full(256, ADE_PORE, dtype=np.int32)
+        react = np.ones(256, dtype=np.int32)
+        for c in bio_codes:
+            dyn[c] = ADE_BIO
+        for c in (bounce_back_code, solid_code):
+            if c >= 0:
+                dyn[c] = ADE_BB
+                react[c] = 0
+        S = len(species)
+        g = lambda k, d: np.array([s.get(k, d) for s in species], dtype=np.float64)
+        gi = lambda k, d: np.array([s.get(k, d) for s in species], dtype=np.int32)
+        wp = g("omega_pore", 1.0)
+        wb = np.array([s.get("omega_biofilm", s["omega_pore"]) for s in species], dtype=np.float64)
+        self._keep = [np.ascontiguousarray(mat, dtype=np.int8), dyn, react, wp, wb, gi("mobile", 1),
+                      gi("left_type", 1), gi("right_type", 1), g("left_bc", 0.0), g("right_bc", 0.0),
+                      g("c0", 0.0), np.ascontiguousarray(u, dtype=np.float64).reshape(-1)]
+        k = self._keep
+        self.N = nx * ny * nz
+        self.S = S
+        self.h = lib().orc_ade_create(nx, ny, nz, _p(k[0]), S, _p(k[1]), _p(k[2]), _p(k[3]), _p(k[4]),
+                                      _p(k[5]), _p(k[6]), _p(k[7]), _p(k[8]), _p(k[9]), _p(k[10]), _p(k[11]))
+        self.M = 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_ade_destroy(self.h)
+            self.h = None
+
+    def set_kinetics(self, law, params, dt):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        self._prm = p
+        lib().orc_ade_set_kinetics(self.h, law, _p(p), p.size, dt)
+
+    def set_biomass(self, b):
+        b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1)
+        self.M = b.size // self.N
+        lib().orc_ade_set_biomass(self.h, self.M, _p(b))
+
+    def step(self, n=1):
+        lib().orc_ade_step(self.h, n)
+
+    def concentration(self, s):
+        c = np.empty(self.N)
+        lib().orc_ade_density(self.h, s, _p(c))
+        return c
+
+    def populations(self, s):
+        g = np.empty(7 * self.N)
+        lib().orc_ade_populations(self.h, s, _p(g))
+        return g.reshape(7, self.N)
+
+    def biomass(self):
+        b = np.empty(self.M * self.N)
+        lib().orc_ade_biomass(self.h, _p(b))
+        return b.reshape(self.M, self.N)

@@ -1,0 +1,65 @@
+"""Regenerates tests/golden/geometry.json from the reference's own geometry generator
+(complab3d_geometry.hh, compiled into oracle/_ref/libref_geometry.so by `make -C oracle ref`).
+
+Run from the repository root in a checkout that has the reference sources:
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+import ctypes as C
+import hashlib
+import json
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+REF = os.path.join(ROOT, "oracle", "_ref", "libref_geometry.so")
+
+CASES = [
+    dict(kind="channel", nx=12, ny=9, nz=7, walls="y"),
+    dict(kind="spheres", nx=24, ny=20, nz=16, radius=4.0, count=12, seed=7, walls="y"),
+    dict(kind="spheres", nx=40, ny=32, nz=32, radius=6.0, count=20, seed=1, walls="yz"),
+    dict(kind="cylinders", nx=30, ny=24, nz=5, radius=3.5, count=9, seed=3, walls="y"),
+    dict(kind="random", nx=20, ny=16, nz=12, porosity=0.35, seed=11, walls="y"),
+    dict(kind="random", nx=32, ny=32, nz=32, porosity=0.5, seed=2, walls="none"),
+    dict(kind="fracture", nx=48, ny=40, nz=6, aperture=12.0, roughness=0.3, seed=1004, walls="none"),
+    dict(kind="fracture", nx=30, ny=30, nz=4, aperture=6.0, roughness=2.0, seed=5, walls="y"),
+    dict(kind="layered", nx=20, ny=24, nz=10, porosity=0.4, layers=4, seed=9, walls="z"),
+]
+DEFAULTS = dict(porosity=0.4, radius=6.0, aperture=6.0, roughness=2.0, count=20, layers=4, seed=1, walls="y")
+
+
+def ref_generate(L, c):
+    o = dict(DEFAULTS, **c)
+    n = o["nx"] * o["ny"] * o["nz"]
+    out = np.empty(n, dtype=np.int32)
+    rc = L.ref_geom_generate(o["kind"].encode(), o["nx"], o["ny"], o["nz"], C.c_double(o["porosity"]),
+                             C.c_double(o["radius"]), C.c_double(o["aperture"]), C.c_double(o["roughness"]),
+                             o["count"], o["layers"], C.c_ulonglong(o["seed"]), o["walls"].encode(),
+                             out.ctypes.data_as(C.c_void_p))
+    assert rc == 0
+    xs = out.reshape(o["nz"], o["ny"], o["nx"]).transpose(2, 1, 0).astype(np.int8)  # -> x slowest
+    po, op, iso = C.c_double(), C.c_long(), C.c_long()
+    cl, sp, pe = C.c_int(), C.c_int(), C.c_int()
+    L.ref_geom_inspect(out.ctypes.data_as(C.c_void_p), o["nx"], o["ny"], o["nz"], C.byref(po), C.byref(op),
+                       C.byref(iso), C.byref(cl), C.byref(sp), C.byref(pe))
+    return o, np.ascontiguousarray(xs).ravel(), dict(porosity=po.value, open_voxels=op.value,
+                                                      isolated_voxels=iso.value, clusters=cl.value,
+                                                      spanning_clusters=sp.value, percolates=pe.value)
+
+
+def main():
+    L = C.CDLL(REF)
+    out = []
+    for c in CASES:
+        o, arr, ins = ref_generate(L, c)
+        rec = dict(options=o, sha256=hashlib.sha256(arr.tobytes()).hexdigest(), inspection=ins)
+        if arr.size <= 1000:
+            rec["voxels"] = arr.tolist()
+        out.append(rec)
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "geometry.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"wrote {len(out)} geometry cases")
+
+
+if __name__ == "__main__":
+    main()

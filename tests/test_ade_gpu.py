@@ -1,0 +1,121 @@
+"""Fused D3Q7 transport + kinetics on the GPU against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from helpers import mixed_geometry, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+BIO = dict(bio_codes=(3, 4), perm_ratio=(0.3, 0.3))
+
+
+def flow_field(oracle, mat, shape, steps=300):
+    O = oracle.OracleFlow(mat, *shape, 0.8, 3e-4, bio_codes=(3, 4), perm_ratio=(0.3, 0.3))
+    O.step(steps)
+    return O.velocity()
+
+
+def pair(clb, oracle, mat, shape, species, prec, u, law=0, params=(), dt=1.0, biomass=None):
+    D = clb.Domain(mat, *shape, 0.8, ade_precision=prec, **BIO)
+    D.ade_init(species)
+    D.set_velocity(u)
+    O = oracle.OracleAde(mat, *shape, species, u, bio_codes=(3, 4))
+    if biomass is not None:
+        D.set_biomass(biomass)
+        O.set_biomass(biomass)
+    if law:
+        D.set_kinetics(law, params, dt)
+        O.set_kinetics(law, params, dt)
+    return D, O
+
+
+SPECIES = [
+    dict(omega_pore=1 / 0.9, omega_biofilm=1 / 0.7, left_type=0, right_type=1, left_bc=1.0, c0=0.0),
+    dict(omega_pore=1 / 0.62, omega_biofilm=1 / 0.56, left_type=1, right_type=0, right_bc=0.4, c0=0.2),
+    dict(omega_pore=1 / 1.3, omega_biofilm=1 / 0.9, left_type=2, right_type=2, c0=0.6),
+]
+
+
+@pytest.mark.parametrize("steps", [1, 2, 25, 120])
+def test_f64_multispecies_decay_matches_oracle(clb, oracle, steps):
+    shape = (20, 10, 9)
+    mat = mixed_geometry(*shape)
+    u = flow_field(oracle, mat, shape)
+    D, O = pair(clb, oracle, mat, shape, SPECIES, clb.F64, u, law=1, params=[1e-3, 2e-2, 5e-3])
+    D.ade_step(steps)
+    O.step(steps)
+    for s in range(3):
+        pg, po = D.ade_populations(s), O.populations(s)
+        assert np.max(np.abs(pg - po)) < 1e-12, s
+        np.testing.assert_allclose(D.concentration(s), O.concentration(s), rtol=0, atol=1e-12)
+
+
+def test_f64_monod_with_immobile_species(clb, oracle):
+    shape = (16, 9, 8)
+    mat = mixed_geometry(*shape, seed=3)
+    u = flow_field(oracle, mat, shape)
+    sp = SPECIES[:2] + [dict(omega_pore=1.0, mobile=0, left_type=1, right_type=1, c0=0.8)]
+    D, O = pair(clb, oracle, mat, shape, sp, clb.F64, u, law=2, params=[1e-2, 3e-2, 1e-3, 0.1, 0.2, 0.5])
+    D.ade_step(60)
+    O.step(60)
+    for s in range(3):
+        np.testing.assert_allclose(D.concentration(s), O.concentration(s), rtol=0, atol=1e-12)
+
+
+def test_f64_dual_monod_biomass(clb, oracle):
+    shape = (16, 9, 8)
+    mat = mixed_geometry(*shape, seed=4)
+    u = flow_field(oracle, mat, shape)
+    N = mat.size
+    rng = np.random.default_rng(2)
+    bio = np.zeros((2, N))
+    bio[0, mat == 3] = rng.uniform(10, 60, size=(mat == 3).sum())
+    bio[1, mat == 4] = rng.uniform(10, 60, size=(mat == 4).sum())
+    D, O = pair(clb, oracle, mat, shape, SPECIES, clb.F64, u, law=3, params=[1e-3, 0.1, 0.4, 1e-5], biomass=bio)
+    D.ade_step(80)
+    O.step(80)
+    for s in range(3):
+        np.testing.assert_allclose(D.concentration(s), O.concentration(s), rtol=0, atol=1e-12)
+    ob = O.biomass()
+    for m in range(2):
+        np.testing.assert_allclose(D.biomass(m), ob[m], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("prec,tol", [("F32", 1e-5), ("F16S", 2e-2)])
+def test_reduced_precision_concentration_error(clb, oracle, prec, tol):
+    shape = (20, 10, 9)
+    mat = mixed_geometry(*shape)
+    u = flow_field(oracle, mat, shape)
+    D, O = pair(clb, oracle, mat, shape, SPECIES, getattr(clb, prec), u, law=1, params=[1e-3, 2e-2, 5e-3])
+    D.ade_step(200)
+    O.step(200)
+    for s in range(3):
+        err = rel_l2(D.concentration(s), O.concentration(s))
+        print(f"{prec} species {s} rel L2 {err:.3e}")
+        assert err < tol
+
+
+def test_closed_box_content_conserved_f64(clb, oracle):
+    shape = (18, 10, 9)
+    mat = mixed_geometry(*shape)
+    u = flow_field(oracle, mat, shape)
+    sp = [dict(omega_pore=1 / 0.9, omega_biofilm=1 / 0.7, left_type=2, right_type=2, c0=0.3)]
+    D, _ = pair(clb, oracle, mat, shape, sp, clb.F64, u)
+    c0 = D.reduce()["content"][0]
+    D.ade_step(301)
+    c1 = D.reduce()["content"][0]
+    assert abs(c1 - c0) <= 1e-12 * abs(c0)
+
+
+def test_coupled_velocity_equals_flow_velocity(clb):
+    shape = (14, 8, 8)
+    mat = mixed_geometry(*shape)
+    D = clb.Domain(mat, *shape, 0.8, flow_precision=clb.F64, ade_precision=clb.F64, **BIO)
+    D.flow_init(1e-4)
+    D.flow_step(50)
+    D.ade_init(SPECIES[:1])
+    D.couple_velocity()
+    u = np.empty(3 * D.N)
+    lib = clb.lib()
+    assert lib.clb_get_field(D.h, clb.FIELD_ADE_VELOCITY, 0, u.ctypes.data_as(clb.C.c_void_p), 0) == 0
+    np.testing.assert_array_equal(u.reshape(3, -1), D.velocity())

@@ -1,0 +1,84 @@
+"""D3Q19 flow lattice on the GPU (through the C ABI) against the FP64 oracle.
+
+Tolerances: FP64 storage must match to round-off (relative max 1e-11 on every population);
+FP32 storage within 1e-5 relative L2 of the velocity; FP16-shifted within 3e-2 (its
+populations carry 11 significant bits)."""
+import numpy as np
+import pytest
+
+from helpers import mixed_geometry, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+BIO = dict(bio_codes=(3, 4), perm_ratio=(0.3, 0.0))
+
+
+def make_pair(clb, oracle, mat, shape, tau, dp, prec, **bio):
+    nx, ny, nz = shape
+    D = clb.Domain(mat, nx, ny, nz, tau, flow_precision=prec, **bio)
+    D.flow_init(dp)
+    O = oracle.OracleFlow(mat, nx, ny, nz, tau, dp, bio_codes=bio.get("bio_codes", ()),
+                          perm_ratio=bio.get("perm_ratio", ()))
+    return D, O
+
+
+@pytest.mark.parametrize("walls", [True, False])
+@pytest.mark.parametrize("steps", [1, 2, 37, 200])
+def test_f64_populations_match_oracle(clb, oracle, walls, steps):
+    shape = (18, 11, 9)
+    mat = mixed_geometry(*shape, walls=walls)
+    D, O = make_pair(clb, oracle, mat, shape, 0.8, 3e-4, clb.F64, **BIO)
+    D.flow_step(steps)
+    O.step(steps)
+    fg, fo = D.flow_populations(), O.populations()
+    scale = np.max(np.abs(fo))
+    assert np.max(np.abs(fg - fo)) <= 1e-11 * scale
+    np.testing.assert_allclose(D.velocity(), O.velocity(), rtol=0, atol=1e-12 * np.max(np.abs(O.velocity())))
+
+
+def test_f64_solve_matches_oracle_iterations(clb, oracle):
+    shape = (22, 12, 12)
+    mat = mixed_geometry(*shape, solid_block=False, biofilm=False)
+    D, O = make_pair(clb, oracle, mat, shape, 0.8, 1e-4, clb.F64)
+    it_g, conv = D.flow_solve(40000, 1e-6)
+    it_o = O.solve(40000, 1e-6)
+    assert conv
+    assert abs(it_g - it_o) <= 1
+    assert rel_l2(D.velocity(), O.velocity()) < 1e-9
+    st = D.flow_stats(8.0)
+    assert st["permeability"] > 0
+
+
+@pytest.mark.parametrize("prec,tol", [("F32", 1e-5), ("F16S", 3e-2)])
+def test_reduced_precision_velocity_error(clb, oracle, prec, tol):
+    shape = (26, 14, 14)
+    mat = mixed_geometry(*shape, seed=9)
+    D, O = make_pair(clb, oracle, mat, shape, 0.8, 1e-4, getattr(clb, prec), **BIO)
+    D.flow_step(400)
+    O.step(400)
+    err = rel_l2(D.velocity(), O.velocity())
+    print(f"{prec} velocity rel L2 after 400 steps: {err:.3e}")
+    assert err < tol
+
+
+def test_set_populations_round_trip(clb, oracle):
+    shape = (12, 7, 6)
+    mat = mixed_geometry(*shape)
+    D, O = make_pair(clb, oracle, mat, shape, 0.7, 1e-4, clb.F64)
+    D.flow_step(3)  # odd parity: the scatter must invert the gather
+    f = D.flow_populations()
+    rng = np.random.default_rng(1)
+    g = f + 1e-5 * rng.standard_normal(f.shape)
+    D.set_flow_populations(g)
+    np.testing.assert_array_equal(D.flow_populations(), g)
+    O.set_populations(g)
+    D.flow_step(5)
+    O.step(5)
+    assert np.max(np.abs(D.flow_populations() - O.populations())) < 1e-13
+
+
+def test_flow_step_before_init_is_an_error(clb):
+    D = clb.Domain(np.full(4 * 4 * 4, 2, np.int8), 4, 4, 4, 0.8)
+    with pytest.raises(clb.ClbError) as e:
+        D.flow_step(1)
+    assert e.value.status == 7
