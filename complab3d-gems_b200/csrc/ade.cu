@@ -10,12 +10,14 @@
 //   post-collision populations.  BGK conserves a node's density, so the rate is evaluated
 //   on the density the thread already holds: one read and one write per population.
 //
-// Layout: mobile species populations g[m][7][N] of the storage type (m = rank of the species
-// among the mobile ones), AA in-place pattern as in flow.cu; immobile species and biomass
-// are FP64 scalar fields; the advection velocity u[3][N] in the arithmetic type.
-// Algorithmic bytes per node update: 2*7*sizeof(storage) per mobile species, plus the
-// velocity (3*sizeof(arith)) and the material byte shared by all species.
-#include "clb_internal.cuh"
+// Layout: the compacted node layout of sparse.cuh over the nodes that are not bounce-back for
+// the species lattices (pore and biofilm); mobile species populations g[m][7][K] of the storage
+// type (m = rank of the species among the mobile ones) with their wall link slots
+// glink[m][L]; AA in-place pattern as in flow.cu. Immobile species and biomass are FP64 fields
+// imm[s][K], bio[m][K]; the advection velocity u[3][K] is in the arithmetic type.
+// Algorithmic bytes per node update: 2*7*sizeof(storage) per mobile species, plus the velocity
+// (3*sizeof(arith)) and the material byte shared by all species.
+#include "sparse.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -23,43 +25,6 @@
 namespace clb {
 
 constexpr int ADE_THREADS = 256;
-
-template <typename TS, typename TC, bool ODD>
-__device__ __forceinline__ void load7(const TS* __restrict__ f, int64_t N, const Geom& G, int64_t n, int x, int y,
-                                      int z, TC (&g)[7]) {
-#pragma unroll
-    for (int i = 0; i < 7; ++i) {
-        if (!ODD || i == 0) {
-            g[i] = ld<TS, TC>(f + (int64_t)i * N + n);
-        } else {
-            const int cx = q7cx(i), cy = q7cy(i), cz = q7cz(i);
-            const bool in = (cx == 0 || ((unsigned)(x - cx) < (unsigned)G.nx)) &&
-                            (cy == 0 || ((unsigned)(y - cy) < (unsigned)G.ny)) &&
-                            (cz == 0 || ((unsigned)(z - cz) < (unsigned)G.nz));
-            const int64_t off = (int64_t)cx * G.plane + cy * G.nz + cz;
-            g[i] = in ? ld<TS, TC>(f + (int64_t)q7opp(i) * N + n - off) : ld<TS, TC>(f + (int64_t)i * N + n);
-        }
-    }
-}
-
-template <typename TS, typename TC, bool ODD>
-__device__ __forceinline__ void store7(TS* __restrict__ f, int64_t N, const Geom& G, int64_t n, int x, int y, int z,
-                                       const TC (&o)[7]) {
-#pragma unroll
-    for (int i = 0; i < 7; ++i) {
-        if (!ODD || i == 0) {
-            st<TS, TC>(f + (int64_t)q7opp(i) * N + n, o[i]);
-        } else {
-            const int cx = q7cx(i), cy = q7cy(i), cz = q7cz(i);
-            const bool in = (cx == 0 || ((unsigned)(x + cx) < (unsigned)G.nx)) &&
-                            (cy == 0 || ((unsigned)(y + cy) < (unsigned)G.ny)) &&
-                            (cz == 0 || ((unsigned)(z + cz) < (unsigned)G.nz));
-            const int64_t off = (int64_t)cx * G.plane + cy * G.nz + cz;
-            if (in) st<TS, TC>(f + (int64_t)i * N + n + off, o[i]);
-            else st<TS, TC>(f + (int64_t)q7opp(i) * N + n, o[i]);
-        }
-    }
-}
 
 // Rate laws (clb_law). C, B are the floored concentrations / biomasses.
 __device__ __forceinline__ void eval_rates(const AdeParams& P, const double* C, const double* B, double* R,
@@ -92,20 +57,39 @@ __device__ __forceinline__ void eval_rates(const AdeParams& P, const double* C, 
     }
 }
 
+
 template <typename TS, typename TC, bool ODD, int NM>
 __global__ void __launch_bounds__(ADE_THREADS)
-    k_ade_aa(TS* __restrict__ g, double* __restrict__ imm, double* __restrict__ bio, const TC* __restrict__ u,
-             const int32_t* __restrict__ list, int64_t nlist, const int8_t* __restrict__ mat,
-             const double* __restrict__ neu, const AdeParams P, int n_mobile, const int* __restrict__ mob_species) {
+    k_ade_aa(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm, double* __restrict__ bio,
+             const TC* __restrict__ u, const SparseView S, const double* __restrict__ neu, const AdeParams P,
+             int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin) {
     const Geom G = P.g;
-    const int64_t N = G.N;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nlist; k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t n = list[k];
-        int x, y, z;
-        decode(G, n, x, y, z);
-        const int code = mat[n];
+    const int64_t K = S.K, L = S.L;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
+        const int code = S.code[k];
         const int dyn = P.dyn[code];
-        const bool west = (x == 0), east = (x == G.nx - 1);
+        const bool west = k < k_west_end, east = k >= k_east_begin;
+        int x = 0, y = 0, z = 0, p = 0;
+        uint32_t wm = 0;
+        int lb = 0;
+        int64_t nb[7];  // compact index of the source node a - c_i (odd step)
+        if (ODD || west || east) {
+            const int64_t n = S.node[k];
+            decode(G, n, x, y, z);
+            p = (int)(n - (int64_t)x * G.plane);
+        }
+        if (ODD) {
+            wm = S.wall[k];
+            lb = S.linkbase[k];
+            const int r = x * G.ny + y;
+            nb[0] = k;
+            nb[1] = (x + 1 < G.nx) ? row_rank(S, r + G.ny, z) : -1;  // -x population comes from x+1
+            nb[4] = (x >= 1) ? row_rank(S, r - G.ny, z) : -1;
+            nb[2] = (y + 1 < G.ny) ? row_rank(S, r + 1, z) : -1;
+            nb[5] = (y >= 1) ? row_rank(S, r - 1, z) : -1;
+            nb[3] = k + 1;
+            nb[6] = k - 1;
+        }
         TC pop[NM][7];
         TC rb[NM];
         bool act[NM];
@@ -117,15 +101,26 @@ __global__ void __launch_bounds__(ADE_THREADS)
             const int s = mob_species[m];
             if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
             act[m] = true;
-            const TS* base = g + (int64_t)m * 7 * N;
-            load7<TS, TC, ODD>(base, N, G, n, x, y, z, pop[m]);
+            const TS* f = g + (int64_t)m * 7 * K;
+            const TS* lk = glink + (int64_t)m * L;
+#pragma unroll
+            for (int i = 0; i < 7; ++i) {
+                if (!ODD || i == 0) { pop[m][i] = ld<TS, TC>(f + (int64_t)i * K + k); continue; }
+                const int cx = q7cx(i), cy = q7cy(i), cz = q7cz(i), oi = q7opp(i);
+                const bool in = (cx == 0 || (unsigned)(x - cx) < (unsigned)G.nx) &&
+                                (cy == 0 || (unsigned)(y - cy) < (unsigned)G.ny) &&
+                                (cz == 0 || (unsigned)(z - cz) < (unsigned)G.nz);
+                if (!in) pop[m][i] = ld<TS, TC>(f + (int64_t)i * K + k);
+                else if ((wm >> oi) & 1u) pop[m][i] = ld<TS, TC>(lk + lb + __popc(wm & ((1u << oi) - 1u)));
+                else pop[m][i] = ld<TS, TC>(f + (int64_t)oi * K + nb[i]);
+            }
             if ((west || east) && dyn != ADE_NONE) {
                 // AdvectionDiffusionBoundaryDynamics: the one inward population makes the
                 // node's density equal to the stored value
                 const int type = west ? P.ltype[s] : P.rtype[s];
                 double rs;
                 if (type == CLB_DIRICHLET) rs = west ? P.lbc[s] : P.rbc[s];
-                else rs = neu[((int64_t)s * 2 + (west ? 0 : 1)) * G.plane + (n - (int64_t)x * G.plane)];
+                else rs = neu[((int64_t)s * 2 + (west ? 0 : 1)) * G.plane + p];
                 const int miss = west ? 4 : 1;
                 TC sum = 0;
 #pragma unroll
@@ -152,12 +147,12 @@ __global__ void __launch_bounds__(ADE_THREADS)
                     for (int mm = 0; mm < NM; ++mm)
                         if (mm == m) c = (double)rb[mm] + 1.0;
                 } else {
-                    c = imm[(int64_t)s * N + n];
+                    c = imm[(int64_t)s * K + k];
                 }
                 C[s] = c < THRD ? 0.0 : c;
             }
             for (int mb = 0; mb < P.M; ++mb) {
-                const double b = bio[(int64_t)mb * N + n];
+                const double b = bio[(int64_t)mb * K + k];
                 B[mb] = b < THRD ? 0.0 : b;
             }
             eval_rates(P, C, B, R, RB);
@@ -167,17 +162,17 @@ __global__ void __launch_bounds__(ADE_THREADS)
                 if (d + C[s] < 0.0) d = -C[s];
                 if (!(d > THRD || d < -THRD)) continue;
                 if (P.slot[s] >= 0) dC[s] = d;
-                else imm[(int64_t)s * N + n] += d;
+                else imm[(int64_t)s * K + k] += d;
             }
             for (int mb = 0; mb < P.M; ++mb) {
                 double d = RB[mb] * P.dt;
                 if (!(d > THRD || d < -THRD)) continue;
                 if (d + B[mb] < 0.0) d = -B[mb];
-                bio[(int64_t)mb * N + n] += d;
+                bio[(int64_t)mb * K + k] += d;
             }
         }
         // ---- collide, deposit, stream
-        const TC ux = u[n], uy = u[N + n], uz = u[2 * N + n];
+        const TC ux = u[k], uy = u[K + k], uz = u[2 * K + k];
 #pragma unroll
         for (int m = 0; m < NM; ++m) {
             if (!act[m]) continue;
@@ -199,26 +194,40 @@ __global__ void __launch_bounds__(ADE_THREADS)
                     o[i] += (TC)q7w(i) * d;
                 }
             }
-            store7<TS, TC, ODD>(g + (int64_t)m * 7 * N, N, G, n, x, y, z, o);
+            TS* f = g + (int64_t)m * 7 * K;
+            TS* lk = glink + (int64_t)m * L;
+#pragma unroll
+            for (int i = 0; i < 7; ++i) {
+                if (!ODD || i == 0) { st<TS, TC>(f + (int64_t)q7opp(i) * K + k, o[i]); continue; }
+                const int cx = q7cx(i), cy = q7cy(i), cz = q7cz(i), oi = q7opp(i);
+                const bool in = (cx == 0 || (unsigned)(x + cx) < (unsigned)G.nx) &&
+                                (cy == 0 || (unsigned)(y + cy) < (unsigned)G.ny) &&
+                                (cz == 0 || (unsigned)(z + cz) < (unsigned)G.nz);
+                if (!in) st<TS, TC>(f + (int64_t)oi * K + k, o[i]);
+                else if ((wm >> i) & 1u) st<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)), o[i]);
+                else st<TS, TC>(f + (int64_t)i * K + nb[oi], o[i]);  // destination a + c_i = source of opp(i)
+            }
         }
     }
 }
 
-// The stored density of every Neumann plane node: the density of its inner neighbour as
-// it stands before the step (FlatAdiabaticBoundaryFunctional3D after the previous stream).
-// A node whose inner neighbour is not a fluid node keeps its previous value.
-template <typename TS, typename TC, bool ODD>
-__global__ void k_ade_neumann(const TS* __restrict__ g, const int8_t* __restrict__ mat, double* __restrict__ neu,
-                              const AdeParams P, int s, int m, int side) {
+// The stored density of every Neumann plane node: the density of its inner neighbour as it
+// stands before the step (FlatAdiabaticBoundaryFunctional3D after the previous stream). A node
+// whose inner neighbour is not a fluid node keeps its previous value.
+template <typename TS, typename TC>
+__global__ void k_ade_neumann(const TS* __restrict__ g, const TS* __restrict__ glink, const SparseView S,
+                              const int8_t* __restrict__ mat, double* __restrict__ neu, const AdeParams P, int s,
+                              int m, int side, int odd, double c0) {
     const Geom G = P.g;
     const int xb = side == 0 ? 0 : G.nx - 1, xi = side == 0 ? 1 : G.nx - 2;
+    TC init[7];
+    for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - 1.0));
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < G.plane; p += gridDim.x * blockDim.x) {
-        const int y = p / G.nz, z = p - y * G.nz;
         const int64_t nb = (int64_t)xb * G.plane + p, ni = (int64_t)xi * G.plane + p;
         const int db = P.dyn[mat[nb]], di = P.dyn[mat[ni]];
         if (!(db == ADE_PORE || db == ADE_BIO) || !(di == ADE_PORE || di == ADE_BIO)) continue;
         TC pop[7];
-        load7<TS, TC, ODD>(g + (int64_t)m * 7 * G.N, G.N, G, ni, xi, y, z, pop);
+        natural<TS, TC, 7>(S, G, g + (int64_t)m * 7 * S.K, glink + (int64_t)m * S.L, ni, odd, init, pop);
         double r = 1.0;
         for (int i = 0; i < 7; ++i) r += (double)pop[i];
         neu[((int64_t)s * 2 + side) * G.plane + p] = r;
@@ -226,122 +235,103 @@ __global__ void k_ade_neumann(const TS* __restrict__ g, const int8_t* __restrict
 }
 
 template <typename TS>
-__global__ void k_ade_init(TS* __restrict__ g, int64_t N, int n_mobile, const double* __restrict__ c0m) {
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+__global__ void k_ade_init(TS* __restrict__ g, TS* __restrict__ glink, int64_t K, int64_t L, int n_mobile,
+                           const double* __restrict__ c0m) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K || k < L;
+         k += (int64_t)gridDim.x * blockDim.x) {
         for (int m = 0; m < n_mobile; ++m) {
             double c = c0m[m];
             if (c < THRD && c > -THRD) c = 0.0;
-            for (int i = 0; i < 7; ++i) {
-                double v = q7w(i) * (c - 1.0);
-                if constexpr (std::is_same<TS, __half>::value) g[((int64_t)m * 7 + i) * N + n] = __double2half(v);
-                else g[((int64_t)m * 7 + i) * N + n] = (TS)v;
+            if (k < K)
+                for (int i = 0; i < 7; ++i) {
+                    double v = q7w(i) * (c - 1.0);
+                    if constexpr (std::is_same<TS, __half>::value) g[((int64_t)m * 7 + i) * K + k] = __double2half(v);
+                    else g[((int64_t)m * 7 + i) * K + k] = (TS)v;
+                }
+            if (k < L) {
+                // a wall slot holds population j of the wall node; every j != 0 has weight 1/8
+                double v = 0.125 * (c - 1.0);
+                if constexpr (std::is_same<TS, __half>::value) glink[(int64_t)m * L + k] = __double2half(v);
+                else glink[(int64_t)m * L + k] = (TS)v;
             }
         }
     }
 }
 
-// Natural-layout incoming populations of one mobile species (parity rule), as FP64.
 template <typename TS>
-__global__ void k_ade_get_pops(const TS* __restrict__ g, const Geom G, int odd, double* __restrict__ out) {
+__global__ void k_ade_get_pops(const TS* __restrict__ g, const TS* __restrict__ glink, const SparseView S,
+                               const Geom G, int odd, double c0, double* __restrict__ out) {
+    double init[7];
+    for (int i = 0; i < 7; ++i) init[i] = q7w(i) * (c0 - 1.0);
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        decode(G, n, x, y, z);
         double v[7];
-        if constexpr (std::is_same<TS, double>::value) {
-            if (odd) load7<TS, double, true>(g, G.N, G, n, x, y, z, v);
-            else load7<TS, double, false>(g, G.N, G, n, x, y, z, v);
-        } else {
-            float h[7];
-            if (odd) load7<TS, float, true>(g, G.N, G, n, x, y, z, h);
-            else load7<TS, float, false>(g, G.N, G, n, x, y, z, h);
-            for (int i = 0; i < 7; ++i) v[i] = h[i];
-        }
+        natural<TS, double, 7>(S, G, g, glink, n, odd, init, v);
         for (int i = 0; i < 7; ++i) out[(int64_t)i * G.N + n] = v[i];
     }
 }
 
 template <typename TS>
-__global__ void k_ade_set_pops(TS* __restrict__ g, const Geom G, int odd, const double* __restrict__ in) {
+__global__ void k_ade_set_pops(TS* __restrict__ g, TS* __restrict__ glink, const SparseView S, const Geom G, int odd,
+                               const double* __restrict__ in) {
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        decode(G, n, x, y, z);
-        for (int i = 0; i < 7; ++i) {
-            int64_t slot = (int64_t)i * G.N + n;
-            if (odd && i != 0) {
-                const int cx = q7cx(i), cy = q7cy(i), cz = q7cz(i);
-                const bool inb = ((unsigned)(x - cx) < (unsigned)G.nx) && ((unsigned)(y - cy) < (unsigned)G.ny) &&
-                                 ((unsigned)(z - cz) < (unsigned)G.nz);
-                const int64_t off = (int64_t)cx * G.plane + cy * G.nz + cz;
-                if (inb) slot = (int64_t)q7opp(i) * G.N + n - off;
-            }
-            double v = in[(int64_t)i * G.N + n];
-            if constexpr (std::is_same<TS, __half>::value) g[slot] = __double2half(v);
-            else g[slot] = (TS)v;
-        }
+        double v[7];
+        for (int i = 0; i < 7; ++i) v[i] = in[(int64_t)i * G.N + n];
+        put_natural<TS, 7>(S, G, g, glink, n, odd, v);
     }
 }
 
-// Per-block FP64 partials of the live fields: for each species the sum of concentration over
-// open voxels of x=1..nx-2, the node content sum (sum of populations + 1 over every node),
-// min, max; biomass sums; non-finite count.
+// Per-block FP64 partials of the live fields. Layout per block:
+// [S total][S content][S min][S max][M bio][1 nonfinite][1 open]. total/min/max/nonfinite over
+// open voxels of x=1..nx-2 (stored nodes that react); content = sum over stored nodes of
+// (sum of populations + 1) plus the wall link slots (the content held in walls that can move).
 template <typename TS>
-__global__ void k_ade_reduce(const TS* __restrict__ g, const double* __restrict__ imm,
-                             const double* __restrict__ bio, const int8_t* __restrict__ mat, const AdeParams P,
-                             int n_mobile, const int* __restrict__ mob_species, int odd, double* __restrict__ part,
-                             int nq) {
-    const Geom G = P.g;
-    // part layout per block: [S total][S content][S min][S max][M bio][1 nonfinite][1 open]
+__global__ void k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ glink, const double* __restrict__ imm,
+                             const double* __restrict__ bio, const SparseView S, const AdeParams P,
+                             const int* __restrict__ mob_species, int n_mobile, double* __restrict__ part, int nq,
+                             int64_t k_west_end, int64_t k_east_begin) {
     extern __shared__ double shq[];
+    const int S_ = P.S, M = P.M;
     for (int q = threadIdx.x; q < nq; q += blockDim.x) shq[q] = 0.0;
-    const int S = P.S, M = P.M;
-    for (int s = threadIdx.x; s < S; s += blockDim.x) {
-        shq[2 * S + s] = 1e300;
-        shq[3 * S + s] = -1e300;
+    __syncthreads();
+    for (int s = threadIdx.x; s < S_; s += blockDim.x) {
+        shq[2 * S_ + s] = 1e300;
+        shq[3 * S_ + s] = -1e300;
     }
     __syncthreads();
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        decode(G, n, x, y, z);
-        const int code = mat[n];
-        const bool inner = (x >= 1 && x <= G.nx - 2);
-        const bool open = inner && P.react[code] && P.dyn[code] != ADE_BB;
-        if (open) atomicAdd(&shq[4 * S + M + 1], 1.0);
-        for (int s = 0; s < S; ++s) {
-            double c, content;
+    const int64_t K = S.K;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K || k < S.L;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        if (k < S.L)
+            for (int m = 0; m < n_mobile; ++m) atomicAdd(&shq[S_ + mob_species[m]], ldd(glink + (int64_t)m * S.L + k));
+        if (k >= K) continue;
+        const int code = S.code[k];
+        const bool inner = k >= k_west_end && k < k_east_begin;
+        const bool open = inner && P.react[code];
+        if (open) atomicAdd(&shq[4 * S_ + M + 1], 1.0);
+        for (int s = 0; s < S_; ++s) {
+            double c;
             const int m = P.slot[s];
             if (m >= 0) {
-                double v[7];
-                if constexpr (std::is_same<TS, double>::value) {
-                    if (odd) load7<TS, double, true>(g + (int64_t)m * 7 * G.N, G.N, G, n, x, y, z, v);
-                    else load7<TS, double, false>(g + (int64_t)m * 7 * G.N, G.N, G, n, x, y, z, v);
-                } else {
-                    float h[7];
-                    if (odd) load7<TS, float, true>(g + (int64_t)m * 7 * G.N, G.N, G, n, x, y, z, h);
-                    else load7<TS, float, false>(g + (int64_t)m * 7 * G.N, G.N, G, n, x, y, z, h);
-                    for (int i = 0; i < 7; ++i) v[i] = h[i];
-                }
-                content = 1.0;
-                for (int i = 0; i < 7; ++i) content += v[i];
-                c = content;
+                double sum = 1.0;
+                for (int i = 0; i < 7; ++i) sum += ldd(g + ((int64_t)m * 7 + i) * K + k);
+                c = sum;
             } else {
-                c = imm[(int64_t)s * G.N + n];
-                content = c;
+                c = imm[(int64_t)s * K + k];
             }
-            atomicAdd(&shq[S + s], content);
+            atomicAdd(&shq[S_ + s], c);
             if (open) {
                 atomicAdd(&shq[s], c);
-                if (!isfinite(c)) atomicAdd(&shq[4 * S + M], 1.0);
-                // min / max through CAS on shared doubles
-                double cur = shq[2 * S + s];
+                if (!isfinite(c)) atomicAdd(&shq[4 * S_ + M], 1.0);
+                double cur = shq[2 * S_ + s];
                 while (c < cur) {
-                    unsigned long long old = atomicCAS((unsigned long long*)&shq[2 * S + s],
+                    unsigned long long old = atomicCAS((unsigned long long*)&shq[2 * S_ + s],
                                                        __double_as_longlong(cur), __double_as_longlong(c));
                     if (old == (unsigned long long)__double_as_longlong(cur)) break;
                     cur = __longlong_as_double(old);
                 }
-                cur = shq[3 * S + s];
+                cur = shq[3 * S_ + s];
                 while (c > cur) {
-                    unsigned long long old = atomicCAS((unsigned long long*)&shq[3 * S + s],
+                    unsigned long long old = atomicCAS((unsigned long long*)&shq[3 * S_ + s],
                                                        __double_as_longlong(cur), __double_as_longlong(c));
                     if (old == (unsigned long long)__double_as_longlong(cur)) break;
                     cur = __longlong_as_double(old);
@@ -349,10 +339,22 @@ __global__ void k_ade_reduce(const TS* __restrict__ g, const double* __restrict_
             }
         }
         if (inner)
-            for (int mb = 0; mb < M; ++mb) atomicAdd(&shq[4 * S + mb], bio[(int64_t)mb * G.N + n]);
+            for (int mb = 0; mb < M; ++mb) atomicAdd(&shq[4 * S_ + mb], bio[(int64_t)mb * K + k]);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < nq; q += blockDim.x) part[(int64_t)blockIdx.x * nq + q] = shq[q];
+}
+
+// dense [N] <-> compact [K] transfers of per-node FP64 fields
+__global__ void k_gather_dense(const double* __restrict__ dense, const int32_t* __restrict__ node, int64_t K,
+                               double* __restrict__ compact) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
+        compact[k] = dense[node[k]];
+}
+__global__ void k_scatter_dense(const double* __restrict__ compact, const int32_t* __restrict__ node, int64_t K,
+                                double* __restrict__ dense) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
+        dense[node[k]] = compact[k];
 }
 
 // ------------------------------------------------------------------ host side
@@ -362,16 +364,17 @@ static size_t usize(int prec) { return prec == CLB_F64 ? 8 : 4; }
 
 void ade_free(clb_handle* h) {
     cudaFree(h->d_g); h->d_g = nullptr;
+    cudaFree(h->d_glink); h->d_glink = nullptr;
     cudaFree(h->d_imm); h->d_imm = nullptr;
     cudaFree(h->d_bio); h->d_bio = nullptr;
     cudaFree(h->d_u); h->d_u = nullptr;
-    cudaFree(h->d_ade_list); h->d_ade_list = nullptr;
     cudaFree(h->d_neu); h->d_neu = nullptr;
+    sparse_free(h->ade_sp);
     h->ade_ready = false;
 }
 
 static int* mob_table(clb_handle* h) {
-    // device copy of the mobile-species table lives after the neumann buffer
+    // device copy of the mobile-species table lives after the boundary store
     return (int*)(h->d_neu + (size_t)h->S * 2 * h->g.plane);
 }
 
@@ -422,27 +425,32 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
 
     int8_t cls[MAX_CODES];
     for (int c = 0; c < MAX_CODES; ++c) cls[c] = (P.dyn[c] != ADE_BB);
-    std::vector<int32_t> list = build_list(h, cls);
-    const size_t N = (size_t)h->g.N;
+    clb_status st = sparse_build(h, cls, 7, h->ade_sp);
+    if (st != CLB_OK) return st;
+    const int64_t K = h->ade_sp.K, L = h->ade_sp.L;
+    int64_t kw = 0, ke = 0;
+    for (int64_t n = 0; n < h->g.plane; ++n) kw += cls[(uint8_t)h->h_mat[n] & 127] != 0;
+    for (int64_t n = h->g.N - h->g.plane; n < h->g.N; ++n) ke += cls[(uint8_t)h->h_mat[n] & 127] != 0;
+    h->ade_west_end = kw;
+    h->ade_east_begin = K - ke;
+    const size_t K1 = (size_t)std::max<int64_t>(1, K), L1 = (size_t)std::max<int64_t>(1, L);
+    const int nm1 = std::max(1, h->n_mobile);
     cudaError_t e;
-    if ((e = cudaMalloc(&h->d_g, esize(h->ade_prec) * 7 * N * std::max(1, h->n_mobile))) != cudaSuccess)
+    if ((e = cudaMalloc(&h->d_g, esize(h->ade_prec) * 7 * K1 * nm1)) != cudaSuccess)
         return cuda_check(h, e, "species populations");
-    if ((e = cudaMalloc(&h->d_imm, sizeof(double) * N * S)) != cudaSuccess) return cuda_check(h, e, "immobile fields");
-    if ((e = cudaMalloc(&h->d_u, usize(h->ade_prec) * 3 * N)) != cudaSuccess) return cuda_check(h, e, "velocity");
-    if ((e = cudaMalloc(&h->d_ade_list, sizeof(int32_t) * std::max<size_t>(1, list.size()))) != cudaSuccess)
-        return cuda_check(h, e, "ade list");
+    if ((e = cudaMalloc(&h->d_glink, esize(h->ade_prec) * L1 * nm1)) != cudaSuccess)
+        return cuda_check(h, e, "species links");
+    if ((e = cudaMalloc(&h->d_imm, sizeof(double) * K1 * S)) != cudaSuccess) return cuda_check(h, e, "immobile fields");
+    if ((e = cudaMalloc(&h->d_u, usize(h->ade_prec) * 3 * K1)) != cudaSuccess) return cuda_check(h, e, "velocity");
     if ((e = cudaMalloc(&h->d_neu, sizeof(double) * S * 2 * h->g.plane + sizeof(int) * 16)) != cudaSuccess)
         return cuda_check(h, e, "boundary store");
-    h->n_ade_list = (int64_t)list.size();
-    if (!list.empty())
-        cudaMemcpyAsync(h->d_ade_list, list.data(), sizeof(int32_t) * list.size(), cudaMemcpyHostToDevice, h->stream);
-    cudaMemsetAsync(h->d_u, 0, usize(h->ade_prec) * 3 * N, h->stream);
+    cudaMemsetAsync(h->d_u, 0, usize(h->ade_prec) * 3 * K1, h->stream);
     // immobile species: uniform c0 (initial_concentration applies to the whole domain)
-    std::vector<double> immh(N);
+    std::vector<double> immh(K1);
     for (int s = 0; s < S; ++s) {
         if (sp[s].mobile) continue;
         std::fill(immh.begin(), immh.end(), sp[s].c0);
-        cudaMemcpy(h->d_imm + (size_t)s * N, immh.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
+        cudaMemcpy(h->d_imm + (size_t)s * K1, immh.data(), sizeof(double) * K1, cudaMemcpyHostToDevice);
     }
     // stored boundary densities: Dirichlet value, else c0 (lattice.initialize() runs the
     // Neumann processor once on the equilibrium field)
@@ -458,15 +466,15 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
     int mt[16] = {0};
     for (size_t k = 0; k < mob.size(); ++k) mt[k] = mob[k];
     cudaMemcpy(mob_table(h), mt, sizeof(mt), cudaMemcpyHostToDevice);
-    double* dc0 = nullptr;
     if (!c0m.empty()) {
+        double* dc0 = nullptr;
         cudaMalloc(&dc0, sizeof(double) * c0m.size());
         cudaMemcpy(dc0, c0m.data(), sizeof(double) * c0m.size(), cudaMemcpyHostToDevice);
         const int grid = h->num_sms * 8;
         switch (h->ade_prec) {
-            case CLB_F64: k_ade_init<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g, h->g.N, h->n_mobile, dc0); break;
-            case CLB_F32: k_ade_init<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g, h->g.N, h->n_mobile, dc0); break;
-            default: k_ade_init<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g, h->g.N, h->n_mobile, dc0); break;
+            case CLB_F64: k_ade_init<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g, (double*)h->d_glink, K, L, h->n_mobile, dc0); break;
+            case CLB_F32: k_ade_init<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g, (float*)h->d_glink, K, L, h->n_mobile, dc0); break;
+            default: k_ade_init<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g, (__half*)h->d_glink, K, L, h->n_mobile, dc0); break;
         }
         cudaStreamSynchronize(h->stream);
         cudaFree(dc0);
@@ -489,6 +497,35 @@ clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm,
     return CLB_OK;
 }
 
+// dense [rows][N] host field <-> compact [rows][K] device field
+static clb_status to_compact(clb_handle* h, const double* host_dense, int rows, double* dev_compact) {
+    const int64_t N = h->g.N, K = h->ade_sp.K;
+    double* tmp = nullptr;
+    cudaError_t e = cudaMalloc(&tmp, sizeof(double) * N);
+    if (e != cudaSuccess) return cuda_check(h, e, "field buffer");
+    for (int r = 0; r < rows && e == cudaSuccess; ++r) {
+        e = cudaMemcpyAsync(tmp, host_dense + (size_t)r * N, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream);
+        k_gather_dense<<<h->num_sms * 4, 256, 0, h->stream>>>(tmp, h->ade_sp.node, K, dev_compact + (size_t)r * K);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    return cuda_check(h, e, "field upload");
+}
+
+static clb_status to_dense(clb_handle* h, const double* dev_compact, double fill, double* host_dense) {
+    const int64_t N = h->g.N, K = h->ade_sp.K;
+    std::vector<double> init((size_t)N, fill);
+    double* tmp = nullptr;
+    cudaError_t e = cudaMalloc(&tmp, sizeof(double) * N);
+    if (e != cudaSuccess) return cuda_check(h, e, "field buffer");
+    e = cudaMemcpyAsync(tmp, init.data(), sizeof(double) * N, cudaMemcpyHostToDevice, h->stream);
+    k_scatter_dense<<<h->num_sms * 4, 256, 0, h->stream>>>(dev_compact, h->ade_sp.node, K, tmp);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host_dense, tmp, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    return cuda_check(h, e, "field download");
+}
+
 clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (M < 0 || M > CLB_MAX_MICROBES) return fail(h, CLB_INVALID_ARG, "microbe count out of range");
@@ -497,10 +534,9 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
     h->M = M;
     h->ap.M = M;
     if (M == 0) return CLB_OK;
-    cudaError_t e = cudaMalloc(&h->d_bio, sizeof(double) * M * (size_t)h->g.N);
+    cudaError_t e = cudaMalloc(&h->d_bio, sizeof(double) * M * (size_t)std::max<int64_t>(1, h->ade_sp.K));
     if (e != cudaSuccess) return cuda_check(h, e, "biomass");
-    e = cudaMemcpy(h->d_bio, b, sizeof(double) * M * (size_t)h->g.N, cudaMemcpyHostToDevice);
-    return cuda_check(h, e, "biomass copy");
+    return to_compact(h, b, M, h->d_bio);
 }
 
 template <typename TS, typename TC, bool ODD>
@@ -508,11 +544,14 @@ static void launch_ade_t(clb_handle* h) {
     const int grid = h->ade_grid;
     const int nm = h->n_mobile;
     TS* g = (TS*)h->d_g;
+    TS* gl = (TS*)h->d_glink;
     const TC* u = (const TC*)h->d_u;
     int* mt = mob_table(h);
-#define CLB_ADE(NM)                                                                                        \
-    k_ade_aa<TS, TC, ODD, NM><<<grid, ADE_THREADS, 0, h->stream>>>(g, h->d_imm, h->d_bio, u, h->d_ade_list, \
-                                                                  h->n_ade_list, h->d_mat, h->d_neu, h->ap, nm, mt)
+    const SparseView S = view_of(h->ade_sp);
+#define CLB_ADE(NM)                                                                                          \
+    k_ade_aa<TS, TC, ODD, NM><<<grid, ADE_THREADS, 0, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, \
+                                                                  h->ap, nm, mt, h->ade_west_end,            \
+                                                                  h->ade_east_begin)
     if (nm <= 1) CLB_ADE(1);
     else if (nm <= 2) CLB_ADE(2);
     else if (nm <= 4) CLB_ADE(4);
@@ -521,26 +560,28 @@ static void launch_ade_t(clb_handle* h) {
 #undef CLB_ADE
 }
 
-template <typename TS, typename TC, bool ODD>
-static void launch_neumann(clb_handle* h) {
+template <typename TS, typename TC>
+static void launch_neumann(clb_handle* h, int odd) {
+    const SparseView S = view_of(h->ade_sp);
     for (int s = 0; s < h->S; ++s) {
         const int m = h->ap.slot[s];
         if (m < 0) continue;
         for (int side = 0; side < 2; ++side) {
             int t = side == 0 ? h->ap.ltype[s] : h->ap.rtype[s];
             if (t != CLB_NEUMANN) continue;
-            k_ade_neumann<TS, TC, ODD><<<std::max(1, std::min(h->num_sms * 2, (h->g.plane + 255) / 256)), 256, 0,
-                                         h->stream>>>((const TS*)h->d_g, h->d_mat, h->d_neu, h->ap, s, m, side);
+            k_ade_neumann<TS, TC><<<std::max(1, std::min(h->num_sms * 2, (h->g.plane + 255) / 256)), 256, 0,
+                                    h->stream>>>((const TS*)h->d_g, (const TS*)h->d_glink, S, h->d_mat, h->d_neu,
+                                                 h->ap, s, m, side, odd, h->ap.c0[s]);
         }
     }
 }
 
 static void refresh_neumann(clb_handle* h) {
-    const bool odd = (h->ade_iters & 1) != 0;
+    const int odd = (int)(h->ade_iters & 1);
     switch (h->ade_prec) {
-        case CLB_F64: if (odd) launch_neumann<double, double, true>(h); else launch_neumann<double, double, false>(h); break;
-        case CLB_F32: if (odd) launch_neumann<float, float, true>(h); else launch_neumann<float, float, false>(h); break;
-        default: if (odd) launch_neumann<__half, float, true>(h); else launch_neumann<__half, float, false>(h); break;
+        case CLB_F64: launch_neumann<double, double>(h, odd); break;
+        case CLB_F32: launch_neumann<float, float>(h, odd); break;
+        default: launch_neumann<__half, float>(h, odd); break;
     }
 }
 
@@ -549,19 +590,11 @@ clb_status ade_step(clb_handle* h, int n) {
     if (h->M > 0 && h->d_bio == nullptr) return fail(h, CLB_INVALID_ARG, "biomass missing");
     for (int k = 0; k < n; ++k) {
         const bool odd = (h->ade_iters & 1) != 0;
+        refresh_neumann(h);
         switch (h->ade_prec) {
-            case CLB_F64:
-                if (odd) { launch_neumann<double, double, true>(h); launch_ade_t<double, double, true>(h); }
-                else { launch_neumann<double, double, false>(h); launch_ade_t<double, double, false>(h); }
-                break;
-            case CLB_F32:
-                if (odd) { launch_neumann<float, float, true>(h); launch_ade_t<float, float, true>(h); }
-                else { launch_neumann<float, float, false>(h); launch_ade_t<float, float, false>(h); }
-                break;
-            default:
-                if (odd) { launch_neumann<__half, float, true>(h); launch_ade_t<__half, float, true>(h); }
-                else { launch_neumann<__half, float, false>(h); launch_ade_t<__half, float, false>(h); }
-                break;
+            case CLB_F64: if (odd) launch_ade_t<double, double, true>(h); else launch_ade_t<double, double, false>(h); break;
+            case CLB_F32: if (odd) launch_ade_t<float, float, true>(h); else launch_ade_t<float, float, false>(h); break;
+            default: if (odd) launch_ade_t<__half, float, true>(h); else launch_ade_t<__half, float, false>(h); break;
         }
         h->ade_iters += 1;
     }
@@ -571,7 +604,7 @@ clb_status ade_step(clb_handle* h, int n) {
 clb_status ade_couple(clb_handle* h) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
-    return flow_velocity(h, h->d_u, h->ade_prec == CLB_F64 ? 0 : 1, false);
+    return flow_velocity_at(h, h->ade_sp.node, h->ade_sp.K, h->d_u, h->ade_sp.K, h->ade_prec == CLB_F64 ? 0 : 1);
 }
 
 clb_status ade_populations(clb_handle* h, int s, double* host) {
@@ -583,11 +616,13 @@ clb_status ade_populations(clb_handle* h, int s, double* host) {
     if (e != cudaSuccess) return cuda_check(h, e, "population buffer");
     const int odd = (int)(h->ade_iters & 1);
     const int grid = h->num_sms * 8;
-    const size_t off = (size_t)m * 7 * h->g.N;
+    const size_t off = (size_t)m * 7 * h->ade_sp.K, loff = (size_t)m * h->ade_sp.L;
+    const SparseView S = view_of(h->ade_sp);
+    const double c0 = h->ap.c0[s];
     switch (h->ade_prec) {
-        case CLB_F64: k_ade_get_pops<double><<<grid, 256, 0, h->stream>>>((const double*)h->d_g + off, h->g, odd, buf); break;
-        case CLB_F32: k_ade_get_pops<float><<<grid, 256, 0, h->stream>>>((const float*)h->d_g + off, h->g, odd, buf); break;
-        default: k_ade_get_pops<__half><<<grid, 256, 0, h->stream>>>((const __half*)h->d_g + off, h->g, odd, buf); break;
+        case CLB_F64: k_ade_get_pops<double><<<grid, 256, 0, h->stream>>>((const double*)h->d_g + off, (const double*)h->d_glink + loff, S, h->g, odd, c0, buf); break;
+        case CLB_F32: k_ade_get_pops<float><<<grid, 256, 0, h->stream>>>((const float*)h->d_g + off, (const float*)h->d_glink + loff, S, h->g, odd, c0, buf); break;
+        default: k_ade_get_pops<__half><<<grid, 256, 0, h->stream>>>((const __half*)h->d_g + off, (const __half*)h->d_glink + loff, S, h->g, odd, c0, buf); break;
     }
     e = cudaMemcpyAsync(host, buf, sizeof(double) * 7 * (size_t)h->g.N, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -605,11 +640,12 @@ clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
     cudaMemcpy(buf, host, sizeof(double) * 7 * (size_t)h->g.N, cudaMemcpyHostToDevice);
     const int odd = (int)(h->ade_iters & 1);
     const int grid = h->num_sms * 8;
-    const size_t off = (size_t)m * 7 * h->g.N;
+    const size_t off = (size_t)m * 7 * h->ade_sp.K, loff = (size_t)m * h->ade_sp.L;
+    const SparseView S = view_of(h->ade_sp);
     switch (h->ade_prec) {
-        case CLB_F64: k_ade_set_pops<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g + off, h->g, odd, buf); break;
-        case CLB_F32: k_ade_set_pops<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g + off, h->g, odd, buf); break;
-        default: k_ade_set_pops<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g + off, h->g, odd, buf); break;
+        case CLB_F64: k_ade_set_pops<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g + off, (double*)h->d_glink + loff, S, h->g, odd, buf); break;
+        case CLB_F32: k_ade_set_pops<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g + off, (float*)h->d_glink + loff, S, h->g, odd, buf); break;
+        default: k_ade_set_pops<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g + off, (__half*)h->d_glink + loff, S, h->g, odd, buf); break;
     }
     e = cudaStreamSynchronize(h->stream);
     cudaFree(buf);
@@ -617,15 +653,12 @@ clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
 }
 
 // computeDensity: BGK nodes of a Dirichlet / Neumann plane report the stored value; every
-// other node the sum of its populations + 1; immobile species their field.
+// other node the sum of its populations + 1; immobile species their field (zero off the nodes).
 clb_status ade_density(clb_handle* h, int s, double* host) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
     const size_t N = (size_t)h->g.N;
-    if (h->ap.slot[s] < 0) {
-        cudaError_t e = cudaMemcpy(host, h->d_imm + (size_t)s * N, sizeof(double) * N, cudaMemcpyDeviceToHost);
-        return cuda_check(h, e, "immobile copy");
-    }
+    if (h->ap.slot[s] < 0) return to_dense(h, h->d_imm + (size_t)s * std::max<int64_t>(1, h->ade_sp.K), h->ap.c0[s], host);
     // the Neumann planes' stored values as the reference holds them after the last stream
     refresh_neumann(h);
     std::vector<double> pops(7 * N);
@@ -656,18 +689,55 @@ clb_status ade_density(clb_handle* h, int s, double* host) {
 
 clb_status ade_biomass(clb_handle* h, int m, double* host) {
     if (!h->ade_ready || m < 0 || m >= h->M) return fail(h, CLB_INVALID_ARG, "no such biomass field");
-    cudaError_t e = cudaMemcpy(host, h->d_bio + (size_t)m * h->g.N, sizeof(double) * h->g.N, cudaMemcpyDeviceToHost);
-    return cuda_check(h, e, "biomass copy");
+    return to_dense(h, h->d_bio + (size_t)m * std::max<int64_t>(1, h->ade_sp.K), 0.0, host);
+}
+
+clb_status ade_set_biomass_field(clb_handle* h, int m, const double* host) {
+    if (!h->ade_ready || m < 0 || m >= h->M) return fail(h, CLB_INVALID_ARG, "no such biomass field");
+    return to_compact(h, host, 1, h->d_bio + (size_t)m * std::max<int64_t>(1, h->ade_sp.K));
+}
+
+__global__ void k_u_to_dense(const void* __restrict__ u, int f64, const int32_t* __restrict__ node, int64_t K,
+                             int64_t N, double* __restrict__ out) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
+        for (int a = 0; a < 3; ++a)
+            out[a * N + node[k]] = f64 ? ((const double*)u)[a * K + k] : (double)((const float*)u)[a * K + k];
+}
+
+__global__ void k_u_to_compact(const double* __restrict__ in, int f64, const int32_t* __restrict__ node, int64_t K,
+                               int64_t N, void* __restrict__ u) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
+        for (int a = 0; a < 3; ++a) {
+            if (f64) ((double*)u)[a * K + k] = in[a * N + node[k]];
+            else ((float*)u)[a * K + k] = (float)in[a * N + node[k]];
+        }
 }
 
 clb_status ade_velocity(clb_handle* h, double* host) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     const size_t N = (size_t)h->g.N;
-    if (h->ade_prec == CLB_F64) return cuda_check(h, cudaMemcpy(host, h->d_u, 8 * 3 * N, cudaMemcpyDeviceToHost), "u");
-    std::vector<float> tmp(3 * N);
-    cudaError_t e = cudaMemcpy(tmp.data(), h->d_u, 4 * 3 * N, cudaMemcpyDeviceToHost);
-    for (size_t k = 0; k < 3 * N; ++k) host[k] = tmp[k];
-    return cuda_check(h, e, "u");
+    double* tmp = nullptr;
+    cudaError_t e = cudaMalloc(&tmp, sizeof(double) * 3 * N);
+    if (e != cudaSuccess) return cuda_check(h, e, "velocity buffer");
+    cudaMemsetAsync(tmp, 0, sizeof(double) * 3 * N, h->stream);
+    k_u_to_dense<<<h->num_sms * 4, 256, 0, h->stream>>>(h->d_u, h->ade_prec == CLB_F64, h->ade_sp.node, h->ade_sp.K, N, tmp);
+    e = cudaMemcpyAsync(host, tmp, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    return cuda_check(h, e, "velocity copy");
+}
+
+clb_status ade_set_velocity(clb_handle* h, const double* host) {
+    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+    const size_t N = (size_t)h->g.N;
+    double* tmp = nullptr;
+    cudaError_t e = cudaMalloc(&tmp, sizeof(double) * 3 * N);
+    if (e != cudaSuccess) return cuda_check(h, e, "velocity buffer");
+    e = cudaMemcpyAsync(tmp, host, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, h->stream);
+    k_u_to_compact<<<h->num_sms * 4, 256, 0, h->stream>>>(tmp, h->ade_prec == CLB_F64, h->ade_sp.node, h->ade_sp.K, N, h->d_u);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    return cuda_check(h, e, "velocity upload");
 }
 
 clb_status ade_reduce(clb_handle* h, clb_stats* out) {
@@ -679,13 +749,13 @@ clb_status ade_reduce(clb_handle* h, clb_stats* out) {
     double* part = nullptr;
     cudaError_t e = cudaMalloc(&part, sizeof(double) * nq * grid);
     if (e != cudaSuccess) return cuda_check(h, e, "reduce buffer");
-    const int odd = (int)(h->ade_iters & 1);
     int* mt = mob_table(h);
     const size_t sh = sizeof(double) * nq;
+    const SparseView Sv = view_of(h->ade_sp);
     switch (h->ade_prec) {
-        case CLB_F64: k_ade_reduce<double><<<grid, 256, sh, h->stream>>>((const double*)h->d_g, h->d_imm, h->d_bio, h->d_mat, h->ap, h->n_mobile, mt, odd, part, nq); break;
-        case CLB_F32: k_ade_reduce<float><<<grid, 256, sh, h->stream>>>((const float*)h->d_g, h->d_imm, h->d_bio, h->d_mat, h->ap, h->n_mobile, mt, odd, part, nq); break;
-        default: k_ade_reduce<__half><<<grid, 256, sh, h->stream>>>((const __half*)h->d_g, h->d_imm, h->d_bio, h->d_mat, h->ap, h->n_mobile, mt, odd, part, nq); break;
+        case CLB_F64: k_ade_reduce<double><<<grid, 256, sh, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
+        case CLB_F32: k_ade_reduce<float><<<grid, 256, sh, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
+        default: k_ade_reduce<__half><<<grid, 256, sh, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
     }
     std::vector<double> hp((size_t)nq * grid);
     e = cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, h->stream);

@@ -260,21 +260,8 @@ clb_status clb_set_field(clb_handle* h, int field, int index, const void* host, 
             if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
             return flow_set_populations(h, (const double*)host);
         case CLB_FIELD_ADE_POPULATIONS: return ade_set_populations(h, index, (const double*)host);
-        case CLB_FIELD_ADE_VELOCITY: {
-            if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
-            const size_t N = (size_t)h->g.N;
-            const double* src = (const double*)host;
-            if (h->ade_prec == CLB_F64)
-                return cuda_check(h, cudaMemcpy(h->d_u, src, 8 * 3 * N, cudaMemcpyHostToDevice), "u");
-            std::vector<float> tmp(3 * N);
-            for (size_t k = 0; k < 3 * N; ++k) tmp[k] = (float)src[k];
-            return cuda_check(h, cudaMemcpy(h->d_u, tmp.data(), 4 * 3 * N, cudaMemcpyHostToDevice), "u");
-        }
-        case CLB_FIELD_BIOMASS: {
-            if (!h->ade_ready || index < 0 || index >= h->M) return fail(h, CLB_INVALID_ARG, "no such biomass field");
-            return cuda_check(h, cudaMemcpy(h->d_bio + (size_t)index * h->g.N, host, 8 * (size_t)h->g.N,
-                                            cudaMemcpyHostToDevice), "biomass");
-        }
+        case CLB_FIELD_ADE_VELOCITY: return ade_set_velocity(h, (const double*)host);
+        case CLB_FIELD_BIOMASS: return ade_set_biomass_field(h, index, (const double*)host);
         default: return fail(h, CLB_INVALID_ARG, "field is read-only");
     }
 }

@@ -50,6 +50,10 @@ template <typename TS, typename TC>
 __device__ __forceinline__ TC ld(const TS* p) { return (TC)(*p); }
 template <>
 __device__ __forceinline__ float ld<__half, float>(const __half* p) { return __half2float(*p); }
+template <typename TS>
+__device__ __forceinline__ double ldd(const TS* p) { return (double)(*p); }
+template <>
+__device__ __forceinline__ double ldd<__half>(const __half* p) { return (double)__half2float(*p); }
 template <typename TS, typename TC>
 __device__ __forceinline__ void st(TS* p, TC v) { *p = (TS)v; }
 template <>
@@ -116,6 +120,22 @@ struct AdeParams {
 
 }  // namespace clb
 
+namespace clb {
+// Host-owned device buffers of one compacted node layout (sparse.cuh).
+struct SparseBuffers {
+    int32_t* node = nullptr;
+    int8_t* code = nullptr;
+    uint32_t* wall = nullptr;
+    int32_t* linkbase = nullptr;
+    int32_t* rowstart = nullptr;
+    uint32_t* rowmask = nullptr;
+    int32_t* rowpre = nullptr;
+    int32_t* idx_of = nullptr;
+    int64_t K = 0, L = 0;
+    int W = 0;
+};
+}  // namespace clb
+
 // ------------------------------------------------------------------ the handle
 struct clb_handle_s {
     clb_domain_desc d;
@@ -131,9 +151,10 @@ struct clb_handle_s {
     // flow
     bool flow_ready = false;
     int flow_prec = CLB_F32;
-    void* d_f = nullptr;              // [19][N] storage type
-    int32_t* d_flow_list = nullptr;   // active (collide or stream) nodes, lexicographic
-    int64_t n_flow_list = 0;
+    void* d_f = nullptr;              // [19][K] storage type, compacted stored nodes
+    void* d_flink = nullptr;          // [L] wall link slots
+    clb::SparseBuffers flow_sp;
+    int64_t k_west_end = 0, k_east_begin = 0;  // compact index ranges of the planes x=0, x=nx-1
     clb::FlowParams fp;
     clb::Tracer* d_tracer = nullptr;
     double* d_partials = nullptr;     // per-block partial sums (scratch)
@@ -147,12 +168,13 @@ struct clb_handle_s {
     int ade_prec = CLB_F32;
     int S = 0, n_mobile = 0, M = 0;
     std::vector<clb_species_desc> species;
-    void* d_g = nullptr;              // [n_mobile][7][N] storage type
-    double* d_imm = nullptr;          // [S][N] immobile concentrations (unused rows stay empty)
-    double* d_bio = nullptr;          // [M][N] biomass
-    float* d_u = nullptr;             // [3][N] advection velocity
-    int32_t* d_ade_list = nullptr;
-    int64_t n_ade_list = 0;
+    void* d_g = nullptr;              // [n_mobile][7][K] storage type, compacted stored nodes
+    void* d_glink = nullptr;          // [n_mobile][L] wall link slots
+    clb::SparseBuffers ade_sp;
+    int64_t ade_west_end = 0, ade_east_begin = 0;
+    double* d_imm = nullptr;          // [S][K] immobile concentrations (unused rows stay empty)
+    double* d_bio = nullptr;          // [M][K] biomass
+    void* d_u = nullptr;              // [3][K] advection velocity (arithmetic type)
     double* d_neu = nullptr;          // [S][2][ny*nz] stored boundary densities
     clb::AdeParams ap;
     int64_t ade_iters = 0;
@@ -170,6 +192,7 @@ clb_status flow_step(clb_handle* h, int n, bool trace, double eps);
 clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations);
 clb_status flow_stats(clb_handle* h, double char_length, clb_flow_stats* out);
 clb_status flow_velocity(clb_handle* h, void* dst, int dtype_device, bool to_host);
+clb_status flow_velocity_at(clb_handle* h, const int32_t* nodes, int64_t count, void* u, int64_t stride, int dtype);
 clb_status flow_populations(clb_handle* h, double* host);
 clb_status flow_set_populations(clb_handle* h, const double* host);
 void flow_free(clb_handle* h);
@@ -185,6 +208,8 @@ clb_status ade_populations(clb_handle* h, int s, double* host);
 clb_status ade_set_populations(clb_handle* h, int s, const double* host);
 clb_status ade_biomass(clb_handle* h, int m, double* host);
 clb_status ade_velocity(clb_handle* h, double* host);
+clb_status ade_set_velocity(clb_handle* h, const double* host);
+clb_status ade_set_biomass_field(clb_handle* h, int m, const double* host);
 clb_status ade_reduce(clb_handle* h, clb_stats* out);
 void ade_free(clb_handle* h);
 

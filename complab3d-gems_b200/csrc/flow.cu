@@ -8,20 +8,23 @@
 //   through), Palabos' local regularized density boundary on the planes x = 0 (rho = 1) and
 //   x = nx-1 (rho = 1 - 3 dP), reflection of populations whose source lies outside the box.
 //
-// Layout: populations direction-major f[19][N] (N = nx*ny*nz, x slowest, z fastest) of the
-// storage type; one array, updated in place with the AA pattern:
-//   even step: node x reads f[i][x], collides, writes outgoing i to f[opp(i)][x];
-//   odd step:  node x reads incoming i from f[opp(i)][x - c_i], collides, writes outgoing
-//              i to f[i][x + c_i].
-// Each slot is read and written by exactly one node per step, so a step needs no second
-// array and no synchronisation. A bounce-back node is a no-op in both steps (its swap is the
-// identity on its AA slots), so only collide-or-stream nodes are launched: a compacted list
-// of them, in lexicographic order. A source or destination outside the box maps to the node's
-// own opposite slot, which is Palabos' reflection at the block edge.
+// Layout: only collide-or-stream nodes are stored (sparse.cuh): f[19][K] of the storage type
+// in lexicographic node order, plus one link slot per (node, direction into a wall). One array,
+// updated in place with the AA pattern:
+//   even step: node a reads f[i][a], collides, writes outgoing i to f[opp(i)][a];
+//   odd step:  node a reads incoming i from f[opp(i)][a - c_i], collides, writes outgoing
+//              i to f[i][a + c_i].
+// Each slot is read and written by exactly one node per step, so a step needs no second array
+// and no synchronisation. A full-way bounce-back node is the identity on its AA slots, so it is
+// never launched; the slot f[i][b] of a wall node b that its fluid neighbour a = b - c_i writes
+// on an odd step (and reads back two steps later) is a's link slot for direction i. A source or
+// destination outside the box maps to the node's own opposite slot: Palabos' reflection at the
+// block edge. The even step touches only the node's own slots (perfectly coalesced); the odd
+// step finds neighbours through the row bitmasks.
 //
-// Algorithmic bytes per node update: 2 * 19 * sizeof(storage) (+1 byte material, +4 bytes
-// list index that count against the roofline fraction).
-#include "clb_internal.cuh"
+// Algorithmic bytes per node update: 2 * 19 * sizeof(storage). Metadata read per node: 1 byte
+// material code (both steps), 12 bytes dense index + wall mask + link base (odd step only).
+#include "sparse.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -71,43 +74,6 @@ __device__ __forceinline__ void regularize19(TC (&g)[19], int orient, TC rb) {
         TC s = (cx * cx - third) * pxx + (cy * cy - third) * pyy + (cz * cz - third) * pzz +
                (TC)2 * (cx * cy * pxy + cx * cz * pxz + cy * cz * pyz);
         g[i] = feq19<TC>(i, rb, jx, (TC)0, (TC)0, jsq) + (TC)q19w(i) * (TC)4.5 * s;
-    }
-}
-
-template <typename TS, typename TC, bool ODD>
-__device__ __forceinline__ void load19(const TS* __restrict__ f, int64_t N, const Geom& G, int64_t n, int x, int y,
-                                       int z, TC (&g)[19]) {
-#pragma unroll
-    for (int i = 0; i < 19; ++i) {
-        if (!ODD || i == 0) {
-            g[i] = ld<TS, TC>(f + (int64_t)i * N + n);
-        } else {
-            const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i);
-            const bool in = (cx == 0 || ((unsigned)(x - cx) < (unsigned)G.nx)) &&
-                            (cy == 0 || ((unsigned)(y - cy) < (unsigned)G.ny)) &&
-                            (cz == 0 || ((unsigned)(z - cz) < (unsigned)G.nz));
-            const int64_t off = (int64_t)cx * G.plane + cy * G.nz + cz;
-            g[i] = in ? ld<TS, TC>(f + (int64_t)q19opp(i) * N + n - off) : ld<TS, TC>(f + (int64_t)i * N + n);
-        }
-    }
-}
-
-template <typename TS, typename TC, bool ODD>
-__device__ __forceinline__ void store19(TS* __restrict__ f, int64_t N, const Geom& G, int64_t n, int x, int y, int z,
-                                        const TC (&o)[19]) {
-#pragma unroll
-    for (int i = 0; i < 19; ++i) {
-        if (!ODD || i == 0) {
-            st<TS, TC>(f + (int64_t)q19opp(i) * N + n, o[i]);
-        } else {
-            const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i);
-            const bool in = (cx == 0 || ((unsigned)(x + cx) < (unsigned)G.nx)) &&
-                            (cy == 0 || ((unsigned)(y + cy) < (unsigned)G.ny)) &&
-                            (cz == 0 || ((unsigned)(z + cz) < (unsigned)G.nz));
-            const int64_t off = (int64_t)cx * G.plane + cy * G.nz + cz;
-            if (in) st<TS, TC>(f + (int64_t)i * N + n + off, o[i]);
-            else st<TS, TC>(f + (int64_t)q19opp(i) * N + n, o[i]);
-        }
     }
 }
 
@@ -179,24 +145,67 @@ __device__ void finish_step(Tracer* tr, double* partials, double block_total, in
     (void)s_energy;
 }
 
+
+// slot of row (dx, dy) among the 3x3 neighbourhood of a row
+__host__ __device__ constexpr int rslot(int dx, int dy) { return (dx + 1) * 3 + (dy + 1); }
+
 template <typename TS, typename TC, bool ODD>
-__global__ void __launch_bounds__(FLOW_THREADS)
-    k_flow_aa(TS* __restrict__ f, const int32_t* __restrict__ list, int64_t nlist, const int8_t* __restrict__ mat,
-              const FlowParams P, Tracer* __restrict__ tr, double* __restrict__ partials, int trace) {
+__global__ void __launch_bounds__(FLOW_THREADS, 3)
+    k_flow_aa(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const FlowParams P,
+              Tracer* __restrict__ tr, double* __restrict__ partials, int trace, int64_t k_west_end,
+              int64_t k_east_begin) {
     if (trace && tr->converged) return;  // a batch continues past convergence as no-ops
     const Geom G = P.g;
-    const int64_t N = G.N;
+    const int64_t K = S.K;
     double esum = 0;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nlist; k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t n = list[k];
-        int x, y, z;
-        decode(G, n, x, y, z);
-        const int code = mat[n];
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
+        const int code = S.code[k];
         TC g[19];
-        load19<TS, TC, ODD>(f, N, G, n, x, y, z, g);
+        int x = 0, y = 0, z = 0, rb_[9];
+        uint32_t wm = 0, rbit = 0;
+        int lb = 0;
+        if (!ODD) {
+#pragma unroll
+            for (int i = 0; i < 19; ++i) g[i] = ld<TS, TC>(f + (int64_t)i * K + k);
+        } else {
+            decode(G, S.node[k], x, y, z);
+            wm = S.wall[k];
+            lb = S.linkbase[k];
+            const int r = x * G.ny + y;
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int s = rslot(dx, dy);
+                    rb_[s] = 0;
+                    if ((dx == 0 && dy == 0) || (unsigned)(x + dx) >= (unsigned)G.nx ||
+                        (unsigned)(y + dy) >= (unsigned)G.ny)
+                        continue;
+                    const int rr = r + dx * G.ny + dy;
+                    rb_[s] = row_rank(S, rr, z);
+                    rbit |= (uint32_t)row_bit(S, rr, z) << s;
+                }
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                if (i == 0) { g[0] = ld<TS, TC>(f + k); continue; }
+                const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
+                const bool in = (cx == 0 || (unsigned)(x - cx) < (unsigned)G.nx) &&
+                                (cy == 0 || (unsigned)(y - cy) < (unsigned)G.ny) &&
+                                (cz == 0 || (unsigned)(z - cz) < (unsigned)G.nz);
+                if (!in) { g[i] = ld<TS, TC>(f + (int64_t)i * K + k); continue; }
+                if ((wm >> oi) & 1u) { g[i] = ld<TS, TC>(link + lb + __popc(wm & ((1u << oi) - 1u))); continue; }
+                int64_t src;
+                if (cx == 0 && cy == 0) src = k - cz;
+                else {
+                    const int s = rslot(-cx, -cy);
+                    src = (cz == 0) ? rb_[s] : (-cz > 0 ? rb_[s] + ((rbit >> s) & 1u) : rb_[s] - 1);
+                }
+                g[i] = ld<TS, TC>(f + (int64_t)oi * K + src);
+            }
+        }
         if (P.dyn[code] == DYN_BGK) {
-            if (x == 0) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
-            else if (x == G.nx - 1) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
+            if (k < k_west_end) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
+            else if (k >= k_east_begin) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
             TC rb = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
             for (int i = 0; i < 19; ++i) {
@@ -212,58 +221,78 @@ __global__ void __launch_bounds__(FLOW_THREADS)
             for (int i = 0; i < 19; ++i) g[i] = g[i] * omw + w * feq19<TC>(i, rb, jx, jy, jz, jsq);
             esum += (double)jsq;
         }
-        store19<TS, TC, ODD>(f, N, G, n, x, y, z, g);
+        if (!ODD) {
+#pragma unroll
+            for (int i = 0; i < 19; ++i) st<TS, TC>(f + (int64_t)q19opp(i) * K + k, g[i]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                if (i == 0) { st<TS, TC>(f + k, g[0]); continue; }
+                const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
+                const bool in = (cx == 0 || (unsigned)(x + cx) < (unsigned)G.nx) &&
+                                (cy == 0 || (unsigned)(y + cy) < (unsigned)G.ny) &&
+                                (cz == 0 || (unsigned)(z + cz) < (unsigned)G.nz);
+                if (!in) { st<TS, TC>(f + (int64_t)oi * K + k, g[i]); continue; }
+                if ((wm >> i) & 1u) { st<TS, TC>(link + lb + __popc(wm & ((1u << i) - 1u)), g[i]); continue; }
+                int64_t dst;
+                if (cx == 0 && cy == 0) dst = k + cz;
+                else {
+                    const int s = rslot(cx, cy);
+                    dst = (cz == 0) ? rb_[s] : (cz > 0 ? rb_[s] + ((rbit >> s) & 1u) : rb_[s] - 1);
+                }
+                st<TS, TC>(f + (int64_t)i * K + dst, g[i]);
+            }
+        }
     }
     __shared__ double sh[32];
     double bt = block_sum(esum, sh);
     finish_step(tr, partials, bt, P.n_bgk, trace);
 }
 
-// PressureGradient equilibrium (complab_functions.hh:82-94): BGK nodes t_i (rho(x) - 1),
-// every other node zero (BounceBack / NoDynamics equilibria are zero).
+// PressureGradient equilibrium (complab_functions.hh:82-94): BGK nodes t_i (rho(x) - 1); no-dynamics
+// nodes and the wall link slots zero (BounceBack / NoDynamics equilibria are zero).
 template <typename TS>
-__global__ void k_flow_init(TS* __restrict__ f, const int8_t* __restrict__ mat, const FlowParams P, double delta_p) {
+__global__ void k_flow_init(TS* __restrict__ f, const SparseView S, const FlowParams P, double delta_p) {
     const Geom G = P.g;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(n / G.plane);
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < S.K; k += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(S.node[k] / G.plane);
         const double rho = 1.0 - delta_p * 3.0 / (double)(G.nx - 1) * (double)x;
-        const bool bgk = P.dyn[mat[n]] == DYN_BGK;
+        const bool bgk = P.dyn[S.code[k]] == DYN_BGK;
 #pragma unroll
         for (int i = 0; i < 19; ++i) {
             double v = bgk ? q19w(i) * (rho - 1.0) : 0.0;
-            if constexpr (std::is_same<TS, __half>::value) f[(int64_t)i * G.N + n] = __double2half(v);
-            else f[(int64_t)i * G.N + n] = (TS)v;
+            if constexpr (std::is_same<TS, __half>::value) f[(int64_t)i * S.K + k] = __double2half(v);
+            else f[(int64_t)i * S.K + k] = (TS)v;
         }
     }
 }
 
-// computeVelocity of every node: BGK u = j; pressure-plane BGK nodes (j_x from the known
-// populations, 0, 0); others 0. The incoming populations are gathered with the parity rule,
-// which holds for unlaunched bounce-back nodes too.
+// computeVelocity at the dense nodes `nodes[0..count)` (all nodes when nodes == nullptr):
+// BGK u = j; pressure-plane BGK nodes (j_x from the known populations, 0, 0); others 0.
+// Output u[3][stride] at position t (the node's rank in `nodes`).
 template <typename TS, typename TC, typename TO>
-__global__ void k_flow_velocity(const TS* __restrict__ f, const int8_t* __restrict__ mat, const FlowParams P, int odd,
-                                TO* __restrict__ u) {
+__global__ void k_flow_velocity(const TS* __restrict__ f, const TS* __restrict__ link, const SparseView S,
+                                const int8_t* __restrict__ mat, const FlowParams P, int odd,
+                                const int32_t* __restrict__ nodes, int64_t count, TO* __restrict__ u, int64_t stride) {
     const Geom G = P.g;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        decode(G, n, x, y, z);
-        TC g[19];
-        if (odd) load19<TS, TC, true>(f, G.N, G, n, x, y, z, g);
-        else load19<TS, TC, false>(f, G.N, G, n, x, y, z, g);
+    const TC zero[19] = {};
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n = nodes ? nodes[t] : t;
         TC jx = 0, jy = 0, jz = 0;
         if (P.dyn[mat[n]] == DYN_BGK) {
+            TC g[19];
+            natural<TS, TC, 19>(S, G, f, link, n, odd, zero, g);
+            const int x = (int)(n / G.plane);
             if (x == 0 || x == G.nx - 1) {
                 const int o = (x == 0) ? -1 : 1;
                 const TC rb = (TC)((x == 0 ? P.rho_w : P.rho_e) - 1.0);
                 TC r0 = 0, rn = 0;
-#pragma unroll
                 for (int i = 0; i < 19; ++i) {
                     if (q19cx(i) == 0) r0 += g[i];
                     else if (q19cx(i) == o) rn += g[i];
                 }
                 jx = (TC)o * (r0 + (TC)2 * rn - rb);
             } else {
-#pragma unroll
                 for (int i = 0; i < 19; ++i) {
                     jx += (TC)q19cx(i) * g[i];
                     jy += (TC)q19cy(i) * g[i];
@@ -271,56 +300,33 @@ __global__ void k_flow_velocity(const TS* __restrict__ f, const int8_t* __restri
                 }
             }
         }
-        u[n] = (TO)jx;
-        u[G.N + n] = (TO)jy;
-        u[2 * G.N + n] = (TO)jz;
+        u[t] = (TO)jx;
+        u[stride + t] = (TO)jy;
+        u[2 * stride + t] = (TO)jz;
     }
 }
 
-// Incoming populations in natural layout, or back from it (scatter through the parity rule).
 template <typename TS>
-__global__ void k_flow_get_pops(const TS* __restrict__ f, const FlowParams P, int odd, double* __restrict__ out) {
-    const Geom G = P.g;
+__global__ void k_flow_get_pops(const TS* __restrict__ f, const TS* __restrict__ link, const SparseView S,
+                                const Geom G, int odd, double* __restrict__ out) {
+    const double zero[19] = {};
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        decode(G, n, x, y, z);
         double g[19];
-        if constexpr (std::is_same<TS, double>::value) {
-            if (odd) load19<TS, double, true>(f, G.N, G, n, x, y, z, g);
-            else load19<TS, double, false>(f, G.N, G, n, x, y, z, g);
-        } else {
-            float h[19];
-            if (odd) load19<TS, float, true>(f, G.N, G, n, x, y, z, h);
-            else load19<TS, float, false>(f, G.N, G, n, x, y, z, h);
-            for (int i = 0; i < 19; ++i) g[i] = h[i];
-        }
+        natural<TS, double, 19>(S, G, f, link, n, odd, zero, g);
         for (int i = 0; i < 19; ++i) out[(int64_t)i * G.N + n] = g[i];
     }
 }
 
 template <typename TS>
-__global__ void k_flow_set_pops(TS* __restrict__ f, const FlowParams P, int odd, const double* __restrict__ in) {
-    const Geom G = P.g;
+__global__ void k_flow_set_pops(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const Geom G, int odd,
+                                const double* __restrict__ in) {
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        decode(G, n, x, y, z);
-        for (int i = 0; i < 19; ++i) {
-            int64_t slot = (int64_t)i * G.N + n;
-            if (odd && i != 0) {
-                const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i);
-                const bool inb = ((unsigned)(x - cx) < (unsigned)G.nx) && ((unsigned)(y - cy) < (unsigned)G.ny) &&
-                                 ((unsigned)(z - cz) < (unsigned)G.nz);
-                const int64_t off = (int64_t)cx * G.plane + cy * G.nz + cz;
-                if (inb) slot = (int64_t)q19opp(i) * G.N + n - off;
-            }
-            double v = in[(int64_t)i * G.N + n];
-            if constexpr (std::is_same<TS, __half>::value) f[slot] = __double2half(v);
-            else f[slot] = (TS)v;
-        }
+        double g[19];
+        for (int i = 0; i < 19; ++i) g[i] = in[(int64_t)i * G.N + n];
+        put_natural<TS, 19>(S, G, f, link, n, odd, g);
     }
 }
 
-// FP64 plane / volume statistics of the velocity field (complab.cpp:1136-1160).
 __global__ void k_flow_vstats(const double* __restrict__ u, const Geom G, double* __restrict__ acc) {
     // acc[0] sum |u| over x=1..nx-2, acc[1] max u_x (as ordered bits), acc[2] sum u_x on x=nx-2
     __shared__ double sh[32];
@@ -354,6 +360,9 @@ __global__ void k_flow_vstats(const double* __restrict__ u, const Geom G, double
 
 // ------------------------------------------------------------------ host side
 
+
+// ------------------------------------------------------------------ host side
+
 static size_t storage_size(int prec) { return prec == CLB_F64 ? 8 : (prec == CLB_F32 ? 4 : 2); }
 
 template <typename F>
@@ -366,7 +375,8 @@ static int grid_for(clb_handle* h, F kernel, int threads) {
 
 void flow_free(clb_handle* h) {
     cudaFree(h->d_f); h->d_f = nullptr;
-    cudaFree(h->d_flow_list); h->d_flow_list = nullptr;
+    cudaFree(h->d_flink); h->d_flink = nullptr;
+    sparse_free(h->flow_sp);
     cudaFree(h->d_tracer); h->d_tracer = nullptr;
     cudaFree(h->d_partials); h->d_partials = nullptr;
     h->flow_ready = false;
@@ -396,42 +406,52 @@ clb_status flow_init(clb_handle* h, double delta_p) {
     P.rho_w = 1.0;
     P.rho_e = 1.0 - delta_p * 3.0;
     h->delta_p = delta_p;
-    int64_t nbgk = 0;
-    for (int64_t n = 0; n < h->g.N; ++n) nbgk += (P.dyn[(uint8_t)h->h_mat[n]] == DYN_BGK);
+    int64_t nbgk = 0, kw = 0, ke = 0;
+    for (int64_t n = 0; n < h->g.N; ++n) {
+        const int dn = P.dyn[(uint8_t)h->h_mat[n]];
+        nbgk += (dn == DYN_BGK);
+        if (dn != DYN_BB) {
+            if (n < h->g.plane) ++kw;
+            if (n >= h->g.N - h->g.plane) ++ke;
+        }
+    }
     P.n_bgk = nbgk;
 
+    flow_free(h);
     int8_t cls[MAX_CODES];
     for (int c = 0; c < MAX_CODES; ++c) cls[c] = (P.dyn[c] != DYN_BB);
-    std::vector<int32_t> list = build_list(h, cls);
-
-    flow_free(h);
+    clb_status s = sparse_build(h, cls, 19, h->flow_sp);
+    if (s != CLB_OK) return s;
+    const int64_t K = h->flow_sp.K;
+    h->k_west_end = kw;
+    h->k_east_begin = K - ke;
     h->flow_prec = d.flow_precision;
     const size_t es = storage_size(h->flow_prec);
     cudaError_t e;
-    if ((e = cudaMalloc(&h->d_f, es * 19 * (size_t)h->g.N)) != cudaSuccess) return cuda_check(h, e, "flow populations");
-    if ((e = cudaMalloc(&h->d_flow_list, sizeof(int32_t) * std::max<size_t>(1, list.size()))) != cudaSuccess)
-        return cuda_check(h, e, "flow list");
+    if ((e = cudaMalloc(&h->d_f, es * 19 * (size_t)std::max<int64_t>(1, K))) != cudaSuccess)
+        return cuda_check(h, e, "flow populations");
+    if ((e = cudaMalloc(&h->d_flink, es * (size_t)std::max<int64_t>(1, h->flow_sp.L))) != cudaSuccess)
+        return cuda_check(h, e, "flow links");
     if ((e = cudaMalloc(&h->d_tracer, sizeof(Tracer))) != cudaSuccess) return cuda_check(h, e, "tracer");
-    h->n_flow_list = (int64_t)list.size();
-    if (!list.empty())
-        cudaMemcpyAsync(h->d_flow_list, list.data(), sizeof(int32_t) * list.size(), cudaMemcpyHostToDevice, h->stream);
     cudaMemsetAsync(h->d_tracer, 0, sizeof(Tracer), h->stream);
+    cudaMemsetAsync(h->d_flink, 0, es * (size_t)std::max<int64_t>(1, h->flow_sp.L), h->stream);
 
     int grid = 0;
     switch (h->flow_prec) {
-        case CLB_F64: grid = grid_for(h, k_flow_aa<double, double, false>, FLOW_THREADS); break;
-        case CLB_F32: grid = grid_for(h, k_flow_aa<float, float, false>, FLOW_THREADS); break;
-        default: grid = grid_for(h, k_flow_aa<__half, float, false>, FLOW_THREADS); break;
+        case CLB_F64: grid = grid_for(h, k_flow_aa<double, double, true>, FLOW_THREADS); break;
+        case CLB_F32: grid = grid_for(h, k_flow_aa<float, float, true>, FLOW_THREADS); break;
+        default: grid = grid_for(h, k_flow_aa<__half, float, true>, FLOW_THREADS); break;
     }
     h->flow_grid = grid;
     if ((e = cudaMalloc(&h->d_partials, sizeof(double) * grid)) != cudaSuccess) return cuda_check(h, e, "partials");
     h->partial_cap = grid;
 
     const int ig = h->num_sms * 8;
+    const SparseView S = view_of(h->flow_sp);
     switch (h->flow_prec) {
-        case CLB_F64: k_flow_init<double><<<ig, 256, 0, h->stream>>>((double*)h->d_f, h->d_mat, P, delta_p); break;
-        case CLB_F32: k_flow_init<float><<<ig, 256, 0, h->stream>>>((float*)h->d_f, h->d_mat, P, delta_p); break;
-        default: k_flow_init<__half><<<ig, 256, 0, h->stream>>>((__half*)h->d_f, h->d_mat, P, delta_p); break;
+        case CLB_F64: k_flow_init<double><<<ig, 256, 0, h->stream>>>((double*)h->d_f, S, P, delta_p); break;
+        case CLB_F32: k_flow_init<float><<<ig, 256, 0, h->stream>>>((float*)h->d_f, S, P, delta_p); break;
+        default: k_flow_init<__half><<<ig, 256, 0, h->stream>>>((__half*)h->d_f, S, P, delta_p); break;
     }
     h->flow_iters = 0;
     h->flow_ready = true;
@@ -440,14 +460,17 @@ clb_status flow_init(clb_handle* h, double delta_p) {
 
 static void launch_flow(clb_handle* h, bool odd, int trace) {
     const FlowParams& P = h->fp;
+    const SparseView S = view_of(h->flow_sp);
     const int grid = h->flow_grid;
-#define CLB_LAUNCH(TS, TC)                                                                                        \
-    if (odd)                                                                                                      \
-        k_flow_aa<TS, TC, true><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, h->d_flow_list, h->n_flow_list, \
-                                                                       h->d_mat, P, h->d_tracer, h->d_partials, trace); \
-    else                                                                                                          \
-        k_flow_aa<TS, TC, false><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, h->d_flow_list, h->n_flow_list, \
-                                                                        h->d_mat, P, h->d_tracer, h->d_partials, trace);
+#define CLB_LAUNCH(TS, TC)                                                                                     \
+    if (odd)                                                                                                   \
+        k_flow_aa<TS, TC, true><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, (TS*)h->d_flink, S, P,       \
+                                                                       h->d_tracer, h->d_partials, trace,      \
+                                                                       h->k_west_end, h->k_east_begin);        \
+    else                                                                                                       \
+        k_flow_aa<TS, TC, false><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, (TS*)h->d_flink, S, P,      \
+                                                                        h->d_tracer, h->d_partials, trace,     \
+                                                                        h->k_west_end, h->k_east_begin);
     switch (h->flow_prec) {
         case CLB_F64: CLB_LAUNCH(double, double); break;
         case CLB_F32: CLB_LAUNCH(float, float); break;
@@ -501,32 +524,44 @@ clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations) {
     return conv ? CLB_OK : CLB_NOT_CONVERGED;
 }
 
-clb_status flow_velocity(clb_handle* h, void* dst, int dtype_device, bool to_host) {
+// Velocity at `count` dense nodes (all nodes when nodes == nullptr) into a device buffer
+// u[3][stride] of float64 (dtype 0) or float32 (dtype 1).
+clb_status flow_velocity_at(clb_handle* h, const int32_t* nodes, int64_t count, void* u, int64_t stride, int dtype) {
     const FlowParams& P = h->fp;
+    const SparseView S = view_of(h->flow_sp);
     const int odd = (int)(h->flow_iters & 1);
-    void* out = dst;
-    const size_t es = dtype_device == 0 ? 8 : 4;
-    if (to_host) {
-        cudaError_t e = cudaMalloc(&out, es * 3 * (size_t)h->g.N);
-        if (e != cudaSuccess) return cuda_check(h, e, "velocity buffer");
-    }
     const int grid = h->num_sms * 8;
-#define CLB_VEL(TS, TC)                                                                                           \
-    if (dtype_device == 0) k_flow_velocity<TS, TC, double><<<grid, 256, 0, h->stream>>>((const TS*)h->d_f, h->d_mat, P, odd, (double*)out); \
-    else k_flow_velocity<TS, TC, float><<<grid, 256, 0, h->stream>>>((const TS*)h->d_f, h->d_mat, P, odd, (float*)out);
+#define CLB_VEL(TS, TC)                                                                                         \
+    if (dtype == 0)                                                                                             \
+        k_flow_velocity<TS, TC, double><<<grid, 256, 0, h->stream>>>((const TS*)h->d_f, (const TS*)h->d_flink, S, \
+                                                                     h->d_mat, P, odd, nodes, count, (double*)u, stride); \
+    else                                                                                                        \
+        k_flow_velocity<TS, TC, float><<<grid, 256, 0, h->stream>>>((const TS*)h->d_f, (const TS*)h->d_flink, S,  \
+                                                                    h->d_mat, P, odd, nodes, count, (float*)u, stride);
     switch (h->flow_prec) {
         case CLB_F64: CLB_VEL(double, double); break;
         case CLB_F32: CLB_VEL(float, float); break;
         default: CLB_VEL(__half, float); break;
     }
 #undef CLB_VEL
+    return cuda_check(h, cudaGetLastError(), "flow velocity");
+}
+
+clb_status flow_velocity(clb_handle* h, void* dst, int dtype_device, bool to_host) {
+    void* out = dst;
+    const size_t es = dtype_device == 0 ? 8 : 4;
+    if (to_host) {
+        cudaError_t e = cudaMalloc(&out, es * 3 * (size_t)h->g.N);
+        if (e != cudaSuccess) return cuda_check(h, e, "velocity buffer");
+    }
+    clb_status s = flow_velocity_at(h, nullptr, h->g.N, out, h->g.N, dtype_device);
     if (to_host) {
         cudaError_t e = cudaMemcpyAsync(dst, out, es * 3 * (size_t)h->g.N, cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         cudaFree(out);
         if (e != cudaSuccess) return cuda_check(h, e, "velocity copy");
     }
-    return cuda_check(h, cudaGetLastError(), "flow velocity");
+    return s;
 }
 
 clb_status flow_populations(clb_handle* h, double* host) {
@@ -535,10 +570,11 @@ clb_status flow_populations(clb_handle* h, double* host) {
     if (e != cudaSuccess) return cuda_check(h, e, "population buffer");
     const int odd = (int)(h->flow_iters & 1);
     const int grid = h->num_sms * 8;
+    const SparseView S = view_of(h->flow_sp);
     switch (h->flow_prec) {
-        case CLB_F64: k_flow_get_pops<double><<<grid, 256, 0, h->stream>>>((const double*)h->d_f, h->fp, odd, buf); break;
-        case CLB_F32: k_flow_get_pops<float><<<grid, 256, 0, h->stream>>>((const float*)h->d_f, h->fp, odd, buf); break;
-        default: k_flow_get_pops<__half><<<grid, 256, 0, h->stream>>>((const __half*)h->d_f, h->fp, odd, buf); break;
+        case CLB_F64: k_flow_get_pops<double><<<grid, 256, 0, h->stream>>>((const double*)h->d_f, (const double*)h->d_flink, S, h->g, odd, buf); break;
+        case CLB_F32: k_flow_get_pops<float><<<grid, 256, 0, h->stream>>>((const float*)h->d_f, (const float*)h->d_flink, S, h->g, odd, buf); break;
+        default: k_flow_get_pops<__half><<<grid, 256, 0, h->stream>>>((const __half*)h->d_f, (const __half*)h->d_flink, S, h->g, odd, buf); break;
     }
     e = cudaMemcpyAsync(host, buf, sizeof(double) * 19 * (size_t)h->g.N, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -554,10 +590,11 @@ clb_status flow_set_populations(clb_handle* h, const double* host) {
     if (e != cudaSuccess) { cudaFree(buf); return cuda_check(h, e, "population copy"); }
     const int odd = (int)(h->flow_iters & 1);
     const int grid = h->num_sms * 8;
+    const SparseView S = view_of(h->flow_sp);
     switch (h->flow_prec) {
-        case CLB_F64: k_flow_set_pops<double><<<grid, 256, 0, h->stream>>>((double*)h->d_f, h->fp, odd, buf); break;
-        case CLB_F32: k_flow_set_pops<float><<<grid, 256, 0, h->stream>>>((float*)h->d_f, h->fp, odd, buf); break;
-        default: k_flow_set_pops<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_f, h->fp, odd, buf); break;
+        case CLB_F64: k_flow_set_pops<double><<<grid, 256, 0, h->stream>>>((double*)h->d_f, (double*)h->d_flink, S, h->g, odd, buf); break;
+        case CLB_F32: k_flow_set_pops<float><<<grid, 256, 0, h->stream>>>((float*)h->d_f, (float*)h->d_flink, S, h->g, odd, buf); break;
+        default: k_flow_set_pops<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_f, (__half*)h->d_flink, S, h->g, odd, buf); break;
     }
     e = cudaStreamSynchronize(h->stream);
     cudaFree(buf);
@@ -600,7 +637,7 @@ clb_status flow_stats(clb_handle* h, double char_length, clb_flow_stats* out) {
     out->energy = t.energy;
     out->iterations = t.iterations;
     out->bgk_nodes = h->fp.n_bgk;
-    out->active_nodes = h->n_flow_list;
+    out->active_nodes = h->flow_sp.K;
     return CLB_OK;
 }
 

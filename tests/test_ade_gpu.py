@@ -36,9 +36,9 @@ SPECIES = [
 ]
 
 
+@pytest.mark.parametrize("shape", [(20, 10, 9), (12, 8, 41)])
 @pytest.mark.parametrize("steps", [1, 2, 25, 120])
-def test_f64_multispecies_decay_matches_oracle(clb, oracle, steps):
-    shape = (20, 10, 9)
+def test_f64_multispecies_decay_matches_oracle(clb, oracle, shape, steps):
     mat = mixed_geometry(*shape)
     u = flow_field(oracle, mat, shape)
     D, O = pair(clb, oracle, mat, shape, SPECIES, clb.F64, u, law=1, params=[1e-3, 2e-2, 5e-3])
