@@ -26,37 +26,59 @@ namespace clb {
 
 constexpr int ADE_THREADS = 256;
 
-// Rate laws (clb_law). C, B are the floored concentrations / biomasses.
-__device__ __forceinline__ void eval_rates(const AdeParams& P, const double* C, const double* B, double* R,
+// Rate laws (clb_law), over the species in internal order (mobile first). C and B are the
+// floored concentrations / biomasses; loops are unrolled to the species bucket NB so every array
+// stays in registers.
+template <int NB>
+__device__ __forceinline__ void eval_rates(const AdeParams& P, const double (&C)[NB], const double* B, double (&R)[NB],
                                            double* RB) {
-    for (int s = 0; s < P.S; ++s) R[s] = 0.0;
-    for (int m = 0; m < P.M; ++m) RB[m] = 0.0;
+#pragma unroll
+    for (int s = 0; s < NB; ++s) R[s] = 0.0;
     switch (P.law) {
         case CLB_LAW_DECAY:
-            for (int s = 0; s < P.S; ++s) R[s] = -P.prm[s] * C[s];
+#pragma unroll
+            for (int s = 0; s < NB; ++s)
+                if (s < P.S) R[s] = -P.prm[s] * C[s];
             break;
         case CLB_LAW_MONOD:
-            for (int s = 0; s < P.S; ++s) R[s] = -P.prm[s] * C[s] / (P.prm[P.S + s] + C[s]);
+#pragma unroll
+            for (int s = 0; s < NB; ++s)
+                if (s < P.S) R[s] = -P.prm[s] * C[s] / (P.prm[CLB_MAX_SPECIES + s] + C[s]);
             break;
         case CLB_LAW_DUAL_MONOD: {
             const double mu = P.prm[0], ks = P.prm[1], Y = P.prm[2], kd = P.prm[3];
+            const int don = P.donor;
+            double Cd = 0.0;
+#pragma unroll
+            for (int s = 0; s < NB; ++s)
+                if (s == don) Cd = C[s];
+            double Rd = 0.0;
             for (int m = 0; m < P.M; ++m) {
-                const int a = 1 + m;
-                if (a >= P.S) break;
+                const int a = P.acceptor[m];
+                RB[m] = 0.0;
+                if (a < 0) continue;
+                double Ca = 0.0;
+#pragma unroll
+                for (int s = 0; s < NB; ++s)
+                    if (s == a) Ca = C[s];
                 const double Bm = B[m];
                 if (Bm <= 0.0) continue;
-                const double growth = mu * (C[0] / (ks + C[0])) * (C[a] / (ks + C[a])) * Bm;
+                const double growth = mu * (Cd / (ks + Cd)) * (Ca / (ks + Ca)) * Bm;
                 RB[m] += growth - kd * Bm;
-                R[0] -= growth / Y;
-                R[a] -= growth / Y;
+                Rd -= growth / Y;
+#pragma unroll
+                for (int s = 0; s < NB; ++s)
+                    if (s == a) R[s] -= growth / Y;
             }
+#pragma unroll
+            for (int s = 0; s < NB; ++s)
+                if (s == don) R[s] += Rd;
             break;
         }
         default:
             break;
     }
 }
-
 
 template <typename TS, typename TC, bool ODD, int NM>
 __global__ void __launch_bounds__(ADE_THREADS)
@@ -65,30 +87,36 @@ __global__ void __launch_bounds__(ADE_THREADS)
              int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin) {
     const Geom G = P.g;
     const int64_t K = S.K, L = S.L;
+    const uint32_t K32 = (uint32_t)K;  // 7 K < 2^31 is checked when the layout is built
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
         const int code = S.code[k];
         const int dyn = P.dyn[code];
         const bool west = k < k_west_end, east = k >= k_east_begin;
-        int x = 0, y = 0, z = 0, p = 0;
-        uint32_t wm = 0;
+        int p = 0;
+        uint32_t wm = 0, blk = 0;
         int lb = 0;
-        int64_t nb[7];  // compact index of the source node a - c_i (odd step)
-        if (ODD || west || east) {
+        int nb[7];  // compact index of the source node a - c_i (odd step)
+        if (west || east) {
             const int64_t n = S.node[k];
-            decode(G, n, x, y, z);
-            p = (int)(n - (int64_t)x * G.plane);
+            p = (int)(n % G.plane);
+        }
+        {
+            const uint32_t mt = S.meta[k];
+            wm = mt & 0x7Fu;
+            blk = wm | ((mt >> 7) & 0x7Fu);  // wall or outside the box
+            lb = S.tlb[(int)(k >> 8)] + (int)(mt >> 14);
         }
         if (ODD) {
-            wm = S.wall[k];
-            lb = S.linkbase[k];
-            const int r = x * G.ny + y;
-            nb[0] = k;
-            nb[1] = (x + 1 < G.nx) ? row_rank(S, r + G.ny, z) : -1;  // -x population comes from x+1
-            nb[4] = (x >= 1) ? row_rank(S, r - G.ny, z) : -1;
-            nb[2] = (y + 1 < G.ny) ? row_rank(S, r + 1, z) : -1;
-            nb[5] = (y >= 1) ? row_rank(S, r - 1, z) : -1;
-            nb[3] = k + 1;
-            nb[6] = k - 1;
+            const int t = (int)(k >> 8);
+            const int2 dv = *reinterpret_cast<const int2*>(S.dres + 4 * k);
+            const int* tb = S.tdb + 4 * t;
+            nb[0] = (int)k;
+            nb[1] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);           // -x population comes from x+1
+            nb[4] = (int)k + tb[1] + (int16_t)((uint32_t)dv.x >> 16);    // +x from x-1
+            nb[2] = (int)k + tb[2] + (int16_t)(dv.y & 0xFFFF);           // -y from y+1
+            nb[5] = (int)k + tb[3] + (int16_t)((uint32_t)dv.y >> 16);    // +y from y-1
+            nb[3] = (int)k + 1;
+            nb[6] = (int)k - 1;
         }
         TC pop[NM][7];
         TC rb[NM];
@@ -101,18 +129,25 @@ __global__ void __launch_bounds__(ADE_THREADS)
             const int s = mob_species[m];
             if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
             act[m] = true;
-            const TS* f = g + (int64_t)m * 7 * K;
+            TS* f = g + (int64_t)m * 7 * K;
             const TS* lk = glink + (int64_t)m * L;
 #pragma unroll
             for (int i = 0; i < 7; ++i) {
-                if (!ODD || i == 0) { pop[m][i] = ld<TS, TC>(f + (int64_t)i * K + k); continue; }
-                const int cx = q7cx(i), cy = q7cy(i), cz = q7cz(i), oi = q7opp(i);
-                const bool in = (cx == 0 || (unsigned)(x - cx) < (unsigned)G.nx) &&
-                                (cy == 0 || (unsigned)(y - cy) < (unsigned)G.ny) &&
-                                (cz == 0 || (unsigned)(z - cz) < (unsigned)G.nz);
-                if (!in) pop[m][i] = ld<TS, TC>(f + (int64_t)i * K + k);
-                else if ((wm >> oi) & 1u) pop[m][i] = ld<TS, TC>(lk + lb + __popc(wm & ((1u << oi) - 1u)));
-                else pop[m][i] = ld<TS, TC>(f + (int64_t)oi * K + nb[i]);
+                if (!ODD || i == 0) { pop[m][i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
+                const int oi = q7opp(i);
+                if ((blk >> oi) & 1u) pop[m][i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k);
+                else pop[m][i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)nb[i]);
+            }
+            if (!ODD && wm) {
+                // wall link (a, i): incoming opp(i) from the even-step slot X; the odd-step slot
+                // Y = f[opp(i)][a] is written back unchanged so its sector is written whole
+#pragma unroll
+                for (int i = 1; i < 7; ++i) {
+                    if (!((wm >> i) & 1u)) continue;
+                    const int oi = q7opp(i);
+                    st<TS, TC>(f + (uint32_t)(oi * K32) + k, pop[m][oi]);
+                    pop[m][oi] = ld<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)));
+                }
             }
             if ((west || east) && dyn != ADE_NONE) {
                 // AdvectionDiffusionBoundaryDynamics: the one inward population makes the
@@ -134,34 +169,31 @@ __global__ void __launch_bounds__(ADE_THREADS)
             rb[m] = r;
         }
         // ---- kinetics (x = 1..nx-2, mask neither solid nor wall)
-        double dC[CLB_MAX_SPECIES];
-        for (int s = 0; s < P.S; ++s) dC[s] = 0.0;
-        if (P.law != CLB_LAW_NONE && !west && !east && P.react[code]) {
-            double C[CLB_MAX_SPECIES], R[CLB_MAX_SPECIES], B[CLB_MAX_MICROBES], RB[CLB_MAX_MICROBES];
-            for (int s = 0; s < P.S; ++s) {
-                double c;
-                const int m = P.slot[s];
-                if (m >= 0) {
-                    c = 0.0;
+        double dC[NM];
 #pragma unroll
-                    for (int mm = 0; mm < NM; ++mm)
-                        if (mm == m) c = (double)rb[mm] + 1.0;
-                } else {
-                    c = imm[(int64_t)s * K + k];
-                }
+        for (int s = 0; s < NM; ++s) dC[s] = 0.0;
+        if (P.law != CLB_LAW_NONE && !west && !east && P.react[code]) {
+            double C[NM], R[NM], B[CLB_MAX_MICROBES], RB[CLB_MAX_MICROBES];
+#pragma unroll
+            for (int s = 0; s < NM; ++s) {
+                double c = 0.0;
+                if (s < n_mobile) c = (double)rb[s] + 1.0;
+                else if (s < P.S) c = imm[(int64_t)s * K + k];
                 C[s] = c < THRD ? 0.0 : c;
             }
             for (int mb = 0; mb < P.M; ++mb) {
                 const double b = bio[(int64_t)mb * K + k];
                 B[mb] = b < THRD ? 0.0 : b;
             }
-            eval_rates(P, C, B, R, RB);
-            for (int s = 0; s < P.S; ++s) {
+            eval_rates<NM>(P, C, B, R, RB);
+#pragma unroll
+            for (int s = 0; s < NM; ++s) {
+                if (s >= P.S) continue;
                 double d = R[s] * P.dt;
                 if (!(d > THRD || d < -THRD)) continue;
                 if (d + C[s] < 0.0) d = -C[s];
                 if (!(d > THRD || d < -THRD)) continue;
-                if (P.slot[s] >= 0) dC[s] = d;
+                if (s < n_mobile) dC[s] = d;
                 else imm[(int64_t)s * K + k] += d;
             }
             for (int mb = 0; mb < P.M; ++mb) {
@@ -186,7 +218,7 @@ __global__ void __launch_bounds__(ADE_THREADS)
                 const TC omw = (TC)1 - w;
                 const TC rho = rb[m] + (TC)1;
                 const TC jx = rho * ux, jy = rho * uy, jz = rho * uz;
-                const TC d = (TC)dC[s];
+                const TC d = (TC)dC[m];
 #pragma unroll
                 for (int i = 0; i < 7; ++i) {
                     const TC cj = (TC)q7cx(i) * jx + (TC)q7cy(i) * jy + (TC)q7cz(i) * jz;
@@ -198,14 +230,15 @@ __global__ void __launch_bounds__(ADE_THREADS)
             TS* lk = glink + (int64_t)m * L;
 #pragma unroll
             for (int i = 0; i < 7; ++i) {
-                if (!ODD || i == 0) { st<TS, TC>(f + (int64_t)q7opp(i) * K + k, o[i]); continue; }
-                const int cx = q7cx(i), cy = q7cy(i), cz = q7cz(i), oi = q7opp(i);
-                const bool in = (cx == 0 || (unsigned)(x + cx) < (unsigned)G.nx) &&
-                                (cy == 0 || (unsigned)(y + cy) < (unsigned)G.ny) &&
-                                (cz == 0 || (unsigned)(z + cz) < (unsigned)G.nz);
-                if (!in) st<TS, TC>(f + (int64_t)oi * K + k, o[i]);
-                else if ((wm >> i) & 1u) st<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)), o[i]);
-                else st<TS, TC>(f + (int64_t)i * K + nb[oi], o[i]);  // destination a + c_i = source of opp(i)
+                if (!ODD) {
+                    if ((wm >> i) & 1u) st<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)), o[i]);
+                    else st<TS, TC>(f + (uint32_t)(q7opp(i) * K32) + k, o[i]);
+                    continue;
+                }
+                if (i == 0) { st<TS, TC>(f + k, o[0]); continue; }
+                const int oi = q7opp(i);
+                if ((blk >> i) & 1u) st<TS, TC>(f + (uint32_t)(oi * K32) + k, o[i]);
+                else st<TS, TC>(f + (uint32_t)(i * K32) + (uint32_t)nb[oi], o[i]);  // a + c_i = source of opp(i)
             }
         }
     }
@@ -403,20 +436,29 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
         P.react[d.solid_code] = 0;
     }
     h->species.assign(sp, sp + S);
+    // internal order: mobile species first (user order), then immobile ones
+    std::vector<int> order;
+    for (int s = 0; s < S; ++s) if (sp[s].mobile) order.push_back(s);
+    for (int s = 0; s < S; ++s) if (!sp[s].mobile) order.push_back(s);
     std::vector<int> mob;
     std::vector<double> c0m;
-    for (int s = 0; s < S; ++s) {
-        P.mobile[s] = sp[s].mobile ? 1 : 0;
-        P.slot[s] = -1;
-        if (sp[s].mobile) { P.slot[s] = (int)mob.size(); mob.push_back(s); c0m.push_back(sp[s].c0); }
-        P.ltype[s] = sp[s].left_type;
-        P.rtype[s] = sp[s].right_type;
-        P.lbc[s] = sp[s].left_bc;
-        P.rbc[s] = sp[s].right_bc;
-        P.wpore[s] = sp[s].omega_pore;
-        P.wbio[s] = sp[s].omega_biofilm;
-        P.c0[s] = sp[s].c0;
+    for (int i = 0; i < S; ++i) {
+        const clb_species_desc& d_ = sp[order[i]];
+        h->i2u[i] = order[i];
+        h->u2i[order[i]] = i;
+        P.mobile[i] = d_.mobile ? 1 : 0;
+        P.slot[i] = -1;
+        if (d_.mobile) { P.slot[i] = (int)mob.size(); mob.push_back(i); c0m.push_back(d_.c0); }
+        P.ltype[i] = d_.left_type;
+        P.rtype[i] = d_.right_type;
+        P.lbc[i] = d_.left_bc;
+        P.rbc[i] = d_.right_bc;
+        P.wpore[i] = d_.omega_pore;
+        P.wbio[i] = d_.omega_biofilm;
+        P.c0[i] = d_.c0;
     }
+    P.donor = 0;
+    for (int m = 0; m < CLB_MAX_MICROBES; ++m) P.acceptor[m] = -1;
     h->S = S;
     h->n_mobile = (int)mob.size();
     if (h->n_mobile > 16) return fail(h, CLB_INVALID_ARG, "at most 16 mobile species");
@@ -447,20 +489,20 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
     cudaMemsetAsync(h->d_u, 0, usize(h->ade_prec) * 3 * K1, h->stream);
     // immobile species: uniform c0 (initial_concentration applies to the whole domain)
     std::vector<double> immh(K1);
-    for (int s = 0; s < S; ++s) {
-        if (sp[s].mobile) continue;
-        std::fill(immh.begin(), immh.end(), sp[s].c0);
-        cudaMemcpy(h->d_imm + (size_t)s * K1, immh.data(), sizeof(double) * K1, cudaMemcpyHostToDevice);
+    for (int i = 0; i < S; ++i) {
+        if (P.mobile[i]) continue;
+        std::fill(immh.begin(), immh.end(), P.c0[i]);
+        cudaMemcpy(h->d_imm + (size_t)i * K1, immh.data(), sizeof(double) * K1, cudaMemcpyHostToDevice);
     }
     // stored boundary densities: Dirichlet value, else c0 (lattice.initialize() runs the
     // Neumann processor once on the equilibrium field)
     std::vector<double> neu((size_t)S * 2 * h->g.plane);
-    for (int s = 0; s < S; ++s)
+    for (int i = 0; i < S; ++i)
         for (int side = 0; side < 2; ++side) {
-            int t = side == 0 ? sp[s].left_type : sp[s].right_type;
-            double v = t == CLB_DIRICHLET ? (side == 0 ? sp[s].left_bc : sp[s].right_bc) : sp[s].c0;
-            std::fill(neu.begin() + ((size_t)s * 2 + side) * h->g.plane,
-                      neu.begin() + ((size_t)s * 2 + side + 1) * h->g.plane, v);
+            int t = side == 0 ? P.ltype[i] : P.rtype[i];
+            double v = t == CLB_DIRICHLET ? (side == 0 ? P.lbc[i] : P.rbc[i]) : P.c0[i];
+            std::fill(neu.begin() + ((size_t)i * 2 + side) * h->g.plane,
+                      neu.begin() + ((size_t)i * 2 + side + 1) * h->g.plane, v);
         }
     cudaMemcpy(h->d_neu, neu.data(), sizeof(double) * neu.size(), cudaMemcpyHostToDevice);
     int mt[16] = {0};
@@ -490,9 +532,30 @@ clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm,
     if (nprm < 0 || nprm > 4 * CLB_MAX_SPECIES) return fail(h, CLB_INVALID_ARG, "too many kinetics parameters");
     if (law < 0 || law > CLB_LAW_DUAL_MONOD) return fail(h, CLB_INVALID_ARG, "unknown rate law");
     AdeParams& P = h->ap;
+    const int S = h->S;
     P.law = law;
     std::memset(P.prm, 0, sizeof(P.prm));
-    for (int k = 0; k < nprm; ++k) P.prm[k] = prm[k];
+    switch (law) {
+        case CLB_LAW_DECAY:
+            if (nprm < S) return fail(h, CLB_INVALID_ARG, "decay needs one rate per species");
+            for (int i = 0; i < S; ++i) P.prm[i] = prm[h->i2u[i]];
+            break;
+        case CLB_LAW_MONOD:
+            if (nprm < 2 * S) return fail(h, CLB_INVALID_ARG, "Monod needs k[S] then Ks[S]");
+            for (int i = 0; i < S; ++i) {
+                P.prm[i] = prm[h->i2u[i]];
+                P.prm[CLB_MAX_SPECIES + i] = prm[S + h->i2u[i]];
+            }
+            break;
+        case CLB_LAW_DUAL_MONOD:
+            if (nprm < 4) return fail(h, CLB_INVALID_ARG, "dual Monod needs mu_max, Ks, Y, kd");
+            for (int k = 0; k < 4; ++k) P.prm[k] = prm[k];
+            P.donor = h->u2i[0];
+            for (int m = 0; m < CLB_MAX_MICROBES; ++m) P.acceptor[m] = (1 + m < S) ? h->u2i[1 + m] : -1;
+            break;
+        default:
+            break;
+    }
     P.dt = dt;
     return CLB_OK;
 }
@@ -543,6 +606,7 @@ template <typename TS, typename TC, bool ODD>
 static void launch_ade_t(clb_handle* h) {
     const int grid = h->ade_grid;
     const int nm = h->n_mobile;
+    const int nb = h->S;  // register bucket covers every species (mobile first, then immobile)
     TS* g = (TS*)h->d_g;
     TS* gl = (TS*)h->d_glink;
     const TC* u = (const TC*)h->d_u;
@@ -552,10 +616,10 @@ static void launch_ade_t(clb_handle* h) {
     k_ade_aa<TS, TC, ODD, NM><<<grid, ADE_THREADS, 0, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, \
                                                                   h->ap, nm, mt, h->ade_west_end,            \
                                                                   h->ade_east_begin)
-    if (nm <= 1) CLB_ADE(1);
-    else if (nm <= 2) CLB_ADE(2);
-    else if (nm <= 4) CLB_ADE(4);
-    else if (nm <= 8) CLB_ADE(8);
+    if (nb <= 1) CLB_ADE(1);
+    else if (nb <= 2) CLB_ADE(2);
+    else if (nb <= 4) CLB_ADE(4);
+    else if (nb <= 8) CLB_ADE(8);
     else CLB_ADE(16);
 #undef CLB_ADE
 }
@@ -607,9 +671,8 @@ clb_status ade_couple(clb_handle* h) {
     return flow_velocity_at(h, h->ade_sp.node, h->ade_sp.K, h->d_u, h->ade_sp.K, h->ade_prec == CLB_F64 ? 0 : 1);
 }
 
-clb_status ade_populations(clb_handle* h, int s, double* host) {
-    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
-    if (s < 0 || s >= h->S || h->ap.slot[s] < 0) return fail(h, CLB_INVALID_ARG, "not a mobile species");
+static clb_status ade_populations_i(clb_handle* h, int s, double* host) {
+    if (h->ap.slot[s] < 0) return fail(h, CLB_INVALID_ARG, "not a mobile species");
     const int m = h->ap.slot[s];
     double* buf = nullptr;
     cudaError_t e = cudaMalloc(&buf, sizeof(double) * 7 * (size_t)h->g.N);
@@ -630,9 +693,17 @@ clb_status ade_populations(clb_handle* h, int s, double* host) {
     return cuda_check(h, e, "population copy");
 }
 
+clb_status ade_populations(clb_handle* h, int s, double* host) {
+    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+    if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
+    return ade_populations_i(h, h->u2i[s], host);
+}
+
 clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
-    if (s < 0 || s >= h->S || h->ap.slot[s] < 0) return fail(h, CLB_INVALID_ARG, "not a mobile species");
+    if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
+    s = h->u2i[s];
+    if (h->ap.slot[s] < 0) return fail(h, CLB_INVALID_ARG, "not a mobile species");
     const int m = h->ap.slot[s];
     double* buf = nullptr;
     cudaError_t e = cudaMalloc(&buf, sizeof(double) * 7 * (size_t)h->g.N);
@@ -657,12 +728,13 @@ clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
 clb_status ade_density(clb_handle* h, int s, double* host) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
+    s = h->u2i[s];
     const size_t N = (size_t)h->g.N;
     if (h->ap.slot[s] < 0) return to_dense(h, h->d_imm + (size_t)s * std::max<int64_t>(1, h->ade_sp.K), h->ap.c0[s], host);
     // the Neumann planes' stored values as the reference holds them after the last stream
     refresh_neumann(h);
     std::vector<double> pops(7 * N);
-    clb_status st = ade_populations(h, s, pops.data());
+    clb_status st = ade_populations_i(h, s, pops.data());
     if (st != CLB_OK) return st;
     std::vector<double> neu((size_t)2 * h->g.plane);
     cudaMemcpy(neu.data(), h->d_neu + (size_t)s * 2 * h->g.plane, sizeof(double) * neu.size(), cudaMemcpyDeviceToHost);
@@ -765,11 +837,12 @@ clb_status ade_reduce(clb_handle* h, clb_stats* out) {
     for (int s = 0; s < S; ++s) { out->min_c[s] = 1e300; out->max_c[s] = -1e300; }
     for (int b = 0; b < grid; ++b) {
         const double* q = &hp[(size_t)b * nq];
-        for (int s = 0; s < S; ++s) {
-            out->total[s] += q[s];
-            out->content[s] += q[S + s];
-            out->min_c[s] = std::min(out->min_c[s], q[2 * S + s]);
-            out->max_c[s] = std::max(out->max_c[s], q[3 * S + s]);
+        for (int i = 0; i < S; ++i) {
+            const int s = h->i2u[i];
+            out->total[s] += q[i];
+            out->content[s] += q[S + i];
+            out->min_c[s] = std::min(out->min_c[s], q[2 * S + i]);
+            out->max_c[s] = std::max(out->max_c[s], q[3 * S + i]);
         }
         for (int mb = 0; mb < M; ++mb) out->biomass[mb] += q[4 * S + mb];
         out->nonfinite += (int64_t)q[4 * S + M];

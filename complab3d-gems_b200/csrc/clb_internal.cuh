@@ -116,6 +116,8 @@ struct AdeParams {
     double lbc[CLB_MAX_SPECIES], rbc[CLB_MAX_SPECIES];
     double wpore[CLB_MAX_SPECIES], wbio[CLB_MAX_SPECIES];
     double c0[CLB_MAX_SPECIES];
+    int donor;                          // internal index of the dual-Monod donor
+    int acceptor[CLB_MAX_MICROBES];     // internal index of each microbe's acceptor, -1 none
 };
 
 }  // namespace clb
@@ -131,8 +133,13 @@ struct SparseBuffers {
     uint32_t* rowmask = nullptr;
     int32_t* rowpre = nullptr;
     int32_t* idx_of = nullptr;
+    // odd-step metadata (see sparse.cuh)
+    uint32_t* meta = nullptr;   // [K][MW] packed wall / edge / row bits / link residual
+    int16_t* dres = nullptr;    // [K][NR] neighbour-row rank residuals
+    int32_t* tlb = nullptr;     // [T] link base of each 256-node tile
+    int32_t* tdb = nullptr;     // [T][NR] neighbour-row rank bases of each tile
     int64_t K = 0, L = 0;
-    int W = 0;
+    int W = 0, NR = 0;
 };
 }  // namespace clb
 
@@ -167,7 +174,9 @@ struct clb_handle_s {
     bool ade_ready = false;
     int ade_prec = CLB_F32;
     int S = 0, n_mobile = 0, M = 0;
-    std::vector<clb_species_desc> species;
+    std::vector<clb_species_desc> species;  // user order
+    int u2i[CLB_MAX_SPECIES];               // user species index -> internal (mobile first)
+    int i2u[CLB_MAX_SPECIES];
     void* d_g = nullptr;              // [n_mobile][7][K] storage type, compacted stored nodes
     void* d_glink = nullptr;          // [n_mobile][L] wall link slots
     clb::SparseBuffers ade_sp;

@@ -16,14 +16,16 @@
 //              i to f[i][a + c_i].
 // Each slot is read and written by exactly one node per step, so a step needs no second array
 // and no synchronisation. A full-way bounce-back node is the identity on its AA slots, so it is
-// never launched; the slot f[i][b] of a wall node b that its fluid neighbour a = b - c_i writes
-// on an odd step (and reads back two steps later) is a's link slot for direction i. A source or
-// destination outside the box maps to the node's own opposite slot: Palabos' reflection at the
-// block edge. The even step touches only the node's own slots (perfectly coalesced); the odd
-// step finds neighbours through the row bitmasks.
+// never launched; each link from a stored node into a wall is a two-step delay line held in the
+// node's own opposite slot on odd steps and in a link slot on even steps (sparse.cuh). A source
+// or destination outside the box maps to the node's own opposite slot: Palabos' reflection at the
+// block edge. The even step touches only the node's own slots and its link slots; the odd step
+// gathers and scatters through the precomputed neighbour-row offsets and writes every stored slot
+// exactly once.
 //
 // Algorithmic bytes per node update: 2 * 19 * sizeof(storage). Metadata read per node: 1 byte
-// material code (both steps), 12 bytes dense index + wall mask + link base (odd step only).
+// material code and 4 bytes wall mask + link offset (even step); 1 byte code, 8 bytes masks and
+// 16 bytes neighbour-row offsets (odd step).
 #include "sparse.cuh"
 
 #include <algorithm>
@@ -146,8 +148,6 @@ __device__ void finish_step(Tracer* tr, double* partials, double block_total, in
 }
 
 
-// slot of row (dx, dy) among the 3x3 neighbourhood of a row
-__host__ __device__ constexpr int rslot(int dx, int dy) { return (dx + 1) * 3 + (dy + 1); }
 
 template <typename TS, typename TC, bool ODD>
 __global__ void __launch_bounds__(FLOW_THREADS, 3)
@@ -155,52 +155,59 @@ __global__ void __launch_bounds__(FLOW_THREADS, 3)
               Tracer* __restrict__ tr, double* __restrict__ partials, int trace, int64_t k_west_end,
               int64_t k_east_begin) {
     if (trace && tr->converged) return;  // a batch continues past convergence as no-ops
-    const Geom G = P.g;
     const int64_t K = S.K;
+    const uint32_t K32 = (uint32_t)K;  // 19 K < 2^31 is checked when the layout is built
     double esum = 0;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
         const int code = S.code[k];
         TC g[19];
-        int x = 0, y = 0, z = 0, rb_[9];
-        uint32_t wm = 0, rbit = 0;
+        int rb_[8];
+        uint32_t blk = 0, rbit = 0, wm = 0;
         int lb = 0;
         if (!ODD) {
+            // own slots; a wall link (a, i) takes its incoming opp(i) from its even-step slot X
+            // and its odd-step slot Y = f[opp(i)][a] is written back unchanged (whole sectors)
+            const uint32_t m0 = S.meta[2 * k];
+            wm = m0 & 0x7FFFFu;
+            lb = S.tlb[(int)(k >> 8)] + (int)(m0 >> 19);
 #pragma unroll
-            for (int i = 0; i < 19; ++i) g[i] = ld<TS, TC>(f + (int64_t)i * K + k);
-        } else {
-            decode(G, S.node[k], x, y, z);
-            wm = S.wall[k];
-            lb = S.linkbase[k];
-            const int r = x * G.ny + y;
+            for (int i = 0; i < 19; ++i) g[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k);
+            if (wm) {
 #pragma unroll
-            for (int dx = -1; dx <= 1; ++dx)
-#pragma unroll
-                for (int dy = -1; dy <= 1; ++dy) {
-                    const int s = rslot(dx, dy);
-                    rb_[s] = 0;
-                    if ((dx == 0 && dy == 0) || (unsigned)(x + dx) >= (unsigned)G.nx ||
-                        (unsigned)(y + dy) >= (unsigned)G.ny)
-                        continue;
-                    const int rr = r + dx * G.ny + dy;
-                    rb_[s] = row_rank(S, rr, z);
-                    rbit |= (uint32_t)row_bit(S, rr, z) << s;
+                for (int i = 1; i < 19; ++i) {
+                    if (!((wm >> i) & 1u)) continue;
+                    const int oi = q19opp(i);
+                    st<TS, TC>(f + (uint32_t)(oi * K32) + k, g[oi]);
+                    g[oi] = ld<TS, TC>(link + lb + __popc(wm & ((1u << i) - 1u)));
                 }
+            }
+        } else {
+            const uint32_t m0 = S.meta[2 * k], m1 = S.meta[2 * k + 1];
+            const int t = (int)(k >> 8);
+            blk = (m0 | m1) & 0x7FFFFu;  // wall or outside the box: the node's own opposite slot
+            rbit = m1 >> 19;
+            const int4 dv = *reinterpret_cast<const int4*>(S.dres + 8 * k);
+            const int* tb = S.tdb + 8 * t;
+            rb_[0] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);
+            rb_[1] = (int)k + tb[1] + (int16_t)((uint32_t)dv.x >> 16);
+            rb_[2] = (int)k + tb[2] + (int16_t)(dv.y & 0xFFFF);
+            rb_[3] = (int)k + tb[3] + (int16_t)((uint32_t)dv.y >> 16);
+            rb_[4] = (int)k + tb[4] + (int16_t)(dv.z & 0xFFFF);
+            rb_[5] = (int)k + tb[5] + (int16_t)((uint32_t)dv.z >> 16);
+            rb_[6] = (int)k + tb[6] + (int16_t)(dv.w & 0xFFFF);
+            rb_[7] = (int)k + tb[7] + (int16_t)((uint32_t)dv.w >> 16);
 #pragma unroll
             for (int i = 0; i < 19; ++i) {
                 if (i == 0) { g[0] = ld<TS, TC>(f + k); continue; }
                 const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
-                const bool in = (cx == 0 || (unsigned)(x - cx) < (unsigned)G.nx) &&
-                                (cy == 0 || (unsigned)(y - cy) < (unsigned)G.ny) &&
-                                (cz == 0 || (unsigned)(z - cz) < (unsigned)G.nz);
-                if (!in) { g[i] = ld<TS, TC>(f + (int64_t)i * K + k); continue; }
-                if ((wm >> oi) & 1u) { g[i] = ld<TS, TC>(link + lb + __popc(wm & ((1u << oi) - 1u))); continue; }
-                int64_t src;
-                if (cx == 0 && cy == 0) src = k - cz;
+                if ((blk >> oi) & 1u) { g[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
+                int src;
+                if (cx == 0 && cy == 0) src = (int)k - cz;
                 else {
-                    const int s = rslot(-cx, -cy);
-                    src = (cz == 0) ? rb_[s] : (-cz > 0 ? rb_[s] + ((rbit >> s) & 1u) : rb_[s] - 1);
+                    const int s8 = row8(-cx, -cy);
+                    src = (cz == 0) ? rb_[s8] : (-cz > 0 ? rb_[s8] + (int)((rbit >> s8) & 1u) : rb_[s8] - 1);
                 }
-                g[i] = ld<TS, TC>(f + (int64_t)oi * K + src);
+                g[i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)src);
             }
         }
         if (P.dyn[code] == DYN_BGK) {
@@ -223,24 +230,23 @@ __global__ void __launch_bounds__(FLOW_THREADS, 3)
         }
         if (!ODD) {
 #pragma unroll
-            for (int i = 0; i < 19; ++i) st<TS, TC>(f + (int64_t)q19opp(i) * K + k, g[i]);
+            for (int i = 0; i < 19; ++i) {
+                if ((wm >> i) & 1u) st<TS, TC>(link + lb + __popc(wm & ((1u << i) - 1u)), g[i]);
+                else st<TS, TC>(f + (uint32_t)(q19opp(i) * K32) + k, g[i]);
+            }
         } else {
 #pragma unroll
             for (int i = 0; i < 19; ++i) {
                 if (i == 0) { st<TS, TC>(f + k, g[0]); continue; }
                 const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
-                const bool in = (cx == 0 || (unsigned)(x + cx) < (unsigned)G.nx) &&
-                                (cy == 0 || (unsigned)(y + cy) < (unsigned)G.ny) &&
-                                (cz == 0 || (unsigned)(z + cz) < (unsigned)G.nz);
-                if (!in) { st<TS, TC>(f + (int64_t)oi * K + k, g[i]); continue; }
-                if ((wm >> i) & 1u) { st<TS, TC>(link + lb + __popc(wm & ((1u << i) - 1u)), g[i]); continue; }
-                int64_t dst;
-                if (cx == 0 && cy == 0) dst = k + cz;
+                if ((blk >> i) & 1u) { st<TS, TC>(f + (uint32_t)(oi * K32) + k, g[i]); continue; }
+                int dst;
+                if (cx == 0 && cy == 0) dst = (int)k + cz;
                 else {
-                    const int s = rslot(cx, cy);
-                    dst = (cz == 0) ? rb_[s] : (cz > 0 ? rb_[s] + ((rbit >> s) & 1u) : rb_[s] - 1);
+                    const int s8 = row8(cx, cy);
+                    dst = (cz == 0) ? rb_[s8] : (cz > 0 ? rb_[s8] + (int)((rbit >> s8) & 1u) : rb_[s8] - 1);
                 }
-                st<TS, TC>(f + (int64_t)i * K + dst, g[i]);
+                st<TS, TC>(f + (uint32_t)(i * K32) + (uint32_t)dst, g[i]);
             }
         }
     }
@@ -249,20 +255,31 @@ __global__ void __launch_bounds__(FLOW_THREADS, 3)
     finish_step(tr, partials, bt, P.n_bgk, trace);
 }
 
-// PressureGradient equilibrium (complab_functions.hh:82-94): BGK nodes t_i (rho(x) - 1); no-dynamics
-// nodes and the wall link slots zero (BounceBack / NoDynamics equilibria are zero).
+// PressureGradient equilibrium (complab_functions.hh:82-94): BGK nodes t_i (rho(x) - 1),
+// no-dynamics nodes zero (BounceBack / NoDynamics equilibria are zero). For a wall link (a, i)
+// the even-step slot X holds a's equilibrium incoming opp(i) and the odd-step slot
+// Y = f[opp(i)][a] the wall's initial (zero) population.
 template <typename TS>
-__global__ void k_flow_init(TS* __restrict__ f, const SparseView S, const FlowParams P, double delta_p) {
+__global__ void k_flow_init(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const FlowParams P,
+                            double delta_p) {
     const Geom G = P.g;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < S.K; k += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(S.node[k] / G.plane);
         const double rho = 1.0 - delta_p * 3.0 / (double)(G.nx - 1) * (double)x;
         const bool bgk = P.dyn[S.code[k]] == DYN_BGK;
+        const uint32_t wm = S.wall[k];
 #pragma unroll
         for (int i = 0; i < 19; ++i) {
-            double v = bgk ? q19w(i) * (rho - 1.0) : 0.0;
+            const double eq = bgk ? q19w(i) * (rho - 1.0) : 0.0;
+            const bool wall_src = i != 0 && ((wm >> q19opp(i)) & 1u);
+            const double v = wall_src ? 0.0 : eq;
             if constexpr (std::is_same<TS, __half>::value) f[(int64_t)i * S.K + k] = __double2half(v);
             else f[(int64_t)i * S.K + k] = (TS)v;
+            if (wall_src) {
+                TS* x_ = link_slot(S, link, (int)k, q19opp(i));
+                if constexpr (std::is_same<TS, __half>::value) *x_ = __double2half(eq);
+                else *x_ = (TS)eq;
+            }
         }
     }
 }
@@ -449,9 +466,9 @@ clb_status flow_init(clb_handle* h, double delta_p) {
     const int ig = h->num_sms * 8;
     const SparseView S = view_of(h->flow_sp);
     switch (h->flow_prec) {
-        case CLB_F64: k_flow_init<double><<<ig, 256, 0, h->stream>>>((double*)h->d_f, S, P, delta_p); break;
-        case CLB_F32: k_flow_init<float><<<ig, 256, 0, h->stream>>>((float*)h->d_f, S, P, delta_p); break;
-        default: k_flow_init<__half><<<ig, 256, 0, h->stream>>>((__half*)h->d_f, S, P, delta_p); break;
+        case CLB_F64: k_flow_init<double><<<ig, 256, 0, h->stream>>>((double*)h->d_f, (double*)h->d_flink, S, P, delta_p); break;
+        case CLB_F32: k_flow_init<float><<<ig, 256, 0, h->stream>>>((float*)h->d_f, (float*)h->d_flink, S, P, delta_p); break;
+        default: k_flow_init<__half><<<ig, 256, 0, h->stream>>>((__half*)h->d_f, (__half*)h->d_flink, S, P, delta_p); break;
     }
     h->flow_iters = 0;
     h->flow_ready = true;

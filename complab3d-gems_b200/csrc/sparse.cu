@@ -9,6 +9,7 @@ namespace clb {
 void sparse_free(SparseBuffers& b) {
     cudaFree(b.node); cudaFree(b.code); cudaFree(b.wall); cudaFree(b.linkbase);
     cudaFree(b.rowstart); cudaFree(b.rowmask); cudaFree(b.rowpre); cudaFree(b.idx_of);
+    cudaFree(b.meta); cudaFree(b.dres); cudaFree(b.tlb); cudaFree(b.tdb);
     b = SparseBuffers();
 }
 
@@ -72,6 +73,67 @@ clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, Spar
         L += __builtin_popcount(wm);
     }
     if (L > INT32_MAX) return fail(h, CLB_INVALID_ARG, "too many wall links");
+    if ((int64_t)K * q > INT32_MAX) return fail(h, CLB_INVALID_ARG, "lattice exceeds 2^31 populations per species");
+
+    // ---- odd-step metadata
+    const int NR = q == 19 ? 8 : 4;
+    const int64_t T = ((int64_t)K + TILE - 1) / TILE;
+    std::vector<uint32_t> meta((size_t)K * (q == 19 ? 2 : 1));
+    std::vector<int16_t> dres((size_t)K * NR);
+    std::vector<int32_t> tlb(std::max<int64_t>(1, T)), tdb((size_t)std::max<int64_t>(1, T) * NR);
+    std::vector<int64_t> dkf((size_t)TILE * NR);
+    auto rank = [&](int r, int z) -> int64_t {
+        const int w = z >> 5;
+        const uint32_t m = rowmask[(size_t)r * W + w] & ((1u << (z & 31)) - 1u);
+        return (int64_t)rowstart[r] + rowpre[(size_t)r * W + w] + __builtin_popcount(m);
+    };
+    for (int64_t t = 0; t < T; ++t) {
+        const int64_t k0 = t * TILE, k1 = std::min<int64_t>(K, k0 + TILE);
+        tlb[t] = linkbase[k0];
+        std::vector<int64_t> lo(NR, INT64_MAX), hi(NR, INT64_MIN);
+        std::fill(dkf.begin(), dkf.end(), 0);
+        for (int64_t k = k0; k < k1; ++k) {
+            const int64_t n = node[k];
+            const int x = (int)(n / G.plane), rr = (int)(n - (int64_t)x * G.plane), y = rr / nz, z = rr - y * nz;
+            uint32_t edge = 0, rbits = 0;
+            for (int i = 1; i < q; ++i) {
+                const int cx = q == 19 ? q19cx(i) : q7cx(i), cy = q == 19 ? q19cy(i) : q7cy(i),
+                          cz = q == 19 ? q19cz(i) : q7cz(i);
+                const int X = x + cx, Y = y + cy, Z = z + cz;
+                if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) edge |= 1u << i;
+            }
+            for (int dx = -1; dx <= 1; ++dx)
+                for (int dy = -1; dy <= 1; ++dy) {
+                    if (dx == 0 && dy == 0) continue;
+                    if (q == 7 && dx != 0 && dy != 0) continue;
+                    const int s_ = q == 19 ? row8(dx, dy) : row4(dx, dy);
+                    int64_t d = 0;
+                    if (x + dx >= 0 && x + dx < nx && y + dy >= 0 && y + dy < ny) {
+                        const int r2 = (x + dx) * ny + (y + dy);
+                        d = rank(r2, z) - k;
+                        if (q == 19 && ((rowmask[(size_t)r2 * W + (z >> 5)] >> (z & 31)) & 1u)) rbits |= 1u << s_;
+                    }
+                    dkf[(size_t)(k - k0) * NR + s_] = d;
+                    lo[(size_t)s_] = std::min(lo[(size_t)s_], d);
+                    hi[(size_t)s_] = std::max(hi[(size_t)s_], d);
+                }
+            const uint32_t lres = (uint32_t)(linkbase[k] - tlb[t]);
+            if (q == 19) {
+                meta[(size_t)2 * k] = (wall[k] & 0x7FFFFu) | (lres << 19);
+                meta[(size_t)2 * k + 1] = (edge & 0x7FFFFu) | (rbits << 19);
+            } else {
+                meta[(size_t)k] = (wall[k] & 0x7Fu) | ((edge & 0x7Fu) << 7) | (lres << 14);
+            }
+        }
+        for (int s_ = 0; s_ < NR; ++s_) {
+            const int64_t base = lo[(size_t)s_] == INT64_MAX ? 0 : (lo[(size_t)s_] + hi[(size_t)s_]) / 2;
+            if (lo[(size_t)s_] != INT64_MAX && (hi[(size_t)s_] - base > 32767 || base - lo[(size_t)s_] > 32767))
+                return fail(h, CLB_INVALID_ARG, "neighbour-row offsets within a 256-node tile exceed 16 bits");
+            tdb[(size_t)t * NR + s_] = (int32_t)base;
+            for (int64_t k = k0; k < k1; ++k)
+                dres[(size_t)k * NR + s_] = (int16_t)(dkf[(size_t)(k - k0) * NR + s_] - base);
+        }
+    }
     cudaError_t e = cudaSuccess;
     cudaStream_t s = h->stream;
     if (e == cudaSuccess) e = upload(out.node, node, s);
@@ -82,10 +144,15 @@ clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, Spar
     if (e == cudaSuccess) e = upload(out.rowmask, rowmask, s);
     if (e == cudaSuccess) e = upload(out.rowpre, rowpre, s);
     if (e == cudaSuccess) e = upload(out.idx_of, idx, s);
+    if (e == cudaSuccess) e = upload(out.meta, meta, s);
+    if (e == cudaSuccess) e = upload(out.dres, dres, s);
+    if (e == cudaSuccess) e = upload(out.tlb, tlb, s);
+    if (e == cudaSuccess) e = upload(out.tdb, tdb, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // host vectors die here
     out.K = K;
     out.L = L;
     out.W = W;
+    out.NR = NR;
     return cuda_check(h, e, "sparse layout");
 }
 

@@ -25,12 +25,35 @@ struct SparseView {
     const uint32_t* rowmask;  // [R*W] stored bits of row r
     const int32_t* rowpre;    // [R*W] stored nodes of row r in words < w
     const int32_t* idx_of;    // [N] compact index or -1 (non-hot kernels)
+    const uint32_t* meta;     // odd-step metadata, see below
+    const int16_t* dres;
+    const int32_t* tlb;
+    const int32_t* tdb;
     int64_t K, L;
-    int W;
+    int W, NR;
 };
 
 inline SparseView view_of(const SparseBuffers& b) {
-    return SparseView{b.node, b.code, b.wall, b.linkbase, b.rowstart, b.rowmask, b.rowpre, b.idx_of, b.K, b.L, b.W};
+    return SparseView{b.node, b.code, b.wall, b.linkbase, b.rowstart, b.rowmask, b.rowpre, b.idx_of,
+                      b.meta, b.dres, b.tlb, b.tdb, b.K, b.L, b.W, b.NR};
+}
+
+// Odd-step metadata, built once per geometry so the gather step needs no coordinate decode and
+// no row lookups. Nodes are grouped in tiles of 256 (tile t = k >> 8).
+//   D3Q19, two words per node:
+//     meta[2k]   bits 0..18 wall mask, bits 19..31 link slot of the node minus tlb[t]
+//     meta[2k+1] bits 0..18 edge mask (a + c_i outside the box), bits 19..26 row bits: whether
+//                (x+dx, y+dy, z) is stored, for the 8 neighbour rows
+//   D3Q7, one word per node: bits 0..6 wall mask, 7..13 edge mask, 14..31 link residual.
+//   dres[k*NR + s] + tdb[t*NR + s] = rank of (x+dx, y+dy, z) in its row (compact index of the
+//   first stored node of that row at or above z) minus k, for the NR neighbour rows
+//   (D3Q19: the 8 rows (dx, dy) != (0, 0) in row-slot order; D3Q7: (+1,0), (-1,0), (0,+1), (0,-1)).
+constexpr int TILE = 256;
+__host__ __device__ constexpr int row8(int dx, int dy) {
+    return (dx + 1) * 3 + (dy + 1) < 4 ? (dx + 1) * 3 + (dy + 1) : (dx + 1) * 3 + (dy + 1) - 1;
+}
+__host__ __device__ constexpr int row4(int dx, int dy) {
+    return dx == 1 ? 0 : (dx == -1 ? 1 : (dy == 1 ? 2 : 3));
 }
 
 // Build on the host from the material map: a node is stored when stored_by_code[code] != 0.
@@ -48,28 +71,59 @@ __device__ __forceinline__ bool row_bit(const SparseView& S, int r, int z) {
     return (S.rowmask[r * S.W + (z >> 5)] >> (z & 31)) & 1u;
 }
 
-// Value of the dense AA slot (j, m) (population j stored at node m) in the sparse layout:
-// stored node -> f; wall node reached by a link from m - c_j -> that link slot; otherwise the
-// slot is never touched and holds its initial value `init`.
-template <typename TS, typename TC, int Q>
-__device__ __forceinline__ TC dense_slot(const SparseView& S, const Geom& G, const TS* __restrict__ f,
-                                         const TS* __restrict__ link, int j, int64_t m, int mx, int my, int mz,
-                                         TC init) {
-    const int k = S.idx_of[m];
-    if (k >= 0) return ld<TS, TC>(f + (int64_t)j * S.K + k);
-    const int cx = (Q == 19) ? q19cx(j) : q7cx(j);
-    const int cy = (Q == 19) ? q19cy(j) : q7cy(j);
-    const int cz = (Q == 19) ? q19cz(j) : q7cz(j);
-    const int px = mx - cx, py = my - cy, pz = mz - cz;
-    if (j == 0 || (unsigned)px >= (unsigned)G.nx || (unsigned)py >= (unsigned)G.ny || (unsigned)pz >= (unsigned)G.nz)
-        return init;
-    const int p = S.idx_of[(int64_t)px * G.plane + py * G.nz + pz];
-    if (p < 0) return init;
-    const uint32_t wm = S.wall[p];
-    return ld<TS, TC>(link + S.linkbase[p] + __popc(wm & ((1u << j) - 1u)));
+// Wall links and the AA parity. A full-way bounce-back link (a, i) (a stored, b = a + c_i a
+// wall) is a two-step delay line: what a sends into b comes back as a's incoming opp(i) two
+// steps later. It needs two slots, one per step parity:
+//   odd steps  use Y = f[opp(i)][a] (a's own slot): read as incoming opp(i), then overwritten
+//              with outgoing i -- exactly the edge-reflection rule, so an odd step touches no
+//              link and writes every stored slot once (no partially written sectors);
+//   even steps use X = link slot (a, i): read as incoming opp(i), overwritten with outgoing i;
+//              Y keeps its value (the even step writes it back unchanged so its sector is whole).
+// Natural (post-stream, incoming) populations of dense node n in terms of this storage:
+//   n stored (k), source s = n - c_i:
+//     out of box -> f[i][k];  wall -> even state X(k, opp(i)), odd state f[i][k];
+//     stored (ks) -> even state f[i][k], odd state f[opp(i)][ks]
+//   n a wall node, a = n - c_i stored (ka) -> even state f[opp(i)][ka], odd state X(ka, i);
+//   anything else is never touched and keeps its initial value.
+// "even state" = the next step is even (after an odd step, or at initialisation).
+template <typename TS>
+__device__ __forceinline__ TS* link_slot(const SparseView& S, TS* link, int k, int j) {
+    return link + S.linkbase[k] + __popc(S.wall[k] & ((1u << j) - 1u));
 }
 
-// Natural (incoming, post-stream) populations of dense node n under the AA parity rule.
+template <int Q>
+__device__ __forceinline__ void qdir(int i, int& cx, int& cy, int& cz, int& oi) {
+    cx = (Q == 19) ? q19cx(i) : q7cx(i);
+    cy = (Q == 19) ? q19cy(i) : q7cy(i);
+    cz = (Q == 19) ? q19cz(i) : q7cz(i);
+    oi = (Q == 19) ? q19opp(i) : q7opp(i);
+}
+
+// Storage location of natural population i of dense node n (nullptr: untouched, initial value).
+template <typename TS, int Q>
+__device__ __forceinline__ TS* natural_slot(const SparseView& S, const Geom& G, TS* f, TS* link, int64_t n, int x,
+                                            int y, int z, int i, int odd) {
+    const int k = S.idx_of[n];
+    int cx, cy, cz, oi;
+    qdir<Q>(i, cx, cy, cz, oi);
+    if (k >= 0) {
+        if (i == 0) return f + k;
+        const int sx = x - cx, sy = y - cy, sz = z - cz;
+        if ((unsigned)sx >= (unsigned)G.nx || (unsigned)sy >= (unsigned)G.ny || (unsigned)sz >= (unsigned)G.nz)
+            return f + (int64_t)i * S.K + k;
+        const int ks = S.idx_of[(int64_t)sx * G.plane + sy * G.nz + sz];
+        if (ks < 0) return odd ? f + (int64_t)i * S.K + k : link_slot(S, link, k, oi);
+        return odd ? f + (int64_t)oi * S.K + ks : f + (int64_t)i * S.K + k;
+    }
+    if (i == 0) return nullptr;
+    const int ax = x - cx, ay = y - cy, az = z - cz;
+    if ((unsigned)ax >= (unsigned)G.nx || (unsigned)ay >= (unsigned)G.ny || (unsigned)az >= (unsigned)G.nz)
+        return nullptr;
+    const int ka = S.idx_of[(int64_t)ax * G.plane + ay * G.nz + az];
+    if (ka < 0) return nullptr;
+    return odd ? link_slot(S, link, ka, i) : f + (int64_t)oi * S.K + ka;
+}
+
 template <typename TS, typename TC, int Q>
 __device__ __forceinline__ void natural(const SparseView& S, const Geom& G, const TS* __restrict__ f,
                                         const TS* __restrict__ link, int64_t n, int odd, const TC* init,
@@ -77,64 +131,23 @@ __device__ __forceinline__ void natural(const SparseView& S, const Geom& G, cons
     int x, y, z;
     decode(G, n, x, y, z);
     for (int i = 0; i < Q; ++i) {
-        const int cx = (Q == 19) ? q19cx(i) : q7cx(i);
-        const int cy = (Q == 19) ? q19cy(i) : q7cy(i);
-        const int cz = (Q == 19) ? q19cz(i) : q7cz(i);
-        const int oi = (Q == 19) ? q19opp(i) : q7opp(i);
-        if (!odd || i == 0) {
-            out[i] = dense_slot<TS, TC, Q>(S, G, f, link, i, n, x, y, z, init[i]);
-        } else {
-            const int sx = x - cx, sy = y - cy, sz = z - cz;
-            if ((unsigned)sx < (unsigned)G.nx && (unsigned)sy < (unsigned)G.ny && (unsigned)sz < (unsigned)G.nz)
-                out[i] = dense_slot<TS, TC, Q>(S, G, f, link, oi, (int64_t)sx * G.plane + sy * G.nz + sz, sx, sy,
-                                               sz, init[oi]);
-            else
-                out[i] = dense_slot<TS, TC, Q>(S, G, f, link, i, n, x, y, z, init[i]);
-        }
+        const TS* p = natural_slot<const TS, Q>(S, G, f, link, n, x, y, z, i, odd);
+        out[i] = p ? ld<TS, TC>(p) : init[i];
     }
 }
 
-// Inverse of natural(): write the natural populations of node n into the sparse layout; slots
-// that are never touched by a stored node are dropped.
-template <typename TS, int Q>
-__device__ __forceinline__ void put_dense_slot(const SparseView& S, const Geom& G, TS* __restrict__ f,
-                                               TS* __restrict__ link, int j, int64_t m, int mx, int my, int mz,
-                                               double v) {
-    const int k = S.idx_of[m];
-    TS* dst = nullptr;
-    if (k >= 0) {
-        dst = f + (int64_t)j * S.K + k;
-    } else if (j != 0) {
-        const int cx = (Q == 19) ? q19cx(j) : q7cx(j);
-        const int cy = (Q == 19) ? q19cy(j) : q7cy(j);
-        const int cz = (Q == 19) ? q19cz(j) : q7cz(j);
-        const int px = mx - cx, py = my - cy, pz = mz - cz;
-        if ((unsigned)px < (unsigned)G.nx && (unsigned)py < (unsigned)G.ny && (unsigned)pz < (unsigned)G.nz) {
-            const int p = S.idx_of[(int64_t)px * G.plane + py * G.nz + pz];
-            if (p >= 0) dst = link + S.linkbase[p] + __popc(S.wall[p] & ((1u << j) - 1u));
-        }
-    }
-    if (!dst) return;
-    if constexpr (std::is_same<TS, __half>::value) *dst = __double2half(v);
-    else *dst = (TS)v;
-}
-
+// Inverse of natural(): write the natural populations of node n into the storage; populations
+// that no stored node ever reads are dropped.
 template <typename TS, int Q>
 __device__ __forceinline__ void put_natural(const SparseView& S, const Geom& G, TS* __restrict__ f,
                                             TS* __restrict__ link, int64_t n, int odd, const double* in) {
     int x, y, z;
     decode(G, n, x, y, z);
     for (int i = 0; i < Q; ++i) {
-        const int cx = (Q == 19) ? q19cx(i) : q7cx(i);
-        const int cy = (Q == 19) ? q19cy(i) : q7cy(i);
-        const int cz = (Q == 19) ? q19cz(i) : q7cz(i);
-        const int oi = (Q == 19) ? q19opp(i) : q7opp(i);
-        const int sx = x - cx, sy = y - cy, sz = z - cz;
-        if (odd && i != 0 && (unsigned)sx < (unsigned)G.nx && (unsigned)sy < (unsigned)G.ny &&
-            (unsigned)sz < (unsigned)G.nz)
-            put_dense_slot<TS, Q>(S, G, f, link, oi, (int64_t)sx * G.plane + sy * G.nz + sz, sx, sy, sz, in[i]);
-        else
-            put_dense_slot<TS, Q>(S, G, f, link, i, n, x, y, z, in[i]);
+        TS* p = natural_slot<TS, Q>(S, G, f, link, n, x, y, z, i, odd);
+        if (!p) continue;
+        if constexpr (std::is_same<TS, __half>::value) *p = __double2half(in[i]);
+        else *p = (TS)in[i];
     }
 }
 
