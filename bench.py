@@ -209,6 +209,7 @@ def main():
     stream = torch.cuda.Stream()
     D.set_stream(stream.cuda_stream)
     D.flow_init(cfg["delta_p"])
+    tuned = D.autotune(20)
     st = D.flow_stats()
     n_open, n_active = st["bgk_nodes"], st["active_nodes"]
 
@@ -288,7 +289,8 @@ def main():
             "config": {"workload": cfg["name"] + f", D3Q19 IncBGK, {a.precision.upper()} populations",
                        "nx": nx, "ny": ny, "nz": nz, "open_voxels": n_open, "active_nodes": n_active,
                        "all_voxel_mlups": all_vox, "l2": "flushed between timed steps (256 MB write); "
-                       "compacted lattice %.0f MB" % (19 * es * n_active / 1e6), "parallelism": f"replicas x{world}"},
+                       "compacted lattice %.0f MB" % (19 * es * n_active / 1e6), "parallelism": f"replicas x{world}",
+                       "autotune": tuned},
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "MLUPS", "h2d_bytes_per_step": h2d / k_e2e,

@@ -78,6 +78,8 @@ SIGNATURES = {
     "clb_global_error": [],
     "clb_synchronize": [C.c_void_p],
     "clb_set_stream": [C.c_void_p, C.c_void_p],
+    "clb_tune": [C.c_void_p, C.c_char_p, C.c_int],
+    "clb_autotune": [C.c_void_p, C.c_int, C.c_char_p, C.c_int],
     "clb_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
     "clb_flow_init": [C.c_void_p, C.c_double],
     "clb_flow_step": [C.c_void_p, C.c_int],
@@ -208,6 +210,14 @@ class Domain:
             self.close()
         except Exception:
             pass
+
+    def tune(self, key, value):
+        self._check(lib().clb_tune(self.h, key.encode(), int(value)))
+
+    def autotune(self, steps=20):
+        buf = C.create_string_buffer(512)
+        self._check(lib().clb_autotune(self.h, steps, buf, 512))
+        return buf.value.decode()
 
     def set_stream(self, stream_ptr):
         self._check(lib().clb_set_stream(self.h, C.c_void_p(stream_ptr)))

@@ -87,7 +87,8 @@ __global__ void __launch_bounds__(ADE_THREADS)
              int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin) {
     const Geom G = P.g;
     const int64_t K = S.K, L = S.L;
-    const uint32_t K32 = (uint32_t)K;  // 7 K < 2^31 is checked when the layout is built
+    const int64_t KS = S.KS;
+    const uint32_t K32 = (uint32_t)KS;  // row stride; 7 KS < 2^31 is checked when the layout is built
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
         const int code = S.code[k];
         const int dyn = P.dyn[code];
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(ADE_THREADS)
             const int s = mob_species[m];
             if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
             act[m] = true;
-            TS* f = g + (int64_t)m * 7 * K;
+            TS* f = g + (int64_t)m * 7 * KS;
             const TS* lk = glink + (int64_t)m * L;
 #pragma unroll
             for (int i = 0; i < 7; ++i) {
@@ -219,14 +220,17 @@ __global__ void __launch_bounds__(ADE_THREADS)
                 const TC rho = rb[m] + (TC)1;
                 const TC jx = rho * ux, jy = rho * uy, jz = rho * uz;
                 const TC d = (TC)dC[m];
-#pragma unroll
-                for (int i = 0; i < 7; ++i) {
-                    const TC cj = (TC)q7cx(i) * jx + (TC)q7cy(i) * jy + (TC)q7cz(i) * jz;
-                    o[i] = pop[m][i] * omw + w * ((TC)q7w(i) * (rb[m] + (TC)4 * cj));
-                    o[i] += (TC)q7w(i) * d;
-                }
+                // feq_i = t_i (rb + 4 c_i . j), in opposite-pair form (no zero products)
+                const TC r8 = (TC)0.125 * rb[m], d8 = (TC)0.125 * d;
+                o[0] = pop[m][0] * omw + w * ((TC)0.25 * rb[m]) + (TC)0.25 * d;
+                o[1] = pop[m][1] * omw + w * (r8 - (TC)0.5 * jx) + d8;
+                o[4] = pop[m][4] * omw + w * (r8 + (TC)0.5 * jx) + d8;
+                o[2] = pop[m][2] * omw + w * (r8 - (TC)0.5 * jy) + d8;
+                o[5] = pop[m][5] * omw + w * (r8 + (TC)0.5 * jy) + d8;
+                o[3] = pop[m][3] * omw + w * (r8 - (TC)0.5 * jz) + d8;
+                o[6] = pop[m][6] * omw + w * (r8 + (TC)0.5 * jz) + d8;
             }
-            TS* f = g + (int64_t)m * 7 * K;
+            TS* f = g + (int64_t)m * 7 * KS;
             TS* lk = glink + (int64_t)m * L;
 #pragma unroll
             for (int i = 0; i < 7; ++i) {
@@ -260,7 +264,7 @@ __global__ void k_ade_neumann(const TS* __restrict__ g, const TS* __restrict__ g
         const int db = P.dyn[mat[nb]], di = P.dyn[mat[ni]];
         if (!(db == ADE_PORE || db == ADE_BIO) || !(di == ADE_PORE || di == ADE_BIO)) continue;
         TC pop[7];
-        natural<TS, TC, 7>(S, G, g + (int64_t)m * 7 * S.K, glink + (int64_t)m * S.L, ni, odd, init, pop);
+        natural<TS, TC, 7>(S, G, g + (int64_t)m * 7 * S.KS, glink + (int64_t)m * S.L, ni, odd, init, pop);
         double r = 1.0;
         for (int i = 0; i < 7; ++i) r += (double)pop[i];
         neu[((int64_t)s * 2 + side) * G.plane + p] = r;
@@ -270,6 +274,7 @@ __global__ void k_ade_neumann(const TS* __restrict__ g, const TS* __restrict__ g
 template <typename TS>
 __global__ void k_ade_init(TS* __restrict__ g, TS* __restrict__ glink, int64_t K, int64_t L, int n_mobile,
                            const double* __restrict__ c0m) {
+    // K here is the padded row stride: the padding slots are initialised too
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K || k < L;
          k += (int64_t)gridDim.x * blockDim.x) {
         for (int m = 0; m < n_mobile; ++m) {
@@ -346,7 +351,7 @@ __global__ void k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ gl
             const int m = P.slot[s];
             if (m >= 0) {
                 double sum = 1.0;
-                for (int i = 0; i < 7; ++i) sum += ldd(g + ((int64_t)m * 7 + i) * K + k);
+                for (int i = 0; i < 7; ++i) sum += ldd(g + ((int64_t)m * 7 + i) * S.KS + k);
                 c = sum;
             } else {
                 c = imm[(int64_t)s * K + k];
@@ -478,7 +483,8 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
     const size_t K1 = (size_t)std::max<int64_t>(1, K), L1 = (size_t)std::max<int64_t>(1, L);
     const int nm1 = std::max(1, h->n_mobile);
     cudaError_t e;
-    if ((e = cudaMalloc(&h->d_g, esize(h->ade_prec) * 7 * K1 * nm1)) != cudaSuccess)
+    const size_t KS = (size_t)h->ade_sp.KS;
+    if ((e = cudaMalloc(&h->d_g, esize(h->ade_prec) * 7 * KS * nm1)) != cudaSuccess)
         return cuda_check(h, e, "species populations");
     if ((e = cudaMalloc(&h->d_glink, esize(h->ade_prec) * L1 * nm1)) != cudaSuccess)
         return cuda_check(h, e, "species links");
@@ -514,9 +520,9 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
         cudaMemcpy(dc0, c0m.data(), sizeof(double) * c0m.size(), cudaMemcpyHostToDevice);
         const int grid = h->num_sms * 8;
         switch (h->ade_prec) {
-            case CLB_F64: k_ade_init<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g, (double*)h->d_glink, K, L, h->n_mobile, dc0); break;
-            case CLB_F32: k_ade_init<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g, (float*)h->d_glink, K, L, h->n_mobile, dc0); break;
-            default: k_ade_init<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g, (__half*)h->d_glink, K, L, h->n_mobile, dc0); break;
+            case CLB_F64: k_ade_init<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g, (double*)h->d_glink, (int64_t)KS, L, h->n_mobile, dc0); break;
+            case CLB_F32: k_ade_init<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g, (float*)h->d_glink, (int64_t)KS, L, h->n_mobile, dc0); break;
+            default: k_ade_init<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g, (__half*)h->d_glink, (int64_t)KS, L, h->n_mobile, dc0); break;
         }
         cudaStreamSynchronize(h->stream);
         cudaFree(dc0);
@@ -679,7 +685,7 @@ static clb_status ade_populations_i(clb_handle* h, int s, double* host) {
     if (e != cudaSuccess) return cuda_check(h, e, "population buffer");
     const int odd = (int)(h->ade_iters & 1);
     const int grid = h->num_sms * 8;
-    const size_t off = (size_t)m * 7 * h->ade_sp.K, loff = (size_t)m * h->ade_sp.L;
+    const size_t off = (size_t)m * 7 * h->ade_sp.KS, loff = (size_t)m * h->ade_sp.L;
     const SparseView S = view_of(h->ade_sp);
     const double c0 = h->ap.c0[s];
     switch (h->ade_prec) {
@@ -711,7 +717,7 @@ clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
     cudaMemcpy(buf, host, sizeof(double) * 7 * (size_t)h->g.N, cudaMemcpyHostToDevice);
     const int odd = (int)(h->ade_iters & 1);
     const int grid = h->num_sms * 8;
-    const size_t off = (size_t)m * 7 * h->ade_sp.K, loff = (size_t)m * h->ade_sp.L;
+    const size_t off = (size_t)m * 7 * h->ade_sp.KS, loff = (size_t)m * h->ade_sp.L;
     const SparseView S = view_of(h->ade_sp);
     switch (h->ade_prec) {
         case CLB_F64: k_ade_set_pops<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g + off, (double*)h->d_glink + loff, S, h->g, odd, buf); break;

@@ -93,6 +93,7 @@ clb_status clb_destroy(clb_handle* h) {
     flow_free(h);
     ade_free(h);
     cudaFree(h->d_mat);
+    cudaFree(h->d_err);
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
     return CLB_OK;
@@ -101,7 +102,12 @@ clb_status clb_destroy(clb_handle* h) {
 clb_status clb_synchronize(clb_handle* h) {
     if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
     CLB_ON_DEVICE(h);
-    return cuda_check(h, cudaStreamSynchronize(h->stream), "synchronize");
+    clb_status s = cuda_check(h, cudaStreamSynchronize(h->stream), "synchronize");
+    if (s != CLB_OK || !h->d_err) return s;
+    int flag = 0;
+    cudaMemcpy(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (flag) return fail(h, CLB_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
+    return CLB_OK;
 }
 
 clb_status clb_set_stream(clb_handle* h, void* stream) {
@@ -120,6 +126,25 @@ clb_status clb_get_stream(clb_handle* h, void** stream) {
     CLB_ON_DEVICE(h);
     *stream = (void*)h->stream;
     return CLB_OK;
+}
+
+clb_status clb_tune(clb_handle* h, const char* key, int value) {
+    if (!h || !key) return fail(h, CLB_INVALID_ARG, "null argument");
+    const std::string k = key;
+    if (k == "flow_even_tma") { h->flow_even_tma = value ? 1 : 0; return CLB_OK; }
+    if (k == "flow_min_blocks") {
+        if (value != 2 && value != 3) return fail(h, CLB_INVALID_ARG, "flow_min_blocks is 2 or 3");
+        h->flow_minb = value;
+        return CLB_OK;
+    }
+    return fail(h, CLB_INVALID_ARG, "unknown tuning key '" + k + "'");
+}
+
+clb_status clb_autotune(clb_handle* h, int steps, char* report, int report_len) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
+    return flow_autotune(h, steps, report, report_len);
 }
 
 clb_status clb_flow_init(clb_handle* h, double delta_p) {

@@ -139,6 +139,7 @@ struct SparseBuffers {
     int32_t* tlb = nullptr;     // [T] link base of each 256-node tile
     int32_t* tdb = nullptr;     // [T][NR] neighbour-row rank bases of each tile
     int64_t K = 0, L = 0;
+    int64_t KS = 0;             // population row stride: K rounded up to a multiple of 256
     int W = 0, NR = 0;
 };
 }  // namespace clb
@@ -167,6 +168,10 @@ struct clb_handle_s {
     double* d_partials = nullptr;     // per-block partial sums (scratch)
     int partial_cap = 0;
     int flow_grid = 0;
+    int flow_even_tma = 1;            // even AA step through shared-memory tiles and bulk copies
+    int flow_minb = 3;                // minimum resident CTAs per SM of the gather/scatter step (2 or 3)
+    int flow_even_grid = 0;
+    int* d_err = nullptr;             // device error flag (bounded waits that gave up)
     int64_t flow_iters = 0;           // host mirror of the device iteration count
     double delta_p = 0;
 
@@ -199,6 +204,7 @@ clb_status cuda_check(clb_handle* h, cudaError_t e, const char* what);
 clb_status flow_init(clb_handle* h, double delta_p);
 clb_status flow_step(clb_handle* h, int n, bool trace, double eps);
 clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations);
+clb_status flow_autotune(clb_handle* h, int steps, char* report, int report_len);
 clb_status flow_stats(clb_handle* h, double char_length, clb_flow_stats* out);
 clb_status flow_velocity(clb_handle* h, void* dst, int dtype_device, bool to_host);
 clb_status flow_velocity_at(clb_handle* h, const int32_t* nodes, int64_t count, void* u, int64_t stride, int dtype);

@@ -27,6 +27,7 @@
 // material code and 4 bytes wall mask + link offset (even step); 1 byte code, 8 bytes masks and
 // 16 bytes neighbour-row offsets (odd step).
 #include "sparse.cuh"
+#include "tma.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -77,6 +78,44 @@ __device__ __forceinline__ void regularize19(TC (&g)[19], int orient, TC rb) {
                (TC)2 * (cx * cy * pxy + cx * cz * pxz + cy * cz * pyz);
         g[i] = feq19<TC>(i, rb, jx, (TC)0, (TC)0, jsq) + (TC)q19w(i) * (TC)4.5 * s;
     }
+}
+
+
+// IncBGK collision of one node in place, in opposite-pair form: for the pair (i, opp(i)) with
+// cj = c_i . j, feq = t (rb - 1.5 |j|^2 + 4.5 cj^2) +- 3 t cj. Written out per direction so no
+// term is multiplied by a zero velocity component (IEEE-strict code cannot fold 0 * x away).
+// Returns |j|^2.
+template <typename TC>
+__device__ __forceinline__ TC bgk19(TC (&g)[19], TC w) {
+    const TC rb = (((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7]))) +
+                  (((g[8] + g[9]) + (g[10] + g[11])) + ((g[12] + g[13]) + (g[14] + g[15]))) + ((g[16] + g[17]) + g[18]);
+    const TC jx = ((g[10] + g[13]) + (g[14] + g[15]) + g[16]) - ((g[1] + g[4]) + (g[5] + g[6]) + g[7]);
+    const TC jy = ((g[5] + g[11]) + (g[13] + g[17]) + g[18]) - ((g[2] + g[4]) + (g[8] + g[9]) + g[14]);
+    const TC jz = ((g[7] + g[9]) + (g[12] + g[15]) + g[17]) - ((g[3] + g[6]) + (g[8] + g[16]) + g[18]);
+    const TC jsq = jx * jx + jy * jy + jz * jz;
+    const TC omw = (TC)1 - w;
+    const TC base = rb - (TC)1.5 * jsq;
+    const TC t1 = (TC)(1.0 / 18.0), t2 = (TC)(1.0 / 36.0);
+    g[0] = omw * g[0] + w * ((TC)(1.0 / 3.0) * base);
+#define CLB_PAIR(I, CJ, T)                                          \
+    {                                                               \
+        const TC cj = (CJ);                                         \
+        const TC sym = (T) * (base + (TC)4.5 * cj * cj);            \
+        const TC asym = (T) * ((TC)3 * cj);                         \
+        g[I] = omw * g[I] + w * (sym + asym);                       \
+        g[I + 9] = omw * g[I + 9] + w * (sym - asym);               \
+    }
+    CLB_PAIR(1, -jx, t1)
+    CLB_PAIR(2, -jy, t1)
+    CLB_PAIR(3, -jz, t1)
+    CLB_PAIR(4, -jx - jy, t2)
+    CLB_PAIR(5, -jx + jy, t2)
+    CLB_PAIR(6, -jx - jz, t2)
+    CLB_PAIR(7, -jx + jz, t2)
+    CLB_PAIR(8, -jy - jz, t2)
+    CLB_PAIR(9, -jy + jz, t2)
+#undef CLB_PAIR
+    return jsq;
 }
 
 // Block-wide FP64 sum; result valid in thread 0.
@@ -149,14 +188,14 @@ __device__ void finish_step(Tracer* tr, double* partials, double block_total, in
 
 
 
-template <typename TS, typename TC, bool ODD>
-__global__ void __launch_bounds__(FLOW_THREADS, 3)
+template <typename TS, typename TC, bool ODD, int MINB>
+__global__ void __launch_bounds__(FLOW_THREADS, MINB)
     k_flow_aa(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const FlowParams P,
               Tracer* __restrict__ tr, double* __restrict__ partials, int trace, int64_t k_west_end,
               int64_t k_east_begin) {
     if (trace && tr->converged) return;  // a batch continues past convergence as no-ops
     const int64_t K = S.K;
-    const uint32_t K32 = (uint32_t)K;  // 19 K < 2^31 is checked when the layout is built
+    const uint32_t K32 = (uint32_t)S.KS;  // row stride; 19 KS < 2^31 is checked when the layout is built
     double esum = 0;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
         const int code = S.code[k];
@@ -213,20 +252,7 @@ __global__ void __launch_bounds__(FLOW_THREADS, 3)
         if (P.dyn[code] == DYN_BGK) {
             if (k < k_west_end) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
             else if (k >= k_east_begin) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
-            TC rb = 0, jx = 0, jy = 0, jz = 0;
-#pragma unroll
-            for (int i = 0; i < 19; ++i) {
-                rb += g[i];
-                jx += (TC)q19cx(i) * g[i];
-                jy += (TC)q19cy(i) * g[i];
-                jz += (TC)q19cz(i) * g[i];
-            }
-            const TC jsq = jx * jx + jy * jy + jz * jz;
-            const TC w = (TC)P.omega[code];
-            const TC omw = (TC)1 - w;
-#pragma unroll
-            for (int i = 0; i < 19; ++i) g[i] = g[i] * omw + w * feq19<TC>(i, rb, jx, jy, jz, jsq);
-            esum += (double)jsq;
+            esum += (double)bgk19<TC>(g, (TC)P.omega[code]);
         }
         if (!ODD) {
 #pragma unroll
@@ -255,6 +281,114 @@ __global__ void __launch_bounds__(FLOW_THREADS, 3)
     finish_step(tr, partials, bt, P.n_bgk, trace);
 }
 
+
+// Even AA step through shared memory: a persistent CTA walks 256-node tiles; one thread moves the
+// tile's 19 population rows (contiguous, 16-byte aligned thanks to the padded row stride) into
+// shared memory with bulk copies completing on an mbarrier, keeping NSTAGE-1 tiles in flight
+// ahead of the one being collided. Each thread collides its node in place in shared memory; the
+// rows go back with bulk stores. A wall link (a, i) takes its incoming opp(i) from its even-step
+// slot X (a global load issued alongside the tile's), writes outgoing i to X, and leaves its
+// odd-step slot Y = f[opp(i)][a] untouched in the tile, so the bulk store rewrites it unchanged.
+constexpr int NSTAGE = 3;
+
+template <typename TS, typename TC>
+__global__ void __launch_bounds__(TILE, 2)
+    k_flow_even_tma(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const FlowParams P,
+                    Tracer* __restrict__ tr, double* __restrict__ partials, int trace, int64_t k_west_end,
+                    int64_t k_east_begin, int* __restrict__ err) {
+    if (trace && tr->converged) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    TS* stages = reinterpret_cast<TS*>(smem_raw);
+    __shared__ __align__(8) uint64_t full[NSTAGE];
+    __shared__ int s_abort;
+    const int tid = threadIdx.x;
+    const int64_t K = S.K, KS = S.KS;
+    const int ntiles = (int)((K + TILE - 1) / TILE);
+    const uint32_t row_bytes = TILE * sizeof(TS);
+    if (tid == 0) {
+        for (int q = 0; q < NSTAGE; ++q) mbar_init(&full[q], 1);
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+    auto issue_load = [&](int t, int q) {
+        TS* dst = stages + (size_t)q * 19 * TILE;
+        mbar_expect_tx(&full[q], 19 * row_bytes);
+        for (int i = 0; i < 19; ++i) bulk_g2s(dst + i * TILE, f + (int64_t)i * KS + (int64_t)t * TILE, row_bytes, &full[q]);
+    };
+    double esum = 0;
+    if (tid == 0)
+        for (int q = 0; q < NSTAGE - 1; ++q) {
+            const int t = blockIdx.x + q * gridDim.x;
+            if (t < ntiles) issue_load(t, q);
+        }
+    int j = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
+        const int q = j % NSTAGE;
+        TS* buf = stages + (size_t)q * 19 * TILE;
+        // keep NSTAGE-1 tiles in flight: refill the stage freed two iterations ago
+        const int tn = t + (NSTAGE - 1) * gridDim.x;
+        if (tid == 0 && tn < ntiles) {
+            bulk_wait_read_all();
+            issue_load(tn, (j + NSTAGE - 1) % NSTAGE);
+        }
+        const int64_t k = (int64_t)t * TILE + tid;
+        const bool live = k < K;
+        uint32_t wm = 0;
+        int lb = 0, code = 0;
+        TC xv[19];
+        if (live) {
+            const uint32_t m0 = S.meta[2 * k];
+            wm = m0 & 0x7FFFFu;
+            lb = S.tlb[t] + (int)(m0 >> 19);
+            code = S.code[k];
+            int r = 0;
+#pragma unroll
+            for (int i = 1; i < 19; ++i) {
+                const bool wl = (wm >> i) & 1u;
+                xv[q19opp(i)] = wl ? ld<TS, TC>(link + lb + r) : (TC)0;
+                r += wl;
+            }
+        }
+        if (!mbar_wait(&full[q], (uint32_t)((j / NSTAGE) & 1))) {
+            if (tid == 0) { atomicExch(err, 1); s_abort = 1; }
+        }
+        __syncthreads();
+        if (s_abort) break;
+        if (live) {
+            TC g[19];
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                const bool wsrc = i != 0 && ((wm >> q19opp(i)) & 1u);
+                g[i] = wsrc ? xv[i] : ld<TS, TC>(buf + i * TILE + tid);
+            }
+            if (P.dyn[code] == DYN_BGK) {
+                if (k < k_west_end) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
+                else if (k >= k_east_begin) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
+                esum += (double)bgk19<TC>(g, (TC)P.omega[code]);
+            }
+            int r = 0;
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                const bool wl = (wm >> i) & 1u;
+                if (wl) st<TS, TC>(link + lb + r, g[i]);
+                else st<TS, TC>(buf + q19opp(i) * TILE + tid, g[i]);
+                r += wl;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            fence_async_smem();
+            for (int i = 0; i < 19; ++i) bulk_s2g(f + (int64_t)i * KS + (int64_t)t * TILE, buf + i * TILE, row_bytes);
+            bulk_commit();
+        }
+    }
+    if (tid == 0) bulk_wait_all();
+    __shared__ double sh[32];
+    double bt = block_sum(esum, sh);
+    finish_step(tr, partials, bt, P.n_bgk, trace);
+}
+
 // PressureGradient equilibrium (complab_functions.hh:82-94): BGK nodes t_i (rho(x) - 1),
 // no-dynamics nodes zero (BounceBack / NoDynamics equilibria are zero). For a wall link (a, i)
 // the even-step slot X holds a's equilibrium incoming opp(i) and the odd-step slot
@@ -273,8 +407,8 @@ __global__ void k_flow_init(TS* __restrict__ f, TS* __restrict__ link, const Spa
             const double eq = bgk ? q19w(i) * (rho - 1.0) : 0.0;
             const bool wall_src = i != 0 && ((wm >> q19opp(i)) & 1u);
             const double v = wall_src ? 0.0 : eq;
-            if constexpr (std::is_same<TS, __half>::value) f[(int64_t)i * S.K + k] = __double2half(v);
-            else f[(int64_t)i * S.K + k] = (TS)v;
+            if constexpr (std::is_same<TS, __half>::value) f[(int64_t)i * S.KS + k] = __double2half(v);
+            else f[(int64_t)i * S.KS + k] = (TS)v;
             if (wall_src) {
                 TS* x_ = link_slot(S, link, (int)k, q19opp(i));
                 if constexpr (std::is_same<TS, __half>::value) *x_ = __double2half(eq);
@@ -382,6 +516,12 @@ __global__ void k_flow_vstats(const double* __restrict__ u, const Geom G, double
 
 static size_t storage_size(int prec) { return prec == CLB_F64 ? 8 : (prec == CLB_F32 ? 4 : 2); }
 
+template <typename TS>
+static size_t even_smem() {
+    return (size_t)NSTAGE * 19 * TILE * sizeof(TS);
+}
+
+
 template <typename F>
 static int grid_for(clb_handle* h, F kernel, int threads) {
     int per_sm = 0;
@@ -397,6 +537,14 @@ void flow_free(clb_handle* h) {
     cudaFree(h->d_tracer); h->d_tracer = nullptr;
     cudaFree(h->d_partials); h->d_partials = nullptr;
     h->flow_ready = false;
+}
+
+static int flow_gather_grid(clb_handle* h) {
+    switch (h->flow_prec) {
+        case CLB_F64: return h->flow_minb == 2 ? grid_for(h, k_flow_aa<double, double, true, 2>, FLOW_THREADS) : grid_for(h, k_flow_aa<double, double, true, 3>, FLOW_THREADS);
+        case CLB_F32: return h->flow_minb == 2 ? grid_for(h, k_flow_aa<float, float, true, 2>, FLOW_THREADS) : grid_for(h, k_flow_aa<float, float, true, 3>, FLOW_THREADS);
+        default: return h->flow_minb == 2 ? grid_for(h, k_flow_aa<__half, float, true, 2>, FLOW_THREADS) : grid_for(h, k_flow_aa<__half, float, true, 3>, FLOW_THREADS);
+    }
 }
 
 clb_status flow_init(clb_handle* h, double delta_p) {
@@ -445,23 +593,48 @@ clb_status flow_init(clb_handle* h, double delta_p) {
     h->flow_prec = d.flow_precision;
     const size_t es = storage_size(h->flow_prec);
     cudaError_t e;
-    if ((e = cudaMalloc(&h->d_f, es * 19 * (size_t)std::max<int64_t>(1, K))) != cudaSuccess)
+    if ((e = cudaMalloc(&h->d_f, es * 19 * (size_t)h->flow_sp.KS)) != cudaSuccess)
         return cuda_check(h, e, "flow populations");
-    if ((e = cudaMalloc(&h->d_flink, es * (size_t)std::max<int64_t>(1, h->flow_sp.L))) != cudaSuccess)
+    // +16 bytes: the FP16 even step copies whole aligned 4-byte words around each link slot
+    if ((e = cudaMalloc(&h->d_flink, es * (size_t)std::max<int64_t>(1, h->flow_sp.L) + 16)) != cudaSuccess)
         return cuda_check(h, e, "flow links");
     if ((e = cudaMalloc(&h->d_tracer, sizeof(Tracer))) != cudaSuccess) return cuda_check(h, e, "tracer");
     cudaMemsetAsync(h->d_tracer, 0, sizeof(Tracer), h->stream);
     cudaMemsetAsync(h->d_flink, 0, es * (size_t)std::max<int64_t>(1, h->flow_sp.L), h->stream);
 
-    int grid = 0;
-    switch (h->flow_prec) {
-        case CLB_F64: grid = grid_for(h, k_flow_aa<double, double, true>, FLOW_THREADS); break;
-        case CLB_F32: grid = grid_for(h, k_flow_aa<float, float, true>, FLOW_THREADS); break;
-        default: grid = grid_for(h, k_flow_aa<__half, float, true>, FLOW_THREADS); break;
-    }
+    int grid = flow_gather_grid(h);
     h->flow_grid = grid;
-    if ((e = cudaMalloc(&h->d_partials, sizeof(double) * grid)) != cudaSuccess) return cuda_check(h, e, "partials");
-    h->partial_cap = grid;
+    // the even step's tiled kernel: persistent CTAs, shared-memory stages sized by precision
+    {
+        int per_sm = 0;
+        size_t sm = 0;
+        switch (h->flow_prec) {
+            case CLB_F64:
+                sm = even_smem<double>();
+                cudaFuncSetAttribute(k_flow_even_tma<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_even_tma<double, double>, TILE, sm);
+                break;
+            case CLB_F32:
+                sm = even_smem<float>();
+                cudaFuncSetAttribute(k_flow_even_tma<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_even_tma<float, float>, TILE, sm);
+                break;
+            default:
+                sm = even_smem<__half>();
+                cudaFuncSetAttribute(k_flow_even_tma<__half, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_even_tma<__half, float>, TILE, sm);
+                break;
+        }
+        h->flow_even_grid = h->num_sms * std::max(1, per_sm);
+    }
+    // partials sized for the largest grid any variant uses
+    const int pcap = h->num_sms * 8;
+    if ((e = cudaMalloc(&h->d_partials, sizeof(double) * pcap)) != cudaSuccess) return cuda_check(h, e, "partials");
+    h->partial_cap = pcap;
+    if (!h->d_err) {
+        if ((e = cudaMalloc(&h->d_err, sizeof(int))) != cudaSuccess) return cuda_check(h, e, "error flag");
+    }
+    cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
 
     const int ig = h->num_sms * 8;
     const SparseView S = view_of(h->flow_sp);
@@ -479,21 +652,37 @@ static void launch_flow(clb_handle* h, bool odd, int trace) {
     const FlowParams& P = h->fp;
     const SparseView S = view_of(h->flow_sp);
     const int grid = h->flow_grid;
-#define CLB_LAUNCH(TS, TC)                                                                                     \
+    if (!odd && h->flow_even_tma) {
+        const int eg = h->flow_even_grid;
+#define CLB_EVEN(TS, TC)                                                                                       \
+        k_flow_even_tma<TS, TC><<<eg, TILE, even_smem<TS>(), h->stream>>>((TS*)h->d_f, (TS*)h->d_flink, S, P,  \
+                                                                       h->d_tracer, h->d_partials, trace,     \
+                                                                       h->k_west_end, h->k_east_begin, h->d_err);
+        switch (h->flow_prec) {
+            case CLB_F64: CLB_EVEN(double, double); break;
+            case CLB_F32: CLB_EVEN(float, float); break;
+            default: CLB_EVEN(__half, float); break;
+        }
+#undef CLB_EVEN
+        return;
+    }
+#define CLB_LAUNCH_B(TS, TC, B)                                                                                \
     if (odd)                                                                                                   \
-        k_flow_aa<TS, TC, true><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, (TS*)h->d_flink, S, P,       \
-                                                                       h->d_tracer, h->d_partials, trace,      \
-                                                                       h->k_west_end, h->k_east_begin);        \
+        k_flow_aa<TS, TC, true, B><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, (TS*)h->d_flink, S, P,    \
+                                                                          h->d_tracer, h->d_partials, trace,   \
+                                                                          h->k_west_end, h->k_east_begin);     \
     else                                                                                                       \
-        k_flow_aa<TS, TC, false><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, (TS*)h->d_flink, S, P,      \
-                                                                        h->d_tracer, h->d_partials, trace,     \
-                                                                        h->k_west_end, h->k_east_begin);
+        k_flow_aa<TS, TC, false, B><<<grid, FLOW_THREADS, 0, h->stream>>>((TS*)h->d_f, (TS*)h->d_flink, S, P,   \
+                                                                           h->d_tracer, h->d_partials, trace,  \
+                                                                           h->k_west_end, h->k_east_begin);
+#define CLB_LAUNCH(TS, TC) if (h->flow_minb == 2) { CLB_LAUNCH_B(TS, TC, 2) } else { CLB_LAUNCH_B(TS, TC, 3) }
     switch (h->flow_prec) {
         case CLB_F64: CLB_LAUNCH(double, double); break;
         case CLB_F32: CLB_LAUNCH(float, float); break;
         default: CLB_LAUNCH(__half, float); break;
     }
 #undef CLB_LAUNCH
+#undef CLB_LAUNCH_B
 }
 
 clb_status flow_step(clb_handle* h, int n, bool trace, double eps) {
@@ -656,6 +845,71 @@ clb_status flow_stats(clb_handle* h, double char_length, clb_flow_stats* out) {
     out->bgk_nodes = h->fp.n_bgk;
     out->active_nodes = h->flow_sp.K;
     return CLB_OK;
+}
+
+// Times every kernel variant (even step through TMA tiles or not; gather step compiled for 2 or
+// 3 resident CTAs) over `steps` steps and keeps the fastest. The lattice state is saved before
+// and restored after, so the run is unchanged. Writes a one-line report into `report`.
+clb_status flow_autotune(clb_handle* h, int steps, char* report, int report_len) {
+    if (steps < 2) steps = 2;
+    steps += steps & 1;
+    const size_t es = storage_size(h->flow_prec);
+    const size_t fb = es * 19 * (size_t)h->flow_sp.KS, lb = es * (size_t)std::max<int64_t>(1, h->flow_sp.L) + 16;
+    void* sf = nullptr;
+    void* sl = nullptr;
+    cudaError_t e = cudaMalloc(&sf, fb);
+    if (e == cudaSuccess) e = cudaMalloc(&sl, lb);
+    if (e != cudaSuccess) { cudaFree(sf); return cuda_check(h, e, "autotune buffers"); }
+    Tracer tsave;
+    cudaMemcpyAsync(sf, h->d_f, fb, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(sl, h->d_flink, lb, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(&tsave, h->d_tracer, sizeof(Tracer), cudaMemcpyDeviceToHost, h->stream);
+    cudaStreamSynchronize(h->stream);
+    const int64_t iters0 = h->flow_iters;
+    const int save_tma = h->flow_even_tma, save_minb = h->flow_minb;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    int best_tma = save_tma, best_minb = save_minb;
+    std::string rep;
+    for (int tma = 1; tma >= 0; --tma)
+        for (int minb = 3; minb >= 2; --minb) {
+            h->flow_even_tma = tma;
+            h->flow_minb = minb;
+            h->flow_grid = flow_gather_grid(h);
+            flow_step(h, 2, false, 0.0);  // warm
+            cudaEventRecord(a, h->stream);
+            flow_step(h, steps, false, 0.0);
+            cudaEventRecord(b, h->stream);
+            cudaEventSynchronize(b);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            char buf[96];
+            snprintf(buf, sizeof(buf), "%stma=%d,minb=%d:%.1fus", rep.empty() ? "" : " ", tma, minb, 1e3f * ms / steps);
+            rep += buf;
+            if (ms < best) { best = ms; best_tma = tma; best_minb = minb; }
+        }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    h->flow_even_tma = best_tma;
+    h->flow_minb = best_minb;
+    h->flow_grid = flow_gather_grid(h);
+    cudaMemcpyAsync(h->d_f, sf, fb, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->d_flink, sl, lb, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->d_tracer, &tsave, sizeof(Tracer), cudaMemcpyHostToDevice, h->stream);
+    e = cudaStreamSynchronize(h->stream);
+    cudaFree(sf);
+    cudaFree(sl);
+    h->flow_iters = iters0;
+    char buf[64];
+    snprintf(buf, sizeof(buf), " -> tma=%d,minb=%d", best_tma, best_minb);
+    rep += buf;
+    if (report && report_len > 0) {
+        std::strncpy(report, rep.c_str(), (size_t)report_len - 1);
+        report[report_len - 1] = 0;
+    }
+    return cuda_check(h, e, "autotune");
 }
 
 }  // namespace clb

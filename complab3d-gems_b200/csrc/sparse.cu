@@ -73,7 +73,8 @@ clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, Spar
         L += __builtin_popcount(wm);
     }
     if (L > INT32_MAX) return fail(h, CLB_INVALID_ARG, "too many wall links");
-    if ((int64_t)K * q > INT32_MAX) return fail(h, CLB_INVALID_ARG, "lattice exceeds 2^31 populations per species");
+    const int64_t KS = ((int64_t)K + TILE - 1) / TILE * TILE;
+    if (KS * q > INT32_MAX) return fail(h, CLB_INVALID_ARG, "lattice exceeds 2^31 populations per species");
 
     // ---- odd-step metadata
     const int NR = q == 19 ? 8 : 4;
@@ -153,6 +154,7 @@ clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, Spar
     out.L = L;
     out.W = W;
     out.NR = NR;
+    out.KS = std::max<int64_t>(KS, TILE);
     return cuda_check(h, e, "sparse layout");
 }
 

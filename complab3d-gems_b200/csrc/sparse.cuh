@@ -30,12 +30,13 @@ struct SparseView {
     const int32_t* tlb;
     const int32_t* tdb;
     int64_t K, L;
+    int64_t KS;               // population row stride (K rounded up to a multiple of TILE)
     int W, NR;
 };
 
 inline SparseView view_of(const SparseBuffers& b) {
     return SparseView{b.node, b.code, b.wall, b.linkbase, b.rowstart, b.rowmask, b.rowpre, b.idx_of,
-                      b.meta, b.dres, b.tlb, b.tdb, b.K, b.L, b.W, b.NR};
+                      b.meta, b.dres, b.tlb, b.tdb, b.K, b.L, b.KS, b.W, b.NR};
 }
 
 // Odd-step metadata, built once per geometry so the gather step needs no coordinate decode and
@@ -110,10 +111,10 @@ __device__ __forceinline__ TS* natural_slot(const SparseView& S, const Geom& G, 
         if (i == 0) return f + k;
         const int sx = x - cx, sy = y - cy, sz = z - cz;
         if ((unsigned)sx >= (unsigned)G.nx || (unsigned)sy >= (unsigned)G.ny || (unsigned)sz >= (unsigned)G.nz)
-            return f + (int64_t)i * S.K + k;
+            return f + (int64_t)i * S.KS + k;
         const int ks = S.idx_of[(int64_t)sx * G.plane + sy * G.nz + sz];
-        if (ks < 0) return odd ? f + (int64_t)i * S.K + k : link_slot(S, link, k, oi);
-        return odd ? f + (int64_t)oi * S.K + ks : f + (int64_t)i * S.K + k;
+        if (ks < 0) return odd ? f + (int64_t)i * S.KS + k : link_slot(S, link, k, oi);
+        return odd ? f + (int64_t)oi * S.KS + ks : f + (int64_t)i * S.KS + k;
     }
     if (i == 0) return nullptr;
     const int ax = x - cx, ay = y - cy, az = z - cz;
@@ -121,7 +122,7 @@ __device__ __forceinline__ TS* natural_slot(const SparseView& S, const Geom& G, 
         return nullptr;
     const int ka = S.idx_of[(int64_t)ax * G.plane + ay * G.nz + az];
     if (ka < 0) return nullptr;
-    return odd ? link_slot(S, link, ka, i) : f + (int64_t)oi * S.K + ka;
+    return odd ? link_slot(S, link, ka, i) : f + (int64_t)oi * S.KS + ka;
 }
 
 template <typename TS, typename TC, int Q>

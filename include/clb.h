@@ -144,6 +144,19 @@ clb_status clb_synchronize(clb_handle* h);
 clb_status clb_set_stream(clb_handle* h, void* stream);
 clb_status clb_get_stream(clb_handle* h, void** stream);
 
+/* Launch-shape and kernel-variant knobs (used by the autotuner; defaults are tuned for B200):
+ *   "flow_even_tma"  1: even AA step through shared-memory tiles and bulk copies (default),
+ *                    0: the plain per-thread load/store step;
+ *   "flow_min_blocks" 2 or 3: resident CTAs per SM the gather/scatter step is compiled for
+ *                    (register budget 128 or 80 per thread); takes effect at clb_flow_init.
+ * Unknown keys are an error. */
+clb_status clb_tune(clb_handle* h, const char* key, int value);
+
+/* Times every kernel variant of the flow step over `steps` steps on this domain and keeps the
+ * fastest; the lattice state is saved and restored, so the simulation is unchanged. A one-line
+ * report of the timings is written to `report` (may be NULL). */
+clb_status clb_autotune(clb_handle* h, int steps, char* report, int report_len);
+
 /* ---------------------------------------------------------------- flow (D3Q19) */
 
 /* Dynamics from the material map, pressure planes at x=0 (rho=1) and x=nx-1

@@ -13,21 +13,23 @@ pytestmark = pytest.mark.gpu
 BIO = dict(bio_codes=(3, 4), perm_ratio=(0.3, 0.0))
 
 
-def make_pair(clb, oracle, mat, shape, tau, dp, prec, **bio):
+def make_pair(clb, oracle, mat, shape, tau, dp, prec, even_tma=1, **bio):
     nx, ny, nz = shape
     D = clb.Domain(mat, nx, ny, nz, tau, flow_precision=prec, **bio)
+    D.tune("flow_even_tma", even_tma)
     D.flow_init(dp)
     O = oracle.OracleFlow(mat, nx, ny, nz, tau, dp, bio_codes=bio.get("bio_codes", ()),
                           perm_ratio=bio.get("perm_ratio", ()))
     return D, O
 
 
-@pytest.mark.parametrize("shape", [(18, 11, 9), (12, 7, 45)])
+@pytest.mark.parametrize("even_tma", [1, 0])
+@pytest.mark.parametrize("shape", [(18, 11, 9), (12, 7, 45), (40, 21, 33)])
 @pytest.mark.parametrize("walls", [True, False])
 @pytest.mark.parametrize("steps", [1, 2, 37, 200])
-def test_f64_populations_match_oracle(clb, oracle, shape, walls, steps):
+def test_f64_populations_match_oracle(clb, oracle, shape, walls, steps, even_tma):
     mat = mixed_geometry(*shape, walls=walls)
-    D, O = make_pair(clb, oracle, mat, shape, 0.8, 3e-4, clb.F64, **BIO)
+    D, O = make_pair(clb, oracle, mat, shape, 0.8, 3e-4, clb.F64, even_tma=even_tma, **BIO)
     D.flow_step(steps)
     O.step(steps)
     fg, fo = D.flow_populations(), O.populations()
@@ -49,11 +51,12 @@ def test_f64_solve_matches_oracle_iterations(clb, oracle):
     assert st["permeability"] > 0
 
 
+@pytest.mark.parametrize("even_tma", [1, 0])
 @pytest.mark.parametrize("prec,tol", [("F32", 1e-5), ("F16S", 3e-2)])
-def test_reduced_precision_velocity_error(clb, oracle, prec, tol):
+def test_reduced_precision_velocity_error(clb, oracle, prec, tol, even_tma):
     shape = (26, 14, 14)
     mat = mixed_geometry(*shape, seed=9)
-    D, O = make_pair(clb, oracle, mat, shape, 0.8, 1e-4, getattr(clb, prec), **BIO)
+    D, O = make_pair(clb, oracle, mat, shape, 0.8, 1e-4, getattr(clb, prec), even_tma=even_tma, **BIO)
     D.flow_step(400)
     O.step(400)
     err = rel_l2(D.velocity(), O.velocity())
@@ -85,3 +88,22 @@ def test_flow_step_before_init_is_an_error(clb):
     with pytest.raises(clb.ClbError) as e:
         D.flow_step(1)
     assert e.value.status == 7
+
+
+def test_autotune_leaves_state_unchanged(clb, oracle):
+    shape = (30, 16, 20)
+    mat = mixed_geometry(*shape, seed=11)
+    D, O = make_pair(clb, oracle, mat, shape, 0.8, 2e-4, clb.F64, **BIO)
+    D.flow_step(7)
+    O.step(7)
+    rep = D.autotune(4)
+    assert "->" in rep and "tma=" in rep
+    D.flow_step(5)
+    O.step(5)
+    fluid = mat != 1
+    assert np.max(np.abs(D.flow_populations()[:, fluid] - O.populations()[:, fluid])) < 1e-13
+    D.tune("flow_min_blocks", 2)
+    with pytest.raises(clb.ClbError):
+        D.tune("flow_min_blocks", 5)
+    with pytest.raises(clb.ClbError):
+        D.tune("no_such_knob", 1)
