@@ -27,6 +27,8 @@ STATUS = {0: "OK", 1: "INVALID_ARG", 2: "NOT_CONVERGED", 3: "NONFINITE", 4: "PER
           5: "CUDA_ERROR", 6: "TIMEOUT", 7: "NOT_INITIALIZED", 8: "OUT_OF_MEMORY"}
 
 MAX_MICROBES, MAX_PORE_CODES, MAX_SPECIES = 8, 8, 16
+MAX_EQ_SPECIES, MAX_COMPONENTS = 16, 8
+SPEC_OFF, SPEC_NR, SPEC_MLP, SPEC_MLP_NR = 0, 1, 2, 3
 
 
 class DomainDesc(C.Structure):
@@ -69,6 +71,29 @@ class Inspection(C.Structure):
                 ("quasi_2d", C.c_int32)]
 
 
+class SpeciationDesc(C.Structure):
+    _fields_ = [("n_species", C.c_int32), ("n_components", C.c_int32),
+                ("stoich", (C.c_double * MAX_COMPONENTS) * MAX_EQ_SPECIES), ("logK", C.c_double * MAX_EQ_SPECIES),
+                ("component_species", C.c_int32 * MAX_COMPONENTS), ("tolerance", C.c_double),
+                ("max_iterations", C.c_int32)]
+
+
+class SpeciationStats(C.Structure):
+    _fields_ = [("solves", C.c_int64), ("converged", C.c_int64), ("surrogate_used", C.c_int64),
+                ("fallbacks", C.c_int64), ("iterations", C.c_int64)]
+
+
+class SurrogateTrainDesc(C.Structure):
+    _fields_ = [("n_samples", C.c_int32), ("epochs", C.c_int32), ("batch", C.c_int32), ("patience", C.c_int32),
+                ("learning_rate", C.c_double), ("val_fraction", C.c_double), ("seed", C.c_uint64),
+                ("log_c_lo", C.c_double * MAX_EQ_SPECIES), ("log_c_hi", C.c_double * MAX_EQ_SPECIES)]
+
+
+class SurrogateReport(C.Structure):
+    _fields_ = [("train_mse", C.c_double), ("val_mse", C.c_double), ("seconds", C.c_double),
+                ("epochs", C.c_int32), ("steps", C.c_int32), ("n_train", C.c_int32), ("n_val", C.c_int32)]
+
+
 # every symbol include/clb.h declares, with its argument types
 SIGNATURES = {
     "clb_set_device": [C.c_int],
@@ -93,6 +118,16 @@ SIGNATURES = {
     "clb_set_biomass": [C.c_void_p, C.c_int, C.c_void_p],
     "clb_ade_step": [C.c_void_p, C.c_int],
     "clb_reduce": [C.c_void_p, C.POINTER(Stats)],
+    "clb_speciation_setup": [C.c_void_p, C.POINTER(SpeciationDesc)],
+    "clb_set_speciation_mode": [C.c_void_p, C.c_int],
+    "clb_speciation_stats_get": [C.c_void_p, C.POINTER(SpeciationStats)],
+    "clb_speciation_solve": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
+    "clb_surrogate_train": [C.c_void_p, C.POINTER(SurrogateTrainDesc), C.POINTER(SurrogateReport)],
+    "clb_surrogate_set_check": [C.c_void_p, C.c_double, C.c_double],
+    "clb_surrogate_predict": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int],
+    "clb_surrogate_params": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "clb_surrogate_param_count": [],
+    "clb_surrogate_gradient": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
     "clb_get_field": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int],
     "clb_set_field": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int],
     "clb_geom_generate": [C.POINTER(GeomOptions), C.c_int, C.c_int, C.c_int, C.c_void_p],
@@ -323,3 +358,75 @@ class Domain:
         return {"total": np.array(s.total[:S]), "content": np.array(s.content[:S]),
                 "biomass": np.array(s.biomass[:]), "min": np.array(s.min_c[:S]), "max": np.array(s.max_c[:S]),
                 "open_voxels": s.open_voxels, "nonfinite": s.nonfinite, "ade_iterations": s.ade_iterations}
+
+    # ---- equilibrium speciation and its surrogate
+    def speciation_setup(self, stoich, logK, component_species, tol=1e-10, max_iterations=200):
+        S = np.asarray(stoich, dtype=np.float64)
+        d = SpeciationDesc()
+        d.n_species, d.n_components = S.shape
+        for i in range(S.shape[0]):
+            for j in range(S.shape[1]):
+                d.stoich[i][j] = S[i, j]
+            d.logK[i] = float(logK[i])
+        for j, cs in enumerate(component_species):
+            d.component_species[j] = int(cs)
+        d.tolerance, d.max_iterations = tol, max_iterations
+        self.eq_ns = S.shape[0]
+        self._check(lib().clb_speciation_setup(self.h, C.byref(d)))
+
+    def set_speciation_mode(self, mode):
+        self._check(lib().clb_set_speciation_mode(self.h, mode))
+
+    def speciation_stats(self):
+        s = SpeciationStats()
+        self._check(lib().clb_speciation_stats_get(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in SpeciationStats._fields_}
+
+    def speciation_solve(self, conc):
+        c = np.ascontiguousarray(conc, dtype=np.float64)
+        n = c.shape[0]
+        out = np.empty_like(c)
+        it = np.empty(n, dtype=np.int32)
+        self._check(lib().clb_speciation_solve(self.h, _ptr(c), n, _ptr(out), _ptr(it)))
+        return out, it
+
+    def surrogate_train(self, log_c_lo, log_c_hi, n_samples=100000, epochs=30, batch=4096, patience=5,
+                        learning_rate=2e-3, val_fraction=0.15, seed=1):
+        d = SurrogateTrainDesc()
+        d.n_samples, d.epochs, d.batch, d.patience = n_samples, epochs, batch, patience
+        d.learning_rate, d.val_fraction, d.seed = learning_rate, val_fraction, seed
+        for i, (lo, hi) in enumerate(zip(log_c_lo, log_c_hi)):
+            d.log_c_lo[i], d.log_c_hi[i] = lo, hi
+        r = SurrogateReport()
+        self._check(lib().clb_surrogate_train(self.h, C.byref(d), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in SurrogateReport._fields_}
+
+    def surrogate_set_check(self, range_margin=0.02, residual_tol=1e-3):
+        self._check(lib().clb_surrogate_set_check(self.h, range_margin, residual_tol))
+
+    def surrogate_predict(self, conc, residual_check=True):
+        c = np.ascontiguousarray(conc, dtype=np.float64)
+        n = c.shape[0]
+        out = np.empty_like(c)
+        acc = np.empty(n, dtype=np.int32)
+        self._check(lib().clb_surrogate_predict(self.h, _ptr(c), n, _ptr(out), _ptr(acc), int(residual_check)))
+        return out, acc.astype(bool)
+
+    def surrogate_params(self, params=None, scaling=None):
+        n = lib().clb_surrogate_param_count()
+        out = np.empty(n, dtype=np.float32)
+        sc = np.empty(64, dtype=np.float32)
+        pin = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        sin = None if scaling is None else np.ascontiguousarray(scaling, dtype=np.float32)
+        self._check(lib().clb_surrogate_params(self.h, _ptr(out), None if pin is None else _ptr(pin), _ptr(sc),
+                                               None if sin is None else _ptr(sin)))
+        return out, sc
+
+    def surrogate_gradient(self, X, Y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        n = X.shape[0]
+        g = np.empty(lib().clb_surrogate_param_count(), dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        self._check(lib().clb_surrogate_gradient(self.h, _ptr(X), _ptr(Y), n, _ptr(g), _ptr(loss)))
+        return g, float(loss[0])

@@ -667,6 +667,10 @@ clb_status ade_step(clb_handle* h, int n) {
             default: if (odd) launch_ade_t<__half, float, true>(h); else launch_ade_t<__half, float, false>(h); break;
         }
         h->ade_iters += 1;
+        if (h->spec_mode != CLB_SPEC_OFF) {
+            clb_status st = speciation_step(h);
+            if (st != CLB_OK) return st;
+        }
     }
     return cuda_check(h, cudaGetLastError(), "ade step");
 }

@@ -94,6 +94,9 @@ clb_status clb_destroy(clb_handle* h) {
     ade_free(h);
     cudaFree(h->d_mat);
     cudaFree(h->d_err);
+    cudaFree(h->d_spec_stats);
+    cudaFree(h->d_mlp);
+    cudaFree(h->d_mlp_bf16);
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
     return CLB_OK;
@@ -249,6 +252,71 @@ clb_status clb_reduce(clb_handle* h, clb_stats* out) {
     if (!h || !out) return fail(h, CLB_INVALID_ARG, "null argument");
     CLB_ON_DEVICE(h);
     return ade_reduce(h, out);
+}
+
+clb_status clb_speciation_setup(clb_handle* h, const clb_speciation_desc* desc) {
+    if (!h || !desc) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return speciation_setup(h, desc);
+}
+
+clb_status clb_set_speciation_mode(clb_handle* h, int mode) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    if (mode < CLB_SPEC_OFF || mode > CLB_SPEC_MLP_NR) return fail(h, CLB_INVALID_ARG, "unknown speciation mode");
+    if (mode != CLB_SPEC_OFF && !h->spec_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_speciation_setup first");
+    if ((mode == CLB_SPEC_MLP || mode == CLB_SPEC_MLP_NR) && !h->mlp_ready)
+        return fail(h, CLB_NOT_INITIALIZED, "train or load the surrogate first");
+    h->spec_mode = mode;
+    return CLB_OK;
+}
+
+clb_status clb_speciation_stats_get(clb_handle* h, clb_speciation_stats* out) {
+    if (!h || !out) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return speciation_stats(h, out);
+}
+
+clb_status clb_speciation_solve(clb_handle* h, const double* conc_in, int n, double* conc_out, int* iterations) {
+    if (!h || (n > 0 && (!conc_in || !conc_out))) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return speciation_solve(h, conc_in, n, conc_out, iterations);
+}
+
+clb_status clb_surrogate_train(clb_handle* h, const clb_surrogate_train_desc* desc, clb_surrogate_report* out) {
+    if (!h || !desc) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return surrogate_train(h, desc, out);
+}
+
+clb_status clb_surrogate_set_check(clb_handle* h, double range_margin, double residual_tol) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    if (!(range_margin >= 0) || !(residual_tol > 0)) return fail(h, CLB_INVALID_ARG, "bad acceptance settings");
+    h->mlp_margin = (float)range_margin;
+    h->mlp_resid_tol = (float)residual_tol;
+    return CLB_OK;
+}
+
+clb_status clb_surrogate_predict(clb_handle* h, const double* conc_in, int n, double* conc_out, int* accepted,
+                                 int residual_check) {
+    if (!h || (n > 0 && (!conc_in || !conc_out))) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return surrogate_predict(h, conc_in, n, conc_out, accepted, residual_check);
+}
+
+clb_status clb_surrogate_params(clb_handle* h, float* params_out, const float* params_in, float* scaling_out,
+                                const float* scaling_in) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    if (!h->spec_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_speciation_setup first");
+    return surrogate_params(h, params_out, params_in, scaling_out, scaling_in);
+}
+
+int clb_surrogate_param_count(void) { return surrogate_param_count(); }
+
+clb_status clb_surrogate_gradient(clb_handle* h, const float* X, const float* Y, int n, float* grad, float* loss) {
+    if (!h || !X || !Y || !grad || !loss || n < 1) return fail(h, CLB_INVALID_ARG, "bad arguments");
+    CLB_ON_DEVICE(h);
+    return surrogate_gradient(h, X, Y, n, grad, loss);
 }
 
 clb_status clb_get_field(clb_handle* h, int field, int index, void* host, int dtype) {

@@ -193,6 +193,16 @@ struct clb_handle_s {
     clb::AdeParams ap;
     int64_t ade_iters = 0;
     int ade_grid = 0;
+
+    // speciation (SpecParams lives in speciation.cuh; kept as raw storage here)
+    alignas(16) unsigned char sp_storage[2048];
+    bool spec_ready = false;
+    int spec_mode = 0;
+    unsigned long long* d_spec_stats = nullptr;
+    float* d_mlp = nullptr;             // params, Adam m, v, grad, scaling
+    void* d_mlp_bf16 = nullptr;         // BF16 operand copies of W1, W2, W3
+    bool mlp_ready = false;
+    float mlp_margin = 0.02f, mlp_resid_tol = 1e-3f;
 };
 
 namespace clb {
@@ -227,6 +237,18 @@ clb_status ade_set_velocity(clb_handle* h, const double* host);
 clb_status ade_set_biomass_field(clb_handle* h, int m, const double* host);
 clb_status ade_reduce(clb_handle* h, clb_stats* out);
 void ade_free(clb_handle* h);
+
+// speciation.cu
+clb_status speciation_setup(clb_handle* h, const clb_speciation_desc* d);
+clb_status speciation_step(clb_handle* h);
+clb_status speciation_solve(clb_handle* h, const double* cin, int n, double* cout, int* iters);
+clb_status speciation_solve_device(clb_handle* h, const double* d_in, int n, double* d_out);
+clb_status speciation_stats(clb_handle* h, clb_speciation_stats* out);
+clb_status surrogate_train(clb_handle* h, const clb_surrogate_train_desc* d, clb_surrogate_report* rep);
+clb_status surrogate_predict(clb_handle* h, const double* cin, int n, double* cout, int* accepted, int check);
+clb_status surrogate_gradient(clb_handle* h, const float* X, const float* Y, int n, float* grad, float* loss);
+clb_status surrogate_params(clb_handle* h, float* out, const float* in, float* scaling_out, const float* scaling_in);
+int surrogate_param_count();
 
 // list building (api.cu)
 std::vector<int32_t> build_list(const clb_handle* h, const int8_t* cls_by_code);

@@ -149,14 +149,13 @@ __device__ void finish_step(Tracer* tr, double* partials, double block_total, in
     double v = 0;
     for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) v += ((volatile double*)partials)[k];
     double tot = block_sum(v, sh);
-    __shared__ double s_energy, s_mean;
+    __shared__ double s_mean;
     __shared__ int s_count;
     if (threadIdx.x == 0) {
         double e = n_bgk > 0 ? 0.5 * tot / (double)n_bgk : 0.0;
         tr->energy = e;
         tr->iterations += 1;
         tr->done_blocks = 0;
-        s_energy = e;
         s_count = 0;
         if (trace) {
             tr->ring[tr->head] = e;
@@ -183,7 +182,6 @@ __device__ void finish_step(Tracer* tr, double* partials, double block_total, in
         double r = sd / s_mean;
         if (isnan(r) || fabs(r) < tr->eps) tr->converged = 1;
     }
-    (void)s_energy;
 }
 
 

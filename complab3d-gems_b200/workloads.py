@@ -86,3 +86,38 @@ def config3(scale=1, seed=1003):
                 delta_p=1e-4, eps=1e-6, species=species, law=clb.LAW_DUAL_MONOD,
                 params=[1e-4, 0.1, 0.4, 1e-6], dt=1.0, biomass=bio, bio_codes=(3, 4), perm_ratio=(0.1, 0.1),
                 bmax=100.0)
+
+
+def carbonate_tableau():
+    """The two-component carbonate tableau of the reference's equilibrium example
+    (examples/04_equilibrium/CompLaB.xml): HCO3 and H are components; CO3 = HCO3 - H
+    (log K -10.33), H2CO3 = HCO3 + H (log K 6.35)."""
+    S = np.array([[1, 0], [0, 1], [1, -1], [1, 1]], dtype=np.float64)
+    logK = np.array([0.0, 0.0, -10.33, 6.35])
+    return S, logK, [0, 1]
+
+
+def tableau_5x12(seed=1004):
+    """A 5-component, 12-species carbonate-like tableau: species 0..4 are the components
+    (component 0 plays H+), species 5..11 complexes of one or two components with an H+
+    coefficient in {-1, 0, 1}; log K drawn uniformly from [-12, 2] with a seeded generator."""
+    rng = np.random.default_rng(seed)
+    S = np.zeros((12, 5))
+    S[:5, :5] = np.eye(5)
+    logK = np.zeros(12)
+    for k in range(5, 12):
+        p = rng.integers(1, 5)
+        S[k, p] = 1.0
+        if rng.random() < 0.5:
+            q = rng.integers(1, 5)
+            if q != p:
+                S[k, q] = 1.0
+        S[k, 0] = float(rng.integers(-1, 2))
+        logK[k] = rng.uniform(-12.0, 2.0)
+    return S, logK, [0, 1, 2, 3, 4]
+
+
+def species_states(n, ns, lo, hi, seed):
+    """n species states with log10 c uniform in [lo, hi] per species."""
+    rng = np.random.default_rng(seed)
+    return 10.0 ** rng.uniform(lo, hi, size=(n, ns))

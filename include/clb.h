@@ -209,6 +209,93 @@ clb_status clb_ade_step(clb_handle* h, int n);
 /* FP64 reductions over the live fields (complab3d_processors_part3.hh:387-600). */
 clb_status clb_reduce(clb_handle* h, clb_stats* out);
 
+/* ---------------------------------------------------------------- equilibrium speciation */
+
+#define CLB_MAX_EQ_SPECIES 16
+#define CLB_MAX_COMPONENTS 8
+
+/* The <equilibrium> block of CompLaB.xml: tableau rows are the handle's species 0..n_species-1
+ * (user order), columns the components (complab.cpp:614-723). */
+typedef struct clb_speciation_desc {
+    int32_t n_species, n_components;
+    double stoich[CLB_MAX_EQ_SPECIES][CLB_MAX_COMPONENTS];
+    double logK[CLB_MAX_EQ_SPECIES];
+    int32_t component_species[CLB_MAX_COMPONENTS]; /* species that is each component, -1 none */
+    double tolerance;             /* Newton-Raphson: |S^T c - T|_2 below this (absolute)      */
+    int32_t max_iterations;
+} clb_speciation_desc;
+
+typedef enum clb_speciation_mode {
+    CLB_SPEC_OFF = 0,
+    CLB_SPEC_NR = 1,              /* FP64 Newton-Raphson in log10 concentration              */
+    CLB_SPEC_MLP = 2,             /* trained surrogate only                                   */
+    CLB_SPEC_MLP_NR = 3           /* surrogate, Newton-Raphson where the input is outside the
+                                     trained range or the surrogate's residual check fails    */
+} clb_speciation_mode;
+
+typedef struct clb_speciation_stats {
+    int64_t solves, converged, surrogate_used, fallbacks, iterations;
+} clb_speciation_stats;
+
+/* Replaces: EquilibriumChemistry configuration (complab.cpp:614-723). */
+clb_status clb_speciation_setup(clb_handle* h, const clb_speciation_desc* desc);
+
+/* Runs the speciation step inside every later clb_ade_step, after the kinetics and before the
+ * stream, as run_equilibrium_biotic does (complab3d_processors_part4_eqsolver.hh:1393-1545:
+ * x = 1..nx-2, mask neither solid nor wall, dC capped at max(1e-9, 0.1 |C|), floored at 1e-20). */
+clb_status clb_set_speciation_mode(clb_handle* h, int mode);
+clb_status clb_speciation_stats_get(clb_handle* h, clb_speciation_stats* out);
+
+/* Solves n independent tableau problems: conc_in [n][n_species] (host), conc_out likewise,
+ * iterations [n] (may be NULL). Replaces: EquilibriumChemistry::calculate_species_concentrations
+ * (complab3d_processors_part4_eqsolver.hh:1195-1215), here by Newton-Raphson on the GPU. */
+clb_status clb_speciation_solve(clb_handle* h, const double* conc_in, int n, double* conc_out, int* iterations);
+
+/* ---------------------------------------------------------------- speciation surrogate */
+
+/* The surrogate replaces the per-voxel Newton-Raphson solve: n_components log10 totals in, two
+ * hidden layers of 64 tanh units, n_species log10 concentrations out, mapminmax scaling of
+ * inputs and outputs (the recipe of the reference's FBA surrogate, complab3d_surrogate.hh:117-258
+ * evalAll and :660-806 fitNetwork: Adam, held-out early stopping). Training data are Newton-
+ * Raphson solves made on the GPU from species states with log10 c uniform in
+ * [log_c_lo, log_c_hi]. Forward passes run on the tensor cores (BF16 operands, FP32 accumulate);
+ * the backward pass and the Adam update are FP32. */
+typedef struct clb_surrogate_train_desc {
+    int32_t n_samples, epochs, batch, patience;
+    double learning_rate, val_fraction;
+    uint64_t seed;
+    double log_c_lo[CLB_MAX_EQ_SPECIES], log_c_hi[CLB_MAX_EQ_SPECIES];
+} clb_surrogate_train_desc;
+
+typedef struct clb_surrogate_report {
+    double train_mse, val_mse, seconds;  /* mean squared error on the scaled outputs            */
+    int32_t epochs, steps, n_train, n_val;
+} clb_surrogate_report;
+
+clb_status clb_surrogate_train(clb_handle* h, const clb_surrogate_train_desc* desc, clb_surrogate_report* out);
+
+/* Acceptance of a surrogate answer inside the speciation step: every scaled input within
+ * 1 + range_margin of the trained range, and (mode CLB_SPEC_MLP_NR) the relative mass-balance
+ * residual max_j |S^T c - T|_j / T_j at most residual_tol. Defaults 0.02 and 1e-3. */
+clb_status clb_surrogate_set_check(clb_handle* h, double range_margin, double residual_tol);
+
+/* Surrogate speciation of n states ([n][n_species] host arrays); accepted[n] (may be NULL)
+ * reports the acceptance test (with the residual check when residual_check != 0). */
+clb_status clb_surrogate_predict(clb_handle* h, const double* conc_in, int n, double* conc_out, int* accepted,
+                                 int residual_check);
+
+/* Parameter blob (clb_surrogate_param_count() floats: W1[64][16], b1[64], W2[64][64], b2[64],
+ * W3[16][64], b3[16]) and the 64-float scaling block (input lo[16], hi[16], output lo[16],
+ * hi[16]); either pointer pair may be NULL. Setting parameters makes the surrogate usable. */
+clb_status clb_surrogate_params(clb_handle* h, float* params_out, const float* params_in, float* scaling_out,
+                                const float* scaling_in);
+int clb_surrogate_param_count(void);
+
+/* Loss (sum of squared errors over the n x n_species scaled outputs) and its gradient with
+ * respect to the parameter blob, for scaled inputs X[n][16] and targets Y[n][16], computed by
+ * the training kernels themselves (gradient of the mean: the blob is scaled by 1/(n n_species)). */
+clb_status clb_surrogate_gradient(clb_handle* h, const float* X, const float* Y, int n, float* grad, float* loss);
+
 /* ---------------------------------------------------------------- fields */
 
 clb_status clb_get_field(clb_handle* h, int field, int index, void* host, int dtype);

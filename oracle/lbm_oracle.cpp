@@ -362,6 +362,7 @@ struct OrcAde {
     std::vector<double> prm;
     double dt = 1.0;
     long iters = 0;
+    void* spec = nullptr;  // EqTableau of the speciation step, or none
     size_t id(int x, int y, int z) const { return ((size_t)x * ny + y) * nz + z; }
     // the lattice dynamics of species s at node n
     int node_dyn(int s, int x, size_t n) const {
@@ -466,6 +467,8 @@ static void rates(const OrcAde* A, const double* C, const double* B, double* R, 
     }
 }
 
+static void apply_speciation(OrcAde* A);
+
 static void ade_step(OrcAde* A) {
     const int nx = A->nx, ny = A->ny, nz = A->nz, S = A->S;
     const size_t N = A->N, P = (size_t)ny * nz;
@@ -553,6 +556,8 @@ static void ade_step(OrcAde* A) {
                 }
         }
     }
+    // ---- speciation on the post-kinetics populations (complab.cpp:2564-2569)
+    if (A->spec) apply_speciation(A);
     // ---- 3. stream, then the Neumann planes take the inner neighbour's density
     for (int s = 0; s < S; ++s) {
         if (!A->mobile[s]) continue;
@@ -631,3 +636,214 @@ void orc_ade_biomass(OrcAde* A, double* out) {
 void orc_ade_set_velocity(OrcAde* A, const double* u) { A->u.assign(u, u + 3 * A->N); }
 
 }  // extern "C"
+
+// =====================================================================================
+//                     EQUILIBRIUM SPECIATION (Newton-Raphson in log10)
+// =====================================================================================
+// Restates the reference's Newton-Raphson reserve solver
+// (complab3d_processors_part4_eqsolver_NR_reserve.hh: calc_residual :309-328, calc_jacobian
+// :356-375, partial-pivot Gaussian elimination :377-440 with singular threshold 1e-30,
+// solve_equilibrium_NR :512-640 with Armijo backtracking of at most 40 halvings) on the species
+// model of the active solver (complab3d_processors_part4_eqsolver.hh: calc_species :450-505 with
+// log10 c clamped to [-30, 1] and c to [1e-30, 10], calc_component_totals :520-535,
+// isEquilibriumSpecies :386-395), and the speciation step run_equilibrium_biotic (:1393-1545):
+// x = 1..nx-2, mask neither solid nor wall, dC capped at max(1e-9, 0.1 |C|), the new
+// concentration floored at 1e-20, deposited as t_i dC when |dC| > 1e-12.
+namespace {
+const double EQ_MIN_C = 1e-30, EQ_MAX_C = 10.0, EQ_MIN_LOG = -30.0, EQ_MAX_LOG = 1.0;
+// Two departures from the reserve solver, both for robustness from a far initial guess: inside
+// the Newton loop the species are taken without the [1e-30, 10] clamps (a species saturated at the
+// clamp has a zero derivative the Jacobian does not see, and the iteration stalls); the clamps
+// apply to the answer only. And no log10 component concentration moves by more than EQ_MAX_STEP
+// in one step.
+const double EQ_MAX_STEP = 2.0;
+
+struct EqTableau {
+    int ns = 0, nc = 0;
+    std::vector<double> S, logK;  // S[i*nc + j]
+    std::vector<int> comp;        // species index of component j or -1
+    double tol = 1e-10;
+    int max_it = 200;
+    bool eq_species(int i) const {
+        for (int j = 0; j < nc; ++j) if (std::fabs(S[i * nc + j]) > 1e-10) return true;
+        return false;
+    }
+};
+
+void eq_species_conc(const EqTableau& t, const double* x, const double* init, double* c) {
+    for (int i = 0; i < t.ns; ++i) {
+        if (!t.eq_species(i)) {
+            c[i] = init[i] > EQ_MIN_C ? std::min(init[i], EQ_MAX_C) : EQ_MIN_C;
+            continue;
+        }
+        double lc = t.logK[i];
+        for (int j = 0; j < t.nc; ++j) lc += t.S[i * t.nc + j] * x[j];
+        lc = std::max(std::min(lc, EQ_MAX_LOG), EQ_MIN_LOG);
+        double v = std::pow(10.0, lc);
+        if (std::isnan(v) || std::isinf(v)) v = init[i] > EQ_MIN_C ? init[i] : EQ_MIN_C;
+        c[i] = std::max(std::min(v, EQ_MAX_C), EQ_MIN_C);
+    }
+}
+
+// species inside the Newton loop: mass action without the concentration clamps
+void eq_species_free(const EqTableau& t, const double* x, const double* init, double* c) {
+    for (int i = 0; i < t.ns; ++i) {
+        if (!t.eq_species(i)) {
+            c[i] = init[i] > EQ_MIN_C ? std::min(init[i], EQ_MAX_C) : EQ_MIN_C;
+            continue;
+        }
+        double lc = t.logK[i];
+        for (int j = 0; j < t.nc; ++j) lc += t.S[i * t.nc + j] * x[j];
+        c[i] = std::pow(10.0, std::max(std::min(lc, 300.0), -300.0));
+    }
+}
+
+double eq_residual(const EqTableau& t, const double* x, const double* Ttot, const double* init, double* F) {
+    double c[64];
+    eq_species_free(t, x, init, c);
+    double s = 0;
+    for (int j = 0; j < t.nc; ++j) {
+        double v = -Ttot[j];
+        for (int i = 0; i < t.ns; ++i)
+            if (t.eq_species(i)) v += t.S[i * t.nc + j] * c[i];
+        F[j] = v;
+        s += v * v;
+    }
+    return std::sqrt(s);
+}
+
+// returns iterations; *conv set
+int eq_solve_nr(const EqTableau& t, const double* init, double* out, int* conv) {
+    const int nc = t.nc, ns = t.ns;
+    double Ttot[16], x[16], F[16], Fn[16], xn[16], d[16], A[16][17];
+    *conv = 0;
+    for (int j = 0; j < nc; ++j) {
+        double v = 0;
+        for (int i = 0; i < ns; ++i)
+            if (t.eq_species(i)) v += t.S[i * nc + j] * std::max(std::min(init[i], EQ_MAX_C), EQ_MIN_C);
+        Ttot[j] = std::max(v, EQ_MIN_C);
+        double cc = t.comp[j] >= 0 ? init[t.comp[j]] : 1e-7;
+        x[j] = std::log10(std::max(std::min(cc, EQ_MAX_C), EQ_MIN_C));
+    }
+    int it = 0;
+    for (; it < t.max_it; ++it) {
+        double fn = eq_residual(t, x, Ttot, init, F);
+        if (fn < t.tol) { *conv = 1; ++it; break; }
+        double c[64];
+        eq_species_free(t, x, init, c);
+        const double ln10 = std::log(10.0);
+        for (int j = 0; j < nc; ++j) {
+            for (int k = 0; k < nc; ++k) {
+                double v = 0;
+                for (int i = 0; i < ns; ++i)
+                    if (t.eq_species(i)) v += ln10 * t.S[i * nc + j] * t.S[i * nc + k] * c[i];
+                A[j][k] = v;
+            }
+            A[j][nc] = -F[j];
+        }
+        bool ok = true;
+        for (int p = 0; p < nc && ok; ++p) {
+            int r = p;
+            double mv = std::fabs(A[p][p]);
+            for (int q = p + 1; q < nc; ++q) if (std::fabs(A[q][p]) > mv) { mv = std::fabs(A[q][p]); r = q; }
+            if (mv < 1e-30) { ok = false; break; }
+            if (r != p) for (int q = 0; q <= nc; ++q) std::swap(A[p][q], A[r][q]);
+            for (int q = p + 1; q < nc; ++q) {
+                double fct = A[q][p] / A[p][p];
+                for (int m = p; m <= nc; ++m) A[q][m] -= fct * A[p][m];
+            }
+        }
+        if (!ok) { ++it; break; }
+        for (int p = nc - 1; p >= 0; --p) {
+            double v = A[p][nc];
+            for (int q = p + 1; q < nc; ++q) v -= A[p][q] * d[q];
+            d[p] = v / A[p][p];
+        }
+        // step limit: no log10 concentration moves by more than EQ_MAX_STEP in one iteration
+        double dmax = 0;
+        for (int j = 0; j < nc; ++j) dmax = std::max(dmax, std::fabs(d[j]));
+        if (dmax > EQ_MAX_STEP)
+            for (int j = 0; j < nc; ++j) d[j] *= EQ_MAX_STEP / dmax;
+        double alpha = 1.0, fnew = 0;
+        for (int ls = 0; ls < 40; ++ls) {
+            for (int j = 0; j < nc; ++j) xn[j] = std::max(std::min(x[j] + alpha * d[j], EQ_MAX_LOG), EQ_MIN_LOG);
+            fnew = eq_residual(t, xn, Ttot, init, Fn);
+            if (fnew < fn * (1.0 - 0.0001 * alpha) || alpha < 1e-15) break;
+            alpha *= 0.5;
+        }
+        for (int j = 0; j < nc; ++j) x[j] = xn[j];
+        double dn = 0;
+        for (int j = 0; j < nc; ++j) dn += d[j] * d[j];
+        if (alpha * std::sqrt(dn) < t.tol * 1e-3 && fnew < t.tol * 100) { *conv = 1; ++it; break; }
+    }
+    eq_species_conc(t, x, init, out);
+    for (int i = 0; i < ns; ++i) {
+        if (std::isnan(out[i]) || std::isinf(out[i])) out[i] = init[i] > EQ_MIN_C ? std::min(init[i], EQ_MAX_C) : EQ_MIN_C;
+        out[i] = std::max(std::min(out[i], EQ_MAX_C), EQ_MIN_C);
+    }
+    return it;
+}
+}  // namespace
+
+extern "C" int orc_eq_nr(int ns, int nc, const double* stoich, const double* logK, const int* comp, double tol,
+                         int max_it, const double* cin, double* cout, int* conv) {
+    EqTableau t;
+    t.ns = ns; t.nc = nc;
+    t.S.assign(stoich, stoich + ns * nc);
+    t.logK.assign(logK, logK + ns);
+    t.comp.assign(comp, comp + nc);
+    t.tol = tol;
+    t.max_it = max_it;
+    return eq_solve_nr(t, cin, cout, conv);
+}
+
+static void apply_speciation(OrcAde* A) {
+    const EqTableau& t = *static_cast<const EqTableau*>(A->spec);
+    const int nx = A->nx, ny = A->ny, nz = A->nz, ns = t.ns;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int x = 1; x < nx - 1; ++x) {
+        double c[64], e[64];
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = A->id(x, y, z);
+                if (!A->react[(uint8_t)A->mat[n]]) continue;
+                for (int s = 0; s < ns; ++s) {
+                    double v;
+                    if (A->mobile[s]) {
+                        v = 1.0;
+                        for (int i = 0; i < Q7; ++i) v += A->gp[s][n * Q7 + i];
+                    } else {
+                        v = A->imm[s][n];
+                    }
+                    c[s] = std::max(v, EQ_MIN_C);
+                }
+                int conv;
+                eq_solve_nr(t, c, e, &conv);
+                for (int s = 0; s < ns; ++s) {
+                    double dC = e[s] - c[s];
+                    const double cap = std::max(1e-9, 0.1 * std::fabs(c[s]));
+                    if (std::fabs(dC) > cap) dC = dC > 0 ? cap : -cap;
+                    if (c[s] + dC < 1e-20) dC = 1e-20 - c[s];
+                    if (!(std::fabs(dC) > THRD)) continue;
+                    if (A->mobile[s]) {
+                        for (int i = 0; i < Q7; ++i) A->gp[s][n * Q7 + i] += dC * T7[i];
+                    } else {
+                        A->imm[s][n] += dC;
+                    }
+                }
+            }
+    }
+}
+
+extern "C" void orc_ade_set_speciation(OrcAde* A, int ns, int nc, const double* stoich, const double* logK,
+                                       const int* comp, double tol, int max_it) {
+    if (A->spec) delete static_cast<EqTableau*>(A->spec);
+    EqTableau* t = new EqTableau();
+    t->ns = ns; t->nc = nc;
+    t->S.assign(stoich, stoich + ns * nc);
+    t->logK.assign(logK, logK + ns);
+    t->comp.assign(comp, comp + nc);
+    t->tol = tol;
+    t->max_it = max_it;
+    A->spec = t;
+}

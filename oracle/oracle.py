@@ -52,6 +52,8 @@ def lib():
             "orc_ade_set_biomass": ([vp, ip, vp], None), "orc_ade_step": ([vp, ip], None),
             "orc_ade_density": ([vp, ip, vp], None), "orc_ade_populations": ([vp, ip, vp], None),
             "orc_ade_biomass": ([vp, vp], None), "orc_ade_set_velocity": ([vp, vp], None),
+            "orc_eq_nr": ([ip, ip, vp, vp, vp, dp, ip, vp, vp, vp], ip),
+            "orc_ade_set_speciation": ([vp, ip, ip, vp, vp, vp, dp, ip], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -71,6 +73,25 @@ def set_threads(n):
 
 def max_threads():
     return lib().orc_max_threads()
+
+
+def eq_nr(stoich, logK, comp, conc, tol=1e-10, max_it=200):
+    """Newton-Raphson speciation of each row of conc (the oracle's restatement)."""
+    S = np.ascontiguousarray(stoich, dtype=np.float64)
+    lk = np.ascontiguousarray(logK, dtype=np.float64)
+    cp = np.ascontiguousarray(comp, dtype=np.int32)
+    conc = np.atleast_2d(np.asarray(conc, dtype=np.float64))
+    out = np.empty_like(conc)
+    conv = np.empty(conc.shape[0], dtype=np.int32)
+    its = np.empty(conc.shape[0], dtype=np.int32)
+    cv = C.c_int()
+    for r in range(conc.shape[0]):
+        ci = np.ascontiguousarray(conc[r])
+        o = np.empty(S.shape[0])
+        its[r] = lib().orc_eq_nr(S.shape[0], S.shape[1], _p(S), _p(lk), _p(cp), tol, max_it, _p(ci), _p(o), C.byref(cv))
+        conv[r] = cv.value
+        out[r] = o
+    return out, conv.astype(bool), its
 
 
 class OracleFlow:
@@ -163,6 +184,12 @@ class OracleAde:
         b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1)
         self.M = b.size // self.N
         lib().orc_ade_set_biomass(self.h, self.M, _p(b))
+
+    def set_speciation(self, stoich, logK, comp, tol=1e-10, max_it=200):
+        S = np.ascontiguousarray(stoich, dtype=np.float64)
+        self._spec = [S, np.ascontiguousarray(logK, dtype=np.float64), np.ascontiguousarray(comp, dtype=np.int32)]
+        lib().orc_ade_set_speciation(self.h, S.shape[0], S.shape[1], _p(self._spec[0]), _p(self._spec[1]),
+                                     _p(self._spec[2]), tol, max_it)
 
     def step(self, n=1):
         lib().orc_ade_step(self.h, n)

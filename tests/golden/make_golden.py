@@ -1,5 +1,7 @@
 """Regenerates tests/golden/geometry.json from the reference's own geometry generator
-(complab3d_geometry.hh, compiled into oracle/_ref/libref_geometry.so by `make -C oracle ref`).
+(complab3d_geometry.hh, compiled into oracle/_ref/libref_geometry.so by `make -C oracle ref`) and
+tests/golden/speciation.json from the reference's own equilibrium solver (EquilibriumChemistry,
+compiled into oracle/_ref/libref_eqsolver.so with the reference's tests/palabos_stub.hh).
 
 Run from the repository root in a checkout that has the reference sources:
     make -C oracle ref && python tests/golden/make_golden.py
@@ -47,7 +49,39 @@ def ref_generate(L, c):
                                                       spanning_clusters=sp.value, percolates=pe.value)
 
 
+def speciation_cases():
+    """Reference AA-PCF solutions (complab3d_processors_part4_eqsolver.hh, compiled into
+    oracle/_ref/libref_eqsolver.so) of the carbonate example tableau and the 5x12 tableau."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "complab3d-gems_b200"))
+    import workloads
+    L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_eqsolver.so"))
+    out = []
+    for name, (S, logK, comp), n, lo, hi in [
+        ("carbonate", workloads.carbonate_tableau(), 24, [-5, -9, -8, -6], [-2, -5, -4, -3]),
+        ("tableau_5x12", workloads.tableau_5x12(), 48, [-7] * 5 + [-10] * 7, [-3] * 5 + [-5] * 7),
+    ]:
+        ns, nc = S.shape
+        states = workloads.species_states(n, ns, np.array(lo), np.array(hi), seed=17)
+        res, conv, its = [], [], []
+        for c in states:
+            o = np.zeros(ns)
+            cv, it = C.c_int(), C.c_int()
+            L.ref_eq_solve(ns, nc, np.ascontiguousarray(S).ctypes.data_as(C.c_void_p),
+                           np.ascontiguousarray(logK).ctypes.data_as(C.c_void_p),
+                           np.array(comp, dtype=np.int32).ctypes.data_as(C.c_void_p), C.c_double(1e-10), 200,
+                           np.ascontiguousarray(c).ctypes.data_as(C.c_void_p), o.ctypes.data_as(C.c_void_p),
+                           C.byref(cv), C.byref(it))
+            res.append(o.tolist()); conv.append(cv.value); its.append(it.value)
+        out.append(dict(name=name, stoich=S.tolist(), logK=logK.tolist(), component_species=comp, tol=1e-10,
+                        inputs=states.tolist(), reference_outputs=res, converged=conv, iterations=its))
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "speciation.json"), "w") as f:
+        json.dump(out, f)
+    print(f"wrote {sum(len(c['inputs']) for c in out)} speciation cases")
+
+
 def main():
+    speciation_cases()
     L = C.CDLL(REF)
     out = []
     for c in CASES:

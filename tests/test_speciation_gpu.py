@@ -1,0 +1,171 @@
+"""FP64 Newton-Raphson speciation on the GPU against the oracle and the reference's own solver,
+the speciation step inside the transport step, and the BF16 surrogate (training, gradients
+against a CPU restatement, accuracy against Newton-Raphson, the gain over the solver)."""
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+
+import workloads
+from helpers import mixed_geometry
+
+pytestmark = pytest.mark.gpu
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "speciation.json")))
+
+
+def handle(clb, S, logK, comp, n_species=None, tol=1e-10, prec=None):
+    ns = S.shape[0]
+    mat = np.full(4 * 4 * 4, 2, np.int8)
+    D = clb.Domain(mat, 4, 4, 4, 0.8, ade_precision=clb.F64 if prec is None else prec)
+    D.ade_init([dict(omega_pore=1.0, c0=1e-6)] * ns)
+    D.speciation_setup(S, logK, comp, tol=tol)
+    return D
+
+
+@pytest.mark.parametrize("case", GOLD, ids=[c["name"] for c in GOLD])
+def test_gpu_nr_matches_oracle_and_reference(clb, oracle, case):
+    S = np.array(case["stoich"])
+    cin = np.array(case["inputs"])
+    D = handle(clb, S, case["logK"], case["component_species"])
+    out, its = D.speciation_solve(cin)
+    ora, conv, oits = oracle.eq_nr(S, case["logK"], case["component_species"], cin)
+    pos = (cin @ S > 0).all(axis=1)
+    np.testing.assert_allclose(out[pos], ora[pos], rtol=1e-9, atol=1e-20)
+    ref = np.array(case["reference_outputs"])
+    np.testing.assert_allclose(out[pos], ref[pos], rtol=2e-5, atol=1e-14)
+    assert np.all(np.abs(its[pos] - oits[pos]) <= 1)
+
+
+def test_speciation_step_in_transport_matches_oracle(clb, oracle):
+    S, logK, comp = workloads.carbonate_tableau()
+    shape = (14, 8, 7)
+    mat = mixed_geometry(*shape, seed=21, biofilm=False)
+    sp = [dict(omega_pore=1 / 0.9, left_type=0, right_type=1, left_bc=b, c0=c)
+          for b, c in zip([2e-3, 1e-6, 1e-5, 5e-4], [1e-4, 3e-7, 2e-6, 1e-5])]
+    rng = np.random.default_rng(3)
+    u = np.zeros((3, mat.size))
+    u[0] = 0.02 * rng.random(mat.size) * (mat == 2)
+    D = clb.Domain(mat, *shape, 0.8, ade_precision=clb.F64)
+    D.ade_init(sp)
+    D.set_velocity(u)
+    D.speciation_setup(S, logK, comp, tol=1e-10)
+    D.set_speciation_mode(clb.SPEC_NR)
+    O = oracle.OracleAde(mat, *shape, sp, u)
+    O.set_speciation(S, logK, comp, tol=1e-10)
+    D.ade_step(9)
+    O.step(9)
+    for s in range(4):
+        np.testing.assert_allclose(D.concentration(s), O.concentration(s), rtol=1e-9, atol=1e-16)
+    st = D.speciation_stats()
+    assert st["solves"] > 0 and st["converged"] == st["solves"]
+
+
+def bf16(a):
+    a = np.asarray(a, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u >> 16) & 1) + 0x7FFF
+    return (((u + r) >> 16) << 16).astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def cpu_loss_grad(p, X, Y, ns):
+    """The network's loss and parameter gradient in FP64, with the forward GEMM operands rounded
+    to BF16 as the tensor cores see them and the backward pass in full precision."""
+    W1 = p[:1024].reshape(64, 16); b1 = p[1024:1088]
+    W2 = p[1088:5184].reshape(64, 64); b2 = p[5184:5248]
+    W3 = p[5248:6272].reshape(16, 64); b3 = p[6272:6288]
+    h1 = np.tanh(bf16(X) @ bf16(W1).T + b1)
+    h2 = np.tanh(bf16(h1) @ bf16(W2).T + b2)
+    y = bf16(h2) @ bf16(W3).T + b3
+    n = X.shape[0]
+    diff = np.zeros_like(y)
+    diff[:, :ns] = y[:, :ns] - Y[:, :ns]
+    loss = np.sum(diff ** 2)
+    dy = 2 * diff / (n * ns)
+    d2 = (dy @ W3) * (1 - h2 ** 2)
+    d1 = (d2 @ W2) * (1 - h1 ** 2)
+    g = np.concatenate([(d1.T @ X).ravel(), d1.sum(0), (d2.T @ h1).ravel(), d2.sum(0), (dy.T @ h2).ravel(), dy.sum(0)])
+    return loss, g
+
+
+def test_surrogate_gradient_matches_cpu(clb):
+    S, logK, comp = workloads.tableau_5x12()
+    D = handle(clb, S, logK, comp)
+    rng = np.random.default_rng(5)
+    n_par = clb.lib().clb_surrogate_param_count()
+    p = (0.2 * rng.standard_normal(n_par)).astype(np.float32)
+    p[1024:1088] = 0.05 * rng.standard_normal(64)
+    p[np.arange(1024).reshape(64, 16)[:, 5:].ravel()] = 0.0   # inputs beyond the 5 components are padding
+    sc = np.concatenate([-np.ones(16), np.ones(16), -np.ones(16), np.ones(16)]).astype(np.float32)
+    D.surrogate_params(p, sc)
+    X = np.zeros((300, 16), np.float32)
+    X[:, :5] = rng.uniform(-1, 1, size=(300, 5))
+    Y = np.zeros((300, 16), np.float32)
+    Y[:, :12] = rng.uniform(-1, 1, size=(300, 12))
+    g, loss = D.surrogate_gradient(X, Y)
+    loss_c, g_c = cpu_loss_grad(p.astype(np.float64), X.astype(np.float64), Y.astype(np.float64), 12)
+    assert loss == pytest.approx(loss_c, rel=1e-4)
+    scale = np.abs(g_c).max()
+    assert np.max(np.abs(g - g_c)) < 2e-3 * scale
+    assert np.dot(g, g_c) / (np.linalg.norm(g) * np.linalg.norm(g_c)) > 0.99999
+
+
+@pytest.fixture(scope="module")
+def trained(clb):
+    S, logK, comp = workloads.carbonate_tableau()
+    D = handle(clb, S, logK, comp)
+    lo, hi = [-5, -9, -8, -6], [-2, -5, -4, -3]
+    rep = D.surrogate_train(lo, hi, n_samples=120000, epochs=40, batch=4096, patience=6, learning_rate=3e-3, seed=11)
+    return D, S, logK, comp, lo, hi, rep
+
+
+def test_surrogate_trains_and_matches_newton(trained, oracle):
+    D, S, logK, comp, lo, hi, rep = trained
+    print("training:", rep)
+    assert rep["val_mse"] < 2e-4
+    states = workloads.species_states(4000, 4, np.array(lo), np.array(hi), seed=99)
+    states = states[(states @ S > 0).all(axis=1)]
+    pred, acc = D.surrogate_predict(states, residual_check=False)
+    nr, _ = D.speciation_solve(states)
+    rel = np.abs(np.log10(pred) - np.log10(nr))
+    print("surrogate |dlog10 c|: median %.2e  p95 %.2e" % (np.median(rel), np.percentile(rel, 95)))
+    assert np.median(rel) < 2e-2
+    assert acc.mean() > 0.9
+
+
+def test_surrogate_gain_over_newton(trained):
+    D, S, logK, comp, lo, hi, rep = trained
+    states = workloads.species_states(400000, 4, np.array(lo), np.array(hi), seed=7)
+    D.speciation_solve(states[:1000])
+    D.surrogate_predict(states[:1000])
+    t0 = time.perf_counter(); D.speciation_solve(states); t1 = time.perf_counter()
+    D.surrogate_predict(states, residual_check=False); t2 = time.perf_counter()
+    print("Newton-Raphson %.1f ms, surrogate %.1f ms (400k states, host transfers included)"
+          % ((t1 - t0) * 1e3, (t2 - t1) * 1e3))
+    assert (t2 - t1) < (t1 - t0)
+
+
+def test_surrogate_with_fallback_in_transport(clb, oracle, trained):
+    D0, S, logK, comp, lo, hi, rep = trained
+    params, scaling = D0.surrogate_params()
+    shape = (14, 8, 7)
+    mat = mixed_geometry(*shape, seed=21, biofilm=False)
+    sp = [dict(omega_pore=1 / 0.9, left_type=0, right_type=1, left_bc=b, c0=c)
+          for b, c in zip([2e-3, 1e-6, 1e-5, 5e-4], [1e-4, 3e-7, 2e-6, 1e-5])]
+    results = {}
+    for mode in (clb.SPEC_NR, clb.SPEC_MLP_NR):
+        D = clb.Domain(mat, *shape, 0.8, ade_precision=clb.F64)
+        D.ade_init(sp)
+        D.speciation_setup(S, logK, comp, tol=1e-10)
+        D.surrogate_params(params, scaling)
+        D.surrogate_set_check(0.02, 1e-3)
+        D.set_speciation_mode(mode)
+        D.ade_step(12)
+        results[mode] = (np.array([D.concentration(s) for s in range(4)]), D.speciation_stats())
+    a, st = results[clb.SPEC_MLP_NR]
+    b, _ = results[clb.SPEC_NR]
+    print("surrogate step stats:", st)
+    assert st["surrogate_used"] + st["fallbacks"] == st["solves"]
+    open_ = (mat == 2)
+    np.testing.assert_allclose(a[:, open_], b[:, open_], rtol=5e-3)
