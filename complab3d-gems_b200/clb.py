@@ -123,7 +123,7 @@ SIGNATURES = {
     "clb_speciation_stats_get": [C.c_void_p, C.POINTER(SpeciationStats)],
     "clb_speciation_solve": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
     "clb_surrogate_train": [C.c_void_p, C.POINTER(SurrogateTrainDesc), C.POINTER(SurrogateReport)],
-    "clb_surrogate_set_check": [C.c_void_p, C.c_double, C.c_double],
+    "clb_surrogate_set_check": [C.c_void_p, C.c_double, C.c_int, C.c_double],
     "clb_surrogate_predict": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int],
     "clb_surrogate_params": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "clb_surrogate_param_count": [],
@@ -390,8 +390,8 @@ class Domain:
         self._check(lib().clb_speciation_solve(self.h, _ptr(c), n, _ptr(out), _ptr(it)))
         return out, it
 
-    def surrogate_train(self, log_c_lo, log_c_hi, n_samples=100000, epochs=30, batch=4096, patience=5,
-                        learning_rate=2e-3, val_fraction=0.15, seed=1):
+    def surrogate_train(self, log_c_lo, log_c_hi, n_samples=200000, epochs=60, batch=1024, patience=8,
+                        learning_rate=3e-3, val_fraction=0.15, seed=1):
         d = SurrogateTrainDesc()
         d.n_samples, d.epochs, d.batch, d.patience = n_samples, epochs, batch, patience
         d.learning_rate, d.val_fraction, d.seed = learning_rate, val_fraction, seed
@@ -401,8 +401,8 @@ class Domain:
         self._check(lib().clb_surrogate_train(self.h, C.byref(d), C.byref(r)))
         return {k: getattr(r, k) for k, _ in SurrogateReport._fields_}
 
-    def surrogate_set_check(self, range_margin=0.02, residual_tol=1e-3):
-        self._check(lib().clb_surrogate_set_check(self.h, range_margin, residual_tol))
+    def surrogate_set_check(self, range_margin=0.02, newton_polish=2, residual_tol=1e-6):
+        self._check(lib().clb_surrogate_set_check(self.h, range_margin, int(newton_polish), residual_tol))
 
     def surrogate_predict(self, conc, residual_check=True):
         c = np.ascontiguousarray(conc, dtype=np.float64)

@@ -288,10 +288,12 @@ clb_status clb_surrogate_train(clb_handle* h, const clb_surrogate_train_desc* de
     return surrogate_train(h, desc, out);
 }
 
-clb_status clb_surrogate_set_check(clb_handle* h, double range_margin, double residual_tol) {
+clb_status clb_surrogate_set_check(clb_handle* h, double range_margin, int newton_polish, double residual_tol) {
     if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
-    if (!(range_margin >= 0) || !(residual_tol > 0)) return fail(h, CLB_INVALID_ARG, "bad acceptance settings");
+    if (!(range_margin >= 0) || newton_polish < 0 || newton_polish > 50 || !(residual_tol > 0))
+        return fail(h, CLB_INVALID_ARG, "bad acceptance settings");
     h->mlp_margin = (float)range_margin;
+    h->mlp_polish = newton_polish;
     h->mlp_resid_tol = (float)residual_tol;
     return CLB_OK;
 }

@@ -202,7 +202,8 @@ struct clb_handle_s {
     float* d_mlp = nullptr;             // params, Adam m, v, grad, scaling
     void* d_mlp_bf16 = nullptr;         // BF16 operand copies of W1, W2, W3
     bool mlp_ready = false;
-    float mlp_margin = 0.02f, mlp_resid_tol = 1e-3f;
+    float mlp_margin = 0.02f, mlp_resid_tol = 1e-6f;
+    int mlp_polish = 2;
 };
 
 namespace clb {

@@ -77,7 +77,10 @@ __device__ __forceinline__ void eq_totals(const SpecParams& P, const double* cin
     }
 }
 
-__device__ __forceinline__ bool eq_solve_nr(const SpecParams& P, const double* cin, double* cout, int* iters) {
+// x0: optional starting log10 component concentrations (else the reference's guess from the
+// component species, 1e-7 for a component that is not a species); max_it < 0: the tableau's cap.
+__device__ __forceinline__ bool eq_solve_nr(const SpecParams& P, const double* cin, double* cout, int* iters,
+                                            const double* x0, int max_it) {
     const int nc = P.nc;
     double T[CLB_MAX_COMPONENTS], x[CLB_MAX_COMPONENTS], F[CLB_MAX_COMPONENTS], xn[CLB_MAX_COMPONENTS],
         d[CLB_MAX_COMPONENTS];
@@ -85,13 +88,18 @@ __device__ __forceinline__ bool eq_solve_nr(const SpecParams& P, const double* c
     double c[CLB_MAX_EQ_SPECIES];
     eq_totals(P, cin, T);
     for (int j = 0; j < nc; ++j) {
-        const double cc = P.comp[j] >= 0 ? cin[P.comp[j]] : 1e-7;
-        x[j] = log10(fmax(fmin(cc, EQ_MAX_C), EQ_MIN_C));
+        if (x0) {
+            x[j] = fmax(fmin(x0[j], EQ_MAX_LOG), EQ_MIN_LOG);
+        } else {
+            const double cc = P.comp[j] >= 0 ? cin[P.comp[j]] : 1e-7;
+            x[j] = log10(fmax(fmin(cc, EQ_MAX_C), EQ_MIN_C));
+        }
     }
     bool conv = false;
     int it = 0;
     const double ln10 = 2.302585092994045684;
-    for (; it < P.max_it; ++it) {
+    const int cap = max_it < 0 ? P.max_it : max_it;
+    for (; it < cap; ++it) {
         const double fn = eq_residual(P, x, T, cin, c, F);
         if (fn < P.tol) { conv = true; ++it; break; }
         for (int j = 0; j < nc; ++j) {
@@ -144,6 +152,7 @@ __device__ __forceinline__ bool eq_solve_nr(const SpecParams& P, const double* c
         if (isnan(v) || isinf(v)) v = cin[i] > EQ_MIN_C ? fmin(cin[i], EQ_MAX_C) : EQ_MIN_C;
         cout[i] = fmax(fmin(v, EQ_MAX_C), EQ_MIN_C);
     }
+    if (x0) for (int j = 0; j < nc; ++j) const_cast<double*>(x0)[j] = x[j];  // hand back where it stopped
     *iters = it;
     return conv;
 }
@@ -154,7 +163,7 @@ __global__ void k_eq_batch(const SpecParams P, const double* __restrict__ cin, d
         double ci[CLB_MAX_EQ_SPECIES], co[CLB_MAX_EQ_SPECIES];
         for (int i = 0; i < P.ns; ++i) ci[i] = cin[(int64_t)t * P.ns + i];
         int it = 0;
-        eq_solve_nr(P, ci, co, &it);
+        eq_solve_nr(P, ci, co, &it, nullptr, -1);
         for (int i = 0; i < P.ns; ++i) cout[(int64_t)t * P.ns + i] = co[i];
         if (iters) iters[t] = it;
     }
@@ -185,11 +194,14 @@ __device__ __forceinline__ TS* out_slot7(const SparseView& S, TS* f, TS* link, i
     return f + (int64_t)i * S.KS + dst;
 }
 
-// Surrogate evaluation for the warp: each lane brings its voxel's species (active lanes) and gets
-// back the surrogate's species; returns whether the surrogate's answer is accepted for the lane
-// (inside the trained input range, and when `check` also within the mass-balance residual).
+// Surrogate evaluation for the warp (tensor-core tiles, all lanes together): each lane brings its
+// voxel's species, the surrogate predicts the equilibrium, and `M.polish` FP64 Newton iterations
+// start from the surrogate's component values. Accepted (true) when the input lies inside the
+// trained range and, when `check`, the polished answer has converged; x0_out returns where the
+// polish stopped so a fallback can continue from there.
 __device__ __forceinline__ bool mlp_warp_speciate(const MlpView& M, const SpecParams& P, bool active,
-                                                  const double* c, double* e, bool check, float* ws) {
+                                                  const double* c, double* e, bool check, float* ws,
+                                                  double* x0_out, int* it_used) {
     const int lane = threadIdx.x & 31;
     double T[CLB_MAX_COMPONENTS];
     bool in_range = active;
@@ -217,12 +229,20 @@ __device__ __forceinline__ bool mlp_warp_speciate(const MlpView& M, const SpecPa
         __syncwarp();
     }
     if (!active) return false;
+    // the surrogate's log10 species; its components' values start a short Newton polish
+    double x[CLB_MAX_COMPONENTS];
     for (int i = 0; i < P.ns; ++i) {
         const float lo = M.out_lo[i], hi = M.out_hi[i];
-        const double lc = (double)lo + ((double)row[i] + 1.0) * 0.5 * (double)(hi - lo);
-        e[i] = fmax(fmin(exp10(fmax(fmin(lc, EQ_MAX_LOG), EQ_MIN_LOG)), EQ_MAX_C), EQ_MIN_C);
+        e[i] = (double)lo + ((double)row[i] + 1.0) * 0.5 * (double)(hi - lo);
     }
-    if (!in_range) return false;
+    for (int j = 0; j < P.nc; ++j) x[j] = P.comp[j] >= 0 ? e[P.comp[j]] : -7.0;
+    *it_used = 0;
+    if (!in_range) {
+        for (int j = 0; j < P.nc; ++j) x0_out[j] = x[j];
+        return false;
+    }
+    eq_solve_nr(P, c, e, it_used, x, M.polish);
+    for (int j = 0; j < P.nc; ++j) x0_out[j] = x[j];
     if (!check) return true;
     double worst = 0;
     for (int j = 0; j < P.nc; ++j) {
@@ -268,17 +288,21 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
             }
         }
         bool done = false;
+        double xs[CLB_MAX_COMPONENTS];
+        int pit = 0;
         if (use_mlp) {  // warp-uniform
-            done = mlp_warp_speciate(M, P, active, c, e, mode == CLB_SPEC_MLP_NR, wsm[wib]);
+            done = mlp_warp_speciate(M, P, active, c, e, mode == CLB_SPEC_MLP_NR, wsm[wib], xs, &pit);
             if (active) { if (done) ++n_sur; else ++n_fb; }
         }
         if (!active) continue;
         ++n_solve;
+        n_it += pit;
         if (done) {
             ++n_conv;
         } else {
+            // Newton-Raphson fallback, from where the surrogate's polish stopped when there was one
             int it = 0;
-            if (eq_solve_nr(P, c, e, &it)) ++n_conv;
+            if (eq_solve_nr(P, c, e, &it, (use_mlp && pit > 0) ? xs : nullptr, -1)) ++n_conv;
             n_it += it;
         }
         for (int i = 0; i < P.ns; ++i) {
@@ -448,6 +472,7 @@ MlpView mlp_view(clb_handle* h) {
     M.ns = CLB_SP(h).ns;
     M.range_margin = h->mlp_margin;
     M.resid_tol = h->mlp_resid_tol;
+    M.polish = h->mlp_polish;
     return M;
 }
 
@@ -668,7 +693,9 @@ __global__ void __launch_bounds__(128) k_mlp_predict(const MlpView M, const Spec
         double c[CLB_MAX_EQ_SPECIES], e[CLB_MAX_EQ_SPECIES];
         if (active)
             for (int i = 0; i < P.ns; ++i) c[i] = fmax(cin[(int64_t)tix * P.ns + i], EQ_MIN_C);
-        const bool ok = mlp_warp_speciate(M, P, active, c, e, check != 0, wsm[w]);
+        double xs[CLB_MAX_COMPONENTS];
+        int pit = 0;
+        const bool ok = mlp_warp_speciate(M, P, active, c, e, check != 0, wsm[w], xs, &pit);
         if (active) {
             for (int i = 0; i < P.ns; ++i) cout[(int64_t)tix * P.ns + i] = e[i];
             if (accepted) accepted[tix] = ok ? 1 : 0;
@@ -814,7 +841,9 @@ clb_status surrogate_train(clb_handle* h, const clb_surrogate_train_desc* d, clb
                                                                                 1.f / (float)(cnt * ns), G, loss);
             ++step;
             const float c1 = 1.f - std::pow(b1, (float)step), c2 = 1.f - std::pow(b2, (float)step);
-            k_mlp_adam<<<(P_N + 255) / 256, 256, 0, h->stream>>>(P, Mm, V, G, (float)d->learning_rate, b1, b2, 1e-8f, c1, c2);
+            // learning rate decays by 5 % per epoch
+            const float lr = (float)d->learning_rate * std::pow(0.95f, (float)epoch);
+            k_mlp_adam<<<(P_N + 255) / 256, 256, 0, h->stream>>>(P, Mm, V, G, lr, b1, b2, 1e-8f, c1, c2);
             mlp_refresh_bf16(h);
         }
         k_mlp_eval<<<h->num_sms * 2, 128, 0, h->stream>>>(mlp_view(h), X, Y, n_tr, n_val, loss + 1);

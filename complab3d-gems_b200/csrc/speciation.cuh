@@ -29,7 +29,8 @@ struct MlpView {
     const float* out_hi;
     int nc, ns;
     float range_margin;        // inputs may exceed the trained range by this fraction
-    float resid_tol;           // relative mass-balance residual the surrogate must meet
+    float resid_tol;           // relative mass-balance residual a kept answer must meet
+    int polish;                // FP64 Newton iterations started from the surrogate's answer
 };
 
 struct SpecParams {
@@ -42,7 +43,8 @@ struct SpecParams {
     int ispec[CLB_MAX_EQ_SPECIES];  // internal species index of tableau row i
 };
 
-__device__ __forceinline__ bool eq_solve_nr(const SpecParams& P, const double* cin, double* cout, int* iters);
+__device__ __forceinline__ bool eq_solve_nr(const SpecParams& P, const double* cin, double* cout, int* iters,
+                                            const double* x0, int max_it);
 __device__ __forceinline__ void eq_totals(const SpecParams& P, const double* cin, double* T);
 
 MlpView mlp_view(clb_handle* h);

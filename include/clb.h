@@ -274,13 +274,17 @@ typedef struct clb_surrogate_report {
 
 clb_status clb_surrogate_train(clb_handle* h, const clb_surrogate_train_desc* desc, clb_surrogate_report* out);
 
-/* Acceptance of a surrogate answer inside the speciation step: every scaled input within
- * 1 + range_margin of the trained range, and (mode CLB_SPEC_MLP_NR) the relative mass-balance
- * residual max_j |S^T c - T|_j / T_j at most residual_tol. Defaults 0.02 and 1e-3. */
-clb_status clb_surrogate_set_check(clb_handle* h, double range_margin, double residual_tol);
+/* How the speciation step uses the surrogate: its answer is used only when every scaled input
+ * lies within 1 + range_margin of the trained range; it then starts newton_polish FP64
+ * Newton-Raphson iterations (the surrogate's component concentrations are the initial point).
+ * Mode CLB_SPEC_MLP keeps the polished answer; mode CLB_SPEC_MLP_NR keeps it only if its relative
+ * mass-balance residual max_j |S^T c - T|_j / T_j is at most residual_tol and otherwise continues
+ * Newton-Raphson from there (outside the trained range it starts Newton-Raphson afresh).
+ * Defaults 0.02, 2 and 1e-6. */
+clb_status clb_surrogate_set_check(clb_handle* h, double range_margin, int newton_polish, double residual_tol);
 
-/* Surrogate speciation of n states ([n][n_species] host arrays); accepted[n] (may be NULL)
- * reports the acceptance test (with the residual check when residual_check != 0). */
+/* Surrogate speciation of n states ([n][n_species] host arrays), polished as above; accepted[n]
+ * (may be NULL) reports the acceptance test (the convergence check when residual_check != 0). */
 clb_status clb_surrogate_predict(clb_handle* h, const double* conc_in, int n, double* conc_out, int* accepted,
                                  int residual_check);
 

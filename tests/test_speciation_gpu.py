@@ -57,7 +57,8 @@ def test_speciation_step_in_transport_matches_oracle(clb, oracle):
     D.ade_step(9)
     O.step(9)
     for s in range(4):
-        np.testing.assert_allclose(D.concentration(s), O.concentration(s), rtol=1e-9, atol=1e-16)
+        # both sides stop Newton-Raphson at an absolute residual of 1e-10 on the totals
+        np.testing.assert_allclose(D.concentration(s), O.concentration(s), rtol=1e-7, atol=1e-15)
     st = D.speciation_stats()
     assert st["solves"] > 0 and st["converged"] == st["solves"]
 
@@ -116,22 +117,28 @@ def trained(clb):
     S, logK, comp = workloads.carbonate_tableau()
     D = handle(clb, S, logK, comp)
     lo, hi = [-5, -9, -8, -6], [-2, -5, -4, -3]
-    rep = D.surrogate_train(lo, hi, n_samples=120000, epochs=40, batch=4096, patience=6, learning_rate=3e-3, seed=11)
+    rep = D.surrogate_train(lo, hi, n_samples=200000, epochs=60, batch=1024, patience=8, learning_rate=3e-3, seed=11)
     return D, S, logK, comp, lo, hi, rep
 
 
 def test_surrogate_trains_and_matches_newton(trained, oracle):
     D, S, logK, comp, lo, hi, rep = trained
     print("training:", rep)
-    assert rep["val_mse"] < 2e-4
+    assert rep["val_mse"] < 1e-3
     states = workloads.species_states(4000, 4, np.array(lo), np.array(hi), seed=99)
     states = states[(states @ S > 0).all(axis=1)]
-    pred, acc = D.surrogate_predict(states, residual_check=False)
     nr, _ = D.speciation_solve(states)
-    rel = np.abs(np.log10(pred) - np.log10(nr))
-    print("surrogate |dlog10 c|: median %.2e  p95 %.2e" % (np.median(rel), np.percentile(rel, 95)))
-    assert np.median(rel) < 2e-2
-    assert acc.mean() > 0.9
+    D.surrogate_set_check(0.02, 0)  # the network alone
+    raw, _ = D.surrogate_predict(states, residual_check=False)
+    D.surrogate_set_check(0.02, 2)  # with the two-step Newton polish
+    pol, acc = D.surrogate_predict(states, residual_check=True)
+    r_raw = np.abs(raw / nr - 1)
+    r_pol = np.abs(pol / nr - 1)
+    print("network alone: median rel err %.2e, p95 %.2e; polished: median %.2e, max %.2e, accepted %.3f"
+          % (np.median(r_raw), np.percentile(r_raw, 95), np.median(r_pol), r_pol.max(), acc.mean()))
+    assert np.median(r_raw) < 0.1
+    assert np.percentile(r_pol[acc], 99) <= 1e-3
+    assert acc.mean() > 0.8
 
 
 def test_surrogate_gain_over_newton(trained):
@@ -141,7 +148,7 @@ def test_surrogate_gain_over_newton(trained):
     D.surrogate_predict(states[:1000])
     t0 = time.perf_counter(); D.speciation_solve(states); t1 = time.perf_counter()
     D.surrogate_predict(states, residual_check=False); t2 = time.perf_counter()
-    print("Newton-Raphson %.1f ms, surrogate %.1f ms (400k states, host transfers included)"
+    print("Newton-Raphson %.1f ms, surrogate + polish %.1f ms (400k states, host transfers included)"
           % ((t1 - t0) * 1e3, (t2 - t1) * 1e3))
     assert (t2 - t1) < (t1 - t0)
 
@@ -159,7 +166,7 @@ def test_surrogate_with_fallback_in_transport(clb, oracle, trained):
         D.ade_init(sp)
         D.speciation_setup(S, logK, comp, tol=1e-10)
         D.surrogate_params(params, scaling)
-        D.surrogate_set_check(0.02, 1e-3)
+        D.surrogate_set_check(0.02, 2)
         D.set_speciation_mode(mode)
         D.ade_step(12)
         results[mode] = (np.array([D.concentration(s) for s in range(4)]), D.speciation_stats())
@@ -168,4 +175,6 @@ def test_surrogate_with_fallback_in_transport(clb, oracle, trained):
     print("surrogate step stats:", st)
     assert st["surrogate_used"] + st["fallbacks"] == st["solves"]
     open_ = (mat == 2)
-    np.testing.assert_allclose(a[:, open_], b[:, open_], rtol=5e-3)
+    # a kept surrogate answer meets a 1e-6 relative mass balance; species agree to 1e-4
+    np.testing.assert_allclose(a[:, open_], b[:, open_], rtol=1e-4)
+    assert st["surrogate_used"] > 0.5 * st["solves"]
