@@ -14,7 +14,8 @@
 // the species lattices (pore and biofilm); mobile species populations g[m][7][K] of the storage
 // type (m = rank of the species among the mobile ones) with their wall link slots
 // glink[m][L]; AA in-place pattern as in flow.cu. Immobile species and biomass are FP64 fields
-// imm[s][K], bio[m][K]; the advection velocity u[3][K] is in the arithmetic type.
+// dense per-voxel fields imm[s][N], bio[m][N] (they must outlive a voxel's change of class); the
+// advection velocity u[3][K] is in the arithmetic type.
 // Algorithmic bytes per node update: 2*7*sizeof(storage) per mobile species, plus the velocity
 // (3*sizeof(arith)) and the material byte shared by all species.
 #include "sparse.cuh"
@@ -174,16 +175,17 @@ __global__ void __launch_bounds__(ADE_THREADS)
 #pragma unroll
         for (int s = 0; s < NM; ++s) dC[s] = 0.0;
         if (P.law != CLB_LAW_NONE && !west && !east && P.react[code]) {
+            const int64_t nd = S.node[k];  // dense index of the per-voxel fields
             double C[NM], R[NM], B[CLB_MAX_MICROBES], RB[CLB_MAX_MICROBES];
 #pragma unroll
             for (int s = 0; s < NM; ++s) {
                 double c = 0.0;
                 if (s < n_mobile) c = (double)rb[s] + 1.0;
-                else if (s < P.S) c = imm[(int64_t)s * K + k];
+                else if (s < P.S) c = imm[(int64_t)s * G.N + nd];
                 C[s] = c < THRD ? 0.0 : c;
             }
             for (int mb = 0; mb < P.M; ++mb) {
-                const double b = bio[(int64_t)mb * K + k];
+                const double b = bio[(int64_t)mb * G.N + nd];
                 B[mb] = b < THRD ? 0.0 : b;
             }
             eval_rates<NM>(P, C, B, R, RB);
@@ -195,13 +197,13 @@ __global__ void __launch_bounds__(ADE_THREADS)
                 if (d + C[s] < 0.0) d = -C[s];
                 if (!(d > THRD || d < -THRD)) continue;
                 if (s < n_mobile) dC[s] = d;
-                else imm[(int64_t)s * K + k] += d;
+                else imm[(int64_t)s * G.N + nd] += d;
             }
             for (int mb = 0; mb < P.M; ++mb) {
                 double d = RB[mb] * P.dt;
                 if (!(d > THRD || d < -THRD)) continue;
                 if (d + B[mb] < 0.0) d = -B[mb];
-                bio[(int64_t)mb * K + k] += d;
+                bio[(int64_t)mb * G.N + nd] += d;
             }
         }
         // ---- collide, deposit, stream
@@ -354,7 +356,7 @@ __global__ void k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ gl
                 for (int i = 0; i < 7; ++i) sum += ldd(g + ((int64_t)m * 7 + i) * S.KS + k);
                 c = sum;
             } else {
-                c = imm[(int64_t)s * K + k];
+                c = imm[(int64_t)s * P.g.N + S.node[k]];
             }
             atomicAdd(&shq[S_ + s], c);
             if (open) {
@@ -377,22 +379,10 @@ __global__ void k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ gl
             }
         }
         if (inner)
-            for (int mb = 0; mb < M; ++mb) atomicAdd(&shq[4 * S_ + mb], bio[(int64_t)mb * K + k]);
+            for (int mb = 0; mb < M; ++mb) atomicAdd(&shq[4 * S_ + mb], bio[(int64_t)mb * P.g.N + S.node[k]]);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < nq; q += blockDim.x) part[(int64_t)blockIdx.x * nq + q] = shq[q];
-}
-
-// dense [N] <-> compact [K] transfers of per-node FP64 fields
-__global__ void k_gather_dense(const double* __restrict__ dense, const int32_t* __restrict__ node, int64_t K,
-                               double* __restrict__ compact) {
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
-        compact[k] = dense[node[k]];
-}
-__global__ void k_scatter_dense(const double* __restrict__ compact, const int32_t* __restrict__ node, int64_t K,
-                                double* __restrict__ dense) {
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
-        dense[node[k]] = compact[k];
 }
 
 // ------------------------------------------------------------------ host side
@@ -488,17 +478,18 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
         return cuda_check(h, e, "species populations");
     if ((e = cudaMalloc(&h->d_glink, esize(h->ade_prec) * L1 * nm1)) != cudaSuccess)
         return cuda_check(h, e, "species links");
-    if ((e = cudaMalloc(&h->d_imm, sizeof(double) * K1 * S)) != cudaSuccess) return cuda_check(h, e, "immobile fields");
+    const size_t N1 = (size_t)h->g.N;
+    if ((e = cudaMalloc(&h->d_imm, sizeof(double) * N1 * S)) != cudaSuccess) return cuda_check(h, e, "immobile fields");
     if ((e = cudaMalloc(&h->d_u, usize(h->ade_prec) * 3 * K1)) != cudaSuccess) return cuda_check(h, e, "velocity");
     if ((e = cudaMalloc(&h->d_neu, sizeof(double) * S * 2 * h->g.plane + sizeof(int) * 16)) != cudaSuccess)
         return cuda_check(h, e, "boundary store");
     cudaMemsetAsync(h->d_u, 0, usize(h->ade_prec) * 3 * K1, h->stream);
     // immobile species: uniform c0 (initial_concentration applies to the whole domain)
-    std::vector<double> immh(K1);
+    std::vector<double> immh(N1);
     for (int i = 0; i < S; ++i) {
         if (P.mobile[i]) continue;
         std::fill(immh.begin(), immh.end(), P.c0[i]);
-        cudaMemcpy(h->d_imm + (size_t)i * K1, immh.data(), sizeof(double) * K1, cudaMemcpyHostToDevice);
+        cudaMemcpy(h->d_imm + (size_t)i * N1, immh.data(), sizeof(double) * N1, cudaMemcpyHostToDevice);
     }
     // stored boundary densities: Dirichlet value, else c0 (lattice.initialize() runs the
     // Neumann processor once on the equilibrium field)
@@ -566,35 +557,6 @@ clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm,
     return CLB_OK;
 }
 
-// dense [rows][N] host field <-> compact [rows][K] device field
-static clb_status to_compact(clb_handle* h, const double* host_dense, int rows, double* dev_compact) {
-    const int64_t N = h->g.N, K = h->ade_sp.K;
-    double* tmp = nullptr;
-    cudaError_t e = cudaMalloc(&tmp, sizeof(double) * N);
-    if (e != cudaSuccess) return cuda_check(h, e, "field buffer");
-    for (int r = 0; r < rows && e == cudaSuccess; ++r) {
-        e = cudaMemcpyAsync(tmp, host_dense + (size_t)r * N, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream);
-        k_gather_dense<<<h->num_sms * 4, 256, 0, h->stream>>>(tmp, h->ade_sp.node, K, dev_compact + (size_t)r * K);
-    }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(tmp);
-    return cuda_check(h, e, "field upload");
-}
-
-static clb_status to_dense(clb_handle* h, const double* dev_compact, double fill, double* host_dense) {
-    const int64_t N = h->g.N, K = h->ade_sp.K;
-    std::vector<double> init((size_t)N, fill);
-    double* tmp = nullptr;
-    cudaError_t e = cudaMalloc(&tmp, sizeof(double) * N);
-    if (e != cudaSuccess) return cuda_check(h, e, "field buffer");
-    e = cudaMemcpyAsync(tmp, init.data(), sizeof(double) * N, cudaMemcpyHostToDevice, h->stream);
-    k_scatter_dense<<<h->num_sms * 4, 256, 0, h->stream>>>(dev_compact, h->ade_sp.node, K, tmp);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(host_dense, tmp, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(tmp);
-    return cuda_check(h, e, "field download");
-}
-
 clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (M < 0 || M > CLB_MAX_MICROBES) return fail(h, CLB_INVALID_ARG, "microbe count out of range");
@@ -603,9 +565,9 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
     h->M = M;
     h->ap.M = M;
     if (M == 0) return CLB_OK;
-    cudaError_t e = cudaMalloc(&h->d_bio, sizeof(double) * M * (size_t)std::max<int64_t>(1, h->ade_sp.K));
+    cudaError_t e = cudaMalloc(&h->d_bio, sizeof(double) * M * (size_t)h->g.N);
     if (e != cudaSuccess) return cuda_check(h, e, "biomass");
-    return to_compact(h, b, M, h->d_bio);
+    return cuda_check(h, cudaMemcpy(h->d_bio, b, sizeof(double) * M * (size_t)h->g.N, cudaMemcpyHostToDevice), "biomass copy");
 }
 
 template <typename TS, typename TC, bool ODD>
@@ -740,7 +702,8 @@ clb_status ade_density(clb_handle* h, int s, double* host) {
     if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
     s = h->u2i[s];
     const size_t N = (size_t)h->g.N;
-    if (h->ap.slot[s] < 0) return to_dense(h, h->d_imm + (size_t)s * std::max<int64_t>(1, h->ade_sp.K), h->ap.c0[s], host);
+    if (h->ap.slot[s] < 0)
+        return cuda_check(h, cudaMemcpy(host, h->d_imm + (size_t)s * N, sizeof(double) * N, cudaMemcpyDeviceToHost), "immobile copy");
     // the Neumann planes' stored values as the reference holds them after the last stream
     refresh_neumann(h);
     std::vector<double> pops(7 * N);
@@ -771,12 +734,12 @@ clb_status ade_density(clb_handle* h, int s, double* host) {
 
 clb_status ade_biomass(clb_handle* h, int m, double* host) {
     if (!h->ade_ready || m < 0 || m >= h->M) return fail(h, CLB_INVALID_ARG, "no such biomass field");
-    return to_dense(h, h->d_bio + (size_t)m * std::max<int64_t>(1, h->ade_sp.K), 0.0, host);
+    return cuda_check(h, cudaMemcpy(host, h->d_bio + (size_t)m * h->g.N, sizeof(double) * h->g.N, cudaMemcpyDeviceToHost), "biomass copy");
 }
 
 clb_status ade_set_biomass_field(clb_handle* h, int m, const double* host) {
     if (!h->ade_ready || m < 0 || m >= h->M) return fail(h, CLB_INVALID_ARG, "no such biomass field");
-    return to_compact(h, host, 1, h->d_bio + (size_t)m * std::max<int64_t>(1, h->ade_sp.K));
+    return cuda_check(h, cudaMemcpy(h->d_bio + (size_t)m * h->g.N, host, sizeof(double) * h->g.N, cudaMemcpyHostToDevice), "biomass copy");
 }
 
 __global__ void k_u_to_dense(const void* __restrict__ u, int f64, const int32_t* __restrict__ node, int64_t K,

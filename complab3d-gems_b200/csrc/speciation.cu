@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
                     v = 1.0;
                     for (int q = 0; q < 7; ++q) v += ldd(out_slot7(S, f, lk, (int)k, q, odd));
                 } else {
-                    v = imm[(int64_t)si * S.K + k];
+                    v = imm[(int64_t)si * A.g.N + S.node[k]];
                 }
                 c[i] = fmax(v, EQ_MIN_C);
             }
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
                     else *p = (TS)v;
                 }
             } else {
-                imm[(int64_t)si * S.K + k] += dC;
+                imm[(int64_t)si * A.g.N + S.node[k]] += dC;
             }
         }
     }
