@@ -118,6 +118,7 @@ SIGNATURES = {
     "clb_set_biomass": [C.c_void_p, C.c_int, C.c_void_p],
     "clb_ade_step": [C.c_void_p, C.c_int],
     "clb_reduce": [C.c_void_p, C.POINTER(Stats)],
+    "clb_reduce_noalloc": [C.c_void_p, C.POINTER(Stats)],
     "clb_speciation_setup": [C.c_void_p, C.POINTER(SpeciationDesc)],
     "clb_set_speciation_mode": [C.c_void_p, C.c_int],
     "clb_speciation_stats_get": [C.c_void_p, C.POINTER(SpeciationStats)],
@@ -354,6 +355,16 @@ class Domain:
     def reduce(self):
         s = Stats()
         self._check(lib().clb_reduce(self.h, C.byref(s)))
+        S = self.S
+        return {"total": np.array(s.total[:S]), "content": np.array(s.content[:S]),
+                "biomass": np.array(s.biomass[:]), "min": np.array(s.min_c[:S]), "max": np.array(s.max_c[:S]),
+                "open_voxels": s.open_voxels, "nonfinite": s.nonfinite, "ade_iterations": s.ade_iterations}
+
+    def reduce_noalloc(self):
+        """clb_reduce_noalloc: the reductions of reduce() from the library's fixed per-device
+        buffer, with no allocation; calls on one device must not overlap in time."""
+        s = Stats()
+        self._check(lib().clb_reduce_noalloc(self.h, C.byref(s)))
         S = self.S
         return {"total": np.array(s.total[:S]), "content": np.array(s.content[:S]),
                 "biomass": np.array(s.biomass[:]), "min": np.array(s.min_c[:S]), "max": np.array(s.max_c[:S]),

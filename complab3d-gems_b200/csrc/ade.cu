@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 namespace clb {
 
@@ -821,6 +822,97 @@ clb_status ade_reduce(clb_handle* h, clb_stats* out) {
         out->nonfinite += (int64_t)q[4 * S + M];
         out->open_voxels += (int64_t)q[4 * S + M + 1];
     }
+    out->ade_iterations = h->ade_iters;
+    return CLB_OK;
+}
+
+
+// ------------------------------------------------------------------ reduction without allocation
+//
+// clb_reduce_noalloc computes what clb_reduce computes, but takes its per-block partial sums from
+// a fixed buffer compiled into the library instead of a cudaMalloc'd one, and combines them on
+// the device, so the call neither allocates nor frees memory, on the device or on the host. It
+// is meant for callers that must not allocate while they monitor a run: an application whose
+// device memory is all handed to its own pool (where a cudaMalloc fails), or a loop that cannot
+// afford the device-wide synchronisation a cudaFree implies.
+//
+// Limit: the buffer holds REDUCE_SCRATCH_DOUBLES doubles; a call needs (blocks + 1) x (4 S + M + 2)
+// of them (blocks = 2 x the SM count, S species, M microbes) and is refused with
+// CLB_INVALID_ARG when that does not fit. Every word of the buffer a call reads was written
+// earlier in the same call, so nothing has to start at zero. The buffer is one per device and
+// shared by all handles on it: two calls that overlap in time on one device (different host
+// threads, or different streams without ordering between them) race on it and return wrong
+// sums. The first call on each device looks up the buffer's device address (set-up); make that
+// first call before any stream capture begins.
+constexpr int REDUCE_SCRATCH_DOUBLES = 65536;  // 512 KiB
+static __device__ __align__(256) double g_reduce_scratch[REDUCE_SCRATCH_DOUBLES];
+
+// combine the per-block partials in block order (the order the host loop of ade_reduce uses)
+__global__ void k_reduce_combine(const double* __restrict__ part, int blocks, int nq, int S, double* __restrict__ out) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const bool is_min = q >= 2 * S && q < 3 * S, is_max = q >= 3 * S && q < 4 * S;
+        double acc = is_min ? 1e300 : (is_max ? -1e300 : 0.0);
+        for (int b = 0; b < blocks; ++b) {
+            const double v = part[(int64_t)b * nq + q];
+            acc = is_min ? fmin(acc, v) : (is_max ? fmax(acc, v) : acc + v);
+        }
+        out[q] = acc;
+    }
+}
+
+static std::mutex g_scratch_mutex;
+constexpr int MAX_DEVICES = 64;
+static double* g_scratch_addr[MAX_DEVICES] = {};
+
+// Device address of g_reduce_scratch on the current device (looked up once per device).
+static clb_status reduce_scratch(clb_handle* h, double** ptr) {
+    if (h->device < 0 || h->device >= MAX_DEVICES) return fail(h, CLB_INVALID_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[h->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_reduce_scratch);
+        if (e != cudaSuccess) return cuda_check(h, e, "scratch buffer address");
+        g_scratch_addr[h->device] = (double*)p;
+    }
+    *ptr = g_scratch_addr[h->device];
+    return CLB_OK;
+}
+
+clb_status ade_reduce_noalloc(clb_handle* h, clb_stats* out) {
+    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+    std::memset(out, 0, sizeof(*out));
+    const int S = h->S, M = h->M;
+    const int nq = 4 * S + M + 2;
+    const int grid = h->num_sms * 2;
+    if ((int64_t)(grid + 1) * nq > REDUCE_SCRATCH_DOUBLES)
+        return fail(h, CLB_INVALID_ARG, "reduction needs more scratch than the fixed 65536-double buffer holds");
+    double* part = nullptr;
+    clb_status st = reduce_scratch(h, &part);
+    if (st != CLB_OK) return st;
+    double* fin = part + (size_t)grid * nq;
+    int* mt = mob_table(h);
+    const size_t sh = sizeof(double) * nq;
+    const SparseView Sv = view_of(h->ade_sp);
+    switch (h->ade_prec) {
+        case CLB_F64: k_ade_reduce<double><<<grid, 256, sh, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
+        case CLB_F32: k_ade_reduce<float><<<grid, 256, sh, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
+        default: k_ade_reduce<__half><<<grid, 256, sh, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
+    }
+    k_reduce_combine<<<1, 128, 0, h->stream>>>(part, grid, nq, S, fin);
+    double q[4 * CLB_MAX_SPECIES + CLB_MAX_MICROBES + 2];
+    cudaError_t e = cudaMemcpyAsync(q, fin, sizeof(double) * nq, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_check(h, e, "reduce");
+    for (int i = 0; i < S; ++i) {
+        const int s = h->i2u[i];
+        out->total[s] = q[i];
+        out->content[s] = q[S + i];
+        out->min_c[s] = q[2 * S + i];
+        out->max_c[s] = q[3 * S + i];
+    }
+    for (int mb = 0; mb < M; ++mb) out->biomass[mb] = q[4 * S + mb];
+    out->nonfinite = (int64_t)q[4 * S + M];
+    out->open_voxels = (int64_t)q[4 * S + M + 1];
     out->ade_iterations = h->ade_iters;
     return CLB_OK;
 }

@@ -254,6 +254,12 @@ clb_status clb_reduce(clb_handle* h, clb_stats* out) {
     return ade_reduce(h, out);
 }
 
+clb_status clb_reduce_noalloc(clb_handle* h, clb_stats* out) {
+    if (!h || !out) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return ade_reduce_noalloc(h, out);
+}
+
 clb_status clb_speciation_setup(clb_handle* h, const clb_speciation_desc* desc) {
     if (!h || !desc) return fail(h, CLB_INVALID_ARG, "null argument");
     CLB_ON_DEVICE(h);

@@ -237,6 +237,7 @@ clb_status ade_velocity(clb_handle* h, double* host);
 clb_status ade_set_velocity(clb_handle* h, const double* host);
 clb_status ade_set_biomass_field(clb_handle* h, int m, const double* host);
 clb_status ade_reduce(clb_handle* h, clb_stats* out);
+clb_status ade_reduce_noalloc(clb_handle* h, clb_stats* out);
 void ade_free(clb_handle* h);
 
 // speciation.cu

@@ -209,6 +209,17 @@ clb_status clb_ade_step(clb_handle* h, int n);
 /* FP64 reductions over the live fields (complab3d_processors_part3.hh:387-600). */
 clb_status clb_reduce(clb_handle* h, clb_stats* out);
 
+/* The same reductions as clb_reduce, computed without allocating: no counterpart in the
+ * reference, whose reductions run inside Palabos data processors. For callers that must not
+ * allocate while they monitor a run (an application that hands all device memory to its own
+ * pool, or a loop that cannot absorb the device-wide synchronisation of a free). The partial
+ * sums live in one fixed 65536-double buffer per device, built into the library; a handle whose
+ * reduction needs more ((2 x SMs + 1) x (4 x species + microbes + 2) doubles) gets
+ * CLB_INVALID_ARG. The buffer is shared by every handle on a device, so calls must not overlap
+ * in time on one device (they would race on it). The first call on a device looks the buffer
+ * up; make it before any stream capture begins. */
+clb_status clb_reduce_noalloc(clb_handle* h, clb_stats* out);
+
 /* ---------------------------------------------------------------- equilibrium speciation */
 
 #define CLB_MAX_EQ_SPECIES 16
