@@ -20,6 +20,8 @@ LIB_PATH = os.path.join(HERE, "libclb.so")
 F64, F32, F16S = 0, 1, 2
 DIRICHLET, NEUMANN, CLOSED = 0, 1, 2
 LAW_NONE, LAW_DECAY, LAW_MONOD, LAW_DUAL_MONOD = 0, 1, 2, 3
+LAW_PRECIP, LAW_MINERAL = 4, 5  # abiotic laws
+DISSOL_NONE, DISSOL_FIRST_ORDER, DISSOL_MINERAL = 0, 1, 2
 FIELD_MATERIAL, FIELD_FLOW_VELOCITY, FIELD_FLOW_POPULATIONS = 0, 1, 2
 FIELD_CONCENTRATION, FIELD_ADE_POPULATIONS, FIELD_BIOMASS, FIELD_ADE_VELOCITY = 3, 4, 5, 6
 
@@ -78,6 +80,14 @@ class SpeciationDesc(C.Structure):
                 ("max_iterations", C.c_int32)]
 
 
+class PrecipDesc(C.Structure):
+    _fields_ = [("mineral_species", C.c_int32), ("full_density", C.c_double), ("precip_code", C.c_int32),
+                ("seal_flow", C.c_int32), ("seal_perm_ratio", C.c_double), ("flow_max_iterations", C.c_int32),
+                ("flow_eps", C.c_double), ("dissolution", C.c_int32), ("reopen_fraction", C.c_double),
+                ("pore_code", C.c_int32), ("dissolution_law", C.c_int32),
+                ("dissolution_params", C.c_double * (MAX_SPECIES + 2)), ("dissolution_surface_only", C.c_int32)]
+
+
 class SpeciationStats(C.Structure):
     _fields_ = [("solves", C.c_int64), ("converged", C.c_int64), ("surrogate_used", C.c_int64),
                 ("fallbacks", C.c_int64), ("iterations", C.c_int64)]
@@ -119,6 +129,9 @@ SIGNATURES = {
     "clb_ade_step": [C.c_void_p, C.c_int],
     "clb_reduce": [C.c_void_p, C.POINTER(Stats)],
     "clb_reduce_noalloc": [C.c_void_p, C.POINTER(Stats)],
+    "clb_set_abiotic_kinetics": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int],
+    "clb_precip_setup": [C.c_void_p, C.POINTER(PrecipDesc)],
+    "clb_geometry_update": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "clb_speciation_setup": [C.c_void_p, C.POINTER(SpeciationDesc)],
     "clb_set_speciation_mode": [C.c_void_p, C.c_int],
     "clb_speciation_stats_get": [C.c_void_p, C.POINTER(SpeciationStats)],
@@ -328,6 +341,36 @@ class Domain:
     def set_kinetics(self, law, params, dt):
         p = np.ascontiguousarray(params, dtype=np.float64)
         self._check(lib().clb_set_kinetics(self.h, law, _ptr(p), p.size, dt))
+
+    def set_abiotic_kinetics(self, law, params, surface_only=0):
+        p = np.ascontiguousarray(params if len(params) else [0.0], dtype=np.float64)
+        self._check(lib().clb_set_abiotic_kinetics(self.h, law, _ptr(p), len(params), int(surface_only)))
+
+    def precip_setup(self, mineral, full_density, precip_code=-1, seal_flow=0, seal_perm_ratio=0.0,
+                     flow_max_iterations=100000, flow_eps=1e-6, dissolution=0, reopen_fraction=0.9, pore_code=-1,
+                     dissolution_law=DISSOL_NONE, dissolution_params=(), dissolution_surface_only=1):
+        d = PrecipDesc()
+        d.mineral_species, d.full_density, d.precip_code = int(mineral), float(full_density), int(precip_code)
+        d.seal_flow, d.seal_perm_ratio = int(seal_flow), float(seal_perm_ratio)
+        d.flow_max_iterations, d.flow_eps = int(flow_max_iterations), float(flow_eps)
+        d.dissolution, d.reopen_fraction, d.pore_code = int(dissolution), float(reopen_fraction), int(pore_code)
+        d.dissolution_law, d.dissolution_surface_only = int(dissolution_law), int(dissolution_surface_only)
+        for i, v in enumerate(dissolution_params):
+            d.dissolution_params[i] = float(v)
+        self._check(lib().clb_precip_setup(self.h, C.byref(d)))
+
+    def geometry_update(self, allow_unconverged=False):
+        """Seal / reopen voxels; returns (sealed, reopened)."""
+        a, b = C.c_int(), C.c_int()
+        st = lib().clb_geometry_update(self.h, C.byref(a), C.byref(b))
+        if not (allow_unconverged and st == 2):
+            self._check(st)
+        return a.value, b.value
+
+    def material(self):
+        m = np.empty(self.N, dtype=np.int8)
+        self._check(lib().clb_get_field(self.h, FIELD_MATERIAL, 0, _ptr(m), 2))
+        return m
 
     def set_biomass(self, b):
         b = np.ascontiguousarray(b, dtype=np.float64)

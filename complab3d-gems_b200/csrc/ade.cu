@@ -18,7 +18,7 @@
 // advection velocity u[3][K] is in the arithmetic type.
 // Algorithmic bytes per node update: 2*7*sizeof(storage) per mobile species, plus the velocity
 // (3*sizeof(arith)) and the material byte shared by all species.
-#include "sparse.cuh"
+#include "kinetics.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -28,65 +28,14 @@ namespace clb {
 
 constexpr int ADE_THREADS = 256;
 
-// Rate laws (clb_law), over the species in internal order (mobile first). C and B are the
-// floored concentrations / biomasses; loops are unrolled to the species bucket NB so every array
-// stays in registers.
-template <int NB>
-__device__ __forceinline__ void eval_rates(const AdeParams& P, const double (&C)[NB], const double* B, double (&R)[NB],
-                                           double* RB) {
-#pragma unroll
-    for (int s = 0; s < NB; ++s) R[s] = 0.0;
-    switch (P.law) {
-        case CLB_LAW_DECAY:
-#pragma unroll
-            for (int s = 0; s < NB; ++s)
-                if (s < P.S) R[s] = -P.prm[s] * C[s];
-            break;
-        case CLB_LAW_MONOD:
-#pragma unroll
-            for (int s = 0; s < NB; ++s)
-                if (s < P.S) R[s] = -P.prm[s] * C[s] / (P.prm[CLB_MAX_SPECIES + s] + C[s]);
-            break;
-        case CLB_LAW_DUAL_MONOD: {
-            const double mu = P.prm[0], ks = P.prm[1], Y = P.prm[2], kd = P.prm[3];
-            const int don = P.donor;
-            double Cd = 0.0;
-#pragma unroll
-            for (int s = 0; s < NB; ++s)
-                if (s == don) Cd = C[s];
-            double Rd = 0.0;
-            for (int m = 0; m < P.M; ++m) {
-                const int a = P.acceptor[m];
-                RB[m] = 0.0;
-                if (a < 0) continue;
-                double Ca = 0.0;
-#pragma unroll
-                for (int s = 0; s < NB; ++s)
-                    if (s == a) Ca = C[s];
-                const double Bm = B[m];
-                if (Bm <= 0.0) continue;
-                const double growth = mu * (Cd / (ks + Cd)) * (Ca / (ks + Ca)) * Bm;
-                RB[m] += growth - kd * Bm;
-                Rd -= growth / Y;
-#pragma unroll
-                for (int s = 0; s < NB; ++s)
-                    if (s == a) R[s] -= growth / Y;
-            }
-#pragma unroll
-            for (int s = 0; s < NB; ++s)
-                if (s == don) R[s] += Rd;
-            break;
-        }
-        default:
-            break;
-    }
-}
-
-template <typename TS, typename TC, bool ODD, int NM>
+// EXT: the abiotic law and the increments gathered from dissolving neighbours (AdeExtra) are
+// applied after the biotic ones (complab.cpp:2460-2525).
+template <typename TS, typename TC, bool ODD, int NM, bool EXT>
 __global__ void __launch_bounds__(ADE_THREADS)
     k_ade_aa(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm, double* __restrict__ bio,
              const TC* __restrict__ u, const SparseView S, const double* __restrict__ neu, const AdeParams P,
-             int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin) {
+             int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin,
+             const AdeExtra X) {
     const Geom G = P.g;
     const int64_t K = S.K, L = S.L;
     const int64_t KS = S.KS;
@@ -94,6 +43,8 @@ __global__ void __launch_bounds__(ADE_THREADS)
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
         const int code = S.code[k];
         const int dyn = P.dyn[code];
+        // a voxel sealed by precipitation bounces back: on AA slots that is the identity
+        if (dyn == ADE_BB) continue;
         const bool west = k < k_west_end, east = k >= k_east_begin;
         int p = 0;
         uint32_t wm = 0, blk = 0;
@@ -205,6 +156,48 @@ __global__ void __launch_bounds__(ADE_THREADS)
                 if (!(d > THRD || d < -THRD)) continue;
                 if (d + B[mb] < 0.0) d = -B[mb];
                 bio[(int64_t)mb * G.N + nd] += d;
+            }
+        }
+        if (EXT && !west && !east && P.react[code]) {
+            // abiotic block: increments from the concentrations the biotic law left, applied once
+            // (update_abiotic_rxnLattices); next to a dissolving voxel they were computed ahead of
+            // the step together with the gathered products
+            const int64_t nd = S.node[k];
+            double T2[NM];
+#pragma unroll
+            for (int s = 0; s < NM; ++s) T2[s] = 0.0;
+            const int xi = X.xidx[k];
+            if (xi >= 0) {
+#pragma unroll
+                for (int s = 0; s < NM; ++s)
+                    if (s < P.S) T2[s] = X.xdc[(int64_t)s * X.ng + xi];
+            } else if (P.law2 != CLB_LAW_NONE && (!P.surf || X.iface[k])) {
+                double C[NM], R[NM];
+#pragma unroll
+                for (int s = 0; s < NM; ++s) {
+                    double c = 0.0;
+                    if (s < n_mobile) c = (double)rb[s] + 1.0 + dC[s];
+                    else if (s < P.S) c = imm[(int64_t)s * G.N + nd];
+                    C[s] = c < THRD ? 0.0 : c;
+                }
+                eval_rates2<NM>(P, C, R);
+#pragma unroll
+                for (int s = 0; s < NM; ++s) {
+                    if (s >= P.S) continue;
+                    double d = R[s] * P.dt;
+                    if (!(d > THRD || d < -THRD)) continue;
+                    if (d + C[s] < 0.0) d = -C[s];
+                    if (!(d > THRD || d < -THRD)) continue;
+                    T2[s] = d;
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < NM; ++s) {
+                if (s >= P.S) continue;
+                const double d = T2[s];
+                if (!(d > THRD || d < -THRD)) continue;
+                if (s < n_mobile) dC[s] += d;
+                else imm[(int64_t)s * G.N + nd] += d;
             }
         }
         // ---- collide, deposit, stream
@@ -398,6 +391,7 @@ void ade_free(clb_handle* h) {
     cudaFree(h->d_bio); h->d_bio = nullptr;
     cudaFree(h->d_u); h->d_u = nullptr;
     cudaFree(h->d_neu); h->d_neu = nullptr;
+    precip_free(h);
     sparse_free(h->ade_sp);
     h->ade_ready = false;
 }
@@ -520,6 +514,7 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
         cudaFree(dc0);
     }
     h->ade_iters = 0;
+    h->neu_iter = -1;
     h->ade_grid = h->num_sms * 4;
     h->ade_ready = true;
     return cuda_check(h, cudaGetLastError(), "ade init");
@@ -558,6 +553,49 @@ clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm,
     return CLB_OK;
 }
 
+clb_status ade_set_abiotic(clb_handle* h, int law, const double* prm, int nprm, int surface_only) {
+    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+    AdeParams& P = h->ap;
+    const int S = h->S;
+    auto species = [&](double v, int& out) {
+        const int s = (int)v;
+        if ((double)s != v || s < 0 || s >= S) return false;
+        out = h->u2i[s];
+        return true;
+    };
+    std::memset(P.prm2, 0, sizeof(P.prm2));
+    switch (law) {
+        case CLB_LAW_NONE:
+            break;
+        case CLB_LAW_PRECIP: {
+            if (nprm < 4) return fail(h, CLB_INVALID_ARG, "precipitation law needs kp, a, b, p");
+            int a, b, q;
+            if (!species(prm[1], a) || !species(prm[2], b) || !species(prm[3], q))
+                return fail(h, CLB_INVALID_ARG, "precipitation law: species index out of range");
+            P.prm2[0] = prm[0];
+            P.prm2[1] = a;
+            P.prm2[2] = b;
+            P.prm2[3] = q;
+            break;
+        }
+        case CLB_LAW_MINERAL: {
+            if (nprm < 3 + S) return fail(h, CLB_INVALID_ARG, "mineral law needs k, log10 Ksp, p, nu[S]");
+            int q;
+            if (!species(prm[2], q)) return fail(h, CLB_INVALID_ARG, "mineral law: species index out of range");
+            P.prm2[0] = prm[0];
+            P.prm2[1] = prm[1];
+            P.prm2[2] = q;
+            for (int i = 0; i < S; ++i) P.prm2[3 + i] = prm[3 + h->i2u[i]];
+            break;
+        }
+        default:
+            return fail(h, CLB_INVALID_ARG, "not an abiotic rate law");
+    }
+    P.law2 = law;
+    P.surf = surface_only ? 1 : 0;
+    return geometry_refresh(h);
+}
+
 clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (M < 0 || M > CLB_MAX_MICROBES) return fail(h, CLB_INVALID_ARG, "microbe count out of range");
@@ -581,15 +619,21 @@ static void launch_ade_t(clb_handle* h) {
     const TC* u = (const TC*)h->d_u;
     int* mt = mob_table(h);
     const SparseView S = view_of(h->ade_sp);
-#define CLB_ADE(NM)                                                                                          \
-    k_ade_aa<TS, TC, ODD, NM><<<grid, ADE_THREADS, 0, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, \
-                                                                  h->ap, nm, mt, h->ade_west_end,            \
-                                                                  h->ade_east_begin)
-    if (nb <= 1) CLB_ADE(1);
-    else if (nb <= 2) CLB_ADE(2);
-    else if (nb <= 4) CLB_ADE(4);
-    else if (nb <= 8) CLB_ADE(8);
-    else CLB_ADE(16);
+    const bool ext = h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on;
+    const AdeExtra X = ade_extra(h);
+#define CLB_ADE(NM, EXT)                                                                                          \
+    k_ade_aa<TS, TC, ODD, NM, EXT><<<grid, ADE_THREADS, 0, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, \
+                                                                       h->ap, nm, mt, h->ade_west_end,            \
+                                                                       h->ade_east_begin, X)
+    if (ext) {
+        if (nb <= 4) CLB_ADE(4, true);
+        else if (nb <= 8) CLB_ADE(8, true);
+        else CLB_ADE(16, true);
+    } else if (nb <= 1) CLB_ADE(1, false);
+    else if (nb <= 2) CLB_ADE(2, false);
+    else if (nb <= 4) CLB_ADE(4, false);
+    else if (nb <= 8) CLB_ADE(8, false);
+    else CLB_ADE(16, false);
 #undef CLB_ADE
 }
 
@@ -609,7 +653,12 @@ static void launch_neumann(clb_handle* h, int odd) {
     }
 }
 
+// The stored densities are those after the latest stream; they are recomputed lazily, once per
+// transport iteration, so that a readback or a change of the material map between two steps
+// (clb_geometry_update refreshes them before it converts voxels) does not alter them.
 static void refresh_neumann(clb_handle* h) {
+    if (h->neu_iter == h->ade_iters) return;
+    h->neu_iter = h->ade_iters;
     const int odd = (int)(h->ade_iters & 1);
     switch (h->ade_prec) {
         case CLB_F64: launch_neumann<double, double>(h, odd); break;
@@ -618,11 +667,17 @@ static void refresh_neumann(clb_handle* h) {
     }
 }
 
+void ade_refresh_neumann(clb_handle* h) { refresh_neumann(h); }
+
 clb_status ade_step(clb_handle* h, int n) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (h->M > 0 && h->d_bio == nullptr) return fail(h, CLB_INVALID_ARG, "biomass missing");
     for (int k = 0; k < n; ++k) {
         const bool odd = (h->ade_iters & 1) != 0;
+        if (h->ap.dis_on) {
+            clb_status st = dissolution_pre_step(h);
+            if (st != CLB_OK) return st;
+        }
         refresh_neumann(h);
         switch (h->ade_prec) {
             case CLB_F64: if (odd) launch_ade_t<double, double, true>(h); else launch_ade_t<double, double, false>(h); break;
@@ -693,6 +748,7 @@ clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
     }
     e = cudaStreamSynchronize(h->stream);
     cudaFree(buf);
+    h->neu_iter = -1;
     return cuda_check(h, e, "set populations");
 }
 

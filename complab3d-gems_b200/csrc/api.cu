@@ -93,6 +93,7 @@ clb_status clb_destroy(clb_handle* h) {
     flow_free(h);
     ade_free(h);
     cudaFree(h->d_mat);
+    cudaFree(h->d_mat_flow);
     cudaFree(h->d_err);
     cudaFree(h->d_spec_stats);
     cudaFree(h->d_mlp);
@@ -252,6 +253,25 @@ clb_status clb_reduce(clb_handle* h, clb_stats* out) {
     if (!h || !out) return fail(h, CLB_INVALID_ARG, "null argument");
     CLB_ON_DEVICE(h);
     return ade_reduce(h, out);
+}
+
+clb_status clb_set_abiotic_kinetics(clb_handle* h, int law, const double* params, int n_params, int surface_only) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    if (n_params > 0 && !params) return fail(h, CLB_INVALID_ARG, "null parameters");
+    CLB_ON_DEVICE(h);
+    return ade_set_abiotic(h, law, params, n_params, surface_only);
+}
+
+clb_status clb_precip_setup(clb_handle* h, const clb_precip_desc* desc) {
+    if (!h || !desc) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return precip_setup(h, desc);
+}
+
+clb_status clb_geometry_update(clb_handle* h, int* sealed, int* reopened) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    return geometry_update(h, sealed, reopened);
 }
 
 clb_status clb_reduce_noalloc(clb_handle* h, clb_stats* out) {

@@ -118,6 +118,23 @@ struct AdeParams {
     double c0[CLB_MAX_SPECIES];
     int donor;                          // internal index of the dual-Monod donor
     int acceptor[CLB_MAX_MICROBES];     // internal index of each microbe's acceptor, -1 none
+    // abiotic law (internal species indices)
+    int law2;                           // CLB_LAW_NONE, CLB_LAW_PRECIP, CLB_LAW_MINERAL
+    int surf;                           // surface-only gate of the abiotic law
+    double prm2[3 + CLB_MAX_SPECIES];
+    // dissolution of sealed mineral voxels
+    int dis_on, dis_law, dis_surf, sM;  // sM: internal index of the mineral
+    double dprm[2 + CLB_MAX_SPECIES];
+};
+
+// Per-node state of the precipitation / dissolution machinery (geometry_update.cu), passed to the
+// fused transport step when an abiotic law or dissolution is active.
+struct AdeExtra {
+    const uint8_t* iface;   // [K] 1: a solid or wall face neighbour (surface-only abiotic gate)
+    const int32_t* xidx;    // [K] row of the node in xdc, -1: none
+    const double* xdc;      // [S][ng] abiotic increments of the nodes next to sealed voxels,
+                            // gathered dissolution shares included
+    int64_t ng;
 };
 
 }  // namespace clb
@@ -186,12 +203,13 @@ struct clb_handle_s {
     void* d_glink = nullptr;          // [n_mobile][L] wall link slots
     clb::SparseBuffers ade_sp;
     int64_t ade_west_end = 0, ade_east_begin = 0;
-    double* d_imm = nullptr;          // [S][K] immobile concentrations (unused rows stay empty)
-    double* d_bio = nullptr;          // [M][K] biomass
+    double* d_imm = nullptr;          // [S][N] immobile concentrations (unused rows stay empty)
+    double* d_bio = nullptr;          // [M][N] biomass
     void* d_u = nullptr;              // [3][K] advection velocity (arithmetic type)
     double* d_neu = nullptr;          // [S][2][ny*nz] stored boundary densities
     clb::AdeParams ap;
     int64_t ade_iters = 0;
+    int64_t neu_iter = -1;            // iteration whose stream the Neumann store reflects
     int ade_grid = 0;
 
     // speciation (SpecParams lives in speciation.cuh; kept as raw storage here)
@@ -204,6 +222,23 @@ struct clb_handle_s {
     bool mlp_ready = false;
     float mlp_margin = 0.02f, mlp_resid_tol = 1e-6f;
     int mlp_polish = 2;
+
+    // precipitation / dissolution (geometry_update.cu)
+    bool prc_ready = false;
+    clb_precip_desc prc;
+    uint8_t* d_stamp = nullptr;       // [N] 1 where precipitation sealed the voxel
+    unsigned int* d_count = nullptr;  // conversion counters
+    int8_t* d_mat_flow = nullptr;     // [N] the flow lattice's own material map once they differ
+    std::vector<int8_t> h_mat_flow;
+    uint8_t* d_iface = nullptr;       // [K_ade] surface gate of the abiotic law
+    int32_t* d_seal = nullptr;        // sealed voxels: compact species-lattice index
+    int64_t n_seal = 0, seal_cap = 0;
+    int32_t* d_gath = nullptr;        // open voxels next to a sealed one: compact index
+    int32_t* d_gath_nb = nullptr;     // [ng][6] row in the sealed list of each face neighbour, -1
+    int64_t n_gath = 0, gath_cap = 0;
+    int32_t* d_xidx = nullptr;        // [K_ade] row in the gather list, -1
+    double* d_park = nullptr;         // [S][seal_cap] parked dissolution shares
+    double* d_xdc = nullptr;          // [S][gath_cap] abiotic increments of the gather list
 };
 
 namespace clb {
@@ -238,7 +273,18 @@ clb_status ade_set_velocity(clb_handle* h, const double* host);
 clb_status ade_set_biomass_field(clb_handle* h, int m, const double* host);
 clb_status ade_reduce(clb_handle* h, clb_stats* out);
 clb_status ade_reduce_noalloc(clb_handle* h, clb_stats* out);
+clb_status ade_set_abiotic(clb_handle* h, int law, const double* prm, int nprm, int surface_only);
+void ade_refresh_neumann(clb_handle* h);
 void ade_free(clb_handle* h);
+
+// geometry_update.cu
+clb_status precip_setup(clb_handle* h, const clb_precip_desc* d);
+clb_status geometry_update(clb_handle* h, int* sealed, int* reopened);
+clb_status geometry_refresh(clb_handle* h);   // surface gate and dissolution lists from the map
+clb_status dissolution_pre_step(clb_handle* h); // park + gather before a transport step
+AdeExtra ade_extra(clb_handle* h);
+void precip_free(clb_handle* h);
+inline const int8_t* flow_mat(const clb_handle* h) { return h->d_mat_flow ? h->d_mat_flow : h->d_mat; }
 
 // speciation.cu
 clb_status speciation_setup(clb_handle* h, const clb_speciation_desc* d);

@@ -197,6 +197,8 @@ __global__ void __launch_bounds__(FLOW_THREADS, MINB)
     double esum = 0;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
         const int code = S.code[k];
+        // a stored bounce-back node (a voxel sealed by precipitation): the identity on AA slots
+        if (P.dyn[code] == DYN_BB) continue;
         TC g[19];
         int rb_[8];
         uint32_t blk = 0, rbit = 0, wm = 0;
@@ -331,15 +333,17 @@ __global__ void __launch_bounds__(TILE, 2)
             issue_load(tn, (j + NSTAGE - 1) % NSTAGE);
         }
         const int64_t k = (int64_t)t * TILE + tid;
-        const bool live = k < K;
+        int code = 0;
+        if (k < K) code = S.code[k];
+        // a stored bounce-back node leaves its tile slots and links as they are (identity)
+        const bool live = k < K && P.dyn[code] != DYN_BB;
         uint32_t wm = 0;
-        int lb = 0, code = 0;
+        int lb = 0;
         TC xv[19];
         if (live) {
             const uint32_t m0 = S.meta[2 * k];
             wm = m0 & 0x7FFFFu;
             lb = S.tlb[t] + (int)(m0 >> 19);
-            code = S.code[k];
             int r = 0;
 #pragma unroll
             for (int i = 1; i < 19; ++i) {
@@ -569,9 +573,11 @@ clb_status flow_init(clb_handle* h, double delta_p) {
     P.rho_w = 1.0;
     P.rho_e = 1.0 - delta_p * 3.0;
     h->delta_p = delta_p;
+    // the flow lattice's own map once precipitation has changed the species' one
+    const std::vector<int8_t>& fmat = h->h_mat_flow.empty() ? h->h_mat : h->h_mat_flow;
     int64_t nbgk = 0, kw = 0, ke = 0;
     for (int64_t n = 0; n < h->g.N; ++n) {
-        const int dn = P.dyn[(uint8_t)h->h_mat[n]];
+        const int dn = P.dyn[(uint8_t)fmat[n] & 127];
         nbgk += (dn == DYN_BGK);
         if (dn != DYN_BB) {
             if (n < h->g.plane) ++kw;
@@ -583,7 +589,7 @@ clb_status flow_init(clb_handle* h, double delta_p) {
     flow_free(h);
     int8_t cls[MAX_CODES];
     for (int c = 0; c < MAX_CODES; ++c) cls[c] = (P.dyn[c] != DYN_BB);
-    clb_status s = sparse_build(h, cls, 19, h->flow_sp);
+    clb_status s = sparse_build(h, cls, 19, h->flow_sp, &fmat);
     if (s != CLB_OK) return s;
     const int64_t K = h->flow_sp.K;
     h->k_west_end = kw;
@@ -738,10 +744,10 @@ clb_status flow_velocity_at(clb_handle* h, const int32_t* nodes, int64_t count, 
 #define CLB_VEL(TS, TC)                                                                                         \
     if (dtype == 0)                                                                                             \
         k_flow_velocity<TS, TC, double><<<grid, 256, 0, h->stream>>>((const TS*)h->d_f, (const TS*)h->d_flink, S, \
-                                                                     h->d_mat, P, odd, nodes, count, (double*)u, stride); \
+                                                                     flow_mat(h), P, odd, nodes, count, (double*)u, stride); \
     else                                                                                                        \
         k_flow_velocity<TS, TC, float><<<grid, 256, 0, h->stream>>>((const TS*)h->d_f, (const TS*)h->d_flink, S,  \
-                                                                    h->d_mat, P, odd, nodes, count, (float*)u, stride);
+                                                                    flow_mat(h), P, odd, nodes, count, (float*)u, stride);
     switch (h->flow_prec) {
         case CLB_F64: CLB_VEL(double, double); break;
         case CLB_F32: CLB_VEL(float, float); break;

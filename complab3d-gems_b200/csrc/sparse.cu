@@ -20,8 +20,10 @@ static cudaError_t upload(T*& dst, const std::vector<T>& src, cudaStream_t s) {
     return cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, s);
 }
 
-clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, SparseBuffers& out) {
+clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, SparseBuffers& out,
+                        const std::vector<int8_t>* map) {
     sparse_free(out);
+    const std::vector<int8_t>& mat = map ? *map : h->h_mat;
     const Geom& G = h->g;
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const int64_t N = G.N;
@@ -42,7 +44,7 @@ clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, Spar
                 const int z = w * 32 + b;
                 if (z >= nz) break;
                 const int64_t n = (int64_t)r * nz + z;
-                const int8_t c = h->h_mat[n];
+                const int8_t c = mat[n];
                 if (stored_by_code[(uint8_t)c & 127]) {
                     m |= 1u << b;
                     idx[n] = K++;

@@ -59,7 +59,9 @@ __host__ __device__ constexpr int row4(int dx, int dy) {
 
 // Build on the host from the material map: a node is stored when stored_by_code[code] != 0.
 // q = 19 or 7 selects the velocity set of the wall masks.
-clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, SparseBuffers& out);
+// `map` (default: the handle's material map) gives the material of every voxel.
+clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, SparseBuffers& out,
+                        const std::vector<int8_t>* map = nullptr);
 void sparse_free(SparseBuffers& b);
 
 // rank of z in row r: stored nodes of the row below z, plus the row's start

@@ -50,10 +50,18 @@ typedef enum clb_law {
     CLB_LAW_NONE = 0,
     CLB_LAW_DECAY = 1,      /* params k[S]:          R_s = -k_s C_s                        */
     CLB_LAW_MONOD = 2,      /* params k[S], Ks[S]:   R_s = -k_s C_s / (Ks_s + C_s)           */
-    CLB_LAW_DUAL_MONOD = 3  /* params mu_max, Ks, Y, kd; microbe m grows on species 0 (donor)
+    CLB_LAW_DUAL_MONOD = 3, /* params mu_max, Ks, Y, kd; microbe m grows on species 0 (donor)
                                and species 1+m (acceptor):
                                growth = mu_max C0/(Ks+C0) Ca/(Ks+Ca) B_m,
                                R_B = growth - kd B_m, R_0 -= growth/Y, R_a -= growth/Y     */
+    /* abiotic laws (clb_set_abiotic_kinetics; defineAbioticRxnKinetics of the reference) */
+    CLB_LAW_PRECIP = 4,     /* params kp, a, b, p: A + B -> P(s), R = kp max(C_a,0) max(C_b,0),
+                               R_a = R_b = -R, R_p = +R (examples/13_precipitation)          */
+    CLB_LAW_MINERAL = 5     /* params k, log10 Ksp, p, nu[S]: saturation
+                               Omega = 10^(sum_{j != p} nu_j log10 C_j - log10 Ksp),
+                               R_p = k (Omega - 1), R_j = -nu_j R_p: the mineral p grows when the
+                               water is supersaturated and dissolves (clamped at what there
+                               is) when it is undersaturated                                 */
 } clb_law;
 
 #define CLB_MAX_MICROBES 8
@@ -199,6 +207,14 @@ clb_status clb_couple_velocity(clb_handle* h);
  * 406-497) with the clamp dC = max(R dt, -C). */
 clb_status clb_set_kinetics(clb_handle* h, int law, const double* params, int n_params, double dt);
 
+/* The abiotic rate law, evaluated after the biotic one on the concentrations it left
+ * (run_abiotic_kinetics, complab3d_processors_part1.hh:199-297; complab.cpp:2460-2525), with the
+ * same clamp dC = max(R dt, -C) and the time step of clb_set_kinetics. surface_only != 0 limits it
+ * to voxels with a solid or wall face neighbour (surfaceAbioticKinetics3D,
+ * precipitationVOP.hh:53-153). law: CLB_LAW_NONE, CLB_LAW_PRECIP or CLB_LAW_MINERAL; species
+ * indices in params are user species indices. */
+clb_status clb_set_abiotic_kinetics(clb_handle* h, int law, const double* params, int n_params, int surface_only);
+
 /* Biomass fields of the CA microbes, [n_microbes][N] float64. */
 clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass);
 
@@ -219,6 +235,55 @@ clb_status clb_reduce(clb_handle* h, clb_stats* out);
  * in time on one device (they would race on it). The first call on a device looks the buffer
  * up; make it before any stream capture begins. */
 clb_status clb_reduce_noalloc(clb_handle* h, clb_stats* out);
+
+/* ---------------------------------------------------------------- precipitation / dissolution */
+
+/* Dissolution law of a sealed mineral voxel (defineDissolutionRate of the reference). */
+typedef enum clb_dissolution_law {
+    CLB_DISSOL_NONE = 0,
+    CLB_DISSOL_FIRST_ORDER = 1, /* params kd, h, sigma[S]: rate = kd max(water_h,0) max(mineral,0)
+                                   (h < 0: no water factor); the mineral loses rate, species j
+                                   gains sigma_j rate (examples/15_precip_and_dissolution)    */
+    CLB_DISSOL_MINERAL = 2      /* params k, log10 Ksp, nu[S]: Omega of the water; below 1 the
+                                   mineral dissolves at k (1 - Omega), releasing nu_j times it */
+} clb_dissolution_law;
+
+/* <precipitation> and <dissolution> of CompLaB.xml with one precipitate phase. */
+typedef struct clb_precip_desc {
+    int32_t mineral_species;      /* immobile species holding the precipitate (user index)      */
+    double full_density;          /* max_precipRho: a voxel seals at mineral >= this            */
+    int32_t precip_code;          /* material code of sealed voxels; -1: the solid code         */
+    int32_t seal_flow;            /* 0: the flow lattice keeps its dynamics at sealed voxels, as
+                                     the reference's updateNsLatticesDynamics3D does (it skips
+                                     solid voxels, complab3d_processors_part2.hh:785-806);
+                                     1: sealed voxels become bounce-back on the flow lattice
+                                     (permeable IncBGK if seal_perm_ratio > 0) and the flow is
+                                     re-solved after every change                             */
+    double seal_perm_ratio;       /* <precipitation><perm_ratio>                               */
+    int32_t flow_max_iterations;  /* re-solve cap (ns_max_iT2)                                 */
+    double flow_eps;              /* re-solve convergence (ns_convergence_iT2)                 */
+    int32_t dissolution;          /* 1: sealed voxels dissolve and may reopen                   */
+    double reopen_fraction;       /* reopen below this fraction of full_density (0.9)           */
+    int32_t pore_code;            /* material of a reopened voxel; -1: the first pore code      */
+    int32_t dissolution_law;      /* clb_dissolution_law                                        */
+    double dissolution_params[CLB_MAX_SPECIES + 2];
+    int32_t dissolution_surface_only; /* 1: a voxel with no open face neighbour does not dissolve */
+} clb_precip_desc;
+
+/* Replaces: the <precipitation>/<dissolution> set-up of complab.cpp (phase lattice, precipitate
+ * phase). Dissolution, when on, runs inside every later clb_ade_step as the reference runs it in
+ * the abiotic block: surfaceDissolutionKinetics3D (dissolutionVOP.hh:379-605) parks the products
+ * per open face, dissolutionGather3D (:608-742) lets the open neighbours collect them. */
+clb_status clb_precip_setup(clb_handle* h, const clb_precip_desc* desc);
+
+/* The node conversions of one update interval: precipNodeConversion3D (precipitationVOP.hh:166-227)
+ * seals open voxels of x = 1..nx-2 whose mineral reached full_density, dissolNodeConversion3D
+ * (dissolutionVOP.hh:745-810) reopens sealed voxels below reopen_fraction x full_density. The
+ * species lattices switch dynamics there and keep their populations
+ * (updateSoluteSolidDynamics3D, complab3d_processors_part2.hh:585-647); with seal_flow the flow
+ * lattice does too and is re-solved, then its velocity is coupled again (complab.cpp:3139-3247).
+ * sealed / reopened (may be NULL) receive the voxel counts. */
+clb_status clb_geometry_update(clb_handle* h, int* sealed, int* reopened);
 
 /* ---------------------------------------------------------------- equilibrium speciation */
 

@@ -270,6 +270,12 @@ static void flow_collide_stream(OrcFlow* F) {
     F->iters += 1;
 }
 
+void orc_flow_set_material(OrcFlow* F, const int8_t* mat) { F->mat.assign(mat, mat + F->N); }
+void orc_flow_set_dynamics(OrcFlow* F, int code, int dyn, double omega) {
+    F->dyn[code & 255] = dyn;
+    F->omega[code & 255] = omega;
+}
+
 void orc_flow_step(OrcFlow* F, int n) {
     for (int k = 0; k < n; ++k) flow_collide_stream(F);
 }
@@ -343,7 +349,8 @@ void orc_flow_set_populations(OrcFlow* F, const double* in) {
 // =====================================================================================
 enum { ADE_BB = 0, ADE_NONE = 1, ADE_PORE = 2, ADE_BIO = 3 };
 enum { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_CLOSED = 2 };
-enum { LAW_NONE = 0, LAW_DECAY = 1, LAW_MONOD = 2, LAW_DUAL_MONOD = 3 };
+enum { LAW_NONE = 0, LAW_DECAY = 1, LAW_MONOD = 2, LAW_DUAL_MONOD = 3, LAW_PRECIP = 4, LAW_MINERAL = 5 };
+enum { DISSOL_NONE = 0, DISSOL_FIRST_ORDER = 1, DISSOL_MINERAL = 2 };
 
 struct OrcAde {
     int nx, ny, nz, S, M;
@@ -363,6 +370,15 @@ struct OrcAde {
     double dt = 1.0;
     long iters = 0;
     void* spec = nullptr;  // EqTableau of the speciation step, or none
+    // abiotic rate law (run_abiotic_kinetics / surfaceAbioticKinetics3D)
+    int law2 = LAW_NONE;
+    std::vector<double> prm2;
+    int surf = 0;
+    // precipitation sealing and dissolution (precipitationVOP.hh, dissolutionVOP.hh)
+    int pr_on = 0, sM = -1, pcode = 0, porecode = 2, dis_on = 0, dis_law = DISSOL_NONE, dis_surf = 1;
+    double full = 0, reopen = 0.9;
+    std::vector<double> dprm;
+    std::vector<uint8_t> stamp;  // 1 where the voxel was sealed by precipitation (phase id)
     size_t id(int x, int y, int z) const { return ((size_t)x * ny + y) * nz + z; }
     // the lattice dynamics of species s at node n
     int node_dyn(int s, int x, size_t n) const {
@@ -467,6 +483,208 @@ static void rates(const OrcAde* A, const double* C, const double* B, double* R, 
     }
 }
 
+/* abiotic laws:
+ *   LAW_PRECIP:  kp, a, b, p            A + B -> P,  R = kp max(C_a,0) max(C_b,0): R_a = R_b = -R, R_p = +R
+ *                                       (defineAbioticRxnKinetics of examples/13_precipitation)
+ *   LAW_MINERAL: k, log10 Ksp, p, nu[S] Omega = 10^(sum_j nu_j log10 C_j - log10 Ksp) over the dissolved
+ *                                       species j != p; R_p = k (Omega - 1), R_j = -nu_j R_p */
+static void rates2(const OrcAde* A, const double* C, double* R) {
+    const int S = A->S;
+    for (int s = 0; s < S; ++s) R[s] = 0;
+    const std::vector<double>& p = A->prm2;
+    if (A->law2 == LAW_PRECIP) {
+        const int a = (int)p[1], b = (int)p[2], q = (int)p[3];
+        const double r = p[0] * std::max(C[a], 0.0) * std::max(C[b], 0.0);
+        R[a] -= r;
+        R[b] -= r;
+        R[q] += r;
+    } else if (A->law2 == LAW_MINERAL) {
+        const int q = (int)p[2];
+        double la = 0;
+        for (int j = 0; j < S; ++j)
+            if (j != q && p[3 + j] != 0.0) la += p[3 + j] * std::log10(std::max(C[j], 1e-30));
+        const double rm = p[0] * (std::pow(10.0, la - p[1]) - 1.0);
+        R[q] += rm;
+        for (int j = 0; j < S; ++j)
+            if (j != q) R[j] -= p[3 + j] * rm;
+    }
+}
+
+/* dissolution laws of a sealed mineral voxel (defineDissolutionRate):
+ *   DISSOL_FIRST_ORDER: kd, h, sigma[S]  rate = kd max(water_h,0) max(mineral,0) (h < 0: no water factor);
+ *                                        mineral -rate, species j sigma_j rate (examples/15)
+ *   DISSOL_MINERAL:     k, log10 Ksp, nu[S]  Omega of the water; below 1 the mineral dissolves at
+ *                                        k (Omega - 1), releasing -nu_j times that */
+static void dissol_rate(const OrcAde* A, const double* water, double mineral, double* subsR, double& mR) {
+    const int S = A->S;
+    for (int s = 0; s < S; ++s) subsR[s] = 0;
+    mR = 0;
+    const std::vector<double>& p = A->dprm;
+    if (A->dis_law == DISSOL_FIRST_ORDER) {
+        const int h = (int)p[1];
+        const double rate = p[0] * (h >= 0 ? std::max(water[h], 0.0) : 1.0) * std::max(mineral, 0.0);
+        mR = -rate;
+        for (int j = 0; j < S; ++j) subsR[j] = p[2 + j] * rate;
+    } else if (A->dis_law == DISSOL_MINERAL) {
+        double la = 0;
+        for (int j = 0; j < S; ++j)
+            if (j != A->sM && p[2 + j] != 0.0) la += p[2 + j] * std::log10(std::max(water[j], 1e-30));
+        const double om = std::pow(10.0, la - p[1]);
+        if (om < 1.0) {
+            mR = p[0] * (om - 1.0);
+            for (int j = 0; j < S; ++j)
+                if (j != A->sM) subsR[j] = -p[2 + j] * mR;
+        }
+    }
+}
+
+static const int DLOC[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+
+// density of species s at voxel n as the processors see it between collide and stream
+static double dens_post(const OrcAde* A, int s, size_t n) {
+    if (!A->mobile[s]) return A->imm[s][n];
+    double c = 0;
+    for (int i = 0; i < Q7; ++i) c += A->gp[s][n * Q7 + i];
+    return c + 1.0;
+}
+
+/* The abiotic block of complab.cpp:2460-2525 after the biotic increments are applied: abiotic
+ * rates (with the clamp dC = max(R dt, -C)), dissolution of sealed mineral voxels parked per open
+ * face (surfaceDissolutionKinetics3D, dissolutionVOP.hh:379-605), gathered by the open neighbours
+ * with the headroom clamp (dissolutionGather3D, :608-742), all applied once
+ * (update_abiotic_rxnLattices, complab3d_processors_part1.hh:299-404). */
+static void abiotic_block(OrcAde* A) {
+    const int nx = A->nx, ny = A->ny, nz = A->nz, S = A->S;
+    const size_t N = A->N;
+    std::vector<double> dC((size_t)S * N, 0.0);
+    auto inbox = [&](int x, int y, int z) { return x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz; };
+    if (A->law2 != LAW_NONE) {
+#pragma omp parallel for schedule(static)
+        for (int x = 1; x < nx - 1; ++x) {
+            std::vector<double> C(S), R(S);
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    size_t n = A->id(x, y, z);
+                    if (!A->react[(uint8_t)A->mat[n]]) continue;
+                    if (A->surf) {
+                        bool iface = false;
+                        for (int d = 0; d < 6 && !iface; ++d) {
+                            int X = x + DLOC[d][0], Y = y + DLOC[d][1], Z = z + DLOC[d][2];
+                            if (!inbox(X, Y, Z)) continue;
+                            if (!A->react[(uint8_t)A->mat[A->id(X, Y, Z)]]) iface = true;
+                        }
+                        if (!iface) continue;
+                    }
+                    for (int s2 = 0; s2 < S; ++s2) {
+                        double c = dens_post(A, s2, n);
+                        C[s2] = c < THRD ? 0.0 : c;
+                    }
+                    rates2(A, C.data(), R.data());
+                    for (int s2 = 0; s2 < S; ++s2) {
+                        double d = R[s2] * A->dt;
+                        if (!(d > THRD || d < -THRD)) continue;
+                        if (d + C[s2] < 0.0) d = -C[s2];
+                        if (!(d > THRD || d < -THRD)) continue;
+                        dC[(size_t)s2 * N + n] += d;
+                    }
+                }
+        }
+    }
+    if (A->dis_on && A->sM >= 0) {
+        const int sM = A->sM;
+        // pass 1: park
+        std::vector<double> water(S), subsR(S);
+        for (int x = 1; x < nx - 1; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    size_t n = A->id(x, y, z);
+                    if (!A->stamp[n]) continue;
+                    const double mineral = A->imm[sM][n];
+                    if (!(mineral > THRD)) continue;
+                    int open[6], no = 0;
+                    for (int d = 0; d < 6; ++d) {
+                        int X = x + DLOC[d][0], Y = y + DLOC[d][1], Z = z + DLOC[d][2];
+                        if (X < 1 || X > nx - 2 || Y < 0 || Y > ny - 1 || Z < 0 || Z > nz - 1) continue;
+                        if (!A->react[(uint8_t)A->mat[A->id(X, Y, Z)]]) continue;
+                        open[no++] = d;
+                    }
+                    if (no == 0 && A->dis_surf) continue;
+                    for (int s2 = 0; s2 < S; ++s2) water[s2] = 0;
+                    if (no > 0) {
+                        for (int k = 0; k < no; ++k) {
+                            const int d = open[k];
+                            size_t m = A->id(x + DLOC[d][0], y + DLOC[d][1], z + DLOC[d][2]);
+                            for (int s2 = 0; s2 < S; ++s2) water[s2] += dens_post(A, s2, m);
+                        }
+                        for (int s2 = 0; s2 < S; ++s2) water[s2] /= (double)no;
+                    }
+                    for (int s2 = 0; s2 < S; ++s2)
+                        if (water[s2] < 0) water[s2] = 0;
+                    double mR;
+                    dissol_rate(A, water.data(), mineral, subsR.data(), mR);
+                    if (!(mR < 0)) continue;
+                    double dM = mR * A->dt;
+                    double scale = 1.0;
+                    const double maxRemove = 0.5 * mineral;
+                    if (-dM > maxRemove) scale = maxRemove / (-dM);
+                    dM *= scale;
+                    if (!(-dM > THRD)) continue;
+                    dC[(size_t)sM * N + n] += dM;
+                    if (no > 0)
+                        for (int s2 = 0; s2 < S; ++s2) {
+                            if (s2 == sM) continue;
+                            const double rel = subsR[s2] * A->dt * scale;
+                            if (std::fabs(rel) <= THRD) continue;
+                            dC[(size_t)s2 * N + n] += rel / (double)no;
+                        }
+                }
+        // pass 2: gather
+        for (int x = 1; x < nx - 1; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    size_t n = A->id(x, y, z);
+                    if (!A->react[(uint8_t)A->mat[n]]) continue;
+                    for (int d = 0; d < 6; ++d) {
+                        int X = x + DLOC[d][0], Y = y + DLOC[d][1], Z = z + DLOC[d][2];
+                        if (X < 1 || X > nx - 2 || Y < 0 || Y > ny - 1 || Z < 0 || Z > nz - 1) continue;
+                        size_t m = A->id(X, Y, Z);
+                        if (!A->stamp[m]) continue;
+                        for (int s2 = 0; s2 < S; ++s2) {
+                            if (s2 == sM) continue;
+                            const double share = dC[(size_t)s2 * N + m];
+                            if (std::fabs(share) <= 1e-14) continue;
+                            double give = share;
+                            if (give < 0) {
+                                const double have = dens_post(A, s2, n);
+                                const double head = (have > 0 ? have : 0.0) + dC[(size_t)s2 * N + n];
+                                if (give + head < 0) give = -head;
+                                if (give > 0) give = 0;
+                            }
+                            if (!(std::fabs(give) > 1e-14)) continue;
+                            dC[(size_t)s2 * N + n] += give;
+                        }
+                    }
+                }
+    }
+    // apply
+#pragma omp parallel for schedule(static)
+    for (int x = 1; x < nx - 1; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = A->id(x, y, z);
+                const bool open = A->react[(uint8_t)A->mat[n]];
+                for (int s2 = 0; s2 < S; ++s2) {
+                    if (!open && A->mobile[s2]) continue;
+                    const double d = dC[(size_t)s2 * N + n];
+                    if (!(d > THRD || d < -THRD)) continue;
+                    if (A->mobile[s2])
+                        for (int i = 0; i < Q7; ++i) A->gp[s2][n * Q7 + i] += d * T7[i];
+                    else
+                        A->imm[s2][n] += d;
+                }
+            }
+}
+
 static void apply_speciation(OrcAde* A);
 
 static void ade_step(OrcAde* A) {
@@ -556,6 +774,7 @@ static void ade_step(OrcAde* A) {
                 }
         }
     }
+    if (A->law2 != LAW_NONE || (A->dis_on && A->sM >= 0)) abiotic_block(A);
     // ---- speciation on the post-kinetics populations (complab.cpp:2564-2569)
     if (A->spec) apply_speciation(A);
     // ---- 3. stream, then the Neumann planes take the inner neighbour's density
@@ -634,6 +853,63 @@ void orc_ade_biomass(OrcAde* A, double* out) {
 }
 
 void orc_ade_set_velocity(OrcAde* A, const double* u) { A->u.assign(u, u + 3 * A->N); }
+
+void orc_ade_set_abiotic(OrcAde* A, int law, const double* prm, int nprm, int surface_only) {
+    A->law2 = law;
+    A->prm2.assign(prm, prm + nprm);
+    A->surf = surface_only;
+}
+
+void orc_ade_set_precip(OrcAde* A, int mineral, double full, int precip_code, int dissolution, double reopen,
+                        int pore_code, int dis_law, const double* dprm, int ndprm, int dis_surface_only) {
+    A->pr_on = 1;
+    A->sM = mineral;
+    A->full = full;
+    A->pcode = precip_code;
+    A->dis_on = dissolution;
+    A->reopen = reopen;
+    A->porecode = pore_code;
+    A->dis_law = dis_law;
+    A->dprm.assign(dprm, dprm + ndprm);
+    A->dis_surf = dis_surface_only;
+    if (A->stamp.size() != A->N) A->stamp.assign(A->N, 0);
+}
+
+/* precipNodeConversion3D over Box3D(1, nx-2, ...) (precipitationVOP.hh:166-227, complab.cpp:3139-3146)
+ * then, with dissolution, dissolNodeConversion3D (dissolutionVOP.hh:745-810). A voxel that changes
+ * material changes dynamics on every species lattice (updateSoluteSolidDynamics3D) and keeps its
+ * populations. Returns the number of voxels sealed and reopened. */
+void orc_ade_geometry_update(OrcAde* A, int* sealed, int* reopened) {
+    int ns = 0, nr = 0;
+    const int nx = A->nx, ny = A->ny, nz = A->nz;
+    for (int x = 1; x < nx - 1; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = A->id(x, y, z);
+                if (!A->react[(uint8_t)A->mat[n]]) continue;
+                if (A->imm[A->sM][n] >= A->full) {
+                    A->mat[n] = (int8_t)A->pcode;
+                    A->stamp[n] = 1;
+                    ++ns;
+                }
+            }
+    if (A->dis_on)
+        for (int x = 1; x < nx - 1; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    size_t n = A->id(x, y, z);
+                    if (!A->stamp[n]) continue;
+                    if (A->imm[A->sM][n] < A->reopen * A->full) {
+                        A->mat[n] = (int8_t)A->porecode;
+                        A->stamp[n] = 0;
+                        ++nr;
+                    }
+                }
+    *sealed = ns;
+    *reopened = nr;
+}
+
+void orc_ade_material(OrcAde* A, int8_t* out) { std::copy(A->mat.begin(), A->mat.end(), out); }
 
 }  // extern "C"
 

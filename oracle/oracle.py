@@ -54,6 +54,12 @@ def lib():
             "orc_ade_biomass": ([vp, vp], None), "orc_ade_set_velocity": ([vp, vp], None),
             "orc_eq_nr": ([ip, ip, vp, vp, vp, dp, ip, vp, vp, vp], ip),
             "orc_ade_set_speciation": ([vp, ip, ip, vp, vp, vp, dp, ip], None),
+            "orc_ade_set_abiotic": ([vp, ip, vp, ip, ip], None),
+            "orc_ade_set_precip": ([vp, ip, dp, ip, ip, dp, ip, ip, vp, ip, ip], None),
+            "orc_ade_geometry_update": ([vp, vp, vp], None),
+            "orc_ade_material": ([vp, vp], None),
+            "orc_flow_set_material": ([vp, vp], None),
+            "orc_flow_set_dynamics": ([vp, ip, ip, dp], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -144,6 +150,13 @@ class OracleFlow:
         f = np.ascontiguousarray(f, dtype=np.float64)
         lib().orc_flow_set_populations(self.h, _p(f))
 
+    def set_material(self, mat):
+        self._mat = np.ascontiguousarray(mat, dtype=np.int8)
+        lib().orc_flow_set_material(self.h, _p(self._mat))
+
+    def set_dynamics(self, code, dyn, omega):
+        lib().orc_flow_set_dynamics(self.h, int(code), int(dyn), float(omega))
+
 
 class OracleAde:
     def __init__(self, mat, nx, ny, nz, species, u, solid_code=0, bounce_back_code=1, bio_codes=()):
@@ -185,11 +198,37 @@ class OracleAde:
         self.M = b.size // self.N
         lib().orc_ade_set_biomass(self.h, self.M, _p(b))
 
+    def set_velocity(self, u):
+        self._keep[11] = np.ascontiguousarray(u, dtype=np.float64).reshape(-1)
+        lib().orc_ade_set_velocity(self.h, _p(self._keep[11]))
+
     def set_speciation(self, stoich, logK, comp, tol=1e-10, max_it=200):
         S = np.ascontiguousarray(stoich, dtype=np.float64)
         self._spec = [S, np.ascontiguousarray(logK, dtype=np.float64), np.ascontiguousarray(comp, dtype=np.int32)]
         lib().orc_ade_set_speciation(self.h, S.shape[0], S.shape[1], _p(self._spec[0]), _p(self._spec[1]),
                                      _p(self._spec[2]), tol, max_it)
+
+    def set_abiotic(self, law, params, surface_only=0):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        self._prm2 = p
+        lib().orc_ade_set_abiotic(self.h, law, _p(p), p.size, int(surface_only))
+
+    def set_precip(self, mineral, full, precip_code=0, dissolution=0, reopen=0.9, pore_code=2, dis_law=0,
+                   dis_params=(), dis_surface_only=1):
+        d = np.ascontiguousarray(dis_params if len(dis_params) else [0.0], dtype=np.float64)
+        self._dprm = d
+        lib().orc_ade_set_precip(self.h, int(mineral), float(full), int(precip_code), int(dissolution),
+                                 float(reopen), int(pore_code), int(dis_law), _p(d), d.size, int(dis_surface_only))
+
+    def geometry_update(self):
+        a, b = C.c_int(), C.c_int()
+        lib().orc_ade_geometry_update(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def material(self):
+        m = np.empty(self.N, dtype=np.int8)
+        lib().orc_ade_material(self.h, _p(m))
+        return m
 
     def step(self, n=1):
         lib().orc_ade_step(self.h, n)
