@@ -24,6 +24,7 @@ LAW_PRECIP, LAW_MINERAL = 4, 5  # abiotic laws
 DISSOL_NONE, DISSOL_FIRST_ORDER, DISSOL_MINERAL = 0, 1, 2
 FIELD_MATERIAL, FIELD_FLOW_VELOCITY, FIELD_FLOW_POPULATIONS = 0, 1, 2
 FIELD_CONCENTRATION, FIELD_ADE_POPULATIONS, FIELD_BIOMASS, FIELD_ADE_VELOCITY = 3, 4, 5, 6
+FIELD_CA_TOTAL, FIELD_CA_AGE = 7, 8
 
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "NOT_CONVERGED", 3: "NONFINITE", 4: "PERCOLATION_LOST",
           5: "CUDA_ERROR", 6: "TIMEOUT", 7: "NOT_INITIALIZED", 8: "OUT_OF_MEMORY"}
@@ -88,6 +89,10 @@ class PrecipDesc(C.Structure):
                 ("dissolution_params", C.c_double * (MAX_SPECIES + 2)), ("dissolution_surface_only", C.c_int32)]
 
 
+class CaDesc(C.Structure):
+    _fields_ = [("max_biomass", C.c_double), ("biofilm_fraction", C.c_double), ("seed", C.c_uint64)]
+
+
 class SpeciationStats(C.Structure):
     _fields_ = [("solves", C.c_int64), ("converged", C.c_int64), ("surrogate_used", C.c_int64),
                 ("fallbacks", C.c_int64), ("iterations", C.c_int64)]
@@ -130,6 +135,9 @@ SIGNATURES = {
     "clb_reduce": [C.c_void_p, C.POINTER(Stats)],
     "clb_reduce_noalloc": [C.c_void_p, C.POINTER(Stats)],
     "clb_set_abiotic_kinetics": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int],
+    "clb_ca_setup": [C.c_void_p, C.POINTER(CaDesc)],
+    "clb_ca_step": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "clb_refresh_dynamics": [C.c_void_p, C.c_int, C.c_int],
     "clb_precip_setup": [C.c_void_p, C.POINTER(PrecipDesc)],
     "clb_geometry_update": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "clb_speciation_setup": [C.c_void_p, C.POINTER(SpeciationDesc)],
@@ -366,6 +374,31 @@ class Domain:
         if not (allow_unconverged and st == 2):
             self._check(st)
         return a.value, b.value
+
+    def ca_setup(self, max_biomass, biofilm_fraction, seed):
+        d = CaDesc(float(max_biomass), float(biofilm_fraction), int(seed))
+        self._check(lib().clb_ca_setup(self.h, C.byref(d)))
+
+    def ca_step(self, allow_stall=False):
+        """One iteration's biofilm automaton; returns (status, sweeps, mask_changed)."""
+        a, b = C.c_int(), C.c_int()
+        st = lib().clb_ca_step(self.h, C.byref(a), C.byref(b))
+        if not (allow_stall and st == 2):
+            self._check(st)
+        return st, a.value, bool(b.value)
+
+    def refresh_dynamics(self, species=True, flow=True):
+        self._check(lib().clb_refresh_dynamics(self.h, int(species), int(flow)))
+
+    def ca_total(self):
+        t = np.empty(self.N)
+        self._check(lib().clb_get_field(self.h, FIELD_CA_TOTAL, 0, _ptr(t), 0))
+        return t
+
+    def ca_age(self):
+        a = np.empty(self.N)
+        self._check(lib().clb_get_field(self.h, FIELD_CA_AGE, 0, _ptr(a), 0))
+        return a.astype(np.int64)
 
     def material(self):
         m = np.empty(self.N, dtype=np.int8)

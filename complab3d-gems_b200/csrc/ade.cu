@@ -392,6 +392,7 @@ void ade_free(clb_handle* h) {
     cudaFree(h->d_u); h->d_u = nullptr;
     cudaFree(h->d_neu); h->d_neu = nullptr;
     precip_free(h);
+    ca_free(h);
     sparse_free(h->ade_sp);
     h->ade_ready = false;
 }

@@ -274,6 +274,24 @@ clb_status clb_geometry_update(clb_handle* h, int* sealed, int* reopened) {
     return geometry_update(h, sealed, reopened);
 }
 
+clb_status clb_ca_setup(clb_handle* h, const clb_ca_desc* desc) {
+    if (!h || !desc) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return ca_setup(h, desc);
+}
+
+clb_status clb_ca_step(clb_handle* h, int* sweeps, int* mask_changed) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    return ca_step(h, sweeps, mask_changed);
+}
+
+clb_status clb_refresh_dynamics(clb_handle* h, int species, int flow) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    return refresh_dynamics(h, species, flow);
+}
+
 clb_status clb_reduce_noalloc(clb_handle* h, clb_stats* out) {
     if (!h || !out) return fail(h, CLB_INVALID_ARG, "null argument");
     CLB_ON_DEVICE(h);
@@ -368,6 +386,8 @@ clb_status clb_get_field(clb_handle* h, int field, int index, void* host, int dt
         case CLB_FIELD_ADE_POPULATIONS: return ade_populations(h, index, (double*)host);
         case CLB_FIELD_BIOMASS: return ade_biomass(h, index, (double*)host);
         case CLB_FIELD_ADE_VELOCITY: return ade_velocity(h, (double*)host);
+        case CLB_FIELD_CA_TOTAL: return ca_fields(h, 0, (double*)host);
+        case CLB_FIELD_CA_AGE: return ca_fields(h, 1, (double*)host);
         default: return fail(h, CLB_INVALID_ARG, "unknown field");
     }
 }

@@ -1,0 +1,698 @@
+// biofilm_ca.cu -- the biofilm cellular automaton: excess biomass pushed to face neighbours
+// ('fraction' mode), the mask / total-biomass update and the age wavefront, on the GPU with the
+// same results as the sequential lexicographic algorithm.
+//
+// Reference behaviour (complab.cpp:2792-3055 and :3074-3079):
+//   updateLocalMaskNtotalLattices3D (complab3d_processors_part2.hh:71-259): the total biomass of
+//     every open voxel (species above 1e-14), pore -> biofilm at thrd_bFilmFrac x Bmax (the mask
+//     becomes the sum of the present microbes' codes), biofilm -> pore below it;
+//   while max(total) exceeds Bmax: pushExcessBiomass3D (complab3d_processors_part1.hh:499-732)
+//     over the voxels in lexicographic order: the excess goes to the face neighbours in a random
+//     order, each taking up to its room (Bmax - its total, a pore neighbour counting as empty),
+//     split over the microbes in proportion; what is left goes to one neighbour chosen among
+//     those with a lower age (else any); then the mask / total update; every 50 sweeps the age
+//     relaxation (updateAgeDistance3D, part2.hh:840-965) until no age changes; a sweep that does
+//     not lower the maximum for 100 sweeps in a row, or more than 1000 sweeps, is a failure;
+//   after the block, if the mask changed, one age sweep.
+// A single-block run never takes the push's block-boundary path, so the copy lattices and
+// pullExcessBiomass3D (part1.hh:973-1150) have no effect there and are not built.
+//
+// Random choices: the reference draws from std::random_shuffle / std::rand seeded by the clock.
+// Here voxel n of push sweep w draws from splitmix64 steps started at
+// seed ^ (w * 0x9E3779B97F4A7C15) ^ (n * 0xD1B54A32D192ED03) (shuffle: Fisher-Yates from the top,
+// draw % (i + 1); pick: draw % L), so a run is reproducible and the draws do not depend on the
+// order in which voxels are processed.
+//
+// Parallel schedule with sequential results. In a sweep the only state a voxel's push reads that
+// another voxel's push writes is its own per-microbe biomass, which its lexicographically earlier
+// face neighbours (x-1, y-1, z-1) may have pushed into. Every other input (totals, masks, ages)
+// is fixed during the sweep. So the active voxels are processed in rounds: a voxel runs once its
+// earlier active neighbours have run, starting from its biomass plus their pushes into it (added
+// in their lexicographic order), and records its pushes instead of writing them; a final pass
+// adds to every voxel the pushes it received, in the order the sequential sweep adds them. The
+// results are bit-identical to the sequential sweep.
+//
+// The age sweep after a mask change is one in-place lexicographic sweep: it runs as wavefronts
+// over x + y + z, each voxel seeing its earlier neighbours updated and its later ones not. The
+// relaxation to convergence runs as Jacobi sweeps: the update is monotone and only ever raises an
+// age, so Jacobi and the in-place sweeps reach the same least fixed point.
+#include "sparse.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace clb {
+
+constexpr int CA_THREADS = 256;
+constexpr int CA_REC = 7;  // push records per voxel: up to six neighbours plus the remainder
+
+struct CaView {
+    Geom g;
+    double bmax, thr;        // Bmax, thrd_bFilmFrac x Bmax
+    int M;
+    int bb, solid;
+    int n_pore;
+    int pore[CLB_MAX_PORE_CODES];
+    int bio_code[CLB_MAX_MICROBES];
+};
+
+__device__ __forceinline__ bool ca_open(const CaView& C, int m) { return m != C.bb && m != C.solid; }
+__device__ __forceinline__ bool ca_pore(const CaView& C, int m) {
+    for (int i = 0; i < C.n_pore; ++i)
+        if (m == C.pore[i]) return true;
+    return false;
+}
+__device__ __forceinline__ uint64_t sm64(uint64_t& x) {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+// doubles ordered as signed 64-bit integers (for atomicMax)
+__device__ __forceinline__ long long ordered(double v) {
+    long long i = __double_as_longlong(v);
+    return i < 0 ? i ^ 0x7FFFFFFFFFFFFFFFLL : i;
+}
+static double unordered(long long i) {
+    if (i < 0) i ^= 0x7FFFFFFFFFFFFFFFLL;
+    double v;
+    std::memcpy(&v, &i, sizeof v);
+    return v;
+}
+
+struct CaScalars {
+    long long gmax;        // ordered bits of max(total)
+    long long mask_sum;
+    unsigned int active;   // voxels collected for the sweep
+    unsigned int remaining;
+    unsigned int changed;  // ages changed by a sweep
+    unsigned int overflow; // active voxels beyond the capacity
+};
+
+// ------------------------------------------------------------------ set-up and mask update
+
+__global__ void k_ca_init(const CaView C, const int8_t* __restrict__ mat, const double* __restrict__ bio,
+                          double* __restrict__ total, int* __restrict__ age, int8_t* __restrict__ distp,
+                          int* __restrict__ aidx, CaScalars* sc) {
+    const Geom G = C.g;
+    long long msum = 0;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, z;
+        decode(G, n, x, y, z);
+        double t = 0.0;
+        for (int m = 0; m < C.M; ++m) t += bio[(int64_t)m * G.N + n];
+        total[n] = t;
+        const int mk = mat[n];
+        msum += mk;
+        age[n] = !ca_open(C, mk) ? -1 : (ca_pore(C, mk) ? 0 : 1);
+        distp[n] = (ca_open(C, mk) && x < G.nx - 1 && y < G.ny - 1 && z < G.nz - 1) ? 1 : 0;
+        aidx[n] = -1;
+    }
+    atomicAdd((unsigned long long*)&sc->mask_sum, (unsigned long long)msum);
+}
+
+// updateLocalMaskNtotalLattices3D; with several pore codes a reopened voxel copies the first
+// pore neighbour found in `mask_before` (the mask as it stood before the pass).
+__global__ void k_ca_mask_total(const CaView C, int8_t* __restrict__ mat, const int8_t* __restrict__ mask_before,
+                                const double* __restrict__ bio, double* __restrict__ total, CaScalars* sc) {
+    const Geom G = C.g;
+    long long best = LLONG_MIN, msum = 0;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
+        const int mk = mat[n];
+        if (ca_open(C, mk)) {
+            double bmass = 0.0;
+            int newmask = 0;
+            for (int m = 0; m < C.M; ++m) {
+                const double bm = bio[(int64_t)m * G.N + n];
+                if (bm > 1e-14) {
+                    bmass += bm;
+                    newmask += C.bio_code[m];
+                }
+            }
+            if (fabs(bmass - total[n]) > 1e-14) total[n] = bmass;
+            const bool poreflag = ca_pore(C, mk);
+            int out = mk;
+            if (!poreflag && bmass < C.thr) {
+                out = C.pore[0];
+                if (C.n_pore > 1) {
+                    int x, y, z;
+                    decode(G, n, x, y, z);
+                    const int d6[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+                    for (int d = 0; d < 6; ++d) {
+                        const int X = x + d6[d][0], Y = y + d6[d][1], Z = z + d6[d][2];
+                        if (X < 0 || Y < 0 || Z < 0 || X >= G.nx || Y >= G.ny || Z >= G.nz) continue;
+                        const int nm = mask_before[(int64_t)X * G.plane + (int64_t)Y * G.nz + Z];
+                        if (ca_open(C, nm) && ca_pore(C, nm)) { out = nm; break; }
+                    }
+                }
+            } else if (poreflag && bmass >= C.thr && newmask > 0) {
+                out = newmask;
+            }
+            if (out != mk) mat[n] = (int8_t)out;
+            msum += out;
+        } else {
+            msum += mk;
+        }
+        best = max(best, ordered(total[n]));
+    }
+    // block reduction, then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) {
+        best = max(best, __shfl_down_sync(0xffffffffu, best, o));
+        msum += __shfl_down_sync(0xffffffffu, msum, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&sc->gmax, best);
+        atomicAdd((unsigned long long*)&sc->mask_sum, (unsigned long long)msum);
+    }
+}
+
+// ------------------------------------------------------------------ push sweep
+
+__global__ void k_ca_collect(const CaView C, const int8_t* __restrict__ mat, const double* __restrict__ total,
+                             int* __restrict__ aidx, int* __restrict__ act, int* __restrict__ done, int cap,
+                             CaScalars* sc) {
+    const Geom G = C.g;
+    const int64_t lo = G.plane, hi = G.N - G.plane;  // x = 1..nx-2
+    for (int64_t n = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += (int64_t)gridDim.x * blockDim.x) {
+        if (!ca_open(C, mat[n])) continue;
+        const double t = total[n];
+        if (!(t > C.bmax) || !(t - C.bmax > THRD)) continue;
+        const unsigned int i = atomicAdd(&sc->active, 1u);
+        if ((int)i >= cap) { atomicAdd(&sc->overflow, 1u); continue; }
+        act[i] = (int)n;
+        aidx[n] = (int)i;
+        done[i] = 0;
+    }
+}
+
+// the pushes source j recorded into voxel n, added in record order
+__device__ __forceinline__ void add_records(const CaView& C, int j, int64_t n, const int* __restrict__ tgt,
+                                            const double* __restrict__ amt, double* b) {
+    for (int t = 0; t < CA_REC; ++t) {
+        if (tgt[j * CA_REC + t] != (int)n) continue;
+        for (int m = 0; m < C.M; ++m) b[m] += amt[((int64_t)j * CA_REC + t) * C.M + m];
+    }
+}
+
+__global__ void k_ca_round(const CaView C, const int8_t* __restrict__ mat, const double* __restrict__ total,
+                           const int* __restrict__ age, const double* __restrict__ bio, const int* __restrict__ aidx,
+                           const int* __restrict__ act, int* __restrict__ done, int* __restrict__ tgt,
+                           double* __restrict__ amt, double* __restrict__ own, int count, int round, uint64_t seed,
+                           uint64_t sweep, CaScalars* sc) {
+    const Geom G = C.g;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        if (done[i]) continue;
+        const int64_t n = act[i];
+        int x, y, z;
+        decode(G, n, x, y, z);
+        // sources that push before this voxel in lexicographic order: x-1, y-1, z-1
+        int pre[3] = {-1, -1, -1};
+        if (x > 1) pre[0] = aidx[n - G.plane];
+        if (y > 0) pre[1] = aidx[n - G.nz];
+        if (z > 0) pre[2] = aidx[n - 1];
+        bool ready = true;
+        for (int q = 0; q < 3; ++q)
+            if (pre[q] >= 0) {
+                const int dq = done[pre[q]];
+                if (dq == 0 || dq == round) ready = false;
+            }
+        if (!ready) continue;
+        double b[CLB_MAX_MICROBES];
+        for (int m = 0; m < C.M; ++m) b[m] = bio[(int64_t)m * G.N + n];
+        for (int q = 0; q < 3; ++q)
+            if (pre[q] >= 0) add_records(C, pre[q], n, tgt, amt, b);
+        for (int t = 0; t < CA_REC; ++t) tgt[i * CA_REC + t] = -1;
+        double bMt = total[n];
+        double bMd = bMt - C.bmax;
+        int64_t nb[6];
+        int L = 0;
+        const int d6[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        for (int d = 0; d < 6; ++d) {
+            const int X = x + d6[d][0], Y = y + d6[d][1], Z = z + d6[d][2];
+            if (X < 1 || X > G.nx - 2 || Y < 0 || Y >= G.ny || Z < 0 || Z >= G.nz) continue;
+            const int64_t m = (int64_t)X * G.plane + (int64_t)Y * G.nz + Z;
+            if (!ca_open(C, mat[m])) continue;
+            nb[L++] = m;
+        }
+        uint64_t st = seed ^ (sweep * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)n * 0xD1B54A32D192ED03ULL);
+        int perm[6] = {0, 1, 2, 3, 4, 5};
+        if (L > 1)
+            for (int a = L - 1; a >= 1; --a) {
+                const int j = (int)(sm64(st) % (uint64_t)(a + 1));
+                const int tmp = perm[a];
+                perm[a] = perm[j];
+                perm[j] = tmp;
+            }
+        int rec = 0;
+        bool chk = false;
+        for (int t = 0; t < L; ++t) {
+            const int64_t m = nb[L > 1 ? perm[t] : 0];
+            const double nbrbMt = ca_pore(C, mat[m]) ? 0.0 : total[m];
+            if (nbrbMt < C.bmax) {
+                const double hold = C.bmax - nbrbMt;
+                double partial = bMd;
+                if (bMd > hold) { partial = hold; bMd -= hold; }
+                else { bMd = 0.0; chk = true; }
+                tgt[i * CA_REC + rec] = (int)m;
+                for (int mi = 0; mi < C.M; ++mi) {
+                    const double shove = b[mi] / bMt * partial;
+                    double give = 0.0;
+                    if (shove > THRD) {
+                        b[mi] -= shove;
+                        give = shove;
+                    }
+                    amt[((int64_t)i * CA_REC + rec) * C.M + mi] = give;
+                }
+                ++rec;
+                bMt -= partial;
+            }
+            if (chk) break;
+        }
+        if (!chk && L > 0) {
+            const int id0 = age[n];
+            int64_t cand[6];
+            int c = 0;
+            for (int t = 0; t < L; ++t)
+                if (id0 > age[nb[t]]) cand[c++] = nb[t];
+            int64_t m;
+            if (c > 1) m = cand[sm64(st) % (uint64_t)c];
+            else if (c == 1) m = cand[0];
+            else m = nb[L > 1 ? (int)(sm64(st) % (uint64_t)L) : 0];
+            tgt[i * CA_REC + rec] = (int)m;
+            for (int mi = 0; mi < C.M; ++mi) {
+                const double shove = b[mi] / bMt * bMd;
+                b[mi] -= shove;
+                amt[((int64_t)i * CA_REC + rec) * C.M + mi] = shove;
+            }
+        }
+        for (int m = 0; m < C.M; ++m) own[(int64_t)i * C.M + m] = b[m];
+        done[i] = round;
+        atomicSub(&sc->remaining, 1u);
+    }
+}
+
+// every voxel takes the pushes it received, in the order the sequential sweep adds them
+__global__ void k_ca_apply(const CaView C, double* __restrict__ bio, const int* __restrict__ aidx,
+                           const int* __restrict__ tgt, const double* __restrict__ amt, const double* __restrict__ own) {
+    const Geom G = C.g;
+    const int64_t lo = G.plane, hi = G.N - G.plane;
+    for (int64_t n = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, z;
+        decode(G, n, x, y, z);
+        const int a = aidx[n];
+        int pre[3] = {-1, -1, -1}, post[3] = {-1, -1, -1};
+        if (x > 1) pre[0] = aidx[n - G.plane];
+        if (y > 0) pre[1] = aidx[n - G.nz];
+        if (z > 0) pre[2] = aidx[n - 1];
+        if (z < G.nz - 1) post[0] = aidx[n + 1];
+        if (y < G.ny - 1) post[1] = aidx[n + G.nz];
+        if (x < G.nx - 2) post[2] = aidx[n + G.plane];
+        if (a < 0 && pre[0] < 0 && pre[1] < 0 && pre[2] < 0 && post[0] < 0 && post[1] < 0 && post[2] < 0) continue;
+        double b[CLB_MAX_MICROBES];
+        if (a >= 0) {
+            for (int m = 0; m < C.M; ++m) b[m] = own[(int64_t)a * C.M + m];
+        } else {
+            for (int m = 0; m < C.M; ++m) b[m] = bio[(int64_t)m * G.N + n];
+            for (int q = 0; q < 3; ++q)
+                if (pre[q] >= 0) add_records(C, pre[q], n, tgt, amt, b);
+        }
+        for (int q = 0; q < 3; ++q)
+            if (post[q] >= 0) add_records(C, post[q], n, tgt, amt, b);
+        for (int m = 0; m < C.M; ++m) bio[(int64_t)m * G.N + n] = b[m];
+    }
+}
+
+__global__ void k_ca_clear(int* __restrict__ aidx, const int* __restrict__ act, int count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) aidx[act[i]] = -1;
+}
+
+// ------------------------------------------------------------------ age wavefront
+
+// new age of voxel n from the ages it sees (updateAgeDistance3D); returns the old age when unchanged
+__device__ __forceinline__ int age_rule(const CaView& C, int64_t n, const int* __restrict__ age,
+                                        const int8_t* __restrict__ distp, const double* __restrict__ total) {
+    const Geom G = C.g;
+    const int a = age[n];
+    const double B = total[n];
+    if (!(B > 1e-14)) return a;
+    int x, y, z;
+    decode(G, n, x, y, z);
+    int64_t D[6];
+    int nd = 0;
+    const int d6[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    for (int d = 0; d < 6; ++d) {
+        const int X = x + d6[d][0], Y = y + d6[d][1], Z = z + d6[d][2];
+        if (X < 0 || Y < 0 || Z < 0 || X >= G.nx || Y >= G.ny || Z >= G.nz) continue;
+        const int64_t m = (int64_t)X * G.plane + (int64_t)Y * G.nz + Z;
+        if (distp[m]) D[nd++] = m;
+    }
+    if (a == 0) return 1;
+    if (a == 1 && (B - C.bmax) > -1e-14) {
+        for (int t = 0; t < nd; ++t)
+            if (age[D[t]] == 0) return a;
+        return 2;
+    }
+    int cnt = 0;
+    for (int t = 0; t < nd; ++t)
+        if (age[D[t]] >= a && (total[D[t]] - C.bmax) > -1e-14) ++cnt;
+    return cnt == nd ? a + 1 : a;
+}
+
+__global__ void k_age_jacobi(const CaView C, const int* __restrict__ in, int* __restrict__ out,
+                             const int8_t* __restrict__ distp, const double* __restrict__ total, CaScalars* sc) {
+    unsigned int ch = 0;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < C.g.N; n += (int64_t)gridDim.x * blockDim.x) {
+        const int v = age_rule(C, n, in, distp, total);
+        out[n] = v;
+        ch += v != in[n];
+    }
+    for (int o = 16; o > 0; o >>= 1) ch += __shfl_down_sync(0xffffffffu, ch, o);
+    if ((threadIdx.x & 31) == 0 && ch) atomicAdd(&sc->changed, ch);
+}
+
+// voxels with x + y + z = level, in place
+__global__ void k_age_level(const CaView C, int* __restrict__ age, const int8_t* __restrict__ distp,
+                            const double* __restrict__ total, int level) {
+    const Geom G = C.g;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)G.nx * G.ny;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(t / G.ny), y = (int)(t - (int64_t)x * G.ny);
+        const int z = level - x - y;
+        if (z < 0 || z >= G.nz) continue;
+        const int64_t n = (int64_t)x * G.plane + (int64_t)y * G.nz + z;
+        age[n] = age_rule(C, n, age, distp, total);
+    }
+}
+
+// ------------------------------------------------------------------ dynamics refresh
+
+// updateSoluteDynamics3D: open voxels take the pore or the biofilm dynamics from the mask
+__global__ void k_refresh_species(int8_t* __restrict__ code, const int32_t* __restrict__ node, int64_t K,
+                                  const int8_t* __restrict__ mat, const CaView C, int bio0) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
+        const int m = mat[node[k]];
+        if (!ca_open(C, m)) continue;
+        code[k] = (int8_t)(ca_pore(C, m) ? m : bio0);
+    }
+}
+
+// updateNsLatticesDynamics3D (complab3d_processors_part2.hh:785-806): a biofilm voxel with the
+// pore dynamics takes the biofilm dynamics of the first microbe, a pore voxel with any other
+// dynamics the pore dynamics; solid and wall voxels keep theirs.
+__global__ void k_refresh_flow_map(int8_t* __restrict__ fmat, const int8_t* __restrict__ mat, const CaView C,
+                                   const FlowParams F, double pore_omega, int bio0) {
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < C.g.N; n += (int64_t)gridDim.x * blockDim.x) {
+        const int m = mat[n];
+        if (!ca_open(C, m)) continue;
+        const int prev = fmat[n];
+        const bool pore_dyn = F.dyn[prev & 127] == DYN_BGK && fabs(F.omega[prev & 127] - pore_omega) < 1e-14;
+        if (ca_pore(C, m)) {
+            if (!pore_dyn) fmat[n] = (int8_t)m;
+        } else if (pore_dyn && bio0 >= 0) {
+            fmat[n] = (int8_t)bio0;
+        }
+    }
+}
+
+__global__ void k_codes_from_map(int8_t* __restrict__ code, const int32_t* __restrict__ node, int64_t K,
+                                 const int8_t* __restrict__ map) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
+        code[k] = map[node[k]];
+}
+
+// ------------------------------------------------------------------ host side
+
+static CaScalars* SC(clb_handle* h) { return static_cast<CaScalars*>(h->d_ca_sc); }
+
+static CaView ca_view(const clb_handle* h) {
+    CaView C;
+    std::memset(&C, 0, sizeof C);
+    C.g = h->g;
+    C.bmax = h->ca_bmax;
+    C.thr = h->ca_frac * h->ca_bmax;
+    C.M = h->M;
+    C.bb = h->d.bounce_back_code;
+    C.solid = h->d.solid_code;
+    C.n_pore = h->d.n_pore_codes > 0 ? h->d.n_pore_codes : 1;
+    if (h->d.n_pore_codes > 0)
+        for (int i = 0; i < h->d.n_pore_codes; ++i) C.pore[i] = h->d.pore_codes[i];
+    else
+        C.pore[0] = 2;
+    for (int m = 0; m < CLB_MAX_MICROBES; ++m) C.bio_code[m] = m < h->d.n_microbes ? h->d.bio_codes[m] : 0;
+    return C;
+}
+
+void ca_free(clb_handle* h) {
+    cudaFree(h->d_ca_total); h->d_ca_total = nullptr;
+    cudaFree(h->d_ca_age); h->d_ca_age = nullptr;
+    cudaFree(h->d_ca_age2); h->d_ca_age2 = nullptr;
+    cudaFree(h->d_ca_distp); h->d_ca_distp = nullptr;
+    cudaFree(h->d_ca_aidx); h->d_ca_aidx = nullptr;
+    cudaFree(h->d_ca_act); h->d_ca_act = nullptr;
+    cudaFree(h->d_ca_done); h->d_ca_done = nullptr;
+    cudaFree(h->d_ca_tgt); h->d_ca_tgt = nullptr;
+    cudaFree(h->d_ca_amt); h->d_ca_amt = nullptr;
+    cudaFree(h->d_ca_own); h->d_ca_own = nullptr;
+    cudaFree(h->d_ca_sc); h->d_ca_sc = nullptr;
+    cudaFree(h->d_ca_mask0); h->d_ca_mask0 = nullptr;
+    h->ca_cap = 0;
+    h->ca_ready = false;
+}
+
+static clb_status ca_reserve(clb_handle* h, int cap) {
+    cudaFree(h->d_ca_act); cudaFree(h->d_ca_done); cudaFree(h->d_ca_tgt); cudaFree(h->d_ca_amt); cudaFree(h->d_ca_own);
+    h->d_ca_act = h->d_ca_done = h->d_ca_tgt = nullptr;
+    h->d_ca_amt = h->d_ca_own = nullptr;
+    const int M = std::max(1, h->M);
+    cudaError_t e = cudaMalloc(&h->d_ca_act, sizeof(int) * cap);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_done, sizeof(int) * cap);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_tgt, sizeof(int) * cap * CA_REC);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_amt, sizeof(double) * (size_t)cap * CA_REC * M);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_own, sizeof(double) * (size_t)cap * M);
+    if (e != cudaSuccess) return cuda_check(h, e, "cellular automaton buffers");
+    h->ca_cap = cap;
+    return CLB_OK;
+}
+
+clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
+    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+    if (h->M < 1 || !h->d_bio) return fail(h, CLB_INVALID_ARG, "the automaton needs biomass fields (clb_set_biomass)");
+    if (h->M > h->d.n_microbes) return fail(h, CLB_INVALID_ARG, "every biomass field needs a biofilm material code");
+    if (!(d->max_biomass > 0)) return fail(h, CLB_INVALID_ARG, "max_biomass must be positive");
+    int codesum = 0;
+    for (int m = 0; m < h->M; ++m) codesum += h->d.bio_codes[m];
+    if (codesum > 127) return fail(h, CLB_INVALID_ARG, "the sum of the biofilm codes must fit a material code");
+    ca_free(h);
+    const size_t N = (size_t)h->g.N;
+    cudaError_t e = cudaMalloc(&h->d_ca_total, sizeof(double) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_age, sizeof(int) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_age2, sizeof(int) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_distp, N);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_aidx, sizeof(int) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_sc, sizeof(CaScalars));
+    if (e == cudaSuccess && h->d.n_pore_codes > 1) e = cudaMalloc(&h->d_ca_mask0, N);
+    if (e != cudaSuccess) return cuda_check(h, e, "cellular automaton fields");
+    clb_status st = ca_reserve(h, (int)std::max<size_t>(4096, N / 64));
+    if (st != CLB_OK) return st;
+    if (!h->d_mat_flow) {
+        // from now on the mask moves with the automaton; the flow keeps its own map until a refresh
+        h->h_mat_flow = h->h_mat;
+        e = cudaMalloc(&h->d_mat_flow, N);
+        if (e == cudaSuccess) e = cudaMemcpy(h->d_mat_flow, h->h_mat_flow.data(), N, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_check(h, e, "flow material map");
+    }
+    h->ca_bmax = d->max_biomass;
+    h->ca_frac = d->biofilm_fraction;
+    h->ca_seed = d->seed;
+    h->ca_sweeps = 0;
+    CaScalars zero;
+    std::memset(&zero, 0, sizeof zero);
+    cudaMemcpyAsync(SC(h), &zero, sizeof zero, cudaMemcpyHostToDevice, h->stream);
+    const CaView C = ca_view(h);
+    k_ca_init<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_bio, h->d_ca_total, h->d_ca_age,
+                                                             h->d_ca_distp, h->d_ca_aidx, SC(h));
+    CaScalars s;
+    e = cudaMemcpyAsync(&s, SC(h), sizeof s, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_check(h, e, "cellular automaton set-up");
+    h->ca_mask_sum = s.mask_sum;
+    h->ca_ready = true;
+    return CLB_OK;
+}
+
+static clb_status ca_scalars(clb_handle* h, CaScalars& s) {
+    cudaError_t e = cudaMemcpyAsync(&s, SC(h), sizeof s, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return e == cudaSuccess ? CLB_OK : cuda_check(h, e, "cellular automaton counters");
+}
+
+// mask / total pass; returns max(total) and the mask sum
+static clb_status ca_mask_pass(clb_handle* h, const CaView& C, double& gmax, long long& msum) {
+    CaScalars s;
+    std::memset(&s, 0, sizeof s);
+    s.gmax = LLONG_MIN;
+    cudaMemcpyAsync(SC(h), &s, sizeof s, cudaMemcpyHostToDevice, h->stream);
+    if (h->d_ca_mask0) cudaMemcpyAsync(h->d_ca_mask0, h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToDevice, h->stream);
+    k_ca_mask_total<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_ca_mask0, h->d_bio,
+                                                                   h->d_ca_total, SC(h));
+    clb_status st = ca_scalars(h, s);
+    if (st != CLB_OK) return st;
+    gmax = unordered(s.gmax);
+    msum = s.mask_sum;
+    return CLB_OK;
+}
+
+static clb_status ca_push_sweep(clb_handle* h, const CaView& C) {
+    const int grid = h->num_sms * 8;
+    for (;;) {
+        CaScalars s;
+        std::memset(&s, 0, sizeof s);
+        cudaMemcpyAsync(SC(h), &s, sizeof s, cudaMemcpyHostToDevice, h->stream);
+        k_ca_collect<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_ca_total, h->d_ca_aidx, h->d_ca_act,
+                                                         h->d_ca_done, h->ca_cap, SC(h));
+        clb_status st = ca_scalars(h, s);
+        if (st != CLB_OK) return st;
+        const int count = (int)std::min<unsigned int>(s.active, (unsigned int)h->ca_cap);
+        if (s.overflow) {
+            k_ca_clear<<<grid, CA_THREADS, 0, h->stream>>>(h->d_ca_aidx, h->d_ca_act, count);
+            st = ca_reserve(h, (int)s.active * 2);
+            if (st != CLB_OK) return st;
+            continue;
+        }
+        if (count == 0) { ++h->ca_sweeps; return CLB_OK; }
+        s.remaining = (unsigned int)count;
+        cudaMemcpyAsync(&SC(h)->remaining, &s.remaining, sizeof(unsigned int), cudaMemcpyHostToDevice, h->stream);
+        // every round completes at least the lexicographically first unfinished voxel
+        for (int round = 1; round <= count; ++round) {
+            k_ca_round<<<(count + CA_THREADS - 1) / CA_THREADS, CA_THREADS, 0, h->stream>>>(
+                C, h->d_mat, h->d_ca_total, h->d_ca_age, h->d_bio, h->d_ca_aidx, h->d_ca_act, h->d_ca_done,
+                h->d_ca_tgt, h->d_ca_amt, h->d_ca_own, count, round, h->ca_seed, h->ca_sweeps, SC(h));
+            unsigned int rem = 0;
+            cudaError_t e = cudaMemcpyAsync(&rem, &SC(h)->remaining, sizeof rem, cudaMemcpyDeviceToHost, h->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+            if (e != cudaSuccess) return cuda_check(h, e, "push round");
+            if (rem == 0) break;
+        }
+        k_ca_apply<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_bio, h->d_ca_aidx, h->d_ca_tgt, h->d_ca_amt, h->d_ca_own);
+        k_ca_clear<<<grid, CA_THREADS, 0, h->stream>>>(h->d_ca_aidx, h->d_ca_act, count);
+        ++h->ca_sweeps;
+        return cuda_check(h, cudaGetLastError(), "push sweep");
+    }
+}
+
+static clb_status ca_age_converge(clb_handle* h, const CaView& C, bool& settled) {
+    settled = false;
+    for (int sub = 0; sub <= 1000; ++sub) {
+        unsigned int zero = 0;
+        cudaMemcpyAsync(&SC(h)->changed, &zero, sizeof zero, cudaMemcpyHostToDevice, h->stream);
+        k_age_jacobi<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_ca_age, h->d_ca_age2, h->d_ca_distp,
+                                                                    h->d_ca_total, SC(h));
+        std::swap(h->d_ca_age, h->d_ca_age2);
+        unsigned int ch = 0;
+        cudaError_t e = cudaMemcpyAsync(&ch, &SC(h)->changed, sizeof ch, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return cuda_check(h, e, "age relaxation");
+        if (ch == 0) { settled = true; return CLB_OK; }
+    }
+    return CLB_OK;
+}
+
+static void ca_age_sweep_inplace(clb_handle* h, const CaView& C) {
+    const int levels = h->g.nx + h->g.ny + h->g.nz - 2;
+    const int64_t cols = (int64_t)h->g.nx * h->g.ny;
+    const int grid = (int)std::min<int64_t>((cols + CA_THREADS - 1) / CA_THREADS, h->num_sms * 8);
+    for (int l = 0; l < levels; ++l)
+        k_age_level<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_ca_age, h->d_ca_distp, h->d_ca_total, l);
+}
+
+clb_status ca_step(clb_handle* h, int* sweeps_out, int* mask_changed) {
+    if (!h->ca_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ca_setup first");
+    const CaView C = ca_view(h);
+    double gmax;
+    long long msum;
+    clb_status st = ca_mask_pass(h, C, gmax, msum);
+    if (st != CLB_OK) return st;
+    int whilecount = 0;
+    clb_status rc = CLB_OK;
+    if (gmax - h->ca_bmax > THRD) {
+        double prev = gmax;
+        int stall = 0;
+        while (gmax - h->ca_bmax > THRD) {
+            if ((st = ca_push_sweep(h, C)) != CLB_OK) return st;
+            if ((st = ca_mask_pass(h, C, gmax, msum)) != CLB_OK) return st;
+            if (gmax > prev - THRD) {
+                if (++stall >= 100) { rc = fail(h, CLB_NOT_CONVERGED, "biofilm push stalled: excess biomass cannot spread"); break; }
+            } else {
+                stall = 0;
+            }
+            prev = gmax;
+            if (whilecount % 50 == 0) {
+                bool settled;
+                if ((st = ca_age_converge(h, C, settled)) != CLB_OK) return st;
+                if (!settled) { rc = fail(h, CLB_NOT_CONVERGED, "age relaxation did not settle in 1000 sweeps"); break; }
+            }
+            if (whilecount > 1000) { rc = fail(h, CLB_NOT_CONVERGED, "biofilm push did not settle in 1000 sweeps"); break; }
+            ++whilecount;
+        }
+    }
+    const bool changed = msum != h->ca_mask_sum;
+    if (changed) {
+        h->ca_mask_sum = msum;
+        ca_age_sweep_inplace(h, C);
+    }
+    cudaError_t e = cudaMemcpy(h->h_mat.data(), h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_check(h, e, "mask copy");
+    if (changed) {
+        st = geometry_refresh(h);
+        if (st != CLB_OK) return st;
+    }
+    if (sweeps_out) *sweeps_out = whilecount;
+    if (mask_changed) *mask_changed = changed ? 1 : 0;
+    return rc;
+}
+
+clb_status refresh_dynamics(clb_handle* h, int species, int flow) {
+    const CaView C = ca_view(h);
+    const int bio0 = h->d.n_microbes > 0 ? h->d.bio_codes[0] : -1;
+    const int grid = h->num_sms * 8;
+    if (species && h->ade_ready)
+        k_refresh_species<<<grid, CA_THREADS, 0, h->stream>>>(h->ade_sp.code, h->ade_sp.node, h->ade_sp.K, h->d_mat, C,
+                                                              bio0);
+    if (flow && h->flow_ready) {
+        const int64_t N = h->g.N;
+        cudaError_t e = cudaSuccess;
+        if (!h->d_mat_flow) {
+            h->h_mat_flow = h->h_mat;
+            e = cudaMalloc(&h->d_mat_flow, (size_t)N);
+            if (e == cudaSuccess)
+                e = cudaMemcpy(h->d_mat_flow, h->h_mat_flow.data(), (size_t)N, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return cuda_check(h, e, "flow material map");
+        }
+        k_refresh_flow_map<<<grid, CA_THREADS, 0, h->stream>>>(h->d_mat_flow, h->d_mat, C, h->fp, 1.0 / h->d.tau, bio0);
+        k_codes_from_map<<<grid, CA_THREADS, 0, h->stream>>>(h->flow_sp.code, h->flow_sp.node, h->flow_sp.K, h->d_mat_flow);
+        h->h_mat_flow.resize((size_t)N);
+        e = cudaMemcpyAsync(h->h_mat_flow.data(), h->d_mat_flow, (size_t)N, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return cuda_check(h, e, "flow material map");
+        int64_t nbgk = 0;
+        for (int64_t n = 0; n < N; ++n) nbgk += h->fp.dyn[(uint8_t)h->h_mat_flow[n] & 127] == DYN_BGK;
+        h->fp.n_bgk = nbgk;
+    }
+    return cuda_check(h, cudaGetLastError(), "dynamics refresh");
+}
+
+clb_status ca_fields(clb_handle* h, int which, double* host) {
+    if (!h->ca_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ca_setup first");
+    const size_t N = (size_t)h->g.N;
+    cudaError_t e;
+    if (which == 0) {
+        e = cudaMemcpy(host, h->d_ca_total, sizeof(double) * N, cudaMemcpyDeviceToHost);
+    } else {
+        std::vector<int> a(N);
+        e = cudaMemcpy(a.data(), h->d_ca_age, sizeof(int) * N, cudaMemcpyDeviceToHost);
+        for (size_t n = 0; n < N; ++n) host[n] = a[n];
+    }
+    return cuda_check(h, e, "automaton field");
+}
+
+}  // namespace clb

@@ -239,6 +239,25 @@ struct clb_handle_s {
     int32_t* d_xidx = nullptr;        // [K_ade] row in the gather list, -1
     double* d_park = nullptr;         // [S][seal_cap] parked dissolution shares
     double* d_xdc = nullptr;          // [S][gath_cap] abiotic increments of the gather list
+
+    // biofilm cellular automaton (biofilm_ca.cu)
+    bool ca_ready = false;
+    double ca_bmax = 0, ca_frac = 0;
+    uint64_t ca_seed = 0, ca_sweeps = 0;
+    long long ca_mask_sum = 0;
+    double* d_ca_total = nullptr;     // [N] total biomass as the automaton tracks it
+    int* d_ca_age = nullptr;          // [N] age wavefront
+    int* d_ca_age2 = nullptr;
+    int8_t* d_ca_distp = nullptr;     // [N] 1 where the distance-from-wall field is positive
+    int* d_ca_aidx = nullptr;         // [N] row of an active voxel in the sweep, -1
+    int* d_ca_act = nullptr;          // [cap] active voxels of a sweep
+    int* d_ca_done = nullptr;         // [cap] round in which each was processed
+    int* d_ca_tgt = nullptr;          // [cap][7] push targets
+    double* d_ca_amt = nullptr;       // [cap][7][M] pushed biomass
+    double* d_ca_own = nullptr;       // [cap][M] biomass left in the voxel
+    void* d_ca_sc = nullptr;          // device counters of the automaton
+    int8_t* d_ca_mask0 = nullptr;     // mask before a pass (several pore codes)
+    int ca_cap = 0;
 };
 
 namespace clb {
@@ -285,6 +304,13 @@ clb_status dissolution_pre_step(clb_handle* h); // park + gather before a transp
 AdeExtra ade_extra(clb_handle* h);
 void precip_free(clb_handle* h);
 inline const int8_t* flow_mat(const clb_handle* h) { return h->d_mat_flow ? h->d_mat_flow : h->d_mat; }
+
+// biofilm_ca.cu
+clb_status ca_setup(clb_handle* h, const clb_ca_desc* d);
+clb_status ca_step(clb_handle* h, int* sweeps, int* mask_changed);
+clb_status refresh_dynamics(clb_handle* h, int species, int flow);
+clb_status ca_fields(clb_handle* h, int which, double* host);
+void ca_free(clb_handle* h);
 
 // speciation.cu
 clb_status speciation_setup(clb_handle* h, const clb_speciation_desc* d);

@@ -575,11 +575,17 @@ clb_status flow_init(clb_handle* h, double delta_p) {
     h->delta_p = delta_p;
     // the flow lattice's own map once precipitation has changed the species' one
     const std::vector<int8_t>& fmat = h->h_mat_flow.empty() ? h->h_mat : h->h_mat_flow;
+    // biofilm voxels are nodes even when impermeable (bounce-back nodes are skipped by the step),
+    // so that the automaton can turn them back into pore without a new layout
+    int8_t cls[MAX_CODES];
+    for (int c = 0; c < MAX_CODES; ++c) cls[c] = (P.dyn[c] != DYN_BB);
+    for (int m = 0; m < d.n_microbes; ++m)
+        if (d.bio_codes[m] >= 0 && d.bio_codes[m] < MAX_CODES) cls[d.bio_codes[m]] = 1;
     int64_t nbgk = 0, kw = 0, ke = 0;
     for (int64_t n = 0; n < h->g.N; ++n) {
-        const int dn = P.dyn[(uint8_t)fmat[n] & 127];
-        nbgk += (dn == DYN_BGK);
-        if (dn != DYN_BB) {
+        const int c = (uint8_t)fmat[n] & 127;
+        nbgk += (P.dyn[c] == DYN_BGK);
+        if (cls[c]) {
             if (n < h->g.plane) ++kw;
             if (n >= h->g.N - h->g.plane) ++ke;
         }
@@ -587,8 +593,6 @@ clb_status flow_init(clb_handle* h, double delta_p) {
     P.n_bgk = nbgk;
 
     flow_free(h);
-    int8_t cls[MAX_CODES];
-    for (int c = 0; c < MAX_CODES; ++c) cls[c] = (P.dyn[c] != DYN_BB);
     clb_status s = sparse_build(h, cls, 19, h->flow_sp, &fmat);
     if (s != CLB_OK) return s;
     const int64_t K = h->flow_sp.K;

@@ -126,7 +126,9 @@ typedef enum clb_field {
     CLB_FIELD_CONCENTRATION = 3,  /* [N] of species `index`: computeDensity                  */
     CLB_FIELD_ADE_POPULATIONS = 4,/* [7][N] of species `index`                               */
     CLB_FIELD_BIOMASS = 5,        /* [N] of microbe `index`                                  */
-    CLB_FIELD_ADE_VELOCITY = 6    /* [3][N] the advection velocity the species see          */
+    CLB_FIELD_ADE_VELOCITY = 6,   /* [3][N] the advection velocity the species see          */
+    CLB_FIELD_CA_TOTAL = 7,       /* [N] total biofilm biomass the automaton tracks          */
+    CLB_FIELD_CA_AGE = 8          /* [N] age wavefront (integers)                            */
 } clb_field;
 
 typedef struct clb_handle_s clb_handle;
@@ -284,6 +286,39 @@ clb_status clb_precip_setup(clb_handle* h, const clb_precip_desc* desc);
  * lattice does too and is re-solved, then its velocity is coupled again (complab.cpp:3139-3247).
  * sealed / reopened (may be NULL) receive the voxel counts. */
 clb_status clb_geometry_update(clb_handle* h, int* sealed, int* reopened);
+
+/* ---------------------------------------------------------------- biofilm cellular automaton */
+
+/* The <microbiology> settings of the CA microbes (solver type CA; the biomass fields are those of
+ * clb_set_biomass, microbe m living in material bio_codes[m]). */
+typedef struct clb_ca_desc {
+    double max_biomass;           /* max_bMassRho: excess above it is pushed to neighbours      */
+    double biofilm_fraction;      /* thrd_bFilmFrac: pore <-> biofilm at this fraction of max   */
+    uint64_t seed;                /* seed of the random neighbour choices (the reference seeds
+                                     std::rand from the clock); a voxel's draws in a sweep are
+                                     splitmix64 steps from seed ^ sweep*0x9E3779B97F4A7C15
+                                     ^ voxel*0xD1B54A32D192ED03                               */
+} clb_ca_desc;
+
+/* Age and distance fields from the current mask (createAgeDomain3D, calculateDistanceFromSolid;
+ * complab.cpp:1078-1090) and the total biomass (initTotalbFilmLatticeDensity). */
+clb_status clb_ca_setup(clb_handle* h, const clb_ca_desc* desc);
+
+/* The CA block of one iteration (complab.cpp:2792-3055): mask and total update
+ * (updateLocalMaskNtotalLattices3D), then, while the largest total exceeds max_biomass, push
+ * sweeps (pushExcessBiomass3D, 'fraction') each followed by the mask update, with the age
+ * relaxation (updateAgeDistance3D) every 50 sweeps; then one age sweep when the mask changed
+ * (:3074-3079). Results equal the sequential lexicographic sweeps bit for bit. *sweeps receives
+ * the push sweeps made, *mask_changed whether the mask changed. Returns CLB_NOT_CONVERGED where
+ * the reference stops the run (no progress in 100 sweeps, more than 1000 sweeps, or an age
+ * relaxation that does not settle). Voxels of the ghost planes x = 0 and x = nx-1 never push. */
+clb_status clb_ca_step(clb_handle* h, int* sweeps, int* mask_changed);
+
+/* Dynamics follow the mask: species != 0 runs updateSoluteDynamics3D (pore / biofilm relaxation,
+ * complab3d_processors_part2.hh:485-553), flow != 0 updateNsLatticesDynamics3D (:748-818). The
+ * reference runs them every ade_update_interval / ns_update_interval iterations after a mask
+ * change; re-solve the flow and couple its velocity afterwards as it does. */
+clb_status clb_refresh_dynamics(clb_handle* h, int species, int flow);
 
 /* ---------------------------------------------------------------- equilibrium speciation */
 

@@ -379,11 +379,25 @@ struct OrcAde {
     double full = 0, reopen = 0.9;
     std::vector<double> dprm;
     std::vector<uint8_t> stamp;  // 1 where the voxel was sealed by precipitation (phase id)
+    // species dynamics map (the material each species lattice's dynamics were last chosen from);
+    // `mat` is the mask lattice. They differ only between a CA mask change and the next
+    // updateSoluteDynamics3D.
+    std::vector<int8_t> dmat;
+    // biofilm cellular automaton (complab3d_processors_part1.hh:499-732, part2.hh:71-259, :840-965)
+    int ca_on = 0;
+    double Bmax = 0, bfrac = 0;
+    uint64_t seed = 0, sweeps = 0;
+    std::vector<int> pore_codes, bio_code;
+    int bbc = -1, solc = -1;
+    std::vector<double> total;
+    std::vector<int> age;
+    std::vector<int8_t> distp;  // 1 where the distance field is positive
+    long long old_mask_sum = 0;
     size_t id(int x, int y, int z) const { return ((size_t)x * ny + y) * nz + z; }
     // the lattice dynamics of species s at node n
     int node_dyn(int s, int x, size_t n) const {
         if ((x == 0 && ltype[s] == BC_CLOSED) || (x == nx - 1 && rtype[s] == BC_CLOSED)) return ADE_BB;
-        return dyn[(uint8_t)mat[n]];
+        return dyn[(uint8_t)(dmat.empty() ? mat[n] : dmat[n])];
     }
 };
 
@@ -889,6 +903,7 @@ void orc_ade_geometry_update(OrcAde* A, int* sealed, int* reopened) {
                 if (!A->react[(uint8_t)A->mat[n]]) continue;
                 if (A->imm[A->sM][n] >= A->full) {
                     A->mat[n] = (int8_t)A->pcode;
+                    if (!A->dmat.empty()) A->dmat[n] = (int8_t)A->pcode;
                     A->stamp[n] = 1;
                     ++ns;
                 }
@@ -901,6 +916,7 @@ void orc_ade_geometry_update(OrcAde* A, int* sealed, int* reopened) {
                     if (!A->stamp[n]) continue;
                     if (A->imm[A->sM][n] < A->reopen * A->full) {
                         A->mat[n] = (int8_t)A->porecode;
+                        if (!A->dmat.empty()) A->dmat[n] = (int8_t)A->porecode;
                         A->stamp[n] = 0;
                         ++nr;
                     }
@@ -910,6 +926,277 @@ void orc_ade_geometry_update(OrcAde* A, int* sealed, int* reopened) {
 }
 
 void orc_ade_material(OrcAde* A, int8_t* out) { std::copy(A->mat.begin(), A->mat.end(), out); }
+
+// ---------------------------------------------------------------- biofilm cellular automaton
+/* The reference draws its random neighbour order from std::random_shuffle / std::rand, seeded by
+ * the clock, so no two runs agree. The oracle (and the product) replace it with a counter-based
+ * stream: voxel n in push sweep w draws from splitmix64 steps started at
+ * seed ^ (w * 0x9E3779B97F4A7C15) ^ (n * 0xD1B54A32D192ED03); a shuffle of L entries is
+ * Fisher-Yates from the top (j = draw % (i + 1)), a single pick is draw % L. */
+static inline uint64_t sm64(uint64_t& x) {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+static inline bool ca_open(const OrcAde* A, int m) { return m != A->bbc && m != A->solc; }
+static inline bool ca_pore(const OrcAde* A, int m) {
+    for (int c : A->pore_codes)
+        if (m == c) return true;
+    return false;
+}
+
+void orc_ca_setup(OrcAde* A, double Bmax, double frac, uint64_t seed, int n_pore, const int32_t* pore,
+                  int bb, int solid, const int32_t* bio_codes) {
+    const int nx = A->nx, ny = A->ny, nz = A->nz;
+    const size_t N = A->N;
+    A->ca_on = 1;
+    A->Bmax = Bmax;
+    A->bfrac = frac;
+    A->seed = seed;
+    A->sweeps = 0;
+    A->pore_codes.assign(pore, pore + n_pore);
+    A->bio_code.assign(bio_codes, bio_codes + A->M);
+    A->bbc = bb;
+    A->solc = solid;
+    if (A->dmat.empty()) A->dmat = A->mat;
+    // initTotalbFilmLatticeDensity: the sum of the microbes' biomass
+    A->total.assign(N, 0.0);
+    for (size_t n = 0; n < N; ++n) {
+        double t = 0;
+        for (int m = 0; m < A->M; ++m) t += A->bio[(size_t)m * N + n];
+        A->total[n] = t;
+    }
+    // createAgeDomain3D: solid / wall -1, pore 0, anything else (biofilm) 1
+    A->age.assign(N, 0);
+    A->distp.assign(N, 0);
+    long long msum = 0;
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = A->id(x, y, z);
+                const int m = A->mat[n];
+                msum += m;
+                A->age[n] = !ca_open(A, m) ? -1 : (ca_pore(A, m) ? 0 : 1);
+                // calculateDistanceFromSolid (complab_functions.hh:220-291): positive exactly for
+                // the voxels that are neither solid nor wall, off the last x, y and z planes
+                A->distp[n] = (ca_open(A, m) && x < nx - 1 && y < ny - 1 && z < nz - 1) ? 1 : 0;
+            }
+    A->old_mask_sum = msum;
+}
+
+// updateLocalMaskNtotalLattices3D with a single pore code list (in place, lexicographic)
+static void ca_mask_total(OrcAde* A) {
+    const int nx = A->nx, ny = A->ny, nz = A->nz;
+    const size_t N = A->N;
+    const double thr = A->bfrac * A->Bmax;
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = A->id(x, y, z);
+                const int m = A->mat[n];
+                if (!ca_open(A, m)) continue;
+                double bmass = 0;
+                int newmask = 0;
+                for (int mi = 0; mi < A->M; ++mi) {
+                    const double bm = A->bio[(size_t)mi * N + n];
+                    if (bm > 1e-14) {
+                        bmass += bm;
+                        newmask += A->bio_code[mi];
+                    }
+                }
+                if (std::fabs(bmass - A->total[n]) > 1e-14) A->total[n] = bmass;
+                const bool poreflag = ca_pore(A, m);
+                if (!poreflag && bmass < thr) {
+                    newmask = A->pore_codes[0];
+                    if (A->pore_codes.size() > 1) {
+                        const int d6[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+                        for (int d = 0; d < 6; ++d) {
+                            int X = x + d6[d][0], Y = y + d6[d][1], Z = z + d6[d][2];
+                            if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) continue;
+                            const int nm = A->mat[A->id(X, Y, Z)];
+                            if (ca_open(A, nm) && ca_pore(A, nm)) { newmask = nm; break; }
+                        }
+                    }
+                    A->mat[n] = (int8_t)newmask;
+                } else if (poreflag && bmass >= thr) {
+                    if (newmask > 0) A->mat[n] = (int8_t)newmask;
+                }
+            }
+}
+
+// pushExcessBiomass3D ('fraction') of a single-block run, where every push lands inside the block
+static void ca_push(OrcAde* A) {
+    const int nx = A->nx, ny = A->ny, nz = A->nz;
+    const size_t N = A->N;
+    const double Bmax = A->Bmax;
+    const uint64_t w = A->sweeps++;
+    for (int x = 1; x <= nx - 2; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                const size_t n = A->id(x, y, z);
+                if (!ca_open(A, A->mat[n])) continue;
+                double bMt = A->total[n];
+                if (!(bMt > Bmax)) continue;
+                double bMd = bMt - Bmax;
+                if (!(bMd > THRD)) continue;
+                // neighbours in the reference's order, x limited to 1..nx-2
+                size_t nb[6];
+                int L = 0;
+                const int d6[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+                for (int d = 0; d < 6; ++d) {
+                    int X = x + d6[d][0], Y = y + d6[d][1], Z = z + d6[d][2];
+                    if (X < 1 || X > nx - 2 || Y < 0 || Y >= ny || Z < 0 || Z >= nz) continue;
+                    const size_t m = A->id(X, Y, Z);
+                    if (!ca_open(A, A->mat[m])) continue;
+                    nb[L++] = m;
+                }
+                uint64_t st = A->seed ^ (w * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)n * 0xD1B54A32D192ED03ULL);
+                int perm[6] = {0, 1, 2, 3, 4, 5};
+                if (L > 1)
+                    for (int i = L - 1; i >= 1; --i) {
+                        const int j = (int)(sm64(st) % (uint64_t)(i + 1));
+                        std::swap(perm[i], perm[j]);
+                    }
+                bool chk = false;
+                for (int t = 0; t < L; ++t) {
+                    const size_t m = nb[L > 1 ? perm[t] : 0];
+                    const double nbrbMt = ca_pore(A, A->mat[m]) ? 0.0 : A->total[m];
+                    if (nbrbMt < Bmax) {
+                        const double hold = Bmax - nbrbMt;
+                        double partial = bMd;
+                        if (bMd > hold) { partial = hold; bMd -= hold; }
+                        else { bMd = 0; chk = true; }
+                        for (int mi = 0; mi < A->M; ++mi) {
+                            const double shove = A->bio[(size_t)mi * N + n] / bMt * partial;
+                            if (shove > THRD) {
+                                A->bio[(size_t)mi * N + n] -= shove;
+                                A->bio[(size_t)mi * N + m] += shove;
+                            }
+                        }
+                        bMt -= partial;
+                    }
+                    if (chk) break;
+                }
+                if (!chk && L > 0) {
+                    const int id0 = A->age[n];
+                    size_t cand[6];
+                    int c = 0;
+                    for (int t = 0; t < L; ++t)
+                        if (id0 > A->age[nb[t]]) cand[c++] = nb[t];
+                    size_t m;
+                    if (c > 1) m = cand[sm64(st) % (uint64_t)c];
+                    else if (c == 1) m = cand[0];
+                    else m = nb[L > 1 ? (int)(sm64(st) % (uint64_t)L) : 0];
+                    for (int mi = 0; mi < A->M; ++mi) {
+                        const double shove = A->bio[(size_t)mi * N + n] / bMt * bMd;
+                        A->bio[(size_t)mi * N + n] -= shove;
+                        A->bio[(size_t)mi * N + m] += shove;
+                    }
+                }
+            }
+}
+
+// updateAgeDistance3D: one in-place lexicographic sweep; returns the number of ages changed
+static long ca_age_sweep(OrcAde* A) {
+    const int nx = A->nx, ny = A->ny, nz = A->nz;
+    const double Bmax = A->Bmax;
+    long changed = 0;
+    const int d6[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                const size_t n = A->id(x, y, z);
+                const double B = A->total[n];
+                if (!(B > 1e-14)) continue;
+                size_t D[6];
+                int nd = 0;
+                for (int d = 0; d < 6; ++d) {
+                    int X = x + d6[d][0], Y = y + d6[d][1], Z = z + d6[d][2];
+                    if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) continue;
+                    const size_t m = A->id(X, Y, Z);
+                    if (A->distp[m]) D[nd++] = m;
+                }
+                const int a = A->age[n];
+                int na = a;
+                if (a == 0) na = 1;
+                else if (a == 1 && (B - Bmax) > -1e-14) {
+                    bool ok = true;
+                    for (int t = 0; t < nd; ++t)
+                        if (A->age[D[t]] == 0) { ok = false; break; }
+                    if (ok) na = 2;
+                } else {
+                    int cnt = 0;
+                    for (int t = 0; t < nd; ++t)
+                        if (A->age[D[t]] >= a && (A->total[D[t]] - Bmax) > -1e-14) ++cnt;
+                    if (cnt == nd) na = a + 1;
+                }
+                if (na != a) { A->age[n] = na; ++changed; }
+            }
+    return changed;
+}
+
+/* The CA block of one iteration (complab.cpp:2792-3055) followed by the age sweep the main loop
+ * runs when the mask changed (:3074-3079). Returns 0, or -1 when the push stalls for 100 sweeps,
+ * -2 when it does not settle in 1000 sweeps, -3 when the age relaxation does not settle in 1000. */
+int orc_ca_step(OrcAde* A, int* sweeps_out, int* mask_changed) {
+    const size_t N = A->N;
+    ca_mask_total(A);
+    auto gmax = [&]() { double g = -1e300; for (size_t n = 0; n < N; ++n) g = std::max(g, A->total[n]); return g; };
+    double globalBmax = gmax();
+    int whilecount = 0, rc = 0;
+    if (globalBmax - A->Bmax > THRD) {
+        double prev = globalBmax;
+        int stall = 0;
+        while (globalBmax - A->Bmax > THRD) {
+            ca_push(A);
+            ca_mask_total(A);
+            globalBmax = gmax();
+            if (globalBmax > prev - THRD) {
+                if (++stall >= 100) { rc = -1; break; }
+            } else {
+                stall = 0;
+            }
+            prev = globalBmax;
+            if (whilecount % 50 == 0) {
+                int sub = 0;
+                while (ca_age_sweep(A) != 0)
+                    if (++sub > 1000) { rc = -3; break; }
+                if (rc) break;
+            }
+            if (whilecount > 1000) { rc = -2; break; }
+            ++whilecount;
+        }
+    }
+    long long msum = 0;
+    for (size_t n = 0; n < N; ++n) msum += A->mat[n];
+    *mask_changed = msum != A->old_mask_sum;
+    if (*mask_changed) {
+        A->old_mask_sum = msum;
+        ca_age_sweep(A);
+    }
+    *sweeps_out = whilecount;
+    return rc;
+}
+
+/* updateSoluteDynamics3D (complab3d_processors_part2.hh:485-553): every open voxel's species
+ * dynamics follow the mask, pore codes with the pore omega, any other open code with the
+ * biofilm omega (the first microbe's code stands for it). */
+void orc_ade_refresh_dynamics(OrcAde* A) {
+    if (A->dmat.empty()) A->dmat = A->mat;
+    const int bio0 = A->bio_code.empty() ? -1 : A->bio_code[0];
+    for (size_t n = 0; n < A->N; ++n) {
+        const int m = A->mat[n];
+        if (!ca_open(A, m)) continue;
+        A->dmat[n] = ca_pore(A, m) ? (int8_t)m : (int8_t)(bio0 >= 0 ? bio0 : m);
+    }
+}
+
+void orc_ca_fields(OrcAde* A, double* total, int32_t* age) {
+    std::copy(A->total.begin(), A->total.end(), total);
+    std::copy(A->age.begin(), A->age.end(), age);
+}
 
 }  // extern "C"
 

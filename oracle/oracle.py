@@ -58,6 +58,10 @@ def lib():
             "orc_ade_set_precip": ([vp, ip, dp, ip, ip, dp, ip, ip, vp, ip, ip], None),
             "orc_ade_geometry_update": ([vp, vp, vp], None),
             "orc_ade_material": ([vp, vp], None),
+            "orc_ca_setup": ([vp, dp, dp, C.c_uint64, ip, vp, ip, ip, vp], None),
+            "orc_ca_step": ([vp, vp, vp], ip),
+            "orc_ade_refresh_dynamics": ([vp], None),
+            "orc_ca_fields": ([vp, vp, vp], None),
             "orc_flow_set_material": ([vp, vp], None),
             "orc_flow_set_dynamics": ([vp, ip, ip, dp], None),
         }
@@ -229,6 +233,26 @@ class OracleAde:
         m = np.empty(self.N, dtype=np.int8)
         lib().orc_ade_material(self.h, _p(m))
         return m
+
+    def ca_setup(self, bmax, frac, seed, pore_codes=(2,), bb=1, solid=0, bio_codes=(3, 4)):
+        pc = np.ascontiguousarray(pore_codes, dtype=np.int32)
+        bc = np.ascontiguousarray(bio_codes[:self.M], dtype=np.int32)
+        self._ca = (pc, bc)
+        lib().orc_ca_setup(self.h, float(bmax), float(frac), int(seed), pc.size, _p(pc), int(bb), int(solid), _p(bc))
+
+    def ca_step(self):
+        a, b = C.c_int(), C.c_int()
+        rc = lib().orc_ca_step(self.h, C.byref(a), C.byref(b))
+        return rc, a.value, bool(b.value)
+
+    def refresh_dynamics(self):
+        lib().orc_ade_refresh_dynamics(self.h)
+
+    def ca_fields(self):
+        t = np.empty(self.N)
+        a = np.empty(self.N, dtype=np.int32)
+        lib().orc_ca_fields(self.h, _p(t), _p(a))
+        return t, a
 
     def step(self, n=1):
         lib().orc_ade_step(self.h, n)
