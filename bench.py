@@ -9,6 +9,14 @@ between timed steps and times each step with its own event pair.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Side measurements in the same JSON line (rank 0, one GPU; --no-extra skips them):
+  "d3q7"       fused transport of the 256^3 pack, 8 species, 2 microbes, FP32: species-voxel
+               updates per second and its HBM roofline;
+  "precision"  FP64 / FP32 / FP16-shifted flow throughput and the velocity, permeability and
+               concentration errors of the reduced-precision paths against the FP64 path;
+  "speciation" the 5 x 12 tableau in transport: Newton-Raphson against the trained surrogate
+               (time per step, solves per second, speed-up, error against Newton-Raphson).
+
 Multi-GPU: the domain does not shard on this path (single-domain solver); each rank advances
 its own replica and the value is the sum over ranks divided by the slowest rank's time.
 The reference arm times the FP64 CPU restatement of the reference path (the reference itself
@@ -41,6 +49,7 @@ def args_():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="f32", choices=["f64", "f32", "f16s"])
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-extra", action="store_true", help="skip the D3Q7, precision and speciation legs")
     p.add_argument("--scale", type=float, default=1.0, help="shrink the workload (testing only)")
     return p.parse_args()
 
@@ -179,6 +188,161 @@ def run_reference(a, cfg):
     }))
 
 
+def timed_steps(torch, stream, step, steps, warmup):
+    """Device time of `steps` calls of step() on `stream` (one event pair around all of them)."""
+    step(warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def bench_d3q7(clb, workloads, torch, local, peak, steps=60, warmup=5):
+    """Fused transport of the 256^3 sphere pack with 8 species and 2 biofilm microbes (dual Monod),
+    FP32 populations; the lattice (1.5 GB) is far larger than L2, so no flush is needed."""
+    cfg = workloads.config3()
+    nx, ny, nz = cfg["shape"]
+    mat = cfg["mat"]
+    D = clb.Domain(mat, nx, ny, nz, cfg["tau"], flow_precision=clb.F32, ade_precision=clb.F32,
+                   bio_codes=cfg["bio_codes"], perm_ratio=cfg["perm_ratio"], device=local)
+    stream = torch.cuda.Stream()
+    D.set_stream(stream.cuda_stream)
+    D.flow_init(cfg["delta_p"])
+    D.flow_step(400)
+    D.ade_init(cfg["species"])
+    D.couple_velocity()
+    D.set_biomass(cfg["biomass"])
+    D.set_kinetics(cfg["law"], cfg["params"], cfg["dt"])
+    ms = timed_steps(torch, stream, D.ade_step, steps, warmup)
+    S = len(cfg["species"])
+    n_open = int(np.count_nonzero((mat != 0) & (mat != 1)))
+    per = ms / steps
+    M = cfg["biomass"].shape[0]
+    alg_node = S * 2 * 7 * 4 + 3 * 4 + 1 + M * 8
+    achieved = alg_node * n_open / (per * 1e-3) / 1e9
+    D.close()
+    return {"workload": cfg["name"] + ", FP32 populations, dual-Monod kinetics fused",
+            "mlups_d3q7": S * n_open * steps / (ms * 1e-3) / 1e6, "unit": "species x open-voxel updates / s (1e6)",
+            "ms_per_step": per, "open_voxels": n_open, "species": S, "steps": steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "algorithmic_bytes_per_node": alg_node, "kernel": "k_ade_aa (all species fused)"}}
+
+
+def bench_precision(clb, workloads, torch, local, steps=300, warmup=20):
+    """FP64 / FP32 / FP16-shifted storage: flow throughput and velocity / permeability error on the
+    256x128x128 pack (3000 steps from the same state), and the transport error on the 64x32x32
+    pack (flow to 1e-6, 2000 steps of decaying solute), each against the FP64 GPU path, which
+    matches the FP64 oracle to 1e-12."""
+    out = {}
+    cfg = workloads.config2()
+    nx, ny, nz = cfg["shape"]
+    ref_u = ref_k = None
+    for name, prec in (("f64", clb.F64), ("f32", clb.F32), ("f16s", clb.F16S)):
+        D = clb.Domain(cfg["mat"], nx, ny, nz, cfg["tau"], flow_precision=prec, device=local)
+        stream = torch.cuda.Stream()
+        D.set_stream(stream.cuda_stream)
+        D.flow_init(cfg["delta_p"])
+        D.autotune(10)
+        ms = timed_steps(torch, stream, D.flow_step, steps, warmup)
+        D.flow_step(3000 - steps - warmup)
+        st = D.flow_stats(cfg["char_length"])
+        u = D.velocity()
+        n_open = st["bgk_nodes"]
+        r = {"flow_mlups": n_open * steps / (ms * 1e-3) / 1e6, "permeability": st["permeability"]}
+        if ref_u is None:
+            ref_u, ref_k = u, st["permeability"]
+        else:
+            r["velocity_rel_l2_vs_f64"] = float(np.linalg.norm(u - ref_u) / np.linalg.norm(ref_u))
+            r["velocity_rel_max_vs_f64"] = float(np.abs(u - ref_u).max() / np.abs(ref_u).max())
+            r["permeability_rel_err_vs_f64"] = abs(st["permeability"] / ref_k - 1)
+        out[name] = r
+        D.close()
+    out["f32"]["speedup_vs_f64"] = out["f32"]["flow_mlups"] / out["f64"]["flow_mlups"]
+    out["f16s"]["speedup_vs_f64"] = out["f16s"]["flow_mlups"] / out["f64"]["flow_mlups"]
+    c1 = workloads.config1()
+    nx, ny, nz = c1["shape"]
+    ref_c = None
+    for name, prec in (("f64", clb.F64), ("f32", clb.F32), ("f16s", clb.F16S)):
+        D = clb.Domain(c1["mat"], nx, ny, nz, c1["tau"], flow_precision=prec, ade_precision=prec, device=local)
+        D.flow_init(c1["delta_p"])
+        it = D.flow_solve(200000, c1["eps"], allow_unconverged=True)
+        D.ade_init(c1["species"])
+        D.couple_velocity()
+        D.set_kinetics(c1["law"], c1["params"], c1["dt"])
+        D.ade_step(c1["ade_steps"])
+        c = D.concentration(0)
+        u = D.velocity()
+        if ref_c is None:
+            ref_c, ref_u1 = c, u
+            out[name]["config1_flow_iterations"] = it
+        else:
+            out[name]["config1_concentration_rel_l2_vs_f64"] = float(np.linalg.norm(c - ref_c) / np.linalg.norm(ref_c))
+            out[name]["config1_velocity_rel_l2_vs_f64"] = float(np.linalg.norm(u - ref_u1) / np.linalg.norm(ref_u1))
+        D.close()
+    return out
+
+
+def bench_speciation(clb, workloads, torch, local, steps=10):
+    """Equilibrium speciation of the 5-component, 12-species tableau inside the transport step on a
+    96^3 pack: Newton-Raphson (FP64) against the BF16 surrogate with a two-step Newton polish and
+    Newton-Raphson fallback. The surrogate is trained on the GPU from Newton-Raphson solves of the
+    states the run itself generates (1e6 samples of the domain's voxels after 20 steps, each
+    species scaled by 10^U(-0.6, 0.6)). Speciation time = step time with it minus step time
+    without; error = max relative species difference after one step from the same state (open
+    voxels), against Newton-Raphson. The component H+ (species 0) is kept dominant so every
+    component total is positive (the reference clamps non-positive totals to 1e-30)."""
+    S, logK, comp = workloads.tableau_5x12()
+    ns = S.shape[0]
+    mat, shape = workloads.sphere_pack_domain(96, 96, 96, 0.40, 3.0, 6.0, seed=1004)
+    rng = np.random.default_rng(1004)
+    sp = [dict(omega_pore=1 / 0.9, left_type=clb.DIRICHLET, right_type=clb.NEUMANN,
+               left_bc=float(10 ** rng.uniform(-6, -4)), c0=float(10 ** rng.uniform(-6, -4))) for _ in range(ns)]
+    sp[0]["c0"], sp[0]["left_bc"] = 3e-3, 2e-3
+    D = clb.Domain(mat, *shape, 0.8, ade_precision=clb.F32, device=local)
+    stream = torch.cuda.Stream()
+    D.set_stream(stream.cuda_stream)
+    D.ade_init(sp)
+    D.speciation_setup(S, logK, comp, tol=1e-10)
+    D.set_speciation_mode(clb.SPEC_NR)
+    D.ade_step(20)
+    t_train = time.perf_counter()
+    rep = D.surrogate_train([-6.0] * ns, [-2.5] * ns, n_samples=1000000, epochs=60, batch=1024, patience=8,
+                            learning_rate=3e-3, seed=1004, from_domain=True, jitter=0.6)
+    t_train = time.perf_counter() - t_train
+    D.surrogate_set_check(0.02, 2, 1e-6)
+    n_open = int(np.count_nonzero(mat == 2))
+    times = {}
+    for mode in (clb.SPEC_OFF, clb.SPEC_NR, clb.SPEC_MLP_NR):
+        D.set_speciation_mode(mode)
+        times[mode] = timed_steps(torch, stream, D.ade_step, steps, 2) / steps
+    # accuracy: one step from the same state under each mode
+    conc0 = [D.ade_populations(s) for s in range(ns)]
+    res = {}
+    for mode in (clb.SPEC_NR, clb.SPEC_MLP_NR):
+        for s in range(ns):
+            D.set_ade_populations(s, conc0[s])
+        D.set_speciation_mode(mode)
+        D.ade_step(1)
+        res[mode] = np.array([D.concentration(s) for s in range(ns)])
+    st = D.speciation_stats()
+    open_ = (mat == 2)
+    a, b = res[clb.SPEC_MLP_NR][:, open_], res[clb.SPEC_NR][:, open_]
+    rel = np.abs(a / np.where(b == 0, 1, b) - 1)
+    D.close()
+    t_nr = times[clb.SPEC_NR] - times[clb.SPEC_OFF]
+    t_ml = times[clb.SPEC_MLP_NR] - times[clb.SPEC_OFF]
+    return {"workload": "96^3 sphere pack, 5 components x 12 species tableau, FP32 transport, FP64 speciation",
+            "open_voxels": n_open, "nr_ms_per_step": t_nr, "surrogate_ms_per_step": t_ml,
+            "nr_solves_per_s": n_open / (t_nr * 1e-3), "surrogate_solves_per_s": n_open / (t_ml * 1e-3),
+            "speedup": t_nr / t_ml, "max_rel_err_vs_nr": float(rel.max()), "p99_rel_err_vs_nr": float(np.percentile(rel, 99)),
+            "surrogate_used_fraction": st["surrogate_used"] / max(1, st["solves"]),
+            "training": {"seconds": t_train, "val_mse": rep["val_mse"], "epochs": rep["epochs"],
+                         "n_train": rep["n_train"], "source": "the run's own voxel states, jitter 0.6 decades"}}
+
+
 def main():
     a = args_()
     import clb
@@ -275,6 +439,17 @@ def main():
     h2d = nx * ny * nz + 4 * ste["active_nodes"]
     d2h = u.nbytes
 
+    extra = {}
+    if rank == 0 and world == 1 and not a.no_extra and a.scale == 1.0:
+        for key, fn in (("d3q7", lambda: bench_d3q7(clb, workloads, torch, local, peak)),
+                        ("precision", lambda: bench_precision(clb, workloads, torch, local)),
+                        ("speciation", lambda: bench_speciation(clb, workloads, torch, local))):
+            try:
+                extra[key] = fn()
+            except Exception as exc:  # a failed side measurement must not hide the headline line
+                extra[key] = {"error": f"{type(exc).__name__}: {exc}"}
+            torch.cuda.synchronize()
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         v, threads, steps, dt = oracle_mlups(mat, cfg["shape"], cfg["tau"], cfg["delta_p"], 12.0, 2, 50)
@@ -299,6 +474,7 @@ def main():
             "gpu_launches": a.steps,
             "clocks": clocks.summary(),
         }
+        line.update(extra)
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -101,7 +101,8 @@ class SpeciationStats(C.Structure):
 class SurrogateTrainDesc(C.Structure):
     _fields_ = [("n_samples", C.c_int32), ("epochs", C.c_int32), ("batch", C.c_int32), ("patience", C.c_int32),
                 ("learning_rate", C.c_double), ("val_fraction", C.c_double), ("seed", C.c_uint64),
-                ("log_c_lo", C.c_double * MAX_EQ_SPECIES), ("log_c_hi", C.c_double * MAX_EQ_SPECIES)]
+                ("log_c_lo", C.c_double * MAX_EQ_SPECIES), ("log_c_hi", C.c_double * MAX_EQ_SPECIES),
+                ("source", C.c_int32), ("jitter", C.c_double)]
 
 
 class SurrogateReport(C.Structure):
@@ -418,6 +419,10 @@ class Domain:
         self._check(lib().clb_get_field(self.h, FIELD_CONCENTRATION, s, _ptr(c), 0))
         return c
 
+    def set_ade_populations(self, s, g):
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        self._check(lib().clb_set_field(self.h, FIELD_ADE_POPULATIONS, s, _ptr(g), 0))
+
     def ade_populations(self, s):
         g = np.empty(7 * self.N, dtype=np.float64)
         self._check(lib().clb_get_field(self.h, FIELD_ADE_POPULATIONS, s, _ptr(g), 0))
@@ -478,10 +483,13 @@ class Domain:
         return out, it
 
     def surrogate_train(self, log_c_lo, log_c_hi, n_samples=200000, epochs=60, batch=1024, patience=8,
-                        learning_rate=3e-3, val_fraction=0.15, seed=1):
+                        learning_rate=3e-3, val_fraction=0.15, seed=1, from_domain=False, jitter=0.0):
+        """from_domain: train on the species states of the domain's open voxels (each species
+        scaled by 10^U(-jitter, jitter)) instead of states drawn from [log_c_lo, log_c_hi]."""
         d = SurrogateTrainDesc()
         d.n_samples, d.epochs, d.batch, d.patience = n_samples, epochs, batch, patience
         d.learning_rate, d.val_fraction, d.seed = learning_rate, val_fraction, seed
+        d.source, d.jitter = int(bool(from_domain)), float(jitter)
         for i, (lo, hi) in enumerate(zip(log_c_lo, log_c_hi)):
             d.log_c_lo[i], d.log_c_hi[i] = lo, hi
         r = SurrogateReport()

@@ -493,6 +493,42 @@ __global__ void k_mlp_sample(int ns, int n, uint64_t seed, const double* __restr
     }
 }
 
+// Training states from the run itself: species of randomly chosen open voxels (x = 1..nx-2),
+// each scaled by 10^u, u uniform in [-jitter, jitter].
+template <typename TS>
+__global__ void k_mlp_sample_field(const TS* __restrict__ g, const TS* __restrict__ glink,
+                                   const double* __restrict__ imm, const SparseView S, const AdeParams A,
+                                   const SpecParams P, int odd, int64_t k_lo, int64_t k_hi, int n, uint64_t seed,
+                                   double jitter, double* __restrict__ c) {
+    const Geom G = A.g;
+    const double init[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        uint64_t hsh = mix64(seed ^ mix64(0x5DEECE66DULL + (uint64_t)t));
+        int64_t k = k_lo + (int64_t)(hsh % (uint64_t)(k_hi - k_lo));
+        for (int tries = 0; tries < 16 && !A.react[S.code[k]]; ++tries) {
+            hsh = mix64(hsh);
+            k = k_lo + (int64_t)(hsh % (uint64_t)(k_hi - k_lo));
+        }
+        const int64_t nd = S.node[k];
+        for (int i = 0; i < P.ns; ++i) {
+            const int si = P.ispec[i];
+            double v;
+            if (A.slot[si] >= 0) {
+                const int m = A.slot[si];
+                double pop[7];
+                natural<TS, double, 7>(S, G, g + (int64_t)m * 7 * S.KS, glink + (int64_t)m * S.L, nd, odd, init, pop);
+                v = 1.0;
+                for (int q = 0; q < 7; ++q) v += pop[q];
+            } else {
+                v = imm[(int64_t)si * G.N + nd];
+            }
+            hsh = mix64(hsh + 0x9E3779B97F4A7C15ULL);
+            const double u = (double)(hsh >> 11) * (1.0 / 9007199254740992.0);
+            c[(int64_t)t * P.ns + i] = fmax(v, 1e-30) * exp10(jitter * (2.0 * u - 1.0));
+        }
+    }
+}
+
 // X = log10 totals of the sampled state, Y = log10 of its equilibrium species. A state with a
 // total that is not positive (clamped to 1e-30 by the species model, no meaningful root) is
 // marked by a NaN in X[.][0] and dropped from the training set.
@@ -767,7 +803,19 @@ clb_status surrogate_train(clb_handle* h, const clb_surrogate_train_desc* d, clb
     if (e != cudaSuccess) { cleanup(); return cuda_check(h, e, "training buffers"); }
     cudaMemcpyAsync(dlo, d->log_c_lo, sizeof(double) * ns, cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(dhi, d->log_c_hi, sizeof(double) * ns, cudaMemcpyHostToDevice, h->stream);
-    k_mlp_sample<<<h->num_sms * 8, 256, 0, h->stream>>>(ns, n, d->seed, dlo, dhi, cin);
+    if (d->source == 1) {
+        if (h->ade_east_begin <= h->ade_west_end) { cleanup(); return fail(h, CLB_INVALID_ARG, "no interior voxels"); }
+        const SparseView Sv = view_of(h->ade_sp);
+        const int odd = (int)(h->ade_iters & 1);
+        const int gs = h->num_sms * 8;
+        switch (h->ade_prec) {
+            case CLB_F64: k_mlp_sample_field<double><<<gs, 128, 0, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, Sv, h->ap, CLB_SP(h), odd, h->ade_west_end, h->ade_east_begin, n, d->seed, d->jitter, cin); break;
+            case CLB_F32: k_mlp_sample_field<float><<<gs, 128, 0, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, Sv, h->ap, CLB_SP(h), odd, h->ade_west_end, h->ade_east_begin, n, d->seed, d->jitter, cin); break;
+            default: k_mlp_sample_field<__half><<<gs, 128, 0, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, Sv, h->ap, CLB_SP(h), odd, h->ade_west_end, h->ade_east_begin, n, d->seed, d->jitter, cin); break;
+        }
+    } else {
+        k_mlp_sample<<<h->num_sms * 8, 256, 0, h->stream>>>(ns, n, d->seed, dlo, dhi, cin);
+    }
     speciation_solve_device(h, cin, n, ceq);
     k_mlp_xy<<<h->num_sms * 8, 128, 0, h->stream>>>(CLB_SP(h), n, cin, ceq, X, Y);
     // ---- mapminmax ranges over the data

@@ -376,6 +376,11 @@ typedef struct clb_surrogate_train_desc {
     double learning_rate, val_fraction;
     uint64_t seed;
     double log_c_lo[CLB_MAX_EQ_SPECIES], log_c_hi[CLB_MAX_EQ_SPECIES];
+    int32_t source;               /* 0: states with log10 c uniform in [log_c_lo, log_c_hi];
+                                     1: the species states of the domain's open voxels as they
+                                     stand (the states the run itself generates), each species
+                                     scaled by 10^u with u uniform in [-jitter, jitter]        */
+    double jitter;
 } clb_surrogate_train_desc;
 
 typedef struct clb_surrogate_report {

@@ -178,3 +178,37 @@ def test_surrogate_with_fallback_in_transport(clb, oracle, trained):
     # a kept surrogate answer meets a 1e-6 relative mass balance; species agree to 1e-4
     np.testing.assert_allclose(a[:, open_], b[:, open_], rtol=1e-4)
     assert st["surrogate_used"] > 0.5 * st["solves"]
+
+
+def test_surrogate_trained_on_the_runs_own_states(clb):
+    """Training data drawn from the domain's own voxel states (the solves the method generates):
+    the surrogate then answers nearly every voxel of that run, to Newton-Raphson accuracy."""
+    S, logK, comp = workloads.carbonate_tableau()
+    shape = (16, 9, 8)
+    mat = mixed_geometry(*shape, seed=23, biofilm=False)
+    sp = [dict(omega_pore=1 / 0.9, left_type=0, right_type=1, left_bc=b, c0=c)
+          for b, c in zip([2e-3, 1e-6, 1e-5, 5e-4], [1e-4, 3e-7, 2e-6, 1e-5])]
+    out = {}
+    for mode in (clb.SPEC_NR, clb.SPEC_MLP_NR):
+        D = clb.Domain(mat, *shape, 0.8, ade_precision=clb.F64)
+        D.ade_init(sp)
+        D.speciation_setup(S, logK, comp, tol=1e-10)
+        D.set_speciation_mode(clb.SPEC_NR)
+        D.ade_step(6)
+        if mode == clb.SPEC_MLP_NR:
+            rep = D.surrogate_train([-8] * 4, [-2] * 4, n_samples=100000, epochs=40, batch=1024, patience=8,
+                                    learning_rate=3e-3, seed=3, from_domain=True, jitter=0.5)
+            assert rep["n_train"] > 50000
+            D.surrogate_set_check(0.02, 2, 1e-6)
+        D.set_speciation_mode(mode)
+        s0 = D.speciation_stats()
+        D.ade_step(6)
+        s1 = D.speciation_stats()
+        out[mode] = (np.array([D.concentration(s) for s in range(4)]),
+                     (s1["surrogate_used"] - s0["surrogate_used"]) / max(1, s1["solves"] - s0["solves"]))
+    a, used = out[clb.SPEC_MLP_NR]
+    b, _ = out[clb.SPEC_NR]
+    print("surrogate used on", used)
+    assert used > 0.9
+    open_ = mat == 2
+    np.testing.assert_allclose(a[:, open_], b[:, open_], rtol=1e-4)
