@@ -19,6 +19,7 @@
 // Algorithmic bytes per node update: 2*7*sizeof(storage) per mobile species, plus the velocity
 // (3*sizeof(arith)) and the material byte shared by all species.
 #include "kinetics.cuh"
+#include "tma.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -26,12 +27,23 @@
 
 namespace clb {
 
-constexpr int ADE_THREADS = 256;
+constexpr int ADE_THREADS = 128;
 
 // EXT: the abiotic law and the increments gathered from dissolving neighbours (AdeExtra) are
 // applied after the biotic ones (complab.cpp:2460-2525).
+// resident blocks per SM the shared slots allow (about 200 KB of shared memory per SM)
+template <typename TC, int NM>
+constexpr int ade_minb() {
+    constexpr int b = (200 * 1024) / (NM * 7 * 128 * (int)sizeof(TC));
+    return b < 1 ? 1 : (b > 6 ? 6 : b);
+}
+
+// One thread per node. The populations of all species pass through the thread's own slots of
+// shared memory (NM x 7 x ADE_THREADS values of the arithmetic type) between the gather and the
+// collision, so registers hold only the per-species sums and increments and many warps stay
+// resident to hide memory latency.
 template <typename TS, typename TC, bool ODD, int NM, bool EXT>
-__global__ void __launch_bounds__(ADE_THREADS)
+__global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>()))
     k_ade_aa(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm, double* __restrict__ bio,
              const TC* __restrict__ u, const SparseView S, const double* __restrict__ neu, const AdeParams P,
              int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin,
@@ -40,6 +52,8 @@ __global__ void __launch_bounds__(ADE_THREADS)
     const int64_t K = S.K, L = S.L;
     const int64_t KS = S.KS;
     const uint32_t K32 = (uint32_t)KS;  // row stride; 7 KS < 2^31 is checked when the layout is built
+    extern __shared__ __align__(16) unsigned char ade_smem[];
+    TC* sp = reinterpret_cast<TC*>(ade_smem);
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
         const int code = S.code[k];
         const int dyn = P.dyn[code];
@@ -72,40 +86,79 @@ __global__ void __launch_bounds__(ADE_THREADS)
             nb[3] = (int)k + 1;
             nb[6] = (int)k - 1;
         }
-        TC pop[NM][7];
+        // phase 1: every species' incoming populations (after the boundary completion) into this
+        // thread's own shared-memory slots, and their sums; only the sums stay in registers
+        uint32_t actm = 0;
         TC rb[NM];
-        bool act[NM];
 #pragma unroll
         for (int m = 0; m < NM; ++m) {
-            act[m] = false;
             rb[m] = 0;
             if (m >= n_mobile) continue;
             const int s = mob_species[m];
             if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
-            act[m] = true;
+            actm |= 1u << m;
             TS* f = g + (int64_t)m * 7 * KS;
             const TS* lk = glink + (int64_t)m * L;
+            TC* slot = sp + (m * 7) * blockDim.x + threadIdx.x;
+            if constexpr (sizeof(TS) >= 4) {
+                // 4- and 8-byte populations go straight to the slots as asynchronous copies, so a
+                // thread has all of its loads in flight at once without holding them in registers
 #pragma unroll
-            for (int i = 0; i < 7; ++i) {
-                if (!ODD || i == 0) { pop[m][i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
-                const int oi = q7opp(i);
-                if ((blk >> oi) & 1u) pop[m][i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k);
-                else pop[m][i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)nb[i]);
-            }
-            if (!ODD && wm) {
-                // wall link (a, i): incoming opp(i) from the even-step slot X; the odd-step slot
-                // Y = f[opp(i)][a] is written back unchanged so its sector is written whole
-#pragma unroll
-                for (int i = 1; i < 7; ++i) {
-                    if (!((wm >> i) & 1u)) continue;
-                    const int oi = q7opp(i);
-                    st<TS, TC>(f + (uint32_t)(oi * K32) + k, pop[m][oi]);
-                    pop[m][oi] = ld<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)));
+                for (int i = 0; i < 7; ++i) {
+                    const TS* src = f + (uint32_t)(i * K32) + k;
+                    if (!ODD) {
+                        const int oi = q7opp(i);
+                        // wall link (a, opp(i)): incoming i from the even-step slot X
+                        if (i != 0 && ((wm >> oi) & 1u)) src = lk + lb + __popc(wm & ((1u << oi) - 1u));
+                    } else if (i != 0) {
+                        const int oi = q7opp(i);
+                        if (!((blk >> oi) & 1u)) src = f + (uint32_t)(oi * K32) + (uint32_t)nb[i];
+                    }
+                    cp_async<sizeof(TS)>(slot + i * blockDim.x, src);
                 }
+                if (!ODD && wm) {
+                    // the odd-step slot Y = f[opp(i)][a] of a wall link is written back unchanged
+                    // so its sector is written whole
+#pragma unroll
+                    for (int i = 1; i < 7; ++i) {
+                        if (!((wm >> i) & 1u)) continue;
+                        TS* y = f + (uint32_t)(q7opp(i) * K32) + k;
+                        *y = *y;
+                    }
+                }
+            } else {
+                TC q[7];
+#pragma unroll
+                for (int i = 0; i < 7; ++i) {
+                    if (!ODD || i == 0) { q[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
+                    const int oi = q7opp(i);
+                    if ((blk >> oi) & 1u) q[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k);
+                    else q[i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)nb[i]);
+                }
+                if (!ODD && wm) {
+                    // wall link (a, i): incoming opp(i) from the even-step slot X; the odd-step
+                    // slot Y = f[opp(i)][a] is written back unchanged so its sector is written whole
+#pragma unroll
+                    for (int i = 1; i < 7; ++i) {
+                        if (!((wm >> i) & 1u)) continue;
+                        const int oi = q7opp(i);
+                        st<TS, TC>(f + (uint32_t)(oi * K32) + k, q[oi]);
+                        q[oi] = ld<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)));
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 7; ++i) slot[i * blockDim.x] = q[i];
             }
+        }
+        if constexpr (sizeof(TS) >= 4) cp_async_wait_all();  // each thread reads only its own slots
+#pragma unroll
+        for (int m = 0; m < NM; ++m) {
+            if (!((actm >> m) & 1u)) continue;
+            TC* slot = sp + (m * 7) * blockDim.x + threadIdx.x;
             if ((west || east) && dyn != ADE_NONE) {
                 // AdvectionDiffusionBoundaryDynamics: the one inward population makes the
                 // node's density equal to the stored value
+                const int s = mob_species[m];
                 const int type = west ? P.ltype[s] : P.rtype[s];
                 double rs;
                 if (type == CLB_DIRICHLET) rs = west ? P.lbc[s] : P.rbc[s];
@@ -114,12 +167,12 @@ __global__ void __launch_bounds__(ADE_THREADS)
                 TC sum = 0;
 #pragma unroll
                 for (int i = 0; i < 7; ++i)
-                    if (i != miss) sum += pop[m][i];
-                pop[m][miss] = (TC)(rs - 1.0) - sum;
+                    if (i != miss) sum += slot[i * blockDim.x];
+                slot[miss * blockDim.x] = (TC)(rs - 1.0) - sum;
             }
             TC r = 0;
 #pragma unroll
-            for (int i = 0; i < 7; ++i) r += pop[m][i];
+            for (int i = 0; i < 7; ++i) r += slot[i * blockDim.x];
             rb[m] = r;
         }
         // ---- kinetics (x = 1..nx-2, mask neither solid nor wall)
@@ -200,31 +253,36 @@ __global__ void __launch_bounds__(ADE_THREADS)
                 else imm[(int64_t)s * G.N + nd] += d;
             }
         }
-        // ---- collide, deposit, stream
+        // ---- phase 2: collide, deposit, stream, species by species from the shared slots
+        TC dep[NM];
+#pragma unroll
+        for (int m = 0; m < NM; ++m) dep[m] = (TC)dC[m];
         const TC ux = u[k], uy = u[K + k], uz = u[2 * K + k];
 #pragma unroll
         for (int m = 0; m < NM; ++m) {
-            if (!act[m]) continue;
+            if (!((actm >> m) & 1u)) continue;
             const int s = mob_species[m];
-            TC o[7];
+            TC q[7], o[7];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) q[i] = sp[(m * 7 + i) * blockDim.x + threadIdx.x];
             if (dyn == ADE_NONE) {
 #pragma unroll
-                for (int i = 0; i < 7; ++i) o[i] = pop[m][i];
+                for (int i = 0; i < 7; ++i) o[i] = q[i];
             } else {
                 const TC w = (TC)(dyn == ADE_BIO ? P.wbio[s] : P.wpore[s]);
                 const TC omw = (TC)1 - w;
                 const TC rho = rb[m] + (TC)1;
                 const TC jx = rho * ux, jy = rho * uy, jz = rho * uz;
-                const TC d = (TC)dC[m];
+                const TC d = dep[m];
                 // feq_i = t_i (rb + 4 c_i . j), in opposite-pair form (no zero products)
                 const TC r8 = (TC)0.125 * rb[m], d8 = (TC)0.125 * d;
-                o[0] = pop[m][0] * omw + w * ((TC)0.25 * rb[m]) + (TC)0.25 * d;
-                o[1] = pop[m][1] * omw + w * (r8 - (TC)0.5 * jx) + d8;
-                o[4] = pop[m][4] * omw + w * (r8 + (TC)0.5 * jx) + d8;
-                o[2] = pop[m][2] * omw + w * (r8 - (TC)0.5 * jy) + d8;
-                o[5] = pop[m][5] * omw + w * (r8 + (TC)0.5 * jy) + d8;
-                o[3] = pop[m][3] * omw + w * (r8 - (TC)0.5 * jz) + d8;
-                o[6] = pop[m][6] * omw + w * (r8 + (TC)0.5 * jz) + d8;
+                o[0] = q[0] * omw + w * ((TC)0.25 * rb[m]) + (TC)0.25 * d;
+                o[1] = q[1] * omw + w * (r8 - (TC)0.5 * jx) + d8;
+                o[4] = q[4] * omw + w * (r8 + (TC)0.5 * jx) + d8;
+                o[2] = q[2] * omw + w * (r8 - (TC)0.5 * jy) + d8;
+                o[5] = q[5] * omw + w * (r8 + (TC)0.5 * jy) + d8;
+                o[3] = q[3] * omw + w * (r8 - (TC)0.5 * jz) + d8;
+                o[6] = q[6] * omw + w * (r8 + (TC)0.5 * jz) + d8;
             }
             TS* f = g + (int64_t)m * 7 * KS;
             TS* lk = glink + (int64_t)m * L;
@@ -610,9 +668,23 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
     return cuda_check(h, cudaMemcpy(h->d_bio, b, sizeof(double) * M * (size_t)h->g.N, cudaMemcpyHostToDevice), "biomass copy");
 }
 
+// Resident blocks per SM of a transport-step instantiation with `smem` bytes of shared memory
+// (set up once per instantiation), times the SM count: the persistent grid.
+static int ade_grid_for(const void* kern, int smem, int num_sms) {
+    static std::mutex mu;
+    static std::vector<std::pair<const void*, int>> known;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto& kv : known)
+        if (kv.first == kern) return kv.second * num_sms;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, ADE_THREADS, smem) != cudaSuccess || nb < 1) nb = 1;
+    known.push_back({kern, nb});
+    return nb * num_sms;
+}
+
 template <typename TS, typename TC, bool ODD>
 static void launch_ade_t(clb_handle* h) {
-    const int grid = h->ade_grid;
     const int nm = h->n_mobile;
     const int nb = h->S;  // register bucket covers every species (mobile first, then immobile)
     TS* g = (TS*)h->d_g;
@@ -623,9 +695,13 @@ static void launch_ade_t(clb_handle* h) {
     const bool ext = h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on;
     const AdeExtra X = ade_extra(h);
 #define CLB_ADE(NM, EXT)                                                                                          \
-    k_ade_aa<TS, TC, ODD, NM, EXT><<<grid, ADE_THREADS, 0, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, \
-                                                                       h->ap, nm, mt, h->ade_west_end,            \
-                                                                       h->ade_east_begin, X)
+    do {                                                                                                          \
+        auto kern = k_ade_aa<TS, TC, ODD, NM, EXT>;                                                               \
+        const int sm = NM * 7 * ADE_THREADS * (int)sizeof(TC);                                                    \
+        const int gr = ade_grid_for((const void*)kern, sm, h->num_sms);                                           \
+        kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,        \
+                                                 h->ade_west_end, h->ade_east_begin, X);                          \
+    } while (0)
     if (ext) {
         if (nb <= 4) CLB_ADE(4, true);
         else if (nb <= 8) CLB_ADE(8, true);
