@@ -31,11 +31,113 @@ constexpr int ADE_THREADS = 128;
 
 // EXT: the abiotic law and the increments gathered from dissolving neighbours (AdeExtra) are
 // applied after the biotic ones (complab.cpp:2460-2525).
+// Kinetics of node k (x = 1..nx-2, mask neither solid nor wall): biotic rates with the clamp,
+// then, with EXT, the abiotic block. Returns the increments of the mobile species in dC (internal
+// species m = slot m); immobile species and biomass are updated in place.
+template <typename TC, int NM, bool EXT>
+__device__ __forceinline__ void node_kinetics(const AdeParams& P, const SparseView& S, const AdeExtra& X,
+                                              int64_t k, int code, bool west, bool east, int n_mobile,
+                                              const TC (&rb)[NM], double* __restrict__ imm,
+                                              double* __restrict__ bio, TC (&dC)[NM]) {
+    const Geom G = P.g;
+#pragma unroll
+    for (int s = 0; s < NM; ++s) dC[s] = 0;
+    if (P.law != CLB_LAW_NONE && !west && !east && P.react[code]) {
+        const int64_t nd = S.node[k];  // dense index of the per-voxel fields
+        double C[NM], R[NM], B[CLB_MAX_MICROBES], RB[CLB_MAX_MICROBES];
+#pragma unroll
+        for (int s = 0; s < NM; ++s) {
+            double c = 0.0;
+            if (s < n_mobile) c = (double)rb[s] + 1.0;
+            else if (s < P.S) c = imm[(int64_t)s * G.N + nd];
+            C[s] = c < THRD ? 0.0 : c;
+        }
+        for (int mb = 0; mb < P.M; ++mb) {
+            const double b = bio[(int64_t)mb * G.N + nd];
+            B[mb] = b < THRD ? 0.0 : b;
+        }
+        eval_rates<NM>(P, C, B, R, RB);
+#pragma unroll
+        for (int s = 0; s < NM; ++s) {
+            if (s >= P.S) continue;
+            double d = R[s] * P.dt;
+            if (!(d > THRD || d < -THRD)) continue;
+            if (d + C[s] < 0.0) d = -C[s];
+            if (!(d > THRD || d < -THRD)) continue;
+            if (s < n_mobile) dC[s] = (TC)d;
+            else imm[(int64_t)s * G.N + nd] += d;
+        }
+        for (int mb = 0; mb < P.M; ++mb) {
+            double d = RB[mb] * P.dt;
+            if (!(d > THRD || d < -THRD)) continue;
+            if (d + B[mb] < 0.0) d = -B[mb];
+            bio[(int64_t)mb * G.N + nd] += d;
+        }
+    }
+    if (EXT && !west && !east && P.react[code]) {
+        // abiotic block: increments from the concentrations the biotic law left, applied once
+        // (update_abiotic_rxnLattices); next to a dissolving voxel they were computed ahead of
+        // the step together with the gathered products
+        const int64_t nd = S.node[k];
+        double T2[NM];
+#pragma unroll
+        for (int s = 0; s < NM; ++s) T2[s] = 0.0;
+        const int xi = X.xidx[k];
+        if (xi >= 0) {
+#pragma unroll
+            for (int s = 0; s < NM; ++s)
+                if (s < P.S) T2[s] = X.xdc[(int64_t)s * X.ng + xi];
+        } else if (P.law2 != CLB_LAW_NONE && (!P.surf || X.iface[k])) {
+            double C[NM], R[NM];
+#pragma unroll
+            for (int s = 0; s < NM; ++s) {
+                double c = 0.0;
+                if (s < n_mobile) c = (double)rb[s] + 1.0 + (double)dC[s];
+                else if (s < P.S) c = imm[(int64_t)s * G.N + nd];
+                C[s] = c < THRD ? 0.0 : c;
+            }
+            eval_rates2<NM>(P, C, R);
+#pragma unroll
+            for (int s = 0; s < NM; ++s) {
+                if (s >= P.S) continue;
+                double d = R[s] * P.dt;
+                if (!(d > THRD || d < -THRD)) continue;
+                if (d + C[s] < 0.0) d = -C[s];
+                if (!(d > THRD || d < -THRD)) continue;
+                T2[s] = d;
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < NM; ++s) {
+            if (s >= P.S) continue;
+            const double d = T2[s];
+            if (!(d > THRD || d < -THRD)) continue;
+            if (s < n_mobile) dC[s] += (TC)d;
+            else imm[(int64_t)s * G.N + nd] += d;
+        }
+    }
+}
+
+// compact index of the source node a - c_i of each population on an odd step (from the
+// per-tile row bases and per-node residuals)
+__device__ __forceinline__ void odd_sources(const SparseView& S, int64_t k, int (&nb)[7]) {
+    const int t = (int)(k >> 8);
+    const int2 dv = *reinterpret_cast<const int2*>(S.dres + 4 * k);
+    const int* tb = S.tdb + 4 * t;
+    nb[0] = (int)k;
+    nb[1] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);           // -x population comes from x+1
+    nb[4] = (int)k + tb[1] + (int16_t)((uint32_t)dv.x >> 16);    // +x from x-1
+    nb[2] = (int)k + tb[2] + (int16_t)(dv.y & 0xFFFF);           // -y from y+1
+    nb[5] = (int)k + tb[3] + (int16_t)((uint32_t)dv.y >> 16);    // +y from y-1
+    nb[3] = (int)k + 1;
+    nb[6] = (int)k - 1;
+}
+
 // resident blocks per SM the shared slots allow (about 200 KB of shared memory per SM)
 template <typename TC, int NM>
 constexpr int ade_minb() {
     constexpr int b = (200 * 1024) / (NM * 7 * 128 * (int)sizeof(TC));
-    return b < 1 ? 1 : (b > 6 ? 6 : b);
+    return b < 1 ? 1 : (b > 4 ? 4 : b);
 }
 
 // One thread per node. The populations of all species pass through the thread's own slots of
@@ -74,18 +176,7 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>()))
             blk = wm | ((mt >> 7) & 0x7Fu);  // wall or outside the box
             lb = S.tlb[(int)(k >> 8)] + (int)(mt >> 14);
         }
-        if (ODD) {
-            const int t = (int)(k >> 8);
-            const int2 dv = *reinterpret_cast<const int2*>(S.dres + 4 * k);
-            const int* tb = S.tdb + 4 * t;
-            nb[0] = (int)k;
-            nb[1] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);           // -x population comes from x+1
-            nb[4] = (int)k + tb[1] + (int16_t)((uint32_t)dv.x >> 16);    // +x from x-1
-            nb[2] = (int)k + tb[2] + (int16_t)(dv.y & 0xFFFF);           // -y from y+1
-            nb[5] = (int)k + tb[3] + (int16_t)((uint32_t)dv.y >> 16);    // +y from y-1
-            nb[3] = (int)k + 1;
-            nb[6] = (int)k - 1;
-        }
+        if (ODD) odd_sources(S, k, nb);
         // phase 1: every species' incoming populations (after the boundary completion) into this
         // thread's own shared-memory slots, and their sums; only the sums stay in registers
         uint32_t actm = 0;
@@ -175,88 +266,10 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>()))
             for (int i = 0; i < 7; ++i) r += slot[i * blockDim.x];
             rb[m] = r;
         }
-        // ---- kinetics (x = 1..nx-2, mask neither solid nor wall)
-        double dC[NM];
-#pragma unroll
-        for (int s = 0; s < NM; ++s) dC[s] = 0.0;
-        if (P.law != CLB_LAW_NONE && !west && !east && P.react[code]) {
-            const int64_t nd = S.node[k];  // dense index of the per-voxel fields
-            double C[NM], R[NM], B[CLB_MAX_MICROBES], RB[CLB_MAX_MICROBES];
-#pragma unroll
-            for (int s = 0; s < NM; ++s) {
-                double c = 0.0;
-                if (s < n_mobile) c = (double)rb[s] + 1.0;
-                else if (s < P.S) c = imm[(int64_t)s * G.N + nd];
-                C[s] = c < THRD ? 0.0 : c;
-            }
-            for (int mb = 0; mb < P.M; ++mb) {
-                const double b = bio[(int64_t)mb * G.N + nd];
-                B[mb] = b < THRD ? 0.0 : b;
-            }
-            eval_rates<NM>(P, C, B, R, RB);
-#pragma unroll
-            for (int s = 0; s < NM; ++s) {
-                if (s >= P.S) continue;
-                double d = R[s] * P.dt;
-                if (!(d > THRD || d < -THRD)) continue;
-                if (d + C[s] < 0.0) d = -C[s];
-                if (!(d > THRD || d < -THRD)) continue;
-                if (s < n_mobile) dC[s] = d;
-                else imm[(int64_t)s * G.N + nd] += d;
-            }
-            for (int mb = 0; mb < P.M; ++mb) {
-                double d = RB[mb] * P.dt;
-                if (!(d > THRD || d < -THRD)) continue;
-                if (d + B[mb] < 0.0) d = -B[mb];
-                bio[(int64_t)mb * G.N + nd] += d;
-            }
-        }
-        if (EXT && !west && !east && P.react[code]) {
-            // abiotic block: increments from the concentrations the biotic law left, applied once
-            // (update_abiotic_rxnLattices); next to a dissolving voxel they were computed ahead of
-            // the step together with the gathered products
-            const int64_t nd = S.node[k];
-            double T2[NM];
-#pragma unroll
-            for (int s = 0; s < NM; ++s) T2[s] = 0.0;
-            const int xi = X.xidx[k];
-            if (xi >= 0) {
-#pragma unroll
-                for (int s = 0; s < NM; ++s)
-                    if (s < P.S) T2[s] = X.xdc[(int64_t)s * X.ng + xi];
-            } else if (P.law2 != CLB_LAW_NONE && (!P.surf || X.iface[k])) {
-                double C[NM], R[NM];
-#pragma unroll
-                for (int s = 0; s < NM; ++s) {
-                    double c = 0.0;
-                    if (s < n_mobile) c = (double)rb[s] + 1.0 + dC[s];
-                    else if (s < P.S) c = imm[(int64_t)s * G.N + nd];
-                    C[s] = c < THRD ? 0.0 : c;
-                }
-                eval_rates2<NM>(P, C, R);
-#pragma unroll
-                for (int s = 0; s < NM; ++s) {
-                    if (s >= P.S) continue;
-                    double d = R[s] * P.dt;
-                    if (!(d > THRD || d < -THRD)) continue;
-                    if (d + C[s] < 0.0) d = -C[s];
-                    if (!(d > THRD || d < -THRD)) continue;
-                    T2[s] = d;
-                }
-            }
-#pragma unroll
-            for (int s = 0; s < NM; ++s) {
-                if (s >= P.S) continue;
-                const double d = T2[s];
-                if (!(d > THRD || d < -THRD)) continue;
-                if (s < n_mobile) dC[s] += d;
-                else imm[(int64_t)s * G.N + nd] += d;
-            }
-        }
+        TC dC[NM];  // increments of the mobile species, in the arithmetic type of the deposit
+        node_kinetics<TC, NM, EXT>(P, S, X, k, code, west, east, n_mobile, rb, imm, bio, dC);
         // ---- phase 2: collide, deposit, stream, species by species from the shared slots
-        TC dep[NM];
-#pragma unroll
-        for (int m = 0; m < NM; ++m) dep[m] = (TC)dC[m];
+        if (ODD) odd_sources(S, k, nb);  // recomputed rather than kept live through the kinetics
         const TC ux = u[k], uy = u[K + k], uz = u[2 * K + k];
 #pragma unroll
         for (int m = 0; m < NM; ++m) {
@@ -273,7 +286,7 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>()))
                 const TC omw = (TC)1 - w;
                 const TC rho = rb[m] + (TC)1;
                 const TC jx = rho * ux, jy = rho * uy, jz = rho * uz;
-                const TC d = dep[m];
+                const TC d = dC[m];
                 // feq_i = t_i (rb + 4 c_i . j), in opposite-pair form (no zero products)
                 const TC r8 = (TC)0.125 * rb[m], d8 = (TC)0.125 * d;
                 o[0] = q[0] * omw + w * ((TC)0.25 * rb[m]) + (TC)0.25 * d;
@@ -670,7 +683,7 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
 
 // Resident blocks per SM of a transport-step instantiation with `smem` bytes of shared memory
 // (set up once per instantiation), times the SM count: the persistent grid.
-static int ade_grid_for(const void* kern, int smem, int num_sms) {
+static int ade_grid_for(const void* kern, int smem, int num_sms, int threads) {
     static std::mutex mu;
     static std::vector<std::pair<const void*, int>> known;
     std::lock_guard<std::mutex> lock(mu);
@@ -678,7 +691,7 @@ static int ade_grid_for(const void* kern, int smem, int num_sms) {
         if (kv.first == kern) return kv.second * num_sms;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, ADE_THREADS, smem) != cudaSuccess || nb < 1) nb = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, smem) != cudaSuccess || nb < 1) nb = 1;
     known.push_back({kern, nb});
     return nb * num_sms;
 }
@@ -698,7 +711,7 @@ static void launch_ade_t(clb_handle* h) {
     do {                                                                                                          \
         auto kern = k_ade_aa<TS, TC, ODD, NM, EXT>;                                                               \
         const int sm = NM * 7 * ADE_THREADS * (int)sizeof(TC);                                                    \
-        const int gr = ade_grid_for((const void*)kern, sm, h->num_sms);                                           \
+        const int gr = ade_grid_for((const void*)kern, sm, h->num_sms, ADE_THREADS);                                           \
         kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,        \
                                                  h->ade_west_end, h->ade_east_begin, X);                          \
     } while (0)

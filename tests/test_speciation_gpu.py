@@ -146,11 +146,20 @@ def test_surrogate_gain_over_newton(trained):
     states = workloads.species_states(400000, 4, np.array(lo), np.array(hi), seed=7)
     D.speciation_solve(states[:1000])
     D.surrogate_predict(states[:1000])
-    t0 = time.perf_counter(); D.speciation_solve(states); t1 = time.perf_counter()
-    D.surrogate_predict(states, residual_check=False); t2 = time.perf_counter()
-    print("Newton-Raphson %.1f ms, surrogate + polish %.1f ms (400k states, host transfers included)"
-          % ((t1 - t0) * 1e3, (t2 - t1) * 1e3))
-    assert (t2 - t1) < (t1 - t0)
+
+    def best(fn, reps=3):
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return min(ts)
+
+    t_nr = best(lambda: D.speciation_solve(states))
+    t_sg = best(lambda: D.surrogate_predict(states, residual_check=False))
+    print("Newton-Raphson %.1f ms, surrogate + polish %.1f ms (400k states, host transfers included, best of 3)"
+          % (t_nr * 1e3, t_sg * 1e3))
+    assert t_sg < t_nr
 
 
 def test_surrogate_with_fallback_in_transport(clb, oracle, trained):
