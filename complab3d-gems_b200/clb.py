@@ -137,6 +137,11 @@ SIGNATURES = {
     "clb_reduce_noalloc": [C.c_void_p, C.POINTER(Stats)],
     "clb_set_abiotic_kinetics": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int],
     "clb_ca_setup": [C.c_void_p, C.POINTER(CaDesc)],
+    "clb_batch_create": [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)],
+    "clb_batch_step": [C.c_void_p, C.c_int, C.c_int, C.c_int],
+    "clb_batch_autotune": [C.c_void_p, C.c_int, C.c_char_p, C.c_int],
+    "clb_batch_counts": [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
+    "clb_batch_destroy": [C.c_void_p],
     "clb_ca_step": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "clb_refresh_dynamics": [C.c_void_p, C.c_int, C.c_int],
     "clb_precip_setup": [C.c_void_p, C.POINTER(PrecipDesc)],
@@ -525,3 +530,37 @@ class Domain:
         loss = np.zeros(1, dtype=np.float32)
         self._check(lib().clb_surrogate_gradient(self.h, _ptr(X), _ptr(Y), n, _ptr(g), _ptr(loss)))
         return g, float(loss[0])
+
+
+class Batch:
+    """An ensemble of Domains advanced together (clb_batch_*): one launch per lattice and step for
+    all of them, pairs of steps replayed from a CUDA graph. Results equal stepping each domain
+    on its own. The domains must stay alive and unchanged while the batch exists."""
+
+    def __init__(self, domains):
+        self.domains = list(domains)
+        arr = (C.c_void_p * len(self.domains))(*[d.h for d in self.domains])
+        b = C.c_void_p()
+        _check_global(lib().clb_batch_create(arr, len(self.domains), C.byref(b)))
+        self.b = b
+
+    def step(self, n=1, flow=True, transport=True):
+        _check_global(lib().clb_batch_step(self.b, int(n), int(flow), int(transport)))
+
+    def autotune(self, steps=20):
+        buf = C.create_string_buffer(512)
+        _check_global(lib().clb_batch_autotune(self.b, int(steps), buf, 512))
+        return buf.value.decode()
+
+    def counts(self):
+        a, t = C.c_int64(), C.c_int64()
+        _check_global(lib().clb_batch_counts(self.b, C.byref(a), C.byref(t)))
+        return a.value, t.value
+
+    def close(self):
+        if getattr(self, "b", None):
+            lib().clb_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        self.close()

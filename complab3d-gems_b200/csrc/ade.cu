@@ -18,6 +18,7 @@
 // advection velocity u[3][K] is in the arithmetic type.
 // Algorithmic bytes per node update: 2*7*sizeof(storage) per mobile species, plus the velocity
 // (3*sizeof(arith)) and the material byte shared by all species.
+#include "batch.cuh"
 #include "kinetics.cuh"
 #include "tma.cuh"
 
@@ -144,175 +145,189 @@ constexpr int ade_minb() {
 // shared memory (NM x 7 x ADE_THREADS values of the arithmetic type) between the gather and the
 // collision, so registers hold only the per-species sums and increments and many warps stay
 // resident to hide memory latency.
+// One node of the transport step (all species of compact node k): gather, boundary completion,
+// kinetics, collision, deposit, scatter. `sp` is the calling thread's slot base in shared memory
+// (NM x 7 values with stride `stride`). Shared by the single-domain and the batched steps.
+template <typename TS, typename TC, bool ODD, int NM, bool EXT, typename AP>
+__device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm,
+                                         double* __restrict__ bio, const TC* __restrict__ u, const SparseView& S,
+                                         const double* __restrict__ neu, const AP& P, int n_mobile,
+                                         const int* __restrict__ mob_species, int64_t k_west_end,
+                                         int64_t k_east_begin, const AdeExtra& X, TC* sp_base, int stride,
+                                         int64_t k) {
+    const Geom G = P.g;
+    const int64_t K = S.K, L = S.L;
+    const int64_t KS = S.KS;
+    const uint32_t K32 = (uint32_t)KS;  // row stride; 7 KS < 2^31 is checked when the layout is built
+    const int code = S.code[k];
+    const int dyn = P.dyn[code];
+    // a voxel sealed by precipitation bounces back: on AA slots that is the identity
+    if (dyn == ADE_BB) return;
+    const bool west = k < k_west_end, east = k >= k_east_begin;
+    int p = 0;
+    uint32_t wm = 0, blk = 0;
+    int lb = 0;
+    int nb[7];  // compact index of the source node a - c_i (odd step)
+    if (west || east) {
+        const int64_t n = S.node[k];
+        p = (int)(n % G.plane);
+    }
+    {
+        const uint32_t mt = S.meta[k];
+        wm = mt & 0x7Fu;
+        blk = wm | ((mt >> 7) & 0x7Fu);  // wall or outside the box
+        lb = S.tlb[(int)(k >> 8)] + (int)(mt >> 14);
+    }
+    if (ODD) odd_sources(S, k, nb);
+    // phase 1: every species' incoming populations (after the boundary completion) into this
+    // thread's own shared-memory slots, and their sums; only the sums stay in registers
+    uint32_t actm = 0;
+    TC rb[NM];
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+        rb[m] = 0;
+        if (m >= n_mobile) continue;
+        const int s = mob_species[m];
+        if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
+        actm |= 1u << m;
+        TS* f = g + (int64_t)m * 7 * KS;
+        const TS* lk = glink + (int64_t)m * L;
+        TC* slot = sp_base + (m * 7) * stride;
+        if constexpr (sizeof(TS) >= 4) {
+            // 4- and 8-byte populations go straight to the slots as asynchronous copies, so a
+            // thread has all of its loads in flight at once without holding them in registers
+#pragma unroll
+            for (int i = 0; i < 7; ++i) {
+                const TS* src = f + (uint32_t)(i * K32) + k;
+                if (!ODD) {
+                    const int oi = q7opp(i);
+                    // wall link (a, opp(i)): incoming i from the even-step slot X
+                    if (i != 0 && ((wm >> oi) & 1u)) src = lk + lb + __popc(wm & ((1u << oi) - 1u));
+                } else if (i != 0) {
+                    const int oi = q7opp(i);
+                    if (!((blk >> oi) & 1u)) src = f + (uint32_t)(oi * K32) + (uint32_t)nb[i];
+                }
+                cp_async<sizeof(TS)>(slot + i * stride, src);
+            }
+            if (!ODD && wm) {
+                // the odd-step slot Y = f[opp(i)][a] of a wall link is written back unchanged
+                // so its sector is written whole
+#pragma unroll
+                for (int i = 1; i < 7; ++i) {
+                    if (!((wm >> i) & 1u)) continue;
+                    TS* y = f + (uint32_t)(q7opp(i) * K32) + k;
+                    *y = *y;
+                }
+            }
+        } else {
+            TC q[7];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) {
+                if (!ODD || i == 0) { q[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
+                const int oi = q7opp(i);
+                if ((blk >> oi) & 1u) q[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k);
+                else q[i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)nb[i]);
+            }
+            if (!ODD && wm) {
+                // wall link (a, i): incoming opp(i) from the even-step slot X; the odd-step
+                // slot Y = f[opp(i)][a] is written back unchanged so its sector is written whole
+#pragma unroll
+                for (int i = 1; i < 7; ++i) {
+                    if (!((wm >> i) & 1u)) continue;
+                    const int oi = q7opp(i);
+                    st<TS, TC>(f + (uint32_t)(oi * K32) + k, q[oi]);
+                    q[oi] = ld<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)));
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 7; ++i) slot[i * stride] = q[i];
+        }
+    }
+    if constexpr (sizeof(TS) >= 4) cp_async_wait_all();  // each thread reads only its own slots
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+        if (!((actm >> m) & 1u)) continue;
+        TC* slot = sp_base + (m * 7) * stride;
+        if ((west || east) && dyn != ADE_NONE) {
+            // AdvectionDiffusionBoundaryDynamics: the one inward population makes the
+            // node's density equal to the stored value
+            const int s = mob_species[m];
+            const int type = west ? P.ltype[s] : P.rtype[s];
+            double rs;
+            if (type == CLB_DIRICHLET) rs = west ? P.lbc[s] : P.rbc[s];
+            else rs = neu[((int64_t)s * 2 + (west ? 0 : 1)) * G.plane + p];
+            const int miss = west ? 4 : 1;
+            TC sum = 0;
+#pragma unroll
+            for (int i = 0; i < 7; ++i)
+                if (i != miss) sum += slot[i * stride];
+            slot[miss * stride] = (TC)(rs - 1.0) - sum;
+        }
+        TC r = 0;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) r += slot[i * stride];
+        rb[m] = r;
+    }
+    TC dC[NM];  // increments of the mobile species, in the arithmetic type of the deposit
+    node_kinetics<TC, NM, EXT>(P, S, X, k, code, west, east, n_mobile, rb, imm, bio, dC);
+    // ---- phase 2: collide, deposit, stream, species by species from the shared slots
+    if (ODD) odd_sources(S, k, nb);  // recomputed rather than kept live through the kinetics
+    const TC ux = u[k], uy = u[K + k], uz = u[2 * K + k];
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+        if (!((actm >> m) & 1u)) continue;
+        const int s = mob_species[m];
+        TC q[7], o[7];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) q[i] = sp_base[(m * 7 + i) * stride];
+        if (dyn == ADE_NONE) {
+#pragma unroll
+            for (int i = 0; i < 7; ++i) o[i] = q[i];
+        } else {
+            const TC w = (TC)(dyn == ADE_BIO ? P.wbio[s] : P.wpore[s]);
+            const TC omw = (TC)1 - w;
+            const TC rho = rb[m] + (TC)1;
+            const TC jx = rho * ux, jy = rho * uy, jz = rho * uz;
+            const TC d = dC[m];
+            // feq_i = t_i (rb + 4 c_i . j), in opposite-pair form (no zero products)
+            const TC r8 = (TC)0.125 * rb[m], d8 = (TC)0.125 * d;
+            o[0] = q[0] * omw + w * ((TC)0.25 * rb[m]) + (TC)0.25 * d;
+            o[1] = q[1] * omw + w * (r8 - (TC)0.5 * jx) + d8;
+            o[4] = q[4] * omw + w * (r8 + (TC)0.5 * jx) + d8;
+            o[2] = q[2] * omw + w * (r8 - (TC)0.5 * jy) + d8;
+            o[5] = q[5] * omw + w * (r8 + (TC)0.5 * jy) + d8;
+            o[3] = q[3] * omw + w * (r8 - (TC)0.5 * jz) + d8;
+            o[6] = q[6] * omw + w * (r8 + (TC)0.5 * jz) + d8;
+        }
+        TS* f = g + (int64_t)m * 7 * KS;
+        TS* lk = glink + (int64_t)m * L;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            if (!ODD) {
+                if ((wm >> i) & 1u) st<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)), o[i]);
+                else st<TS, TC>(f + (uint32_t)(q7opp(i) * K32) + k, o[i]);
+                continue;
+            }
+            if (i == 0) { st<TS, TC>(f + k, o[0]); continue; }
+            const int oi = q7opp(i);
+            if ((blk >> i) & 1u) st<TS, TC>(f + (uint32_t)(oi * K32) + k, o[i]);
+            else st<TS, TC>(f + (uint32_t)(i * K32) + (uint32_t)nb[oi], o[i]);  // a + c_i = source of opp(i)
+        }
+    }
+}
+
 template <typename TS, typename TC, bool ODD, int NM, bool EXT>
 __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>()))
     k_ade_aa(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm, double* __restrict__ bio,
              const TC* __restrict__ u, const SparseView S, const double* __restrict__ neu, const AdeParams P,
              int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin,
              const AdeExtra X) {
-    const Geom G = P.g;
-    const int64_t K = S.K, L = S.L;
-    const int64_t KS = S.KS;
-    const uint32_t K32 = (uint32_t)KS;  // row stride; 7 KS < 2^31 is checked when the layout is built
+    const int64_t K = S.K;
     extern __shared__ __align__(16) unsigned char ade_smem[];
     TC* sp = reinterpret_cast<TC*>(ade_smem);
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
-        const int code = S.code[k];
-        const int dyn = P.dyn[code];
-        // a voxel sealed by precipitation bounces back: on AA slots that is the identity
-        if (dyn == ADE_BB) continue;
-        const bool west = k < k_west_end, east = k >= k_east_begin;
-        int p = 0;
-        uint32_t wm = 0, blk = 0;
-        int lb = 0;
-        int nb[7];  // compact index of the source node a - c_i (odd step)
-        if (west || east) {
-            const int64_t n = S.node[k];
-            p = (int)(n % G.plane);
-        }
-        {
-            const uint32_t mt = S.meta[k];
-            wm = mt & 0x7Fu;
-            blk = wm | ((mt >> 7) & 0x7Fu);  // wall or outside the box
-            lb = S.tlb[(int)(k >> 8)] + (int)(mt >> 14);
-        }
-        if (ODD) odd_sources(S, k, nb);
-        // phase 1: every species' incoming populations (after the boundary completion) into this
-        // thread's own shared-memory slots, and their sums; only the sums stay in registers
-        uint32_t actm = 0;
-        TC rb[NM];
-#pragma unroll
-        for (int m = 0; m < NM; ++m) {
-            rb[m] = 0;
-            if (m >= n_mobile) continue;
-            const int s = mob_species[m];
-            if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
-            actm |= 1u << m;
-            TS* f = g + (int64_t)m * 7 * KS;
-            const TS* lk = glink + (int64_t)m * L;
-            TC* slot = sp + (m * 7) * blockDim.x + threadIdx.x;
-            if constexpr (sizeof(TS) >= 4) {
-                // 4- and 8-byte populations go straight to the slots as asynchronous copies, so a
-                // thread has all of its loads in flight at once without holding them in registers
-#pragma unroll
-                for (int i = 0; i < 7; ++i) {
-                    const TS* src = f + (uint32_t)(i * K32) + k;
-                    if (!ODD) {
-                        const int oi = q7opp(i);
-                        // wall link (a, opp(i)): incoming i from the even-step slot X
-                        if (i != 0 && ((wm >> oi) & 1u)) src = lk + lb + __popc(wm & ((1u << oi) - 1u));
-                    } else if (i != 0) {
-                        const int oi = q7opp(i);
-                        if (!((blk >> oi) & 1u)) src = f + (uint32_t)(oi * K32) + (uint32_t)nb[i];
-                    }
-                    cp_async<sizeof(TS)>(slot + i * blockDim.x, src);
-                }
-                if (!ODD && wm) {
-                    // the odd-step slot Y = f[opp(i)][a] of a wall link is written back unchanged
-                    // so its sector is written whole
-#pragma unroll
-                    for (int i = 1; i < 7; ++i) {
-                        if (!((wm >> i) & 1u)) continue;
-                        TS* y = f + (uint32_t)(q7opp(i) * K32) + k;
-                        *y = *y;
-                    }
-                }
-            } else {
-                TC q[7];
-#pragma unroll
-                for (int i = 0; i < 7; ++i) {
-                    if (!ODD || i == 0) { q[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
-                    const int oi = q7opp(i);
-                    if ((blk >> oi) & 1u) q[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k);
-                    else q[i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)nb[i]);
-                }
-                if (!ODD && wm) {
-                    // wall link (a, i): incoming opp(i) from the even-step slot X; the odd-step
-                    // slot Y = f[opp(i)][a] is written back unchanged so its sector is written whole
-#pragma unroll
-                    for (int i = 1; i < 7; ++i) {
-                        if (!((wm >> i) & 1u)) continue;
-                        const int oi = q7opp(i);
-                        st<TS, TC>(f + (uint32_t)(oi * K32) + k, q[oi]);
-                        q[oi] = ld<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)));
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < 7; ++i) slot[i * blockDim.x] = q[i];
-            }
-        }
-        if constexpr (sizeof(TS) >= 4) cp_async_wait_all();  // each thread reads only its own slots
-#pragma unroll
-        for (int m = 0; m < NM; ++m) {
-            if (!((actm >> m) & 1u)) continue;
-            TC* slot = sp + (m * 7) * blockDim.x + threadIdx.x;
-            if ((west || east) && dyn != ADE_NONE) {
-                // AdvectionDiffusionBoundaryDynamics: the one inward population makes the
-                // node's density equal to the stored value
-                const int s = mob_species[m];
-                const int type = west ? P.ltype[s] : P.rtype[s];
-                double rs;
-                if (type == CLB_DIRICHLET) rs = west ? P.lbc[s] : P.rbc[s];
-                else rs = neu[((int64_t)s * 2 + (west ? 0 : 1)) * G.plane + p];
-                const int miss = west ? 4 : 1;
-                TC sum = 0;
-#pragma unroll
-                for (int i = 0; i < 7; ++i)
-                    if (i != miss) sum += slot[i * blockDim.x];
-                slot[miss * blockDim.x] = (TC)(rs - 1.0) - sum;
-            }
-            TC r = 0;
-#pragma unroll
-            for (int i = 0; i < 7; ++i) r += slot[i * blockDim.x];
-            rb[m] = r;
-        }
-        TC dC[NM];  // increments of the mobile species, in the arithmetic type of the deposit
-        node_kinetics<TC, NM, EXT>(P, S, X, k, code, west, east, n_mobile, rb, imm, bio, dC);
-        // ---- phase 2: collide, deposit, stream, species by species from the shared slots
-        if (ODD) odd_sources(S, k, nb);  // recomputed rather than kept live through the kinetics
-        const TC ux = u[k], uy = u[K + k], uz = u[2 * K + k];
-#pragma unroll
-        for (int m = 0; m < NM; ++m) {
-            if (!((actm >> m) & 1u)) continue;
-            const int s = mob_species[m];
-            TC q[7], o[7];
-#pragma unroll
-            for (int i = 0; i < 7; ++i) q[i] = sp[(m * 7 + i) * blockDim.x + threadIdx.x];
-            if (dyn == ADE_NONE) {
-#pragma unroll
-                for (int i = 0; i < 7; ++i) o[i] = q[i];
-            } else {
-                const TC w = (TC)(dyn == ADE_BIO ? P.wbio[s] : P.wpore[s]);
-                const TC omw = (TC)1 - w;
-                const TC rho = rb[m] + (TC)1;
-                const TC jx = rho * ux, jy = rho * uy, jz = rho * uz;
-                const TC d = dC[m];
-                // feq_i = t_i (rb + 4 c_i . j), in opposite-pair form (no zero products)
-                const TC r8 = (TC)0.125 * rb[m], d8 = (TC)0.125 * d;
-                o[0] = q[0] * omw + w * ((TC)0.25 * rb[m]) + (TC)0.25 * d;
-                o[1] = q[1] * omw + w * (r8 - (TC)0.5 * jx) + d8;
-                o[4] = q[4] * omw + w * (r8 + (TC)0.5 * jx) + d8;
-                o[2] = q[2] * omw + w * (r8 - (TC)0.5 * jy) + d8;
-                o[5] = q[5] * omw + w * (r8 + (TC)0.5 * jy) + d8;
-                o[3] = q[3] * omw + w * (r8 - (TC)0.5 * jz) + d8;
-                o[6] = q[6] * omw + w * (r8 + (TC)0.5 * jz) + d8;
-            }
-            TS* f = g + (int64_t)m * 7 * KS;
-            TS* lk = glink + (int64_t)m * L;
-#pragma unroll
-            for (int i = 0; i < 7; ++i) {
-                if (!ODD) {
-                    if ((wm >> i) & 1u) st<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)), o[i]);
-                    else st<TS, TC>(f + (uint32_t)(q7opp(i) * K32) + k, o[i]);
-                    continue;
-                }
-                if (i == 0) { st<TS, TC>(f + k, o[0]); continue; }
-                const int oi = q7opp(i);
-                if ((blk >> i) & 1u) st<TS, TC>(f + (uint32_t)(oi * K32) + k, o[i]);
-                else st<TS, TC>(f + (uint32_t)(i * K32) + (uint32_t)nb[oi], o[i]);  // a + c_i = source of opp(i)
-            }
-        }
-    }
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
+        ade_node<TS, TC, ODD, NM, EXT>(g, glink, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end,
+                                       k_east_begin, X, sp + threadIdx.x, blockDim.x, k);
 }
 
 // The stored density of every Neumann plane node: the density of its inner neighbour as it
@@ -684,15 +699,16 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
 // Resident blocks per SM of a transport-step instantiation with `smem` bytes of shared memory
 // (set up once per instantiation), times the SM count: the persistent grid.
 static int ade_grid_for(const void* kern, int smem, int num_sms, int threads) {
+    struct Known { const void* kern; int smem, threads, blocks; };
     static std::mutex mu;
-    static std::vector<std::pair<const void*, int>> known;
+    static std::vector<Known> known;
     std::lock_guard<std::mutex> lock(mu);
     for (auto& kv : known)
-        if (kv.first == kern) return kv.second * num_sms;
+        if (kv.kern == kern && kv.smem == smem && kv.threads == threads) return kv.blocks * num_sms;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, smem) != cudaSuccess || nb < 1) nb = 1;
-    known.push_back({kern, nb});
+    known.push_back({kern, smem, threads, nb});
     return nb * num_sms;
 }
 
@@ -754,6 +770,101 @@ static void refresh_neumann(clb_handle* h) {
         case CLB_F64: launch_neumann<double, double>(h, odd); break;
         case CLB_F32: launch_neumann<float, float>(h, odd); break;
         default: launch_neumann<__half, float>(h, odd); break;
+    }
+}
+
+// ------------------------------------------------------------------ batched step of many domains
+
+__device__ __forceinline__ int batch_find(const int64_t* off, int n, int64_t t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One transport step of every domain (no abiotic law, no dissolution): the species nodes of all
+// domains form one index range; shared memory holds the slots, then the domain offsets.
+template <typename TS, typename TC, bool ODD, int NM>
+__global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>())) k_ade_batch(const BatchView B) {
+    extern __shared__ __align__(16) unsigned char ade_smem[];
+    TC* sp = reinterpret_cast<TC*>(ade_smem);
+    int64_t* soff = reinterpret_cast<int64_t*>(ade_smem + NM * 7 * ADE_THREADS * sizeof(TC));
+    for (int i = threadIdx.x; i <= B.ndom; i += blockDim.x) soff[i] = B.aoff[i];
+    __syncthreads();
+    const int64_t total = soff[B.ndom];
+    AdeExtra X;
+    X.iface = nullptr;
+    X.xidx = nullptr;
+    X.xdc = nullptr;
+    X.ng = 0;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int di = batch_find(soff, B.ndom, t);
+        const BatchDomain& d = B.dom[di];
+        ade_node<TS, TC, ODD, NM, false>((TS*)d.g, (TS*)d.glink, d.imm, d.bio, (const TC*)d.u, d.as, d.neu, d.ap,
+                                         d.n_mobile, d.mob, d.akw, d.ake, X, sp + threadIdx.x, blockDim.x,
+                                         t - soff[di]);
+    }
+}
+
+// the Neumann planes of every domain (as k_ade_neumann, over a list of planes)
+template <typename TS, typename TC>
+__global__ void k_neumann_batch(const BatchView B, int odd) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < B.joff[B.njobs];
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int j = batch_find(B.joff, B.njobs, t);
+        const NeumannJob J = B.jobs[j];
+        const BatchDomain& d = B.dom[J.d];
+        const Geom G = d.ap.g;
+        const int p = (int)(t - B.joff[j]);
+        const int xb = J.side == 0 ? 0 : G.nx - 1, xi = J.side == 0 ? 1 : G.nx - 2;
+        const int64_t nb = (int64_t)xb * G.plane + p, ni = (int64_t)xi * G.plane + p;
+        const int db = d.ap.dyn[d.mat[nb]], di = d.ap.dyn[d.mat[ni]];
+        if (!(db == ADE_PORE || db == ADE_BIO) || !(di == ADE_PORE || di == ADE_BIO)) continue;
+        const double c0 = d.ap.c0[J.s];
+        TC init[7], pop[7];
+        for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - 1.0));
+        natural<TS, TC, 7>(d.as, G, (const TS*)d.g + (int64_t)J.m * 7 * d.as.KS, (const TS*)d.glink + (int64_t)J.m * d.as.L,
+                           ni, odd, init, pop);
+        double r = 1.0;
+        for (int i = 0; i < 7; ++i) r += (double)pop[i];
+        d.neu[((int64_t)J.s * 2 + J.side) * G.plane + p] = r;
+    }
+}
+
+void launch_neumann_batch(const BatchView& B, int prec, bool odd, int grid, cudaStream_t st) {
+    if (B.njobs == 0) return;
+    switch (prec) {
+        case CLB_F64: k_neumann_batch<double, double><<<grid, 256, 0, st>>>(B, odd ? 1 : 0); break;
+        case CLB_F32: k_neumann_batch<float, float><<<grid, 256, 0, st>>>(B, odd ? 1 : 0); break;
+        default: k_neumann_batch<__half, float><<<grid, 256, 0, st>>>(B, odd ? 1 : 0); break;
+    }
+}
+
+template <typename TS, typename TC, bool ODD, int NM>
+static void launch_ade_batch_t(const BatchView& B, int grid_mult, int num_sms, cudaStream_t st) {
+    auto kern = k_ade_batch<TS, TC, ODD, NM>;
+    const int sm = NM * 7 * ADE_THREADS * (int)sizeof(TC) + (int)sizeof(int64_t) * (B.ndom + 1);
+    const int per_sm = ade_grid_for((const void*)kern, sm, 1, ADE_THREADS);
+    kern<<<per_sm * num_sms * grid_mult, ADE_THREADS, sm, st>>>(B);
+}
+
+template <typename TS, typename TC, bool ODD>
+static void launch_ade_batch_p(const BatchView& B, int nm, int grid_mult, int num_sms, cudaStream_t st) {
+    if (nm <= 1) launch_ade_batch_t<TS, TC, ODD, 1>(B, grid_mult, num_sms, st);
+    else if (nm <= 2) launch_ade_batch_t<TS, TC, ODD, 2>(B, grid_mult, num_sms, st);
+    else if (nm <= 4) launch_ade_batch_t<TS, TC, ODD, 4>(B, grid_mult, num_sms, st);
+    else if (nm <= 8) launch_ade_batch_t<TS, TC, ODD, 8>(B, grid_mult, num_sms, st);
+    else launch_ade_batch_t<TS, TC, ODD, 16>(B, grid_mult, num_sms, st);
+}
+
+void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_mult, int num_sms, cudaStream_t st) {
+    switch (prec) {
+        case CLB_F64: if (odd) launch_ade_batch_p<double, double, true>(B, nm, grid_mult, num_sms, st); else launch_ade_batch_p<double, double, false>(B, nm, grid_mult, num_sms, st); break;
+        case CLB_F32: if (odd) launch_ade_batch_p<float, float, true>(B, nm, grid_mult, num_sms, st); else launch_ade_batch_p<float, float, false>(B, nm, grid_mult, num_sms, st); break;
+        default: if (odd) launch_ade_batch_p<__half, float, true>(B, nm, grid_mult, num_sms, st); else launch_ade_batch_p<__half, float, false>(B, nm, grid_mult, num_sms, st); break;
     }
 }
 

@@ -292,6 +292,29 @@ clb_status clb_refresh_dynamics(clb_handle* h, int species, int flow) {
     return refresh_dynamics(h, species, flow);
 }
 
+clb_status clb_batch_create(clb_handle* const* handles, int n, clb_batch** out) {
+    if (!handles || !out) return fail(nullptr, CLB_INVALID_ARG, "null argument");
+    *out = nullptr;
+    return batch_create(handles, n, out);
+}
+
+clb_status clb_batch_step(clb_batch* batch, int n, int flow, int transport) {
+    if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
+    return batch_step(batch, n, flow, transport);
+}
+
+clb_status clb_batch_autotune(clb_batch* batch, int steps, char* report, int report_len) {
+    if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
+    return batch_autotune(batch, steps, report, report_len);
+}
+
+clb_status clb_batch_counts(clb_batch* batch, int64_t* flow_nodes, int64_t* transport_nodes) {
+    if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
+    return batch_counts(batch, flow_nodes, transport_nodes);
+}
+
+clb_status clb_batch_destroy(clb_batch* batch) { return batch_destroy(batch); }
+
 clb_status clb_reduce_noalloc(clb_handle* h, clb_stats* out) {
     if (!h || !out) return fail(h, CLB_INVALID_ARG, "null argument");
     CLB_ON_DEVICE(h);

@@ -305,6 +305,13 @@ AdeExtra ade_extra(clb_handle* h);
 void precip_free(clb_handle* h);
 inline const int8_t* flow_mat(const clb_handle* h) { return h->d_mat_flow ? h->d_mat_flow : h->d_mat; }
 
+// batch.cu
+clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out);
+clb_status batch_step(clb_batch* b, int n, int flow, int ade);
+clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len);
+clb_status batch_destroy(clb_batch* b);
+clb_status batch_counts(clb_batch* b, int64_t* flow_nodes, int64_t* ade_nodes);
+
 // biofilm_ca.cu
 clb_status ca_setup(clb_handle* h, const clb_ca_desc* d);
 clb_status ca_step(clb_handle* h, int* sweeps, int* mask_changed);

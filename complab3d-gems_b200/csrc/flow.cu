@@ -26,7 +26,7 @@
 // Algorithmic bytes per node update: 2 * 19 * sizeof(storage). Metadata read per node: 1 byte
 // material code and 4 bytes wall mask + link offset (even step); 1 byte code, 8 bytes masks and
 // 16 bytes neighbour-row offsets (odd step).
-#include "sparse.cuh"
+#include "batch.cuh"
 #include "tma.cuh"
 
 #include <algorithm>
@@ -186,6 +186,96 @@ __device__ void finish_step(Tracer* tr, double* partials, double block_total, in
 
 
 
+// One node of the AA step (the flow lattice's collide-and-stream at compact index k); returns
+// the node's |u|^2 when it is a BGK node (for the stored average energy), else 0. Shared by the
+// single-domain step and the batched step of many domains.
+template <typename TS, typename TC, bool ODD, typename FP>
+__device__ __forceinline__ double flow_node(TS* __restrict__ f, TS* __restrict__ link, const SparseView& S, const FP& P,
+                                            int64_t k, int64_t k_west_end, int64_t k_east_begin) {
+    const uint32_t K32 = (uint32_t)S.KS;  // row stride; 19 KS < 2^31 is checked when the layout is built
+    double e = 0.0;
+    const int code = S.code[k];
+    // a stored bounce-back node (a voxel sealed by precipitation): the identity on AA slots
+    if (P.dyn[code] == DYN_BB) return 0.0;
+    TC g[19];
+    int rb_[8];
+    uint32_t blk = 0, rbit = 0, wm = 0;
+    int lb = 0;
+    if (!ODD) {
+        // own slots; a wall link (a, i) takes its incoming opp(i) from its even-step slot X
+        // and its odd-step slot Y = f[opp(i)][a] is written back unchanged (whole sectors)
+        const uint32_t m0 = S.meta[2 * k];
+        wm = m0 & 0x7FFFFu;
+        lb = S.tlb[(int)(k >> 8)] + (int)(m0 >> 19);
+#pragma unroll
+        for (int i = 0; i < 19; ++i) g[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k);
+        if (wm) {
+#pragma unroll
+            for (int i = 1; i < 19; ++i) {
+                if (!((wm >> i) & 1u)) continue;
+                const int oi = q19opp(i);
+                st<TS, TC>(f + (uint32_t)(oi * K32) + k, g[oi]);
+                g[oi] = ld<TS, TC>(link + lb + __popc(wm & ((1u << i) - 1u)));
+            }
+        }
+    } else {
+        const uint32_t m0 = S.meta[2 * k], m1 = S.meta[2 * k + 1];
+        const int t = (int)(k >> 8);
+        blk = (m0 | m1) & 0x7FFFFu;  // wall or outside the box: the node's own opposite slot
+        rbit = m1 >> 19;
+        const int4 dv = *reinterpret_cast<const int4*>(S.dres + 8 * k);
+        const int* tb = S.tdb + 8 * t;
+        rb_[0] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);
+        rb_[1] = (int)k + tb[1] + (int16_t)((uint32_t)dv.x >> 16);
+        rb_[2] = (int)k + tb[2] + (int16_t)(dv.y & 0xFFFF);
+        rb_[3] = (int)k + tb[3] + (int16_t)((uint32_t)dv.y >> 16);
+        rb_[4] = (int)k + tb[4] + (int16_t)(dv.z & 0xFFFF);
+        rb_[5] = (int)k + tb[5] + (int16_t)((uint32_t)dv.z >> 16);
+        rb_[6] = (int)k + tb[6] + (int16_t)(dv.w & 0xFFFF);
+        rb_[7] = (int)k + tb[7] + (int16_t)((uint32_t)dv.w >> 16);
+#pragma unroll
+        for (int i = 0; i < 19; ++i) {
+            if (i == 0) { g[0] = ld<TS, TC>(f + k); continue; }
+            const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
+            if ((blk >> oi) & 1u) { g[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
+            int src;
+            if (cx == 0 && cy == 0) src = (int)k - cz;
+            else {
+                const int s8 = row8(-cx, -cy);
+                src = (cz == 0) ? rb_[s8] : (-cz > 0 ? rb_[s8] + (int)((rbit >> s8) & 1u) : rb_[s8] - 1);
+            }
+            g[i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)src);
+        }
+    }
+    if (P.dyn[code] == DYN_BGK) {
+        if (k < k_west_end) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
+        else if (k >= k_east_begin) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
+        e = (double)bgk19<TC>(g, (TC)P.omega[code]);
+    }
+    if (!ODD) {
+#pragma unroll
+        for (int i = 0; i < 19; ++i) {
+            if ((wm >> i) & 1u) st<TS, TC>(link + lb + __popc(wm & ((1u << i) - 1u)), g[i]);
+            else st<TS, TC>(f + (uint32_t)(q19opp(i) * K32) + k, g[i]);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 19; ++i) {
+            if (i == 0) { st<TS, TC>(f + k, g[0]); continue; }
+            const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
+            if ((blk >> i) & 1u) { st<TS, TC>(f + (uint32_t)(oi * K32) + k, g[i]); continue; }
+            int dst;
+            if (cx == 0 && cy == 0) dst = (int)k + cz;
+            else {
+                const int s8 = row8(cx, cy);
+                dst = (cz == 0) ? rb_[s8] : (cz > 0 ? rb_[s8] + (int)((rbit >> s8) & 1u) : rb_[s8] - 1);
+            }
+            st<TS, TC>(f + (uint32_t)(i * K32) + (uint32_t)dst, g[i]);
+        }
+    }
+    return e;
+}
+
 template <typename TS, typename TC, bool ODD, int MINB>
 __global__ void __launch_bounds__(FLOW_THREADS, MINB)
     k_flow_aa(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const FlowParams P,
@@ -193,89 +283,9 @@ __global__ void __launch_bounds__(FLOW_THREADS, MINB)
               int64_t k_east_begin) {
     if (trace && tr->converged) return;  // a batch continues past convergence as no-ops
     const int64_t K = S.K;
-    const uint32_t K32 = (uint32_t)S.KS;  // row stride; 19 KS < 2^31 is checked when the layout is built
     double esum = 0;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
-        const int code = S.code[k];
-        // a stored bounce-back node (a voxel sealed by precipitation): the identity on AA slots
-        if (P.dyn[code] == DYN_BB) continue;
-        TC g[19];
-        int rb_[8];
-        uint32_t blk = 0, rbit = 0, wm = 0;
-        int lb = 0;
-        if (!ODD) {
-            // own slots; a wall link (a, i) takes its incoming opp(i) from its even-step slot X
-            // and its odd-step slot Y = f[opp(i)][a] is written back unchanged (whole sectors)
-            const uint32_t m0 = S.meta[2 * k];
-            wm = m0 & 0x7FFFFu;
-            lb = S.tlb[(int)(k >> 8)] + (int)(m0 >> 19);
-#pragma unroll
-            for (int i = 0; i < 19; ++i) g[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k);
-            if (wm) {
-#pragma unroll
-                for (int i = 1; i < 19; ++i) {
-                    if (!((wm >> i) & 1u)) continue;
-                    const int oi = q19opp(i);
-                    st<TS, TC>(f + (uint32_t)(oi * K32) + k, g[oi]);
-                    g[oi] = ld<TS, TC>(link + lb + __popc(wm & ((1u << i) - 1u)));
-                }
-            }
-        } else {
-            const uint32_t m0 = S.meta[2 * k], m1 = S.meta[2 * k + 1];
-            const int t = (int)(k >> 8);
-            blk = (m0 | m1) & 0x7FFFFu;  // wall or outside the box: the node's own opposite slot
-            rbit = m1 >> 19;
-            const int4 dv = *reinterpret_cast<const int4*>(S.dres + 8 * k);
-            const int* tb = S.tdb + 8 * t;
-            rb_[0] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);
-            rb_[1] = (int)k + tb[1] + (int16_t)((uint32_t)dv.x >> 16);
-            rb_[2] = (int)k + tb[2] + (int16_t)(dv.y & 0xFFFF);
-            rb_[3] = (int)k + tb[3] + (int16_t)((uint32_t)dv.y >> 16);
-            rb_[4] = (int)k + tb[4] + (int16_t)(dv.z & 0xFFFF);
-            rb_[5] = (int)k + tb[5] + (int16_t)((uint32_t)dv.z >> 16);
-            rb_[6] = (int)k + tb[6] + (int16_t)(dv.w & 0xFFFF);
-            rb_[7] = (int)k + tb[7] + (int16_t)((uint32_t)dv.w >> 16);
-#pragma unroll
-            for (int i = 0; i < 19; ++i) {
-                if (i == 0) { g[0] = ld<TS, TC>(f + k); continue; }
-                const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
-                if ((blk >> oi) & 1u) { g[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
-                int src;
-                if (cx == 0 && cy == 0) src = (int)k - cz;
-                else {
-                    const int s8 = row8(-cx, -cy);
-                    src = (cz == 0) ? rb_[s8] : (-cz > 0 ? rb_[s8] + (int)((rbit >> s8) & 1u) : rb_[s8] - 1);
-                }
-                g[i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)src);
-            }
-        }
-        if (P.dyn[code] == DYN_BGK) {
-            if (k < k_west_end) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
-            else if (k >= k_east_begin) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
-            esum += (double)bgk19<TC>(g, (TC)P.omega[code]);
-        }
-        if (!ODD) {
-#pragma unroll
-            for (int i = 0; i < 19; ++i) {
-                if ((wm >> i) & 1u) st<TS, TC>(link + lb + __popc(wm & ((1u << i) - 1u)), g[i]);
-                else st<TS, TC>(f + (uint32_t)(q19opp(i) * K32) + k, g[i]);
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < 19; ++i) {
-                if (i == 0) { st<TS, TC>(f + k, g[0]); continue; }
-                const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
-                if ((blk >> i) & 1u) { st<TS, TC>(f + (uint32_t)(oi * K32) + k, g[i]); continue; }
-                int dst;
-                if (cx == 0 && cy == 0) dst = (int)k + cz;
-                else {
-                    const int s8 = row8(cx, cy);
-                    dst = (cz == 0) ? rb_[s8] : (cz > 0 ? rb_[s8] + (int)((rbit >> s8) & 1u) : rb_[s8] - 1);
-                }
-                st<TS, TC>(f + (uint32_t)(i * K32) + (uint32_t)dst, g[i]);
-            }
-        }
-    }
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
+        esum += flow_node<TS, TC, ODD>(f, link, S, P, k, k_west_end, k_east_begin);
     __shared__ double sh[32];
     double bt = block_sum(esum, sh);
     finish_step(tr, partials, bt, P.n_bgk, trace);
@@ -389,6 +399,46 @@ __global__ void __launch_bounds__(TILE, 2)
     __shared__ double sh[32];
     double bt = block_sum(esum, sh);
     finish_step(tr, partials, bt, P.n_bgk, trace);
+}
+
+// ------------------------------------------------------------------ batched step of many domains
+
+// largest d with off[d] <= t (off ascending, off[0] = 0)
+__device__ __forceinline__ int batch_domain(const int64_t* off, int ndom, int64_t t) {
+    int lo = 0, hi = ndom - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One AA step of every domain's flow lattice: the nodes of all domains form one index range.
+template <typename TS, typename TC, bool ODD>
+__global__ void __launch_bounds__(256) k_flow_batch(const BatchView B) {
+    extern __shared__ int64_t soff[];
+    for (int i = threadIdx.x; i <= B.ndom; i += blockDim.x) soff[i] = B.foff[i];
+    __syncthreads();
+    const int64_t total = soff[B.ndom];
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int di = batch_domain(soff, B.ndom, t);
+        const BatchDomain& d = B.dom[di];
+        flow_node<TS, TC, ODD>((TS*)d.f, (TS*)d.flink, d.fs, d.fp, t - soff[di], d.fkw, d.fke);
+    }
+}
+
+void launch_flow_batch(const BatchView& B, int prec, bool odd, int grid, int threads, cudaStream_t st) {
+    const size_t sm = sizeof(int64_t) * (B.ndom + 1);
+#define CLB_FB(TS, TC)                                                                      \
+    if (odd) k_flow_batch<TS, TC, true><<<grid, threads, sm, st>>>(B);                     \
+    else k_flow_batch<TS, TC, false><<<grid, threads, sm, st>>>(B);
+    switch (prec) {
+        case CLB_F64: CLB_FB(double, double); break;
+        case CLB_F32: CLB_FB(float, float); break;
+        default: CLB_FB(__half, float); break;
+    }
+#undef CLB_FB
 }
 
 // PressureGradient equilibrium (complab_functions.hh:82-94): BGK nodes t_i (rho(x) - 1),

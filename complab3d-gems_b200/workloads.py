@@ -88,6 +88,33 @@ def config3(scale=1, seed=1003):
                 bmax=100.0)
 
 
+def config5(n_domains=96, seed=1005, scale=1.0):
+    """Ensemble sweep: n_domains independent sphere packs of uneven sizes (inner nx in
+    {32, 48, 64, 96}, ny = nz in {24, 32, 48}, drawn from the seeded stream), porosity U[0.3, 0.5],
+    grain radius U[2, 4], flow tau U[0.6, 1.0] at pressure drop 1e-4, three species with D_pore
+    U[0.05, 0.2] (biofilm half of it), Dirichlet inlet / Neumann outlet, Monod decay with rate
+    constants log-uniform in [1e-6, 1e-3] and half-saturation 0.1. FP32. `scale` < 1 shrinks the
+    sizes (tests)."""
+    rng = np.random.default_rng(seed)
+    doms = []
+    for d in range(n_domains):
+        nxi = int(rng.choice([32, 48, 64, 96]))
+        nyz = int(rng.choice([24, 32, 48]))
+        nxi, nyz = max(8, int(nxi * scale)), max(6, int(nyz * scale))
+        phi = float(rng.uniform(0.3, 0.5))
+        mat, shape = sphere_pack_domain(nxi, nyz, nyz, phi, 2.0, 4.0, seed=seed * 1000 + d)
+        tau = float(rng.uniform(0.6, 1.0))
+        species = []
+        for s in range(3):
+            dp = float(rng.uniform(0.05, 0.2))
+            species.append(dict(omega_pore=omega_from_d(dp), omega_biofilm=omega_from_d(0.5 * dp), mobile=1,
+                                left_type=clb.DIRICHLET, right_type=clb.NEUMANN, left_bc=1.0, c0=0.0))
+        k = 10.0 ** rng.uniform(-6, -3, size=3)
+        doms.append(dict(mat=mat, shape=shape, tau=tau, delta_p=1e-4, species=species, law=clb.LAW_MONOD,
+                         params=list(k) + [0.1] * 3, dt=1.0))
+    return dict(name=f"ensemble of {n_domains} uneven sphere packs, D3Q19 + 3 x D3Q7 each", domains=doms)
+
+
 def carbonate_tableau():
     """The two-component carbonate tableau of the reference's equilibrium example
     (examples/04_equilibrium/CompLaB.xml): HCO3 and H are components; CO3 = HCO3 - H

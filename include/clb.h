@@ -320,6 +320,31 @@ clb_status clb_ca_step(clb_handle* h, int* sweeps, int* mask_changed);
  * change; re-solve the flow and couple its velocity afterwards as it does. */
 clb_status clb_refresh_dynamics(clb_handle* h, int species, int flow);
 
+/* ---------------------------------------------------------------- ensembles of domains */
+
+/* A parameter sweep: many independent domains (each its own handle, with its own size, geometry,
+ * relaxation times and species) advanced together. Every step of the batch is one launch per
+ * lattice covering the nodes of all domains, and pairs of steps are replayed from a captured CUDA
+ * graph, so many small uneven domains are not bound by launch overhead. Results are those of
+ * stepping each domain on its own, bit for bit. No counterpart in the reference (one domain per
+ * run there). The handles must share a device and storage precisions, be at the same step
+ * parity, and have no abiotic law, dissolution or speciation; they must stay unchanged (no
+ * re-initialisation) while the batch exists. */
+typedef struct clb_batch_s clb_batch;
+clb_status clb_batch_create(clb_handle* const* handles, int n, clb_batch** out);
+
+/* n steps of the flow lattices (flow != 0) and/or the species lattices (transport != 0) of every
+ * domain; returns once they are done. Each handle's iteration counters advance by n. */
+clb_status clb_batch_step(clb_batch* batch, int n, int flow, int transport);
+
+/* Times the launch shapes of the batched steps over `steps` steps per shape and keeps the
+ * fastest; the timed steps are real steps (the handles' counters show them). */
+clb_status clb_batch_autotune(clb_batch* batch, int steps, char* report, int report_len);
+
+/* Open (collide / stream) nodes of the flow and species lattices over all domains. */
+clb_status clb_batch_counts(clb_batch* batch, int64_t* flow_nodes, int64_t* transport_nodes);
+clb_status clb_batch_destroy(clb_batch* batch);
+
 /* ---------------------------------------------------------------- equilibrium speciation */
 
 #define CLB_MAX_EQ_SPECIES 16

@@ -1,0 +1,81 @@
+"""Ensembles of uneven domains advanced by the batched steps (one launch per lattice and step for
+all domains, pairs of steps replayed from a CUDA graph) against the same domains stepped one by
+one: the populations must agree bit for bit, in FP64 and FP32."""
+import numpy as np
+import pytest
+
+import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def build(clb, cfg, prec):
+    out = []
+    for d in cfg["domains"]:
+        nx, ny, nz = d["shape"]
+        D = clb.Domain(d["mat"], nx, ny, nz, d["tau"], flow_precision=prec, ade_precision=prec)
+        D.flow_init(d["delta_p"])
+        D.flow_step(30)
+        D.ade_init(d["species"])
+        D.couple_velocity()
+        D.set_kinetics(d["law"], d["params"], d["dt"])
+        out.append(D)
+    return out
+
+
+def assert_same(A, B):
+    for a, b in zip(A, B):
+        np.testing.assert_array_equal(a.flow_populations(), b.flow_populations())
+        for s in range(a.S):
+            np.testing.assert_array_equal(a.ade_populations(s), b.ade_populations(s))
+
+
+@pytest.mark.parametrize("prec", ["F64", "F32"])
+def test_batch_matches_single_domains(clb, prec):
+    cfg = workloads.config5(n_domains=7, seed=11, scale=0.5)
+    p = getattr(clb, prec)
+    A = build(clb, cfg, p)
+    B = build(clb, cfg, p)
+    batch = clb.Batch(B)
+    for n, flow, tr in ((10, True, True), (7, True, False), (5, False, True), (1, True, True)):
+        for D in A:
+            if flow:
+                D.flow_step(n)
+            if tr:
+                D.ade_step(n)
+        batch.step(n, flow=flow, transport=tr)
+    assert_same(A, B)
+    fa, ta = batch.counts()
+    assert fa == sum(D.flow_stats()["active_nodes"] for D in B)
+    batch.close()
+
+
+def test_batch_autotune_then_matches(clb):
+    cfg = workloads.config5(n_domains=5, seed=12, scale=0.5)
+    A = build(clb, cfg, clb.F32)
+    B = build(clb, cfg, clb.F32)
+    batch = clb.Batch(B)
+    rep = batch.autotune(4)
+    assert "flow" in rep and "transport" in rep
+    nf = B[0].flow_stats()["iterations"] - A[0].flow_stats()["iterations"]
+    nt = B[0].reduce()["ade_iterations"] - A[0].reduce()["ade_iterations"]
+    assert nf > 0 and nt > 0
+    for D in A:
+        D.flow_step(nf)
+        D.ade_step(nt)
+    batch.step(12)
+    for D in A:
+        D.flow_step(12)
+        D.ade_step(12)
+    assert_same(A, B)
+    batch.close()
+
+
+def test_batch_rejects_mixed_parity(clb):
+    cfg = workloads.config5(n_domains=2, seed=13, scale=0.5)
+    B = build(clb, cfg, clb.F32)
+    B[1].ade_step(1)
+    batch = clb.Batch(B)
+    with pytest.raises(clb.ClbError):
+        batch.step(2)
+    batch.close()
