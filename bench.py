@@ -15,7 +15,9 @@ Side measurements in the same JSON line (rank 0, one GPU; --no-extra skips them)
   "precision"  FP64 / FP32 / FP16-shifted flow throughput and the velocity, permeability and
                concentration errors of the reduced-precision paths against the FP64 path;
   "speciation" the 5 x 12 tableau in transport: Newton-Raphson against the trained surrogate
-               (time per step, solves per second, speed-up, error against Newton-Raphson).
+               (time per step, solves per second, speed-up, error against Newton-Raphson);
+  "ensemble"   96 uneven domains with flow and 3 species advanced by the batched, graph-replayed
+               steps: domain-steps per second and aggregate MLUPS.
 
 Multi-GPU: the domain does not shard on this path (single-domain solver); each rank advances
 its own replica and the value is the sum over ranks divided by the slowest rank's time.
@@ -315,9 +317,14 @@ def bench_speciation(clb, workloads, torch, local, steps=10):
     D.surrogate_set_check(0.02, 2, 1e-6)
     n_open = int(np.count_nonzero(mat == 2))
     times = {}
+    used = 0.0
     for mode in (clb.SPEC_OFF, clb.SPEC_NR, clb.SPEC_MLP_NR):
         D.set_speciation_mode(mode)
+        s0 = D.speciation_stats()
         times[mode] = timed_steps(torch, stream, D.ade_step, steps, 2) / steps
+        s1 = D.speciation_stats()
+        if mode == clb.SPEC_MLP_NR:
+            used = (s1["surrogate_used"] - s0["surrogate_used"]) / max(1, s1["solves"] - s0["solves"])
     # accuracy: one step from the same state under each mode
     conc0 = [D.ade_populations(s) for s in range(ns)]
     res = {}
@@ -327,7 +334,6 @@ def bench_speciation(clb, workloads, torch, local, steps=10):
         D.set_speciation_mode(mode)
         D.ade_step(1)
         res[mode] = np.array([D.concentration(s) for s in range(ns)])
-    st = D.speciation_stats()
     open_ = (mat == 2)
     a, b = res[clb.SPEC_MLP_NR][:, open_], res[clb.SPEC_NR][:, open_]
     rel = np.abs(a / np.where(b == 0, 1, b) - 1)
@@ -338,9 +344,55 @@ def bench_speciation(clb, workloads, torch, local, steps=10):
             "open_voxels": n_open, "nr_ms_per_step": t_nr, "surrogate_ms_per_step": t_ml,
             "nr_solves_per_s": n_open / (t_nr * 1e-3), "surrogate_solves_per_s": n_open / (t_ml * 1e-3),
             "speedup": t_nr / t_ml, "max_rel_err_vs_nr": float(rel.max()), "p99_rel_err_vs_nr": float(np.percentile(rel, 99)),
-            "surrogate_used_fraction": st["surrogate_used"] / max(1, st["solves"]),
+            "surrogate_used_fraction": used,
             "training": {"seconds": t_train, "val_mse": rep["val_mse"], "epochs": rep["epochs"],
                          "n_train": rep["n_train"], "source": "the run's own voxel states, jitter 0.6 decades"}}
+
+
+def bench_ensemble(clb, workloads, torch, local, steps=200):
+    """96 independent uneven domains (the parameter-sweep configuration), FP32, each with a D3Q19
+    flow and 3 D3Q7 species with Monod kinetics, advanced by the batched steps (one launch per
+    lattice and step for all domains, pairs of steps replayed from a CUDA graph) after the
+    batch autotuner, against the same domains stepped one after another."""
+    cfg = workloads.config5()
+    doms = []
+    for d in cfg["domains"]:
+        nx, ny, nz = d["shape"]
+        D = clb.Domain(d["mat"], nx, ny, nz, d["tau"], flow_precision=clb.F32, ade_precision=clb.F32, device=local)
+        D.flow_init(d["delta_p"])
+        D.flow_step(20)
+        D.ade_init(d["species"])
+        D.couple_velocity()
+        D.set_kinetics(d["law"], d["params"], d["dt"])
+        doms.append(D)
+    B = clb.Batch(doms)
+    tuned = B.autotune(10)
+    nf, nt = B.counts()
+    B.step(4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    B.step(steps)
+    dt = time.perf_counter() - t0
+    # the same domains one by one (each call enqueues its own launches)
+    k = 20
+    t1 = time.perf_counter()
+    for D in doms:
+        D.flow_step(k)
+        D.ade_step(k)
+    for D in doms:
+        D.sync()
+    dt1 = (time.perf_counter() - t1) / k
+    B.close()
+    for D in doms:
+        D.close()
+    n = len(doms)
+    upd = nf + 3 * nt
+    return {"workload": cfg["name"] + ", FP32", "domains": n, "flow_nodes": nf, "transport_nodes": nt,
+            "steps": steps, "ms_per_step": dt / steps * 1e3, "domain_steps_per_s": n * steps / dt,
+            "aggregate_mlups": upd * steps / dt / 1e6,
+            "unit": "domain-steps / s; MLUPS = flow node + species x transport node updates / s (1e6)",
+            "one_by_one_ms_per_step": dt1 * 1e3, "speedup_vs_one_by_one": dt1 / (dt / steps),
+            "autotune": tuned, "timing": "host clock around the batched steps (one synchronisation)"}
 
 
 def main():
@@ -443,7 +495,8 @@ def main():
     if rank == 0 and world == 1 and not a.no_extra and a.scale == 1.0:
         for key, fn in (("d3q7", lambda: bench_d3q7(clb, workloads, torch, local, peak)),
                         ("precision", lambda: bench_precision(clb, workloads, torch, local)),
-                        ("speciation", lambda: bench_speciation(clb, workloads, torch, local))):
+                        ("speciation", lambda: bench_speciation(clb, workloads, torch, local)),
+                        ("ensemble", lambda: bench_ensemble(clb, workloads, torch, local))):
             try:
                 extra[key] = fn()
             except Exception as exc:  # a failed side measurement must not hide the headline line
