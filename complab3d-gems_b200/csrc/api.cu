@@ -136,6 +136,12 @@ clb_status clb_tune(clb_handle* h, const char* key, int value) {
     if (!h || !key) return fail(h, CLB_INVALID_ARG, "null argument");
     const std::string k = key;
     if (k == "flow_even_tma") { h->flow_even_tma = value ? 1 : 0; return CLB_OK; }
+    if (k == "flow_odd_pipe") {
+        if (value && h->flow_ready && !h->flow_pipe_grid)
+            return fail(h, CLB_INVALID_ARG, "flow_odd_pipe needs 4- or 8-byte flow storage");
+        h->flow_odd_pipe = value ? 1 : 0;
+        return CLB_OK;
+    }
     if (k == "flow_min_blocks") {
         if (value != 2 && value != 3) return fail(h, CLB_INVALID_ARG, "flow_min_blocks is 2 or 3");
         h->flow_minb = value;

@@ -188,6 +188,8 @@ struct clb_handle_s {
     int flow_even_tma = 1;            // even AA step through shared-memory tiles and bulk copies
     int flow_minb = 3;                // minimum resident CTAs per SM of the gather/scatter step (2 or 3)
     int flow_even_grid = 0;
+    int flow_odd_pipe = 1;            // odd step pipelined through shared memory (4- and 8-byte storage)
+    int flow_pipe_grid = 0;           // its resident-CTA grid; 0 where it is not available
     int* d_err = nullptr;             // device error flag (bounded waits that gave up)
     int64_t flow_iters = 0;           // host mirror of the device iteration count
     double delta_p = 0;

@@ -186,15 +186,91 @@ __device__ void finish_step(Tracer* tr, double* partials, double block_total, in
 
 
 
+// The per-node metadata a step reads before the populations (loaded one node ahead by the
+// single-domain step so its latency overlaps the previous node's work).
+struct FlowMeta {
+    int code;
+    uint32_t m0, m1;
+    int4 dv;
+};
+
+template <bool ODD>
+__device__ __forceinline__ FlowMeta flow_meta(const SparseView& S, int64_t k) {
+    FlowMeta M;
+    M.code = S.code[k];
+    M.m0 = S.meta[2 * k];
+    if (ODD) {
+        M.m1 = S.meta[2 * k + 1];
+        M.dv = *reinterpret_cast<const int4*>(S.dres + 8 * k);
+    } else {
+        M.m1 = 0;
+        M.dv = make_int4(0, 0, 0, 0);
+    }
+    return M;
+}
+
+// Odd-step geometry of node k from its metadata: the compact index bases of its 8 neighbour rows
+// (rb), the directions whose neighbour is a wall or outside the box (blk) and the row-parity bits.
+struct OddRows {
+    int rb[8];
+    uint32_t blk, rbit;
+};
+
+__device__ __forceinline__ OddRows odd_rows(const SparseView& S, int64_t k, const FlowMeta& M) {
+    OddRows R;
+    const int t = (int)(k >> 8);
+    R.blk = (M.m0 | M.m1) & 0x7FFFFu;  // wall or outside the box: the node's own opposite slot
+    R.rbit = M.m1 >> 19;
+    const int4 dv = M.dv;
+    const int* tb = S.tdb + 8 * t;
+    R.rb[0] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);
+    R.rb[1] = (int)k + tb[1] + (int16_t)((uint32_t)dv.x >> 16);
+    R.rb[2] = (int)k + tb[2] + (int16_t)(dv.y & 0xFFFF);
+    R.rb[3] = (int)k + tb[3] + (int16_t)((uint32_t)dv.y >> 16);
+    R.rb[4] = (int)k + tb[4] + (int16_t)(dv.z & 0xFFFF);
+    R.rb[5] = (int)k + tb[5] + (int16_t)((uint32_t)dv.z >> 16);
+    R.rb[6] = (int)k + tb[6] + (int16_t)(dv.w & 0xFFFF);
+    R.rb[7] = (int)k + tb[7] + (int16_t)((uint32_t)dv.w >> 16);
+    return R;
+}
+
+// storage slot (row offset + index) an odd step reads incoming population i of node k from
+__device__ __forceinline__ uint32_t odd_src(int i, int64_t k, const OddRows& R, uint32_t K32) {
+    if (i == 0) return (uint32_t)k;
+    const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
+    if ((R.blk >> oi) & 1u) return (uint32_t)(i * K32) + (uint32_t)k;
+    int src;
+    if (cx == 0 && cy == 0) src = (int)k - cz;
+    else {
+        const int s8 = row8(-cx, -cy);
+        src = (cz == 0) ? R.rb[s8] : (-cz > 0 ? R.rb[s8] + (int)((R.rbit >> s8) & 1u) : R.rb[s8] - 1);
+    }
+    return (uint32_t)(oi * K32) + (uint32_t)src;
+}
+
+// storage slot an odd step writes outgoing population i of node k to
+__device__ __forceinline__ uint32_t odd_dst(int i, int64_t k, const OddRows& R, uint32_t K32) {
+    if (i == 0) return (uint32_t)k;
+    const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
+    if ((R.blk >> i) & 1u) return (uint32_t)(oi * K32) + (uint32_t)k;
+    int dst;
+    if (cx == 0 && cy == 0) dst = (int)k + cz;
+    else {
+        const int s8 = row8(cx, cy);
+        dst = (cz == 0) ? R.rb[s8] : (cz > 0 ? R.rb[s8] + (int)((R.rbit >> s8) & 1u) : R.rb[s8] - 1);
+    }
+    return (uint32_t)(i * K32) + (uint32_t)dst;
+}
+
 // One node of the AA step (the flow lattice's collide-and-stream at compact index k); returns
 // the node's |u|^2 when it is a BGK node (for the stored average energy), else 0. Shared by the
 // single-domain step and the batched step of many domains.
 template <typename TS, typename TC, bool ODD, typename FP>
-__device__ __forceinline__ double flow_node(TS* __restrict__ f, TS* __restrict__ link, const SparseView& S, const FP& P,
-                                            int64_t k, int64_t k_west_end, int64_t k_east_begin) {
+__device__ __forceinline__ double flow_node_m(TS* __restrict__ f, TS* __restrict__ link, const SparseView& S, const FP& P,
+                                              int64_t k, int64_t k_west_end, int64_t k_east_begin, const FlowMeta& M) {
     const uint32_t K32 = (uint32_t)S.KS;  // row stride; 19 KS < 2^31 is checked when the layout is built
     double e = 0.0;
-    const int code = S.code[k];
+    const int code = M.code;
     // a stored bounce-back node (a voxel sealed by precipitation): the identity on AA slots
     if (P.dyn[code] == DYN_BB) return 0.0;
     TC g[19];
@@ -204,7 +280,7 @@ __device__ __forceinline__ double flow_node(TS* __restrict__ f, TS* __restrict__
     if (!ODD) {
         // own slots; a wall link (a, i) takes its incoming opp(i) from its even-step slot X
         // and its odd-step slot Y = f[opp(i)][a] is written back unchanged (whole sectors)
-        const uint32_t m0 = S.meta[2 * k];
+        const uint32_t m0 = M.m0;
         wm = m0 & 0x7FFFFu;
         lb = S.tlb[(int)(k >> 8)] + (int)(m0 >> 19);
 #pragma unroll
@@ -219,11 +295,11 @@ __device__ __forceinline__ double flow_node(TS* __restrict__ f, TS* __restrict__
             }
         }
     } else {
-        const uint32_t m0 = S.meta[2 * k], m1 = S.meta[2 * k + 1];
+        const uint32_t m0 = M.m0, m1 = M.m1;
         const int t = (int)(k >> 8);
         blk = (m0 | m1) & 0x7FFFFu;  // wall or outside the box: the node's own opposite slot
         rbit = m1 >> 19;
-        const int4 dv = *reinterpret_cast<const int4*>(S.dres + 8 * k);
+        const int4 dv = M.dv;
         const int* tb = S.tdb + 8 * t;
         rb_[0] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);
         rb_[1] = (int)k + tb[1] + (int16_t)((uint32_t)dv.x >> 16);
@@ -276,6 +352,79 @@ __device__ __forceinline__ double flow_node(TS* __restrict__ f, TS* __restrict__
     return e;
 }
 
+template <typename TS, typename TC, bool ODD, typename FP>
+__device__ __forceinline__ double flow_node(TS* __restrict__ f, TS* __restrict__ link, const SparseView& S, const FP& P,
+                                            int64_t k, int64_t k_west_end, int64_t k_east_begin) {
+    return flow_node_m<TS, TC, ODD>(f, link, S, P, k, k_west_end, k_east_begin, flow_meta<ODD>(S, k));
+}
+
+// Odd AA step with the gathers of the next node in flight while a node is collided: each thread
+// stages a node's 19 incoming populations in its own two shared-memory slots with asynchronous
+// copies (4- and 8-byte storage), one node ahead, and the node after that has its metadata
+// loading. Same arithmetic and stores as the plain step.
+template <typename TS, typename TC, int MINB>
+__global__ void __launch_bounds__(FLOW_THREADS, MINB)
+    k_flow_odd_pipe(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const FlowParams P,
+                    Tracer* __restrict__ tr, double* __restrict__ partials, int trace, int64_t k_west_end,
+                    int64_t k_east_begin) {
+    if (trace && tr->converged) return;
+    extern __shared__ __align__(16) unsigned char flow_smem[];
+    TS* buf = reinterpret_cast<TS*>(flow_smem);  // [2][19][blockDim.x]
+    const int64_t K = S.K;
+    const uint32_t K32 = (uint32_t)S.KS;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int64_t stride = (int64_t)gridDim.x * nt;
+    double esum = 0;
+    auto issue = [&](int64_t kk, const FlowMeta& M, int q) {
+        const OddRows R = odd_rows(S, kk, M);
+        TS* dst = buf + (q * 19) * nt + tid;
+#pragma unroll
+        for (int i = 0; i < 19; ++i) cp_async<sizeof(TS)>(dst + i * nt, f + odd_src(i, kk, R, K32));
+    };
+    int64_t k = (int64_t)blockIdx.x * nt + tid;
+    FlowMeta cur, nxt;
+    if (k < K) {
+        cur = flow_meta<true>(S, k);
+        issue(k, cur, 0);
+    }
+    cp_async_commit();
+    int64_t kn = k + stride;
+    if (kn < K) nxt = flow_meta<true>(S, kn);
+    int q = 0;
+    while (k < K) {
+        if (kn < K) issue(kn, nxt, q ^ 1);
+        cp_async_commit();
+        const int64_t knn = kn + stride;
+        FlowMeta nn;
+        if (knn < K) nn = flow_meta<true>(S, knn);
+        cp_async_wait_group<1>();  // this node's populations have landed
+        const int code = cur.code;
+        if (P.dyn[code] != DYN_BB) {  // a stored bounce-back node: identity on AA slots
+            TC g[19];
+            const TS* src = buf + (q * 19) * nt + tid;
+#pragma unroll
+            for (int i = 0; i < 19; ++i) g[i] = ld<TS, TC>(src + i * nt);
+            if (P.dyn[code] == DYN_BGK) {
+                if (k < k_west_end) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
+                else if (k >= k_east_begin) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
+                esum += (double)bgk19<TC>(g, (TC)P.omega[code]);
+            }
+            const OddRows R = odd_rows(S, k, cur);
+#pragma unroll
+            for (int i = 0; i < 19; ++i) st<TS, TC>(f + odd_dst(i, k, R, K32), g[i]);
+        }
+        k = kn;
+        kn = knn;
+        cur = nxt;
+        nxt = nn;
+        q ^= 1;
+    }
+    cp_async_wait_group<0>();
+    __shared__ double sh[32];
+    double bt = block_sum(esum, sh);
+    finish_step(tr, partials, bt, P.n_bgk, trace);
+}
+
 template <typename TS, typename TC, bool ODD, int MINB>
 __global__ void __launch_bounds__(FLOW_THREADS, MINB)
     k_flow_aa(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const FlowParams P,
@@ -284,8 +433,18 @@ __global__ void __launch_bounds__(FLOW_THREADS, MINB)
     if (trace && tr->converged) return;  // a batch continues past convergence as no-ops
     const int64_t K = S.K;
     double esum = 0;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
-        esum += flow_node<TS, TC, ODD>(f, link, S, P, k, k_west_end, k_east_begin);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    FlowMeta cur;
+    if (k < K) cur = flow_meta<ODD>(S, k);
+    while (k < K) {
+        const int64_t kn = k + stride;
+        FlowMeta nxt;
+        if (kn < K) nxt = flow_meta<ODD>(S, kn);  // the next node's metadata in flight meanwhile
+        esum += flow_node_m<TS, TC, ODD>(f, link, S, P, k, k_west_end, k_east_begin, cur);
+        cur = nxt;
+        k = kn;
+    }
     __shared__ double sh[32];
     double bt = block_sum(esum, sh);
     finish_step(tr, partials, bt, P.n_bgk, trace);
@@ -573,6 +732,24 @@ static size_t even_smem() {
     return (size_t)NSTAGE * 19 * TILE * sizeof(TS);
 }
 
+// two slots of 19 populations per thread for the pipelined odd step
+template <typename TS>
+static size_t pipe_smem() {
+    return (size_t)2 * 19 * FLOW_THREADS * sizeof(TS);
+}
+
+// resident-CTA grid of the pipelined odd step (0: not available for 2-byte storage, whose
+// populations are below the 4-byte granule of the asynchronous copy)
+template <typename TS, typename TC>
+static int pipe_grid_of(clb_handle* h) {
+    if (sizeof(TS) < 4) return 0;
+    int per_sm = 0;
+    const size_t sm = pipe_smem<TS>();
+    cudaFuncSetAttribute(k_flow_odd_pipe<TS, TC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_odd_pipe<TS, TC, 2>, FLOW_THREADS, sm);
+    return h->num_sms * std::min(8, std::max(1, per_sm));
+}
+
 
 template <typename F>
 static int grid_for(clb_handle* h, F kernel, int threads) {
@@ -685,6 +862,12 @@ clb_status flow_init(clb_handle* h, double delta_p) {
         }
         h->flow_even_grid = h->num_sms * std::max(1, per_sm);
     }
+    switch (h->flow_prec) {
+        case CLB_F64: h->flow_pipe_grid = pipe_grid_of<double, double>(h); break;
+        case CLB_F32: h->flow_pipe_grid = pipe_grid_of<float, float>(h); break;
+        default: h->flow_pipe_grid = 0; break;
+    }
+    if (!h->flow_pipe_grid) h->flow_odd_pipe = 0;
     // partials sized for the largest grid any variant uses
     const int pcap = h->num_sms * 8;
     if ((e = cudaMalloc(&h->d_partials, sizeof(double) * pcap)) != cudaSuccess) return cuda_check(h, e, "partials");
@@ -723,6 +906,18 @@ static void launch_flow(clb_handle* h, bool odd, int trace) {
         }
 #undef CLB_EVEN
         return;
+    }
+    if (odd && h->flow_odd_pipe && h->flow_pipe_grid) {
+        const int pg = h->flow_pipe_grid;
+#define CLB_PIPE(TS, TC)                                                                                       \
+        k_flow_odd_pipe<TS, TC, 2><<<pg, FLOW_THREADS, pipe_smem<TS>(), h->stream>>>(                          \
+            (TS*)h->d_f, (TS*)h->d_flink, S, P, h->d_tracer, h->d_partials, trace, h->k_west_end, h->k_east_begin);
+        switch (h->flow_prec) {
+            case CLB_F64: CLB_PIPE(double, double); return;
+            case CLB_F32: CLB_PIPE(float, float); return;
+            default: break;
+        }
+#undef CLB_PIPE
     }
 #define CLB_LAUNCH_B(TS, TC, B)                                                                                \
     if (odd)                                                                                                   \
@@ -905,8 +1100,8 @@ clb_status flow_stats(clb_handle* h, double char_length, clb_flow_stats* out) {
     return CLB_OK;
 }
 
-// Times every kernel variant (even step through TMA tiles or not; gather step compiled for 2 or
-// 3 resident CTAs) over `steps` steps and keeps the fastest. The lattice state is saved before
+// Times every kernel variant (even step through TMA tiles or not; odd step compiled for 2 or 3
+// resident CTAs, or pipelined through shared memory) over `steps` steps and keeps the fastest. The lattice state is saved before
 // and restored after, so the run is unchanged. Writes a one-line report into `report`.
 clb_status flow_autotune(clb_handle* h, int steps, char* report, int report_len) {
     if (steps < 2) steps = 2;
@@ -924,17 +1119,20 @@ clb_status flow_autotune(clb_handle* h, int steps, char* report, int report_len)
     cudaMemcpyAsync(&tsave, h->d_tracer, sizeof(Tracer), cudaMemcpyDeviceToHost, h->stream);
     cudaStreamSynchronize(h->stream);
     const int64_t iters0 = h->flow_iters;
-    const int save_tma = h->flow_even_tma, save_minb = h->flow_minb;
+    const int save_tma = h->flow_even_tma, save_minb = h->flow_minb, save_pipe = h->flow_odd_pipe;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     float best = 1e30f;
-    int best_tma = save_tma, best_minb = save_minb;
+    int best_tma = save_tma, best_minb = save_minb, best_pipe = save_pipe;
     std::string rep;
     for (int tma = 1; tma >= 0; --tma)
-        for (int minb = 3; minb >= 2; --minb) {
+        for (int v = 0; v < 3; ++v) {  // odd step: 3 or 2 resident CTAs, or pipelined
+            const int minb = v == 1 ? 2 : 3, pipe = v == 2 ? 1 : 0;
+            if (pipe && !h->flow_pipe_grid) continue;
             h->flow_even_tma = tma;
             h->flow_minb = minb;
+            h->flow_odd_pipe = pipe;
             h->flow_grid = flow_gather_grid(h);
             flow_step(h, 2, false, 0.0);  // warm
             cudaEventRecord(a, h->stream);
@@ -944,14 +1142,16 @@ clb_status flow_autotune(clb_handle* h, int steps, char* report, int report_len)
             float ms = 0;
             cudaEventElapsedTime(&ms, a, b);
             char buf[96];
-            snprintf(buf, sizeof(buf), "%stma=%d,minb=%d:%.1fus", rep.empty() ? "" : " ", tma, minb, 1e3f * ms / steps);
+            if (pipe) snprintf(buf, sizeof(buf), "%stma=%d,pipe:%.1fus", rep.empty() ? "" : " ", tma, 1e3f * ms / steps);
+            else snprintf(buf, sizeof(buf), "%stma=%d,minb=%d:%.1fus", rep.empty() ? "" : " ", tma, minb, 1e3f * ms / steps);
             rep += buf;
-            if (ms < best) { best = ms; best_tma = tma; best_minb = minb; }
+            if (ms < best) { best = ms; best_tma = tma; best_minb = minb; best_pipe = pipe; }
         }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     h->flow_even_tma = best_tma;
     h->flow_minb = best_minb;
+    h->flow_odd_pipe = best_pipe;
     h->flow_grid = flow_gather_grid(h);
     cudaMemcpyAsync(h->d_f, sf, fb, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(h->d_flink, sl, lb, cudaMemcpyDeviceToDevice, h->stream);
@@ -961,7 +1161,8 @@ clb_status flow_autotune(clb_handle* h, int steps, char* report, int report_len)
     cudaFree(sl);
     h->flow_iters = iters0;
     char buf[64];
-    snprintf(buf, sizeof(buf), " -> tma=%d,minb=%d", best_tma, best_minb);
+    if (best_pipe) snprintf(buf, sizeof(buf), " -> tma=%d,pipe", best_tma);
+    else snprintf(buf, sizeof(buf), " -> tma=%d,minb=%d", best_tma, best_minb);
     rep += buf;
     if (report && report_len > 0) {
         std::strncpy(report, rep.c_str(), (size_t)report_len - 1);

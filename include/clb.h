@@ -158,7 +158,11 @@ clb_status clb_get_stream(clb_handle* h, void** stream);
  *   "flow_even_tma"  1: even AA step through shared-memory tiles and bulk copies (default),
  *                    0: the plain per-thread load/store step;
  *   "flow_min_blocks" 2 or 3: resident CTAs per SM the gather/scatter step is compiled for
- *                    (register budget 128 or 80 per thread); takes effect at clb_flow_init.
+ *                    (register budget 128 or 80 per thread); takes effect at clb_flow_init;
+ *   "flow_odd_pipe"  1: odd AA step with the next node's gathers staged in shared memory by
+ *                    asynchronous copies while a node is collided (default for FP64/FP32
+ *                    storage; an error for FP16 storage, which always runs the plain step),
+ *                    0: the plain step.
  * Unknown keys are an error. */
 clb_status clb_tune(clb_handle* h, const char* key, int value);
 

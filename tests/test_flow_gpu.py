@@ -13,23 +13,30 @@ pytestmark = pytest.mark.gpu
 BIO = dict(bio_codes=(3, 4), perm_ratio=(0.3, 0.0))
 
 
-def make_pair(clb, oracle, mat, shape, tau, dp, prec, even_tma=1, **bio):
+# kernel variants of the two AA half-steps: (even step through bulk-copied tiles, odd step
+# pipelined through shared memory)
+VARIANTS = {"tma": (1, 0), "plain": (0, 0), "pipe": (1, 1)}
+
+
+def make_pair(clb, oracle, mat, shape, tau, dp, prec, even_tma=1, odd_pipe=0, **bio):
     nx, ny, nz = shape
     D = clb.Domain(mat, nx, ny, nz, tau, flow_precision=prec, **bio)
     D.tune("flow_even_tma", even_tma)
+    D.tune("flow_odd_pipe", odd_pipe)
     D.flow_init(dp)
     O = oracle.OracleFlow(mat, nx, ny, nz, tau, dp, bio_codes=bio.get("bio_codes", ()),
                           perm_ratio=bio.get("perm_ratio", ()))
     return D, O
 
 
-@pytest.mark.parametrize("even_tma", [1, 0])
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
 @pytest.mark.parametrize("shape", [(18, 11, 9), (12, 7, 45), (40, 21, 33)])
 @pytest.mark.parametrize("walls", [True, False])
 @pytest.mark.parametrize("steps", [1, 2, 37, 200])
-def test_f64_populations_match_oracle(clb, oracle, shape, walls, steps, even_tma):
+def test_f64_populations_match_oracle(clb, oracle, shape, walls, steps, variant):
     mat = mixed_geometry(*shape, walls=walls)
-    D, O = make_pair(clb, oracle, mat, shape, 0.8, 3e-4, clb.F64, even_tma=even_tma, **BIO)
+    tma, pipe = VARIANTS[variant]
+    D, O = make_pair(clb, oracle, mat, shape, 0.8, 3e-4, clb.F64, even_tma=tma, odd_pipe=pipe, **BIO)
     D.flow_step(steps)
     O.step(steps)
     fg, fo = D.flow_populations(), O.populations()
@@ -51,12 +58,14 @@ def test_f64_solve_matches_oracle_iterations(clb, oracle):
     assert st["permeability"] > 0
 
 
-@pytest.mark.parametrize("even_tma", [1, 0])
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
 @pytest.mark.parametrize("prec,tol", [("F32", 1e-5), ("F16S", 3e-2)])
-def test_reduced_precision_velocity_error(clb, oracle, prec, tol, even_tma):
+def test_reduced_precision_velocity_error(clb, oracle, prec, tol, variant):
     shape = (26, 14, 14)
     mat = mixed_geometry(*shape, seed=9)
-    D, O = make_pair(clb, oracle, mat, shape, 0.8, 1e-4, getattr(clb, prec), even_tma=even_tma, **BIO)
+    tma, pipe = VARIANTS[variant]
+    # FP16 storage has no pipelined odd step: the knob set before initialisation falls back
+    D, O = make_pair(clb, oracle, mat, shape, 0.8, 1e-4, getattr(clb, prec), even_tma=tma, odd_pipe=pipe, **BIO)
     D.flow_step(400)
     O.step(400)
     err = rel_l2(D.velocity(), O.velocity())
@@ -103,7 +112,30 @@ def test_autotune_leaves_state_unchanged(clb, oracle):
     fluid = mat != 1
     assert np.max(np.abs(D.flow_populations()[:, fluid] - O.populations()[:, fluid])) < 1e-13
     D.tune("flow_min_blocks", 2)
+    D.tune("flow_odd_pipe", 1)
     with pytest.raises(clb.ClbError):
         D.tune("flow_min_blocks", 5)
     with pytest.raises(clb.ClbError):
         D.tune("no_such_knob", 1)
+
+
+def test_pipelined_odd_step_f32_matches_plain_bit_for_bit(clb):
+    """The pipelined odd step does the same arithmetic as the plain one: identical populations."""
+    shape = (34, 19, 23)
+    mat = mixed_geometry(*shape, seed=21)
+    out = []
+    for pipe in (0, 1):
+        D = clb.Domain(mat, *shape, 0.8, flow_precision=clb.F32, **BIO)
+        D.tune("flow_odd_pipe", pipe)
+        D.flow_init(2e-4)
+        D.flow_step(61)
+        out.append(D.flow_populations())
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_pipelined_odd_step_refused_for_fp16_storage(clb):
+    shape = (10, 6, 6)
+    D = clb.Domain(mixed_geometry(*shape), *shape, 0.8, flow_precision=clb.F16S)
+    D.flow_init(1e-4)
+    with pytest.raises(clb.ClbError):
+        D.tune("flow_odd_pipe", 1)
