@@ -53,6 +53,9 @@ def args_():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-extra", action="store_true", help="skip the D3Q7, precision and speciation legs")
     p.add_argument("--scale", type=float, default=1.0, help="shrink the workload (testing only)")
+    p.add_argument("--leg", choices=["d3q7", "precision", "speciation", "ensemble"],
+                   help="run only this side measurement (with --scale for d3q7) and print its JSON; "
+                        "a small case for profilers, not a bench line")
     return p.parse_args()
 
 
@@ -202,10 +205,10 @@ def timed_steps(torch, stream, step, steps, warmup):
     return e0.elapsed_time(e1)
 
 
-def bench_d3q7(clb, workloads, torch, local, peak, steps=60, warmup=5):
+def bench_d3q7(clb, workloads, torch, local, peak, steps=60, warmup=5, scale=1.0):
     """Fused transport of the 256^3 sphere pack with 8 species and 2 biofilm microbes (dual Monod),
     FP32 populations; the lattice (1.5 GB) is far larger than L2, so no flush is needed."""
-    cfg = workloads.config3()
+    cfg = workloads.config3(scale=scale)
     nx, ny, nz = cfg["shape"]
     mat = cfg["mat"]
     D = clb.Domain(mat, nx, ny, nz, cfg["tau"], flow_precision=clb.F32, ade_precision=clb.F32,
@@ -400,12 +403,22 @@ def main():
     import clb
     import workloads
 
-    cfg = workloads.config2(scale=a.scale)
     if a.impl == "reference":
-        run_reference(a, cfg)
+        run_reference(a, workloads.config2(scale=a.scale))
         return
 
     import torch
+
+    if a.leg:
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        fn = {"d3q7": lambda: bench_d3q7(clb, workloads, torch, local, peaks()[0], steps=10, warmup=3, scale=a.scale),
+              "precision": lambda: bench_precision(clb, workloads, torch, local),
+              "speciation": lambda: bench_speciation(clb, workloads, torch, local),
+              "ensemble": lambda: bench_ensemble(clb, workloads, torch, local)}[a.leg]
+        print(json.dumps({"leg": a.leg, "scale": a.scale, a.leg: fn()}))
+        return
+    cfg = workloads.config2(scale=a.scale)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

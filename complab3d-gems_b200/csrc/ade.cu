@@ -134,10 +134,17 @@ __device__ __forceinline__ void odd_sources(const SparseView& S, int64_t k, int 
     nb[6] = (int)k - 1;
 }
 
+// shared memory of a CTA of the transport step: the population slots (NM x 7 per thread, the
+// arithmetic type) and the 7 population offsets per thread
+template <typename TC, int NM>
+constexpr int ade_slot_bytes() {
+    return NM * 7 * ADE_THREADS * (int)sizeof(TC) + 7 * ADE_THREADS * (int)sizeof(uint32_t);
+}
+
 // resident blocks per SM the shared slots allow (about 200 KB of shared memory per SM)
 template <typename TC, int NM>
 constexpr int ade_minb() {
-    constexpr int b = (200 * 1024) / (NM * 7 * 128 * (int)sizeof(TC));
+    constexpr int b = (200 * 1024) / ade_slot_bytes<TC, NM>();
     return b < 1 ? 1 : (b > 4 ? 4 : b);
 }
 
@@ -146,15 +153,23 @@ constexpr int ade_minb() {
 // collision, so registers hold only the per-species sums and increments and many warps stay
 // resident to hide memory latency.
 // One node of the transport step (all species of compact node k): gather, boundary completion,
-// kinetics, collision, deposit, scatter. `sp` is the calling thread's slot base in shared memory
-// (NM x 7 values with stride `stride`). Shared by the single-domain and the batched steps.
+// kinetics, collision, deposit, scatter. `sp_base` is the calling thread's slot base in shared
+// memory (NM x 7 values with stride `stride`), `ob` its 7 slots for the population offsets.
+// Shared by the single-domain and the batched steps.
+//
+// Both AA steps are in-place permutations of 7 storage slots per node that every species shares:
+// incoming j is read from slot j and outgoing opp(j) is written back to slot j. Even step: slot j is
+// the node's own row j, or, for a wall link (a, i) with j = opp(i), the link's even-step slot X.
+// Odd step: slot j is row opp(j) of the source node a - c_j, or the node's own row j when that
+// source is a wall or outside the box. The offsets are computed once per node (bit 31 marks a
+// link slot) and serve the gathers and the scatters of every species.
 template <typename TS, typename TC, bool ODD, int NM, bool EXT, typename AP>
 __device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm,
                                          double* __restrict__ bio, const TC* __restrict__ u, const SparseView& S,
                                          const double* __restrict__ neu, const AP& P, int n_mobile,
                                          const int* __restrict__ mob_species, int64_t k_west_end,
-                                         int64_t k_east_begin, const AdeExtra& X, TC* sp_base, int stride,
-                                         int64_t k) {
+                                         int64_t k_east_begin, const AdeExtra& X, TC* sp_base, uint32_t* ob,
+                                         int stride, int64_t k) {
     const Geom G = P.g;
     const int64_t K = S.K, L = S.L;
     const int64_t KS = S.KS;
@@ -167,7 +182,6 @@ __device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ gl
     int p = 0;
     uint32_t wm = 0, blk = 0;
     int lb = 0;
-    int nb[7];  // compact index of the source node a - c_i (odd step)
     if (west || east) {
         const int64_t n = S.node[k];
         p = (int)(n % G.plane);
@@ -178,7 +192,27 @@ __device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ gl
         blk = wm | ((mt >> 7) & 0x7Fu);  // wall or outside the box
         lb = S.tlb[(int)(k >> 8)] + (int)(mt >> 14);
     }
-    if (ODD) odd_sources(S, k, nb);
+    constexpr uint32_t LINKF = 0x80000000u, OMASK = 0x7FFFFFFFu;
+    uint32_t off[7];
+    if (!ODD) {
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            const int oi = q7opp(i);
+            off[i] = (i != 0 && ((wm >> oi) & 1u)) ? (LINKF | (uint32_t)(lb + __popc(wm & ((1u << oi) - 1u))))
+                                                   : (uint32_t)(i * K32) + (uint32_t)k;
+        }
+    } else {
+        int nb[7];  // compact index of the source node a - c_i
+        odd_sources(S, k, nb);
+        off[0] = (uint32_t)k;
+#pragma unroll
+        for (int i = 1; i < 7; ++i) {
+            const int oi = q7opp(i);
+            off[i] = ((blk >> oi) & 1u) ? (uint32_t)(i * K32) + (uint32_t)k : (uint32_t)(oi * K32) + (uint32_t)nb[i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 7; ++i) ob[i * stride] = off[i];
     // phase 1: every species' incoming populations (after the boundary completion) into this
     // thread's own shared-memory slots, and their sums; only the sums stay in registers
     uint32_t actm = 0;
@@ -191,56 +225,32 @@ __device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ gl
         if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
         actm |= 1u << m;
         TS* f = g + (int64_t)m * 7 * KS;
-        const TS* lk = glink + (int64_t)m * L;
+        TS* lk = glink + (int64_t)m * L;
         TC* slot = sp_base + (m * 7) * stride;
+        if (!ODD && wm) {
+            // the odd-step slot Y = f[opp(i)][a] of a wall link (a, i) is written back unchanged so
+            // that its sector is written whole
+#pragma unroll
+            for (int i = 1; i < 7; ++i) {
+                if (!((wm >> i) & 1u)) continue;
+                TS* y = f + (uint32_t)(q7opp(i) * K32) + k;
+                *y = *y;
+            }
+        }
         if constexpr (sizeof(TS) >= 4) {
             // 4- and 8-byte populations go straight to the slots as asynchronous copies, so a
             // thread has all of its loads in flight at once without holding them in registers
 #pragma unroll
             for (int i = 0; i < 7; ++i) {
-                const TS* src = f + (uint32_t)(i * K32) + k;
-                if (!ODD) {
-                    const int oi = q7opp(i);
-                    // wall link (a, opp(i)): incoming i from the even-step slot X
-                    if (i != 0 && ((wm >> oi) & 1u)) src = lk + lb + __popc(wm & ((1u << oi) - 1u));
-                } else if (i != 0) {
-                    const int oi = q7opp(i);
-                    if (!((blk >> oi) & 1u)) src = f + (uint32_t)(oi * K32) + (uint32_t)nb[i];
-                }
+                const TS* src = (!ODD && (off[i] & LINKF)) ? lk + (off[i] & OMASK) : f + off[i];
                 cp_async<sizeof(TS)>(slot + i * stride, src);
             }
-            if (!ODD && wm) {
-                // the odd-step slot Y = f[opp(i)][a] of a wall link is written back unchanged
-                // so its sector is written whole
-#pragma unroll
-                for (int i = 1; i < 7; ++i) {
-                    if (!((wm >> i) & 1u)) continue;
-                    TS* y = f + (uint32_t)(q7opp(i) * K32) + k;
-                    *y = *y;
-                }
-            }
         } else {
-            TC q[7];
 #pragma unroll
             for (int i = 0; i < 7; ++i) {
-                if (!ODD || i == 0) { q[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
-                const int oi = q7opp(i);
-                if ((blk >> oi) & 1u) q[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k);
-                else q[i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)nb[i]);
+                const TS* src = (!ODD && (off[i] & LINKF)) ? lk + (off[i] & OMASK) : f + off[i];
+                slot[i * stride] = ld<TS, TC>(src);
             }
-            if (!ODD && wm) {
-                // wall link (a, i): incoming opp(i) from the even-step slot X; the odd-step
-                // slot Y = f[opp(i)][a] is written back unchanged so its sector is written whole
-#pragma unroll
-                for (int i = 1; i < 7; ++i) {
-                    if (!((wm >> i) & 1u)) continue;
-                    const int oi = q7opp(i);
-                    st<TS, TC>(f + (uint32_t)(oi * K32) + k, q[oi]);
-                    q[oi] = ld<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)));
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < 7; ++i) slot[i * stride] = q[i];
         }
     }
     if constexpr (sizeof(TS) >= 4) cp_async_wait_all();  // each thread reads only its own slots
@@ -271,7 +281,9 @@ __device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ gl
     TC dC[NM];  // increments of the mobile species, in the arithmetic type of the deposit
     node_kinetics<TC, NM, EXT>(P, S, X, k, code, west, east, n_mobile, rb, imm, bio, dC);
     // ---- phase 2: collide, deposit, stream, species by species from the shared slots
-    if (ODD) odd_sources(S, k, nb);  // recomputed rather than kept live through the kinetics
+    uint32_t off2[7];  // read back rather than kept live through the kinetics
+#pragma unroll
+    for (int i = 0; i < 7; ++i) off2[i] = ob[i * stride];
     const TC ux = u[k], uy = u[K + k], uz = u[2 * K + k];
 #pragma unroll
     for (int m = 0; m < NM; ++m) {
@@ -302,16 +314,9 @@ __device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ gl
         TS* f = g + (int64_t)m * 7 * KS;
         TS* lk = glink + (int64_t)m * L;
 #pragma unroll
-        for (int i = 0; i < 7; ++i) {
-            if (!ODD) {
-                if ((wm >> i) & 1u) st<TS, TC>(lk + lb + __popc(wm & ((1u << i) - 1u)), o[i]);
-                else st<TS, TC>(f + (uint32_t)(q7opp(i) * K32) + k, o[i]);
-                continue;
-            }
-            if (i == 0) { st<TS, TC>(f + k, o[0]); continue; }
-            const int oi = q7opp(i);
-            if ((blk >> i) & 1u) st<TS, TC>(f + (uint32_t)(oi * K32) + k, o[i]);
-            else st<TS, TC>(f + (uint32_t)(i * K32) + (uint32_t)nb[oi], o[i]);  // a + c_i = source of opp(i)
+        for (int j = 0; j < 7; ++j) {  // outgoing opp(j) back to slot j
+            TS* dst = (!ODD && (off2[j] & LINKF)) ? lk + (off2[j] & OMASK) : f + off2[j];
+            st<TS, TC>(dst, o[q7opp(j)]);
         }
     }
 }
@@ -325,9 +330,10 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>()))
     const int64_t K = S.K;
     extern __shared__ __align__(16) unsigned char ade_smem[];
     TC* sp = reinterpret_cast<TC*>(ade_smem);
+    uint32_t* ob = reinterpret_cast<uint32_t*>(ade_smem + (size_t)NM * 7 * blockDim.x * sizeof(TC));
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
         ade_node<TS, TC, ODD, NM, EXT>(g, glink, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end,
-                                       k_east_begin, X, sp + threadIdx.x, blockDim.x, k);
+                                       k_east_begin, X, sp + threadIdx.x, ob + threadIdx.x, blockDim.x, k);
 }
 
 // The stored density of every Neumann plane node: the density of its inner neighbour as it
@@ -726,7 +732,7 @@ static void launch_ade_t(clb_handle* h) {
 #define CLB_ADE(NM, EXT)                                                                                          \
     do {                                                                                                          \
         auto kern = k_ade_aa<TS, TC, ODD, NM, EXT>;                                                               \
-        const int sm = NM * 7 * ADE_THREADS * (int)sizeof(TC);                                                    \
+        const int sm = ade_slot_bytes<TC, NM>();                                                                  \
         const int gr = ade_grid_for((const void*)kern, sm, h->num_sms, ADE_THREADS);                                           \
         kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,        \
                                                  h->ade_west_end, h->ade_east_begin, X);                          \
@@ -791,7 +797,8 @@ template <typename TS, typename TC, bool ODD, int NM>
 __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>())) k_ade_batch(const BatchView B) {
     extern __shared__ __align__(16) unsigned char ade_smem[];
     TC* sp = reinterpret_cast<TC*>(ade_smem);
-    int64_t* soff = reinterpret_cast<int64_t*>(ade_smem + NM * 7 * ADE_THREADS * sizeof(TC));
+    uint32_t* ob = reinterpret_cast<uint32_t*>(ade_smem + (size_t)NM * 7 * ADE_THREADS * sizeof(TC));
+    int64_t* soff = reinterpret_cast<int64_t*>(ade_smem + ade_slot_bytes<TC, NM>());
     for (int i = threadIdx.x; i <= B.ndom; i += blockDim.x) soff[i] = B.aoff[i];
     __syncthreads();
     const int64_t total = soff[B.ndom];
@@ -804,8 +811,8 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>())) k_ade_batch
         const int di = batch_find(soff, B.ndom, t);
         const BatchDomain& d = B.dom[di];
         ade_node<TS, TC, ODD, NM, false>((TS*)d.g, (TS*)d.glink, d.imm, d.bio, (const TC*)d.u, d.as, d.neu, d.ap,
-                                         d.n_mobile, d.mob, d.akw, d.ake, X, sp + threadIdx.x, blockDim.x,
-                                         t - soff[di]);
+                                         d.n_mobile, d.mob, d.akw, d.ake, X, sp + threadIdx.x, ob + threadIdx.x,
+                                         blockDim.x, t - soff[di]);
     }
 }
 
@@ -846,7 +853,7 @@ void launch_neumann_batch(const BatchView& B, int prec, bool odd, int grid, cuda
 template <typename TS, typename TC, bool ODD, int NM>
 static void launch_ade_batch_t(const BatchView& B, int grid_mult, int num_sms, cudaStream_t st) {
     auto kern = k_ade_batch<TS, TC, ODD, NM>;
-    const int sm = NM * 7 * ADE_THREADS * (int)sizeof(TC) + (int)sizeof(int64_t) * (B.ndom + 1);
+    const int sm = ade_slot_bytes<TC, NM>() + (int)sizeof(int64_t) * (B.ndom + 1);
     const int per_sm = ade_grid_for((const void*)kern, sm, 1, ADE_THREADS);
     kern<<<per_sm * num_sms * grid_mult, ADE_THREADS, sm, st>>>(B);
 }

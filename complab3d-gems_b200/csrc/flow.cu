@@ -36,6 +36,7 @@
 namespace clb {
 
 constexpr int FLOW_THREADS = 256;
+constexpr int PIPE_THREADS = 256;  // CTA of the pipelined odd step (shared memory per thread: 2 nodes)
 
 template <typename TC>
 __device__ __forceinline__ TC feq19(int i, TC rb, TC jx, TC jy, TC jz, TC jsq) {
@@ -274,8 +275,8 @@ __device__ __forceinline__ double flow_node_m(TS* __restrict__ f, TS* __restrict
     // a stored bounce-back node (a voxel sealed by precipitation): the identity on AA slots
     if (P.dyn[code] == DYN_BB) return 0.0;
     TC g[19];
-    int rb_[8];
-    uint32_t blk = 0, rbit = 0, wm = 0;
+    uint32_t ad[19];
+    uint32_t wm = 0;
     int lb = 0;
     if (!ODD) {
         // own slots; a wall link (a, i) takes its incoming opp(i) from its even-step slot X
@@ -295,32 +296,12 @@ __device__ __forceinline__ double flow_node_m(TS* __restrict__ f, TS* __restrict
             }
         }
     } else {
-        const uint32_t m0 = M.m0, m1 = M.m1;
-        const int t = (int)(k >> 8);
-        blk = (m0 | m1) & 0x7FFFFu;  // wall or outside the box: the node's own opposite slot
-        rbit = m1 >> 19;
-        const int4 dv = M.dv;
-        const int* tb = S.tdb + 8 * t;
-        rb_[0] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);
-        rb_[1] = (int)k + tb[1] + (int16_t)((uint32_t)dv.x >> 16);
-        rb_[2] = (int)k + tb[2] + (int16_t)(dv.y & 0xFFFF);
-        rb_[3] = (int)k + tb[3] + (int16_t)((uint32_t)dv.y >> 16);
-        rb_[4] = (int)k + tb[4] + (int16_t)(dv.z & 0xFFFF);
-        rb_[5] = (int)k + tb[5] + (int16_t)((uint32_t)dv.z >> 16);
-        rb_[6] = (int)k + tb[6] + (int16_t)(dv.w & 0xFFFF);
-        rb_[7] = (int)k + tb[7] + (int16_t)((uint32_t)dv.w >> 16);
+        // an in-place permutation: incoming i is read from slot ad[i], outgoing opp(i) goes back there
+        const OddRows R = odd_rows(S, k, M);
 #pragma unroll
         for (int i = 0; i < 19; ++i) {
-            if (i == 0) { g[0] = ld<TS, TC>(f + k); continue; }
-            const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
-            if ((blk >> oi) & 1u) { g[i] = ld<TS, TC>(f + (uint32_t)(i * K32) + k); continue; }
-            int src;
-            if (cx == 0 && cy == 0) src = (int)k - cz;
-            else {
-                const int s8 = row8(-cx, -cy);
-                src = (cz == 0) ? rb_[s8] : (-cz > 0 ? rb_[s8] + (int)((rbit >> s8) & 1u) : rb_[s8] - 1);
-            }
-            g[i] = ld<TS, TC>(f + (uint32_t)(oi * K32) + (uint32_t)src);
+            ad[i] = odd_src(i, k, R, K32);
+            g[i] = ld<TS, TC>(f + ad[i]);
         }
     }
     if (P.dyn[code] == DYN_BGK) {
@@ -336,18 +317,7 @@ __device__ __forceinline__ double flow_node_m(TS* __restrict__ f, TS* __restrict
         }
     } else {
 #pragma unroll
-        for (int i = 0; i < 19; ++i) {
-            if (i == 0) { st<TS, TC>(f + k, g[0]); continue; }
-            const int cx = q19cx(i), cy = q19cy(i), cz = q19cz(i), oi = q19opp(i);
-            if ((blk >> i) & 1u) { st<TS, TC>(f + (uint32_t)(oi * K32) + k, g[i]); continue; }
-            int dst;
-            if (cx == 0 && cy == 0) dst = (int)k + cz;
-            else {
-                const int s8 = row8(cx, cy);
-                dst = (cz == 0) ? rb_[s8] : (cz > 0 ? rb_[s8] + (int)((rbit >> s8) & 1u) : rb_[s8] - 1);
-            }
-            st<TS, TC>(f + (uint32_t)(i * K32) + (uint32_t)dst, g[i]);
-        }
+        for (int i = 0; i < 19; ++i) st<TS, TC>(f + ad[q19opp(i)], g[i]);
     }
     return e;
 }
@@ -361,38 +331,45 @@ __device__ __forceinline__ double flow_node(TS* __restrict__ f, TS* __restrict__
 // Odd AA step with the gathers of the next node in flight while a node is collided: each thread
 // stages a node's 19 incoming populations in its own two shared-memory slots with asynchronous
 // copies (4- and 8-byte storage), one node ahead, and the node after that has its metadata
-// loading. Same arithmetic and stores as the plain step.
+// loading. The odd step is an in-place permutation: outgoing population j of node k goes to the
+// slot incoming opp(j) came from, so the 19 slot offsets computed for the gathers are kept in
+// registers (two sets, the loop unrolled by two nodes) and reused by the stores. Same arithmetic
+// as the plain step.
 template <typename TS, typename TC, int MINB>
-__global__ void __launch_bounds__(FLOW_THREADS, MINB)
+__global__ void __launch_bounds__(PIPE_THREADS, MINB)
     k_flow_odd_pipe(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const FlowParams P,
                     Tracer* __restrict__ tr, double* __restrict__ partials, int trace, int64_t k_west_end,
                     int64_t k_east_begin) {
     if (trace && tr->converged) return;
     extern __shared__ __align__(16) unsigned char flow_smem[];
-    TS* buf = reinterpret_cast<TS*>(flow_smem);  // [2][19][blockDim.x]
+    const int tid = threadIdx.x, nt = blockDim.x;
+    TS* buf = reinterpret_cast<TS*>(flow_smem);  // [2][19][nt]
     const int64_t K = S.K;
     const uint32_t K32 = (uint32_t)S.KS;
-    const int tid = threadIdx.x, nt = blockDim.x;
     const int64_t stride = (int64_t)gridDim.x * nt;
     double esum = 0;
-    auto issue = [&](int64_t kk, const FlowMeta& M, int q) {
+    uint32_t A[19], B[19];
+    auto issue = [&](int64_t kk, const FlowMeta& M, int q, uint32_t (&ad)[19]) {
         const OddRows R = odd_rows(S, kk, M);
         TS* dst = buf + (q * 19) * nt + tid;
 #pragma unroll
-        for (int i = 0; i < 19; ++i) cp_async<sizeof(TS)>(dst + i * nt, f + odd_src(i, kk, R, K32));
+        for (int i = 0; i < 19; ++i) {
+            ad[i] = odd_src(i, kk, R, K32);
+            cp_async<sizeof(TS)>(dst + i * nt, f + ad[i]);
+        }
     };
     int64_t k = (int64_t)blockIdx.x * nt + tid;
     FlowMeta cur, nxt;
     if (k < K) {
         cur = flow_meta<true>(S, k);
-        issue(k, cur, 0);
+        issue(k, cur, 0, A);
     }
     cp_async_commit();
     int64_t kn = k + stride;
     if (kn < K) nxt = flow_meta<true>(S, kn);
-    int q = 0;
-    while (k < K) {
-        if (kn < K) issue(kn, nxt, q ^ 1);
+    // one node: gathers of the next node issued into the other slot, then this node collided
+    auto node = [&](int q, uint32_t (&ac)[19], uint32_t (&an)[19]) {
+        if (kn < K) issue(kn, nxt, q ^ 1, an);
         cp_async_commit();
         const int64_t knn = kn + stride;
         FlowMeta nn;
@@ -409,15 +386,18 @@ __global__ void __launch_bounds__(FLOW_THREADS, MINB)
                 else if (k >= k_east_begin) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
                 esum += (double)bgk19<TC>(g, (TC)P.omega[code]);
             }
-            const OddRows R = odd_rows(S, k, cur);
 #pragma unroll
-            for (int i = 0; i < 19; ++i) st<TS, TC>(f + odd_dst(i, k, R, K32), g[i]);
+            for (int i = 0; i < 19; ++i) st<TS, TC>(f + ac[q19opp(i)], g[i]);
         }
         k = kn;
         kn = knn;
         cur = nxt;
         nxt = nn;
-        q ^= 1;
+    };
+    while (k < K) {
+        node(0, A, B);
+        if (k >= K) break;
+        node(1, B, A);
     }
     cp_async_wait_group<0>();
     __shared__ double sh[32];
@@ -735,7 +715,7 @@ static size_t even_smem() {
 // two slots of 19 populations per thread for the pipelined odd step
 template <typename TS>
 static size_t pipe_smem() {
-    return (size_t)2 * 19 * FLOW_THREADS * sizeof(TS);
+    return (size_t)2 * 19 * PIPE_THREADS * sizeof(TS);
 }
 
 // resident-CTA grid of the pipelined odd step (0: not available for 2-byte storage, whose
@@ -746,8 +726,8 @@ static int pipe_grid_of(clb_handle* h) {
     int per_sm = 0;
     const size_t sm = pipe_smem<TS>();
     cudaFuncSetAttribute(k_flow_odd_pipe<TS, TC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_odd_pipe<TS, TC, 2>, FLOW_THREADS, sm);
-    return h->num_sms * std::min(8, std::max(1, per_sm));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_odd_pipe<TS, TC, 2>, PIPE_THREADS, sm);
+    return h->num_sms * std::min(16, std::max(1, per_sm));
 }
 
 
@@ -869,7 +849,7 @@ clb_status flow_init(clb_handle* h, double delta_p) {
     }
     if (!h->flow_pipe_grid) h->flow_odd_pipe = 0;
     // partials sized for the largest grid any variant uses
-    const int pcap = h->num_sms * 8;
+    const int pcap = h->num_sms * 16;
     if ((e = cudaMalloc(&h->d_partials, sizeof(double) * pcap)) != cudaSuccess) return cuda_check(h, e, "partials");
     h->partial_cap = pcap;
     if (!h->d_err) {
@@ -910,7 +890,7 @@ static void launch_flow(clb_handle* h, bool odd, int trace) {
     if (odd && h->flow_odd_pipe && h->flow_pipe_grid) {
         const int pg = h->flow_pipe_grid;
 #define CLB_PIPE(TS, TC)                                                                                       \
-        k_flow_odd_pipe<TS, TC, 2><<<pg, FLOW_THREADS, pipe_smem<TS>(), h->stream>>>(                          \
+        k_flow_odd_pipe<TS, TC, 2><<<pg, PIPE_THREADS, pipe_smem<TS>(), h->stream>>>(                          \
             (TS*)h->d_f, (TS*)h->d_flink, S, P, h->d_tracer, h->d_partials, trace, h->k_west_end, h->k_east_begin);
         switch (h->flow_prec) {
             case CLB_F64: CLB_PIPE(double, double); return;
