@@ -11,10 +11,12 @@
 //   on the density the thread already holds: one read and one write per population.
 //
 // Layout: the compacted node layout of sparse.cuh over the nodes that are not bounce-back for
-// the species lattices (pore and biofilm); mobile species populations g[m][7][K] of the storage
-// type (m = rank of the species among the mobile ones) with their wall link slots
-// glink[m][L]; AA in-place pattern as in flow.cu. Immobile species and biomass are FP64 fields
-// dense per-voxel fields imm[s][N], bio[m][N] (they must outlive a voxel's change of class); the
+// the species lattices (pore and biofilm). Mobile species m (rank of the species among the mobile
+// ones) occupies [m SS, (m + 1) SS) of one buffer of the storage type: its 7 population rows of
+// stride KS, then its wall link slots (glink = g + 7 KS), so that every storage slot of a species
+// is a 32-bit offset from the species base; AA in-place pattern as in flow.cu. Immobile species
+// and biomass are dense FP64 per-voxel fields imm[s][N], bio[m][N] (they must outlive a voxel's
+// change of class); the
 // advection velocity u[3][K] is in the arithmetic type.
 // Algorithmic bytes per node update: 2*7*sizeof(storage) per mobile species, plus the velocity
 // (3*sizeof(arith)) and the material byte shared by all species.
@@ -119,11 +121,28 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const SparseVi
     }
 }
 
+// The per-node metadata a transport step reads before its gathers: material code, wall / box-edge
+// masks with the link base residual, and (odd steps) the neighbour-row residuals. Loaded one node
+// ahead by the pipelined step.
+struct AdeMeta {
+    int code;
+    uint32_t mt;
+    int2 dv;
+};
+
+template <bool ODD>
+__device__ __forceinline__ AdeMeta ade_meta(const SparseView& S, int64_t k) {
+    AdeMeta M;
+    M.code = S.code[k];
+    M.mt = S.meta[k];
+    M.dv = ODD ? *reinterpret_cast<const int2*>(S.dres + 4 * k) : make_int2(0, 0);
+    return M;
+}
+
 // compact index of the source node a - c_i of each population on an odd step (from the
-// per-tile row bases and per-node residuals)
-__device__ __forceinline__ void odd_sources(const SparseView& S, int64_t k, int (&nb)[7]) {
+// per-tile row bases and the node's residuals dv)
+__device__ __forceinline__ void odd_sources(const SparseView& S, int64_t k, int2 dv, int (&nb)[7]) {
     const int t = (int)(k >> 8);
-    const int2 dv = *reinterpret_cast<const int2*>(S.dres + 4 * k);
     const int* tb = S.tdb + 4 * t;
     nb[0] = (int)k;
     nb[1] = (int)k + tb[0] + (int16_t)(dv.x & 0xFFFF);           // -x population comes from x+1
@@ -152,58 +171,43 @@ constexpr int ade_minb() {
 // shared memory (NM x 7 x ADE_THREADS values of the arithmetic type) between the gather and the
 // collision, so registers hold only the per-species sums and increments and many warps stay
 // resident to hide memory latency.
-// One node of the transport step (all species of compact node k): gather, boundary completion,
-// kinetics, collision, deposit, scatter. `sp_base` is the calling thread's slot base in shared
-// memory (NM x 7 values with stride `stride`), `ob` its 7 slots for the population offsets.
-// Shared by the single-domain and the batched steps.
+// One node of the transport step (all species of compact node k) in two halves: ade_gather
+// (slot offsets, then every species' incoming populations into the calling thread's slots of
+// shared memory) and ade_finish (boundary completion, kinetics, collision, deposit, scatter).
+// `sp_base` is the thread's slot base (NM x 7 values with stride `stride`), `ob` its 7 slots for
+// the population offsets. Shared by the single-domain, the pipelined and the batched steps.
 //
 // Both AA steps are in-place permutations of 7 storage slots per node that every species shares:
 // incoming j is read from slot j and outgoing opp(j) is written back to slot j. Even step: slot j is
 // the node's own row j, or, for a wall link (a, i) with j = opp(i), the link's even-step slot X.
 // Odd step: slot j is row opp(j) of the source node a - c_j, or the node's own row j when that
-// source is a wall or outside the box. The offsets are computed once per node (bit 31 marks a
-// link slot) and serve the gathers and the scatters of every species.
-template <typename TS, typename TC, bool ODD, int NM, bool EXT, typename AP>
-__device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm,
-                                         double* __restrict__ bio, const TC* __restrict__ u, const SparseView& S,
-                                         const double* __restrict__ neu, const AP& P, int n_mobile,
-                                         const int* __restrict__ mob_species, int64_t k_west_end,
-                                         int64_t k_east_begin, const AdeExtra& X, TC* sp_base, uint32_t* ob,
-                                         int stride, int64_t k) {
-    const Geom G = P.g;
-    const int64_t K = S.K, L = S.L;
-    const int64_t KS = S.KS;
-    const uint32_t K32 = (uint32_t)KS;  // row stride; 7 KS < 2^31 is checked when the layout is built
-    const int code = S.code[k];
-    const int dyn = P.dyn[code];
-    // a voxel sealed by precipitation bounces back: on AA slots that is the identity
-    if (dyn == ADE_BB) return;
+// source is a wall or outside the box. The offsets (from the species base, link slots at 7 KS +
+// link index) are computed once per node and serve the gathers and the scatters of every species.
+
+// Returns the mask of the species gathered (those that collide and stream at this node); a
+// bounce-back node (a voxel sealed by precipitation: the identity on AA slots) gathers nothing.
+template <typename TS, typename TC, bool ODD, int NM, typename AP>
+__device__ __forceinline__ uint32_t ade_gather(TS* __restrict__ g, TS* __restrict__ glink, const SparseView& S,
+                                               const AP& P, int n_mobile, const int* __restrict__ mob_species,
+                                               int64_t k_west_end, int64_t k_east_begin, TC* sp_base,
+                                               uint32_t* ob, int stride, int64_t k, const AdeMeta& M) {
+    if (P.dyn[M.code] == ADE_BB) return 0u;
+    const uint32_t K32 = (uint32_t)S.KS;  // row stride; SS < 2^31 is checked when the layout is built
     const bool west = k < k_west_end, east = k >= k_east_begin;
-    int p = 0;
-    uint32_t wm = 0, blk = 0;
-    int lb = 0;
-    if (west || east) {
-        const int64_t n = S.node[k];
-        p = (int)(n % G.plane);
-    }
-    {
-        const uint32_t mt = S.meta[k];
-        wm = mt & 0x7Fu;
-        blk = wm | ((mt >> 7) & 0x7Fu);  // wall or outside the box
-        lb = S.tlb[(int)(k >> 8)] + (int)(mt >> 14);
-    }
-    constexpr uint32_t LINKF = 0x80000000u, OMASK = 0x7FFFFFFFu;
+    const uint32_t wm = M.mt & 0x7Fu;
+    const uint32_t blk = wm | ((M.mt >> 7) & 0x7Fu);  // wall or outside the box
     uint32_t off[7];
     if (!ODD) {
+        const uint32_t lb = 7u * K32 + (uint32_t)(S.tlb[(int)(k >> 8)] + (int)(M.mt >> 14));
 #pragma unroll
         for (int i = 0; i < 7; ++i) {
             const int oi = q7opp(i);
-            off[i] = (i != 0 && ((wm >> oi) & 1u)) ? (LINKF | (uint32_t)(lb + __popc(wm & ((1u << oi) - 1u))))
+            off[i] = (i != 0 && ((wm >> oi) & 1u)) ? lb + (uint32_t)__popc(wm & ((1u << oi) - 1u))
                                                    : (uint32_t)(i * K32) + (uint32_t)k;
         }
     } else {
         int nb[7];  // compact index of the source node a - c_i
-        odd_sources(S, k, nb);
+        odd_sources(S, k, M.dv, nb);
         off[0] = (uint32_t)k;
 #pragma unroll
         for (int i = 1; i < 7; ++i) {
@@ -213,49 +217,48 @@ __device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ gl
     }
 #pragma unroll
     for (int i = 0; i < 7; ++i) ob[i * stride] = off[i];
-    // phase 1: every species' incoming populations (after the boundary completion) into this
-    // thread's own shared-memory slots, and their sums; only the sums stay in registers
     uint32_t actm = 0;
-    TC rb[NM];
 #pragma unroll
     for (int m = 0; m < NM; ++m) {
-        rb[m] = 0;
         if (m >= n_mobile) continue;
         const int s = mob_species[m];
         if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
         actm |= 1u << m;
-        TS* f = g + (int64_t)m * 7 * KS;
-        TS* lk = glink + (int64_t)m * L;
+        TS* f = g + (int64_t)m * S.SS;
         TC* slot = sp_base + (m * 7) * stride;
-        if (!ODD && wm) {
-            // the odd-step slot Y = f[opp(i)][a] of a wall link (a, i) is written back unchanged so
-            // that its sector is written whole
-#pragma unroll
-            for (int i = 1; i < 7; ++i) {
-                if (!((wm >> i) & 1u)) continue;
-                TS* y = f + (uint32_t)(q7opp(i) * K32) + k;
-                *y = *y;
-            }
-        }
         if constexpr (sizeof(TS) >= 4) {
             // 4- and 8-byte populations go straight to the slots as asynchronous copies, so a
             // thread has all of its loads in flight at once without holding them in registers
 #pragma unroll
-            for (int i = 0; i < 7; ++i) {
-                const TS* src = (!ODD && (off[i] & LINKF)) ? lk + (off[i] & OMASK) : f + off[i];
-                cp_async<sizeof(TS)>(slot + i * stride, src);
-            }
+            for (int i = 0; i < 7; ++i) cp_async<sizeof(TS)>(slot + i * stride, f + off[i]);
         } else {
 #pragma unroll
-            for (int i = 0; i < 7; ++i) {
-                const TS* src = (!ODD && (off[i] & LINKF)) ? lk + (off[i] & OMASK) : f + off[i];
-                slot[i * stride] = ld<TS, TC>(src);
-            }
+            for (int i = 0; i < 7; ++i) slot[i * stride] = ld<TS, TC>(f + off[i]);
         }
     }
-    if constexpr (sizeof(TS) >= 4) cp_async_wait_all();  // each thread reads only its own slots
+    return actm;
+}
+
+// The second half, once the gathered populations are in the slots: boundary completion, sums,
+// kinetics, collision with the deposit, scatter back to the node's slots.
+template <typename TS, typename TC, bool ODD, int NM, bool EXT, typename AP>
+__device__ __forceinline__ void ade_finish(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm,
+                                           double* __restrict__ bio, const TC* __restrict__ u, const SparseView& S,
+                                           const double* __restrict__ neu, const AP& P, int n_mobile,
+                                           const int* __restrict__ mob_species, int64_t k_west_end,
+                                           int64_t k_east_begin, const AdeExtra& X, TC* sp_base, uint32_t* ob,
+                                           int stride, int64_t k, int code, uint32_t actm) {
+    const int dyn = P.dyn[code];
+    if (dyn == ADE_BB) return;
+    const Geom G = P.g;
+    const int64_t K = S.K;
+    const bool west = k < k_west_end, east = k >= k_east_begin;
+    int p = 0;
+    if (west || east) p = (int)(S.node[k] % G.plane);
+    TC rb[NM];
 #pragma unroll
     for (int m = 0; m < NM; ++m) {
+        rb[m] = 0;
         if (!((actm >> m) & 1u)) continue;
         TC* slot = sp_base + (m * 7) * stride;
         if ((west || east) && dyn != ADE_NONE) {
@@ -311,14 +314,25 @@ __device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ gl
             o[3] = q[3] * omw + w * (r8 - (TC)0.5 * jz) + d8;
             o[6] = q[6] * omw + w * (r8 + (TC)0.5 * jz) + d8;
         }
-        TS* f = g + (int64_t)m * 7 * KS;
-        TS* lk = glink + (int64_t)m * L;
+        TS* f = g + (int64_t)m * S.SS;
 #pragma unroll
-        for (int j = 0; j < 7; ++j) {  // outgoing opp(j) back to slot j
-            TS* dst = (!ODD && (off2[j] & LINKF)) ? lk + (off2[j] & OMASK) : f + off2[j];
-            st<TS, TC>(dst, o[q7opp(j)]);
-        }
+        for (int j = 0; j < 7; ++j) st<TS, TC>(f + off2[j], o[q7opp(j)]);  // outgoing opp(j) back to slot j
     }
+}
+
+template <typename TS, typename TC, bool ODD, int NM, bool EXT, typename AP>
+__device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm,
+                                         double* __restrict__ bio, const TC* __restrict__ u, const SparseView& S,
+                                         const double* __restrict__ neu, const AP& P, int n_mobile,
+                                         const int* __restrict__ mob_species, int64_t k_west_end,
+                                         int64_t k_east_begin, const AdeExtra& X, TC* sp_base, uint32_t* ob,
+                                         int stride, int64_t k) {
+    const AdeMeta M = ade_meta<ODD>(S, k);
+    const uint32_t actm = ade_gather<TS, TC, ODD, NM>(g, glink, S, P, n_mobile, mob_species, k_west_end,
+                                                      k_east_begin, sp_base, ob, stride, k, M);
+    if constexpr (sizeof(TS) >= 4) cp_async_wait_all();  // each thread reads only its own slots
+    ade_finish<TS, TC, ODD, NM, EXT>(g, glink, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end,
+                                     k_east_begin, X, sp_base, ob, stride, k, M.code, actm);
 }
 
 template <typename TS, typename TC, bool ODD, int NM, bool EXT>
@@ -336,14 +350,80 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>()))
                                        k_east_begin, X, sp + threadIdx.x, ob + threadIdx.x, blockDim.x, k);
 }
 
+// resident blocks per SM of the pipelined step (two slot sets per thread); 0: does not fit twice
+template <typename TC, int NM>
+constexpr int ade_pipe_minb() {
+    constexpr int b = (200 * 1024) / (2 * ade_slot_bytes<TC, NM>());
+    return b > 4 ? 4 : b;
+}
+
+// The transport step with the gathers of the next node in flight while a node is finished: two
+// slot sets per thread; node k + stride's populations go to one by asynchronous copies while node
+// k's are finished from the other, and the metadata of the node after that is loading. Same
+// arithmetic and memory traffic as k_ade_aa. For 4- and 8-byte storage where two slot sets leave
+// at least two resident blocks per SM.
+template <typename TS, typename TC, bool ODD, int NM, bool EXT>
+__global__ void __launch_bounds__(ADE_THREADS, (ade_pipe_minb<TC, NM>() < 1 ? 1 : ade_pipe_minb<TC, NM>()))
+    k_ade_pipe(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm, double* __restrict__ bio,
+               const TC* __restrict__ u, const SparseView S, const double* __restrict__ neu, const AdeParams P,
+               int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin,
+               const AdeExtra X) {
+    const int64_t K = S.K;
+    const int nt = blockDim.x, tid = threadIdx.x;
+    extern __shared__ __align__(16) unsigned char ade_smem[];
+    TC* sp = reinterpret_cast<TC*>(ade_smem) + tid;                                        // [2][NM * 7][nt]
+    uint32_t* ob = reinterpret_cast<uint32_t*>(ade_smem + (size_t)2 * NM * 7 * nt * sizeof(TC)) + tid;  // [2][7][nt]
+    const int64_t sk = (int64_t)gridDim.x * nt;
+    int64_t k = (int64_t)blockIdx.x * nt + tid;
+    AdeMeta cur, nxt;
+    uint32_t acur = 0, anxt = 0;
+    if (k < K) {
+        cur = ade_meta<ODD>(S, k);
+        acur = ade_gather<TS, TC, ODD, NM>(g, glink, S, P, n_mobile, mob_species, k_west_end, k_east_begin, sp, ob,
+                                           nt, k, cur);
+    }
+    cp_async_commit();
+    int64_t kn = k + sk;
+    if (kn < K) nxt = ade_meta<ODD>(S, kn);
+    int q = 0;
+    while (k < K) {
+        if (kn < K)
+            anxt = ade_gather<TS, TC, ODD, NM>(g, glink, S, P, n_mobile, mob_species, k_west_end, k_east_begin,
+                                               sp + (q ^ 1) * NM * 7 * nt, ob + (q ^ 1) * 7 * nt, nt, kn, nxt);
+        cp_async_commit();
+        const int64_t knn = kn + sk;
+        AdeMeta nn;
+        if (knn < K) nn = ade_meta<ODD>(S, knn);
+        cp_async_wait_group<1>();  // node k's populations have landed
+        ade_finish<TS, TC, ODD, NM, EXT>(g, glink, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end,
+                                         k_east_begin, X, sp + q * NM * 7 * nt, ob + q * 7 * nt, nt, k, cur.code,
+                                         acur);
+        k = kn;
+        kn = knn;
+        cur = nxt;
+        nxt = nn;
+        acur = anxt;
+        q ^= 1;
+    }
+    cp_async_wait_group<0>();
+}
+
 // The stored density of every Neumann plane node: the density of its inner neighbour as it
 // stands before the step (FlatAdiabaticBoundaryFunctional3D after the previous stream). A node
 // whose inner neighbour is not a fluid node keeps its previous value.
+// The Neumann planes of one step (one grid row per species and side).
+struct NeumannPlanes {
+    int n;
+    int s[2 * CLB_MAX_SPECIES], m[2 * CLB_MAX_SPECIES], side[2 * CLB_MAX_SPECIES];
+};
+
 template <typename TS, typename TC>
 __global__ void k_ade_neumann(const TS* __restrict__ g, const TS* __restrict__ glink, const SparseView S,
-                              const int8_t* __restrict__ mat, double* __restrict__ neu, const AdeParams P, int s,
-                              int m, int side, int odd, double c0) {
+                              const int8_t* __restrict__ mat, double* __restrict__ neu, const AdeParams P,
+                              const NeumannPlanes J, int odd) {
     const Geom G = P.g;
+    const int s = J.s[blockIdx.y], m = J.m[blockIdx.y], side = J.side[blockIdx.y];
+    const double c0 = P.c0[s];
     const int xb = side == 0 ? 0 : G.nx - 1, xi = side == 0 ? 1 : G.nx - 2;
     TC init[7];
     for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - 1.0));
@@ -352,7 +432,7 @@ __global__ void k_ade_neumann(const TS* __restrict__ g, const TS* __restrict__ g
         const int db = P.dyn[mat[nb]], di = P.dyn[mat[ni]];
         if (!(db == ADE_PORE || db == ADE_BIO) || !(di == ADE_PORE || di == ADE_BIO)) continue;
         TC pop[7];
-        natural<TS, TC, 7>(S, G, g + (int64_t)m * 7 * S.KS, glink + (int64_t)m * S.L, ni, odd, init, pop);
+        natural<TS, TC, 7>(S, G, g + (int64_t)m * S.SS, glink + (int64_t)m * S.SS, ni, odd, init, pop);
         double r = 1.0;
         for (int i = 0; i < 7; ++i) r += (double)pop[i];
         neu[((int64_t)s * 2 + side) * G.plane + p] = r;
@@ -360,8 +440,8 @@ __global__ void k_ade_neumann(const TS* __restrict__ g, const TS* __restrict__ g
 }
 
 template <typename TS>
-__global__ void k_ade_init(TS* __restrict__ g, TS* __restrict__ glink, int64_t K, int64_t L, int n_mobile,
-                           const double* __restrict__ c0m) {
+__global__ void k_ade_init(TS* __restrict__ g, TS* __restrict__ glink, int64_t K, int64_t L, int64_t SS,
+                           int n_mobile, const double* __restrict__ c0m) {
     // K here is the padded row stride: the padding slots are initialised too
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K || k < L;
          k += (int64_t)gridDim.x * blockDim.x) {
@@ -371,14 +451,14 @@ __global__ void k_ade_init(TS* __restrict__ g, TS* __restrict__ glink, int64_t K
             if (k < K)
                 for (int i = 0; i < 7; ++i) {
                     double v = q7w(i) * (c - 1.0);
-                    if constexpr (std::is_same<TS, __half>::value) g[((int64_t)m * 7 + i) * K + k] = __double2half(v);
-                    else g[((int64_t)m * 7 + i) * K + k] = (TS)v;
+                    if constexpr (std::is_same<TS, __half>::value) g[(int64_t)m * SS + (int64_t)i * K + k] = __double2half(v);
+                    else g[(int64_t)m * SS + (int64_t)i * K + k] = (TS)v;
                 }
             if (k < L) {
                 // a wall slot holds population j of the wall node; every j != 0 has weight 1/8
                 double v = 0.125 * (c - 1.0);
-                if constexpr (std::is_same<TS, __half>::value) glink[(int64_t)m * L + k] = __double2half(v);
-                else glink[(int64_t)m * L + k] = (TS)v;
+                if constexpr (std::is_same<TS, __half>::value) glink[(int64_t)m * SS + k] = __double2half(v);
+                else glink[(int64_t)m * SS + k] = (TS)v;
             }
         }
     }
@@ -428,7 +508,7 @@ __global__ void k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ gl
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K || k < S.L;
          k += (int64_t)gridDim.x * blockDim.x) {
         if (k < S.L)
-            for (int m = 0; m < n_mobile; ++m) atomicAdd(&shq[S_ + mob_species[m]], ldd(glink + (int64_t)m * S.L + k));
+            for (int m = 0; m < n_mobile; ++m) atomicAdd(&shq[S_ + mob_species[m]], ldd(glink + (int64_t)m * S.SS + k));
         if (k >= K) continue;
         const int code = S.code[k];
         const bool inner = k >= k_west_end && k < k_east_begin;
@@ -439,7 +519,7 @@ __global__ void k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ gl
             const int m = P.slot[s];
             if (m >= 0) {
                 double sum = 1.0;
-                for (int i = 0; i < 7; ++i) sum += ldd(g + ((int64_t)m * 7 + i) * S.KS + k);
+                for (int i = 0; i < 7; ++i) sum += ldd(g + (int64_t)m * S.SS + (int64_t)i * S.KS + k);
                 c = sum;
             } else {
                 c = imm[(int64_t)s * P.g.N + S.node[k]];
@@ -478,7 +558,7 @@ static size_t usize(int prec) { return prec == CLB_F64 ? 8 : 4; }
 
 void ade_free(clb_handle* h) {
     cudaFree(h->d_g); h->d_g = nullptr;
-    cudaFree(h->d_glink); h->d_glink = nullptr;
+    h->d_glink = nullptr;  // inside d_g
     cudaFree(h->d_imm); h->d_imm = nullptr;
     cudaFree(h->d_bio); h->d_bio = nullptr;
     cudaFree(h->d_u); h->d_u = nullptr;
@@ -558,14 +638,15 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
     for (int64_t n = h->g.N - h->g.plane; n < h->g.N; ++n) ke += cls[(uint8_t)h->h_mat[n] & 127] != 0;
     h->ade_west_end = kw;
     h->ade_east_begin = K - ke;
-    const size_t K1 = (size_t)std::max<int64_t>(1, K), L1 = (size_t)std::max<int64_t>(1, L);
+    const size_t K1 = (size_t)std::max<int64_t>(1, K);
     const int nm1 = std::max(1, h->n_mobile);
     cudaError_t e;
     const size_t KS = (size_t)h->ade_sp.KS;
-    if ((e = cudaMalloc(&h->d_g, esize(h->ade_prec) * 7 * KS * nm1)) != cudaSuccess)
+    // one buffer: species m's 7 population rows, then its link slots, at [m SS, (m + 1) SS)
+    const size_t SSz = (size_t)h->ade_sp.SS;
+    if ((e = cudaMalloc(&h->d_g, esize(h->ade_prec) * SSz * nm1)) != cudaSuccess)
         return cuda_check(h, e, "species populations");
-    if ((e = cudaMalloc(&h->d_glink, esize(h->ade_prec) * L1 * nm1)) != cudaSuccess)
-        return cuda_check(h, e, "species links");
+    h->d_glink = (char*)h->d_g + esize(h->ade_prec) * 7 * KS;
     const size_t N1 = (size_t)h->g.N;
     if ((e = cudaMalloc(&h->d_imm, sizeof(double) * N1 * S)) != cudaSuccess) return cuda_check(h, e, "immobile fields");
     if ((e = cudaMalloc(&h->d_u, usize(h->ade_prec) * 3 * K1)) != cudaSuccess) return cuda_check(h, e, "velocity");
@@ -599,9 +680,9 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
         cudaMemcpy(dc0, c0m.data(), sizeof(double) * c0m.size(), cudaMemcpyHostToDevice);
         const int grid = h->num_sms * 8;
         switch (h->ade_prec) {
-            case CLB_F64: k_ade_init<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g, (double*)h->d_glink, (int64_t)KS, L, h->n_mobile, dc0); break;
-            case CLB_F32: k_ade_init<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g, (float*)h->d_glink, (int64_t)KS, L, h->n_mobile, dc0); break;
-            default: k_ade_init<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g, (__half*)h->d_glink, (int64_t)KS, L, h->n_mobile, dc0); break;
+            case CLB_F64: k_ade_init<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g, (double*)h->d_glink, (int64_t)KS, L, (int64_t)SSz, h->n_mobile, dc0); break;
+            case CLB_F32: k_ade_init<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g, (float*)h->d_glink, (int64_t)KS, L, (int64_t)SSz, h->n_mobile, dc0); break;
+            default: k_ade_init<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g, (__half*)h->d_glink, (int64_t)KS, L, (int64_t)SSz, h->n_mobile, dc0); break;
         }
         cudaStreamSynchronize(h->stream);
         cudaFree(dc0);
@@ -731,9 +812,19 @@ static void launch_ade_t(clb_handle* h) {
     const AdeExtra X = ade_extra(h);
 #define CLB_ADE(NM, EXT)                                                                                          \
     do {                                                                                                          \
+        if constexpr (sizeof(TS) >= 4 && ade_pipe_minb<TC, NM>() >= 2) {                                           \
+            if (h->ade_pipe) {                                                                                    \
+            auto kern = k_ade_pipe<TS, TC, ODD, NM, EXT>;                                                          \
+            const int sm = 2 * ade_slot_bytes<TC, NM>();                                                           \
+            const int gr = ade_grid_for((const void*)kern, sm, h->num_sms, ADE_THREADS);                           \
+            kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,    \
+                                                     h->ade_west_end, h->ade_east_begin, X);                      \
+            break;                                                                                                \
+            }                                                                                                     \
+        }                                                                                                         \
         auto kern = k_ade_aa<TS, TC, ODD, NM, EXT>;                                                               \
         const int sm = ade_slot_bytes<TC, NM>();                                                                  \
-        const int gr = ade_grid_for((const void*)kern, sm, h->num_sms, ADE_THREADS);                                           \
+        const int gr = ade_grid_for((const void*)kern, sm, h->num_sms, ADE_THREADS);                              \
         kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,        \
                                                  h->ade_west_end, h->ade_east_begin, X);                          \
     } while (0)
@@ -752,17 +843,24 @@ static void launch_ade_t(clb_handle* h) {
 template <typename TS, typename TC>
 static void launch_neumann(clb_handle* h, int odd) {
     const SparseView S = view_of(h->ade_sp);
+    NeumannPlanes J;
+    J.n = 0;
     for (int s = 0; s < h->S; ++s) {
         const int m = h->ap.slot[s];
         if (m < 0) continue;
         for (int side = 0; side < 2; ++side) {
-            int t = side == 0 ? h->ap.ltype[s] : h->ap.rtype[s];
+            const int t = side == 0 ? h->ap.ltype[s] : h->ap.rtype[s];
             if (t != CLB_NEUMANN) continue;
-            k_ade_neumann<TS, TC><<<std::max(1, std::min(h->num_sms * 2, (h->g.plane + 255) / 256)), 256, 0,
-                                    h->stream>>>((const TS*)h->d_g, (const TS*)h->d_glink, S, h->d_mat, h->d_neu,
-                                                 h->ap, s, m, side, odd, h->ap.c0[s]);
+            J.s[J.n] = s;
+            J.m[J.n] = m;
+            J.side[J.n] = side;
+            ++J.n;
         }
     }
+    if (J.n == 0) return;
+    const dim3 grid(std::max(1, std::min(h->num_sms * 2, (h->g.plane + 255) / 256)), J.n);
+    k_ade_neumann<TS, TC><<<grid, 256, 0, h->stream>>>((const TS*)h->d_g, (const TS*)h->d_glink, S, h->d_mat,
+                                                       h->d_neu, h->ap, J, odd);
 }
 
 // The stored densities are those after the latest stream; they are recomputed lazily, once per
@@ -833,7 +931,7 @@ __global__ void k_neumann_batch(const BatchView B, int odd) {
         const double c0 = d.ap.c0[J.s];
         TC init[7], pop[7];
         for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - 1.0));
-        natural<TS, TC, 7>(d.as, G, (const TS*)d.g + (int64_t)J.m * 7 * d.as.KS, (const TS*)d.glink + (int64_t)J.m * d.as.L,
+        natural<TS, TC, 7>(d.as, G, (const TS*)d.g + (int64_t)J.m * d.as.SS, (const TS*)d.glink + (int64_t)J.m * d.as.SS,
                            ni, odd, init, pop);
         double r = 1.0;
         for (int i = 0; i < 7; ++i) r += (double)pop[i];
@@ -915,7 +1013,7 @@ static clb_status ade_populations_i(clb_handle* h, int s, double* host) {
     if (e != cudaSuccess) return cuda_check(h, e, "population buffer");
     const int odd = (int)(h->ade_iters & 1);
     const int grid = h->num_sms * 8;
-    const size_t off = (size_t)m * 7 * h->ade_sp.KS, loff = (size_t)m * h->ade_sp.L;
+    const size_t off = (size_t)m * h->ade_sp.SS, loff = off;
     const SparseView S = view_of(h->ade_sp);
     const double c0 = h->ap.c0[s];
     switch (h->ade_prec) {
@@ -947,7 +1045,7 @@ clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
     cudaMemcpy(buf, host, sizeof(double) * 7 * (size_t)h->g.N, cudaMemcpyHostToDevice);
     const int odd = (int)(h->ade_iters & 1);
     const int grid = h->num_sms * 8;
-    const size_t off = (size_t)m * 7 * h->ade_sp.KS, loff = (size_t)m * h->ade_sp.L;
+    const size_t off = (size_t)m * h->ade_sp.SS, loff = off;
     const SparseView S = view_of(h->ade_sp);
     switch (h->ade_prec) {
         case CLB_F64: k_ade_set_pops<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g + off, (double*)h->d_glink + loff, S, h->g, odd, buf); break;

@@ -136,6 +136,7 @@ clb_status clb_tune(clb_handle* h, const char* key, int value) {
     if (!h || !key) return fail(h, CLB_INVALID_ARG, "null argument");
     const std::string k = key;
     if (k == "flow_even_tma") { h->flow_even_tma = value ? 1 : 0; return CLB_OK; }
+    if (k == "ade_pipe") { h->ade_pipe = value ? 1 : 0; return CLB_OK; }
     if (k == "flow_odd_pipe") {
         if (value && h->flow_ready && !h->flow_pipe_grid)
             return fail(h, CLB_INVALID_ARG, "flow_odd_pipe needs 4- or 8-byte flow storage");

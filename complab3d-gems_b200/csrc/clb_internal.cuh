@@ -157,6 +157,8 @@ struct SparseBuffers {
     int32_t* tdb = nullptr;     // [T][NR] neighbour-row rank bases of each tile
     int64_t K = 0, L = 0;
     int64_t KS = 0;             // population row stride: K rounded up to a multiple of 256
+    int64_t SS = 0;             // species stride of a lattice whose link slots follow its q rows:
+                                // q KS + L rounded up to a multiple of 256
     int W = 0, NR = 0;
 };
 }  // namespace clb
@@ -202,7 +204,8 @@ struct clb_handle_s {
     int u2i[CLB_MAX_SPECIES];               // user species index -> internal (mobile first)
     int i2u[CLB_MAX_SPECIES];
     void* d_g = nullptr;              // [n_mobile][7][K] storage type, compacted stored nodes
-    void* d_glink = nullptr;          // [n_mobile][L] wall link slots
+    void* d_glink = nullptr;          // d_g + 7 KS: species m's wall link slots start at d_glink + m SS
+                                      // (inside d_g, whose species m occupies [m SS, (m + 1) SS))
     clb::SparseBuffers ade_sp;
     int64_t ade_west_end = 0, ade_east_begin = 0;
     double* d_imm = nullptr;          // [S][N] immobile concentrations (unused rows stay empty)
@@ -213,6 +216,7 @@ struct clb_handle_s {
     int64_t ade_iters = 0;
     int64_t neu_iter = -1;            // iteration whose stream the Neumann store reflects
     int ade_grid = 0;
+    int ade_pipe = 0;                 // transport step with the next node's gathers in flight (where it fits)
 
     // speciation (SpecParams lives in speciation.cuh; kept as raw storage here)
     alignas(16) unsigned char sp_storage[2048];

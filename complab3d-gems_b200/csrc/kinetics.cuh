@@ -135,7 +135,7 @@ __device__ void post_biotic(const AdeParams& P, const SparseView& S, const TS* g
     for (int s = 0; s < P.S; ++s) {
         if (s < n_mobile) {
             TC pop[7];
-            natural<TS, TC, 7>(S, G, g + (int64_t)s * 7 * S.KS, glink + (int64_t)s * S.L, n, odd, init, pop);
+            natural<TS, TC, 7>(S, G, g + (int64_t)s * S.SS, glink + (int64_t)s * S.SS, n, odd, init, pop);
             TC r = 0;
             for (int i = 0; i < 7; ++i) r += pop[i];
             Craw[s] = (double)r + 1.0;

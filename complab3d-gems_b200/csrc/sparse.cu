@@ -157,6 +157,8 @@ clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, Spar
     out.W = W;
     out.NR = NR;
     out.KS = std::max<int64_t>(KS, TILE);
+    out.SS = q * out.KS + std::max<int64_t>(TILE, (L + TILE - 1) / TILE * TILE);
+    if (out.SS > INT32_MAX) return fail(h, CLB_INVALID_ARG, "lattice exceeds 2^31 slots per species");
     return cuda_check(h, e, "sparse layout");
 }
 

@@ -31,12 +31,13 @@ struct SparseView {
     const int32_t* tdb;
     int64_t K, L;
     int64_t KS;               // population row stride (K rounded up to a multiple of TILE)
+    int64_t SS;               // species stride (transport lattices): 7 rows, then the link slots
     int W, NR;
 };
 
 inline SparseView view_of(const SparseBuffers& b) {
     return SparseView{b.node, b.code, b.wall, b.linkbase, b.rowstart, b.rowmask, b.rowpre, b.idx_of,
-                      b.meta, b.dres, b.tlb, b.tdb, b.K, b.L, b.KS, b.W, b.NR};
+                      b.meta, b.dres, b.tlb, b.tdb, b.K, b.L, b.KS, b.SS, b.W, b.NR};
 }
 
 // Odd-step metadata, built once per geometry so the gather step needs no coordinate decode and

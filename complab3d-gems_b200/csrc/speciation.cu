@@ -277,8 +277,8 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
                 double v;
                 if (A.slot[si] >= 0) {
                     const int m = A.slot[si];
-                    TS* f = g + (int64_t)m * 7 * S.KS;
-                    TS* lk = glink + (int64_t)m * S.L;
+                    TS* f = g + (int64_t)m * S.SS;
+                    TS* lk = glink + (int64_t)m * S.SS;
                     v = 1.0;
                     for (int q = 0; q < 7; ++q) v += ldd(out_slot7(S, f, lk, (int)k, q, odd));
                 } else {
@@ -314,8 +314,8 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
             const int si = P.ispec[i];
             if (A.slot[si] >= 0) {
                 const int m = A.slot[si];
-                TS* f = g + (int64_t)m * 7 * S.KS;
-                TS* lk = glink + (int64_t)m * S.L;
+                TS* f = g + (int64_t)m * S.SS;
+                TS* lk = glink + (int64_t)m * S.SS;
                 for (int q = 0; q < 7; ++q) {
                     TS* p = out_slot7(S, f, lk, (int)k, q, odd);
                     const double v = ldd(p) + q7w(q) * dC;
@@ -516,7 +516,7 @@ __global__ void k_mlp_sample_field(const TS* __restrict__ g, const TS* __restric
             if (A.slot[si] >= 0) {
                 const int m = A.slot[si];
                 double pop[7];
-                natural<TS, double, 7>(S, G, g + (int64_t)m * 7 * S.KS, glink + (int64_t)m * S.L, nd, odd, init, pop);
+                natural<TS, double, 7>(S, G, g + (int64_t)m * S.SS, glink + (int64_t)m * S.SS, nd, odd, init, pop);
                 v = 1.0;
                 for (int q = 0; q < 7; ++q) v += pop[q];
             } else {
