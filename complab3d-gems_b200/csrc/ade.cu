@@ -34,8 +34,8 @@ constexpr int ADE_THREADS = 128;
 
 // EXT: the abiotic law and the increments gathered from dissolving neighbours (AdeExtra) are
 // applied after the biotic ones (complab.cpp:2460-2525).
-// Kinetics of node k (x = 1..nx-2, mask neither solid nor wall): biotic rates with the clamp,
-// then, with EXT, the abiotic block. Returns the increments of the mobile species in dC (internal
+// Kinetics of node k (x = 1..nx-2, mask neither solid nor wall): biotic rates with the clamp in
+// the lattice's arithmetic type TC, then, with EXT, the abiotic block in FP64. Returns the increments of the mobile species in dC (internal
 // species m = slot m); immobile species and biomass are updated in place.
 template <typename TC, int NM, bool EXT>
 __device__ __forceinline__ void node_kinetics(const AdeParams& P, const SparseView& S, const AdeExtra& X,
@@ -46,35 +46,27 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const SparseVi
 #pragma unroll
     for (int s = 0; s < NM; ++s) dC[s] = 0;
     if (P.law != CLB_LAW_NONE && !west && !east && P.react[code]) {
+        // biotic block in the lattice's arithmetic type (FP64 lattices: FP64 throughout)
         const int64_t nd = S.node[k];  // dense index of the per-voxel fields
-        double C[NM], R[NM], B[CLB_MAX_MICROBES], RB[CLB_MAX_MICROBES];
+        const TC thr = (TC)THRD;
+        TC C[NM], R[NM];
 #pragma unroll
         for (int s = 0; s < NM; ++s) {
-            double c = 0.0;
-            if (s < n_mobile) c = (double)rb[s] + 1.0;
-            else if (s < P.S) c = imm[(int64_t)s * G.N + nd];
-            C[s] = c < THRD ? 0.0 : c;
+            TC c = 0;
+            if (s < n_mobile) c = rb[s] + (TC)1;
+            else if (s < P.S) c = (TC)imm[(int64_t)s * G.N + nd];
+            C[s] = c < thr ? (TC)0 : c;
         }
-        for (int mb = 0; mb < P.M; ++mb) {
-            const double b = bio[(int64_t)mb * G.N + nd];
-            B[mb] = b < THRD ? 0.0 : b;
-        }
-        eval_rates<NM>(P, C, B, R, RB);
+        biotic_rates<TC, NM, true>(P, C, R, bio, nd, G.N);  // advances the biomass too
 #pragma unroll
         for (int s = 0; s < NM; ++s) {
             if (s >= P.S) continue;
-            double d = R[s] * P.dt;
-            if (!(d > THRD || d < -THRD)) continue;
-            if (d + C[s] < 0.0) d = -C[s];
-            if (!(d > THRD || d < -THRD)) continue;
-            if (s < n_mobile) dC[s] = (TC)d;
-            else imm[(int64_t)s * G.N + nd] += d;
-        }
-        for (int mb = 0; mb < P.M; ++mb) {
-            double d = RB[mb] * P.dt;
-            if (!(d > THRD || d < -THRD)) continue;
-            if (d + B[mb] < 0.0) d = -B[mb];
-            bio[(int64_t)mb * G.N + nd] += d;
+            TC d = R[s] * (TC)P.dt;
+            if (!(d > thr || d < -thr)) continue;
+            if (d + C[s] < (TC)0) d = -C[s];
+            if (!(d > thr || d < -thr)) continue;
+            if (s < n_mobile) dC[s] = d;
+            else imm[(int64_t)s * G.N + nd] += (double)d;
         }
     }
     if (EXT && !west && !east && P.react[code]) {

@@ -6,49 +6,62 @@
 
 namespace clb {
 
-// Rate laws (clb_law), over the species in internal order (mobile first). C and B are the
-// floored concentrations / biomasses; loops are unrolled to the species bucket NB so every array
-// stays in registers.
-template <int NB>
-__device__ __forceinline__ void eval_rates(const AdeParams& P, const double (&C)[NB], const double* B, double (&R)[NB],
-                                           double* RB) {
+// Biotic rate laws (clb_law) over the species in internal order (mobile first), in the kinetics
+// type KT (the lattice's arithmetic type: FP64 for FP64 lattices, FP32 otherwise). C holds the
+// floored concentrations; R receives the species rates. The biomass of microbe m (dense FP64 field
+// bio[m][N] at voxel nd) is read and floored and, with APPLY_BIO, advanced in place with its
+// clamped increment (dB = max(R_B dt, -B), applied when |dB| > THRD), microbe by microbe, so no
+// per-microbe array is kept. Loops over species are unrolled to the bucket NB so every array stays
+// in registers.
+template <typename KT, int NB, bool APPLY_BIO>
+__device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[NB], KT (&R)[NB],
+                                             const double* __restrict__ bio, int64_t nd, int64_t N) {
+    const KT thr = (KT)THRD;
 #pragma unroll
-    for (int s = 0; s < NB; ++s) R[s] = 0.0;
+    for (int s = 0; s < NB; ++s) R[s] = 0;
     switch (P.law) {
         case CLB_LAW_DECAY:
 #pragma unroll
             for (int s = 0; s < NB; ++s)
-                if (s < P.S) R[s] = -P.prm[s] * C[s];
+                if (s < P.S) R[s] = -(KT)P.prm[s] * C[s];
             break;
         case CLB_LAW_MONOD:
 #pragma unroll
             for (int s = 0; s < NB; ++s)
-                if (s < P.S) R[s] = -P.prm[s] * C[s] / (P.prm[CLB_MAX_SPECIES + s] + C[s]);
+                if (s < P.S) R[s] = -(KT)P.prm[s] * C[s] / ((KT)P.prm[CLB_MAX_SPECIES + s] + C[s]);
             break;
         case CLB_LAW_DUAL_MONOD: {
-            const double mu = P.prm[0], ks = P.prm[1], Y = P.prm[2], kd = P.prm[3];
+            const KT mu = (KT)P.prm[0], ks = (KT)P.prm[1], Y = (KT)P.prm[2], kd = (KT)P.prm[3];
             const int don = P.donor;
-            double Cd = 0.0;
+            KT Cd = 0;
 #pragma unroll
             for (int s = 0; s < NB; ++s)
                 if (s == don) Cd = C[s];
-            double Rd = 0.0;
+            KT Rd = 0;
             for (int m = 0; m < P.M; ++m) {
                 const int a = P.acceptor[m];
-                RB[m] = 0.0;
                 if (a < 0) continue;
-                double Ca = 0.0;
+                const double* bp = bio + (int64_t)m * N + nd;
+                const double braw = *bp;
+                const KT Bm = braw < THRD ? (KT)0 : (KT)braw;
+                if (Bm <= (KT)0) continue;
+                KT Ca = 0;
 #pragma unroll
                 for (int s = 0; s < NB; ++s)
                     if (s == a) Ca = C[s];
-                const double Bm = B[m];
-                if (Bm <= 0.0) continue;
-                const double growth = mu * (Cd / (ks + Cd)) * (Ca / (ks + Ca)) * Bm;
-                RB[m] += growth - kd * Bm;
+                const KT growth = mu * (Cd / (ks + Cd)) * (Ca / (ks + Ca)) * Bm;
+                const KT rbm = growth - kd * Bm;
                 Rd -= growth / Y;
 #pragma unroll
                 for (int s = 0; s < NB; ++s)
                     if (s == a) R[s] -= growth / Y;
+                if (APPLY_BIO) {
+                    KT d = rbm * (KT)P.dt;
+                    if (d > thr || d < -thr) {
+                        if (d + Bm < (KT)0) d = -Bm;
+                        *const_cast<double*>(bp) += (double)d;
+                    }
+                }
             }
 #pragma unroll
             for (int s = 0; s < NB; ++s)
@@ -132,31 +145,39 @@ __device__ void post_biotic(const AdeParams& P, const SparseView& S, const TS* g
                             double* Craw) {
     const Geom G = P.g;
     TC init[7] = {};
+    TC rsum[CLB_MAX_SPECIES] = {};
     for (int s = 0; s < P.S; ++s) {
         if (s < n_mobile) {
             TC pop[7];
             natural<TS, TC, 7>(S, G, g + (int64_t)s * S.SS, glink + (int64_t)s * S.SS, n, odd, init, pop);
             TC r = 0;
             for (int i = 0; i < 7; ++i) r += pop[i];
+            rsum[s] = r;
             Craw[s] = (double)r + 1.0;
         } else {
             Craw[s] = imm[(int64_t)s * G.N + n];
         }
     }
     if (P.law == CLB_LAW_NONE) return;
-    double C[CLB_MAX_SPECIES], R[CLB_MAX_SPECIES], B[CLB_MAX_MICROBES], RB[CLB_MAX_MICROBES];
-    for (int s = 0; s < CLB_MAX_SPECIES; ++s) C[s] = s < P.S ? (Craw[s] < THRD ? 0.0 : Craw[s]) : 0.0;
-    for (int mb = 0; mb < P.M; ++mb) {
-        const double b = bio[(int64_t)mb * G.N + n];
-        B[mb] = b < THRD ? 0.0 : b;
+    // the biotic increment exactly as the fused step computes it, in the arithmetic type
+    const TC thr = (TC)THRD;
+    TC C[CLB_MAX_SPECIES], R[CLB_MAX_SPECIES];
+#pragma unroll
+    for (int s = 0; s < CLB_MAX_SPECIES; ++s) {
+        TC c = 0;
+        if (s < n_mobile) c = rsum[s] + (TC)1;
+        else if (s < P.S) c = (TC)Craw[s];
+        C[s] = c < thr ? (TC)0 : c;
     }
-    eval_rates<CLB_MAX_SPECIES>(P, C, B, R, RB);
-    for (int s = 0; s < P.S; ++s) {
-        double d = R[s] * P.dt;
-        if (!(d > THRD || d < -THRD)) continue;
-        if (d + C[s] < 0.0) d = -C[s];
-        if (!(d > THRD || d < -THRD)) continue;
-        Craw[s] += d;
+    biotic_rates<TC, CLB_MAX_SPECIES, false>(P, C, R, bio, n, G.N);
+#pragma unroll
+    for (int s = 0; s < CLB_MAX_SPECIES; ++s) {
+        if (s >= P.S) continue;
+        TC d = R[s] * (TC)P.dt;
+        if (!(d > thr || d < -thr)) continue;
+        if (d + C[s] < (TC)0) d = -C[s];
+        if (!(d > thr || d < -thr)) continue;
+        Craw[s] += (double)d;
     }
 }
 
