@@ -53,6 +53,9 @@ def args_():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-extra", action="store_true", help="skip the D3Q7, precision and speciation legs")
     p.add_argument("--scale", type=float, default=1.0, help="shrink the workload (testing only)")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the library's default kernel variants (profiling runs: timings under a profiler "
+                        "would mislead the autotuner)")
     p.add_argument("--leg", choices=["d3q7", "precision", "speciation", "ensemble"],
                    help="run only this side measurement (with --scale for d3q7) and print its JSON; "
                         "a small case for profilers, not a bench line")
@@ -438,7 +441,7 @@ def main():
     stream = torch.cuda.Stream()
     D.set_stream(stream.cuda_stream)
     D.flow_init(cfg["delta_p"])
-    tuned = D.autotune(20)
+    tuned = "defaults" if a.no_autotune else D.autotune(20)
     st = D.flow_stats()
     n_open, n_active = st["bgk_nodes"], st["active_nodes"]
 

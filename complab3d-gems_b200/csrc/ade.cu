@@ -34,20 +34,21 @@ constexpr int ADE_THREADS = 128;
 
 // EXT: the abiotic law and the increments gathered from dissolving neighbours (AdeExtra) are
 // applied after the biotic ones (complab.cpp:2460-2525).
-// Kinetics of node k (x = 1..nx-2, mask neither solid nor wall): biotic rates with the clamp in
-// the lattice's arithmetic type TC, then, with EXT, the abiotic block in FP64. Returns the increments of the mobile species in dC (internal
-// species m = slot m); immobile species and biomass are updated in place.
+// Kinetics of node k (dense index nd; x = 1..nx-2, mask neither solid nor wall): biotic rates with
+// the clamp in the lattice's arithmetic type TC, then, with EXT, the abiotic block in FP64. Returns
+// the increments of the mobile species in dC (internal species m = slot m); immobile species and
+// biomass are updated in place. `bc` holds the biomass of the first `bn` microbes as staged with
+// the node's gathers (stride ADE_THREADS).
 template <typename TC, int NM, bool EXT>
-__device__ __forceinline__ void node_kinetics(const AdeParams& P, const SparseView& S, const AdeExtra& X,
-                                              int64_t k, int code, bool west, bool east, int n_mobile,
-                                              const TC (&rb)[NM], double* __restrict__ imm,
-                                              double* __restrict__ bio, TC (&dC)[NM]) {
+__device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra& X, int64_t k, int64_t nd, int code,
+                                              bool west, bool east, int n_mobile, const TC (&rb)[NM],
+                                              double* __restrict__ imm, double* __restrict__ bio,
+                                              const double* bc, int bn, TC (&dC)[NM]) {
     const Geom G = P.g;
 #pragma unroll
     for (int s = 0; s < NM; ++s) dC[s] = 0;
     if (P.law != CLB_LAW_NONE && !west && !east && P.react[code]) {
         // biotic block in the lattice's arithmetic type (FP64 lattices: FP64 throughout)
-        const int64_t nd = S.node[k];  // dense index of the per-voxel fields
         const TC thr = (TC)THRD;
         TC C[NM], R[NM];
 #pragma unroll
@@ -57,7 +58,7 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const SparseVi
             else if (s < P.S) c = (TC)imm[(int64_t)s * G.N + nd];
             C[s] = c < thr ? (TC)0 : c;
         }
-        biotic_rates<TC, NM, true>(P, C, R, bio, nd, G.N);  // advances the biomass too
+        biotic_rates<TC, NM, true>(P, C, R, bio, nd, G.N, bc, ADE_THREADS, bn);  // advances the biomass too
 #pragma unroll
         for (int s = 0; s < NM; ++s) {
             if (s >= P.S) continue;
@@ -73,7 +74,6 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const SparseVi
         // abiotic block: increments from the concentrations the biotic law left, applied once
         // (update_abiotic_rxnLattices); next to a dissolving voxel they were computed ahead of
         // the step together with the gathered products
-        const int64_t nd = S.node[k];
         double T2[NM];
 #pragma unroll
         for (int s = 0; s < NM; ++s) T2[s] = 0.0;
@@ -120,6 +120,7 @@ struct AdeMeta {
     int code;
     uint32_t mt;
     int2 dv;
+    int nd;  // dense index of the voxel (per-voxel fields, boundary planes)
 };
 
 template <bool ODD>
@@ -128,6 +129,7 @@ __device__ __forceinline__ AdeMeta ade_meta(const SparseView& S, int64_t k) {
     M.code = S.code[k];
     M.mt = S.meta[k];
     M.dv = ODD ? *reinterpret_cast<const int2*>(S.dres + 4 * k) : make_int2(0, 0);
+    M.nd = S.node[k];
     return M;
 }
 
@@ -145,18 +147,55 @@ __device__ __forceinline__ void odd_sources(const SparseView& S, int64_t k, int2
     nb[6] = (int)k - 1;
 }
 
-// shared memory of a CTA of the transport step: the population slots (NM x 7 per thread, the
-// arithmetic type) and the 7 population offsets per thread
+constexpr int ADE_RESIDENT = 4;   // resident blocks per SM the shared-memory carveout is sized for
+
+// What travels with a node's gathers besides its populations: with 4-byte arithmetic the velocity
+// and the biomass of up to two microbes; FP64 slots already fill the shared memory three blocks
+// can have, so FP64 reads both from memory where it uses them.
+template <typename TC>
+constexpr int ade_bio_cache() { return sizeof(TC) == 4 ? 2 : 0; }
+template <typename TC>
+constexpr int ade_u_staged() { return sizeof(TC) == 4 ? 3 : 0; }
+
+// Shared memory of a CTA of the transport step, per thread (stride ADE_THREADS): the staged
+// biomass (FP64), NM x 7 population slots and the staged velocity (the arithmetic type), and the
+// 7 population offsets. What a node needs from memory beyond its metadata is staged here by
+// asynchronous copies issued together, so one wait covers them all.
 template <typename TC, int NM>
 constexpr int ade_slot_bytes() {
-    return NM * 7 * ADE_THREADS * (int)sizeof(TC) + 7 * ADE_THREADS * (int)sizeof(uint32_t);
+    return ade_bio_cache<TC>() * ADE_THREADS * (int)sizeof(double) +
+           (NM * 7 + ade_u_staged<TC>()) * ADE_THREADS * (int)sizeof(TC) + 7 * ADE_THREADS * (int)sizeof(uint32_t);
 }
 
-// resident blocks per SM the shared slots allow (about 200 KB of shared memory per SM)
+template <typename TC>
+struct AdeFrame {
+    double* bio;    // [ade_bio_cache]
+    TC* pop;        // [NM * 7]
+    TC* u;          // [3]
+    uint32_t* off;  // [7]
+};
+
+// the calling thread's slots in slot set `set` of the CTA's shared memory
+template <typename TC, int NM>
+__device__ __forceinline__ AdeFrame<TC> ade_frame(unsigned char* smem, int set) {
+    unsigned char* b = smem + (size_t)set * ade_slot_bytes<TC, NM>();
+    const int t = threadIdx.x;
+    AdeFrame<TC> F;
+    F.bio = reinterpret_cast<double*>(b) + t;
+    b += ade_bio_cache<TC>() * ADE_THREADS * sizeof(double);
+    F.pop = reinterpret_cast<TC*>(b) + t;
+    b += NM * 7 * ADE_THREADS * sizeof(TC);
+    F.u = reinterpret_cast<TC*>(b) + t;
+    b += ade_u_staged<TC>() * ADE_THREADS * sizeof(TC);
+    F.off = reinterpret_cast<uint32_t*>(b) + t;
+    return F;
+}
+
+// resident blocks per SM the shared slots allow (about 200 KB of shared memory per SM), at most 8
 template <typename TC, int NM>
 constexpr int ade_minb() {
     constexpr int b = (200 * 1024) / ade_slot_bytes<TC, NM>();
-    return b < 1 ? 1 : (b > 4 ? 4 : b);
+    return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
 
 // One thread per node. The populations of all species pass through the thread's own slots of
@@ -164,10 +203,10 @@ constexpr int ade_minb() {
 // collision, so registers hold only the per-species sums and increments and many warps stay
 // resident to hide memory latency.
 // One node of the transport step (all species of compact node k) in two halves: ade_gather
-// (slot offsets, then every species' incoming populations into the calling thread's slots of
-// shared memory) and ade_finish (boundary completion, kinetics, collision, deposit, scatter).
-// `sp_base` is the thread's slot base (NM x 7 values with stride `stride`), `ob` its 7 slots for
-// the population offsets. Shared by the single-domain, the pipelined and the batched steps.
+// (slot offsets, then every species' incoming populations, the node's velocity and biomass into
+// the calling thread's shared-memory frame F, by asynchronous copies where the element is 4 or
+// 8 bytes) and ade_finish (boundary completion, kinetics, collision, deposit, scatter). Shared by
+// the single-domain, the pipelined and the batched steps.
 //
 // Both AA steps are in-place permutations of 7 storage slots per node that every species shares:
 // incoming j is read from slot j and outgoing opp(j) is written back to slot j. Even step: slot j is
@@ -179,10 +218,12 @@ constexpr int ade_minb() {
 // Returns the mask of the species gathered (those that collide and stream at this node); a
 // bounce-back node (a voxel sealed by precipitation: the identity on AA slots) gathers nothing.
 template <typename TS, typename TC, bool ODD, int NM, typename AP>
-__device__ __forceinline__ uint32_t ade_gather(TS* __restrict__ g, TS* __restrict__ glink, const SparseView& S,
-                                               const AP& P, int n_mobile, const int* __restrict__ mob_species,
-                                               int64_t k_west_end, int64_t k_east_begin, TC* sp_base,
-                                               uint32_t* ob, int stride, int64_t k, const AdeMeta& M) {
+__device__ __forceinline__ uint32_t ade_gather(TS* __restrict__ g, const TC* __restrict__ u,
+                                               const double* __restrict__ bio, const SparseView& S, const AP& P,
+                                               int n_mobile, const int* __restrict__ mob_species,
+                                               int64_t k_west_end, int64_t k_east_begin, const AdeFrame<TC>& F,
+                                               int64_t k, const AdeMeta& M) {
+    constexpr int T = ADE_THREADS;
     if (P.dyn[M.code] == ADE_BB) return 0u;
     const uint32_t K32 = (uint32_t)S.KS;  // row stride; SS < 2^31 is checked when the layout is built
     const bool west = k < k_west_end, east = k >= k_east_begin;
@@ -208,7 +249,7 @@ __device__ __forceinline__ uint32_t ade_gather(TS* __restrict__ g, TS* __restric
         }
     }
 #pragma unroll
-    for (int i = 0; i < 7; ++i) ob[i * stride] = off[i];
+    for (int i = 0; i < 7; ++i) F.off[i * T] = off[i];
     uint32_t actm = 0;
 #pragma unroll
     for (int m = 0; m < NM; ++m) {
@@ -216,43 +257,54 @@ __device__ __forceinline__ uint32_t ade_gather(TS* __restrict__ g, TS* __restric
         const int s = mob_species[m];
         if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
         actm |= 1u << m;
-        TS* f = g + (int64_t)m * S.SS;
-        TC* slot = sp_base + (m * 7) * stride;
+        const TS* f = g + (int64_t)m * S.SS;
+        TC* slot = F.pop + (m * 7) * T;
         if constexpr (sizeof(TS) >= 4) {
             // 4- and 8-byte populations go straight to the slots as asynchronous copies, so a
             // thread has all of its loads in flight at once without holding them in registers
 #pragma unroll
-            for (int i = 0; i < 7; ++i) cp_async<sizeof(TS)>(slot + i * stride, f + off[i]);
+            for (int i = 0; i < 7; ++i) cp_async<sizeof(TS)>(slot + i * T, f + off[i]);
         } else {
 #pragma unroll
-            for (int i = 0; i < 7; ++i) slot[i * stride] = ld<TS, TC>(f + off[i]);
+            for (int i = 0; i < 7; ++i) slot[i * T] = ld<TS, TC>(f + off[i]);
         }
+    }
+    // the velocity and the biomass the kinetics reads travel with the populations
+    const int64_t K = S.K;
+    if constexpr (ade_u_staged<TC>() == 3) {
+        cp_async<sizeof(TC)>(F.u, u + k);
+        cp_async<sizeof(TC)>(F.u + T, u + K + k);
+        cp_async<sizeof(TC)>(F.u + 2 * T, u + 2 * K + k);
+    }
+    if (P.law == CLB_LAW_DUAL_MONOD && !west && !east && P.react[M.code]) {
+        const int bn = P.M < ade_bio_cache<TC>() ? P.M : ade_bio_cache<TC>();
+        for (int mb = 0; mb < bn; ++mb) cp_async<8>(F.bio + mb * T, bio + (int64_t)mb * P.g.N + M.nd);
     }
     return actm;
 }
 
-// The second half, once the gathered populations are in the slots: boundary completion, sums,
-// kinetics, collision with the deposit, scatter back to the node's slots.
+// The second half, once the staged values are in the frame: boundary completion, sums, kinetics,
+// collision with the deposit, scatter back to the node's slots.
 template <typename TS, typename TC, bool ODD, int NM, bool EXT, typename AP>
-__device__ __forceinline__ void ade_finish(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm,
-                                           double* __restrict__ bio, const TC* __restrict__ u, const SparseView& S,
-                                           const double* __restrict__ neu, const AP& P, int n_mobile,
-                                           const int* __restrict__ mob_species, int64_t k_west_end,
-                                           int64_t k_east_begin, const AdeExtra& X, TC* sp_base, uint32_t* ob,
-                                           int stride, int64_t k, int code, uint32_t actm) {
+__device__ __forceinline__ void ade_finish(TS* __restrict__ g, double* __restrict__ imm, double* __restrict__ bio,
+                                           const TC* __restrict__ u, const SparseView& S, const double* __restrict__ neu, const AP& P,
+                                           int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end,
+                                           int64_t k_east_begin, const AdeExtra& X, const AdeFrame<TC>& F,
+                                           int64_t k, const AdeMeta& M, uint32_t actm) {
+    constexpr int T = ADE_THREADS;
+    const int code = M.code;
     const int dyn = P.dyn[code];
     if (dyn == ADE_BB) return;
     const Geom G = P.g;
-    const int64_t K = S.K;
     const bool west = k < k_west_end, east = k >= k_east_begin;
     int p = 0;
-    if (west || east) p = (int)(S.node[k] % G.plane);
+    if (west || east) p = (int)(M.nd % G.plane);
     TC rb[NM];
 #pragma unroll
     for (int m = 0; m < NM; ++m) {
         rb[m] = 0;
         if (!((actm >> m) & 1u)) continue;
-        TC* slot = sp_base + (m * 7) * stride;
+        TC* slot = F.pop + (m * 7) * T;
         if ((west || east) && dyn != ADE_NONE) {
             // AdvectionDiffusionBoundaryDynamics: the one inward population makes the
             // node's density equal to the stored value
@@ -265,28 +317,38 @@ __device__ __forceinline__ void ade_finish(TS* __restrict__ g, TS* __restrict__ 
             TC sum = 0;
 #pragma unroll
             for (int i = 0; i < 7; ++i)
-                if (i != miss) sum += slot[i * stride];
-            slot[miss * stride] = (TC)(rs - 1.0) - sum;
+                if (i != miss) sum += slot[i * T];
+            slot[miss * T] = (TC)(rs - 1.0) - sum;
         }
         TC r = 0;
 #pragma unroll
-        for (int i = 0; i < 7; ++i) r += slot[i * stride];
+        for (int i = 0; i < 7; ++i) r += slot[i * T];
         rb[m] = r;
     }
     TC dC[NM];  // increments of the mobile species, in the arithmetic type of the deposit
-    node_kinetics<TC, NM, EXT>(P, S, X, k, code, west, east, n_mobile, rb, imm, bio, dC);
+    node_kinetics<TC, NM, EXT>(P, X, k, M.nd, code, west, east, n_mobile, rb, imm, bio, F.bio,
+                               P.M < ade_bio_cache<TC>() ? P.M : ade_bio_cache<TC>(), dC);
     // ---- phase 2: collide, deposit, stream, species by species from the shared slots
     uint32_t off2[7];  // read back rather than kept live through the kinetics
 #pragma unroll
-    for (int i = 0; i < 7; ++i) off2[i] = ob[i * stride];
-    const TC ux = u[k], uy = u[K + k], uz = u[2 * K + k];
+    for (int i = 0; i < 7; ++i) off2[i] = F.off[i * T];
+    TC ux, uy, uz;
+    if constexpr (ade_u_staged<TC>() == 3) {
+        ux = F.u[0];
+        uy = F.u[T];
+        uz = F.u[2 * T];
+    } else {
+        ux = u[k];
+        uy = u[S.K + k];
+        uz = u[2 * S.K + k];
+    }
 #pragma unroll
     for (int m = 0; m < NM; ++m) {
         if (!((actm >> m) & 1u)) continue;
         const int s = mob_species[m];
         TC q[7], o[7];
 #pragma unroll
-        for (int i = 0; i < 7; ++i) q[i] = sp_base[(m * 7 + i) * stride];
+        for (int i = 0; i < 7; ++i) q[i] = F.pop[(m * 7 + i) * T];
         if (dyn == ADE_NONE) {
 #pragma unroll
             for (int i = 0; i < 7; ++i) o[i] = q[i];
@@ -313,33 +375,30 @@ __device__ __forceinline__ void ade_finish(TS* __restrict__ g, TS* __restrict__ 
 }
 
 template <typename TS, typename TC, bool ODD, int NM, bool EXT, typename AP>
-__device__ __forceinline__ void ade_node(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm,
-                                         double* __restrict__ bio, const TC* __restrict__ u, const SparseView& S,
+__device__ __forceinline__ void ade_node(TS* __restrict__ g, double* __restrict__ imm, double* __restrict__ bio,
+                                         const TC* __restrict__ u, const SparseView& S,
                                          const double* __restrict__ neu, const AP& P, int n_mobile,
                                          const int* __restrict__ mob_species, int64_t k_west_end,
-                                         int64_t k_east_begin, const AdeExtra& X, TC* sp_base, uint32_t* ob,
-                                         int stride, int64_t k) {
+                                         int64_t k_east_begin, const AdeExtra& X, const AdeFrame<TC>& F, int64_t k) {
     const AdeMeta M = ade_meta<ODD>(S, k);
-    const uint32_t actm = ade_gather<TS, TC, ODD, NM>(g, glink, S, P, n_mobile, mob_species, k_west_end,
-                                                      k_east_begin, sp_base, ob, stride, k, M);
-    if constexpr (sizeof(TS) >= 4) cp_async_wait_all();  // each thread reads only its own slots
-    ade_finish<TS, TC, ODD, NM, EXT>(g, glink, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end,
-                                     k_east_begin, X, sp_base, ob, stride, k, M.code, actm);
+    const uint32_t actm = ade_gather<TS, TC, ODD, NM>(g, u, bio, S, P, n_mobile, mob_species, k_west_end,
+                                                      k_east_begin, F, k, M);
+    cp_async_wait_all();  // each thread reads only its own slots
+    ade_finish<TS, TC, ODD, NM, EXT>(g, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end, k_east_begin, X,
+                                     F, k, M, actm);
 }
 
 template <typename TS, typename TC, bool ODD, int NM, bool EXT>
 __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>()))
-    k_ade_aa(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm, double* __restrict__ bio,
-             const TC* __restrict__ u, const SparseView S, const double* __restrict__ neu, const AdeParams P,
-             int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin,
-             const AdeExtra X) {
+    k_ade_aa(TS* __restrict__ g, double* __restrict__ imm, double* __restrict__ bio, const TC* __restrict__ u,
+             const SparseView S, const double* __restrict__ neu, const AdeParams P, int n_mobile,
+             const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin, const AdeExtra X) {
     const int64_t K = S.K;
     extern __shared__ __align__(16) unsigned char ade_smem[];
-    TC* sp = reinterpret_cast<TC*>(ade_smem);
-    uint32_t* ob = reinterpret_cast<uint32_t*>(ade_smem + (size_t)NM * 7 * blockDim.x * sizeof(TC));
+    const AdeFrame<TC> F = ade_frame<TC, NM>(ade_smem, 0);
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x)
-        ade_node<TS, TC, ODD, NM, EXT>(g, glink, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end,
-                                       k_east_begin, X, sp + threadIdx.x, ob + threadIdx.x, blockDim.x, k);
+        ade_node<TS, TC, ODD, NM, EXT>(g, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end, k_east_begin,
+                                       X, F, k);
 }
 
 // resident blocks per SM of the pipelined step (two slot sets per thread); 0: does not fit twice
@@ -350,29 +409,26 @@ constexpr int ade_pipe_minb() {
 }
 
 // The transport step with the gathers of the next node in flight while a node is finished: two
-// slot sets per thread; node k + stride's populations go to one by asynchronous copies while node
-// k's are finished from the other, and the metadata of the node after that is loading. Same
-// arithmetic and memory traffic as k_ade_aa. For 4- and 8-byte storage where two slot sets leave
-// at least two resident blocks per SM.
+// slot sets per thread; node k + stride's values go to one by asynchronous copies while node k is
+// finished from the other, and the metadata of the node after that is loading. Same arithmetic
+// and memory traffic as k_ade_aa. For 4- and 8-byte storage where two slot sets leave at least
+// two resident blocks per SM.
 template <typename TS, typename TC, bool ODD, int NM, bool EXT>
 __global__ void __launch_bounds__(ADE_THREADS, (ade_pipe_minb<TC, NM>() < 1 ? 1 : ade_pipe_minb<TC, NM>()))
-    k_ade_pipe(TS* __restrict__ g, TS* __restrict__ glink, double* __restrict__ imm, double* __restrict__ bio,
-               const TC* __restrict__ u, const SparseView S, const double* __restrict__ neu, const AdeParams P,
-               int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin,
-               const AdeExtra X) {
+    k_ade_pipe(TS* __restrict__ g, double* __restrict__ imm, double* __restrict__ bio, const TC* __restrict__ u,
+               const SparseView S, const double* __restrict__ neu, const AdeParams P, int n_mobile,
+               const int* __restrict__ mob_species, int64_t k_west_end, int64_t k_east_begin, const AdeExtra X) {
     const int64_t K = S.K;
-    const int nt = blockDim.x, tid = threadIdx.x;
     extern __shared__ __align__(16) unsigned char ade_smem[];
-    TC* sp = reinterpret_cast<TC*>(ade_smem) + tid;                                        // [2][NM * 7][nt]
-    uint32_t* ob = reinterpret_cast<uint32_t*>(ade_smem + (size_t)2 * NM * 7 * nt * sizeof(TC)) + tid;  // [2][7][nt]
-    const int64_t sk = (int64_t)gridDim.x * nt;
-    int64_t k = (int64_t)blockIdx.x * nt + tid;
+    const AdeFrame<TC> F0 = ade_frame<TC, NM>(ade_smem, 0), F1 = ade_frame<TC, NM>(ade_smem, 1);
+    const int64_t sk = (int64_t)gridDim.x * blockDim.x;
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     AdeMeta cur, nxt;
     uint32_t acur = 0, anxt = 0;
     if (k < K) {
         cur = ade_meta<ODD>(S, k);
-        acur = ade_gather<TS, TC, ODD, NM>(g, glink, S, P, n_mobile, mob_species, k_west_end, k_east_begin, sp, ob,
-                                           nt, k, cur);
+        acur = ade_gather<TS, TC, ODD, NM>(g, u, bio, S, P, n_mobile, mob_species, k_west_end, k_east_begin, F0, k,
+                                           cur);
     }
     cp_async_commit();
     int64_t kn = k + sk;
@@ -380,16 +436,15 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_pipe_minb<TC, NM>() < 1 ? 1 
     int q = 0;
     while (k < K) {
         if (kn < K)
-            anxt = ade_gather<TS, TC, ODD, NM>(g, glink, S, P, n_mobile, mob_species, k_west_end, k_east_begin,
-                                               sp + (q ^ 1) * NM * 7 * nt, ob + (q ^ 1) * 7 * nt, nt, kn, nxt);
+            anxt = ade_gather<TS, TC, ODD, NM>(g, u, bio, S, P, n_mobile, mob_species, k_west_end, k_east_begin,
+                                               q ? F0 : F1, kn, nxt);
         cp_async_commit();
         const int64_t knn = kn + sk;
         AdeMeta nn;
         if (knn < K) nn = ade_meta<ODD>(S, knn);
-        cp_async_wait_group<1>();  // node k's populations have landed
-        ade_finish<TS, TC, ODD, NM, EXT>(g, glink, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end,
-                                         k_east_begin, X, sp + q * NM * 7 * nt, ob + q * 7 * nt, nt, k, cur.code,
-                                         acur);
+        cp_async_wait_group<1>();  // node k's values have landed
+        ade_finish<TS, TC, ODD, NM, EXT>(g, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end, k_east_begin, X,
+                                         q ? F1 : F0, k, cur, acur);
         k = kn;
         kn = knn;
         cur = nxt;
@@ -785,6 +840,16 @@ static int ade_grid_for(const void* kern, int smem, int num_sms, int threads) {
     for (auto& kv : known)
         if (kv.kern == kern && kv.smem == smem && kv.threads == threads) return kv.blocks * num_sms;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    // Shared memory for at most ADE_RESIDENT blocks per SM; the rest of the SM's 256 KB stays L1
+    // cache, which the odd step's neighbour gathers reuse (more resident blocks with less L1 ran
+    // slower on B200).
+    {
+        const int per_block = smem + 1024;  // the runtime reserves 1 KB per block
+        const int fit = std::max(1, (228 * 1024) / per_block);
+        const int res = std::min(ADE_RESIDENT, fit);
+        const int pct = (int)((100LL * res * per_block + 228 * 1024 - 1) / (228 * 1024));
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct > 100 ? 100 : pct);
+    }
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, smem) != cudaSuccess || nb < 1) nb = 1;
     known.push_back({kern, smem, threads, nb});
@@ -796,7 +861,6 @@ static void launch_ade_t(clb_handle* h) {
     const int nm = h->n_mobile;
     const int nb = h->S;  // register bucket covers every species (mobile first, then immobile)
     TS* g = (TS*)h->d_g;
-    TS* gl = (TS*)h->d_glink;
     const TC* u = (const TC*)h->d_u;
     int* mt = mob_table(h);
     const SparseView S = view_of(h->ade_sp);
@@ -809,7 +873,7 @@ static void launch_ade_t(clb_handle* h) {
             auto kern = k_ade_pipe<TS, TC, ODD, NM, EXT>;                                                          \
             const int sm = 2 * ade_slot_bytes<TC, NM>();                                                           \
             const int gr = ade_grid_for((const void*)kern, sm, h->num_sms, ADE_THREADS);                           \
-            kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,    \
+            kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,        \
                                                      h->ade_west_end, h->ade_east_begin, X);                      \
             break;                                                                                                \
             }                                                                                                     \
@@ -817,7 +881,7 @@ static void launch_ade_t(clb_handle* h) {
         auto kern = k_ade_aa<TS, TC, ODD, NM, EXT>;                                                               \
         const int sm = ade_slot_bytes<TC, NM>();                                                                  \
         const int gr = ade_grid_for((const void*)kern, sm, h->num_sms, ADE_THREADS);                              \
-        kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, gl, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,        \
+        kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,            \
                                                  h->ade_west_end, h->ade_east_begin, X);                          \
     } while (0)
     if (ext) {
@@ -884,10 +948,10 @@ __device__ __forceinline__ int batch_find(const int64_t* off, int n, int64_t t) 
 // One transport step of every domain (no abiotic law, no dissolution): the species nodes of all
 // domains form one index range; shared memory holds the slots, then the domain offsets.
 template <typename TS, typename TC, bool ODD, int NM>
-__global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>())) k_ade_batch(const BatchView B) {
+__global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>() > 6 ? 6 : ade_minb<TC, NM>()))
+    k_ade_batch(const BatchView B) {
     extern __shared__ __align__(16) unsigned char ade_smem[];
-    TC* sp = reinterpret_cast<TC*>(ade_smem);
-    uint32_t* ob = reinterpret_cast<uint32_t*>(ade_smem + (size_t)NM * 7 * ADE_THREADS * sizeof(TC));
+    const AdeFrame<TC> F = ade_frame<TC, NM>(ade_smem, 0);
     int64_t* soff = reinterpret_cast<int64_t*>(ade_smem + ade_slot_bytes<TC, NM>());
     for (int i = threadIdx.x; i <= B.ndom; i += blockDim.x) soff[i] = B.aoff[i];
     __syncthreads();
@@ -900,9 +964,8 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>())) k_ade_batch
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int di = batch_find(soff, B.ndom, t);
         const BatchDomain& d = B.dom[di];
-        ade_node<TS, TC, ODD, NM, false>((TS*)d.g, (TS*)d.glink, d.imm, d.bio, (const TC*)d.u, d.as, d.neu, d.ap,
-                                         d.n_mobile, d.mob, d.akw, d.ake, X, sp + threadIdx.x, ob + threadIdx.x,
-                                         blockDim.x, t - soff[di]);
+        ade_node<TS, TC, ODD, NM, false>((TS*)d.g, d.imm, d.bio, (const TC*)d.u, d.as, d.neu, d.ap, d.n_mobile,
+                                         d.mob, d.akw, d.ake, X, F, t - soff[di]);
     }
 }
 

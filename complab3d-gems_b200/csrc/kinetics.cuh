@@ -9,13 +9,15 @@ namespace clb {
 // Biotic rate laws (clb_law) over the species in internal order (mobile first), in the kinetics
 // type KT (the lattice's arithmetic type: FP64 for FP64 lattices, FP32 otherwise). C holds the
 // floored concentrations; R receives the species rates. The biomass of microbe m (dense FP64 field
-// bio[m][N] at voxel nd) is read and floored and, with APPLY_BIO, advanced in place with its
+// bio[m][N] at voxel nd; the first bn microbes from the staged copy bc, stride bstride) is read and
+// floored and, with APPLY_BIO, advanced in place with its
 // clamped increment (dB = max(R_B dt, -B), applied when |dB| > THRD), microbe by microbe, so no
 // per-microbe array is kept. Loops over species are unrolled to the bucket NB so every array stays
 // in registers.
 template <typename KT, int NB, bool APPLY_BIO>
 __device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[NB], KT (&R)[NB],
-                                             const double* __restrict__ bio, int64_t nd, int64_t N) {
+                                             const double* __restrict__ bio, int64_t nd, int64_t N,
+                                             const double* bc = nullptr, int bstride = 0, int bn = 0) {
     const KT thr = (KT)THRD;
 #pragma unroll
     for (int s = 0; s < NB; ++s) R[s] = 0;
@@ -42,7 +44,7 @@ __device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[N
                 const int a = P.acceptor[m];
                 if (a < 0) continue;
                 const double* bp = bio + (int64_t)m * N + nd;
-                const double braw = *bp;
+                const double braw = m < bn ? bc[m * bstride] : *bp;  // staged copy, else memory
                 const KT Bm = braw < THRD ? (KT)0 : (KT)braw;
                 if (Bm <= (KT)0) continue;
                 KT Ca = 0;

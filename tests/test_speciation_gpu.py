@@ -141,25 +141,40 @@ def test_surrogate_trains_and_matches_newton(trained, oracle):
     assert acc.mean() > 0.8
 
 
-def test_surrogate_gain_over_newton(trained):
-    D, S, logK, comp, lo, hi, rep = trained
-    states = workloads.species_states(400000, 4, np.array(lo), np.array(hi), seed=7)
-    D.speciation_solve(states[:1000])
-    D.surrogate_predict(states[:1000])
-
-    def best(fn, reps=3):
+def test_surrogate_gain_over_newton(clb, trained):
+    """Speciation inside the transport step, where no host transfer is involved: with the trained
+    surrogate (and its Newton polish) a step takes less time than with Newton-Raphson alone."""
+    D0, S, logK, comp, lo, hi, rep = trained
+    params, scaling = D0.surrogate_params()
+    shape = (34, 32, 32)
+    mat = mixed_geometry(*shape, seed=25, biofilm=False)
+    sp = [dict(omega_pore=1 / 0.9, left_type=0, right_type=1, left_bc=b, c0=c)
+          for b, c in zip([2e-3, 1e-6, 1e-5, 5e-4], [1e-4, 3e-7, 2e-6, 1e-5])]
+    times, used = {}, {}
+    for mode in (clb.SPEC_NR, clb.SPEC_MLP_NR):
+        D = clb.Domain(mat, *shape, 0.8, ade_precision=clb.F32)
+        D.ade_init(sp)
+        D.speciation_setup(S, logK, comp, tol=1e-10)
+        D.surrogate_params(params, scaling)
+        D.surrogate_set_check(0.02, 2)
+        D.set_speciation_mode(mode)
+        D.ade_step(4)
+        D.sync()
+        s0 = D.speciation_stats()
         ts = []
-        for _ in range(reps):
+        for _ in range(3):
             t0 = time.perf_counter()
-            fn()
+            D.ade_step(20)
+            D.sync()
             ts.append(time.perf_counter() - t0)
-        return min(ts)
-
-    t_nr = best(lambda: D.speciation_solve(states))
-    t_sg = best(lambda: D.surrogate_predict(states, residual_check=False))
-    print("Newton-Raphson %.1f ms, surrogate + polish %.1f ms (400k states, host transfers included, best of 3)"
-          % (t_nr * 1e3, t_sg * 1e3))
-    assert t_sg < t_nr
+        s1 = D.speciation_stats()
+        times[mode] = min(ts)
+        used[mode] = (s1["surrogate_used"] - s0["surrogate_used"]) / max(1, s1["solves"] - s0["solves"])
+        D.close()
+    print("20 transport steps: Newton-Raphson %.2f ms, surrogate + polish %.2f ms (surrogate kept on %.3f)"
+          % (times[clb.SPEC_NR] * 1e3, times[clb.SPEC_MLP_NR] * 1e3, used[clb.SPEC_MLP_NR]))
+    assert used[clb.SPEC_MLP_NR] > 0.5
+    assert times[clb.SPEC_MLP_NR] < times[clb.SPEC_NR]
 
 
 def test_surrogate_with_fallback_in_transport(clb, oracle, trained):
