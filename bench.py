@@ -71,6 +71,30 @@ def peaks():
         return PEAK_FALLBACK, "fallback"
 
 
+def max_over_ranks(torch, ms, world, device):
+    """The slowest rank's time: every rank takes part in the same all-reduce (MAX)."""
+    if world == 1:
+        return ms
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(n_open, steps, ms_max, world):
+    """Whole-job MLUPS of `world` replicas of the same domain: every rank updates n_open nodes per
+    step; the job takes the slowest rank's time."""
+    return world * n_open * steps / (ms_max * 1e-3) / 1e6
+
+
+def step_kernels(tuned, precision):
+    """Names of the two AA-step kernels the flow step ran (the autotuner's choice, else the
+    library's defaults: tiled even step, pipelined odd step for 4- and 8-byte storage)."""
+    choice = tuned.split("->")[-1] if "->" in tuned else ("tma=1,pipe" if precision != "f16s" else "tma=1,minb=3")
+    even = "k_flow_even_tma" if "tma=1" in choice else "k_flow_aa<even>"
+    odd = "k_flow_odd_pipe" if "pipe" in choice else "k_flow_aa<odd>"
+    return f"{even} + {odd} (AA even/odd steps, mean per launch)"
+
+
 def traffic_per_launch(kernel_key):
     """DRAM bytes per launch from the committed ncu summary (profiles/traffic.txt)."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
@@ -471,12 +495,9 @@ def main():
     barrier()
     ms = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1))
     del flush
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(torch, ms, world, "cuda")
     per_step = ms / a.steps
-    value = world * n_open * a.steps / (ms * 1e-3) / 1e6
+    value = replica_throughput(n_open, a.steps, ms, world)
     all_vox = world * nx * ny * nz * a.steps / (ms * 1e-3) / 1e6
 
     # roofline of the step kernel: algorithmic bytes = 2 * 19 * sizeof(storage) per open node
@@ -487,7 +508,7 @@ def main():
     tr = traffic_per_launch(key)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": tr, "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg,
-            "kernel": "k_flow_aa (AA even/odd)"}
+            "kernel": step_kernels(tuned, a.precision)}
 
     # end to end through the C ABI with host buffers: create (material upload) + init (list upload)
     # + the same steps + velocity read back to the host
@@ -521,7 +542,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        v, threads, steps, dt = oracle_mlups(mat, cfg["shape"], cfg["tau"], cfg["delta_p"], 12.0, 2, 50)
+        v, threads, steps, dt = oracle_mlups(mat, cfg["shape"], cfg["tau"], cfg["delta_p"], 12.0, 2, 400)
         cpu = {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port", "cpu": cpu_name(),
                "sample": f"{steps} FP64 steps of the full 258x128x128 map in {dt:.1f} s (OpenMP)"}
 
