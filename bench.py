@@ -520,7 +520,7 @@ def main():
     E = clb.Domain(mat, nx, ny, nz, cfg["tau"], flow_precision=prec, device=local)
     E.flow_init(cfg["delta_p"])
     E.flow_step(k_e2e)
-    u = E.velocity()
+    u = E.velocity(np.float64 if a.precision == "f64" else np.float32)  # the storage's precision
     t_e2e = time.perf_counter() - t0
     ste = E.flow_stats()
     E.close()

@@ -321,9 +321,13 @@ class Domain:
         self._check(lib().clb_flow_stats_get(self.h, char_length, C.byref(s)))
         return {k: getattr(s, k) for k, _ in FlowStats._fields_}
 
-    def velocity(self):
-        u = np.empty(3 * self.N, dtype=np.float64)
-        self._check(lib().clb_get_field(self.h, FIELD_FLOW_VELOCITY, 0, _ptr(u), 0))
+    def velocity(self, dtype=np.float64):
+        """Flow velocity [3][N]; dtype float64 or float32 (the copy to the host is then half as large)."""
+        dt = np.dtype(dtype)
+        if dt not in (np.dtype(np.float64), np.dtype(np.float32)):
+            raise ValueError("velocity dtype is float64 or float32")
+        u = np.empty(3 * self.N, dtype=dt)
+        self._check(lib().clb_get_field(self.h, FIELD_FLOW_VELOCITY, 0, _ptr(u), 0 if dt == np.float64 else 1))
         return u.reshape(3, self.N)
 
     def flow_populations(self):

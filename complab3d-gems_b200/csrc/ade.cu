@@ -837,9 +837,12 @@ static int ade_grid_for(const void* kern, int smem, int num_sms, int threads) {
     static std::mutex mu;
     static std::vector<Known> known;
     std::lock_guard<std::mutex> lock(mu);
-    for (auto& kv : known)
+    int set_max = 0;  // the kernel's dynamic shared-memory limit so far (one attribute for every caller)
+    for (auto& kv : known) {
         if (kv.kern == kern && kv.smem == smem && kv.threads == threads) return kv.blocks * num_sms;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (kv.kern == kern) set_max = std::max(set_max, kv.smem);
+    }
+    if (smem > 48 * 1024 && smem > set_max) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     // Shared memory for at most ADE_RESIDENT blocks per SM; the rest of the SM's 256 KB stays L1
     // cache, which the odd step's neighbour gathers reuse (more resident blocks with less L1 ran
     // slower on B200).

@@ -404,11 +404,13 @@ clb_status clb_get_field(clb_handle* h, int field, int index, void* host, int dt
         std::memcpy(host, h->h_mat.data(), N);
         return CLB_OK;
     }
+    if (field == CLB_FIELD_FLOW_VELOCITY) {
+        if (dtype != 0 && dtype != 1) return fail(h, CLB_INVALID_ARG, "the flow velocity is read as float64 or float32");
+        if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
+        return flow_velocity(h, host, dtype, true);
+    }
     if (dtype != 0) return fail(h, CLB_INVALID_ARG, "fields are read as float64");
     switch (field) {
-        case CLB_FIELD_FLOW_VELOCITY:
-            if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
-            return flow_velocity(h, host, 0, true);
         case CLB_FIELD_FLOW_POPULATIONS:
             if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
             return flow_populations(h, (double*)host);

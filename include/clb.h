@@ -118,7 +118,8 @@ typedef struct clb_stats {
 } clb_stats;
 
 /* Field identifiers for clb_get_field / clb_set_field. dtype: 0 = float64, 1 = float32,
- * 2 = int8. */
+ * 2 = int8. The material map is int8; clb_get_field reads the flow velocity as float64 or
+ * float32 (half the copy to the host), every other field as float64. */
 typedef enum clb_field {
     CLB_FIELD_MATERIAL = 0,       /* int8 [N]                                                */
     CLB_FIELD_FLOW_VELOCITY = 1,  /* [3][N]  computeVelocity of the flow lattice            */

@@ -139,3 +139,15 @@ def test_pipelined_odd_step_refused_for_fp16_storage(clb):
     D.flow_init(1e-4)
     with pytest.raises(clb.ClbError):
         D.tune("flow_odd_pipe", 1)
+
+
+def test_velocity_read_as_float32_equals_float64_rounded(clb):
+    shape = (16, 9, 8)
+    D = clb.Domain(mixed_geometry(*shape, seed=3), *shape, 0.8, flow_precision=clb.F32, **BIO)
+    D.flow_init(2e-4)
+    D.flow_step(30)
+    u64, u32 = D.velocity(), D.velocity(np.float32)
+    assert u32.dtype == np.float32
+    np.testing.assert_array_equal(u32, u64.astype(np.float32))
+    with pytest.raises(ValueError):
+        D.velocity(np.int32)
