@@ -147,7 +147,8 @@ __device__ __forceinline__ void odd_sources(const SparseView& S, int64_t k, int2
     nb[6] = (int)k - 1;
 }
 
-constexpr int ADE_RESIDENT = 4;   // resident blocks per SM the shared-memory carveout is sized for
+constexpr int ADE_RESIDENT = 4;       // resident blocks per SM the carveout is sized for (odd step)
+constexpr int ADE_RESIDENT_EVEN = 5;  // the even step reads only its own slots: less L1, more blocks
 
 // What travels with a node's gathers besides its populations: with 4-byte arithmetic the velocity
 // and the biomass of up to two microbes; FP64 slots already fill the shared memory three blocks
@@ -832,7 +833,7 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
 
 // Resident blocks per SM of a transport-step instantiation with `smem` bytes of shared memory
 // (set up once per instantiation), times the SM count: the persistent grid.
-static int ade_grid_for(const void* kern, int smem, int num_sms, int threads) {
+static int ade_grid_for(const void* kern, int smem, int num_sms, int threads, int resident = ADE_RESIDENT) {
     struct Known { const void* kern; int smem, threads, blocks; };
     static std::mutex mu;
     static std::vector<Known> known;
@@ -843,13 +844,13 @@ static int ade_grid_for(const void* kern, int smem, int num_sms, int threads) {
         if (kv.kern == kern) set_max = std::max(set_max, kv.smem);
     }
     if (smem > 48 * 1024 && smem > set_max) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    // Shared memory for at most ADE_RESIDENT blocks per SM; the rest of the SM's 256 KB stays L1
-    // cache, which the odd step's neighbour gathers reuse (more resident blocks with less L1 ran
-    // slower on B200).
+    // Shared memory for at most `resident` blocks per SM; the rest of the SM's 256 KB stays L1
+    // cache, which the odd step's neighbour gathers reuse (five resident blocks with less L1 ran
+    // the odd step slower on B200; the even step, which reads only its own slots, gained from five).
     {
         const int per_block = smem + 1024;  // the runtime reserves 1 KB per block
         const int fit = std::max(1, (228 * 1024) / per_block);
-        const int res = std::min(ADE_RESIDENT, fit);
+        const int res = std::min(resident, fit);
         const int pct = (int)((100LL * res * per_block + 228 * 1024 - 1) / (228 * 1024));
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct > 100 ? 100 : pct);
     }
@@ -883,7 +884,7 @@ static void launch_ade_t(clb_handle* h) {
         }                                                                                                         \
         auto kern = k_ade_aa<TS, TC, ODD, NM, EXT>;                                                               \
         const int sm = ade_slot_bytes<TC, NM>();                                                                  \
-        const int gr = ade_grid_for((const void*)kern, sm, h->num_sms, ADE_THREADS);                              \
+        const int gr = ade_grid_for((const void*)kern, sm, h->num_sms, ADE_THREADS, ODD ? ADE_RESIDENT : ADE_RESIDENT_EVEN); \
         kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,            \
                                                  h->ade_west_end, h->ade_east_begin, X);                          \
     } while (0)
