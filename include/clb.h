@@ -165,9 +165,10 @@ clb_status clb_get_stream(clb_handle* h, void** stream);
  *                    storage; an error for FP16 storage, which always runs the plain step),
  *                    0: the plain step;
  *   "ade_pipe"       1: transport step with the next node's gathers staged in shared memory by
- *                    asynchronous copies while a node is finished (default; used for FP64/FP32
- *                    storage where two slot sets per thread leave two resident CTAs per SM,
- *                    i.e. up to 8 FP32 or 4 FP64 species), 0: the plain step.
+ *                    asynchronous copies while a node is finished (used for FP64/FP32 storage
+ *                    where two slot sets per thread leave two resident CTAs per SM, i.e. up to
+ *                    8 FP32 or 4 FP64 species), 0: the plain step (default: fewer resident
+ *                    warps made the pipelined step slower on B200).
  * Unknown keys are an error. */
 clb_status clb_tune(clb_handle* h, const char* key, int value);
 
