@@ -438,10 +438,10 @@ __global__ void __launch_bounds__(FLOW_THREADS, MINB)
 // rows go back with bulk stores. A wall link (a, i) takes its incoming opp(i) from its even-step
 // slot X (a global load issued alongside the tile's), writes outgoing i to X, and leaves its
 // odd-step slot Y = f[opp(i)][a] untouched in the tile, so the bulk store rewrites it unchanged.
-constexpr int NSTAGE = 3;
+constexpr int NSTAGE = 2;  // 2 stages x 4 resident CTAs (4-byte storage) beat 3 x 3 on B200
 
 template <typename TS, typename TC>
-__global__ void __launch_bounds__(TILE, 2)
+__global__ void __launch_bounds__(TILE, sizeof(TS) == 8 ? 2 : 4)
     k_flow_even_tma(TS* __restrict__ f, TS* __restrict__ link, const SparseView S, const FlowParams P,
                     Tracer* __restrict__ tr, double* __restrict__ partials, int trace, int64_t k_west_end,
                     int64_t k_east_begin, int* __restrict__ err) {
@@ -475,7 +475,8 @@ __global__ void __launch_bounds__(TILE, 2)
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
         const int q = j % NSTAGE;
         TS* buf = stages + (size_t)q * 19 * TILE;
-        // keep NSTAGE-1 tiles in flight: refill the stage freed two iterations ago
+        // keep NSTAGE-1 tiles in flight: refill the stage of the previous tile once its bulk store
+        // has read it
         const int tn = t + (NSTAGE - 1) * gridDim.x;
         if (tid == 0 && tn < ntiles) {
             bulk_wait_read_all();
