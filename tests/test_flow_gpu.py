@@ -151,3 +151,43 @@ def test_velocity_read_as_float32_equals_float64_rounded(clb):
     np.testing.assert_array_equal(u32, u64.astype(np.float32))
     with pytest.raises(ValueError):
         D.velocity(np.int32)
+
+
+def test_flow_stats_match_the_reference_formulas_on_the_oracle_field(clb, oracle):
+    """Mean |u| and max u_x over x = 1..nx-2, the outlet-plane Darcy velocity (x = nx-2) and the
+    permeability k = u_darcy nu L / dP (complab.cpp:1136-1160), from the GPU against the same
+    reductions of the oracle's velocity field."""
+    shape = (24, 12, 12)
+    nx, ny, nz = shape
+    mat = mixed_geometry(*shape, seed=13, biofilm=False)
+    D, O = make_pair(clb, oracle, mat, shape, 0.8, 2e-4, clb.F64)
+    D.flow_step(300)
+    O.step(300)
+    L = 8.0
+    st = D.flow_stats(L)
+    u = O.velocity().reshape(3, nx, ny, nz)
+    inner = u[:, 1:nx - 1]
+    nu = (0.8 - 0.5) / 3.0
+    darcy = u[0, nx - 2].mean()
+    np.testing.assert_allclose(st["pore_mean_u"], np.sqrt((inner ** 2).sum(0)).mean(), rtol=1e-10)
+    np.testing.assert_allclose(st["pore_max_ux"], inner[0].max(), rtol=1e-10)
+    np.testing.assert_allclose(st["darcy_outlet_ux"], darcy, rtol=1e-10)
+    np.testing.assert_allclose(st["permeability"], darcy * nu * L / 2e-4, rtol=1e-10)
+
+
+def test_peclet_rescale_reaches_the_target_velocity(clb):
+    """The Péclet rescale (complab.cpp:1156-1179): the pressure drop is scaled so that the outlet
+    Darcy velocity gives Pe = u L / D with D the fixed ADE diffusivity; after the one re-solve the
+    achieved Péclet number is within 2 % (Stokes flow is linear in the pressure drop)."""
+    shape = (30, 14, 14)
+    mat = mixed_geometry(*shape, seed=17, solid_block=False, biofilm=False)
+    D = clb.Domain(mat, *shape, 0.8, flow_precision=clb.F64)
+    D.flow_init(1e-4)
+    pe, L, tau_ade = 1.0, 8.0, 0.8
+    dp, it, conv = D.flow_solve_peclet(pe, L, tau_ade, 60000, 1e-8)
+    assert conv and dp != 1e-4
+    st = D.flow_stats(L)
+    d_fixed = 0.25 * (tau_ade - 0.5)
+    nu = (0.8 - 0.5) / 3.0
+    u_darcy = st["permeability"] * dp / (nu * L)
+    assert abs(u_darcy * L / d_fixed - pe) / pe < 0.02
