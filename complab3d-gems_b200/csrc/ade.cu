@@ -542,7 +542,7 @@ template <typename TS>
 __global__ void k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ glink, const double* __restrict__ imm,
                              const double* __restrict__ bio, const SparseView S, const AdeParams P,
                              const int* __restrict__ mob_species, int n_mobile, double* __restrict__ part, int nq,
-                             int64_t k_west_end, int64_t k_east_begin) {
+                             int64_t k_west_end, int64_t k_east_begin, int odd) {
     extern __shared__ double shq[];
     const int S_ = P.S, M = P.M;
     for (int q = threadIdx.x; q < nq; q += blockDim.x) shq[q] = 0.0;
@@ -566,13 +566,24 @@ __global__ void k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ gl
             double c;
             const int m = P.slot[s];
             if (m >= 0) {
+                // content: the node's own slots (every slot of the lattice counted once)
                 double sum = 1.0;
                 for (int i = 0; i < 7; ++i) sum += ldd(g + (int64_t)m * S.SS + (int64_t)i * S.KS + k);
-                c = sum;
+                atomicAdd(&shq[S_ + s], sum);
+                if (open) {
+                    // concentration: the node's incoming populations wherever the step parity
+                    // keeps them (computeDensity after the stream)
+                    const double zero[7] = {0, 0, 0, 0, 0, 0, 0};
+                    double pop[7];
+                    natural<TS, double, 7>(S, P.g, g + (int64_t)m * S.SS, glink + (int64_t)m * S.SS, S.node[k], odd,
+                                           zero, pop);
+                    c = 1.0;
+                    for (int i = 0; i < 7; ++i) c += pop[i];
+                }
             } else {
                 c = imm[(int64_t)s * P.g.N + S.node[k]];
+                atomicAdd(&shq[S_ + s], c);
             }
-            atomicAdd(&shq[S_ + s], c);
             if (open) {
                 atomicAdd(&shq[s], c);
                 if (!isfinite(c)) atomicAdd(&shq[4 * S_ + M], 1.0);
@@ -1220,9 +1231,9 @@ clb_status ade_reduce(clb_handle* h, clb_stats* out) {
     const size_t sh = sizeof(double) * nq;
     const SparseView Sv = view_of(h->ade_sp);
     switch (h->ade_prec) {
-        case CLB_F64: k_ade_reduce<double><<<grid, 256, sh, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
-        case CLB_F32: k_ade_reduce<float><<<grid, 256, sh, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
-        default: k_ade_reduce<__half><<<grid, 256, sh, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
+        case CLB_F64: k_ade_reduce<double><<<grid, 256, sh, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
+        case CLB_F32: k_ade_reduce<float><<<grid, 256, sh, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
+        default: k_ade_reduce<__half><<<grid, 256, sh, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
     }
     std::vector<double> hp((size_t)nq * grid);
     e = cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, h->stream);
@@ -1315,9 +1326,9 @@ clb_status ade_reduce_noalloc(clb_handle* h, clb_stats* out) {
     const size_t sh = sizeof(double) * nq;
     const SparseView Sv = view_of(h->ade_sp);
     switch (h->ade_prec) {
-        case CLB_F64: k_ade_reduce<double><<<grid, 256, sh, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
-        case CLB_F32: k_ade_reduce<float><<<grid, 256, sh, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
-        default: k_ade_reduce<__half><<<grid, 256, sh, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin); break;
+        case CLB_F64: k_ade_reduce<double><<<grid, 256, sh, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
+        case CLB_F32: k_ade_reduce<float><<<grid, 256, sh, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
+        default: k_ade_reduce<__half><<<grid, 256, sh, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
     }
     k_reduce_combine<<<1, 128, 0, h->stream>>>(part, grid, nq, S, fin);
     double q[4 * CLB_MAX_SPECIES + CLB_MAX_MICROBES + 2];

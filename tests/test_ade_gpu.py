@@ -145,3 +145,33 @@ def test_pipelined_step_matches_plain_bit_for_bit(clb, oracle, prec, n_species):
         out.append([D.ade_populations(s) for s in range(n_species)] + [D.biomass(m) for m in range(2)])
     for a, b in zip(*out):
         np.testing.assert_array_equal(a, b)
+
+
+def test_reductions_match_the_oracle_fields(clb, oracle):
+    """clb_reduce over x = 1..nx-2 and the open (pore + biofilm) voxels (complab3d_processors_part3
+    reductions): totals, minima and maxima of each species and of the biomass, the open-voxel count,
+    against the same reductions of the oracle's fields."""
+    shape = (20, 10, 9)
+    nx, ny, nz = shape
+    mat = mixed_geometry(*shape, seed=8)
+    u = flow_field(oracle, mat, shape)
+    N = mat.size
+    bio = np.zeros((2, N))
+    bio[0, mat == 3] = 30.0
+    bio[1, mat == 4] = 20.0
+    D, O = pair(clb, oracle, mat, shape, SPECIES, clb.F64, u, law=3, params=[1e-3, 0.1, 0.4, 1e-5], biomass=bio)
+    D.ade_step(47)
+    O.step(47)
+    r = D.reduce()
+    inner = np.zeros((nx, ny, nz), bool)
+    inner[1:nx - 1] = True
+    open_ = inner.ravel() & np.isin(mat, (2, 3, 4))
+    assert r["open_voxels"] == open_.sum() and r["nonfinite"] == 0
+    for s in range(len(SPECIES)):
+        c = O.concentration(s)[open_]
+        np.testing.assert_allclose(r["total"][s], c.sum(), rtol=1e-11)
+        np.testing.assert_allclose(r["min"][s], c.min(), rtol=1e-11, atol=1e-14)
+        np.testing.assert_allclose(r["max"][s], c.max(), rtol=1e-11)
+    ob = O.biomass()
+    for m in range(2):
+        np.testing.assert_allclose(r["biomass"][m], ob[m][inner.ravel()].sum(), rtol=1e-11)
