@@ -321,12 +321,18 @@ class Domain:
         self._check(lib().clb_flow_stats_get(self.h, char_length, C.byref(s)))
         return {k: getattr(s, k) for k, _ in FlowStats._fields_}
 
-    def velocity(self, dtype=np.float64):
-        """Flow velocity [3][N]; dtype float64 or float32 (the copy to the host is then half as large)."""
+    def velocity(self, dtype=np.float64, out=None):
+        """Flow velocity [3][N]; dtype float64 or float32 (the copy to the host is then half as large).
+        `out`: a contiguous array of 3 N elements of that dtype to fill (for example in pinned memory)."""
         dt = np.dtype(dtype)
         if dt not in (np.dtype(np.float64), np.dtype(np.float32)):
             raise ValueError("velocity dtype is float64 or float32")
-        u = np.empty(3 * self.N, dtype=dt)
+        if out is None:
+            u = np.empty(3 * self.N, dtype=dt)
+        else:
+            if out.dtype != dt or out.size != 3 * self.N or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous array of 3 N elements of the requested dtype")
+            u = out.reshape(-1)
         self._check(lib().clb_get_field(self.h, FIELD_FLOW_VELOCITY, 0, _ptr(u), 0 if dt == np.float64 else 1))
         return u.reshape(3, self.N)
 
