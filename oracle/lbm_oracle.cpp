@@ -529,25 +529,30 @@ static void rates2(const OrcAde* A, const double* C, double* R) {
  *                                        mineral -rate, species j sigma_j rate (examples/15)
  *   DISSOL_MINERAL:     k, log10 Ksp, nu[S]  Omega of the water; below 1 the mineral dissolves at
  *                                        k (Omega - 1), releasing -nu_j times that */
-static void dissol_rate(const OrcAde* A, const double* water, double mineral, double* subsR, double& mR) {
-    const int S = A->S;
+struct DissolLaw {
+    int law, S, sM;
+    const double* p;
+};
+
+static void dissol_rate_p(const DissolLaw& L, const double* water, double mineral, double* subsR, double& mR) {
+    const int S = L.S;
     for (int s = 0; s < S; ++s) subsR[s] = 0;
     mR = 0;
-    const std::vector<double>& p = A->dprm;
-    if (A->dis_law == DISSOL_FIRST_ORDER) {
+    const double* p = L.p;
+    if (L.law == DISSOL_FIRST_ORDER) {
         const int h = (int)p[1];
         const double rate = p[0] * (h >= 0 ? std::max(water[h], 0.0) : 1.0) * std::max(mineral, 0.0);
         mR = -rate;
         for (int j = 0; j < S; ++j) subsR[j] = p[2 + j] * rate;
-    } else if (A->dis_law == DISSOL_MINERAL) {
+    } else if (L.law == DISSOL_MINERAL) {
         double la = 0;
         for (int j = 0; j < S; ++j)
-            if (j != A->sM && p[2 + j] != 0.0) la += p[2 + j] * std::log10(std::max(water[j], 1e-30));
+            if (j != L.sM && p[2 + j] != 0.0) la += p[2 + j] * std::log10(std::max(water[j], 1e-30));
         const double om = std::pow(10.0, la - p[1]);
         if (om < 1.0) {
             mR = p[0] * (om - 1.0);
             for (int j = 0; j < S; ++j)
-                if (j != A->sM) subsR[j] = -p[2 + j] * mR;
+                if (j != L.sM) subsR[j] = -p[2 + j] * mR;
         }
     }
 }
@@ -561,6 +566,95 @@ static double dens_post(const OrcAde* A, int s, size_t n) {
     for (int i = 0; i < Q7; ++i) c += A->gp[s][n * Q7 + i];
     return c + 1.0;
 }
+
+/* Dissolution of the stamped (precipitated) mineral voxels, added into dC[s][n]: pass 1 parks one
+ * product share per open face in the mineral voxel's own increment slot and takes the mineral out
+ * (surfaceDissolutionKinetics3D, dissolutionVOP.hh:379-605: water averaged over the open faces,
+ * at most half the mineral per step, products scaled alike); pass 2 lets every open voxel collect
+ * the shares of its mineral face neighbours, a negative share clamped to the headroom
+ * (dissolutionGather3D, :608-742). dens(s, n) is the density the processors see, open(n) whether
+ * the voxel is neither solid nor wall. */
+extern "C++" {
+template <typename Dens, typename Open>
+static void dissolution_park_gather(int nx, int ny, int nz, int S, int sM, double dt, int surf, const uint8_t* stamp,
+                                    const DissolLaw& L, Dens dens, Open open, std::vector<double>& dC) {
+    const size_t N = (size_t)nx * ny * nz;
+    auto id = [&](int x, int y, int z) { return ((size_t)x * ny + y) * nz + z; };
+    // pass 1: park
+    std::vector<double> water(S), subsR(S);
+    for (int x = 1; x < nx - 1; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = id(x, y, z);
+                if (!stamp[n]) continue;
+                const double mineral = dens(sM, n);
+                if (!(mineral > THRD)) continue;
+                int opn[6], no = 0;
+                for (int d = 0; d < 6; ++d) {
+                    int X = x + DLOC[d][0], Y = y + DLOC[d][1], Z = z + DLOC[d][2];
+                    if (X < 1 || X > nx - 2 || Y < 0 || Y > ny - 1 || Z < 0 || Z > nz - 1) continue;
+                    if (!open(id(X, Y, Z))) continue;
+                    opn[no++] = d;
+                }
+                if (no == 0 && surf) continue;
+                for (int s2 = 0; s2 < S; ++s2) water[s2] = 0;
+                if (no > 0) {
+                    for (int k = 0; k < no; ++k) {
+                        const int d = opn[k];
+                        size_t m = id(x + DLOC[d][0], y + DLOC[d][1], z + DLOC[d][2]);
+                        for (int s2 = 0; s2 < S; ++s2) water[s2] += dens(s2, m);
+                    }
+                    for (int s2 = 0; s2 < S; ++s2) water[s2] /= (double)no;
+                }
+                for (int s2 = 0; s2 < S; ++s2)
+                    if (water[s2] < 0) water[s2] = 0;
+                double mR;
+                dissol_rate_p(L, water.data(), mineral, subsR.data(), mR);
+                if (!(mR < 0)) continue;
+                double dM = mR * dt;
+                double scale = 1.0;
+                const double maxRemove = 0.5 * mineral;
+                if (-dM > maxRemove) scale = maxRemove / (-dM);
+                dM *= scale;
+                if (!(-dM > THRD)) continue;
+                dC[(size_t)sM * N + n] += dM;
+                if (no > 0)
+                    for (int s2 = 0; s2 < S; ++s2) {
+                        if (s2 == sM) continue;
+                        const double rel = subsR[s2] * dt * scale;
+                        if (std::fabs(rel) <= THRD) continue;
+                        dC[(size_t)s2 * N + n] += rel / (double)no;
+                    }
+            }
+    // pass 2: gather
+    for (int x = 1; x < nx - 1; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = id(x, y, z);
+                if (!open(n)) continue;
+                for (int d = 0; d < 6; ++d) {
+                    int X = x + DLOC[d][0], Y = y + DLOC[d][1], Z = z + DLOC[d][2];
+                    if (X < 1 || X > nx - 2 || Y < 0 || Y > ny - 1 || Z < 0 || Z > nz - 1) continue;
+                    size_t m = id(X, Y, Z);
+                    if (!stamp[m]) continue;
+                    for (int s2 = 0; s2 < S; ++s2) {
+                        if (s2 == sM) continue;
+                        const double share = dC[(size_t)s2 * N + m];
+                        if (std::fabs(share) <= 1e-14) continue;
+                        double give = share;
+                        if (give < 0) {
+                            const double have = dens(s2, n);
+                            const double head = (have > 0 ? have : 0.0) + dC[(size_t)s2 * N + n];
+                            if (give + head < 0) give = -head;
+                            if (give > 0) give = 0;
+                        }
+                        if (!(std::fabs(give) > 1e-14)) continue;
+                        dC[(size_t)s2 * N + n] += give;
+                    }
+                }
+            }
+}
+}  // extern "C++"
 
 /* The abiotic block of complab.cpp:2460-2525 after the biotic increments are applied: abiotic
  * rates (with the clamp dC = max(R dt, -C)), dissolution of sealed mineral voxels parked per open
@@ -605,80 +699,11 @@ static void abiotic_block(OrcAde* A) {
         }
     }
     if (A->dis_on && A->sM >= 0) {
-        const int sM = A->sM;
-        // pass 1: park
-        std::vector<double> water(S), subsR(S);
-        for (int x = 1; x < nx - 1; ++x)
-            for (int y = 0; y < ny; ++y)
-                for (int z = 0; z < nz; ++z) {
-                    size_t n = A->id(x, y, z);
-                    if (!A->stamp[n]) continue;
-                    const double mineral = A->imm[sM][n];
-                    if (!(mineral > THRD)) continue;
-                    int open[6], no = 0;
-                    for (int d = 0; d < 6; ++d) {
-                        int X = x + DLOC[d][0], Y = y + DLOC[d][1], Z = z + DLOC[d][2];
-                        if (X < 1 || X > nx - 2 || Y < 0 || Y > ny - 1 || Z < 0 || Z > nz - 1) continue;
-                        if (!A->react[(uint8_t)A->mat[A->id(X, Y, Z)]]) continue;
-                        open[no++] = d;
-                    }
-                    if (no == 0 && A->dis_surf) continue;
-                    for (int s2 = 0; s2 < S; ++s2) water[s2] = 0;
-                    if (no > 0) {
-                        for (int k = 0; k < no; ++k) {
-                            const int d = open[k];
-                            size_t m = A->id(x + DLOC[d][0], y + DLOC[d][1], z + DLOC[d][2]);
-                            for (int s2 = 0; s2 < S; ++s2) water[s2] += dens_post(A, s2, m);
-                        }
-                        for (int s2 = 0; s2 < S; ++s2) water[s2] /= (double)no;
-                    }
-                    for (int s2 = 0; s2 < S; ++s2)
-                        if (water[s2] < 0) water[s2] = 0;
-                    double mR;
-                    dissol_rate(A, water.data(), mineral, subsR.data(), mR);
-                    if (!(mR < 0)) continue;
-                    double dM = mR * A->dt;
-                    double scale = 1.0;
-                    const double maxRemove = 0.5 * mineral;
-                    if (-dM > maxRemove) scale = maxRemove / (-dM);
-                    dM *= scale;
-                    if (!(-dM > THRD)) continue;
-                    dC[(size_t)sM * N + n] += dM;
-                    if (no > 0)
-                        for (int s2 = 0; s2 < S; ++s2) {
-                            if (s2 == sM) continue;
-                            const double rel = subsR[s2] * A->dt * scale;
-                            if (std::fabs(rel) <= THRD) continue;
-                            dC[(size_t)s2 * N + n] += rel / (double)no;
-                        }
-                }
-        // pass 2: gather
-        for (int x = 1; x < nx - 1; ++x)
-            for (int y = 0; y < ny; ++y)
-                for (int z = 0; z < nz; ++z) {
-                    size_t n = A->id(x, y, z);
-                    if (!A->react[(uint8_t)A->mat[n]]) continue;
-                    for (int d = 0; d < 6; ++d) {
-                        int X = x + DLOC[d][0], Y = y + DLOC[d][1], Z = z + DLOC[d][2];
-                        if (X < 1 || X > nx - 2 || Y < 0 || Y > ny - 1 || Z < 0 || Z > nz - 1) continue;
-                        size_t m = A->id(X, Y, Z);
-                        if (!A->stamp[m]) continue;
-                        for (int s2 = 0; s2 < S; ++s2) {
-                            if (s2 == sM) continue;
-                            const double share = dC[(size_t)s2 * N + m];
-                            if (std::fabs(share) <= 1e-14) continue;
-                            double give = share;
-                            if (give < 0) {
-                                const double have = dens_post(A, s2, n);
-                                const double head = (have > 0 ? have : 0.0) + dC[(size_t)s2 * N + n];
-                                if (give + head < 0) give = -head;
-                                if (give > 0) give = 0;
-                            }
-                            if (!(std::fabs(give) > 1e-14)) continue;
-                            dC[(size_t)s2 * N + n] += give;
-                        }
-                    }
-                }
+        const DissolLaw L{A->dis_law, S, A->sM, A->dprm.data()};
+        dissolution_park_gather(
+            nx, ny, nz, S, A->sM, A->dt, A->dis_surf, A->stamp.data(), L,
+            [&](int s2, size_t n) { return dens_post(A, s2, n); },
+            [&](size_t n) { return A->react[(uint8_t)A->mat[n]] != 0; }, dC);
     }
     // apply
 #pragma omp parallel for schedule(static)
@@ -1409,4 +1434,21 @@ extern "C" void orc_ade_set_speciation(OrcAde* A, int ns, int nc, const double* 
     t->tol = tol;
     t->max_it = max_it;
     A->spec = t;
+}
+
+/* The dissolution increments of one step for given fields, outside any lattice: densities C[s][N]
+ * as the processors see them, material map, stamp (precipitated mineral voxels), the mineral
+ * species sM and the dissolution law; dC[s][N] holds the increments already pending (abiotic
+ * law) and receives the parked and gathered ones. Used to pin the restatement against the
+ * reference's own surfaceDissolutionKinetics3D / dissolutionGather3D. */
+extern "C" void orc_dissolution_increments(int nx, int ny, int nz, int S, int sM, double dt, int law,
+                                           const double* prm, int surface_only, const int8_t* mat, int solid,
+                                           int bb, const uint8_t* stamp, const double* C, double* dC) {
+    const size_t N = (size_t)nx * ny * nz;
+    std::vector<double> d(dC, dC + (size_t)S * N);
+    const DissolLaw L{law, S, sM, prm};
+    dissolution_park_gather(
+        nx, ny, nz, S, sM, dt, surface_only, stamp, L, [&](int s, size_t n) { return C[(size_t)s * N + n]; },
+        [&](size_t n) { return mat[n] != solid && mat[n] != bb; }, d);
+    std::copy(d.begin(), d.end(), dC);
 }

@@ -64,6 +64,7 @@ def lib():
             "orc_ca_fields": ([vp, vp, vp], None),
             "orc_flow_set_material": ([vp, vp], None),
             "orc_flow_set_dynamics": ([vp, ip, ip, dp], None),
+            "orc_dissolution_increments": ([ip, ip, ip, ip, ip, dp, ip, vp, ip, vp, ip, ip, vp, vp, vp], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -271,3 +272,18 @@ class OracleAde:
         b = np.empty(self.M * self.N)
         lib().orc_ade_biomass(self.h, _p(b))
         return b.reshape(self.M, self.N)
+
+
+def dissolution_increments(shape, S, sM, dt, law, prm, surface_only, mat, solid, bb, stamp, C, dC):
+    """The dissolution increments of one step for given fields (park per open face, gather by the
+    open neighbours with the headroom clamp): C [S][N] densities, dC [S][N] pending increments;
+    returns the increments after both passes."""
+    nx, ny, nz = shape
+    prm = np.ascontiguousarray(prm, dtype=np.float64)
+    mat = np.ascontiguousarray(mat, dtype=np.int8)
+    stamp = np.ascontiguousarray(stamp, dtype=np.uint8)
+    C = np.ascontiguousarray(C, dtype=np.float64)
+    out = np.array(dC, dtype=np.float64, copy=True, order="C")
+    lib().orc_dissolution_increments(nx, ny, nz, S, sM, dt, law, _p(prm), int(surface_only), _p(mat), solid, bb,
+                                     _p(stamp), _p(C), _p(out))
+    return out

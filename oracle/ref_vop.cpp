@@ -1,0 +1,94 @@
+// Thin C entry points around the reference's own dissolution processors (surfaceDissolutionKinetics3D
+// and dissolutionGather3D, dissolutionVOP.hh) and node conversions (precipNodeConversion3D,
+// precipitationVOP.hh; dissolNodeConversion3D), compiled from the reference sources where they lie
+// against the minimal lattice stand-ins of palabos_shim.hh (see Makefile target `ref`).
+// TEST INFRASTRUCTURE ONLY: used to pin the oracle's restatement of these passes to the reference.
+#include "palabos_shim.hh"
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+using namespace plb;
+typedef double T;
+const T thrd = 1e-12;  // the reference's threshold (complab3d_processors.hh)
+
+// The dissolution law is the user's compile-time hook in the reference; here it is the library's
+// first-order law (params kd, h, sigma[S]) or its saturation-index law (params k, log10 Ksp, nu[S]).
+static int g_law = 0, g_sM = -1;
+static std::vector<double> g_prm;
+
+inline void defineDissolutionRate(plint, const std::vector<double>& C, double mineral, std::vector<double>& subsR,
+                                  double& mineralR, plint) {
+    const size_t S = subsR.size();
+    mineralR = 0.0;
+    for (size_t i = 0; i < S; ++i) subsR[i] = 0.0;
+    const std::vector<double>& p = g_prm;
+    if (g_law == 1) {
+        const int h = (int)p[1];
+        const double rate = p[0] * (h >= 0 ? std::max(C[(size_t)h], 0.0) : 1.0) * std::max(mineral, 0.0);
+        mineralR = -rate;
+        for (size_t j = 0; j < S; ++j) subsR[j] = p[2 + j] * rate;
+    } else if (g_law == 2) {
+        double la = 0;
+        for (size_t j = 0; j < S; ++j)
+            if ((int)j != g_sM && p[2 + j] != 0.0) la += p[2 + j] * std::log10(std::max(C[j], 1e-30));
+        const double om = std::pow(10.0, la - p[1]);
+        if (om < 1.0) {
+            mineralR = p[0] * (om - 1.0);
+            for (size_t j = 0; j < S; ++j)
+                if ((int)j != g_sM) subsR[j] = -p[2 + j] * mineralR;
+        }
+    }
+}
+
+double g_abioticRateScale = 1.0;  // the reference's global rate scale (1: no scaling)
+
+inline void defineAbioticRxnKinetics(std::vector<double>, std::vector<double>& subsR, plint) {
+    for (size_t i = 0; i < subsR.size(); ++i) subsR[i] = 0.0;
+}
+
+#include "precipitationVOP.hh"
+#include "dissolutionVOP.hh"
+
+typedef BlockLattice3D<T, D3Q7Descriptor> Lat;
+
+extern "C" int ref_dissolution_increments(int nx, int ny, int nz, int S, int sM, double dt, int law, const double* prm,
+                                          int nprm, int surface_only, const int8_t* mat, int solid, int bb,
+                                          const uint8_t* stamp, const double* C, double* dC) {
+    const size_t N = (size_t)nx * ny * nz;
+    g_law = law;
+    g_sM = sM;
+    g_prm.assign(prm, prm + nprm);
+    std::vector<Lat> lat;
+    lat.reserve((size_t)2 * S + 2);
+    for (int i = 0; i < 2 * S + 2; ++i) lat.emplace_back(nx, ny, nz);
+    for (size_t n = 0; n < N; ++n) {
+        for (int s = 0; s < S; ++s) {
+            lat[(size_t)s].cells[n].setDensity(C[(size_t)s * N + n]);
+            lat[(size_t)(S + s)].cells[n].setDensity(dC[(size_t)s * N + n]);
+        }
+        lat[(size_t)(2 * S)].cells[n].setDensity((T)mat[n]);
+        lat[(size_t)(2 * S + 1)].cells[n].setDensity(stamp[n] ? (T)1 : (T)0);
+    }
+    std::vector<Lat*> ptr;
+    for (auto& l : lat) ptr.push_back(&l);
+    DissolutionConfig cfg;
+    cfg.enabled = true;
+    cfg.surface_only = surface_only;
+    SolidPhase ph;
+    ph.id = 1;
+    ph.substrate = sM;
+    ph.full_density = 1;
+    ph.is_precipitate = true;
+    cfg.phases.push_back(ph);
+    const Box3D box{0, nx - 1, 0, ny - 1, 0, nz - 1};
+    std::vector<plint> pore{2};
+    surfaceDissolutionKinetics3D<T, D3Q7Descriptor> park(nx, ny, nz, S, dt, solid, bb, pore, &cfg);
+    park.process(box, ptr);
+    dissolutionGather3D<T, D3Q7Descriptor> gather(nx, ny, nz, S, solid, bb, &cfg);
+    gather.process(box, ptr);
+    for (int s = 0; s < S; ++s)
+        for (size_t n = 0; n < N; ++n) dC[(size_t)s * N + n] = lat[(size_t)(S + s)].cells[n].computeDensity();
+    return 0;
+}

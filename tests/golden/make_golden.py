@@ -1,7 +1,10 @@
 """Regenerates tests/golden/geometry.json from the reference's own geometry generator
-(complab3d_geometry.hh, compiled into oracle/_ref/libref_geometry.so by `make -C oracle ref`) and
+(complab3d_geometry.hh, compiled into oracle/_ref/libref_geometry.so by `make -C oracle ref`),
 tests/golden/speciation.json from the reference's own equilibrium solver (EquilibriumChemistry,
-compiled into oracle/_ref/libref_eqsolver.so with the reference's tests/palabos_stub.hh).
+compiled into oracle/_ref/libref_eqsolver.so with the reference's tests/palabos_stub.hh) and
+tests/golden/dissolution.npz from the reference's own dissolution processors
+(surfaceDissolutionKinetics3D + dissolutionGather3D of dissolutionVOP.hh, compiled into
+oracle/_ref/libref_vop.so against oracle/palabos_shim.hh) on seeded fields.
 
 Run from the repository root in a checkout that has the reference sources:
     make -C oracle ref && python tests/golden/make_golden.py
@@ -80,7 +83,43 @@ def speciation_cases():
     print(f"wrote {sum(len(c['inputs']) for c in out)} speciation cases")
 
 
+def dissolution_cases():
+    """Seeded small fields (open voxels, rock, walls; precipitated mineral voxels; some negative
+    water; pending increments) through the reference's park + gather passes, both dissolution
+    laws, with and without the surface-only rule."""
+    L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_vop.so"))
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    rng = np.random.default_rng(2024)
+    shape, S, sM = (10, 8, 7), 4, 3
+    nx, ny, nz = shape
+    N = nx * ny * nz
+    rec = {}
+    for case in range(6):
+        mat = np.where(rng.random(N) < 0.2, 0, 2).astype(np.int8)
+        mat[rng.random(N) < 0.05] = 1
+        stamp = ((mat == 0) & (rng.random(N) < 0.6)).astype(np.uint8)
+        Cf = rng.uniform(0.0, 1.0, (S, N))
+        Cf[sM] = np.where(stamp == 1, rng.uniform(0.0, 2.0, N), 0.0)
+        Cf[1] -= 0.3
+        dC0 = np.where(rng.random((S, N)) < 0.3, rng.uniform(-0.05, 0.05, (S, N)), 0.0)
+        law = 1 if case % 2 == 0 else 2
+        prm = np.array([0.7, 0 if case < 4 else -1, 1.0, -2.0, 0.5, 0.0] if law == 1
+                       else [0.3, -1.5, 1.0, 1.0, 0.0, 0.0], np.float64)
+        dt = 1.0 if case < 3 else 0.25
+        surf = int(case % 3 != 2)
+        dC = dC0.copy()
+        L.ref_dissolution_increments(nx, ny, nz, S, sM, C.c_double(dt), law, P(prm), len(prm), surf, P(mat), 0, 1,
+                                     P(stamp), P(Cf), P(dC))
+        for k, v in dict(mat=mat, stamp=stamp, C=Cf, dC0=dC0, prm=prm, dC=dC,
+                         meta=np.array([law, surf, dt, S, sM])).items():
+            rec[f"{case}_{k}"] = v
+    rec["shape"] = np.array(shape)
+    np.savez_compressed(os.path.join(os.path.dirname(os.path.abspath(__file__)), "dissolution.npz"), **rec)
+    print("wrote 6 dissolution cases")
+
+
 def main():
+    dissolution_cases()
     speciation_cases()
     L = C.CDLL(REF)
     out = []
