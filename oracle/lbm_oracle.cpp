@@ -1223,6 +1223,18 @@ void orc_ca_fields(OrcAde* A, double* total, int32_t* age) {
     std::copy(A->age.begin(), A->age.end(), age);
 }
 
+// single passes of the automaton on the current state (pinned to the reference's processors):
+// the mask and total update once; the age relaxation until no age changes (at most max_sweeps),
+// returning the number of sweeps that changed something
+void orc_ca_mask_total_once(OrcAde* A) { ca_mask_total(A); }
+int orc_ca_age_relax(OrcAde* A, int max_sweeps) {
+    int k = 0;
+    while (k < max_sweeps && ca_age_sweep(A) != 0) ++k;
+    return k;
+}
+// the age field and its open-region flags (age > -1 region of calculateDistanceFromSolid)
+void orc_ca_age_flags(OrcAde* A, int32_t* distp) { std::copy(A->distp.begin(), A->distp.end(), distp); }
+
 }  // extern "C"
 
 // =====================================================================================

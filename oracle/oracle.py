@@ -64,6 +64,8 @@ def lib():
             "orc_ca_fields": ([vp, vp, vp], None),
             "orc_flow_set_material": ([vp, vp], None),
             "orc_flow_set_dynamics": ([vp, ip, ip, dp], None),
+            "orc_ca_mask_total_once": ([vp], None), "orc_ca_age_relax": ([vp, ip], ip),
+            "orc_ca_age_flags": ([vp, vp], None),
             "orc_dissolution_increments": ([ip, ip, ip, ip, ip, dp, ip, vp, ip, vp, ip, ip, vp, vp, vp], None),
         }
         for name, (args, res) in sig.items():
@@ -254,6 +256,19 @@ class OracleAde:
         a = np.empty(self.N, dtype=np.int32)
         lib().orc_ca_fields(self.h, _p(t), _p(a))
         return t, a
+
+    def ca_mask_total_once(self):
+        """updateLocalMaskNtotalLattices3D once on the current state."""
+        lib().orc_ca_mask_total_once(self.h)
+
+    def ca_age_relax(self, max_sweeps=1000):
+        """updateAgeDistance3D until no age changes; returns the sweeps that changed something."""
+        return lib().orc_ca_age_relax(self.h, int(max_sweeps))
+
+    def ca_open_flags(self):
+        d = np.empty(self.N, dtype=np.int32)
+        lib().orc_ca_age_flags(self.h, _p(d))
+        return d
 
     def step(self, n=1):
         lib().orc_ade_step(self.h, n)

@@ -30,7 +30,7 @@ namespace BlockDomain {
 enum DomainT { bulk, bulkAndEnvelope };
 }
 namespace modif {
-enum ModifT { nothing, staticVariables, allVariables };
+enum ModifT { nothing, staticVariables, dynamicVariables, allVariables, dataStructure };
 }
 template <typename T>
 struct D3Q7Descriptor {};
@@ -51,6 +51,27 @@ struct Cell {
         f[0] = (rho - 1) / 4;
         for (int i = 1; i < 7; ++i) f[i] = (rho - 1) / 8;
     }
+};
+
+// dynamics objects: only declared so that processors which switch dynamics compile; the shim's
+// lattices never run them
+template <typename T, template <typename U> class Descriptor>
+struct Dynamics {
+    virtual ~Dynamics() {}
+    virtual T getOmega() const { return omega; }
+    T omega = 0;
+};
+template <typename T, template <typename U> class Descriptor>
+struct BounceBack : Dynamics<T, Descriptor> {
+    BounceBack() {}
+};
+template <typename T, template <typename U> class Descriptor>
+struct AdvectionDiffusionBGKdynamics : Dynamics<T, Descriptor> {
+    explicit AdvectionDiffusionBGKdynamics(T w) { this->omega = w; }
+};
+template <typename T, template <typename U> class Descriptor>
+struct IncBGKdynamics : Dynamics<T, Descriptor> {
+    explicit IncBGKdynamics(T w) { this->omega = w; }
 };
 
 template <typename T, template <typename U> class Descriptor>
@@ -78,6 +99,11 @@ template <typename T, template <typename U> class Descriptor>
 struct LatticeBoxProcessingFunctional3D {
     virtual ~LatticeBoxProcessingFunctional3D() {}
     virtual void process(Box3D, std::vector<BlockLattice3D<T, Descriptor>*>) = 0;
+};
+
+template <typename T1, template <typename U> class D1, typename T2, template <typename U> class D2>
+struct BoxProcessingFunctional3D_LL {
+    virtual ~BoxProcessingFunctional3D_LL() {}
 };
 
 template <typename T1, template <typename U> class Descriptor, typename T2>

@@ -1,11 +1,14 @@
 // Thin C entry points around the reference's own dissolution processors (surfaceDissolutionKinetics3D
-// and dissolutionGather3D, dissolutionVOP.hh) and node conversions (precipNodeConversion3D,
-// precipitationVOP.hh; dissolNodeConversion3D), compiled from the reference sources where they lie
-// against the minimal lattice stand-ins of palabos_shim.hh (see Makefile target `ref`).
-// TEST INFRASTRUCTURE ONLY: used to pin the oracle's restatement of these passes to the reference.
+// and dissolutionGather3D, dissolutionVOP.hh) and the deterministic passes of its biofilm automaton
+// (updateLocalMaskNtotalLattices3D, updateAgeDistance3D, complab3d_processors_part2.hh), compiled
+// from the reference sources where they lie against the minimal lattice stand-ins of
+// palabos_shim.hh (see Makefile target `ref`). TEST INFRASTRUCTURE ONLY: used to pin the oracle's
+// restatement of these passes to the reference.
 #include "palabos_shim.hh"
 
 #include <algorithm>
+#include <iostream>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -48,8 +51,11 @@ inline void defineAbioticRxnKinetics(std::vector<double>, std::vector<double>& s
     for (size_t i = 0; i < subsR.size(); ++i) subsR[i] = 0.0;
 }
 
+#define COMPLAB_THRD 1e-14  // complab_functions.hh
+
 #include "precipitationVOP.hh"
 #include "dissolutionVOP.hh"
+#include "complab3d_processors_part2.hh"
 
 typedef BlockLattice3D<T, D3Q7Descriptor> Lat;
 
@@ -91,4 +97,67 @@ extern "C" int ref_dissolution_increments(int nx, int ny, int nz, int S, int sM,
     for (int s = 0; s < S; ++s)
         for (size_t n = 0; n < N; ++n) dC[(size_t)s * N + n] = lat[(size_t)(S + s)].cells[n].computeDensity();
     return 0;
+}
+
+// updateLocalMaskNtotalLattices3D over the whole box: biomass bio[M][N], total[N] and mask[N]
+// (material codes) in, total and mask out.
+extern "C" int ref_ca_mask_total(int nx, int ny, int nz, int M, const double* bio, double* total, int* mask, int bb,
+                                 int solid, const int* bio_codes, int n_pore, const int* pore, double frac,
+                                 double Bmax) {
+    const size_t N = (size_t)nx * ny * nz;
+    const int len = 2 * M + 3;
+    std::vector<Lat> lat;
+    lat.reserve((size_t)len);
+    for (int i = 0; i < len; ++i) lat.emplace_back(nx, ny, nz);
+    for (size_t n = 0; n < N; ++n) {
+        for (int m = 0; m < M; ++m) {
+            lat[(size_t)m].cells[n].setDensity(bio[(size_t)m * N + n]);
+            lat[(size_t)(M + m)].cells[n].setDensity(bio[(size_t)m * N + n]);
+        }
+        lat[(size_t)(len - 3)].cells[n].setDensity(total[n]);
+        lat[(size_t)(len - 2)].cells[n].setDensity((T)mask[n]);
+        lat[(size_t)(len - 1)].cells[n].setDensity(0);
+    }
+    std::vector<Lat*> ptr;
+    for (auto& l : lat) ptr.push_back(&l);
+    std::vector<std::vector<plint>> bv;
+    for (int m = 0; m < M; ++m) bv.push_back(std::vector<plint>{bio_codes[m]});
+    std::vector<plint> pv(pore, pore + n_pore);
+    updateLocalMaskNtotalLattices3D<T, D3Q7Descriptor> f(nx, ny, nz, len, bb, solid, bv, pv, frac, Bmax);
+    f.process(Box3D{0, nx - 1, 0, ny - 1, 0, nz - 1}, ptr);
+    for (size_t n = 0; n < N; ++n) {
+        total[n] = lat[(size_t)(len - 3)].cells[n].computeDensity();
+        mask[n] = (int)util::roundToInt(lat[(size_t)(len - 2)].cells[n].computeDensity());
+    }
+    return 0;
+}
+
+// updateAgeDistance3D over the whole box, applied until no age changes (at most max_sweeps):
+// age[N] in/out, dist[N] (the distance field's sign: > 0 inside the open region), total[N].
+// Returns the number of sweeps that changed something.
+extern "C" int ref_ca_age_relax(int nx, int ny, int nz, int* age, const int* dist, const double* total, double Bmax,
+                                int max_sweeps) {
+    const size_t N = (size_t)nx * ny * nz;
+    std::vector<Lat> lat;
+    lat.reserve(3);
+    for (int i = 0; i < 3; ++i) lat.emplace_back(nx, ny, nz);
+    for (size_t n = 0; n < N; ++n) {
+        lat[0].cells[n].setDensity((T)age[n]);
+        lat[1].cells[n].setDensity((T)dist[n]);
+        lat[2].cells[n].setDensity(total[n]);
+    }
+    std::vector<Lat*> ptr{&lat[0], &lat[1], &lat[2]};
+    updateAgeDistance3D<T, D3Q7Descriptor> f(Bmax, nx, ny, nz);
+    int sweeps = 0;
+    for (; sweeps < max_sweeps; ++sweeps) {
+        std::vector<int> before(N);
+        for (size_t n = 0; n < N; ++n) before[n] = (int)util::roundToInt(lat[0].cells[n].computeDensity());
+        f.process(Box3D{0, nx - 1, 0, ny - 1, 0, nz - 1}, ptr);
+        bool changed = false;
+        for (size_t n = 0; n < N; ++n)
+            if ((int)util::roundToInt(lat[0].cells[n].computeDensity()) != before[n]) changed = true;
+        if (!changed) break;
+    }
+    for (size_t n = 0; n < N; ++n) age[n] = (int)util::roundToInt(lat[0].cells[n].computeDensity());
+    return sweeps;
 }

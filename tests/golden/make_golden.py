@@ -4,7 +4,10 @@ tests/golden/speciation.json from the reference's own equilibrium solver (Equili
 compiled into oracle/_ref/libref_eqsolver.so with the reference's tests/palabos_stub.hh) and
 tests/golden/dissolution.npz from the reference's own dissolution processors
 (surfaceDissolutionKinetics3D + dissolutionGather3D of dissolutionVOP.hh, compiled into
-oracle/_ref/libref_vop.so against oracle/palabos_shim.hh) on seeded fields.
+oracle/_ref/libref_vop.so against oracle/palabos_shim.hh) on seeded fields, and
+tests/golden/automaton.npz from the biofilm automaton's mask/total update and age relaxation
+(updateLocalMaskNtotalLattices3D and updateAgeDistance3D of complab3d_processors_part2.hh, the
+same library) on seeded maps.
 
 Run from the repository root in a checkout that has the reference sources:
     make -C oracle ref && python tests/golden/make_golden.py
@@ -118,7 +121,66 @@ def dissolution_cases():
     print("wrote 6 dissolution cases")
 
 
+def ca_cases():
+    """Seeded small maps (pore, two biofilm codes, rock, walls) with biomass at and below the
+    ceiling: the oracle's automaton set-up gives the stored totals, ages and open flags; the
+    biomass then changes and the reference's updateLocalMaskNtotalLattices3D (one pass) and
+    updateAgeDistance3D (3 sweeps, and to a fixed point or 1000 sweeps) give the expected mask,
+    totals and ages."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_vop.so"))
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    rng = np.random.default_rng(31)
+    shape = (9, 7, 6)
+    nx, ny, nz = shape
+    N = nx * ny * nz
+    Bmax, frac = 100.0, 0.3
+    codes, pores = np.array([3, 4], np.int32), np.array([2], np.int32)
+    rec = {}
+    for case in range(5):
+        mat = np.where(rng.random(N) < 0.15, 0, 2).astype(np.int8)
+        mat[rng.random(N) < 0.05] = 1
+        mat[(mat == 2) & (rng.random(N) < 0.45)] = 3
+        mat[(mat == 2) & (rng.random(N) < 0.15)] = 4
+        bio = np.zeros((2, N))
+        bio[0, mat == 3] = rng.uniform(0, Bmax, (mat == 3).sum())
+        bio[1, mat == 4] = rng.uniform(0, Bmax, (mat == 4).sum())
+        full = (mat >= 3) & (rng.random(N) < 0.5)
+        bio[0, full & (mat == 3)] = Bmax
+        bio[1, full & (mat == 4)] = Bmax
+        O = oracle.OracleAde(mat, *shape, [dict(omega_pore=1.0, c0=0.1)], np.zeros(3 * N), bio_codes=(3, 4))
+        O.set_biomass(bio)
+        O.ca_setup(Bmax, frac, 7)
+        total0, age0 = O.ca_fields()
+        flags = O.ca_open_flags()
+        bio2 = bio * rng.uniform(0.0, 1.0 if case < 3 else 1.6, bio.shape)
+        f2 = (mat >= 3) & (rng.random(N) < 0.6)
+        bio2[0, f2 & (mat == 3)] = Bmax
+        bio2[1, f2 & (mat == 4)] = Bmax
+        bio2[:, rng.random(N) < 0.1] = 0.0
+        bio2 = np.ascontiguousarray(bio2)
+        total, mask = total0.copy(), mat.astype(np.int32)
+        L.ref_ca_mask_total(nx, ny, nz, 2, P(bio2), P(total), P(mask), 1, 0, P(codes), 1, P(pores),
+                            C.c_double(frac), C.c_double(Bmax))
+        ages = {}
+        for k in (3, 1000):
+            a = age0.astype(np.int32).copy()
+            sw = L.ref_ca_age_relax(nx, ny, nz, P(a), P(flags), P(total), C.c_double(Bmax), k)
+            ages[k] = (a, sw)
+        for k, v in dict(mat=mat, bio=bio, bio2=bio2, total0=total0, age0=age0, flags=flags, total=total,
+                         mask=mask, age3=ages[3][0], age_fix=ages[1000][0],
+                         sweeps=np.array([ages[3][1], ages[1000][1]])).items():
+            rec[f"{case}_{k}"] = v
+    rec["shape"] = np.array(shape)
+    rec["prm"] = np.array([Bmax, frac])
+    np.savez_compressed(os.path.join(os.path.dirname(os.path.abspath(__file__)), "automaton.npz"), **rec)
+    print("wrote 5 automaton cases")
+
+
 def main():
+    ca_cases()
     dissolution_cases()
     speciation_cases()
     L = C.CDLL(REF)
