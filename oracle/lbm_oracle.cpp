@@ -656,6 +656,76 @@ static void dissolution_park_gather(int nx, int ny, int nz, int S, int sM, doubl
 }
 }  // extern "C++"
 
+/* One voxel of run_kinetics (complab3d_processors_part1.hh:85-187): concentrations and biomass
+ * below the threshold read as zero, the rate law, increments R dt whose magnitude exceeds the
+ * threshold, clamped so that no concentration or biomass goes below zero: dC = max(R dt, -C).
+ * C and B are read and thresholded in place; dC / dB receive the increments (0 where none). */
+static void biotic_voxel(const OrcAde* A, double* C, double* B, double* R, double* RB, double* dC, double* dB) {
+    const int S = A->S;
+    for (int s = 0; s < S; ++s)
+        if (C[s] < THRD) C[s] = 0;
+    for (int m = 0; m < A->M; ++m)
+        if (B[m] < THRD) B[m] = 0;
+    rates(A, C, B, R, RB);
+    for (int s = 0; s < S; ++s) {
+        double d = R[s] * A->dt;
+        dC[s] = 0.0;
+        if (!(d > THRD || d < -THRD)) continue;
+        if (d + C[s] < 0.0) d = -C[s];
+        if (!(d > THRD || d < -THRD)) continue;
+        dC[s] = d;
+    }
+    for (int m = 0; m < A->M; ++m) {
+        double d = RB[m] * A->dt;
+        dB[m] = 0.0;
+        if (!(d > THRD || d < -THRD)) continue;
+        if (d + B[m] < 0.0) d = -B[m];
+        dB[m] = d;
+    }
+}
+
+/* The abiotic rate pass (run_abiotic_kinetics, complab3d_processors_part1.hh:199-297, or with the
+ * surface-only rule surfaceAbioticKinetics3D, precipitationVOP.hh:53-153) over the interior
+ * x-planes: increments R dt of magnitude above the threshold, clamped at -C, added into dC. */
+extern "C++" {
+template <class Dens>
+static void abiotic_rate_pass(const OrcAde* A, Dens dens, double* dC) {
+    const int nx = A->nx, ny = A->ny, nz = A->nz, S = A->S;
+    const size_t N = A->N;
+    auto inbox = [&](int x, int y, int z) { return x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz; };
+#pragma omp parallel for schedule(static)
+    for (int x = 1; x < nx - 1; ++x) {
+        std::vector<double> C(S), R(S);
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                size_t n = A->id(x, y, z);
+                if (!A->react[(uint8_t)A->mat[n]]) continue;
+                if (A->surf) {
+                    bool iface = false;
+                    for (int d = 0; d < 6 && !iface; ++d) {
+                        int X = x + DLOC[d][0], Y = y + DLOC[d][1], Z = z + DLOC[d][2];
+                        if (!inbox(X, Y, Z)) continue;
+                        if (!A->react[(uint8_t)A->mat[A->id(X, Y, Z)]]) iface = true;
+                    }
+                    if (!iface) continue;
+                }
+                for (int s2 = 0; s2 < S; ++s2) {
+                    double c = dens(s2, n);
+                    C[s2] = c < THRD ? 0.0 : c;
+                }
+                rates2(A, C.data(), R.data());
+                for (int s2 = 0; s2 < S; ++s2) {
+                    double d = R[s2] * A->dt;
+                    if (!(d > THRD || d < -THRD)) continue;
+                    if (d + C[s2] < 0.0) d = -C[s2];
+                    if (!(d > THRD || d < -THRD)) continue;
+                    dC[(size_t)s2 * N + n] += d;
+                }
+            }
+    }
+}
+}  // extern "C++"
+
 /* The abiotic block of complab.cpp:2460-2525 after the biotic increments are applied: abiotic
  * rates (with the clamp dC = max(R dt, -C)), dissolution of sealed mineral voxels parked per open
  * face (surfaceDissolutionKinetics3D, dissolutionVOP.hh:379-605), gathered by the open neighbours
@@ -665,39 +735,8 @@ static void abiotic_block(OrcAde* A) {
     const int nx = A->nx, ny = A->ny, nz = A->nz, S = A->S;
     const size_t N = A->N;
     std::vector<double> dC((size_t)S * N, 0.0);
-    auto inbox = [&](int x, int y, int z) { return x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz; };
-    if (A->law2 != LAW_NONE) {
-#pragma omp parallel for schedule(static)
-        for (int x = 1; x < nx - 1; ++x) {
-            std::vector<double> C(S), R(S);
-            for (int y = 0; y < ny; ++y)
-                for (int z = 0; z < nz; ++z) {
-                    size_t n = A->id(x, y, z);
-                    if (!A->react[(uint8_t)A->mat[n]]) continue;
-                    if (A->surf) {
-                        bool iface = false;
-                        for (int d = 0; d < 6 && !iface; ++d) {
-                            int X = x + DLOC[d][0], Y = y + DLOC[d][1], Z = z + DLOC[d][2];
-                            if (!inbox(X, Y, Z)) continue;
-                            if (!A->react[(uint8_t)A->mat[A->id(X, Y, Z)]]) iface = true;
-                        }
-                        if (!iface) continue;
-                    }
-                    for (int s2 = 0; s2 < S; ++s2) {
-                        double c = dens_post(A, s2, n);
-                        C[s2] = c < THRD ? 0.0 : c;
-                    }
-                    rates2(A, C.data(), R.data());
-                    for (int s2 = 0; s2 < S; ++s2) {
-                        double d = R[s2] * A->dt;
-                        if (!(d > THRD || d < -THRD)) continue;
-                        if (d + C[s2] < 0.0) d = -C[s2];
-                        if (!(d > THRD || d < -THRD)) continue;
-                        dC[(size_t)s2 * N + n] += d;
-                    }
-                }
-        }
-    }
+    if (A->law2 != LAW_NONE)
+        abiotic_rate_pass(A, [&](int s2, size_t n) { return dens_post(A, s2, n); }, dC.data());
     if (A->dis_on && A->sM >= 0) {
         const DissolLaw L{A->dis_law, S, A->sM, A->dprm.data()};
         dissolution_park_gather(
@@ -770,46 +809,23 @@ static void ade_step(OrcAde* A) {
     if (A->law != LAW_NONE) {
 #pragma omp parallel for schedule(static)
         for (int x = 1; x < nx - 1; ++x) {
-            std::vector<double> C(S), R(S), B(A->M + 1), RB(A->M + 1);
+            std::vector<double> C(S), R(S), B(A->M + 1), RB(A->M + 1), dC(S), dB(A->M + 1);
             for (int y = 0; y < ny; ++y)
                 for (int z = 0; z < nz; ++z) {
                     size_t n = A->id(x, y, z);
                     if (!A->react[(uint8_t)A->mat[n]]) continue;
+                    for (int s = 0; s < S; ++s) C[s] = dens_post(A, s, n);
+                    for (int m = 0; m < A->M; ++m) B[m] = A->bio[(size_t)m * N + n];
+                    biotic_voxel(A, C.data(), B.data(), R.data(), RB.data(), dC.data(), dB.data());
                     for (int s = 0; s < S; ++s) {
-                        double c;
+                        if (dC[s] == 0.0) continue;
                         if (A->mobile[s]) {
-                            c = 0;
-                            for (int i = 0; i < Q7; ++i) c += A->gp[s][n * Q7 + i];
-                            c += 1.0;
+                            for (int i = 0; i < Q7; ++i) A->gp[s][n * Q7 + i] += dC[s] * T7[i];
                         } else {
-                            c = A->imm[s][n];
-                        }
-                        if (c < THRD) c = 0;
-                        C[s] = c;
-                    }
-                    for (int m = 0; m < A->M; ++m) {
-                        double b = A->bio[(size_t)m * N + n];
-                        if (b < THRD) b = 0;
-                        B[m] = b;
-                    }
-                    rates(A, C.data(), B.data(), R.data(), RB.data());
-                    for (int s = 0; s < S; ++s) {
-                        double dC = R[s] * A->dt;
-                        if (!(dC > THRD || dC < -THRD)) continue;
-                        if (dC + C[s] < 0.0) dC = -C[s];
-                        if (!(dC > THRD || dC < -THRD)) continue;
-                        if (A->mobile[s]) {
-                            for (int i = 0; i < Q7; ++i) A->gp[s][n * Q7 + i] += dC * T7[i];
-                        } else {
-                            A->imm[s][n] += dC;
+                            A->imm[s][n] += dC[s];
                         }
                     }
-                    for (int m = 0; m < A->M; ++m) {
-                        double dB = RB[m] * A->dt;
-                        if (!(dB > THRD || dB < -THRD)) continue;
-                        if (dB + B[m] < 0.0) dB = -B[m];
-                        A->bio[(size_t)m * N + n] += dB;
-                    }
+                    for (int m = 0; m < A->M; ++m) A->bio[(size_t)m * N + n] += dB[m];
                 }
         }
     }
@@ -948,6 +964,34 @@ void orc_ade_geometry_update(OrcAde* A, int* sealed, int* reopened) {
                 }
     *sealed = ns;
     *reopened = nr;
+}
+
+/* One kinetics pass on given fields, without applying it (the increments run_kinetics and
+ * run_abiotic_kinetics / surfaceAbioticKinetics3D leave in their dC / dB lattices, with the clamp):
+ * C is [S][N] (post-collision densities), B is [M][N]; dC, dB receive [S][N], [M][N]. */
+void orc_biotic_increments(OrcAde* A, const double* Cin, const double* Bin, double* dCout, double* dBout) {
+    const int S = A->S, M = A->M;
+    const size_t N = A->N;
+    std::fill(dCout, dCout + (size_t)S * N, 0.0);
+    std::fill(dBout, dBout + (size_t)M * N, 0.0);
+    std::vector<double> C(S), R(S), B(M + 1), RB(M + 1), dC(S), dB(M + 1);
+    for (int x = 1; x < A->nx - 1; ++x)
+        for (int y = 0; y < A->ny; ++y)
+            for (int z = 0; z < A->nz; ++z) {
+                size_t n = A->id(x, y, z);
+                if (!A->react[(uint8_t)A->mat[n]]) continue;
+                for (int s = 0; s < S; ++s) C[s] = Cin[(size_t)s * N + n];
+                for (int m = 0; m < M; ++m) B[m] = Bin[(size_t)m * N + n];
+                biotic_voxel(A, C.data(), B.data(), R.data(), RB.data(), dC.data(), dB.data());
+                for (int s = 0; s < S; ++s) dCout[(size_t)s * N + n] = dC[s];
+                for (int m = 0; m < M; ++m) dBout[(size_t)m * N + n] = dB[m];
+            }
+}
+
+void orc_abiotic_increments(OrcAde* A, const double* Cin, double* dCout) {
+    const size_t N = A->N;
+    std::fill(dCout, dCout + (size_t)A->S * N, 0.0);
+    abiotic_rate_pass(A, [&](int s, size_t n) { return Cin[(size_t)s * N + n]; }, dCout);
 }
 
 void orc_ade_material(OrcAde* A, int8_t* out) { std::copy(A->mat.begin(), A->mat.end(), out); }

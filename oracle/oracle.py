@@ -64,6 +64,7 @@ def lib():
             "orc_ca_fields": ([vp, vp, vp], None),
             "orc_flow_set_material": ([vp, vp], None),
             "orc_flow_set_dynamics": ([vp, ip, ip, dp], None),
+            "orc_biotic_increments": ([vp, vp, vp, vp, vp], None), "orc_abiotic_increments": ([vp, vp, vp], None),
             "orc_ca_mask_total_once": ([vp], None), "orc_ca_age_relax": ([vp, ip], ip),
             "orc_ca_age_flags": ([vp, vp], None),
             "orc_dissolution_increments": ([ip, ip, ip, ip, ip, dp, ip, vp, ip, vp, ip, ip, vp, vp, vp], None),
@@ -256,6 +257,21 @@ class OracleAde:
         a = np.empty(self.N, dtype=np.int32)
         lib().orc_ca_fields(self.h, _p(t), _p(a))
         return t, a
+
+    def biotic_increments(self, C, B):
+        """run_kinetics on given densities C [S][N] and biomass B [M][N]: the clamped increments."""
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        B = np.ascontiguousarray(B, dtype=np.float64).reshape(-1, self.N)
+        dC, dB = np.empty_like(C), np.empty((B.shape[0], self.N))
+        lib().orc_biotic_increments(self.h, _p(C), _p(B), _p(dC), _p(dB))
+        return dC, dB
+
+    def abiotic_increments(self, C):
+        """run_abiotic_kinetics (or the surface-only pass) on given densities C [S][N]."""
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        dC = np.empty_like(C)
+        lib().orc_abiotic_increments(self.h, _p(C), _p(dC))
+        return dC
 
     def ca_mask_total_once(self):
         """updateLocalMaskNtotalLattices3D once on the current state."""

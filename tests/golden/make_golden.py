@@ -5,7 +5,10 @@ compiled into oracle/_ref/libref_eqsolver.so with the reference's tests/palabos_
 tests/golden/dissolution.npz from the reference's own dissolution processors
 (surfaceDissolutionKinetics3D + dissolutionGather3D of dissolutionVOP.hh, compiled into
 oracle/_ref/libref_vop.so against oracle/palabos_shim.hh) on seeded fields, and
-tests/golden/automaton.npz from the biofilm automaton's mask/total update and age relaxation
+tests/golden/kinetics.npz from the reference's kinetics processors (run_kinetics,
+run_abiotic_kinetics of complab3d_processors_part1.hh and surfaceAbioticKinetics3D, compiled into
+oracle/_ref/libref_kinetics.so with the FeS law of examples/15), tests/golden/automaton.npz from
+the biofilm automaton's mask/total update and age relaxation
 (updateLocalMaskNtotalLattices3D and updateAgeDistance3D of complab3d_processors_part2.hh, the
 same library) on seeded maps.
 
@@ -179,7 +182,61 @@ def ca_cases():
     print("wrote 5 automaton cases")
 
 
+def kinetics_cases():
+    """Seeded small fields (rock, walls, pore, biofilm; concentrations with sub-threshold and
+    negative entries) through the reference's run_kinetics with the library's decay, Monod and
+    dual-Monod laws, and through its run_abiotic_kinetics / surfaceAbioticKinetics3D with the FeS
+    precipitation law of examples/15. Some cases have rates that overdraw a voxel, where the
+    reference's increment goes below -C."""
+    L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_kinetics.so"))
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    rng = np.random.default_rng(77)
+    shape = (10, 8, 7)
+    nx, ny, nz = shape
+    N = nx * ny * nz
+
+    def conc(S, scale):
+        c = rng.uniform(0, scale, (S, N))
+        c[rng.random((S, N)) < 0.05] = 1e-13
+        c[rng.random((S, N)) < 0.05] *= -0.1
+        return c
+
+    rec = {}
+    biotic = ((1, [1e-3, 0.5, 2.0], 0, 1.0, 1.0), (2, [0.3, 0.02, 0.1, 0.5, 0.1, 1e-3], 0, 1.0, 1.0),
+              (3, [0.5, 0.2, 0.4, 0.01], 2, 1.0, 1.0), (3, [5.0, 0.2, 0.4, 0.01], 2, 0.5, 0.3))
+    for case, (law, prm, M, dt, scale) in enumerate(biotic):
+        S = 3
+        mat = np.where(rng.random(N) < 0.2, 0, 2).astype(np.int8)
+        mat[rng.random(N) < 0.05] = 1
+        mat[(mat == 2) & (rng.random(N) < 0.3)] = 3
+        Cf = conc(S, scale)
+        B = rng.uniform(0, 2, (M, N))
+        B[:, rng.random(N) < 0.1] = 0.0
+        prm = np.array(prm, np.float64)
+        dC, dB = np.zeros((S, N)), np.zeros((max(M, 1), N))
+        L.ref_biotic_increments(nx, ny, nz, S, M, C.c_double(dt), law, P(prm), len(prm), P(mat), 0, 1, P(Cf),
+                                P(B if M else dB), P(dC), P(dB))
+        for k, v in dict(mat=mat, C=Cf, B=B, prm=prm, dC=dC, dB=dB[:M], meta=np.array([law, M, dt])).items():
+            rec[f"b{case}_{k}"] = v
+    case = 0
+    for surf in (0, 1):
+        for dt, scale in ((1.0, 0.9), (1.0, 2.0), (0.25, 1.0)):
+            S = 4
+            mat = np.where(rng.random(N) < 0.25, 0, 2).astype(np.int8)
+            mat[rng.random(N) < 0.05] = 1
+            Cf = conc(S, scale)
+            dC = np.zeros((S, N))
+            L.ref_abiotic_increments(nx, ny, nz, S, C.c_double(dt), surf, P(mat), 0, 1, P(Cf), P(dC))
+            for k, v in dict(mat=mat, C=Cf, dC=dC, meta=np.array([surf, dt])).items():
+                rec[f"a{case}_{k}"] = v
+            case += 1
+    rec["shape"] = np.array(shape)
+    np.savez_compressed(os.path.join(os.path.dirname(os.path.abspath(__file__)), "kinetics.npz"), **rec)
+    print("wrote 4 biotic and 6 abiotic kinetics cases")
+
+
 def main():
+    kinetics_cases()
     ca_cases()
     dissolution_cases()
     speciation_cases()
