@@ -994,6 +994,11 @@ void orc_abiotic_increments(OrcAde* A, const double* Cin, double* dCout) {
     abiotic_rate_pass(A, [&](int s, size_t n) { return Cin[(size_t)s * N + n]; }, dCout);
 }
 
+// an immobile species' field and the precipitate stamps, as the conversions read them
+void orc_ade_set_immobile(OrcAde* A, int s, const double* c) { A->imm[s].assign(c, c + A->N); }
+void orc_ade_set_stamp(OrcAde* A, const uint8_t* st) { A->stamp.assign(st, st + A->N); }
+void orc_ade_stamp(OrcAde* A, uint8_t* out) { std::copy(A->stamp.begin(), A->stamp.end(), out); }
+
 void orc_ade_material(OrcAde* A, int8_t* out) { std::copy(A->mat.begin(), A->mat.end(), out); }
 
 // ---------------------------------------------------------------- biofilm cellular automaton

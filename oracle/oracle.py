@@ -65,6 +65,8 @@ def lib():
             "orc_flow_set_material": ([vp, vp], None),
             "orc_flow_set_dynamics": ([vp, ip, ip, dp], None),
             "orc_biotic_increments": ([vp, vp, vp, vp, vp], None), "orc_abiotic_increments": ([vp, vp, vp], None),
+            "orc_ade_set_immobile": ([vp, ip, vp], None), "orc_ade_set_stamp": ([vp, vp], None),
+            "orc_ade_stamp": ([vp, vp], None),
             "orc_ca_mask_total_once": ([vp], None), "orc_ca_age_relax": ([vp, ip], ip),
             "orc_ca_age_flags": ([vp, vp], None),
             "orc_dissolution_increments": ([ip, ip, ip, ip, ip, dp, ip, vp, ip, vp, ip, ip, vp, vp, vp], None),
@@ -227,6 +229,19 @@ class OracleAde:
         self._dprm = d
         lib().orc_ade_set_precip(self.h, int(mineral), float(full), int(precip_code), int(dissolution),
                                  float(reopen), int(pore_code), int(dis_law), _p(d), d.size, int(dis_surface_only))
+
+    def set_immobile(self, s, c):
+        c = np.ascontiguousarray(c, dtype=np.float64).reshape(-1)
+        lib().orc_ade_set_immobile(self.h, int(s), _p(c))
+
+    def set_stamp(self, st):
+        st = np.ascontiguousarray(st, dtype=np.uint8).reshape(-1)
+        lib().orc_ade_set_stamp(self.h, _p(st))
+
+    def stamp(self):
+        out = np.empty(self.N, dtype=np.uint8)
+        lib().orc_ade_stamp(self.h, _p(out))
+        return out
 
     def geometry_update(self):
         a, b = C.c_int(), C.c_int()

@@ -161,3 +161,49 @@ extern "C" int ref_ca_age_relax(int nx, int ny, int nz, int* age, const int* dis
     for (size_t n = 0; n < N; ++n) age[n] = (int)util::roundToInt(lat[0].cells[n].computeDensity());
     return sweeps;
 }
+
+/* precipNodeConversion3D over Box3D(1, nx-2, 0, ny-1, 0, nz-1) (complab.cpp:3139-3146) with
+ * lattices [mineral, mask, phase] and the precipitate's phase id 1, then, when dissolution is on,
+ * dissolNodeConversion3D over the same box with lattices [S substrates, mask, phase] and one
+ * declared phase (id 1, the precipitate: material precip_code, substrate sM, full density full).
+ * mat and phase (0 or 1 per voxel) are updated in place. */
+extern "C" void ref_node_conversion(int nx, int ny, int nz, int S, int sM, double full, double reopen,
+                                    int precip_code, int pore_code, int solid, int bb, int dissolution,
+                                    const double* C, int8_t* mat, uint8_t* phase) {
+    const size_t N = (size_t)nx * ny * nz;
+    std::vector<Lat> L;
+    L.reserve(S + 2);
+    for (int i = 0; i < S + 2; ++i) L.emplace_back(nx, ny, nz);
+    for (int s = 0; s < S; ++s)
+        for (size_t n = 0; n < N; ++n) L[s].cells[n].setDensity(C[(size_t)s * N + n]);
+    for (size_t n = 0; n < N; ++n) {
+        L[S].cells[n].setDensity((T)mat[n]);
+        L[S + 1].cells[n].setDensity((T)phase[n]);
+    }
+    const Box3D box{1, nx - 2, 0, ny - 1, 0, nz - 1};
+    {
+        std::vector<Lat*> ptr{&L[sM], &L[S], &L[S + 1]};
+        precipNodeConversion3D<T, D3Q7Descriptor> f(nx, ny, nz, full, solid, bb, precip_code, dissolution ? 1 : 0);
+        f.process(box, ptr);
+    }
+    if (dissolution) {
+        DissolutionConfig cfg;
+        cfg.enabled = true;
+        cfg.reopen_fraction = reopen;
+        SolidPhase ph;
+        ph.id = 1;
+        ph.material_number = precip_code;
+        ph.substrate = sM;
+        ph.full_density = full;
+        ph.is_precipitate = true;
+        cfg.phases.push_back(ph);
+        std::vector<Lat*> ptr;
+        for (auto& l : L) ptr.push_back(&l);
+        dissolNodeConversion3D<T, D3Q7Descriptor> f(S, pore_code, solid, bb, &cfg);
+        f.process(box, ptr);
+    }
+    for (size_t n = 0; n < N; ++n) {
+        mat[n] = (int8_t)util::roundToInt(L[S].cells[n].computeDensity());
+        phase[n] = (uint8_t)util::roundToInt(L[S + 1].cells[n].computeDensity());
+    }
+}

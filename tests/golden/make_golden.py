@@ -5,7 +5,9 @@ compiled into oracle/_ref/libref_eqsolver.so with the reference's tests/palabos_
 tests/golden/dissolution.npz from the reference's own dissolution processors
 (surfaceDissolutionKinetics3D + dissolutionGather3D of dissolutionVOP.hh, compiled into
 oracle/_ref/libref_vop.so against oracle/palabos_shim.hh) on seeded fields, and
-tests/golden/kinetics.npz from the reference's kinetics processors (run_kinetics,
+tests/golden/conversion.npz from the reference's node conversions (precipNodeConversion3D,
+dissolNodeConversion3D, the same library), tests/golden/kinetics.npz from the reference's
+kinetics processors (run_kinetics,
 run_abiotic_kinetics of complab3d_processors_part1.hh and surfaceAbioticKinetics3D, compiled into
 oracle/_ref/libref_kinetics.so with the FeS law of examples/15), tests/golden/automaton.npz from
 the biofilm automaton's mask/total update and age relaxation
@@ -235,7 +237,45 @@ def kinetics_cases():
     print("wrote 4 biotic and 6 abiotic kinetics cases")
 
 
+def conversion_cases():
+    """Seeded small maps with mineral fields at, above and below the sealing density, and stamped
+    (previously sealed) voxels above and below the reopening density, through the reference's
+    precipNodeConversion3D and, with dissolution on, dissolNodeConversion3D; the precipitate
+    code is the solid code or a code of its own."""
+    L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_vop.so"))
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    rng = np.random.default_rng(8)
+    shape, S, sM, full, reopen = (10, 8, 7), 3, 2, 2.0, 0.9
+    nx, ny, nz = shape
+    N = nx * ny * nz
+    rec = {}
+    for case in range(6):
+        pcode = 0 if case < 4 else 5
+        dis = int(case % 2 == 0)
+        mat = np.where(rng.random(N) < 0.2, 0, 2).astype(np.int8)
+        mat[rng.random(N) < 0.05] = 1
+        mat[(mat == 2) & (rng.random(N) < 0.3)] = 3
+        if pcode == 5:
+            mat[(mat == 0) & (rng.random(N) < 0.3)] = 5
+        stamp = ((mat == pcode) & (rng.random(N) < 0.5)).astype(np.uint8)
+        Cf = rng.uniform(0, 1, (S, N))
+        Cf[sM] = rng.uniform(0, 2.5, N)
+        Cf[sM, stamp == 1] = rng.uniform(1.5, 2.1, int((stamp == 1).sum()))
+        Cf[sM, rng.random(N) < 0.03] = full  # exactly at the sealing density
+        m, st = mat.copy(), stamp.copy()
+        L.ref_node_conversion(nx, ny, nz, S, sM, C.c_double(full), C.c_double(reopen), pcode, 2, 0, 1, dis,
+                              P(Cf), P(m), P(st))
+        for k, v in dict(mat=mat, stamp=stamp, C=Cf, mat_out=m, stamp_out=st,
+                         meta=np.array([pcode, dis])).items():
+            rec[f"{case}_{k}"] = v
+    rec["shape"] = np.array(shape)
+    rec["prm"] = np.array([S, sM, full, reopen])
+    np.savez_compressed(os.path.join(os.path.dirname(os.path.abspath(__file__)), "conversion.npz"), **rec)
+    print("wrote 6 node conversion cases")
+
+
 def main():
+    conversion_cases()
     kinetics_cases()
     ca_cases()
     dissolution_cases()
