@@ -1,6 +1,6 @@
 #!/usr/bin/env python
-"""Throughput of the D3Q19 flow step on the 256x128x128 overlapping-sphere pack (BASELINE
-config 2: porosity 0.35, grain radius U[3, 8], tau 0.7), FP32 populations, one GPU per rank.
+"""Throughput of the D3Q19 flow step on the 256x128x128 overlapping-sphere pack (porosity 0.35,
+grain radius U[3, 8], tau 0.7), FP32 populations, one GPU per rank.
 
 A step is one collide-and-stream of the whole lattice (one launch of the AA kernel). MLUPS
 counts open (collide) voxels; the all-voxel figure is reported alongside. Only the collide/stream nodes
@@ -235,7 +235,7 @@ def timed_steps(torch, stream, step, steps, warmup):
 def bench_d3q7(clb, workloads, torch, local, peak, steps=60, warmup=5, scale=1.0):
     """Fused transport of the 256^3 sphere pack with 8 species and 2 biofilm microbes (dual Monod),
     FP32 populations; the lattice (1.5 GB) is far larger than L2, so no flush is needed."""
-    cfg = workloads.config3(scale=scale)
+    cfg = workloads.pack256cube_8species(scale=scale)
     nx, ny, nz = cfg["shape"]
     mat = cfg["mat"]
     D = clb.Domain(mat, nx, ny, nz, cfg["tau"], flow_precision=clb.F32, ade_precision=clb.F32,
@@ -269,7 +269,7 @@ def bench_precision(clb, workloads, torch, local, steps=300, warmup=20):
     pack (flow to 1e-6, 2000 steps of decaying solute), each against the FP64 GPU path, which
     matches the FP64 oracle to 1e-12."""
     out = {}
-    cfg = workloads.config2()
+    cfg = workloads.pack256x128x128()
     nx, ny, nz = cfg["shape"]
     ref_u = ref_k = None
     for name, prec in (("f64", clb.F64), ("f32", clb.F32), ("f16s", clb.F16S)):
@@ -294,7 +294,7 @@ def bench_precision(clb, workloads, torch, local, steps=300, warmup=20):
         D.close()
     out["f32"]["speedup_vs_f64"] = out["f32"]["flow_mlups"] / out["f64"]["flow_mlups"]
     out["f16s"]["speedup_vs_f64"] = out["f16s"]["flow_mlups"] / out["f64"]["flow_mlups"]
-    c1 = workloads.config1()
+    c1 = workloads.pack64x32x32_decay()
     nx, ny, nz = c1["shape"]
     ref_c = None
     for name, prec in (("f64", clb.F64), ("f32", clb.F32), ("f16s", clb.F16S)):
@@ -309,10 +309,10 @@ def bench_precision(clb, workloads, torch, local, steps=300, warmup=20):
         u = D.velocity()
         if ref_c is None:
             ref_c, ref_u1 = c, u
-            out[name]["config1_flow_iterations"] = it
+            out[name]["pack64_flow_iterations"] = it
         else:
-            out[name]["config1_concentration_rel_l2_vs_f64"] = float(np.linalg.norm(c - ref_c) / np.linalg.norm(ref_c))
-            out[name]["config1_velocity_rel_l2_vs_f64"] = float(np.linalg.norm(u - ref_u1) / np.linalg.norm(ref_u1))
+            out[name]["pack64_concentration_rel_l2_vs_f64"] = float(np.linalg.norm(c - ref_c) / np.linalg.norm(ref_c))
+            out[name]["pack64_velocity_rel_l2_vs_f64"] = float(np.linalg.norm(u - ref_u1) / np.linalg.norm(ref_u1))
         D.close()
     return out
 
@@ -384,7 +384,7 @@ def bench_ensemble(clb, workloads, torch, local, steps=200):
     flow and 3 D3Q7 species with Monod kinetics, advanced by the batched steps (one launch per
     lattice and step for all domains, pairs of steps replayed from a CUDA graph) after the
     batch autotuner, against the same domains stepped one after another."""
-    cfg = workloads.config5()
+    cfg = workloads.ensemble_uneven_packs()
     doms = []
     for d in cfg["domains"]:
         nx, ny, nz = d["shape"]
@@ -431,7 +431,7 @@ def main():
     import workloads
 
     if a.impl == "reference":
-        run_reference(a, workloads.config2(scale=a.scale))
+        run_reference(a, workloads.pack256x128x128(scale=a.scale))
         return
 
     import torch
@@ -445,7 +445,7 @@ def main():
               "ensemble": lambda: bench_ensemble(clb, workloads, torch, local)}[a.leg]
         print(json.dumps({"leg": a.leg, "scale": a.scale, a.leg: fn()}))
         return
-    cfg = workloads.config2(scale=a.scale)
+    cfg = workloads.pack256x128x128(scale=a.scale)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -507,7 +507,7 @@ def main():
     alg = 2 * 19 * es * n_open
     peak, peak_kind = peaks()
     achieved = alg / (per_step * 1e-3) / 1e9
-    key = f"k_flow_aa_{a.precision}_config2"
+    key = f"k_flow_aa_{a.precision}_pack256x128x128"
     tr = traffic_per_launch(key)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": tr, "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg,

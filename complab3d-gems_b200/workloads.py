@@ -36,7 +36,7 @@ def sphere_pack_domain(nx_inner, ny, nz, porosity, rmin, rmax, seed, walls="yz")
     return add_ghost_planes(inner, nx_inner, ny, nz), (nx_inner + 2, ny, nz)
 
 
-def config1(scale=1):
+def pack64x32x32_decay(scale=1):
     """64x32x32 sphere pack (r = 4, porosity 0.40, walls on the four side faces), tau 0.8,
     dP 1e-4, one solute D_pore 0.1 / D_biofilm 0.05, C = 1 Dirichlet inlet, Neumann outlet,
     first-order decay k = 1e-3 per step, clamped. `scale` < 1 shrinks the box for quick tests."""
@@ -49,7 +49,7 @@ def config1(scale=1):
                 ade_steps=2000)
 
 
-def config2(scale=1):
+def pack256x128x128(scale=1):
     """256x128x128 overlapping-sphere pack (porosity 0.35, r ~ U[3, 8]), flow only, tau 0.7,
     Peclet rescale (Pe 10, L 8), residual 1e-7."""
     nxi, ny, nz = max(8, int(256 * scale)), max(8, int(128 * scale)), max(8, int(128 * scale))
@@ -58,7 +58,7 @@ def config2(scale=1):
                 eps=1e-7, peclet=10.0, char_length=8.0, tau_ade_fixed=0.8)
 
 
-def config3(scale=1, seed=1003):
+def pack256cube_8species(scale=1, seed=1003):
     """256^3 sphere pack (porosity 0.40), 8 species with D_pore ~ U[0.02, 0.2] and
     D_biofilm = D_pore / 2, two microbes (materials 3 and 4) seeded on 2 % of pore voxels,
     dual-Monod kinetics mu_max 1e-4, Ks 0.1, Y 0.4, decay 1e-6."""
@@ -88,7 +88,7 @@ def config3(scale=1, seed=1003):
                 bmax=100.0)
 
 
-def config5(n_domains=96, seed=1005, scale=1.0):
+def ensemble_uneven_packs(n_domains=96, seed=1005, scale=1.0):
     """Ensemble sweep: n_domains independent sphere packs of uneven sizes (inner nx in
     {32, 48, 64, 96}, ny = nz in {24, 32, 48}, drawn from the seeded stream), porosity U[0.3, 0.5],
     grain radius U[2, 4], flow tau U[0.6, 1.0] at pressure drop 1e-4, three species with D_pore

@@ -1,8 +1,8 @@
 /* lbm_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
  *
  * An FP64 CPU restatement of CompLaB3D's coupled reactive-transport step (flow lattice,
- * per-species advection-diffusion lattices, kinetics increments), used only as the parity
- * checker by tests/, by __graft_entry__.smoke(), and as the timed CPU baseline by bench.py.
+ * per-species advection-diffusion lattices, kinetics increments), used only to check parity
+ * in tests/ and __graft_entry__.smoke(), and as the timed CPU baseline by bench.py.
  * It is never linked into, called by, or shipped with the product library.
  *
  * The LBM arithmetic itself lives in Palabos 2.3.0 (not vendored with the reference). What

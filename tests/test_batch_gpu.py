@@ -32,7 +32,7 @@ def assert_same(A, B):
 
 @pytest.mark.parametrize("prec", ["F64", "F32"])
 def test_batch_matches_single_domains(clb, prec):
-    cfg = workloads.config5(n_domains=7, seed=11, scale=0.5)
+    cfg = workloads.ensemble_uneven_packs(n_domains=7, seed=11, scale=0.5)
     p = getattr(clb, prec)
     A = build(clb, cfg, p)
     B = build(clb, cfg, p)
@@ -51,7 +51,7 @@ def test_batch_matches_single_domains(clb, prec):
 
 
 def test_batch_autotune_then_matches(clb):
-    cfg = workloads.config5(n_domains=5, seed=12, scale=0.5)
+    cfg = workloads.ensemble_uneven_packs(n_domains=5, seed=12, scale=0.5)
     A = build(clb, cfg, clb.F32)
     B = build(clb, cfg, clb.F32)
     batch = clb.Batch(B)
@@ -72,7 +72,7 @@ def test_batch_autotune_then_matches(clb):
 
 
 def test_batch_rejects_mixed_parity(clb):
-    cfg = workloads.config5(n_domains=2, seed=13, scale=0.5)
+    cfg = workloads.ensemble_uneven_packs(n_domains=2, seed=13, scale=0.5)
     B = build(clb, cfg, clb.F32)
     B[1].ade_step(1)
     batch = clb.Batch(B)
