@@ -367,6 +367,12 @@ struct OrcAde {
     std::vector<double> lstore, rstore;     // stored boundary densities [S][ny*nz]
     int law = LAW_NONE;
     std::vector<double> prm;
+    // thermodynamic gate of the biotic rates (complab3d_thermo.hh; one reaction block)
+    int gate_on = 0;
+    std::vector<int> gate_sp;
+    std::vector<double> gate_nu;
+    double gate_dG0 = 0, gate_atp = 0, gate_dGatp = 50, gate_chi = 1, gate_cmin = 1e-9, gate_dGloss = 0;
+    double gate_T = 298.15, gate_R = 8.314462618e-3, gate_cscale = 1;
     double dt = 1.0;
     long iters = 0;
     void* spec = nullptr;  // EqTableau of the speciation step, or none
@@ -461,6 +467,19 @@ void orc_ade_set_kinetics(OrcAde* A, int law, const double* prm, int nprm, doubl
     A->prm.assign(prm, prm + nprm);
     A->dt = dt;
 }
+
+/* One reaction block of a .thm file, energies in kJ/mol: n terms (species, nu), dG0, atp, dGatp,
+ * chi, cmin, dGloss, temperature, gas constant, concentration scale. n = 0 turns the gate off. */
+void orc_ade_set_thermo(OrcAde* A, int n, const int32_t* sp, const double* nu, const double* v) {
+    A->gate_on = n > 0;
+    A->gate_sp.assign(sp, sp + n);
+    A->gate_nu.assign(nu, nu + n);
+    A->gate_dG0 = v[0]; A->gate_atp = v[1]; A->gate_dGatp = v[2]; A->gate_chi = v[3];
+    A->gate_cmin = v[4]; A->gate_dGloss = v[5]; A->gate_T = v[6]; A->gate_R = v[7]; A->gate_cscale = v[8];
+}
+
+static double thermo_factor(const OrcAde* A, const double* C);
+double orc_thermo_factor(OrcAde* A, const double* C) { return thermo_factor(A, C); }
 
 void orc_ade_set_biomass(OrcAde* A, int M, const double* b) {
     A->M = M;
@@ -660,6 +679,29 @@ static void dissolution_park_gather(int nx, int ny, int nz, int S, int sM, doubl
  * below the threshold read as zero, the rate law, increments R dt whose magnitude exceeds the
  * threshold, clamped so that no concentration or biomass goes below zero: dC = max(R dt, -C).
  * C and B are read and thresholded in place; dC / dB receive the increments (0 where none). */
+/* The thermodynamic factor of Jin & Bethke (2003, 2005) on the concentrations the rate law saw,
+ * used as activities (times the concentration scale, floored at cmin):
+ *   ln Q = sum_i nu_i ln a_i,  dG = dG0 + R T ln Q + dGloss,  f = dG + m dG_ATP,
+ *   F_T = max(0, 1 - exp(f / (chi R T)))   (0 at or past the threshold, 1 when exp underflows);
+ * the steps and their order follow complab3d_thermo.hh:215-258. */
+static double thermo_factor(const OrcAde* A, const double* C) {
+    const double RT = A->gate_R * A->gate_T;
+    double lq = 0.0;
+    for (size_t i = 0; i < A->gate_nu.size(); ++i) {
+        double a = C[A->gate_sp[i]] * A->gate_cscale;
+        if (!(a > A->gate_cmin)) a = A->gate_cmin;
+        lq += A->gate_nu[i] * std::log(a);
+    }
+    const double dG = A->gate_dG0 + RT * lq + A->gate_dGloss;
+    const double f = dG + A->gate_atp * A->gate_dGatp;
+    const double chi = A->gate_chi > 0.0 ? A->gate_chi : 1.0;
+    const double x = f / (chi * RT);
+    if (x >= 0.0) return 0.0;
+    if (x < -700.0) return 1.0;
+    const double F = 1.0 - std::exp(x);
+    return F < 0.0 ? 0.0 : (F > 1.0 ? 1.0 : F);
+}
+
 static void biotic_voxel(const OrcAde* A, double* C, double* B, double* R, double* RB, double* dC, double* dB) {
     const int S = A->S;
     for (int s = 0; s < S; ++s)
@@ -667,6 +709,15 @@ static void biotic_voxel(const OrcAde* A, double* C, double* B, double* R, doubl
     for (int m = 0; m < A->M; ++m)
         if (B[m] < THRD) B[m] = 0;
     rates(A, C, B, R, RB);
+    // run_kinetics (complab3d_processors_part1.hh:134-141) scales the whole voxel's rates by the
+    // factor of microbe 0's reaction block, so the gate acts only in a run with a microbe
+    if (A->gate_on && A->M >= 1) {
+        const double ft = thermo_factor(A, C);
+        if (ft < 1.0) {
+            for (int s = 0; s < S; ++s) R[s] *= ft;
+            for (int m = 0; m < A->M; ++m) RB[m] *= ft;
+        }
+    }
     for (int s = 0; s < S; ++s) {
         double d = R[s] * A->dt;
         dC[s] = 0.0;

@@ -65,6 +65,7 @@ def lib():
             "orc_flow_set_material": ([vp, vp], None),
             "orc_flow_set_dynamics": ([vp, ip, ip, dp], None),
             "orc_biotic_increments": ([vp, vp, vp, vp, vp], None), "orc_abiotic_increments": ([vp, vp, vp], None),
+            "orc_ade_set_thermo": ([vp, ip, vp, vp, vp], None), "orc_thermo_factor": ([vp, vp], dp),
             "orc_ade_set_immobile": ([vp, ip, vp], None), "orc_ade_set_stamp": ([vp, vp], None),
             "orc_ade_stamp": ([vp, vp], None),
             "orc_ca_mask_total_once": ([vp], None), "orc_ca_age_relax": ([vp, ip], ip),
@@ -229,6 +230,20 @@ class OracleAde:
         self._dprm = d
         lib().orc_ade_set_precip(self.h, int(mineral), float(full), int(precip_code), int(dissolution),
                                  float(reopen), int(pore_code), int(dis_law), _p(d), d.size, int(dis_surface_only))
+
+    def set_thermo(self, species=(), nu=(), dG0=0.0, atp=0.0, dGatp=50.0, chi=1.0, cmin=1e-9, dGloss=0.0,
+                   temperature=298.15, gas_constant=8.314462618e-3, conc_scale=1.0):
+        """The thermodynamic gate of the biotic rates (one reaction block, energies in kJ/mol);
+        no terms turns it off."""
+        sp = np.ascontiguousarray(species if len(species) else [0], dtype=np.int32)
+        nu_ = np.ascontiguousarray(nu if len(nu) else [0.0], dtype=np.float64)
+        v = np.array([dG0, atp, dGatp, chi, cmin, dGloss, temperature, gas_constant, conc_scale], np.float64)
+        self._thermo = (sp, nu_, v)
+        lib().orc_ade_set_thermo(self.h, len(species), _p(sp), _p(nu_), _p(v))
+
+    def thermo_factor(self, c):
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        return lib().orc_thermo_factor(self.h, _p(c))
 
     def set_immobile(self, s, c):
         c = np.ascontiguousarray(c, dtype=np.float64).reshape(-1)

@@ -112,3 +112,34 @@ extern "C" void ref_abiotic_increments(int nx, int ny, int nz, int S, double dt,
     }
     read(L, S, S, dC, N);
 }
+
+/* The thermodynamic gate (complab3d_thermo.hh): one reaction block (terms sp/nu; v = dG0, atp,
+ * dGatp, chi, cmin, dGloss, temperature, gas constant, concentration scale, energies in kJ/mol),
+ * registered for n_microbes organisms as the kinetics path registers it, so run_kinetics gates its
+ * rates through gateFor(0, ...). n = 0 clears it. */
+extern "C" void ref_set_thermo(int n, const int32_t* sp, const double* nu, const double* v, int n_microbes) {
+    complab_thermo::Runtime& R = complab_thermo::runtime();
+    R = complab_thermo::Runtime();
+    if (n <= 0) return;
+    complab_thermo::Spec s;
+    s.name = "gate";
+    s.microbe = -1;
+    for (int i = 0; i < n; ++i) {
+        s.species.push_back("s" + std::to_string(sp[i]));
+        s.nu.push_back(nu[i]);
+        s.subsOfSpecies.push_back(sp[i]);
+    }
+    s.dG0 = v[0]; s.atp = v[1]; s.dGatp = v[2]; s.chi = v[3]; s.cmin = v[4]; s.dGloss = v[5];
+    R.model.Tkelvin = v[6];
+    R.model.Rgas = v[7];
+    R.model.concScale = v[8];
+    R.model.specs.push_back(s);
+    complab_thermo::registerModel(n_microbes);
+}
+
+// complab_thermo::factor on one concentration vector of S species (scaled as fillConc scales it)
+extern "C" double ref_thermo_factor(int S, const double* C) {
+    std::vector<double> conc;
+    complab_thermo::fillConc(C, S, conc);
+    return complab_thermo::gateFor(0, conc);
+}

@@ -9,7 +9,8 @@ tests/golden/conversion.npz from the reference's node conversions (precipNodeCon
 dissolNodeConversion3D, the same library), tests/golden/kinetics.npz from the reference's
 kinetics processors (run_kinetics,
 run_abiotic_kinetics of complab3d_processors_part1.hh and surfaceAbioticKinetics3D, compiled into
-oracle/_ref/libref_kinetics.so with the FeS law of examples/15), tests/golden/automaton.npz from
+oracle/_ref/libref_kinetics.so with the FeS law of examples/15) and its thermodynamic gate
+(complab3d_thermo.hh, alone and inside run_kinetics), tests/golden/automaton.npz from
 the biofilm automaton's mask/total update and age relaxation
 (updateLocalMaskNtotalLattices3D and updateAgeDistance3D of complab3d_processors_part2.hh, the
 same library) on seeded maps.
@@ -232,9 +233,32 @@ def kinetics_cases():
             for k, v in dict(mat=mat, C=Cf, dC=dC, meta=np.array([surf, dt])).items():
                 rec[f"a{case}_{k}"] = v
             case += 1
+    # the thermodynamic gate: factors of two reaction blocks on seeded concentration vectors, and
+    # run_kinetics gated by it (dual Monod, one microbe)
+    gates = (([0, 1, 2, 3], [-1.0, -1.0, 1.0, 1.0], [-33.12, 0.25, 50.0, 1.0, 1e-9, 0.0, 277.15, 8.314e-3, 1e-3]),
+             ([0, 2], [-1.0, 2.0], [-20.0, 0.5, 45.0, 2.0, 1e-7, 1.5, 298.15, 8.314462618e-3, 1.0]))
+    for case, (sp, nu, v) in enumerate(gates):
+        sp, nu, v = np.array(sp, np.int32), np.array(nu, np.float64), np.array(v, np.float64)
+        S = 4
+        L.ref_set_thermo(len(sp), P(sp), P(nu), P(v), 1)
+        L.ref_thermo_factor.restype = C.c_double
+        cs = 10 ** rng.uniform(-7, 1, (600, S))
+        cs[rng.random((600, S)) < 0.08] = 0.0
+        F = np.array([L.ref_thermo_factor(S, P(np.ascontiguousarray(c))) for c in cs])
+        mat = np.where(rng.random(N) < 0.2, 0, 2).astype(np.int8)
+        mat[(mat == 2) & (rng.random(N) < 0.4)] = 3
+        Cf = 10 ** rng.uniform(-5, 0.5, (S, N))
+        B = rng.uniform(0, 2, (1, N))
+        prm = np.array([0.5, 0.2, 0.4, 0.01], np.float64)
+        dC, dB = np.zeros((S, N)), np.zeros((1, N))
+        L.ref_biotic_increments(nx, ny, nz, S, 1, C.c_double(1.0), 3, P(prm), len(prm), P(mat), 0, 1, P(Cf), P(B),
+                                P(dC), P(dB))
+        L.ref_set_thermo(0, P(sp), P(nu), P(v), 1)
+        for k, val in dict(sp=sp, nu=nu, v=v, cs=cs, F=F, mat=mat, C=Cf, B=B, prm=prm, dC=dC, dB=dB).items():
+            rec[f"g{case}_{k}"] = val
     rec["shape"] = np.array(shape)
     np.savez_compressed(os.path.join(os.path.dirname(os.path.abspath(__file__)), "kinetics.npz"), **rec)
-    print("wrote 4 biotic and 6 abiotic kinetics cases")
+    print("wrote 4 biotic, 6 abiotic and 2 gated kinetics cases")
 
 
 def conversion_cases():

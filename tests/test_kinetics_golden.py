@@ -72,3 +72,25 @@ def test_some_cases_overdraw():
         g = _case(tag)
         n += int((g["dC"] < -np.where(g["C"] < THRD, 0.0, g["C"])).sum())
     assert n > 100
+
+
+@pytest.mark.parametrize("tag", _tags("g"))
+def test_oracle_thermodynamic_gate_matches_the_reference(oracle, tag):
+    """complab3d_thermo.hh's factor F_T = max(0, 1 - exp((dG + m dG_ATP) / (chi R T))) on seeded
+    concentration vectors (equal: both evaluate the same expression with the C library's log and
+    exp), and run_kinetics gated by it (dual Monod, one microbe)."""
+    g = _case(tag)
+    S = g["C"].shape[0]
+    O = oracle.OracleAde(g["mat"], *SHAPE, [dict(omega_pore=1.0)] * S, np.zeros(3 * N), bio_codes=(3,))
+    O.set_thermo(g["sp"], g["nu"], *g["v"])
+    F = np.array([O.thermo_factor(c) for c in g["cs"]])
+    assert (g["F"] == 0).sum() > 20 and ((g["F"] > 0) & (g["F"] < 1)).sum() > 100
+    np.testing.assert_allclose(F, g["F"], rtol=1e-14, atol=1e-15)
+    O.set_kinetics(3, g["prm"], 1.0)
+    O.set_biomass(g["B"])
+    dC, dB = O.biotic_increments(g["C"], g["B"])
+    _check(dC, g["dC"], g["C"], 1e-14)
+    _check(dB, g["dB"], g["B"], 1e-13)
+    O.set_thermo()  # off: the increments change
+    dC0, _ = O.biotic_increments(g["C"], g["B"])
+    assert (np.abs(dC0 - dC) > 1e-12).sum() > 100
