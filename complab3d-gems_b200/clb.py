@@ -81,6 +81,13 @@ class SpeciationDesc(C.Structure):
                 ("max_iterations", C.c_int32)]
 
 
+class ThermoDesc(C.Structure):
+    _fields_ = [("n_terms", C.c_int32), ("species", C.c_int32 * MAX_SPECIES), ("nu", C.c_double * MAX_SPECIES),
+                ("dG0", C.c_double), ("atp", C.c_double), ("dGatp", C.c_double), ("chi", C.c_double),
+                ("cmin", C.c_double), ("dGloss", C.c_double), ("temperature", C.c_double),
+                ("gas_constant", C.c_double), ("conc_scale", C.c_double)]
+
+
 class PrecipDesc(C.Structure):
     _fields_ = [("mineral_species", C.c_int32), ("full_density", C.c_double), ("precip_code", C.c_int32),
                 ("seal_flow", C.c_int32), ("seal_perm_ratio", C.c_double), ("flow_max_iterations", C.c_int32),
@@ -132,6 +139,7 @@ SIGNATURES = {
     "clb_couple_velocity": [C.c_void_p],
     "clb_set_kinetics": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double],
     "clb_set_biomass": [C.c_void_p, C.c_int, C.c_void_p],
+    "clb_set_thermo_gate": [C.c_void_p, C.POINTER(ThermoDesc)],
     "clb_ade_step": [C.c_void_p, C.c_int],
     "clb_reduce": [C.c_void_p, C.POINTER(Stats)],
     "clb_reduce_noalloc": [C.c_void_p, C.POINTER(Stats)],
@@ -425,6 +433,18 @@ class Domain:
         b = np.ascontiguousarray(b, dtype=np.float64)
         M = b.size // self.N
         self._check(lib().clb_set_biomass(self.h, M, _ptr(b)))
+
+    def set_thermo_gate(self, species=(), nu=(), dG0=0.0, atp=0.0, dGatp=50.0, chi=1.0, cmin=1e-9, dGloss=0.0,
+                        temperature=298.15, gas_constant=8.314462618e-3, conc_scale=1.0):
+        """The thermodynamic gate of the biotic rates: one reaction block (user species indices
+        and stoichiometric numbers, energies in kJ/mol). No terms turns it off."""
+        d = ThermoDesc()
+        d.n_terms = len(species)
+        for i, (sp, v) in enumerate(zip(species, nu)):
+            d.species[i], d.nu[i] = int(sp), float(v)
+        d.dG0, d.atp, d.dGatp, d.chi, d.cmin, d.dGloss = dG0, atp, dGatp, chi, cmin, dGloss
+        d.temperature, d.gas_constant, d.conc_scale = temperature, gas_constant, conc_scale
+        self._check(lib().clb_set_thermo_gate(self.h, C.byref(d)))
 
     def ade_step(self, n=1):
         self._check(lib().clb_ade_step(self.h, n))

@@ -58,7 +58,8 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra
             else if (s < P.S) c = (TC)imm[(int64_t)s * G.N + nd];
             C[s] = c < thr ? (TC)0 : c;
         }
-        biotic_rates<TC, NM, true>(P, C, R, bio, nd, G.N, bc, ADE_THREADS, bn);  // advances the biomass too
+        const TC ft = (P.gate_on && P.M >= 1) ? (TC)thermo_gate<TC, NM>(P, C) : (TC)1;
+        biotic_rates<TC, NM, true>(P, C, R, bio, nd, G.N, bc, ADE_THREADS, bn, ft);  // advances the biomass too
 #pragma unroll
         for (int s = 0; s < NM; ++s) {
             if (s >= P.S) continue;
@@ -827,6 +828,37 @@ clb_status ade_set_abiotic(clb_handle* h, int law, const double* prm, int nprm, 
     P.law2 = law;
     P.surf = surface_only ? 1 : 0;
     return geometry_refresh(h);
+}
+
+clb_status ade_set_thermo(clb_handle* h, const clb_thermo_desc* d) {
+    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+    AdeParams& P = h->ap;
+    if (!d || d->n_terms == 0) {
+        P.gate_on = 0;
+        P.gate_n = 0;
+        return CLB_OK;
+    }
+    if (d->n_terms < 0 || d->n_terms > CLB_MAX_SPECIES) return fail(h, CLB_INVALID_ARG, "thermo gate: term count out of range");
+    if (!(d->cmin > 0.0)) return fail(h, CLB_INVALID_ARG, "thermo gate: cmin <= 0, so ln Q can be -inf");
+    if (d->dGloss < 0.0) return fail(h, CLB_INVALID_ARG, "thermo gate: negative dGloss");
+    if (!(d->temperature > 0.0) || !(d->gas_constant > 0.0) || !(d->conc_scale > 0.0))
+        return fail(h, CLB_INVALID_ARG, "thermo gate: temperature, gas constant and concentration scale must be positive");
+    for (int i = 0; i < d->n_terms; ++i) {
+        if (d->species[i] < 0 || d->species[i] >= h->S) return fail(h, CLB_INVALID_ARG, "thermo gate: species index out of range");
+        P.gate_sp[i] = h->u2i[d->species[i]];
+        P.gate_nu[i] = d->nu[i];
+    }
+    P.gate_n = d->n_terms;
+    P.gate_dG0 = d->dG0;
+    P.gate_dGloss = d->dGloss;
+    P.gate_atp = d->atp;
+    P.gate_dGatp = d->dGatp;
+    P.gate_chi = d->chi > 0.0 ? d->chi : 1.0;
+    P.gate_cmin = d->cmin;
+    P.gate_RT = d->gas_constant * d->temperature;
+    P.gate_cscale = d->conc_scale;
+    P.gate_on = 1;
+    return CLB_OK;
 }
 
 clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {

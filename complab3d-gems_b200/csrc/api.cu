@@ -243,6 +243,12 @@ clb_status clb_set_kinetics(clb_handle* h, int law, const double* params, int n_
     return ade_set_kinetics(h, law, params, n_params, dt);
 }
 
+clb_status clb_set_thermo_gate(clb_handle* h, const clb_thermo_desc* desc) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    return ade_set_thermo(h, desc);
+}
+
 clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass) {
     if (!h || (n_microbes > 0 && !biomass)) return fail(h, CLB_INVALID_ARG, "null argument");
     CLB_ON_DEVICE(h);

@@ -125,6 +125,11 @@ struct AdeParams {
     // dissolution of sealed mineral voxels
     int dis_on, dis_law, dis_surf, sM;  // sM: internal index of the mineral
     double dprm[2 + CLB_MAX_SPECIES];
+    // thermodynamic gate of the biotic rates (internal species indices; chi already >= 1 when unset)
+    int gate_on, gate_n;
+    int gate_sp[CLB_MAX_SPECIES];
+    double gate_nu[CLB_MAX_SPECIES];
+    double gate_dG0, gate_dGloss, gate_atp, gate_dGatp, gate_chi, gate_cmin, gate_RT, gate_cscale;
 };
 
 // Per-node state of the precipitation / dissolution machinery (geometry_update.cu), passed to the
@@ -299,6 +304,7 @@ clb_status ade_set_biomass_field(clb_handle* h, int m, const double* host);
 clb_status ade_reduce(clb_handle* h, clb_stats* out);
 clb_status ade_reduce_noalloc(clb_handle* h, clb_stats* out);
 clb_status ade_set_abiotic(clb_handle* h, int law, const double* prm, int nprm, int surface_only);
+clb_status ade_set_thermo(clb_handle* h, const clb_thermo_desc* d);
 void ade_refresh_neumann(clb_handle* h);
 void ade_free(clb_handle* h);
 

@@ -14,10 +14,13 @@ namespace clb {
 // clamped increment (dB = max(R_B dt, -B), applied when |dB| > THRD), microbe by microbe, so no
 // per-microbe array is kept. Loops over species are unrolled to the bucket NB so every array stays
 // in registers.
+// ft: the thermodynamic factor of the voxel (thermo_gate); below 1 it scales every substrate and
+// biomass rate before the increments are formed, as run_kinetics scales them.
 template <typename KT, int NB, bool APPLY_BIO>
 __device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[NB], KT (&R)[NB],
                                              const double* __restrict__ bio, int64_t nd, int64_t N,
-                                             const double* bc = nullptr, int bstride = 0, int bn = 0) {
+                                             const double* bc = nullptr, int bstride = 0, int bn = 0,
+                                             KT ft = (KT)1) {
     const KT thr = (KT)THRD;
 #pragma unroll
     for (int s = 0; s < NB; ++s) R[s] = 0;
@@ -52,7 +55,8 @@ __device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[N
                 for (int s = 0; s < NB; ++s)
                     if (s == a) Ca = C[s];
                 const KT growth = mu * (Cd / (ks + Cd)) * (Ca / (ks + Ca)) * Bm;
-                const KT rbm = growth - kd * Bm;
+                KT rbm = growth - kd * Bm;
+                if (ft < (KT)1) rbm *= ft;
                 Rd -= growth / Y;
 #pragma unroll
                 for (int s = 0; s < NB; ++s)
@@ -73,6 +77,35 @@ __device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[N
         default:
             break;
     }
+    if (ft < (KT)1) {
+#pragma unroll
+        for (int s = 0; s < NB; ++s) R[s] *= ft;
+    }
+}
+
+// The thermodynamic factor of Jin & Bethke (2003, 2005) on the floored concentrations C of the
+// rate law, used as activities: a_i = max(C_i conc_scale, cmin), ln Q = sum nu_i ln a_i,
+// dG = dG0 + RT ln Q + dGloss, x = (dG + m dG_ATP) / (chi RT), F_T = 0 for x >= 0, 1 for
+// x < -700, else 1 - exp(x) (complab3d_thermo.hh:215-258). FP64 throughout.
+template <typename KT, int NB>
+__device__ __forceinline__ double thermo_gate(const AdeParams& P, const KT (&C)[NB]) {
+    double lq = 0.0;
+    for (int i = 0; i < P.gate_n; ++i) {
+        const int sp = P.gate_sp[i];
+        KT c = 0;
+#pragma unroll
+        for (int s = 0; s < NB; ++s)
+            if (s == sp) c = C[s];
+        double a = (double)c * P.gate_cscale;
+        if (!(a > P.gate_cmin)) a = P.gate_cmin;
+        lq += P.gate_nu[i] * log(a);
+    }
+    const double dG = P.gate_dG0 + P.gate_RT * lq + P.gate_dGloss;
+    const double x = (dG + P.gate_atp * P.gate_dGatp) / (P.gate_chi * P.gate_RT);
+    if (x >= 0.0) return 0.0;
+    if (x < -700.0) return 1.0;
+    const double F = 1.0 - exp(x);
+    return F < 0.0 ? 0.0 : (F > 1.0 ? 1.0 : F);
 }
 
 // Abiotic laws (clb_law CLB_LAW_PRECIP / CLB_LAW_MINERAL) over internal species indices, evaluated
@@ -171,7 +204,8 @@ __device__ void post_biotic(const AdeParams& P, const SparseView& S, const TS* g
         else if (s < P.S) c = (TC)Craw[s];
         C[s] = c < thr ? (TC)0 : c;
     }
-    biotic_rates<TC, CLB_MAX_SPECIES, false>(P, C, R, bio, n, G.N);
+    const TC ft = (P.gate_on && P.M >= 1) ? (TC)thermo_gate<TC, CLB_MAX_SPECIES>(P, C) : (TC)1;
+    biotic_rates<TC, CLB_MAX_SPECIES, false>(P, C, R, bio, n, G.N, nullptr, 0, 0, ft);
 #pragma unroll
     for (int s = 0; s < CLB_MAX_SPECIES; ++s) {
         if (s >= P.S) continue;

@@ -227,6 +227,31 @@ clb_status clb_set_kinetics(clb_handle* h, int law, const double* params, int n_
  * indices in params are user species indices. */
 clb_status clb_set_abiotic_kinetics(clb_handle* h, int law, const double* params, int n_params, int surface_only);
 
+/* One reaction block of the thermodynamic gate (a .thm file's `reaction`), energies in kJ/mol. */
+typedef struct clb_thermo_desc {
+    int32_t n_terms;                   /* terms of the stoich line; 0 turns the gate off          */
+    int32_t species[CLB_MAX_SPECIES];  /* user species index of each term                         */
+    double nu[CLB_MAX_SPECIES];        /* stoichiometric number: negative reactant, positive product */
+    double dG0;                        /* standard free energy at `temperature`, kJ/mol           */
+    double atp;                        /* mol ATP conserved per mol reaction (m)                  */
+    double dGatp;                      /* free energy of ATP synthesis, kJ/mol ATP                */
+    double chi;                        /* average stoichiometric number (<= 0 reads as 1)         */
+    double cmin;                       /* activity floor, mol/L (> 0)                             */
+    double dGloss;                     /* constant electron-transfer loss added to dG (>= 0)      */
+    double temperature;                /* kelvin                                                  */
+    double gas_constant;               /* kJ/mol/K (8.314462618e-3)                               */
+    double conc_scale;                 /* solver concentration unit -> mol/L                      */
+} clb_thermo_desc;
+
+/* The thermodynamic gate of the biotic rates: per voxel, on the concentrations the rate law saw
+ * (times conc_scale, floored at cmin), ln Q = sum nu_i ln a_i, dG = dG0 + R T ln Q + dGloss,
+ * F_T = max(0, 1 - exp((dG + atp dGatp) / (chi R T))), and every substrate and biomass rate of the
+ * voxel is multiplied by F_T before dC = max(R dt, -C). As in the reference, the block applies to
+ * microbe 0, so the gate acts only in a run with biomass fields. desc NULL or n_terms 0: off.
+ * Replaces: complab_thermo::gateFor (complab3d_thermo.hh:215-258, 669-692) in run_kinetics
+ * (complab3d_processors_part1.hh:134-141) with one reaction block. */
+clb_status clb_set_thermo_gate(clb_handle* h, const clb_thermo_desc* desc);
+
 /* Biomass fields of the CA microbes, [n_microbes][N] float64. */
 clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass);
 
