@@ -58,7 +58,8 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra
             else if (s < P.S) c = (TC)imm[(int64_t)s * G.N + nd];
             C[s] = c < thr ? (TC)0 : c;
         }
-        const TC ft = (P.gate_on && P.M >= 1) ? (TC)thermo_gate<TC, NM>(P, C) : (TC)1;
+        // the thermodynamic gate is compiled only into the EXT instantiations
+        const TC ft = (EXT && P.gate_on && P.M >= 1) ? (TC)thermo_gate<TC, NM>(P, C) : (TC)1;
         biotic_rates<TC, NM, true>(P, C, R, bio, nd, G.N, bc, ADE_THREADS, bn, ft);  // advances the biomass too
 #pragma unroll
         for (int s = 0; s < NM; ++s) {
@@ -71,7 +72,7 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra
             else imm[(int64_t)s * G.N + nd] += (double)d;
         }
     }
-    if (EXT && !west && !east && P.react[code]) {
+    if (EXT && (P.law2 != CLB_LAW_NONE || P.dis_on) && !west && !east && P.react[code]) {
         // abiotic block: increments from the concentrations the biotic law left, applied once
         // (update_abiotic_rxnLattices); next to a dissolving voxel they were computed ahead of
         // the step together with the gathered products
@@ -911,7 +912,7 @@ static void launch_ade_t(clb_handle* h) {
     const TC* u = (const TC*)h->d_u;
     int* mt = mob_table(h);
     const SparseView S = view_of(h->ade_sp);
-    const bool ext = h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on;
+    const bool ext = h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on || h->ap.gate_on;
     const AdeExtra X = ade_extra(h);
 #define CLB_ADE(NM, EXT)                                                                                          \
     do {                                                                                                          \

@@ -73,9 +73,10 @@ clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out) {
             delete b;
             return fail(nullptr, CLB_INVALID_ARG, "batch handles must share their storage precisions");
         }
-        if (b->has_ade && (h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on || h->spec_mode != CLB_SPEC_OFF)) {
+        if (b->has_ade && (h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on || h->ap.gate_on || h->spec_mode != CLB_SPEC_OFF)) {
             delete b;
-            return fail(nullptr, CLB_INVALID_ARG, "batched transport has no abiotic law, dissolution or speciation");
+            return fail(nullptr, CLB_INVALID_ARG,
+                        "batched transport has no abiotic law, dissolution, thermodynamic gate or speciation");
         }
         if (b->has_ade && h->M > 0 && !h->d_bio) { delete b; return fail(nullptr, CLB_INVALID_ARG, "biomass missing"); }
         if (b->has_ade) b->nm = std::max(b->nm, h->S);

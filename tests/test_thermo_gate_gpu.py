@@ -88,3 +88,10 @@ def test_gate_rejects_bad_blocks(clb, oracle, bad):
     g = dict(GATE, **bad)
     with pytest.raises(clb.ClbError):
         D.set_thermo_gate(**g)
+
+
+def test_batch_refuses_a_gated_domain(clb, oracle):
+    """The batched transport kernels are compiled without the gate, so a gated domain is refused."""
+    D, _ = gated_pair(clb, oracle, clb.F64)
+    with pytest.raises(clb.ClbError):
+        clb.Batch([D])
