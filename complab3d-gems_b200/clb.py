@@ -140,6 +140,9 @@ SIGNATURES = {
     "clb_set_kinetics": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double],
     "clb_set_biomass": [C.c_void_p, C.c_int, C.c_void_p],
     "clb_set_thermo_gate": [C.c_void_p, C.POINTER(ThermoDesc)],
+    "clb_write_vti": [C.c_void_p, C.c_int, C.c_int, C.c_char_p],
+    "clb_vti_write": [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                      C.c_void_p],
     "clb_ade_step": [C.c_void_p, C.c_int],
     "clb_reduce": [C.c_void_p, C.POINTER(Stats)],
     "clb_reduce_noalloc": [C.c_void_p, C.POINTER(Stats)],
@@ -446,6 +449,12 @@ class Domain:
         d.temperature, d.gas_constant, d.conc_scale = temperature, gas_constant, conc_scale
         self._check(lib().clb_set_thermo_gate(self.h, C.byref(d)))
 
+    def write_vti(self, field, path, index=0):
+        """One .vti file of the flow velocity (FIELD_FLOW_VELOCITY), the material map
+        (FIELD_MATERIAL), a species' concentration or a microbe's biomass (FIELD_CONCENTRATION /
+        FIELD_BIOMASS with `index`) over the interior x-planes."""
+        self._check(lib().clb_write_vti(self.h, int(field), int(index), os.fsencode(path)))
+
     def ade_step(self, n=1):
         self._check(lib().clb_ade_step(self.h, n))
 
@@ -560,6 +569,28 @@ class Domain:
         loss = np.zeros(1, dtype=np.float32)
         self._check(lib().clb_surrogate_gradient(self.h, _ptr(X), _ptr(Y), n, _ptr(g), _ptr(loss)))
         return g, float(loss[0])
+
+
+def vti_write(path, shape, arrays):
+    """Writes host arrays as one .vti file over the interior x-planes: `arrays` maps a name to a
+    float64 or float32 array of shape [N] or [components][N] (x slowest, N = nx ny nz)."""
+    nx, ny, nz = shape
+    N = nx * ny * nz
+    keep, names, comps, types = [], [], [], []
+    for name, a in arrays.items():
+        a = np.asarray(a)
+        dt = np.float32 if a.dtype == np.float32 else np.float64
+        a = np.ascontiguousarray(a, dtype=dt).reshape(-1, N)
+        keep.append(a)
+        names.append(name.encode())
+        comps.append(a.shape[0])
+        types.append(1 if dt == np.float32 else 0)
+    n = len(keep)
+    cn = (C.c_char_p * max(n, 1))(*names)
+    cc = (C.c_int32 * max(n, 1))(*comps)
+    ct = (C.c_int32 * max(n, 1))(*types)
+    cd = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in keep])
+    _check_global(lib().clb_vti_write(os.fsencode(path), nx, ny, nz, n, cn, cc, ct, cd))
 
 
 class Batch:

@@ -483,6 +483,24 @@ clb_status clb_surrogate_gradient(clb_handle* h, const float* X, const float* Y,
 clb_status clb_get_field(clb_handle* h, int field, int index, void* host, int dtype);
 clb_status clb_set_field(clb_handle* h, int field, int index, const void* host, int dtype);
 
+/* ---------------------------------------------------------------- output */
+
+/* One VTK ImageData file (.vti, XML, inline base64 binary, UInt64 headers) of a domain field over
+ * the interior x-planes 1..nx-2, x fastest, spacing 1, as the reference's writers produce it:
+ *   CLB_FIELD_FLOW_VELOCITY   "velocityNorm" + "velocity" (float32)  writeNsVTI
+ *   CLB_FIELD_MATERIAL        "tag" (float32)                        writePorousMediumVTI
+ *   CLB_FIELD_CONCENTRATION   "Density" of species `index` (float64) writeAdvVTI
+ *   CLB_FIELD_BIOMASS         "Density" of microbe `index` (float64) writeAdvVTI
+ * Replaces: complab_functions.hh:96-176 (the caller names the file, e.g. nameid + 7-digit
+ * iteration + ".vti" as createFileName does). */
+clb_status clb_write_vti(clb_handle* h, int field, int index, const char* path);
+
+/* The writer itself, for host arrays: n_arrays point-data arrays, array a [components[a]][N] in
+ * this library's layout (x slowest, N = nx ny nz), dtypes[a] 0 float64 or 1 float32 (written as
+ * stored), cropped to x = 1..nx-2. */
+clb_status clb_vti_write(const char* path, int nx, int ny, int nz, int n_arrays, const char* const* names,
+                         const int32_t* components, const int32_t* dtypes, const void* const* data);
+
 /* ---------------------------------------------------------------- geometry (host) */
 
 /* complab_geom::GenOptions (complab3d_geometry.hh:111-120). */
