@@ -58,8 +58,13 @@ clb_status clb_create(const clb_domain_desc* desc, const int8_t* material, clb_h
     if (!(desc->tau > 0.5)) return fail(nullptr, CLB_INVALID_ARG, "tau must exceed 1/2");
     if (desc->n_microbes < 0 || desc->n_microbes > CLB_MAX_MICROBES)
         return fail(nullptr, CLB_INVALID_ARG, "microbe count out of range");
-    for (int64_t n = 0; n < N; ++n)
-        if (material[n] < 0) return fail(nullptr, CLB_INVALID_ARG, "negative material code");
+    {
+        // any negative code sets the sign bit of the OR (a branch-free pass the compiler vectorises)
+        uint8_t acc = 0;
+        const uint8_t* m = reinterpret_cast<const uint8_t*>(material);
+        for (int64_t n = 0; n < N; ++n) acc |= m[n];
+        if (acc & 0x80u) return fail(nullptr, CLB_INVALID_ARG, "negative material code");
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return fail(nullptr, CLB_CUDA_ERROR, "no CUDA device");
     clb_handle* h = new (std::nothrow) clb_handle_s();

@@ -789,13 +789,26 @@ clb_status flow_init(clb_handle* h, double delta_p) {
     for (int c = 0; c < MAX_CODES; ++c) cls[c] = (P.dyn[c] != DYN_BB);
     for (int m = 0; m < d.n_microbes; ++m)
         if (d.bio_codes[m] >= 0 && d.bio_codes[m] < MAX_CODES) cls[d.bio_codes[m]] = 1;
+    // BGK node count from a histogram of the codes (four interleaved counters, no data-dependent
+    // branch), the node counts of the first and last x-planes from those planes alone
     int64_t nbgk = 0, kw = 0, ke = 0;
-    for (int64_t n = 0; n < h->g.N; ++n) {
-        const int c = (uint8_t)fmat[n] & 127;
-        nbgk += (P.dyn[c] == DYN_BGK);
-        if (cls[c]) {
-            if (n < h->g.plane) ++kw;
-            if (n >= h->g.N - h->g.plane) ++ke;
+    {
+        std::vector<int64_t> hist(4 * 128, 0);
+        const uint8_t* m = reinterpret_cast<const uint8_t*>(fmat.data());
+        const int64_t N = h->g.N, plane = h->g.plane;
+        int64_t n = 0;
+        for (; n + 4 <= N; n += 4) {
+            ++hist[m[n] & 127];
+            ++hist[128 + (m[n + 1] & 127)];
+            ++hist[256 + (m[n + 2] & 127)];
+            ++hist[384 + (m[n + 3] & 127)];
+        }
+        for (; n < N; ++n) ++hist[m[n] & 127];
+        for (int c = 0; c < 128; ++c)
+            if (P.dyn[c] == DYN_BGK) nbgk += hist[c] + hist[128 + c] + hist[256 + c] + hist[384 + c];
+        for (int64_t i = 0; i < plane; ++i) {
+            kw += cls[m[i] & 127];
+            ke += cls[m[N - plane + i] & 127];
         }
     }
     P.n_bgk = nbgk;
