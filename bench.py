@@ -525,18 +525,27 @@ def main():
     mat_host[:] = mat
     u_host = torch.empty(3 * mat.size, dtype=udt, pin_memory=True).numpy()
     # the whole job three times; the median job time is reported
-    t_jobs = []
+    t_jobs, phases = [], []
     for _ in range(3):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         E = clb.Domain(mat_host, nx, ny, nz, cfg["tau"], flow_precision=prec, device=local)
+        t1 = time.perf_counter()
         E.flow_init(cfg["delta_p"])
+        E.sync()
+        t2 = time.perf_counter()
         E.flow_step(k_e2e)
+        E.sync()
+        t3 = time.perf_counter()
         u = E.velocity(u_host.dtype, out=u_host)
-        t_jobs.append(time.perf_counter() - t0)
+        t4 = time.perf_counter()
+        t_jobs.append(t4 - t0)
+        phases.append({"create": 1e3 * (t1 - t0), "init": 1e3 * (t2 - t1), "steps": 1e3 * (t3 - t2),
+                       "velocity_to_host": 1e3 * (t4 - t3)})
         E.close()
         del E
     t_e2e = statistics.median(t_jobs)
+    job_phases = phases[t_jobs.index(t_e2e)]
     e2e_val = world * n_open * k_e2e / t_e2e / 1e6
     h2d = mat_host.nbytes  # the compacted layout is built on the device from the map
     d2h = u.nbytes
@@ -574,7 +583,8 @@ def main():
             "e2e": {"value": e2e_val, "unit": "MLUPS", "h2d_bytes_per_step": h2d / k_e2e,
                     "d2h_bytes_per_step": d2h / k_e2e,
                     "note": "one job through the C ABI: create + init + K steps + velocity to host, wall clock; "
-                            "median of 3 jobs", "job_seconds": t_jobs},
+                            "median of 3 jobs", "job_seconds": t_jobs,
+                    "median_job_phases_ms": job_phases},
             "gpu_launches": a.steps,
             "clocks": clocks.summary(),
         }
