@@ -25,6 +25,7 @@ DISSOL_NONE, DISSOL_FIRST_ORDER, DISSOL_MINERAL = 0, 1, 2
 FIELD_MATERIAL, FIELD_FLOW_VELOCITY, FIELD_FLOW_POPULATIONS = 0, 1, 2
 FIELD_CONCENTRATION, FIELD_ADE_POPULATIONS, FIELD_BIOMASS, FIELD_ADE_VELOCITY = 3, 4, 5, 6
 FIELD_CA_TOTAL, FIELD_CA_AGE = 7, 8
+CKPT_FLOW, CKPT_TRANSPORT = 1, 2
 
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "NOT_CONVERGED", 3: "NONFINITE", 4: "PERCOLATION_LOST",
           5: "CUDA_ERROR", 6: "TIMEOUT", 7: "NOT_INITIALIZED", 8: "OUT_OF_MEMORY"}
@@ -141,6 +142,8 @@ SIGNATURES = {
     "clb_set_biomass": [C.c_void_p, C.c_int, C.c_void_p],
     "clb_set_thermo_gate": [C.c_void_p, C.POINTER(ThermoDesc)],
     "clb_write_vti": [C.c_void_p, C.c_int, C.c_int, C.c_char_p],
+    "clb_checkpoint_save": [C.c_void_p, C.c_char_p, C.c_int],
+    "clb_checkpoint_load": [C.c_void_p, C.c_char_p],
     "clb_vti_write": [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                       C.c_void_p],
     "clb_ade_step": [C.c_void_p, C.c_int],
@@ -448,6 +451,15 @@ class Domain:
         d.dG0, d.atp, d.dGatp, d.chi, d.cmin, d.dGloss = dG0, atp, dGatp, chi, cmin, dGloss
         d.temperature, d.gas_constant, d.conc_scale = temperature, gas_constant, conc_scale
         self._check(lib().clb_set_thermo_gate(self.h, C.byref(d)))
+
+    def checkpoint_save(self, path, flow=True, transport=True):
+        """A restart file of the flow and/or transport lattices (FP64, exact)."""
+        what = (CKPT_FLOW if flow else 0) | (CKPT_TRANSPORT if transport else 0)
+        self._check(lib().clb_checkpoint_save(self.h, os.fsencode(path), what))
+
+    def checkpoint_load(self, path):
+        """Restores a restart file into this handle (same material map, same set-up)."""
+        self._check(lib().clb_checkpoint_load(self.h, os.fsencode(path)))
 
     def write_vti(self, field, path, index=0):
         """One .vti file of the flow velocity (FIELD_FLOW_VELOCITY), the material map

@@ -831,6 +831,16 @@ clb_status ade_set_abiotic(clb_handle* h, int law, const double* prm, int nprm, 
     return geometry_refresh(h);
 }
 
+// the concentration field of an immobile species (user index), FP64 [N]
+clb_status ade_set_immobile(clb_handle* h, int s, const double* host) {
+    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+    if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
+    const int si = h->u2i[s];
+    if (h->ap.slot[si] >= 0) return fail(h, CLB_INVALID_ARG, "not an immobile species");
+    return cuda_check(h, cudaMemcpy(h->d_imm + (size_t)si * h->g.N, host, sizeof(double) * (size_t)h->g.N,
+                                    cudaMemcpyHostToDevice), "immobile concentration");
+}
+
 clb_status ade_set_thermo(clb_handle* h, const clb_thermo_desc* d) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     AdeParams& P = h->ap;

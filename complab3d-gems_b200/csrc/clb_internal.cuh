@@ -305,6 +305,7 @@ clb_status ade_reduce(clb_handle* h, clb_stats* out);
 clb_status ade_reduce_noalloc(clb_handle* h, clb_stats* out);
 clb_status ade_set_abiotic(clb_handle* h, int law, const double* prm, int nprm, int surface_only);
 clb_status ade_set_thermo(clb_handle* h, const clb_thermo_desc* d);
+clb_status ade_set_immobile(clb_handle* h, int s, const double* host);
 void ade_refresh_neumann(clb_handle* h);
 void ade_free(clb_handle* h);
 

@@ -483,6 +483,22 @@ clb_status clb_surrogate_gradient(clb_handle* h, const float* X, const float* Y,
 clb_status clb_get_field(clb_handle* h, int field, int index, void* host, int dtype);
 clb_status clb_set_field(clb_handle* h, int field, int index, const void* host, int dtype);
 
+/* ---------------------------------------------------------------- checkpoints */
+
+#define CLB_CKPT_FLOW 1        /* the flow lattice's incoming populations                        */
+#define CLB_CKPT_TRANSPORT 2   /* every species (mobile: populations, immobile: concentration),
+                                  the biomass fields and the advection velocity                  */
+
+/* A restart file of the handle's lattices (`what`: CLB_CKPT_FLOW | CLB_CKPT_TRANSPORT) in FP64,
+ * exact for every storage precision, with the step counters and the material map. Loading it
+ * into a handle created on the same material map and set up the same way (clb_flow_init,
+ * clb_ade_init, kinetics, biomass fields) continues the run exactly as the saved handle would.
+ * Not for runs with the automaton or precipitation set up (their state is not in the file).
+ * Replaces: saveBinaryBlock / loadBinaryBlock of the flow, substrate and biomass lattices
+ * (complab.cpp:2004, 2292-2302; 1106-1108, 2044-2055). */
+clb_status clb_checkpoint_save(clb_handle* h, const char* path, int what);
+clb_status clb_checkpoint_load(clb_handle* h, const char* path);
+
 /* ---------------------------------------------------------------- output */
 
 /* One VTK ImageData file (.vti, XML, inline base64 binary, UInt64 headers) of a domain field over
