@@ -249,6 +249,10 @@ def bench_d3q7(clb, workloads, torch, local, peak, steps=60, warmup=5, scale=1.0
     D.set_biomass(cfg["biomass"])
     D.set_kinetics(cfg["law"], cfg["params"], cfg["dt"])
     ms = timed_steps(torch, stream, D.ade_step, steps, warmup)
+    # the same step with the thermodynamic gate on the biotic rates (species 0 + 1 -> 2)
+    D.set_thermo_gate(species=(0, 1, 2), nu=(-1.0, -1.0, 1.0), dG0=-20.0, atp=0.25, dGatp=50.0)
+    ms_gate = timed_steps(torch, stream, D.ade_step, steps, warmup)
+    D.set_thermo_gate()
     S = len(cfg["species"])
     n_open = int(np.count_nonzero((mat != 0) & (mat != 1)))
     per = ms / steps
@@ -258,7 +262,8 @@ def bench_d3q7(clb, workloads, torch, local, peak, steps=60, warmup=5, scale=1.0
     D.close()
     return {"workload": cfg["name"] + ", FP32 populations, dual-Monod kinetics fused",
             "mlups_d3q7": S * n_open * steps / (ms * 1e-3) / 1e6, "unit": "species x open-voxel updates / s (1e6)",
-            "ms_per_step": per, "open_voxels": n_open, "species": S, "steps": steps,
+            "ms_per_step": per, "thermo_gate_ms_per_step": ms_gate / steps, "open_voxels": n_open, "species": S,
+            "steps": steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "algorithmic_bytes_per_node": alg_node, "kernel": "k_ade_aa (all species fused)"}}
 
