@@ -59,7 +59,7 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra
             C[s] = c < thr ? (TC)0 : c;
         }
         // the thermodynamic gate is compiled only into the EXT instantiations
-        const TC ft = (EXT && P.gate_on && P.M >= 1) ? (TC)thermo_gate<TC, NM>(P, C) : (TC)1;
+        const TC ft = (EXT && P.gate_on && P.M >= 1) ? thermo_gate<TC, NM>(P, C) : (TC)1;
         biotic_rates<TC, NM, true>(P, C, R, bio, nd, G.N, bc, ADE_THREADS, bn, ft);  // advances the biomass too
 #pragma unroll
         for (int s = 0; s < NM; ++s) {

@@ -86,26 +86,29 @@ __device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[N
 // The thermodynamic factor of Jin & Bethke (2003, 2005) on the floored concentrations C of the
 // rate law, used as activities: a_i = max(C_i conc_scale, cmin), ln Q = sum nu_i ln a_i,
 // dG = dG0 + RT ln Q + dGloss, x = (dG + m dG_ATP) / (chi RT), F_T = 0 for x >= 0, 1 for
-// x < -700, else 1 - exp(x) (complab3d_thermo.hh:215-258). FP64 throughout.
+// x < -700, else 1 - exp(x) (complab3d_thermo.hh:215-258). In the lattice's arithmetic type KT:
+// FP64 for FP64 lattices, FP32 (logf, expf) otherwise.
 template <typename KT, int NB>
-__device__ __forceinline__ double thermo_gate(const AdeParams& P, const KT (&C)[NB]) {
-    double lq = 0.0;
+__device__ __forceinline__ KT thermo_gate(const AdeParams& P, const KT (&C)[NB]) {
+    const KT cmin = (KT)P.gate_cmin, scale = (KT)P.gate_cscale;
+    KT lq = 0;
     for (int i = 0; i < P.gate_n; ++i) {
         const int sp = P.gate_sp[i];
         KT c = 0;
 #pragma unroll
         for (int s = 0; s < NB; ++s)
             if (s == sp) c = C[s];
-        double a = (double)c * P.gate_cscale;
-        if (!(a > P.gate_cmin)) a = P.gate_cmin;
-        lq += P.gate_nu[i] * log(a);
+        KT a = c * scale;
+        if (!(a > cmin)) a = cmin;
+        lq += (KT)P.gate_nu[i] * log(a);
     }
-    const double dG = P.gate_dG0 + P.gate_RT * lq + P.gate_dGloss;
-    const double x = (dG + P.gate_atp * P.gate_dGatp) / (P.gate_chi * P.gate_RT);
-    if (x >= 0.0) return 0.0;
-    if (x < -700.0) return 1.0;
-    const double F = 1.0 - exp(x);
-    return F < 0.0 ? 0.0 : (F > 1.0 ? 1.0 : F);
+    const KT RT = (KT)P.gate_RT;
+    const KT dG = (KT)P.gate_dG0 + RT * lq + (KT)P.gate_dGloss;
+    const KT x = (dG + (KT)(P.gate_atp * P.gate_dGatp)) / ((KT)P.gate_chi * RT);
+    if (x >= (KT)0) return (KT)0;
+    if (x < (KT)-700) return (KT)1;
+    const KT F = (KT)1 - exp(x);
+    return F < (KT)0 ? (KT)0 : (F > (KT)1 ? (KT)1 : F);
 }
 
 // Abiotic laws (clb_law CLB_LAW_PRECIP / CLB_LAW_MINERAL) over internal species indices, evaluated
@@ -204,7 +207,7 @@ __device__ void post_biotic(const AdeParams& P, const SparseView& S, const TS* g
         else if (s < P.S) c = (TC)Craw[s];
         C[s] = c < thr ? (TC)0 : c;
     }
-    const TC ft = (P.gate_on && P.M >= 1) ? (TC)thermo_gate<TC, CLB_MAX_SPECIES>(P, C) : (TC)1;
+    const TC ft = (P.gate_on && P.M >= 1) ? thermo_gate<TC, CLB_MAX_SPECIES>(P, C) : (TC)1;
     biotic_rates<TC, CLB_MAX_SPECIES, false>(P, C, R, bio, n, G.N, nullptr, 0, 0, ft);
 #pragma unroll
     for (int s = 0; s < CLB_MAX_SPECIES; ++s) {

@@ -248,6 +248,7 @@ typedef struct clb_thermo_desc {
  * F_T = max(0, 1 - exp((dG + atp dGatp) / (chi R T))), and every substrate and biomass rate of the
  * voxel is multiplied by F_T before dC = max(R dt, -C). As in the reference, the block applies to
  * microbe 0, so the gate acts only in a run with biomass fields. desc NULL or n_terms 0: off.
+ * F_T is evaluated in the lattice's arithmetic type (FP64 lattices: FP64; otherwise FP32).
  * The gate is compiled into the transport instantiations that also carry the abiotic block;
  * clb_batch_create refuses a gated domain.
  * Replaces: complab_thermo::gateFor (complab3d_thermo.hh:215-258, 669-692) in run_kinetics
