@@ -44,15 +44,16 @@ def test_f64_gated_dual_monod_matches_oracle(clb, oracle):
     assert np.max(np.abs(U.biomass()[0] - ob[0])) > 1e-6
 
 
-def test_f32_gated_dual_monod_error(clb, oracle):
-    D, O = gated_pair(clb, oracle, clb.F32)
+@pytest.mark.parametrize("prec,tol", [("F32", 1e-5), ("F16S", 3e-2)])
+def test_reduced_precision_gated_dual_monod_error(clb, oracle, prec, tol):
+    D, O = gated_pair(clb, oracle, getattr(clb, prec))
     D.ade_step(80)
     O.step(80)
     for s in range(3):
-        assert rel_l2(D.concentration(s), O.concentration(s)) < 1e-5, s
+        assert rel_l2(D.concentration(s), O.concentration(s)) < tol, s
     ob = O.biomass()
     for m in range(2):
-        assert rel_l2(D.biomass(m), ob[m]) < 1e-5, m
+        assert rel_l2(D.biomass(m), ob[m]) < tol, m
 
 
 def test_gate_without_microbes_changes_nothing(clb, oracle):
