@@ -328,6 +328,13 @@ __device__ __forceinline__ void ade_finish(TS* __restrict__ g, double* __restric
         for (int i = 0; i < 7; ++i) r += slot[i * T];
         rb[m] = r;
     }
+    {
+        // a NaN or infinite density in any species makes the sum non-finite: flag it for the host
+        TC chk = 0;
+#pragma unroll
+        for (int m = 0; m < NM; ++m) chk += rb[m];
+        if (!isfinite(chk) && P.nonfinite) *(volatile int*)P.nonfinite = 1;
+    }
     TC dC[NM];  // increments of the mobile species, in the arithmetic type of the deposit
     node_kinetics<TC, NM, EXT>(P, X, k, M.nd, code, west, east, n_mobile, rb, imm, bio, F.bio,
                                P.M < ade_bio_cache<TC>() ? P.M : ade_bio_cache<TC>(), dC);
@@ -536,83 +543,143 @@ __global__ void k_ade_set_pops(TS* __restrict__ g, TS* __restrict__ glink, const
     }
 }
 
-// Per-block FP64 partials of the live fields. Layout per block:
-// [S total][S content][S min][S max][M bio][1 nonfinite][1 open]. total/min/max/nonfinite over
-// open voxels of x=1..nx-2 (stored nodes that react); content = sum over stored nodes of
-// (sum of populations + 1) plus the wall link slots (the content held in walls that can move).
-template <typename TS>
-__global__ void k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ glink, const double* __restrict__ imm,
-                             const double* __restrict__ bio, const SparseView S, const AdeParams P,
-                             const int* __restrict__ mob_species, int n_mobile, double* __restrict__ part, int nq,
-                             int64_t k_west_end, int64_t k_east_begin, int odd) {
-    extern __shared__ double shq[];
-    const int S_ = P.S, M = P.M;
-    for (int q = threadIdx.x; q < nq; q += blockDim.x) shq[q] = 0.0;
-    __syncthreads();
-    for (int s = threadIdx.x; s < S_; s += blockDim.x) {
-        shq[2 * S_ + s] = 1e300;
-        shq[3 * S_ + s] = -1e300;
+// Deterministic FP64 reductions of the live fields. Block (b, r) of a grid of RED_BLOCKS x (S + 1)
+// covers the nodes k = b*256 + t + j*RED_BLOCKS*256 (thread t, j = 0, 1, ...) in that order; row
+// r < S reduces species r, row S the biomass fields and the open-voxel count. Each thread
+// accumulates in registers, a warp combines its lanes with a fixed shuffle tree, and warp 0 adds
+// the warps' partials in warp order, so every partial -- and k_reduce_combine's sum of them in
+// block order -- is the same number on every call: no atomics anywhere.
+// Partial rows (each RED_BLOCKS wide): [S total][S content][S min][S max][S non-finite][M bio][open].
+// total/min/max/non-finite over open voxels of x=1..nx-2 (stored nodes that react); content = sum
+// over stored nodes of (sum of populations + 1) plus the wall link slots (the content held in walls
+// that can move).
+constexpr int RED_THREADS = 256;
+
+__device__ __forceinline__ double warp_sum_fixed(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// fixed-order block combination; op 0 sum, 1 min, 2 max; result valid in thread 0
+__device__ __forceinline__ double block_fixed(double v, int op, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_down_sync(0xffffffffu, v, o);
+        v = op == 0 ? v + w : (op == 1 ? fmin(v, w) : fmax(v, w));
     }
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = sh[0];
+    if (threadIdx.x == 0)
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k)
+            r = op == 0 ? r + sh[k] : (op == 1 ? fmin(r, sh[k]) : fmax(r, sh[k]));
+    return r;
+}
+
+template <typename TS>
+__global__ void __launch_bounds__(RED_THREADS)
+    k_ade_reduce(const TS* __restrict__ g, const TS* __restrict__ glink, const double* __restrict__ imm,
+                 const double* __restrict__ bio, const SparseView S, const AdeParams P, double* __restrict__ part,
+                 int64_t k_west_end, int64_t k_east_begin, int odd) {
+    __shared__ double sh[RED_THREADS / 32];
+    const int S_ = P.S, M = P.M, B = gridDim.x, row = blockIdx.y;
     const int64_t K = S.K;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K || k < S.L;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        if (k < S.L)
-            for (int m = 0; m < n_mobile; ++m) atomicAdd(&shq[S_ + mob_species[m]], ldd(glink + (int64_t)m * S.SS + k));
-        if (k >= K) continue;
-        const int code = S.code[k];
-        const bool inner = k >= k_west_end && k < k_east_begin;
-        const bool open = inner && P.react[code];
-        if (open) atomicAdd(&shq[4 * S_ + M + 1], 1.0);
-        for (int s = 0; s < S_; ++s) {
-            double c;
-            const int m = P.slot[s];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t k0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row < S_) {
+        const int s = row, m = P.slot[s];
+        double tot = 0.0, cont = 0.0, mn = 1e300, mx = -1e300, nonf = 0.0;
+        if (m >= 0)
+            for (int64_t k = k0; k < S.L; k += stride) cont += ldd(glink + (int64_t)m * S.SS + k);
+        for (int64_t k = k0; k < K; k += stride) {
+            const int code = S.code[k];
+            const bool open = k >= k_west_end && k < k_east_begin && P.react[code];
+            double c = 0.0;
             if (m >= 0) {
                 // content: the node's own slots (every slot of the lattice counted once)
                 double sum = 1.0;
+#pragma unroll
                 for (int i = 0; i < 7; ++i) sum += ldd(g + (int64_t)m * S.SS + (int64_t)i * S.KS + k);
-                atomicAdd(&shq[S_ + s], sum);
+                cont += sum;
                 if (open) {
-                    // concentration: the node's incoming populations wherever the step parity
-                    // keeps them (computeDensity after the stream)
+                    // concentration: the node's incoming populations wherever the step parity keeps
+                    // them (computeDensity after the stream)
                     const double zero[7] = {0, 0, 0, 0, 0, 0, 0};
                     double pop[7];
                     natural<TS, double, 7>(S, P.g, g + (int64_t)m * S.SS, glink + (int64_t)m * S.SS, S.node[k], odd,
                                            zero, pop);
                     c = 1.0;
+#pragma unroll
                     for (int i = 0; i < 7; ++i) c += pop[i];
                 }
             } else {
                 c = imm[(int64_t)s * P.g.N + S.node[k]];
-                atomicAdd(&shq[S_ + s], c);
+                cont += c;
             }
             if (open) {
-                atomicAdd(&shq[s], c);
-                if (!isfinite(c)) atomicAdd(&shq[4 * S_ + M], 1.0);
-                double cur = shq[2 * S_ + s];
-                while (c < cur) {
-                    unsigned long long old = atomicCAS((unsigned long long*)&shq[2 * S_ + s],
-                                                       __double_as_longlong(cur), __double_as_longlong(c));
-                    if (old == (unsigned long long)__double_as_longlong(cur)) break;
-                    cur = __longlong_as_double(old);
-                }
-                cur = shq[3 * S_ + s];
-                while (c > cur) {
-                    unsigned long long old = atomicCAS((unsigned long long*)&shq[3 * S_ + s],
-                                                       __double_as_longlong(cur), __double_as_longlong(c));
-                    if (old == (unsigned long long)__double_as_longlong(cur)) break;
-                    cur = __longlong_as_double(old);
-                }
+                tot += c;
+                if (!isfinite(c)) nonf += 1.0;
+                mn = fmin(mn, c);
+                mx = fmax(mx, c);
             }
         }
-        if (inner)
-            for (int mb = 0; mb < M; ++mb) atomicAdd(&shq[4 * S_ + mb], bio[(int64_t)mb * P.g.N + S.node[k]]);
+        const double v[5] = {tot, cont, mn, mx, nonf};
+        const int op[5] = {0, 0, 1, 2, 0};
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+            const double r = block_fixed(v[j], op[j], sh);
+            if (threadIdx.x == 0) part[(int64_t)(j * S_ + s) * B + blockIdx.x] = r;
+        }
+    } else {
+        double open_n = 0.0;
+        for (int64_t k = k0; k < K; k += stride) {
+            const bool inner = k >= k_west_end && k < k_east_begin;
+            if (inner && P.react[S.code[k]]) open_n += 1.0;
+        }
+        double r = block_fixed(open_n, 0, sh);
+        if (threadIdx.x == 0) part[(int64_t)(5 * S_ + M) * B + blockIdx.x] = r;
+        for (int mb = 0; mb < M; ++mb) {
+            double b = 0.0;
+            for (int64_t k = k0; k < K; k += stride)
+                if (k >= k_west_end && k < k_east_begin) b += bio[(int64_t)mb * P.g.N + S.node[k]];
+            r = block_fixed(b, 0, sh);
+            if (threadIdx.x == 0) part[(int64_t)(5 * S_ + mb) * B + blockIdx.x] = r;
+        }
     }
-    __syncthreads();
-    for (int q = threadIdx.x; q < nq; q += blockDim.x) part[(int64_t)blockIdx.x * nq + q] = shq[q];
+}
+
+// Combines the partial rows in block order into the result layout
+// [S total][S content][S min][S max][M bio][non-finite][open]: one thread per result, a fixed
+// sequential order, so the result is bit-identical from call to call.
+__global__ void k_reduce_combine(const double* __restrict__ part, int blocks, int S, int M, double* __restrict__ out) {
+    const int nq = 4 * S + M + 2;
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        int row, op = 0, rows = 1;
+        if (q < 4 * S) { row = q; op = (q >= 2 * S && q < 3 * S) ? 1 : (q >= 3 * S ? 2 : 0); }
+        else if (q < 4 * S + M) row = 5 * S + (q - 4 * S);
+        else if (q == 4 * S + M) { row = 4 * S; rows = S; }  // non-finite of every species
+        else row = 5 * S + M;
+        double acc = op == 1 ? 1e300 : (op == 2 ? -1e300 : 0.0);
+        for (int r = 0; r < rows; ++r)
+            for (int b = 0; b < blocks; ++b) {
+                const double v = part[(int64_t)(row + r) * blocks + b];
+                acc = op == 0 ? acc + v : (op == 1 ? fmin(acc, v) : fmax(acc, v));
+            }
+        out[q] = acc;
+    }
 }
 
 // ------------------------------------------------------------------ host side
+
+// Doubles of scratch a reduction needs (S species, M microbes): the partial rows, then the result.
+static int64_t reduce_scratch_doubles(int S, int M, int blocks) {
+    return (int64_t)(5 * S + M + 1) * blocks + (4 * S + M + 2);
+}
+
+static int reduce_blocks(const clb_handle* h) { return h->num_sms * 2; }
 
 static size_t esize(int prec) { return prec == CLB_F64 ? 8 : (prec == CLB_F32 ? 4 : 2); }
 static size_t usize(int prec) { return prec == CLB_F64 ? 8 : 4; }
@@ -624,6 +691,7 @@ void ade_free(clb_handle* h) {
     cudaFree(h->d_bio); h->d_bio = nullptr;
     cudaFree(h->d_u); h->d_u = nullptr;
     cudaFree(h->d_neu); h->d_neu = nullptr;
+    cudaFree(h->d_red); h->d_red = nullptr;
     precip_free(h);
     ca_free(h);
     sparse_free(h->ade_sp);
@@ -713,6 +781,16 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
     if ((e = cudaMalloc(&h->d_u, usize(h->ade_prec) * 3 * K1)) != cudaSuccess) return cuda_check(h, e, "velocity");
     if ((e = cudaMalloc(&h->d_neu, sizeof(double) * S * 2 * h->g.plane + sizeof(int) * 16)) != cudaSuccess)
         return cuda_check(h, e, "boundary store");
+    if (!h->h_flags) {
+        // host-mapped flags the transport step sets (read by the host without a copy)
+        if ((e = cudaHostAlloc((void**)&h->h_flags, 16, cudaHostAllocMapped)) != cudaSuccess)
+            return cuda_check(h, e, "status flags");
+        std::memset(h->h_flags, 0, 16);
+        if ((e = cudaHostGetDevicePointer((void**)&h->d_flags, h->h_flags, 0)) != cudaSuccess)
+            return cuda_check(h, e, "status flags");
+    }
+    if ((e = cudaMalloc(&h->d_red, sizeof(double) * reduce_scratch_doubles(S, CLB_MAX_MICROBES, reduce_blocks(h)))) != cudaSuccess)
+        return cuda_check(h, e, "reduction scratch");
     cudaMemsetAsync(h->d_u, 0, usize(h->ade_prec) * 3 * K1, h->stream);
     // immobile species: uniform c0 (initial_concentration applies to the whole domain)
     std::vector<double> immh(N1);
@@ -751,6 +829,8 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
     h->ade_iters = 0;
     h->neu_iter = -1;
     h->ade_grid = h->num_sms * 4;
+    P.nonfinite = h->d_flags;
+    if (h->h_flags) h->h_flags[0] = 0;
     h->ade_ready = true;
     return cuda_check(h, cudaGetLastError(), "ade init");
 }
@@ -868,6 +948,8 @@ clb_status ade_set_thermo(clb_handle* h, const clb_thermo_desc* d) {
     P.gate_cmin = d->cmin;
     P.gate_RT = d->gas_constant * d->temperature;
     P.gate_cscale = d->conc_scale;
+    P.gate_x0 = (P.gate_dG0 + P.gate_dGloss + P.gate_atp * P.gate_dGatp) / (P.gate_chi * P.gate_RT);
+    P.gate_inv_chi = 1.0 / P.gate_chi;
     P.gate_on = 1;
     return CLB_OK;
 }
@@ -1088,9 +1170,20 @@ void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_m
 
 void ade_refresh_neumann(clb_handle* h) { refresh_neumann(h); }
 
+// A transport step that meets a NaN or infinite density sets a host-mapped flag; the run then
+// stops cleanly, as the reference stops on non-finite biomass or flow energy
+// (complab.cpp:2796, 3116-3117): the next clb_ade_step, and clb_synchronize once that step has
+// completed, return CLB_NONFINITE. Setting a species' populations clears the flag.
+clb_status ade_nonfinite_check(clb_handle* h) {
+    if (h->h_flags && ((volatile int*)h->h_flags)[0])
+        return fail(h, CLB_NONFINITE, "a transport step met a non-finite (NaN or Inf) concentration");
+    return CLB_OK;
+}
+
 clb_status ade_step(clb_handle* h, int n) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (h->M > 0 && h->d_bio == nullptr) return fail(h, CLB_INVALID_ARG, "biomass missing");
+    if (ade_nonfinite_check(h) != CLB_OK) return CLB_NONFINITE;
     for (int k = 0; k < n; ++k) {
         const bool odd = (h->ade_iters & 1) != 0;
         if (h->ap.dis_on) {
@@ -1149,6 +1242,10 @@ clb_status ade_populations(clb_handle* h, int s, double* host) {
 clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
+    if (h->h_flags) {
+        cudaStreamSynchronize(h->stream);  // no step in flight may set the flag after the clear
+        h->h_flags[0] = 0;
+    }
     s = h->u2i[s];
     if (h->ap.slot[s] < 0) return fail(h, CLB_INVALID_ARG, "not a mobile species");
     const int m = h->ap.slot[s];
@@ -1261,46 +1358,46 @@ clb_status ade_set_velocity(clb_handle* h, const double* host) {
     return cuda_check(h, e, "velocity upload");
 }
 
-clb_status ade_reduce(clb_handle* h, clb_stats* out) {
-    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+// Runs the reduction kernels on the handle's stream with scratch `buf` (reduce_scratch_doubles(S, M)
+// doubles) and reads the result back.
+static clb_status reduce_into(clb_handle* h, double* buf, clb_stats* out) {
     std::memset(out, 0, sizeof(*out));
     const int S = h->S, M = h->M;
     const int nq = 4 * S + M + 2;
-    const int grid = h->num_sms * 2;
-    double* part = nullptr;
-    cudaError_t e = cudaMalloc(&part, sizeof(double) * nq * grid);
-    if (e != cudaSuccess) return cuda_check(h, e, "reduce buffer");
-    int* mt = mob_table(h);
-    const size_t sh = sizeof(double) * nq;
+    const int blocks = reduce_blocks(h);
+    double* fin = buf + (size_t)(5 * S + M + 1) * blocks;
     const SparseView Sv = view_of(h->ade_sp);
+    const dim3 grid(blocks, S + 1);
+    const int odd = (int)(h->ade_iters & 1);
     switch (h->ade_prec) {
-        case CLB_F64: k_ade_reduce<double><<<grid, 256, sh, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
-        case CLB_F32: k_ade_reduce<float><<<grid, 256, sh, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
-        default: k_ade_reduce<__half><<<grid, 256, sh, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
+        case CLB_F64: k_ade_reduce<double><<<grid, RED_THREADS, 0, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, buf, h->ade_west_end, h->ade_east_begin, odd); break;
+        case CLB_F32: k_ade_reduce<float><<<grid, RED_THREADS, 0, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, buf, h->ade_west_end, h->ade_east_begin, odd); break;
+        default: k_ade_reduce<__half><<<grid, RED_THREADS, 0, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, buf, h->ade_west_end, h->ade_east_begin, odd); break;
     }
-    std::vector<double> hp((size_t)nq * grid);
-    e = cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, h->stream);
+    k_reduce_combine<<<1, 128, 0, h->stream>>>(buf, blocks, S, M, fin);
+    double q[4 * CLB_MAX_SPECIES + CLB_MAX_MICROBES + 2];
+    cudaError_t e = cudaMemcpyAsync(q, fin, sizeof(double) * nq, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(part);
     if (e != cudaSuccess) return cuda_check(h, e, "reduce");
-    for (int s = 0; s < S; ++s) { out->min_c[s] = 1e300; out->max_c[s] = -1e300; }
-    for (int b = 0; b < grid; ++b) {
-        const double* q = &hp[(size_t)b * nq];
-        for (int i = 0; i < S; ++i) {
-            const int s = h->i2u[i];
-            out->total[s] += q[i];
-            out->content[s] += q[S + i];
-            out->min_c[s] = std::min(out->min_c[s], q[2 * S + i]);
-            out->max_c[s] = std::max(out->max_c[s], q[3 * S + i]);
-        }
-        for (int mb = 0; mb < M; ++mb) out->biomass[mb] += q[4 * S + mb];
-        out->nonfinite += (int64_t)q[4 * S + M];
-        out->open_voxels += (int64_t)q[4 * S + M + 1];
+    for (int i = 0; i < S; ++i) {
+        const int s = h->i2u[i];
+        out->total[s] = q[i];
+        out->content[s] = q[S + i];
+        out->min_c[s] = q[2 * S + i];
+        out->max_c[s] = q[3 * S + i];
     }
+    for (int mb = 0; mb < M; ++mb) out->biomass[mb] = q[4 * S + mb];
+    out->nonfinite = (int64_t)q[4 * S + M];
+    out->open_voxels = (int64_t)q[4 * S + M + 1];
     out->ade_iterations = h->ade_iters;
     return CLB_OK;
 }
 
+// clb_reduce: the scratch is the handle's own buffer, allocated by ade_init.
+clb_status ade_reduce(clb_handle* h, clb_stats* out) {
+    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+    return reduce_into(h, h->d_red, out);
+}
 
 // ------------------------------------------------------------------ reduction without allocation
 //
@@ -1311,9 +1408,9 @@ clb_status ade_reduce(clb_handle* h, clb_stats* out) {
 // device memory is all handed to its own pool (where a cudaMalloc fails), or a loop that cannot
 // afford the device-wide synchronisation a cudaFree implies.
 //
-// Limit: the buffer holds REDUCE_SCRATCH_DOUBLES doubles; a call needs (blocks + 1) x (4 S + M + 2)
-// of them (blocks = 2 x the SM count, S species, M microbes) and is refused with
-// CLB_INVALID_ARG when that does not fit. Every word of the buffer a call reads was written
+// Limit: the buffer holds REDUCE_SCRATCH_DOUBLES doubles; a call needs blocks x (5 S + M + 1) +
+// (4 S + M + 2) of them (blocks = 2 x the SM count, S species, M microbes: 26,418 on a 148-SM B200
+// at the largest S = 16, M = 8) and is refused with CLB_INVALID_ARG when that does not fit. Every word of the buffer a call reads was written
 // earlier in the same call, so nothing has to start at zero. The buffer is one per device and
 // shared by all handles on it: two calls that overlap in time on one device (different host
 // threads, or different streams without ordering between them) race on it and return wrong
@@ -1321,19 +1418,6 @@ clb_status ade_reduce(clb_handle* h, clb_stats* out) {
 // first call before any stream capture begins.
 constexpr int REDUCE_SCRATCH_DOUBLES = 65536;  // 512 KiB
 static __device__ __align__(256) double g_reduce_scratch[REDUCE_SCRATCH_DOUBLES];
-
-// combine the per-block partials in block order (the order the host loop of ade_reduce uses)
-__global__ void k_reduce_combine(const double* __restrict__ part, int blocks, int nq, int S, double* __restrict__ out) {
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
-        const bool is_min = q >= 2 * S && q < 3 * S, is_max = q >= 3 * S && q < 4 * S;
-        double acc = is_min ? 1e300 : (is_max ? -1e300 : 0.0);
-        for (int b = 0; b < blocks; ++b) {
-            const double v = part[(int64_t)b * nq + q];
-            acc = is_min ? fmin(acc, v) : (is_max ? fmax(acc, v) : acc + v);
-        }
-        out[q] = acc;
-    }
-}
 
 static std::mutex g_scratch_mutex;
 constexpr int MAX_DEVICES = 64;
@@ -1356,40 +1440,12 @@ static clb_status reduce_scratch(clb_handle* h, double** ptr) {
 clb_status ade_reduce_noalloc(clb_handle* h, clb_stats* out) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     std::memset(out, 0, sizeof(*out));
-    const int S = h->S, M = h->M;
-    const int nq = 4 * S + M + 2;
-    const int grid = h->num_sms * 2;
-    if ((int64_t)(grid + 1) * nq > REDUCE_SCRATCH_DOUBLES)
+    if (reduce_scratch_doubles(h->S, h->M, reduce_blocks(h)) > REDUCE_SCRATCH_DOUBLES)
         return fail(h, CLB_INVALID_ARG, "reduction needs more scratch than the fixed 65536-double buffer holds");
     double* part = nullptr;
     clb_status st = reduce_scratch(h, &part);
     if (st != CLB_OK) return st;
-    double* fin = part + (size_t)grid * nq;
-    int* mt = mob_table(h);
-    const size_t sh = sizeof(double) * nq;
-    const SparseView Sv = view_of(h->ade_sp);
-    switch (h->ade_prec) {
-        case CLB_F64: k_ade_reduce<double><<<grid, 256, sh, h->stream>>>((const double*)h->d_g, (const double*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
-        case CLB_F32: k_ade_reduce<float><<<grid, 256, sh, h->stream>>>((const float*)h->d_g, (const float*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
-        default: k_ade_reduce<__half><<<grid, 256, sh, h->stream>>>((const __half*)h->d_g, (const __half*)h->d_glink, h->d_imm, h->d_bio, Sv, h->ap, mt, h->n_mobile, part, nq, h->ade_west_end, h->ade_east_begin, (int)(h->ade_iters & 1)); break;
-    }
-    k_reduce_combine<<<1, 128, 0, h->stream>>>(part, grid, nq, S, fin);
-    double q[4 * CLB_MAX_SPECIES + CLB_MAX_MICROBES + 2];
-    cudaError_t e = cudaMemcpyAsync(q, fin, sizeof(double) * nq, cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) return cuda_check(h, e, "reduce");
-    for (int i = 0; i < S; ++i) {
-        const int s = h->i2u[i];
-        out->total[s] = q[i];
-        out->content[s] = q[S + i];
-        out->min_c[s] = q[2 * S + i];
-        out->max_c[s] = q[3 * S + i];
-    }
-    for (int mb = 0; mb < M; ++mb) out->biomass[mb] = q[4 * S + mb];
-    out->nonfinite = (int64_t)q[4 * S + M];
-    out->open_voxels = (int64_t)q[4 * S + M + 1];
-    out->ade_iterations = h->ade_iters;
-    return CLB_OK;
+    return reduce_into(h, part, out);
 }
 
 }  // namespace clb

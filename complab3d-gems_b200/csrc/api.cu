@@ -1,6 +1,7 @@
 // api.cu -- the extern "C" surface: handle lifetime, status reporting, field transfer.
 #include "clb_internal.cuh"
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -103,6 +104,7 @@ clb_status clb_destroy(clb_handle* h) {
     cudaFree(h->d_spec_stats);
     cudaFree(h->d_mlp);
     cudaFree(h->d_mlp_bf16);
+    if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
     return CLB_OK;
@@ -112,11 +114,12 @@ clb_status clb_synchronize(clb_handle* h) {
     if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
     CLB_ON_DEVICE(h);
     clb_status s = cuda_check(h, cudaStreamSynchronize(h->stream), "synchronize");
-    if (s != CLB_OK || !h->d_err) return s;
+    if (s != CLB_OK) return s;
+    if (!h->d_err) return ade_nonfinite_check(h);
     int flag = 0;
     cudaMemcpy(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost);
     if (flag) return fail(h, CLB_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
-    return CLB_OK;
+    return ade_nonfinite_check(h);
 }
 
 clb_status clb_set_stream(clb_handle* h, void* stream) {
@@ -185,7 +188,7 @@ clb_status clb_flow_solve(clb_handle* h, int max_it, double eps, int* iterations
     if (max_it < 0 || !(eps > 0)) return fail(h, CLB_INVALID_ARG, "bad solve arguments");
     clb_status s = flow_solve(h, max_it, eps, iterations);
     if (s == CLB_NOT_CONVERGED) h->err = "flow did not converge within the iteration cap";
-    return s;
+    return s;  // CLB_NONFINITE: diverged; CLB_PERCOLATION_LOST: no outlet flow at the cap
 }
 
 clb_status clb_flow_stats_get(clb_handle* h, double char_length, clb_flow_stats* out) {

@@ -39,6 +39,7 @@
 #include "sparse.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 namespace clb {
@@ -87,6 +88,7 @@ struct CaScalars {
     unsigned int remaining;
     unsigned int changed;  // ages changed by a sweep
     unsigned int overflow; // active voxels beyond the capacity
+    unsigned int nonfinite; // biomass values that are NaN or infinite (mask pass)
 };
 
 // ------------------------------------------------------------------ set-up and mask update
@@ -124,6 +126,7 @@ __global__ void k_ca_mask_total(const CaView C, int8_t* __restrict__ mat, const 
             int newmask = 0;
             for (int m = 0; m < C.M; ++m) {
                 const double bm = bio[(int64_t)m * G.N + n];
+                if (!isfinite(bm)) atomicAdd(&sc->nonfinite, 1u);  // the run stops (complab.cpp:2796)
                 if (bm > 1e-14) {
                     bmass += bm;
                     newmask += C.bio_code[m];
@@ -528,6 +531,8 @@ static clb_status ca_scalars(clb_handle* h, CaScalars& s) {
 
 // mask / total pass; returns max(total) and the mask sum
 static clb_status ca_mask_pass(clb_handle* h, const CaView& C, double& gmax, long long& msum) {
+    // non-finite biomass stops the run cleanly, as the reference does after this pass
+    // (complab.cpp:2794-2796)
     CaScalars s;
     std::memset(&s, 0, sizeof s);
     s.gmax = LLONG_MIN;
@@ -539,6 +544,8 @@ static clb_status ca_mask_pass(clb_handle* h, const CaView& C, double& gmax, lon
     if (st != CLB_OK) return st;
     gmax = unordered(s.gmax);
     msum = s.mask_sum;
+    if (s.nonfinite || !std::isfinite(gmax))
+        return fail(h, CLB_NONFINITE, "non-finite biomass (NaN or Inf) in the biofilm fields");
     return CLB_OK;
 }
 

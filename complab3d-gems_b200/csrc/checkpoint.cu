@@ -5,6 +5,13 @@
 // immobile: concentration), the biomass fields and the advection velocity, in FP64 (exact for
 // every storage precision), with the step counters; loading it into a handle set up on the same
 // material map continues the run exactly as the saved handle would.
+//
+// The header records which species are mobile and the biofilm material codes, because a species'
+// block size follows from its mobility: a handle whose mobile set differs would otherwise read
+// misaligned blocks. A save writes `path`.tmp and renames it over `path` once the file is complete,
+// so a crash or a full disk during a save leaves the previous restart point intact. A load reads
+// and checks the whole file into host memory before it changes the handle, so a truncated or
+// mismatched file leaves the handle exactly as it was.
 #include "clb_internal.cuh"
 
 #include <cstdio>
@@ -17,17 +24,29 @@ using namespace clb;
 namespace {
 
 const char MAGIC[8] = {'C', 'L', 'B', 'C', 'K', 'P', 'T', '1'};
+constexpr int32_t VERSION = 2;
 
 struct Header {
     char magic[8];
     int32_t version, nx, ny, nz, flow_prec, ade_prec, S, M, what, pad;
     int64_t flow_iters, ade_iters;
+    uint32_t mobile_mask;                   // bit s: user species s is mobile
+    int32_t n_microbes;                     // the domain's biofilm materials
+    int32_t bio_codes[CLB_MAX_MICROBES];
+    int32_t pad2;
 };
 
 bool put(std::FILE* f, const void* p, size_t n) { return std::fwrite(p, 1, n, f) == n; }
 bool get(std::FILE* f, void* p, size_t n) { return std::fread(p, 1, n, f) == n; }
 
 bool mobile(const clb_handle* h, int s) { return h->ap.slot[h->u2i[s]] >= 0; }
+
+uint32_t mobile_mask(const clb_handle* h) {
+    uint32_t m = 0;
+    for (int s = 0; s < h->S; ++s)
+        if (mobile(h, s)) m |= 1u << s;
+    return m;
+}
 
 }  // namespace
 
@@ -45,7 +64,7 @@ clb_status clb_checkpoint_save(clb_handle* h, const char* path, int what) {
     Header hd;
     std::memset(&hd, 0, sizeof(hd));
     std::memcpy(hd.magic, MAGIC, 8);
-    hd.version = 1;
+    hd.version = VERSION;
     hd.nx = h->g.nx; hd.ny = h->g.ny; hd.nz = h->g.nz;
     hd.flow_prec = h->flow_prec;
     hd.ade_prec = h->ade_prec;
@@ -54,8 +73,12 @@ clb_status clb_checkpoint_save(clb_handle* h, const char* path, int what) {
     hd.what = what;
     hd.flow_iters = h->flow_iters;
     hd.ade_iters = h->ade_iters;
-    std::FILE* f = std::fopen(path, "wb");
-    if (!f) return fail(h, CLB_INVALID_ARG, std::string("cannot open ") + path);
+    hd.mobile_mask = (what & CLB_CKPT_TRANSPORT) ? mobile_mask(h) : 0;
+    hd.n_microbes = h->d.n_microbes;
+    for (int m = 0; m < h->d.n_microbes && m < CLB_MAX_MICROBES; ++m) hd.bio_codes[m] = h->d.bio_codes[m];
+    const std::string tmp = std::string(path) + ".tmp";
+    std::FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return fail(h, CLB_INVALID_ARG, "cannot open " + tmp);
     bool ok = put(f, &hd, sizeof(hd)) && put(f, h->h_mat.data(), N);
     clb_status st = CLB_OK;
     std::vector<double> buf;
@@ -82,9 +105,17 @@ clb_status clb_checkpoint_save(clb_handle* h, const char* path, int what) {
             ok = st == CLB_OK && put(f, buf.data(), sizeof(double) * buf.size());
         }
     }
+    if (ok && std::fflush(f) != 0) ok = false;
     if (std::fclose(f) != 0) ok = false;
-    if (st != CLB_OK) return st;
-    if (!ok) return fail(h, CLB_INVALID_ARG, std::string("cannot write ") + path);
+    if (!ok || st != CLB_OK) {
+        std::remove(tmp.c_str());
+        if (st != CLB_OK) return st;
+        return fail(h, CLB_INVALID_ARG, "cannot write " + tmp);
+    }
+    if (std::rename(tmp.c_str(), path) != 0) {
+        std::remove(tmp.c_str());
+        return fail(h, CLB_INVALID_ARG, std::string("cannot replace ") + path);
+    }
     return CLB_OK;
 }
 
@@ -100,11 +131,14 @@ clb_status clb_checkpoint_load(clb_handle* h, const char* path) {
         std::fclose(f);
         return fail(h, CLB_INVALID_ARG, "checkpoint " + std::string(path) + ": " + why);
     };
-    if (!get(f, &hd, sizeof(hd)) || std::memcmp(hd.magic, MAGIC, 8) != 0 || hd.version != 1)
-        return bad("not a checkpoint of this library");
+    if (!get(f, &hd, sizeof(hd)) || std::memcmp(hd.magic, MAGIC, 8) != 0 || hd.version != VERSION)
+        return bad("not a checkpoint of this library version");
     if (hd.nx != h->g.nx || hd.ny != h->g.ny || hd.nz != h->g.nz) return bad("lattice size differs");
     if (!get(f, mat.data(), N)) return bad("truncated");
     if (std::memcmp(mat.data(), h->h_mat.data(), N) != 0) return bad("saved on a different material map");
+    if (hd.n_microbes != h->d.n_microbes) return bad("biofilm materials differ");
+    for (int m = 0; m < hd.n_microbes && m < CLB_MAX_MICROBES; ++m)
+        if (hd.bio_codes[m] != h->d.bio_codes[m]) return bad("biofilm materials differ");
     if (hd.what & CLB_CKPT_FLOW) {
         if (!h->flow_ready) return bad("holds the flow lattice; clb_flow_init first");
         if (hd.flow_prec != h->flow_prec) return bad("flow storage precision differs");
@@ -113,40 +147,55 @@ clb_status clb_checkpoint_load(clb_handle* h, const char* path) {
         if (!h->ade_ready) return bad("holds the species lattices; clb_ade_init first");
         if (hd.ade_prec != h->ade_prec) return bad("transport storage precision differs");
         if (hd.S != h->S || hd.M != h->M) return bad("species or microbe count differs");
+        if (hd.mobile_mask != mobile_mask(h)) return bad("mobile species differ");
     }
-    std::vector<double> buf;
+    // the whole payload into host memory first: nothing of the handle changes unless all of it is there
+    std::vector<double> flow, vel;
+    std::vector<std::vector<double>> spec, bio;
+    if (hd.what & CLB_CKPT_FLOW) {
+        flow.resize(19 * N);
+        if (!get(f, flow.data(), sizeof(double) * flow.size())) return bad("truncated");
+    }
+    if (hd.what & CLB_CKPT_TRANSPORT) {
+        spec.resize(h->S);
+        for (int s = 0; s < h->S; ++s) {
+            spec[s].resize((mobile(h, s) ? 7 : 1) * N);
+            if (!get(f, spec[s].data(), sizeof(double) * spec[s].size())) return bad("truncated");
+        }
+        bio.resize(h->M);
+        for (int m = 0; m < h->M; ++m) {
+            bio[m].resize(N);
+            if (!get(f, bio[m].data(), sizeof(double) * N)) return bad("truncated");
+        }
+        vel.resize(3 * N);
+        if (!get(f, vel.data(), sizeof(double) * vel.size())) return bad("truncated");
+    }
+    if (std::fgetc(f) != EOF) return bad("trailing data after the last field");
+    std::fclose(f);
+
+    const int64_t save_flow = h->flow_iters, save_ade = h->ade_iters;
     clb_status st = CLB_OK;
     if (hd.what & CLB_CKPT_FLOW) {
-        buf.resize(19 * N);
-        if (!get(f, buf.data(), sizeof(double) * buf.size())) return bad("truncated");
         // the counter first: the populations go into the slots of the step parity it gives
         h->flow_iters = hd.flow_iters;
         Tracer tz;
         std::memset(&tz, 0, sizeof(tz));
         tz.iterations = hd.flow_iters;
         cudaError_t e = cudaMemcpy(h->d_tracer, &tz, sizeof(tz), cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) { std::fclose(f); return cuda_check(h, e, "tracer"); }
-        if ((st = clb_set_field(h, CLB_FIELD_FLOW_POPULATIONS, 0, buf.data(), 0)) != CLB_OK) { std::fclose(f); return st; }
+        if (e != cudaSuccess) { h->flow_iters = save_flow; return cuda_check(h, e, "tracer"); }
+        if ((st = clb_set_field(h, CLB_FIELD_FLOW_POPULATIONS, 0, flow.data(), 0)) != CLB_OK) return st;
     }
     if (hd.what & CLB_CKPT_TRANSPORT) {
         h->ade_iters = hd.ade_iters;
         for (int s = 0; s < h->S; ++s) {
-            const bool mob = mobile(h, s);
-            buf.resize((mob ? 7 : 1) * N);
-            if (!get(f, buf.data(), sizeof(double) * buf.size())) return bad("truncated");
-            st = mob ? clb_set_field(h, CLB_FIELD_ADE_POPULATIONS, s, buf.data(), 0) : ade_set_immobile(h, s, buf.data());
-            if (st != CLB_OK) { std::fclose(f); return st; }
+            st = mobile(h, s) ? clb_set_field(h, CLB_FIELD_ADE_POPULATIONS, s, spec[s].data(), 0)
+                              : ade_set_immobile(h, s, spec[s].data());
+            if (st != CLB_OK) { h->ade_iters = save_ade; return st; }
         }
-        for (int m = 0; m < h->M; ++m) {
-            buf.resize(N);
-            if (!get(f, buf.data(), sizeof(double) * N)) return bad("truncated");
-            if ((st = clb_set_field(h, CLB_FIELD_BIOMASS, m, buf.data(), 0)) != CLB_OK) { std::fclose(f); return st; }
-        }
-        buf.resize(3 * N);
-        if (!get(f, buf.data(), sizeof(double) * buf.size())) return bad("truncated");
-        if ((st = clb_set_field(h, CLB_FIELD_ADE_VELOCITY, 0, buf.data(), 0)) != CLB_OK) { std::fclose(f); return st; }
+        for (int m = 0; m < h->M; ++m)
+            if ((st = clb_set_field(h, CLB_FIELD_BIOMASS, m, bio[m].data(), 0)) != CLB_OK) return st;
+        if ((st = clb_set_field(h, CLB_FIELD_ADE_VELOCITY, 0, vel.data(), 0)) != CLB_OK) return st;
     }
-    std::fclose(f);
     return CLB_OK;
 }
 

@@ -130,6 +130,8 @@ struct AdeParams {
     int gate_sp[CLB_MAX_SPECIES];
     double gate_nu[CLB_MAX_SPECIES];
     double gate_dG0, gate_dGloss, gate_atp, gate_dGatp, gate_chi, gate_cmin, gate_RT, gate_cscale;
+    double gate_x0, gate_inv_chi;   // (dG0 + dGloss + atp dGatp) / (chi RT) and 1 / chi
+    int* nonfinite;                 // host-mapped flag a transport step sets on a NaN / Inf density
 };
 
 // Per-node state of the precipitation / dissolution machinery (geometry_update.cu), passed to the
@@ -198,6 +200,8 @@ struct clb_handle_s {
     int flow_odd_pipe = 1;            // odd step pipelined through shared memory (4- and 8-byte storage)
     int flow_pipe_grid = 0;           // its resident-CTA grid; 0 where it is not available
     int* d_err = nullptr;             // device error flag (bounded waits that gave up)
+    int* h_flags = nullptr;           // host-mapped pinned flags: [0] a transport step met a non-finite
+    int* d_flags = nullptr;           // density (its device alias)
     int64_t flow_iters = 0;           // host mirror of the device iteration count
     double delta_p = 0;
 
@@ -217,6 +221,7 @@ struct clb_handle_s {
     double* d_bio = nullptr;          // [M][N] biomass
     void* d_u = nullptr;              // [3][K] advection velocity (arithmetic type)
     double* d_neu = nullptr;          // [S][2][ny*nz] stored boundary densities
+    double* d_red = nullptr;          // scratch of clb_reduce (partials, then the result)
     clb::AdeParams ap;
     int64_t ade_iters = 0;
     int64_t neu_iter = -1;            // iteration whose stream the Neumann store reflects
@@ -291,6 +296,7 @@ void flow_free(clb_handle* h);
 // ade.cu
 clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S);
 clb_status ade_step(clb_handle* h, int n);
+clb_status ade_nonfinite_check(clb_handle* h);
 clb_status ade_couple(clb_handle* h);
 clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm, double dt);
 clb_status ade_set_biomass(clb_handle* h, int M, const double* b);

@@ -974,7 +974,21 @@ clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations) {
     int zero = 0;
     cudaMemcpyAsync(&h->d_tracer->converged, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream);
     cudaStreamSynchronize(h->stream);
-    return conv ? CLB_OK : CLB_NOT_CONVERGED;
+    // a diverged solve (NaN or Inf stored energy; the tracer reads a NaN window as settled) stops
+    // the run cleanly, as complab.cpp:3116-3117 does
+    if (!std::isfinite(cur.energy))
+        return fail(h, CLB_NONFINITE, "flow solve diverged: the stored average energy is not finite");
+    if (!conv) {
+        // at the cap with nothing leaving through the outlet plane the flow path is sealed: the
+        // reference's percolation limit (complab.cpp:3106-3113, outlet u_x <= 1e-12)
+        clb_flow_stats st;
+        clb_status s = flow_stats(h, 1.0, &st);
+        if (s != CLB_OK) return s;
+        if (!(st.darcy_outlet_ux > THRD))
+            return fail(h, CLB_PERCOLATION_LOST, "percolation lost: no flow through the outlet plane at the iteration cap");
+        return CLB_NOT_CONVERGED;
+    }
+    return CLB_OK;
 }
 
 // Velocity at `count` dense nodes (all nodes when nodes == nullptr) into a device buffer

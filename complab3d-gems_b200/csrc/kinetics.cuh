@@ -102,12 +102,14 @@ __device__ __forceinline__ KT thermo_gate(const AdeParams& P, const KT (&C)[NB])
         if (!(a > cmin)) a = cmin;
         lq += (KT)P.gate_nu[i] * log(a);
     }
-    const KT RT = (KT)P.gate_RT;
-    const KT dG = (KT)P.gate_dG0 + RT * lq + (KT)P.gate_dGloss;
-    const KT x = (dG + (KT)(P.gate_atp * P.gate_dGatp)) / ((KT)P.gate_chi * RT);
+    // x = (dG0 + RT lnQ + dGloss + atp dGatp) / (chi RT) = x0 + lnQ / chi, with the constant x0
+    // formed on the host in FP64 so that FP32 lattices do not lose x to the cancellation of dG0
+    // against atp dGatp near the threshold; F = -expm1(x) keeps full relative precision there
+    // (1 - exp(x) would cancel as x -> 0-)
+    const KT x = (KT)P.gate_x0 + lq * (KT)P.gate_inv_chi;
     if (x >= (KT)0) return (KT)0;
     if (x < (KT)-700) return (KT)1;
-    const KT F = (KT)1 - exp(x);
+    const KT F = -expm1(x);
     return F < (KT)0 ? (KT)0 : (F > (KT)1 ? (KT)1 : F);
 }
 

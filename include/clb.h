@@ -189,7 +189,10 @@ clb_status clb_flow_step(clb_handle* h, int n);
 
 /* Runs collideAndStream until util::ValueTracer(1,1000,eps) on the stored average energy
  * converges or max_it calls are made (complab.cpp:1113-1124). *iterations receives the
- * number of collideAndStream calls made. Returns CLB_NOT_CONVERGED at the cap. */
+ * number of collideAndStream calls made. Returns CLB_NOT_CONVERGED at the cap while the outlet
+ * plane x = nx-2 still flows, CLB_PERCOLATION_LOST at the cap when its mean u_x is at most 1e-12
+ * (the flow path is sealed; complab.cpp:3106-3113), and CLB_NONFINITE when the stored energy is
+ * NaN or infinite (the solve diverged; complab.cpp:3116-3117). */
 clb_status clb_flow_solve(clb_handle* h, int max_it, double eps, int* iterations);
 
 /* Velocity statistics and permeability (complab.cpp:1136-1160). */
@@ -259,10 +262,16 @@ clb_status clb_set_thermo_gate(clb_handle* h, const clb_thermo_desc* desc);
 clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass);
 
 /* n transport iterations: collide every mobile species, kinetics, deposit, stream, Neumann
- * planes (complab.cpp:2307-2315, 2340-2452, 3251-3259), fused in one pass per step. */
+ * planes (complab.cpp:2307-2315, 2340-2452, 3251-3259), fused in one pass per step.
+ * A step that meets a NaN or infinite concentration sets a flag the host reads without a copy;
+ * the run then stops as the reference stops on non-finite values (complab.cpp:2796, 3116-3117):
+ * the next clb_ade_step, and clb_synchronize once that step has completed, return
+ * CLB_NONFINITE. clb_set_field of a species' populations clears the flag. */
 clb_status clb_ade_step(clb_handle* h, int n);
 
-/* FP64 reductions over the live fields (complab3d_processors_part3.hh:387-600). */
+/* FP64 reductions over the live fields (complab3d_processors_part3.hh:387-600). Warp shuffles and
+ * a fixed order over warps and blocks, no atomics: the same fields give the same bits on every
+ * call. Scratch is the handle's own (allocated by clb_ade_init); nothing is allocated per call. */
 clb_status clb_reduce(clb_handle* h, clb_stats* out);
 
 /* The same reductions as clb_reduce, computed without allocating: no counterpart in the
@@ -270,8 +279,9 @@ clb_status clb_reduce(clb_handle* h, clb_stats* out);
  * allocate while they monitor a run (an application that hands all device memory to its own
  * pool, or a loop that cannot absorb the device-wide synchronisation of a free). The partial
  * sums live in one fixed 65536-double buffer per device, built into the library; a handle whose
- * reduction needs more ((2 x SMs + 1) x (4 x species + microbes + 2) doubles) gets
- * CLB_INVALID_ARG. The buffer is shared by every handle on a device, so calls must not overlap
+ * reduction needs more (2 x SMs x (5 x species + microbes + 1) + 4 x species + microbes + 2
+ * doubles; 26,418 at 16 species and 8 microbes on 148 SMs) gets CLB_INVALID_ARG. Same
+ * fixed-order tree as clb_reduce, so the two give the same bits. The buffer is shared by every handle on a device, so calls must not overlap
  * in time on one device (they would race on it). The first call on a device looks the buffer
  * up; make it before any stream capture begins. */
 clb_status clb_reduce_noalloc(clb_handle* h, clb_stats* out);
@@ -351,6 +361,7 @@ clb_status clb_ca_setup(clb_handle* h, const clb_ca_desc* desc);
  * the reference stops the run (no progress in 100 sweeps, more than 1000 sweeps, or an age
  * relaxation that does not settle). Voxels of the ghost planes x = 0 and x = nx-1 never push. */
 clb_status clb_ca_step(clb_handle* h, int* sweeps, int* mask_changed);
+/* (clb_ca_step returns CLB_NONFINITE when a biomass value is NaN or infinite, complab.cpp:2796.) */
 
 /* Dynamics follow the mask: species != 0 runs updateSoluteDynamics3D (pore / biofilm relaxation,
  * complab3d_processors_part2.hh:485-553), flow != 0 updateNsLatticesDynamics3D (:748-818). The

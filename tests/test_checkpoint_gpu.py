@@ -71,3 +71,78 @@ def test_load_refuses_another_map(clb, tmp_path):
         E.checkpoint_load(path)
     with pytest.raises(clb.ClbError):
         D.checkpoint_save(path, flow=False, transport=False)
+
+
+def test_truncated_file_leaves_the_handle_unchanged(clb, tmp_path):
+    """A load that fails part-way (the file ends early) changes nothing: the step counters, the
+    populations and the concentrations are those the handle had before the call."""
+    shape = (14, 8, 7)
+    mat = mixed_geometry(*shape, seed=3)
+    bio = np.zeros((2, mat.size))
+    A = setup(clb, mat, shape, clb.F64, bio)
+    A.flow_step(11)
+    A.couple_velocity()
+    A.ade_step(9)
+    path = os.path.join(tmp_path, "full.chk")
+    A.checkpoint_save(path)
+    assert not os.path.exists(path + ".tmp")
+    raw = open(path, "rb").read()
+    B = setup(clb, mat, shape, clb.F64, bio)
+    B.flow_step(4)
+    B.couple_velocity()
+    B.ade_step(5)
+    before = state(B)
+    for cut in (len(raw) - 8, len(raw) // 2, 200):
+        short = os.path.join(tmp_path, f"cut{cut}.chk")
+        open(short, "wb").write(raw[:cut])
+        with pytest.raises(clb.ClbError, match="truncated|not a checkpoint"):
+            B.checkpoint_load(short)
+        for a, b in zip(before, state(B)):
+            np.testing.assert_array_equal(a, b)
+    # one more step runs from the unchanged state at the unchanged parity
+    C = setup(clb, mat, shape, clb.F64, bio)
+    C.flow_step(4)
+    C.couple_velocity()
+    C.ade_step(5)
+    B.ade_step(3)
+    C.ade_step(3)
+    np.testing.assert_array_equal(B.concentration(0), C.concentration(0))
+
+
+def test_load_refuses_a_different_mobile_set(clb, tmp_path):
+    """Two handles with the same species and microbe counts but mobile and immobile species
+    swapped: the blocks would have different sizes, so the load is refused."""
+    shape = (12, 8, 7)
+    mat = mixed_geometry(*shape, seed=5)
+    sp_a = [dict(omega_pore=1.0, left_type=1, right_type=1, c0=0.1),
+            dict(omega_pore=1.0, mobile=0, left_type=1, right_type=1, c0=0.2)]
+    sp_b = [dict(omega_pore=1.0, mobile=0, left_type=1, right_type=1, c0=0.1),
+            dict(omega_pore=1.0, left_type=1, right_type=1, c0=0.2)]
+    A = clb.Domain(mat, *shape, 0.8, flow_precision=clb.F64, ade_precision=clb.F64)
+    A.flow_init(3e-4)
+    A.ade_init(sp_a)
+    path = os.path.join(tmp_path, "m.chk")
+    A.checkpoint_save(path)
+    B = clb.Domain(mat, *shape, 0.8, flow_precision=clb.F64, ade_precision=clb.F64)
+    B.flow_init(3e-4)
+    B.ade_init(sp_b)
+    with pytest.raises(clb.ClbError, match="mobile species differ"):
+        B.checkpoint_load(path)
+
+
+def test_save_replaces_the_file_whole(clb, tmp_path):
+    """Saving over an existing restart file goes through a temporary file and a rename: the old
+    file stays readable until the new one is complete, and no temporary file is left behind."""
+    shape = (12, 8, 7)
+    mat = mixed_geometry(*shape, seed=6)
+    D = clb.Domain(mat, *shape, 0.8, flow_precision=clb.F64)
+    D.flow_init(3e-4)
+    path = os.path.join(tmp_path, "r.chk")
+    D.checkpoint_save(path, transport=False)
+    D.flow_step(3)
+    D.checkpoint_save(path, transport=False)
+    assert sorted(os.listdir(tmp_path)) == ["r.chk"]
+    E = clb.Domain(mat, *shape, 0.8, flow_precision=clb.F64)
+    E.flow_init(3e-4)
+    E.checkpoint_load(path)
+    np.testing.assert_array_equal(E.flow_populations(), D.flow_populations())

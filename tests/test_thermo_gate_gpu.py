@@ -96,3 +96,38 @@ def test_batch_refuses_a_gated_domain(clb, oracle):
     D, _ = gated_pair(clb, oracle, clb.F64)
     with pytest.raises(clb.ClbError):
         clb.Batch([D])
+
+
+def test_fp32_gate_keeps_relative_precision_near_the_threshold(clb, oracle):
+    """With x = (dG + m dG_ATP)/(chi R T) in [-1e-3, 0) the gate is F_T = -expm1(x) ~ |x|. The FP32
+    lattice evaluates it to the FP64 lattice's value within 1e-4 relative per voxel: the constant
+    part of x is formed in FP64 (no cancellation of dG0 against m dG_ATP in FP32) and F_T comes
+    from expm1 (no cancellation of 1 - exp(x)). Compared on one step's biomass increment (decay
+    off), which is the gated growth rate itself."""
+    shape = (16, 9, 8)
+    mat = mixed_geometry(*shape, seed=4)
+    u = flow_field(oracle, mat, shape)
+    rng = np.random.default_rng(7)
+    bio = np.zeros((2, mat.size))
+    bio[0, mat == 3] = rng.uniform(10, 60, size=(mat == 3).sum())
+    bio[1, mat == 4] = rng.uniform(10, 60, size=(mat == 4).sum())
+    RT = 8.314462618e-3 * 298.15
+    incs = {}
+    for xs in (-1e-4, -7e-4):
+        # a tiny stoichiometric number keeps ln Q's part of x (|nu ln a| <= 1e-8 x 20.8) below
+        # 1 % of it; the donor starts at 0.5 everywhere so every biofilm voxel grows in the first step
+        gate = dict(GATE, species=(0,), nu=(1e-8,), atp=0.25, dGatp=50.0, dG0=-12.5 + xs * RT)
+        species = [dict(SPECIES[0], c0=0.5)] + SPECIES[1:]
+        for prec in (clb.F64, clb.F32):
+            D, _ = pair(clb, oracle, mat, shape, species, prec, u, law=3, params=[1e-3, 0.1, 0.4, 0.0],
+                        biomass=bio)
+            D.set_thermo_gate(**gate)
+            D.ade_step(1)
+            incs[prec] = D.biomass(0) - bio[0]
+            D.close()
+        live = incs[clb.F64] > 0
+        assert live.sum() > 10
+        ratio = incs[clb.F64][live] / (-np.expm1(xs))
+        assert np.all(ratio > 0)
+        err = np.abs(incs[clb.F32][live] / incs[clb.F64][live] - 1.0)
+        assert err.max() < 1e-4, (xs, err.max())

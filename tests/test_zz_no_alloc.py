@@ -1,10 +1,10 @@
 """clb_reduce_noalloc (reductions from the library's fixed per-device buffer, no allocation)
 against clb_reduce on the same live fields, two calls in a row.
 
-The per-block partial sums of both entry points are accumulated with shared-memory atomics, whose
-order varies from call to call, so sums agree to a relative 1e-12; minima, maxima and counts are
-exact. This file is named to be collected last, so the entry point is also exercised after every
-other GPU test has used the device."""
+Both entry points run the same fixed-order reduction tree (warp shuffles, then warps and blocks in
+a fixed order, no atomics), so their results are the same bits, call after call; only the scratch
+they use differs. This file is named to be collected last, so the entry point is also exercised
+after every other GPU test has used the device."""
 import numpy as np
 import pytest
 
@@ -17,7 +17,6 @@ SPECIES = [
     dict(omega_pore=1 / 0.62, omega_biofilm=1 / 0.56, left_type=1, right_type=0, right_bc=0.4, c0=0.2),
     dict(omega_pore=1.0, mobile=0, left_type=1, right_type=1, c0=0.8),
 ]
-SUM_RTOL = 1e-12
 
 
 def make_domain(clb, prec):
@@ -38,15 +37,13 @@ def make_domain(clb, prec):
 
 
 def assert_same(a, b):
-    for key in ("total", "content", "biomass"):
-        np.testing.assert_allclose(a[key], b[key], rtol=SUM_RTOL, atol=0, err_msg=key)
-    for key in ("min", "max"):
-        np.testing.assert_array_equal(a[key], b[key], err_msg=key)
+    for key in ("total", "content", "biomass", "min", "max"):
+        assert a[key].tobytes() == b[key].tobytes(), key
     for key in ("open_voxels", "nonfinite", "ade_iterations"):
         assert a[key] == b[key], key
 
 
-@pytest.mark.parametrize("prec", ["F64", "F32"])
+@pytest.mark.parametrize("prec", ["F64", "F32", "F16S"])
 def test_noalloc_reduce_matches_reduce_twice_in_a_row(clb, prec):
     D = make_domain(clb, getattr(clb, prec))
     D.ade_step(37)
