@@ -1,28 +1,32 @@
 #!/usr/bin/env python
-"""Throughput of the D3Q19 flow step on the 256x128x128 overlapping-sphere pack (porosity 0.35,
-grain radius U[3, 8], tau 0.7), FP32 populations, one GPU per rank.
+"""Throughput of the coupled reactive-transport step on the 256^3 sphere pack (porosity 0.40):
+D3Q19 flow (FP32) + 8 D3Q7 species (FP32) with dual-Monod kinetics of two biofilm microbes, the
+biofilm automaton every iteration and the flow re-solved every 500 iterations -- the largest
+configuration that fits one GPU.
 
-A step is one collide-and-stream of the whole lattice (one launch of the AA kernel). MLUPS
-counts open (collide) voxels; the all-voxel figure is reported alongside. Only the collide/stream nodes
-are stored (sparse layout), so the FP32 lattice is about the size of L2: the benchmark flushes L2
-between timed steps and times each step with its own event pair.
+A step is one update interval: 500 coupled iterations (fused transport step of all species,
+automaton, dynamics refresh) followed by the flow re-solve to the ValueTracer criterion 1e-6 and
+the velocity coupling, driven by clb_run in the reference's loop order. The default 20 steps are
+the configuration's 10,000 iterations. MLUPS counts lattice-node updates of both lattices: species
+x open voxels per transport iteration plus open voxels per flow iteration. The lattices (about
+1.5 GB of species populations) are far larger than L2, so no flush is needed.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Side measurements in the same JSON line (rank 0, one GPU; --no-extra skips them):
-  "d3q7"       fused transport of the 256^3 pack, 8 species, 2 microbes, FP32: species-voxel
-               updates per second and its HBM roofline;
+  "flow"       the D3Q19 step alone on the 256x128x128 pack (FP32, L2 flushed between steps) and
+               its roofline;
+  "d3q7"       the fused transport step alone with and without the thermodynamic gate;
   "precision"  FP64 / FP32 / FP16-shifted flow throughput and the velocity, permeability and
                concentration errors of the reduced-precision paths against the FP64 path;
-  "speciation" the 5 x 12 tableau in transport: Newton-Raphson against the trained surrogate
-               (time per step, solves per second, speed-up, error against Newton-Raphson);
-  "ensemble"   96 uneven domains with flow and 3 species advanced by the batched, graph-replayed
-               steps: domain-steps per second and aggregate MLUPS.
+  "speciation" the 5 x 12 tableau in transport: Newton-Raphson against the trained surrogate;
+  "ensemble"   96 uneven domains with flow and 3 species advanced by the batched steps.
 
 Multi-GPU: the domain does not shard on this path (single-domain solver); each rank advances
 its own replica and the value is the sum over ranks divided by the slowest rank's time.
 The reference arm times the FP64 CPU restatement of the reference path (the reference itself
-needs Palabos, which is not available) on all host cores, on a bounded x-slab of the same map.
+needs Palabos, which is not available) on all host cores, on the full map of the same
+configuration, built without the product library.
 """
 from __future__ import annotations
 
@@ -46,17 +50,16 @@ PEAK_FALLBACK = 6650.0
 def args_():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=4000)
-    p.add_argument("--warmup", type=int, default=50)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--precision", default="f32", choices=["f64", "f32", "f16s"])
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-extra", action="store_true", help="skip the D3Q7, precision and speciation legs")
     p.add_argument("--scale", type=float, default=1.0, help="shrink the workload (testing only)")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the library's default kernel variants (profiling runs: timings under a profiler "
                         "would mislead the autotuner)")
-    p.add_argument("--leg", choices=["d3q7", "precision", "speciation", "ensemble"],
+    p.add_argument("--leg", choices=["flow", "d3q7", "precision", "speciation", "ensemble"],
                    help="run only this side measurement (with --scale for d3q7) and print its JSON; "
                         "a small case for profilers, not a bench line")
     return p.parse_args()
@@ -166,13 +169,6 @@ def cpu_name():
     return "unknown"
 
 
-def slab(mat, shape, nx_s):
-    nx, ny, nz = shape
-    m = mat.reshape(nx, ny, nz)[:nx_s].copy()
-    m[-1] = m[-2]
-    return m.ravel(), (nx_s, ny, nz)
-
-
 def oracle_mlups(mat, shape, tau, dp, min_seconds, min_steps, max_steps):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -190,31 +186,84 @@ def oracle_mlups(mat, shape, tau, dp, min_seconds, min_steps, max_steps):
     return n_open * steps / dt / 1e6, threads, steps, dt
 
 
-def run_reference(a, cfg):
+class CoupledOracle:
+    """The FP64 CPU restatement of the coupled step (oracle/) on a configuration's full map: flow
+    lattice, the species lattices with the kinetics, the biofilm automaton. Built from the workload
+    description only (maps from the oracle's own generator), so the product library is not loaded."""
+
+    def __init__(self, cfg):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        self.threads = oracle.max_threads()
+        oracle.set_threads(self.threads)
+        nx, ny, nz = cfg["shape"]
+        mat = cfg["mat"]
+        self.F = oracle.OracleFlow(mat, nx, ny, nz, cfg["tau"], cfg["delta_p"], bio_codes=cfg["bio_codes"],
+                                   perm_ratio=cfg["perm_ratio"])
+        self.F.step(2)
+        self.A = oracle.OracleAde(mat, nx, ny, nz, cfg["species"], self.F.velocity(), bio_codes=cfg["bio_codes"])
+        self.A.set_biomass(cfg["biomass"])
+        self.A.set_kinetics(cfg["law"], cfg["params"], cfg["dt"])
+        self.A.ca_setup(cfg["bmax"], cfg["biofilm_fraction"], cfg["ca_seed"], bio_codes=cfg["bio_codes"])
+        self.S = len(cfg["species"])
+        self.n_open = int(np.count_nonzero((mat != 0) & (mat != 1)))
+        self.n_flow = self.n_open  # flow BGK nodes: pore and (permeable) biofilm
+
+    def transport_iteration(self):
+        """One coupled iteration: the species step with kinetics, then the automaton."""
+        t0 = time.perf_counter()
+        self.A.step(1)
+        self.A.ca_step()
+        return time.perf_counter() - t0
+
+    def flow_iteration(self):
+        t0 = time.perf_counter()
+        self.F.step(1)
+        return time.perf_counter() - t0
+
+    def mixed_mlups(self, t_transport, t_flow, flow_per_transport):
+        """MLUPS of the coupled step's mix: per transport iteration S x n_open species updates and
+        flow_per_transport x n_flow flow updates (the re-solve's iterations spread over its interval)."""
+        upd = self.S * self.n_open + flow_per_transport * self.n_flow
+        return upd / (t_transport + flow_per_transport * t_flow) / 1e6
+
+
+def run_reference(a, workloads):
+    """The reference arm: the oracle's coupled step on the full map of the headline configuration,
+    all host threads, rank 0 only. Each step is one transport iteration (8 species + automaton) and
+    one flow iteration, timed separately; the step's MLUPS weights them by the configuration's mix
+    (flow iterations of a re-solve over its 500-iteration interval)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    mat, shape = slab(cfg["mat"], cfg["shape"], 18)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    threads = oracle.max_threads()
-    oracle.set_threads(threads)
-    O = oracle.OracleFlow(mat, *shape, cfg["tau"], cfg["delta_p"])
-    n_open = int(np.sum(mat == 2))
-    O.step(max(1, a.warmup))
-    t0 = time.perf_counter()
-    O.step(a.steps)
-    dt = time.perf_counter() - t0
-    v = n_open * a.steps / dt / 1e6
-    sample = f"x-slab 16+2 planes of the 256x128x128 map ({shape[0]}x{shape[1]}x{shape[2]}), FP64, {a.steps} steps"
+    cfg = workloads.pack256cube_8species(scale=a.scale, gen=oracle.sphere_pack)
+    t_build = time.perf_counter()
+    O = CoupledOracle(cfg)
+    t_build = time.perf_counter() - t_build
+    mix = workloads.FLOW_PER_TRANSPORT_CONFIG3
+    for _ in range(max(1, a.warmup)):
+        O.transport_iteration()
+        O.flow_iteration()
+    tt = tf = 0.0
+    for _ in range(a.steps):
+        tt += O.transport_iteration()
+        tf += O.flow_iteration()
+    v = O.mixed_mlups(tt / a.steps, tf / a.steps, mix)
+    nx, ny, nz = cfg["shape"]
+    sample = (f"{a.steps} coupled iterations (8 species + automaton) and {a.steps} flow iterations of the full "
+              f"{nx}x{ny}x{nz} map, FP64, weighted {mix:.3f} flow iterations per transport iteration")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": a.gpus, "steps": a.steps,
-        "warmup": a.warmup, "ms_per_step": dt / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "warmup": a.warmup, "ms_per_step": (tt + tf) / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sphere pack)",
-        "config": {"workload": cfg["name"] + " (x-slab sample)", "nx": shape[0], "ny": shape[1], "nz": shape[2],
-                   "open_voxels": n_open},
-        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port", "cpu": cpu_name(),
+        "config": {"workload": cfg["name"] + ", coupled step", "nx": nx, "ny": ny, "nz": nz,
+                   "open_voxels": O.n_open, "transport_s_per_iteration": tt / a.steps,
+                   "flow_s_per_iteration": tf / a.steps, "build_s": t_build},
+        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": O.threads, "kind": "port", "cpu": cpu_name(),
                          "sample": sample},
         "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -430,134 +479,193 @@ def bench_ensemble(clb, workloads, torch, local, steps=200):
             "autotune": tuned, "timing": "host clock around the batched steps (one synchronisation)"}
 
 
+def bench_flow(clb, workloads, torch, local, peak, steps=200, warmup=20, precision="f32", autotune=True):
+    """The D3Q19 step alone on the 256x128x128 overlapping-sphere pack (porosity 0.35, tau 0.7):
+    the compacted FP32 lattice (~113 MB) is about the size of L2, so L2 is flushed between timed
+    steps on the same stream (a 256 MB buffer written and then read back, so the L2 holds clean
+    lines of that buffer); one event pair per step."""
+    cfg = workloads.pack256x128x128()
+    prec = {"f64": clb.F64, "f32": clb.F32, "f16s": clb.F16S}[precision]
+    es = {"f64": 8, "f32": 4, "f16s": 2}[precision]
+    nx, ny, nz = cfg["shape"]
+    D = clb.Domain(cfg["mat"], nx, ny, nz, cfg["tau"], flow_precision=prec, device=local)
+    stream = torch.cuda.Stream()
+    D.set_stream(stream.cuda_stream)
+    D.flow_init(cfg["delta_p"])
+    tuned = D.autotune(20) if autotune else "defaults"
+    st = D.flow_stats()
+    n_open = st["bgk_nodes"]
+    D.flow_step(warmup)
+    D.sync()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush_sum = torch.empty((), dtype=torch.int64, device="cuda")
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        ev0[k].record(stream)
+        D.flow_step(1)
+        ev1[k].record(stream)
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 255)
+            torch.sum(flush.view(torch.int64), dim=0, out=flush_sum)
+    ev1[-1].synchronize()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1))
+    D.close()
+    per = ms / steps
+    alg = 2 * 19 * es * n_open
+    achieved = alg / (per * 1e-3) / 1e9
+    return {"workload": cfg["name"] + f", D3Q19 IncBGK, {precision.upper()} populations",
+            "mlups_d3q19": n_open * steps / (ms * 1e-3) / 1e6, "ms_per_step": per, "open_voxels": n_open,
+            "autotune": tuned, "l2": "flushed between timed steps (256 MB write, then read back)",
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic_per_launch(f"k_flow_aa_{precision}_pack256x128x128"),
+                         "algorithmic_bytes_per_launch": alg, "kernel": step_kernels(tuned, precision)}}
+
+
+def setup_config3(clb, cfg, local, stream=None, autotune=True, mat=None, biomass=None):
+    """The coupled configuration on one device: flow to the ValueTracer criterion from rest, the
+    species lattices at rest, the biomass fields, the kinetics, the automaton."""
+    nx, ny, nz = cfg["shape"]
+    D = clb.Domain(cfg["mat"] if mat is None else mat, nx, ny, nz, cfg["tau"], flow_precision=clb.F32,
+                   ade_precision=clb.F32, bio_codes=cfg["bio_codes"], perm_ratio=cfg["perm_ratio"], device=local)
+    if stream is not None:
+        D.set_stream(stream.cuda_stream)
+    D.flow_init(cfg["delta_p"])
+    tuned = D.autotune(10) if autotune else "defaults"
+    it, conv = D.flow_solve(cfg["flow_max_iterations"], cfg["eps"], allow_unconverged=True)
+    D.ade_init(cfg["species"])
+    D.couple_velocity()
+    D.set_biomass(cfg["biomass"] if biomass is None else biomass)
+    D.set_kinetics(cfg["law"], cfg["params"], cfg["dt"])
+    D.ca_setup(cfg["bmax"], cfg["biofilm_fraction"], cfg["ca_seed"])
+    return D, {"initial_flow_iterations": it, "initial_flow_converged": conv, "autotune": tuned}
+
+
+def run_block(D, cfg):
+    """One step of the headline: one update interval of the coupled step."""
+    return D.run(cfg["resolve_every"], ca=True, ade_update_interval=1, resolve_every=cfg["resolve_every"],
+                 flow_max_iterations=cfg["flow_max_iterations"], flow_eps=cfg["eps"])
+
+
 def main():
     a = args_()
-    import clb
     import workloads
 
     if a.impl == "reference":
-        run_reference(a, workloads.pack256x128x128(scale=a.scale))
+        run_reference(a, workloads)
         return
 
+    import clb
     import torch
-
-    if a.leg:
-        local = int(os.environ.get("LOCAL_RANK", "0"))
-        torch.cuda.set_device(local)
-        fn = {"d3q7": lambda: bench_d3q7(clb, workloads, torch, local, peaks()[0], steps=10, warmup=3, scale=a.scale),
-              "precision": lambda: bench_precision(clb, workloads, torch, local),
-              "speciation": lambda: bench_speciation(clb, workloads, torch, local),
-              "ensemble": lambda: bench_ensemble(clb, workloads, torch, local)}[a.leg]
-        print(json.dumps({"leg": a.leg, "scale": a.scale, a.leg: fn()}))
-        return
-    cfg = workloads.pack256x128x128(scale=a.scale)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    peak, peak_kind = peaks()
+    if a.leg:
+        fn = {"d3q7": lambda: bench_d3q7(clb, workloads, torch, local, peak, steps=10, warmup=3, scale=a.scale),
+              "flow": lambda: bench_flow(clb, workloads, torch, local, peak, autotune=not a.no_autotune),
+              "precision": lambda: bench_precision(clb, workloads, torch, local),
+              "speciation": lambda: bench_speciation(clb, workloads, torch, local),
+              "ensemble": lambda: bench_ensemble(clb, workloads, torch, local)}.get(a.leg)
+        if fn is not None:
+            print(json.dumps({"leg": a.leg, "scale": a.scale, a.leg: fn()}))
+            return
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    prec = {"f64": clb.F64, "f32": clb.F32, "f16s": clb.F16S}[a.precision]
-    es = {"f64": 8, "f32": 4, "f16s": 2}[a.precision]
-    nx, ny, nz = cfg["shape"]
-    mat = cfg["mat"]
-
-    D = clb.Domain(mat, nx, ny, nz, cfg["tau"], flow_precision=prec, device=local)
-    stream = torch.cuda.Stream()
-    D.set_stream(stream.cuda_stream)
-    D.flow_init(cfg["delta_p"])
-    tuned = "defaults" if a.no_autotune else D.autotune(20)
-    st = D.flow_stats()
-    n_open, n_active = st["bgk_nodes"], st["active_nodes"]
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
 
-    D.flow_step(a.warmup)
+    cfg = workloads.pack256cube_8species(scale=a.scale)
+    nx, ny, nz = cfg["shape"]
+    S = len(cfg["species"])
+    M = cfg["biomass"].shape[0]
+    stream = torch.cuda.Stream()
+    D, setup_info = setup_config3(clb, cfg, local, stream, autotune=not a.no_autotune)
+    n_open = int(np.count_nonzero((cfg["mat"] != 0) & (cfg["mat"] != 1)))
+    n_flow = D.flow_stats()["bgk_nodes"]
+    for _ in range(a.warmup):
+        run_block(D, cfg)
     D.sync()
     barrier()
     torch.cuda.synchronize()
-    # The compacted FP32 lattice (~120 MB) is about the size of L2, so L2 is flushed between
-    # timed steps on the same stream: a 256 MB buffer is written and then read back, so the L2
-    # ends up holding clean lines of that buffer (none of the lattice, and no dirty lines whose
-    # write-back the next step would pay for). Only the steps are timed (one event pair each).
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    flush_sum = torch.empty((), dtype=torch.int64, device="cuda")
-    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
-    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    reps, ms_blocks = [], []
     with ClockSampler(local) as clocks:
-        for s in range(a.steps):
-            ev0[s].record(stream)
-            D.flow_step(1)
-            ev1[s].record(stream)
-            with torch.cuda.stream(stream):
-                flush.fill_(s & 255)
-                torch.sum(flush.view(torch.int64), dim=0, out=flush_sum)
-        ev1[-1].synchronize()
+        for _ in range(a.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            reps.append(run_block(D, cfg))
+            e1.record(stream)
+            e1.synchronize()
+            ms_blocks.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
     barrier()
-    ms = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1))
-    del flush, flush_sum
-    ms = max_over_ranks(torch, ms, world, "cuda")
-    per_step = ms / a.steps
-    value = replica_throughput(n_open, a.steps, ms, world)
-    all_vox = world * nx * ny * nz * a.steps / (ms * 1e-3) / 1e6
-
-    # roofline of the step kernel: algorithmic bytes = 2 * 19 * sizeof(storage) per open node
-    alg = 2 * 19 * es * n_open
-    peak, peak_kind = peaks()
-    achieved = alg / (per_step * 1e-3) / 1e9
-    key = f"k_flow_aa_{a.precision}_pack256x128x128"
-    tr = traffic_per_launch(key)
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": tr, "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg,
-            "kernel": step_kernels(tuned, a.precision)}
-
+    final = D.reduce()
     D.close()
     del D
-    torch.cuda.synchronize()
-    # end to end through the C ABI with host buffers: create (the material map goes in from pinned
-    # host memory) + init (the layout is built on the device) + the same steps + the velocity back
-    # into pinned host memory, in the storage's precision
-    k_e2e = a.steps
-    udt = torch.float64 if a.precision == "f64" else torch.float32
-    mat_host = torch.empty(mat.size, dtype=torch.int8, pin_memory=True).numpy()
-    mat_host[:] = mat
-    u_host = torch.empty(3 * mat.size, dtype=udt, pin_memory=True).numpy()
-    # the whole job three times; the median job time is reported
-    t_jobs, phases = [], []
-    for _ in range(3):
+    ms = max_over_ranks(torch, sum(ms_blocks), world, "cuda")
+    iters = sum(r["iterations"] for r in reps)
+    flow_its = sum(r["flow_iterations"] for r in reps)
+    upd = S * n_open * iters + n_flow * flow_its
+    value = world * upd / (ms * 1e-3) / 1e6
+    ms_transport = sum(r["ms_transport"] for r in reps)
+    launches = sum(r["launches"] for r in reps)
+
+    # roofline of the dominant kernel, the fused transport step: algorithmic bytes per open node =
+    # S x 2 x 7 x 4 B populations + 12 B velocity + 1 B material + M x 8 B biomass
+    alg_node = S * 2 * 7 * 4 + 3 * 4 + 1 + M * 8
+    per_launch = ms_transport / max(1, iters)
+    achieved = alg_node * n_open / (per_launch * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic_per_launch("k_ade_aa_f32_pack256cube_8species"), "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": alg_node * n_open, "algorithmic_bytes_per_node": alg_node,
+            "kernel": "k_ade_aa (all 8 species fused, even/odd AA steps) + k_ade_neumann, the fused transport "
+                      "step; mean device time per iteration from CUDA events on the handle's stream",
+            "share_of_step": ms_transport / sum(ms_blocks)}
+
+    # end to end through the C ABI with host buffers: the material map and the biomass fields go in
+    # from pinned host memory; create, flow solve from rest, species set-up, the same K update
+    # intervals, and every species' concentration and the biomass back into pinned host memory
+    t_e2e = None
+    job = {}
+    if rank == 0 or world > 1:
+        mat_host = torch.empty(cfg["mat"].size, dtype=torch.int8, pin_memory=True).numpy()
+        mat_host[:] = cfg["mat"]
+        bio_host = torch.empty(cfg["biomass"].size, dtype=torch.float64, pin_memory=True).numpy()
+        bio_host[:] = cfg["biomass"].ravel()
+        out_host = torch.empty((S + M, nx * ny * nz), dtype=torch.float64, pin_memory=True).numpy()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        E = clb.Domain(mat_host, nx, ny, nz, cfg["tau"], flow_precision=prec, device=local)
+        E, _ = setup_config3(clb, cfg, local, None, autotune=False, mat=mat_host, biomass=bio_host)
+        E.sync()
         t1 = time.perf_counter()
-        E.flow_init(cfg["delta_p"])
+        for _ in range(a.steps):
+            run_block(E, cfg)
         E.sync()
         t2 = time.perf_counter()
-        E.flow_step(k_e2e)
-        E.sync()
+        lib = clb.lib()
+        for s in range(S):
+            E._check(lib.clb_get_field(E.h, clb.FIELD_CONCENTRATION, s, out_host[s].ctypes.data_as(clb.C.c_void_p), 0))
+        for m in range(M):
+            E._check(lib.clb_get_field(E.h, clb.FIELD_BIOMASS, m, out_host[S + m].ctypes.data_as(clb.C.c_void_p), 0))
         t3 = time.perf_counter()
-        u = E.velocity(u_host.dtype, out=u_host)
-        t4 = time.perf_counter()
-        t_jobs.append(t4 - t0)
-        phases.append({"create": 1e3 * (t1 - t0), "init": 1e3 * (t2 - t1), "steps": 1e3 * (t3 - t2),
-                       "velocity_to_host": 1e3 * (t4 - t3)})
         E.close()
-        del E
-    t_e2e = statistics.median(t_jobs)
-    job_phases = phases[t_jobs.index(t_e2e)]
-    e2e_val = world * n_open * k_e2e / t_e2e / 1e6
-    h2d = mat_host.nbytes  # the compacted layout is built on the device from the map
-    d2h = u.nbytes
+        t_e2e = t3 - t0
+        job = {"setup_s": t1 - t0, "steps_s": t2 - t1, "result_to_host_s": t3 - t2}
+        e2e_val = world * upd / t_e2e / 1e6
+        h2d = mat_host.nbytes + bio_host.nbytes
+        d2h = out_host.nbytes
 
     extra = {}
     if rank == 0 and world == 1 and not a.no_extra and a.scale == 1.0:
-        for key, fn in (("d3q7", lambda: bench_d3q7(clb, workloads, torch, local, peak)),
+        for key, fn in (("flow", lambda: bench_flow(clb, workloads, torch, local, peak, autotune=not a.no_autotune)),
+                        ("d3q7", lambda: bench_d3q7(clb, workloads, torch, local, peak)),
                         ("precision", lambda: bench_precision(clb, workloads, torch, local)),
                         ("speciation", lambda: bench_speciation(clb, workloads, torch, local)),
                         ("ensemble", lambda: bench_ensemble(clb, workloads, torch, local))):
@@ -569,28 +677,50 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        v, threads, steps, dt = oracle_mlups(mat, cfg["shape"], cfg["tau"], cfg["delta_p"], 12.0, 2, 400)
-        cpu = {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port", "cpu": cpu_name(),
-               "sample": f"{steps} FP64 steps of the full 258x128x128 map in {dt:.1f} s (OpenMP)"}
+        # the oracle on the full map (its own map generator, the same voxels), a bounded sample:
+        # two coupled iterations and two flow iterations, weighted by this run's own mix
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        ocfg = workloads.pack256cube_8species(scale=a.scale, gen=oracle.sphere_pack)
+        O = CoupledOracle(ocfg)
+        O.transport_iteration()
+        tt = sum(O.transport_iteration() for _ in range(2)) / 2
+        tf = sum(O.flow_iteration() for _ in range(2)) / 2
+        mix = flow_its / max(1, iters)
+        cpu = {"value": O.mixed_mlups(tt, tf, mix), "unit": "MLUPS", "cores": O.threads, "kind": "port",
+               "cpu": cpu_name(),
+               "sample": f"2 coupled iterations (8 species + automaton, {tt:.2f} s each) and 2 flow iterations "
+                         f"({tf:.2f} s each) of the full map, FP64, weighted by this run's {mix:.3f} flow "
+                         "iterations per transport iteration"}
+        del O
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": a.precision, "data": "synthetic (seeded sphere pack)",
-            "config": {"workload": cfg["name"] + f", D3Q19 IncBGK, {a.precision.upper()} populations",
-                       "nx": nx, "ny": ny, "nz": nz, "open_voxels": n_open, "active_nodes": n_active,
-                       "all_voxel_mlups": all_vox, "l2": "flushed between timed steps (256 MB write, then read back); "
-                       "compacted lattice %.0f MB" % (19 * es * n_active / 1e6), "parallelism": f"replicas x{world}",
-                       "autotune": tuned},
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sphere pack)",
+            "config": {"workload": cfg["name"] + ", coupled step: FP32 D3Q19 flow + 8 x FP32 D3Q7, dual-Monod, "
+                       "biofilm automaton every iteration, flow re-solved every 500 iterations",
+                       "step": "one update interval = 500 coupled iterations + the flow re-solve (1e-6)",
+                       "nx": nx, "ny": ny, "nz": nz, "species": S, "microbes": M, "open_voxels": n_open,
+                       "flow_nodes": n_flow, "iterations": iters, "flow_iterations": flow_its,
+                       "ca_sweeps": sum(r["ca_sweeps"] for r in reps),
+                       "mask_changes": sum(r["mask_changes"] for r in reps),
+                       "ms_transport": ms_transport, "ms_ca": sum(r["ms_ca"] for r in reps),
+                       "ms_flow": sum(r["ms_flow"] for r in reps),
+                       "l2": "not flushed: 1.5 GB of species populations per step, far larger than L2",
+                       "parallelism": f"replicas x{world}", "final_totals": list(map(float, final["total"])),
+                       "final_biomass": list(map(float, final["biomass"][:M])), **setup_info},
             "roofline": roof,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": "MLUPS", "h2d_bytes_per_step": h2d / k_e2e,
-                    "d2h_bytes_per_step": d2h / k_e2e,
-                    "note": "one job through the C ABI: create + init + K steps + velocity to host, wall clock; "
-                            "median of 3 jobs", "job_seconds": t_jobs,
-                    "median_job_phases_ms": job_phases},
-            "gpu_launches": a.steps,
+            "e2e": None if t_e2e is None else {
+                "value": e2e_val, "unit": "MLUPS", "h2d_bytes_per_step": h2d / a.steps,
+                "d2h_bytes_per_step": d2h / a.steps,
+                "note": "one job through the C ABI: create from pinned host buffers, flow solve from rest, "
+                        "species set-up, K update intervals, every concentration and biomass field to pinned "
+                        "host memory; wall clock", "job_phases_s": job},
+            "gpu_launches": launches,
             "clocks": clocks.summary(),
         }
         line.update(extra)

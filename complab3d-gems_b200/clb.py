@@ -98,7 +98,22 @@ class PrecipDesc(C.Structure):
 
 
 class CaDesc(C.Structure):
-    _fields_ = [("max_biomass", C.c_double), ("biofilm_fraction", C.c_double), ("seed", C.c_uint64)]
+    _fields_ = [("max_biomass", C.c_double), ("biofilm_fraction", C.c_double), ("seed", C.c_uint64),
+                ("push_mode", C.c_int32)]
+
+
+class RunDesc(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("ca", C.c_int32), ("ade_update_interval", C.c_int32),
+                ("ns_update_interval", C.c_int32), ("resolve_every", C.c_int32), ("geometry_interval", C.c_int32),
+                ("flow_max_iterations", C.c_int32), ("flow_eps", C.c_double)]
+
+
+class RunReport(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("ca_sweeps", C.c_int64), ("mask_changes", C.c_int64),
+                ("flow_resolves", C.c_int64), ("flow_iterations", C.c_int64), ("flow_unconverged", C.c_int64),
+                ("sealed", C.c_int64), ("reopened", C.c_int64), ("ms_transport", C.c_double), ("ms_ca", C.c_double),
+                ("ms_flow", C.c_double), ("ms_geometry", C.c_double), ("seconds", C.c_double),
+                ("launches", C.c_int64)]
 
 
 class SpeciationStats(C.Structure):
@@ -151,6 +166,7 @@ SIGNATURES = {
     "clb_reduce_noalloc": [C.c_void_p, C.POINTER(Stats)],
     "clb_set_abiotic_kinetics": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int],
     "clb_ca_setup": [C.c_void_p, C.POINTER(CaDesc)],
+    "clb_run": [C.c_void_p, C.POINTER(RunDesc), C.POINTER(RunReport)],
     "clb_batch_create": [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)],
     "clb_batch_step": [C.c_void_p, C.c_int, C.c_int, C.c_int],
     "clb_batch_autotune": [C.c_void_p, C.c_int, C.c_char_p, C.c_int],
@@ -405,8 +421,9 @@ class Domain:
             self._check(st)
         return a.value, b.value
 
-    def ca_setup(self, max_biomass, biofilm_fraction, seed):
-        d = CaDesc(float(max_biomass), float(biofilm_fraction), int(seed))
+    def ca_setup(self, max_biomass, biofilm_fraction, seed, half=False):
+        """half: the 'half' push (halfPushExcessBiomass3D) instead of 'fraction'."""
+        d = CaDesc(float(max_biomass), float(biofilm_fraction), int(seed), 1 if half else 0)
         self._check(lib().clb_ca_setup(self.h, C.byref(d)))
 
     def ca_step(self, allow_stall=False):
@@ -416,6 +433,20 @@ class Domain:
         if not (allow_stall and st == 2):
             self._check(st)
         return st, a.value, bool(b.value)
+
+    def run(self, iterations, ca=False, ade_update_interval=1, ns_update_interval=0, resolve_every=0,
+            geometry_interval=0, flow_max_iterations=100000, flow_eps=1e-6, allow_stop=False):
+        """clb_run: `iterations` coupled iterations in the reference's loop order; returns the
+        report as a dict (its "status" is the call's status when allow_stop lets a stop through)."""
+        d = RunDesc(int(iterations), int(bool(ca)), int(ade_update_interval), int(ns_update_interval),
+                    int(resolve_every), int(geometry_interval), int(flow_max_iterations), float(flow_eps))
+        r = RunReport()
+        st = lib().clb_run(self.h, C.byref(d), C.byref(r))
+        if not (allow_stop and st in (2, 3, 4)):
+            self._check(st)
+        out = {k: getattr(r, k) for k, _ in RunReport._fields_}
+        out["status"] = st
+        return out
 
     def refresh_dynamics(self, species=True, flow=True):
         self._check(lib().clb_refresh_dynamics(self.h, int(species), int(flow)))
@@ -474,6 +505,12 @@ class Domain:
         c = np.empty(self.N, dtype=np.float64)
         self._check(lib().clb_get_field(self.h, FIELD_CONCENTRATION, s, _ptr(c), 0))
         return c
+
+    def set_concentration(self, s, c):
+        """A species' concentration field: immobile species take it as it is, mobile ones the
+        equilibrium populations at rest with that density."""
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        self._check(lib().clb_set_field(self.h, FIELD_CONCENTRATION, s, _ptr(c), 0))
 
     def set_ade_populations(self, s, g):
         g = np.ascontiguousarray(g, dtype=np.float64)

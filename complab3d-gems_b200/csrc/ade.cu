@@ -921,6 +921,23 @@ clb_status ade_set_immobile(clb_handle* h, int s, const double* host) {
                                     cudaMemcpyHostToDevice), "immobile concentration");
 }
 
+// A species' concentration field (user index s, FP64 [N]): an immobile species takes it as it is; a
+// mobile species gets the populations of the equilibrium at rest with that density,
+// f_i - t_i = t_i (C - 1) (initializeScalarLattice3D / the reference's initial concentration,
+// complab3d_processors_part3.hh:215-258), at every node of its lattice.
+clb_status ade_set_concentration(clb_handle* h, int s, const double* host) {
+    if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
+    if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
+    if (h->ap.slot[h->u2i[s]] < 0) return ade_set_immobile(h, s, host);
+    const size_t N = (size_t)h->g.N;
+    std::vector<double> pops(7 * N);
+    for (int i = 0; i < 7; ++i) {
+        const double w = q7w(i);
+        for (size_t n = 0; n < N; ++n) pops[(size_t)i * N + n] = w * (host[n] - 1.0);
+    }
+    return ade_set_populations(h, s, pops.data());
+}
+
 clb_status ade_set_thermo(clb_handle* h, const clb_thermo_desc* d) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     AdeParams& P = h->ap;
@@ -998,6 +1015,7 @@ static int ade_grid_for(const void* kern, int smem, int num_sms, int threads, in
 
 template <typename TS, typename TC, bool ODD>
 static void launch_ade_t(clb_handle* h) {
+    ++h->launches;  // one transport launch per call
     const int nm = h->n_mobile;
     const int nb = h->S;  // register bucket covers every species (mobile first, then immobile)
     TS* g = (TS*)h->d_g;
@@ -1055,6 +1073,7 @@ static void launch_neumann(clb_handle* h, int odd) {
     }
     if (J.n == 0) return;
     const dim3 grid(std::max(1, std::min(h->num_sms * 2, (h->g.plane + 255) / 256)), J.n);
+    ++h->launches;
     k_ade_neumann<TS, TC><<<grid, 256, 0, h->stream>>>((const TS*)h->d_g, (const TS*)h->d_glink, S, h->d_mat,
                                                        h->d_neu, h->ap, J, odd);
 }

@@ -313,6 +313,13 @@ clb_status clb_refresh_dynamics(clb_handle* h, int species, int flow) {
     return refresh_dynamics(h, species, flow);
 }
 
+clb_status clb_run(clb_handle* h, const clb_run_desc* d, clb_run_report* report) {
+    if (!h || !d) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    clb_run_report local;
+    return run(h, d, report ? report : &local);
+}
+
 clb_status clb_batch_create(clb_handle* const* handles, int n, clb_batch** out) {
     if (!handles || !out) return fail(nullptr, CLB_INVALID_ARG, "null argument");
     *out = nullptr;
@@ -447,6 +454,7 @@ clb_status clb_set_field(clb_handle* h, int field, int index, const void* host, 
             if (!h->flow_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_flow_init first");
             return flow_set_populations(h, (const double*)host);
         case CLB_FIELD_ADE_POPULATIONS: return ade_set_populations(h, index, (const double*)host);
+        case CLB_FIELD_CONCENTRATION: return ade_set_concentration(h, index, (const double*)host);
         case CLB_FIELD_ADE_VELOCITY: return ade_set_velocity(h, (const double*)host);
         case CLB_FIELD_BIOMASS: return ade_set_biomass_field(h, index, (const double*)host);
         default: return fail(h, CLB_INVALID_ARG, "field is read-only");

@@ -51,6 +51,7 @@ struct CaView {
     Geom g;
     double bmax, thr;        // Bmax, thrd_bFilmFrac x Bmax
     int M;
+    int half;                // push mode: 0 'fraction' (pushExcessBiomass3D), 1 'half' (halfPushExcessBiomass3D)
     int bb, solid;
     int n_pore;
     int pore[CLB_MAX_PORE_CODES];
@@ -179,7 +180,12 @@ __global__ void k_ca_collect(const CaView C, const int8_t* __restrict__ mat, con
     for (int64_t n = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += (int64_t)gridDim.x * blockDim.x) {
         if (!ca_open(C, mat[n])) continue;
         const double t = total[n];
-        if (!(t > C.bmax) || !(t - C.bmax > THRD)) continue;
+        if (C.half) {
+            // 'half': only biofilm voxels push, any total above the maximum
+            if (ca_pore(C, mat[n]) || !(t > C.bmax)) continue;
+        } else if (!(t > C.bmax) || !(t - C.bmax > THRD)) {
+            continue;
+        }
         const unsigned int i = atomicAdd(&sc->active, 1u);
         if ((int)i >= cap) { atomicAdd(&sc->overflow, 1u); continue; }
         act[i] = (int)n;
@@ -226,7 +232,7 @@ __global__ void k_ca_round(const CaView C, const int8_t* __restrict__ mat, const
             if (pre[q] >= 0) add_records(C, pre[q], n, tgt, amt, b);
         for (int t = 0; t < CA_REC; ++t) tgt[i * CA_REC + t] = -1;
         double bMt = total[n];
-        double bMd = bMt - C.bmax;
+        double bMd = C.half ? bMt * 0.5 : bMt - C.bmax;  // 'half' pushes half the voxel's biomass
         int64_t nb[6];
         int L = 0;
         const int d6[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
@@ -276,7 +282,7 @@ __global__ void k_ca_round(const CaView C, const int8_t* __restrict__ mat, const
             int64_t cand[6];
             int c = 0;
             for (int t = 0; t < L; ++t)
-                if (id0 > age[nb[t]]) cand[c++] = nb[t];
+                if (C.half ? id0 >= age[nb[t]] : id0 > age[nb[t]]) cand[c++] = nb[t];
             int64_t m;
             if (c > 1) m = cand[sm64(st) % (uint64_t)c];
             else if (c == 1) m = cand[0];
@@ -286,6 +292,14 @@ __global__ void k_ca_round(const CaView C, const int8_t* __restrict__ mat, const
                 const double shove = b[mi] / bMt * bMd;
                 b[mi] -= shove;
                 amt[((int64_t)i * CA_REC + rec) * C.M + mi] = shove;
+            }
+        } else if (C.half) {
+            // 'half' always makes the last push; with everything placed (bMd = 0) or no open
+            // neighbour its target is the voxel itself: subtracted, then added back
+            for (int mi = 0; mi < C.M; ++mi) {
+                const double shove = b[mi] / bMt * bMd;
+                b[mi] -= shove;
+                b[mi] += shove;
             }
         }
         for (int m = 0; m < C.M; ++m) own[(int64_t)i * C.M + m] = b[m];
@@ -434,6 +448,7 @@ static CaView ca_view(const clb_handle* h) {
     C.bmax = h->ca_bmax;
     C.thr = h->ca_frac * h->ca_bmax;
     C.M = h->M;
+    C.half = h->ca_half;
     C.bb = h->d.bounce_back_code;
     C.solid = h->d.solid_code;
     C.n_pore = h->d.n_pore_codes > 0 ? h->d.n_pore_codes : 1;
@@ -482,6 +497,8 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
     if (h->M < 1 || !h->d_bio) return fail(h, CLB_INVALID_ARG, "the automaton needs biomass fields (clb_set_biomass)");
     if (h->M > h->d.n_microbes) return fail(h, CLB_INVALID_ARG, "every biomass field needs a biofilm material code");
     if (!(d->max_biomass > 0)) return fail(h, CLB_INVALID_ARG, "max_biomass must be positive");
+    if (d->push_mode != CLB_PUSH_FRACTION && d->push_mode != CLB_PUSH_HALF)
+        return fail(h, CLB_INVALID_ARG, "push_mode is CLB_PUSH_FRACTION or CLB_PUSH_HALF");
     int codesum = 0;
     for (int m = 0; m < h->M; ++m) codesum += h->d.bio_codes[m];
     if (codesum > 127) return fail(h, CLB_INVALID_ARG, "the sum of the biofilm codes must fit a material code");
@@ -506,6 +523,7 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
     }
     h->ca_bmax = d->max_biomass;
     h->ca_frac = d->biofilm_fraction;
+    h->ca_half = d->push_mode;
     h->ca_seed = d->seed;
     h->ca_sweeps = 0;
     CaScalars zero;
@@ -538,6 +556,7 @@ static clb_status ca_mask_pass(clb_handle* h, const CaView& C, double& gmax, lon
     s.gmax = LLONG_MIN;
     cudaMemcpyAsync(SC(h), &s, sizeof s, cudaMemcpyHostToDevice, h->stream);
     if (h->d_ca_mask0) cudaMemcpyAsync(h->d_ca_mask0, h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToDevice, h->stream);
+    ++h->launches;
     k_ca_mask_total<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_ca_mask0, h->d_bio,
                                                                    h->d_ca_total, SC(h));
     clb_status st = ca_scalars(h, s);
@@ -555,12 +574,14 @@ static clb_status ca_push_sweep(clb_handle* h, const CaView& C) {
         CaScalars s;
         std::memset(&s, 0, sizeof s);
         cudaMemcpyAsync(SC(h), &s, sizeof s, cudaMemcpyHostToDevice, h->stream);
+        h->launches += 1;
         k_ca_collect<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_ca_total, h->d_ca_aidx, h->d_ca_act,
                                                          h->d_ca_done, h->ca_cap, SC(h));
         clb_status st = ca_scalars(h, s);
         if (st != CLB_OK) return st;
         const int count = (int)std::min<unsigned int>(s.active, (unsigned int)h->ca_cap);
         if (s.overflow) {
+            ++h->launches;
             k_ca_clear<<<grid, CA_THREADS, 0, h->stream>>>(h->d_ca_aidx, h->d_ca_act, count);
             st = ca_reserve(h, (int)s.active * 2);
             if (st != CLB_OK) return st;
@@ -569,17 +590,26 @@ static clb_status ca_push_sweep(clb_handle* h, const CaView& C) {
         if (count == 0) { ++h->ca_sweeps; return CLB_OK; }
         s.remaining = (unsigned int)count;
         cudaMemcpyAsync(&SC(h)->remaining, &s.remaining, sizeof(unsigned int), cudaMemcpyHostToDevice, h->stream);
-        // every round completes at least the lexicographically first unfinished voxel
-        for (int round = 1; round <= count; ++round) {
-            k_ca_round<<<(count + CA_THREADS - 1) / CA_THREADS, CA_THREADS, 0, h->stream>>>(
-                C, h->d_mat, h->d_ca_total, h->d_ca_age, h->d_bio, h->d_ca_aidx, h->d_ca_act, h->d_ca_done,
-                h->d_ca_tgt, h->d_ca_amt, h->d_ca_own, count, round, h->ca_seed, h->ca_sweeps, SC(h));
+        // every round completes at least the lexicographically first unfinished voxel, so `count`
+        // rounds always suffice. Rounds go out in batches and the host reads the remaining count once
+        // per batch: a round after the last voxel finished finds every voxel done and changes nothing,
+        // so the batching leaves the result bit for bit the same.
+        constexpr int ROUND_BATCH = 16;
+        for (int round = 1; round <= count; round += ROUND_BATCH) {
+            const int last = std::min(count, round + ROUND_BATCH - 1);
+            for (int r = round; r <= last; ++r) {
+                ++h->launches;
+                k_ca_round<<<(count + CA_THREADS - 1) / CA_THREADS, CA_THREADS, 0, h->stream>>>(
+                    C, h->d_mat, h->d_ca_total, h->d_ca_age, h->d_bio, h->d_ca_aidx, h->d_ca_act, h->d_ca_done,
+                    h->d_ca_tgt, h->d_ca_amt, h->d_ca_own, count, r, h->ca_seed, h->ca_sweeps, SC(h));
+            }
             unsigned int rem = 0;
             cudaError_t e = cudaMemcpyAsync(&rem, &SC(h)->remaining, sizeof rem, cudaMemcpyDeviceToHost, h->stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
             if (e != cudaSuccess) return cuda_check(h, e, "push round");
             if (rem == 0) break;
         }
+        h->launches += 2;  // apply + clear
         k_ca_apply<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_bio, h->d_ca_aidx, h->d_ca_tgt, h->d_ca_amt, h->d_ca_own);
         k_ca_clear<<<grid, CA_THREADS, 0, h->stream>>>(h->d_ca_aidx, h->d_ca_act, count);
         ++h->ca_sweeps;
@@ -587,14 +617,28 @@ static clb_status ca_push_sweep(clb_handle* h, const CaView& C) {
     }
 }
 
+// Jacobi sweeps of the age field until one changes nothing, at most 1001 sweeps (the reference's
+// limit of 1000 after the first). Sweeps go out in batches; the change counter is cleared before
+// the last sweep of a batch and read after it. A sweep of a settled field changes nothing, so a
+// batch that continues past the settling sweep leaves the same field, and the total number of
+// sweeps never exceeds the sequential loop's, so an unsettled field ends the same too.
 static clb_status ca_age_converge(clb_handle* h, const CaView& C, bool& settled) {
     settled = false;
-    for (int sub = 0; sub <= 1000; ++sub) {
-        unsigned int zero = 0;
-        cudaMemcpyAsync(&SC(h)->changed, &zero, sizeof zero, cudaMemcpyHostToDevice, h->stream);
-        k_age_jacobi<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_ca_age, h->d_ca_age2, h->d_ca_distp,
-                                                                    h->d_ca_total, SC(h));
-        std::swap(h->d_ca_age, h->d_ca_age2);
+    constexpr int SWEEP_BATCH = 8, MAX_SWEEPS = 1001;
+    int done = 0;
+    while (done < MAX_SWEEPS) {
+        const int b = std::min(SWEEP_BATCH, MAX_SWEEPS - done);
+        for (int k = 0; k < b; ++k) {
+            if (k == b - 1) {
+                unsigned int zero = 0;
+                cudaMemcpyAsync(&SC(h)->changed, &zero, sizeof zero, cudaMemcpyHostToDevice, h->stream);
+            }
+            ++h->launches;
+            k_age_jacobi<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_ca_age, h->d_ca_age2, h->d_ca_distp,
+                                                                        h->d_ca_total, SC(h));
+            std::swap(h->d_ca_age, h->d_ca_age2);
+        }
+        done += b;
         unsigned int ch = 0;
         cudaError_t e = cudaMemcpyAsync(&ch, &SC(h)->changed, sizeof ch, cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -608,6 +652,7 @@ static void ca_age_sweep_inplace(clb_handle* h, const CaView& C) {
     const int levels = h->g.nx + h->g.ny + h->g.nz - 2;
     const int64_t cols = (int64_t)h->g.nx * h->g.ny;
     const int grid = (int)std::min<int64_t>((cols + CA_THREADS - 1) / CA_THREADS, h->num_sms * 8);
+    h->launches += levels;
     for (int l = 0; l < levels; ++l)
         k_age_level<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_ca_age, h->d_ca_distp, h->d_ca_total, l);
 }
@@ -662,6 +707,7 @@ clb_status refresh_dynamics(clb_handle* h, int species, int flow) {
     const CaView C = ca_view(h);
     const int bio0 = h->d.n_microbes > 0 ? h->d.bio_codes[0] : -1;
     const int grid = h->num_sms * 8;
+    if (species && h->ade_ready) ++h->launches;
     if (species && h->ade_ready)
         k_refresh_species<<<grid, CA_THREADS, 0, h->stream>>>(h->ade_sp.code, h->ade_sp.node, h->ade_sp.K, h->d_mat, C,
                                                               bio0);
@@ -675,6 +721,7 @@ clb_status refresh_dynamics(clb_handle* h, int species, int flow) {
                 e = cudaMemcpy(h->d_mat_flow, h->h_mat_flow.data(), (size_t)N, cudaMemcpyHostToDevice);
             if (e != cudaSuccess) return cuda_check(h, e, "flow material map");
         }
+        h->launches += 2;
         k_refresh_flow_map<<<grid, CA_THREADS, 0, h->stream>>>(h->d_mat_flow, h->d_mat, C, h->fp, 1.0 / h->d.tau, bio0);
         k_codes_from_map<<<grid, CA_THREADS, 0, h->stream>>>(h->flow_sp.code, h->flow_sp.node, h->flow_sp.K, h->d_mat_flow);
         h->h_mat_flow.resize((size_t)N);

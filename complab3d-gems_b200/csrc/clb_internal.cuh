@@ -179,6 +179,7 @@ struct clb_handle_s {
     int device = 0;
     int num_sms = 148;
     std::string err;
+    int64_t launches = 0;             // kernels this handle enqueued on the coupled step's path
     std::vector<int8_t> h_mat;
     int8_t* d_mat = nullptr;
 
@@ -259,6 +260,7 @@ struct clb_handle_s {
     // biofilm cellular automaton (biofilm_ca.cu)
     bool ca_ready = false;
     double ca_bmax = 0, ca_frac = 0;
+    int ca_half = 0;                  // push mode: 0 'fraction', 1 'half' 
     uint64_t ca_seed = 0, ca_sweeps = 0;
     long long ca_mask_sum = 0;
     double* d_ca_total = nullptr;     // [N] total biomass as the automaton tracks it
@@ -312,6 +314,7 @@ clb_status ade_reduce_noalloc(clb_handle* h, clb_stats* out);
 clb_status ade_set_abiotic(clb_handle* h, int law, const double* prm, int nprm, int surface_only);
 clb_status ade_set_thermo(clb_handle* h, const clb_thermo_desc* d);
 clb_status ade_set_immobile(clb_handle* h, int s, const double* host);
+clb_status ade_set_concentration(clb_handle* h, int s, const double* host);
 void ade_refresh_neumann(clb_handle* h);
 void ade_free(clb_handle* h);
 
@@ -337,6 +340,9 @@ clb_status ca_step(clb_handle* h, int* sweeps, int* mask_changed);
 clb_status refresh_dynamics(clb_handle* h, int species, int flow);
 clb_status ca_fields(clb_handle* h, int which, double* host);
 void ca_free(clb_handle* h);
+
+// driver.cu
+clb_status run(clb_handle* h, const clb_run_desc* d, clb_run_report* r);
 
 // speciation.cu
 clb_status speciation_setup(clb_handle* h, const clb_speciation_desc* d);

@@ -884,6 +884,7 @@ clb_status flow_init(clb_handle* h, double delta_p) {
 }
 
 static void launch_flow(clb_handle* h, bool odd, int trace) {
+    ++h->launches;  // one step launch per call
     const FlowParams& P = h->fp;
     const SparseView S = view_of(h->flow_sp);
     const int grid = h->flow_grid;
@@ -998,6 +999,7 @@ clb_status flow_velocity_at(clb_handle* h, const int32_t* nodes, int64_t count, 
     const SparseView S = view_of(h->flow_sp);
     const int odd = (int)(h->flow_iters & 1);
     const int grid = h->num_sms * 8;
+    ++h->launches;
 #define CLB_VEL(TS, TC)                                                                                         \
     if (dtype == 0)                                                                                             \
         k_flow_velocity<TS, TC, double><<<grid, 256, 0, h->stream>>>((const TS*)h->d_f, (const TS*)h->d_flink, S, \

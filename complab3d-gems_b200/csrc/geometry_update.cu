@@ -318,6 +318,7 @@ static void launch_dissolution(clb_handle* h) {
     const SparseView S = view_of(h->ade_sp);
     const TS* g = (const TS*)h->d_g;
     const TS* gl = (const TS*)h->d_glink;
+    h->launches += (h->n_seal > 0) + (h->n_gath > 0);
     if (h->n_seal > 0)
         k_dissolve_park<TS, TC><<<(int)std::min<int64_t>((h->n_seal + GU_THREADS - 1) / GU_THREADS, h->num_sms * 4),
                                   GU_THREADS, 0, h->stream>>>(g, gl, h->d_imm, h->d_bio, h->d_mat, S, h->ap,
@@ -420,6 +421,7 @@ static clb_status flow_follow(clb_handle* h) {
     }
     e = cudaMemcpy(h->d_mat_flow, h->h_mat_flow.data(), (size_t)N, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_check(h, e, "flow material map");
+    ++h->launches;
     k_flow_codes<<<h->num_sms * 4, 256, 0, h->stream>>>(h->flow_sp.code, h->flow_sp.node, h->flow_sp.K, h->d_mat_flow);
     int64_t nbgk = 0;
     for (int64_t n = 0; n < N; ++n) nbgk += h->fp.dyn[(uint8_t)h->h_mat_flow[n] & 127] == DYN_BGK;
@@ -437,6 +439,7 @@ clb_status geometry_update(clb_handle* h, int* sealed, int* reopened) {
     // the Neumann planes' stored densities belong to the last stream, with the map before the change
     ade_refresh_neumann(h);
     cudaMemsetAsync(h->d_count, 0, sizeof(unsigned int) * 4, h->stream);
+    h->launches += 1 + (h->prc.dissolution ? 1 : 0);
     k_seal<<<grid, 256, 0, h->stream>>>(h->ade_sp.code, h->d_mat, h->d_stamp, mineral, S, P, lo, hi,
                                         h->prc.full_density, (int8_t)h->prc.precip_code, h->d_count);
     if (h->prc.dissolution)

@@ -391,6 +391,7 @@ clb_status speciation_step(clb_handle* h) {
     const SparseView S = view_of(h->ade_sp);
     const int grid = h->num_sms * 4;
     const MlpView M = mlp_view(h);
+    ++h->launches;
     switch (h->ade_prec) {
         case CLB_F64: k_speciate_step<double><<<grid, 128, 0, h->stream>>>((double*)h->d_g, (double*)h->d_glink, h->d_imm, S, h->ap, CLB_SP(h), odd, h->ade_west_end, h->ade_east_begin, M, h->spec_mode, h->d_spec_stats); break;
         case CLB_F32: k_speciate_step<float><<<grid, 128, 0, h->stream>>>((float*)h->d_g, (float*)h->d_glink, h->d_imm, S, h->ap, CLB_SP(h), odd, h->ade_west_end, h->ade_east_begin, M, h->spec_mode, h->d_spec_stats); break;

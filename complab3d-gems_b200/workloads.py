@@ -13,9 +13,17 @@ from __future__ import annotations
 
 import numpy as np
 
-import clb
-
 CS2_ADE = 0.25
+
+# constants of the library's C ABI used in the workload descriptions (include/clb.h), kept here so
+# that building a workload does not load the library
+DIRICHLET, NEUMANN = 0, 1
+LAW_DECAY, LAW_MONOD, LAW_DUAL_MONOD = 1, 2, 3
+
+
+def _library_sphere_pack(*args, **kw):
+    import clb
+    return clb.sphere_pack(*args, **kw)
 
 
 def add_ghost_planes(inner, nx_inner, ny, nz):
@@ -31,39 +39,45 @@ def omega_from_d(d):
     return 1.0 / (d / CS2_ADE + 0.5)
 
 
-def sphere_pack_domain(nx_inner, ny, nz, porosity, rmin, rmax, seed, walls="yz"):
-    inner = clb.sphere_pack(nx_inner, ny, nz, porosity, rmin, rmax, seed, walls, grain=1, wall=1, pore=2)
+def sphere_pack_domain(nx_inner, ny, nz, porosity, rmin, rmax, seed, walls="yz", gen=None):
+    """`gen`: the sphere-pack generator (default: the library's clb_geom_sphere_pack; the CPU
+    baseline passes the oracle's restatement of it, which gives the same voxels)."""
+    gen = gen or _library_sphere_pack
+    inner = gen(nx_inner, ny, nz, porosity, rmin, rmax, seed, walls, grain=1, wall=1, pore=2)
     return add_ghost_planes(inner, nx_inner, ny, nz), (nx_inner + 2, ny, nz)
 
 
-def pack64x32x32_decay(scale=1):
+def pack64x32x32_decay(scale=1, gen=None):
     """64x32x32 sphere pack (r = 4, porosity 0.40, walls on the four side faces), tau 0.8,
     dP 1e-4, one solute D_pore 0.1 / D_biofilm 0.05, C = 1 Dirichlet inlet, Neumann outlet,
     first-order decay k = 1e-3 per step, clamped. `scale` < 1 shrinks the box for quick tests."""
     nxi, ny, nz = max(8, int(64 * scale)), max(6, int(32 * scale)), max(6, int(32 * scale))
-    mat, shape = sphere_pack_domain(nxi, ny, nz, 0.40, 4.0, 4.0, seed=1001)
+    mat, shape = sphere_pack_domain(nxi, ny, nz, 0.40, 4.0, 4.0, seed=1001, gen=gen)
     species = [dict(omega_pore=omega_from_d(0.1), omega_biofilm=omega_from_d(0.05), mobile=1,
-                    left_type=clb.DIRICHLET, right_type=clb.NEUMANN, left_bc=1.0, c0=0.0)]
+                    left_type=DIRICHLET, right_type=NEUMANN, left_bc=1.0, c0=0.0)]
     return dict(name="sphere-pack 64x32x32 flow + 1 decaying solute", mat=mat, shape=shape, tau=0.8,
-                delta_p=1e-4, eps=1e-6, species=species, law=clb.LAW_DECAY, params=[1e-3], dt=1.0,
+                delta_p=1e-4, eps=1e-6, species=species, law=LAW_DECAY, params=[1e-3], dt=1.0,
                 ade_steps=2000)
 
 
-def pack256x128x128(scale=1):
+def pack256x128x128(scale=1, gen=None):
     """256x128x128 overlapping-sphere pack (porosity 0.35, r ~ U[3, 8]), flow only, tau 0.7,
     Peclet rescale (Pe 10, L 8), residual 1e-7."""
     nxi, ny, nz = max(8, int(256 * scale)), max(8, int(128 * scale)), max(8, int(128 * scale))
-    mat, shape = sphere_pack_domain(nxi, ny, nz, 0.35, 3.0, 8.0, seed=1002)
+    mat, shape = sphere_pack_domain(nxi, ny, nz, 0.35, 3.0, 8.0, seed=1002, gen=gen)
     return dict(name="overlapping-sphere pack 256x128x128 flow", mat=mat, shape=shape, tau=0.7, delta_p=1e-4,
                 eps=1e-7, peclet=10.0, char_length=8.0, tau_ade_fixed=0.8)
 
 
-def pack256cube_8species(scale=1, seed=1003):
+def pack256cube_8species(scale=1, seed=1003, gen=None):
     """256^3 sphere pack (porosity 0.40), 8 species with D_pore ~ U[0.02, 0.2] and
     D_biofilm = D_pore / 2, two microbes (materials 3 and 4) seeded on 2 % of pore voxels,
-    dual-Monod kinetics mu_max 1e-4, Ks 0.1, Y 0.4, decay 1e-6."""
+    dual-Monod kinetics mu_max 1e-4, Ks 0.1, Y 0.4, decay 1e-6; the biofilm automaton ('fraction'
+    push, max density 100, biofilm threshold 0.1 of it) every iteration; the flow (tau 0.8,
+    pressure drop 1e-4, FP32) solved to 1e-6 first and re-solved every 500 iterations; 10,000
+    iterations."""
     nxi, ny, nz = max(8, int(256 * scale)), max(8, int(256 * scale)), max(8, int(256 * scale))
-    mat, shape = sphere_pack_domain(nxi, ny, nz, 0.40, 3.0, 8.0, seed=seed)
+    mat, shape = sphere_pack_domain(nxi, ny, nz, 0.40, 3.0, 8.0, seed=seed, gen=gen)
     rng = np.random.default_rng(seed)
     pore = np.flatnonzero(mat == 2)
     seeded = rng.choice(pore, size=max(2, int(0.02 * pore.size)), replace=False)
@@ -80,12 +94,20 @@ def pack256cube_8species(scale=1, seed=1003):
     species = []
     for k in range(8):
         species.append(dict(omega_pore=omega_from_d(d[k]), omega_biofilm=omega_from_d(0.5 * d[k]), mobile=1,
-                            left_type=clb.DIRICHLET if k < 3 else clb.NEUMANN, right_type=clb.NEUMANN,
+                            left_type=DIRICHLET if k < 3 else NEUMANN, right_type=NEUMANN,
                             left_bc=1.0 if k < 3 else 0.0, c0=0.1 if k < 3 else 0.0))
     return dict(name="sphere-pack 256^3, 8 species, 2 biofilm microbes", mat=mat, shape=shape, tau=0.8,
-                delta_p=1e-4, eps=1e-6, species=species, law=clb.LAW_DUAL_MONOD,
+                delta_p=1e-4, eps=1e-6, species=species, law=LAW_DUAL_MONOD,
                 params=[1e-4, 0.1, 0.4, 1e-6], dt=1.0, biomass=bio, bio_codes=(3, 4), perm_ratio=(0.1, 0.1),
-                bmax=100.0)
+                bmax=100.0, biofilm_fraction=0.1, ca_seed=seed, resolve_every=500, iterations=10000,
+                flow_max_iterations=100000)
+
+
+# Flow iterations per transport iteration of the 256^3 coupled configuration: the re-solve's
+# collide-and-stream calls over its 500-iteration interval, as measured on one B200 (bench.py's
+# headline reports the run's own figure). The CPU baseline weights its flow and transport samples
+# by it so that both arms time the same mix of work.
+FLOW_PER_TRANSPORT_CONFIG3 = 2.0
 
 
 def ensemble_uneven_packs(n_domains=96, seed=1005, scale=1.0):
@@ -108,9 +130,9 @@ def ensemble_uneven_packs(n_domains=96, seed=1005, scale=1.0):
         for s in range(3):
             dp = float(rng.uniform(0.05, 0.2))
             species.append(dict(omega_pore=omega_from_d(dp), omega_biofilm=omega_from_d(0.5 * dp), mobile=1,
-                                left_type=clb.DIRICHLET, right_type=clb.NEUMANN, left_bc=1.0, c0=0.0))
+                                left_type=DIRICHLET, right_type=NEUMANN, left_bc=1.0, c0=0.0))
         k = 10.0 ** rng.uniform(-6, -3, size=3)
-        doms.append(dict(mat=mat, shape=shape, tau=tau, delta_p=1e-4, species=species, law=clb.LAW_MONOD,
+        doms.append(dict(mat=mat, shape=shape, tau=tau, delta_p=1e-4, species=species, law=LAW_MONOD,
                          params=list(k) + [0.1] * 3, dt=1.0))
     return dict(name=f"ensemble of {n_domains} uneven sphere packs, D3Q19 + 3 x D3Q7 each", domains=doms)
 

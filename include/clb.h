@@ -124,7 +124,9 @@ typedef enum clb_field {
     CLB_FIELD_MATERIAL = 0,       /* int8 [N]                                                */
     CLB_FIELD_FLOW_VELOCITY = 1,  /* [3][N]  computeVelocity of the flow lattice            */
     CLB_FIELD_FLOW_POPULATIONS = 2, /* [19][N] incoming (post-stream) populations            */
-    CLB_FIELD_CONCENTRATION = 3,  /* [N] of species `index`: computeDensity                  */
+    CLB_FIELD_CONCENTRATION = 3,  /* [N] of species `index`: computeDensity. Written: an
+                                     immobile species takes the field, a mobile one the
+                                     equilibrium populations at rest with that density      */
     CLB_FIELD_ADE_POPULATIONS = 4,/* [7][N] of species `index`                               */
     CLB_FIELD_BIOMASS = 5,        /* [N] of microbe `index`                                  */
     CLB_FIELD_ADE_VELOCITY = 6,   /* [3][N] the advection velocity the species see          */
@@ -339,6 +341,16 @@ clb_status clb_geometry_update(clb_handle* h, int* sealed, int* reopened);
 
 /* The <microbiology> settings of the CA microbes (solver type CA; the biomass fields are those of
  * clb_set_biomass, microbe m living in material bio_codes[m]). */
+/* Push modes of the automaton (<microbiology><CA_method> of CompLaB.xml, halfflag):
+ * CLB_PUSH_FRACTION  pushExcessBiomass3D (complab3d_processors_part1.hh:499-732): every open voxel
+ *                    above max_biomass pushes the excess over it;
+ * CLB_PUSH_HALF      halfPushExcessBiomass3D (:735-970): every biofilm voxel above max_biomass
+ *                    pushes half its biomass, the fallback neighbour may have an equal age, and the
+ *                    fallback push always runs (into the voxel itself when nothing is left or no
+ *                    neighbour is open). */
+#define CLB_PUSH_FRACTION 0
+#define CLB_PUSH_HALF 1
+
 typedef struct clb_ca_desc {
     double max_biomass;           /* max_bMassRho: excess above it is pushed to neighbours      */
     double biofilm_fraction;      /* thrd_bFilmFrac: pore <-> biofilm at this fraction of max   */
@@ -346,6 +358,7 @@ typedef struct clb_ca_desc {
                                      std::rand from the clock); a voxel's draws in a sweep are
                                      splitmix64 steps from seed ^ sweep*0x9E3779B97F4A7C15
                                      ^ voxel*0xD1B54A32D192ED03                               */
+    int32_t push_mode;            /* CLB_PUSH_FRACTION or CLB_PUSH_HALF                          */
 } clb_ca_desc;
 
 /* Age and distance fields from the current mask (createAgeDomain3D, calculateDistanceFromSolid;
@@ -354,7 +367,8 @@ clb_status clb_ca_setup(clb_handle* h, const clb_ca_desc* desc);
 
 /* The CA block of one iteration (complab.cpp:2792-3055): mask and total update
  * (updateLocalMaskNtotalLattices3D), then, while the largest total exceeds max_biomass, push
- * sweeps (pushExcessBiomass3D, 'fraction') each followed by the mask update, with the age
+ * sweeps (pushExcessBiomass3D or halfPushExcessBiomass3D, by push_mode) each followed by the mask
+ * update, with the age
  * relaxation (updateAgeDistance3D) every 50 sweeps; then one age sweep when the mask changed
  * (:3074-3079). Results equal the sequential lexicographic sweeps bit for bit. *sweeps receives
  * the push sweeps made, *mask_changed whether the mask changed. Returns CLB_NOT_CONVERGED where
@@ -368,6 +382,52 @@ clb_status clb_ca_step(clb_handle* h, int* sweeps, int* mask_changed);
  * reference runs them every ade_update_interval / ns_update_interval iterations after a mask
  * change; re-solve the flow and couple its velocity afterwards as it does. */
 clb_status clb_refresh_dynamics(clb_handle* h, int species, int flow);
+
+/* ---------------------------------------------------------------- the coupled step, driven */
+
+/* The schedule of the reference's main loop (complab.cpp:2178-3262) for clb_run. */
+typedef struct clb_run_desc {
+    int32_t iterations;           /* transport iterations this call advances                      */
+    int32_t ca;                   /* 1: the biofilm automaton every iteration (clb_ca_setup first) */
+    int32_t ade_update_interval;  /* species dynamics follow a changed mask at iterations that are
+                                     multiples of it (<ade_update_interval>; 0: never)            */
+    int32_t ns_update_interval;   /* flow dynamics follow a changed mask and the flow is re-solved
+                                     at iterations that are multiples of it (the reference's
+                                     schedule: the mask changed at that very iteration; 0: never) */
+    int32_t resolve_every;        /* re-solve the flow every this many iterations whatever the mask
+                                     did (the flow dynamics follow the mask first if it changed since
+                                     the previous re-solve); 0: off                               */
+    int32_t geometry_interval;    /* precipitation / dissolution node conversion every this many
+                                     iterations (clb_geometry_update; clb_precip_setup first); 0: off */
+    int32_t flow_max_iterations;  /* cap of each re-solve (ns_max_iT2)                              */
+    double flow_eps;              /* ValueTracer criterion of each re-solve (ns_converge_iT2)        */
+} clb_run_desc;
+
+typedef struct clb_run_report {
+    int64_t iterations;           /* transport iterations made                                      */
+    int64_t ca_sweeps;            /* push sweeps of the automaton                                   */
+    int64_t mask_changes;         /* iterations whose automaton changed the mask                    */
+    int64_t flow_resolves;        /* flow re-solves made (not counting clb_geometry_update's own)   */
+    int64_t flow_iterations;      /* collide-and-stream calls of those re-solves                    */
+    int64_t flow_unconverged;     /* re-solves that reached their cap with the outlet still flowing */
+    int64_t sealed, reopened;     /* voxels converted by the geometry updates                       */
+    double ms_transport;          /* device time of the fused transport steps (CUDA events)         */
+    double ms_ca;                 /* device time of the automaton and the species' dynamics refresh */
+    double ms_flow;               /* device time of the re-solves and velocity couplings            */
+    double ms_geometry;           /* device time of the geometry updates (their re-solves included) */
+    double seconds;               /* wall clock of the call                                         */
+    int64_t launches;             /* kernels the call launched                                      */
+} clb_run_report;
+
+/* Advances d->iterations coupled iterations in the reference's order: the fused transport step
+ * (collide, kinetics, speciation, stream), the biofilm automaton, the dynamics refresh and flow
+ * re-solve after a mask change, the precipitation / dissolution conversions. Stops where the
+ * reference stops: CLB_NONFINITE (non-finite concentrations, biomass or flow energy),
+ * CLB_PERCOLATION_LOST (a re-solve found no flow through the outlet), CLB_NOT_CONVERGED (the
+ * automaton could not settle); a re-solve that reaches its cap while the outlet still flows is
+ * counted in report->flow_unconverged and the run goes on. report may be NULL.
+ * Replaces: the body of the main loop, complab.cpp:2178-3262. */
+clb_status clb_run(clb_handle* h, const clb_run_desc* d, clb_run_report* report);
 
 /* ---------------------------------------------------------------- ensembles of domains */
 

@@ -53,6 +53,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <string>
 #include <vector>
 #include <algorithm>
 #ifdef _OPENMP
@@ -391,6 +392,7 @@ struct OrcAde {
     std::vector<int8_t> dmat;
     // biofilm cellular automaton (complab3d_processors_part1.hh:499-732, part2.hh:71-259, :840-965)
     int ca_on = 0;
+    int half = 0;       // push mode: 0 'fraction' (pushExcessBiomass3D), 1 'half' (halfPushExcessBiomass3D)
     double Bmax = 0, bfrac = 0;
     uint64_t seed = 0, sweeps = 0;
     std::vector<int> pore_codes, bio_code;
@@ -1077,6 +1079,7 @@ void orc_ca_setup(OrcAde* A, double Bmax, double frac, uint64_t seed, int n_pore
     const int nx = A->nx, ny = A->ny, nz = A->nz;
     const size_t N = A->N;
     A->ca_on = 1;
+    A->half = 0;
     A->Bmax = Bmax;
     A->bfrac = frac;
     A->seed = seed;
@@ -1151,7 +1154,12 @@ static void ca_mask_total(OrcAde* A) {
             }
 }
 
-// pushExcessBiomass3D ('fraction') of a single-block run, where every push lands inside the block
+// pushExcessBiomass3D ('fraction', complab3d_processors_part1.hh:499-732) or
+// halfPushExcessBiomass3D ('half', :735-970) of a single-block run, where every push lands inside
+// the block. 'half' differs in four places: only biofilm voxels push (not pore), the excess is half
+// the voxel's total (no threshold on it), the fallback target is a neighbour whose age is not above
+// the voxel's (>= instead of >), and the fallback push always runs -- into the voxel itself
+// (subtracted, then added back) when the first pass placed everything or no neighbour is open.
 static void ca_push(OrcAde* A) {
     const int nx = A->nx, ny = A->ny, nz = A->nz;
     const size_t N = A->N;
@@ -1162,10 +1170,11 @@ static void ca_push(OrcAde* A) {
             for (int z = 0; z < nz; ++z) {
                 const size_t n = A->id(x, y, z);
                 if (!ca_open(A, A->mat[n])) continue;
+                if (A->half && ca_pore(A, A->mat[n])) continue;
                 double bMt = A->total[n];
                 if (!(bMt > Bmax)) continue;
-                double bMd = bMt - Bmax;
-                if (!(bMd > THRD)) continue;
+                double bMd = A->half ? bMt * 0.5 : bMt - Bmax;
+                if (!A->half && !(bMd > THRD)) continue;
                 // neighbours in the reference's order, x limited to 1..nx-2
                 size_t nb[6];
                 int L = 0;
@@ -1204,16 +1213,18 @@ static void ca_push(OrcAde* A) {
                     }
                     if (chk) break;
                 }
+                size_t m = n;  // 'half': with no fallback neighbour the push goes back into the voxel
                 if (!chk && L > 0) {
                     const int id0 = A->age[n];
                     size_t cand[6];
                     int c = 0;
                     for (int t = 0; t < L; ++t)
-                        if (id0 > A->age[nb[t]]) cand[c++] = nb[t];
-                    size_t m;
+                        if (A->half ? id0 >= A->age[nb[t]] : id0 > A->age[nb[t]]) cand[c++] = nb[t];
                     if (c > 1) m = cand[sm64(st) % (uint64_t)c];
                     else if (c == 1) m = cand[0];
                     else m = nb[L > 1 ? (int)(sm64(st) % (uint64_t)L) : 0];
+                }
+                if (A->half || (!chk && L > 0)) {
                     for (int mi = 0; mi < A->M; ++mi) {
                         const double shove = A->bio[(size_t)mi * N + n] / bMt * bMd;
                         A->bio[(size_t)mi * N + n] -= shove;
@@ -1327,6 +1338,7 @@ void orc_ca_fields(OrcAde* A, double* total, int32_t* age) {
 // the mask and total update once; the age relaxation until no age changes (at most max_sweeps),
 // returning the number of sweeps that changed something
 void orc_ca_mask_total_once(OrcAde* A) { ca_mask_total(A); }
+void orc_ca_set_half(OrcAde* A, int half) { A->half = half ? 1 : 0; }
 int orc_ca_age_relax(OrcAde* A, int max_sweeps) {
     int k = 0;
     while (k < max_sweeps && ca_age_sweep(A) != 0) ++k;
@@ -1563,4 +1575,62 @@ extern "C" void orc_dissolution_increments(int nx, int ny, int nz, int S, int sM
         nx, ny, nz, S, sM, dt, surface_only, stamp, L, [&](int s, size_t n) { return C[(size_t)s * N + n]; },
         [&](size_t n) { return mat[n] != solid && mat[n] != bb; }, d);
     std::copy(d.begin(), d.end(), dC);
+}
+
+// =====================================================================================
+//                 POROSITY-TARGETED SPHERE PACK (input maps of the CPU baseline)
+// =====================================================================================
+// The library's clb_geom_sphere_pack restated so the CPU baseline builds its input without the
+// product library: walls on the listed axes, then spheres of radius U[rmin, rmax] at centres drawn
+// from the reference's xorshift64* stream (complab3d_geometry.hh:77-83) carved as `grain` until
+// the open fraction reaches `porosity`. Same voxels for the same arguments (tests/test_geometry.py).
+namespace {
+struct OrcXorShift {
+    uint64_t s;
+    explicit OrcXorShift(uint64_t seed) : s(seed ? seed : 1) {}
+    uint64_t next() {
+        s ^= s >> 12;
+        s ^= s << 25;
+        s ^= s >> 27;
+        return s * 2685821657736338717ULL;
+    }
+    double uniform() { return (double)(next() >> 11) / 9007199254740992.0; }
+    int below(int n) { return n > 0 ? (int)(uniform() * (double)n) : 0; }
+};
+}  // namespace
+
+extern "C" int orc_sphere_pack(int nx, int ny, int nz, double porosity, double rmin, double rmax, uint64_t seed,
+                               const char* walls, int grain, int wall, int pore, int8_t* out) {
+    if (!out || nx < 1 || ny < 1 || nz < 1 || !(porosity > 0 && porosity < 1) || !(rmin > 0) || rmax < rmin) return 1;
+    const size_t N = (size_t)nx * ny * nz;
+    std::vector<int8_t> m(N, (int8_t)pore);
+    const std::string w = walls ? walls : "";
+    const bool all = w == "all";
+    const bool wx = all || w.find('x') != std::string::npos, wy = all || w.find('y') != std::string::npos,
+               wz = all || w.find('z') != std::string::npos;
+    size_t open = N;
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                const bool on = (wx && (x == 0 || x == nx - 1)) || (wy && (y == 0 || y == ny - 1)) ||
+                                (wz && (z == 0 || z == nz - 1));
+                if (on) { m[((size_t)x * ny + y) * nz + z] = (int8_t)wall; --open; }
+            }
+    OrcXorShift rng(seed);
+    const size_t target = (size_t)(porosity * (double)N);
+    for (int guard = 0; open > target && guard < 10000000; ++guard) {
+        const int cx = rng.below(nx), cy = rng.below(ny), cz = rng.below(nz);
+        const double r = rmin + (rmax - rmin) * rng.uniform();
+        const int ri = (int)std::ceil(r);
+        for (int x = std::max(0, cx - ri); x <= std::min(nx - 1, cx + ri); ++x)
+            for (int y = std::max(0, cy - ri); y <= std::min(ny - 1, cy + ri); ++y)
+                for (int z = std::max(0, cz - ri); z <= std::min(nz - 1, cz + ri); ++z) {
+                    const double dx = x - cx, dy = y - cy, dz = z - cz;
+                    if (dx * dx + dy * dy + dz * dz > r * r) continue;
+                    int8_t& v = m[((size_t)x * ny + y) * nz + z];
+                    if (v == (int8_t)pore) { v = (int8_t)grain; --open; }
+                }
+    }
+    std::copy(m.begin(), m.end(), out);
+    return 0;
 }

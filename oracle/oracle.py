@@ -68,9 +68,10 @@ def lib():
             "orc_ade_set_thermo": ([vp, ip, vp, vp, vp], None), "orc_thermo_factor": ([vp, vp], dp),
             "orc_ade_set_immobile": ([vp, ip, vp], None), "orc_ade_set_stamp": ([vp, vp], None),
             "orc_ade_stamp": ([vp, vp], None),
-            "orc_ca_mask_total_once": ([vp], None), "orc_ca_age_relax": ([vp, ip], ip),
+            "orc_ca_mask_total_once": ([vp], None), "orc_ca_set_half": ([vp, ip], None), "orc_ca_age_relax": ([vp, ip], ip),
             "orc_ca_age_flags": ([vp, vp], None),
             "orc_dissolution_increments": ([ip, ip, ip, ip, ip, dp, ip, vp, ip, vp, ip, ip, vp, vp, vp], None),
+            "orc_sphere_pack": ([ip, ip, ip, dp, dp, dp, C.c_uint64, C.c_char_p, ip, ip, ip, vp], ip),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -82,6 +83,15 @@ def lib():
 
 def _p(a):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def sphere_pack(nx, ny, nz, porosity, rmin, rmax, seed, walls="yz", grain=1, wall=1, pore=2):
+    """The porosity-targeted sphere pack of the library's clb_geom_sphere_pack, restated in the
+    oracle (the CPU baseline builds its input maps with it, without the product library)."""
+    out = np.empty(nx * ny * nz, dtype=np.int8)
+    if lib().orc_sphere_pack(nx, ny, nz, porosity, rmin, rmax, seed, walls.encode(), grain, wall, pore, _p(out)):
+        raise ValueError("bad sphere-pack arguments")
+    return out
 
 
 def set_threads(n):
@@ -268,11 +278,13 @@ class OracleAde:
         lib().orc_ade_material(self.h, _p(m))
         return m
 
-    def ca_setup(self, bmax, frac, seed, pore_codes=(2,), bb=1, solid=0, bio_codes=(3, 4)):
+    def ca_setup(self, bmax, frac, seed, pore_codes=(2,), bb=1, solid=0, bio_codes=(3, 4), half=False):
+        """half: the 'half' push (halfPushExcessBiomass3D) instead of 'fraction'."""
         pc = np.ascontiguousarray(pore_codes, dtype=np.int32)
         bc = np.ascontiguousarray(bio_codes[:self.M], dtype=np.int32)
         self._ca = (pc, bc)
         lib().orc_ca_setup(self.h, float(bmax), float(frac), int(seed), pc.size, _p(pc), int(bb), int(solid), _p(bc))
+        lib().orc_ca_set_half(self.h, int(bool(half)))
 
     def ca_step(self):
         a, b = C.c_int(), C.c_int()

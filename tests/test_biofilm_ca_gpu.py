@@ -15,7 +15,7 @@ SP = [dict(omega_pore=1 / 0.9, omega_biofilm=1 / 0.7, left_type=0, right_type=1,
       dict(omega_pore=1 / 0.75, omega_biofilm=1 / 0.6, left_type=1, right_type=1, c0=0.5)]
 
 
-def setup(clb, oracle, shape, seed, lo, hi, bmax=100.0, frac=0.1, ca_seed=77):
+def setup(clb, oracle, shape, seed, lo, hi, bmax=100.0, frac=0.1, ca_seed=77, half=False):
     mat = mixed_geometry(*shape, seed=seed)
     N = mat.size
     P = shape[1] * shape[2]
@@ -32,8 +32,8 @@ def setup(clb, oracle, shape, seed, lo, hi, bmax=100.0, frac=0.1, ca_seed=77):
     D.set_biomass(bio)
     O = oracle.OracleAde(mat, *shape, SP, np.zeros(3 * N), bio_codes=(3, 4))
     O.set_biomass(bio)
-    D.ca_setup(bmax, frac, ca_seed)
-    O.ca_setup(bmax, frac, ca_seed)
+    D.ca_setup(bmax, frac, ca_seed, half=half)
+    O.ca_setup(bmax, frac, ca_seed, half=half)
     return D, O, mat
 
 
@@ -126,3 +126,35 @@ def test_ca_then_flow_refresh_runs(clb, oracle):
     biofilm = (m != 0) & (m != 1) & (m != 2)
     assert np.abs(u[:, biofilm]).max() == 0.0
     assert np.abs(u[0, m == 2]).max() > 0.0
+
+
+@pytest.mark.parametrize("shape,seed", [((18, 12, 10), 41), ((24, 16, 13), 42)])
+def test_ca_half_push_bit_exact_over_growth_cycles(clb, oracle, shape, seed):
+    """'half' push mode (halfPushExcessBiomass3D, complab3d_processors_part1.hh:735-970): biofilm
+    voxels above the maximum push half their biomass; the GPU equals the sequential oracle bit for
+    bit after every iteration, and the total biomass is conserved to round-off."""
+    D, O, mat = setup(clb, oracle, shape, seed, 60.0, 420.0, half=True)
+    swept = 0
+    for cycle in range(4):
+        before = sum(D.biomass(m).sum() for m in range(2))
+        st, sw, ch = D.ca_step()
+        rc, sw_o, ch_o = O.ca_step()
+        assert rc == 0 and (sw, ch) == (sw_o, ch_o), (cycle, sw, ch, sw_o, ch_o)
+        swept += sw
+        assert_same(D, O)
+        after = sum(D.biomass(m).sum() for m in range(2))
+        assert abs(after - before) <= 1e-12 * before
+        grown = np.stack([D.biomass(m) for m in range(2)]) * 1.25
+        D.set_biomass(grown)
+        O.set_biomass(grown)
+    assert swept > 1
+
+
+def test_half_and_fraction_differ(clb, oracle):
+    """The two push modes are different automata on the same state."""
+    runs = []
+    for half in (False, True):
+        D, O, mat = setup(clb, oracle, (18, 12, 10), 43, 60.0, 420.0, half=half)
+        D.ca_step()
+        runs.append(np.stack([D.biomass(m) for m in range(2)]))
+    assert np.max(np.abs(runs[0] - runs[1])) > 1.0

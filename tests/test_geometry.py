@@ -71,3 +71,11 @@ def test_sphere_pack_hits_porosity_and_is_seeded(clb, phi, rmin, rmax):
     g = a.reshape(n)
     assert np.all(g[:, 0, :] == 1) and np.all(g[:, :, -1] == 1)
     assert clb.inspect(a, *n)["percolates"] == 1
+
+
+def test_oracle_sphere_pack_equals_the_library(clb, oracle):
+    """The oracle's restatement of the sphere pack (the CPU baseline's input maps) is the
+    library's generator voxel for voxel."""
+    for args in ((40, 24, 20, 0.40, 4.0, 4.0, 1001, "yz"), (30, 17, 19, 0.35, 3.0, 8.0, 1002, "y"),
+                 (25, 25, 25, 0.6, 2.0, 5.5, 7, "all")):
+        np.testing.assert_array_equal(clb.sphere_pack(*args), oracle.sphere_pack(*args))
