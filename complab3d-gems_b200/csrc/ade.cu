@@ -257,7 +257,7 @@ __device__ __forceinline__ uint32_t ade_gather(TS* __restrict__ g, const TC* __r
 #pragma unroll
     for (int m = 0; m < NM; ++m) {
         if (m >= n_mobile) continue;
-        const int s = mob_species[m];
+        const int s = m;  // internal order puts the mobile species first: mobile slot m is species m
         if ((west && P.ltype[s] == CLB_CLOSED) || (east && P.rtype[s] == CLB_CLOSED)) continue;  // bounce-back
         actm |= 1u << m;
         const TS* f = g + (int64_t)m * S.SS;
@@ -311,7 +311,7 @@ __device__ __forceinline__ void ade_finish(TS* __restrict__ g, double* __restric
         if ((west || east) && dyn != ADE_NONE) {
             // AdvectionDiffusionBoundaryDynamics: the one inward population makes the
             // node's density equal to the stored value
-            const int s = mob_species[m];
+            const int s = m;  // internal order puts the mobile species first: mobile slot m is species m
             const int type = west ? P.ltype[s] : P.rtype[s];
             double rs;
             if (type == CLB_DIRICHLET) rs = west ? P.lbc[s] : P.rbc[s];
@@ -355,7 +355,7 @@ __device__ __forceinline__ void ade_finish(TS* __restrict__ g, double* __restric
 #pragma unroll
     for (int m = 0; m < NM; ++m) {
         if (!((actm >> m) & 1u)) continue;
-        const int s = mob_species[m];
+        const int s = m;  // internal order puts the mobile species first: mobile slot m is species m
         TC q[7], o[7];
 #pragma unroll
         for (int i = 0; i < 7; ++i) q[i] = F.pop[(m * 7 + i) * T];

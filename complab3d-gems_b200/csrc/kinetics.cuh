@@ -36,7 +36,7 @@ __device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[N
                 if (s < P.S) R[s] = -(KT)P.prm[s] * C[s] / ((KT)P.prm[CLB_MAX_SPECIES + s] + C[s]);
             break;
         case CLB_LAW_DUAL_MONOD: {
-            const KT mu = (KT)P.prm[0], ks = (KT)P.prm[1], Y = (KT)P.prm[2], kd = (KT)P.prm[3];
+            const KT mu = (KT)P.prm[0], ks = (KT)P.prm[1], invY = (KT)(1.0 / P.prm[2]), kd = (KT)P.prm[3];
             const int don = P.donor;
             KT Cd = 0;
 #pragma unroll
@@ -54,13 +54,16 @@ __device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[N
 #pragma unroll
                 for (int s = 0; s < NB; ++s)
                     if (s == a) Ca = C[s];
-                const KT growth = mu * (Cd / (ks + Cd)) * (Ca / (ks + Ca)) * Bm;
+                // mu Cd/(ks + Cd) Ca/(ks + Ca) B with one division, and 1/Y formed once: the same
+                // rate to the last bits or two
+                const KT growth = mu * Cd * Ca * Bm / ((ks + Cd) * (ks + Ca));
                 KT rbm = growth - kd * Bm;
                 if (ft < (KT)1) rbm *= ft;
-                Rd -= growth / Y;
+                const KT gy = growth * invY;
+                Rd -= gy;
 #pragma unroll
                 for (int s = 0; s < NB; ++s)
-                    if (s == a) R[s] -= growth / Y;
+                    if (s == a) R[s] -= gy;
                 if (APPLY_BIO) {
                     KT d = rbm * (KT)P.dt;
                     if (d > thr || d < -thr) {
