@@ -188,6 +188,12 @@ SIGNATURES = {
     "clb_surrogate_gradient": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
     "clb_get_field": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int],
     "clb_set_field": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int],
+    "clb_case_load": [C.c_char_p, C.POINTER(C.c_void_p)],
+    "clb_case_free": [C.c_void_p],
+    "clb_case_error": [],
+    "clb_case_get": [C.c_void_p, C.c_char_p, C.POINTER(C.c_double)],
+    "clb_case_setup": [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
+    "clb_case_run": [C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.POINTER(RunReport)],
     "clb_geom_generate": [C.POINTER(GeomOptions), C.c_int, C.c_int, C.c_int, C.c_void_p],
     "clb_geom_sphere_pack": [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint64,
                              C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p],
@@ -208,7 +214,7 @@ def lib():
         for name, args in SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = C.c_char_p if name in ("clb_last_error", "clb_global_error") else C.c_int
+            fn.restype = C.c_char_p if name in ("clb_last_error", "clb_global_error", "clb_case_error") else C.c_int
         _lib = L
     return _lib
 
@@ -640,6 +646,54 @@ def vti_write(path, shape, arrays):
     ct = (C.c_int32 * max(n, 1))(*types)
     cd = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in keep])
     _check_global(lib().clb_vti_write(os.fsencode(path), nx, ny, nz, n, cn, cc, ct, cd))
+
+
+class Case:
+    """A CompLaB.xml run description (clb_case_*): parse, set up a Domain from it with the
+    reference's unit chain, run it."""
+
+    def __init__(self, xml_path):
+        c = C.c_void_p()
+        st = lib().clb_case_load(os.fsencode(xml_path), C.byref(c))
+        if st != 0:
+            raise ClbError(st, lib().clb_case_error().decode())
+        self.c = c
+
+    def get(self, key):
+        v = C.c_double()
+        st = lib().clb_case_get(self.c, key.encode(), C.byref(v))
+        if st != 0:
+            raise ClbError(st, lib().clb_case_error().decode())
+        return v.value
+
+    def setup(self, flow_precision=F64, ade_precision=F64):
+        """The Domain the description builds (its handle owned by the returned object)."""
+        h = C.c_void_p()
+        st = lib().clb_case_setup(self.c, int(flow_precision), int(ade_precision), C.byref(h))
+        if st != 0:
+            raise ClbError(st, lib().clb_case_error().decode())
+        D = Domain.__new__(Domain)
+        D.h = h
+        D.nx, D.ny, D.nz = int(self.get("nx")), int(self.get("ny")), int(self.get("nz"))
+        D.N = D.nx * D.ny * D.nz
+        D.S = int(self.get("n_substrates"))
+        return D
+
+    def run(self, D, iterations=-1, output_dir=None):
+        r = RunReport()
+        st = lib().clb_case_run(self.c, D.h, int(iterations), None if output_dir is None else os.fsencode(output_dir),
+                                C.byref(r))
+        if st != 0:
+            raise ClbError(st, lib().clb_case_error().decode())
+        return {k: getattr(r, k) for k, _ in RunReport._fields_}
+
+    def close(self):
+        if getattr(self, "c", None):
+            lib().clb_case_free(self.c)
+            self.c = None
+
+    def __del__(self):
+        self.close()
 
 
 class Batch:

@@ -589,6 +589,45 @@ clb_status clb_write_vti(clb_handle* h, int field, int index, const char* path);
 clb_status clb_vti_write(const char* path, int nx, int ny, int nz, int n_arrays, const char* const* names,
                          const int32_t* components, const int32_t* dtypes, const void* const* data);
 
+/* ---------------------------------------------------------------- run descriptions (CompLaB.xml) */
+
+/* A parsed CompLaB.xml. Replaces: initialize_complab (complab_functions.hh:825-1602) for the
+ * parameters of the reactive-transport path -- <path>, <LB_numerics> (domain, material numbers,
+ * delta_P, Peclet, tau, iteration), <chemistry> (substrates, <immobile>), <microbiology>
+ * (cellular-automaton microbes, maximum_biomass_density, thrd_biofilm_fraction, CA_method),
+ * <equilibrium>, <precipitation> -- with the reference's element names, defaults and checks.
+ * Errors (a missing required element, a malformed number, an unknown boundary type, ...) return
+ * CLB_INVALID_ARG with the message in clb_case_error(). Rate laws are compiled code in the
+ * reference (defineRxnKinetics); after clb_case_setup they are selected with clb_set_kinetics. */
+typedef struct clb_case_s clb_case;
+clb_status clb_case_load(const char* xml_path, clb_case** out);
+clb_status clb_case_free(clb_case* c);
+const char* clb_case_error(void);
+
+/* A number of the run description by name: "nx" (ghost planes included), "ny", "nz", "dx" (m),
+ * "char_length" (lattice units), "tau", "delta_P", "Peclet", "ns_max_iT1", "ns_max_iT2",
+ * "ns_converge_iT1", "ns_converge_iT2", "ns_update_interval", "ade_update_interval", "ade_max_iT",
+ * "n_substrates", "n_microbes", "substrate.<i>.{c0,d_pore,d_biofilm,left_type,right_type,left_bc,
+ * right_bc,mobile}", "microbe.<m>.{code,perm_ratio}"; after clb_case_setup also the unit chain
+ * "refNu", "refTau", "ade_dt" (s per iteration), "substrate.<i>.omega_pore" / "omega_biofilm", and
+ * with flow "pore_mean_u", "delta_P_used", "flow_iterations", "flow_converged". */
+clb_status clb_case_get(const clb_case* c, const char* key, double* value);
+
+/* The set-up phases of the reference's main program (complab.cpp:1036-1290) on the current
+ * device: the geometry file (<input_path>/<filename> beside the XML) with its ghost planes, the
+ * handle, at Pe > 0 the flow solved to ns_converge_iT1 with the Peclet rescale and PoreMeanU
+ * (complab.cpp:1093-1183), the unit chain refNu / refTau / ade_dt and every species' relaxation
+ * rates (complab.cpp:1213-1253), the species lattices with the velocity coupled, the biomass fields
+ * from initial_densities and the automaton, the equilibrium tableau (Newton-Raphson speciation in
+ * every step), the precipitation phase. *out receives the handle (the caller destroys it). */
+clb_status clb_case_setup(clb_case* c, int flow_precision, int ade_precision, clb_handle** out);
+
+/* iterations (< 0: the description's ade_max_iT) coupled iterations through clb_run with the
+ * description's schedule (ade/ns update intervals, ns_max_iT2 / ns_converge_iT2 re-solves, the
+ * precipitation interval); with output_dir and save_VTK_interval > 0, one .vti file per substrate
+ * every interval (<name>_<7-digit iteration>.vti, as writeAdvVTI names them). */
+clb_status clb_case_run(clb_case* c, clb_handle* h, int iterations, const char* output_dir, clb_run_report* report);
+
 /* ---------------------------------------------------------------- geometry (host) */
 
 /* complab_geom::GenOptions (complab3d_geometry.hh:111-120). */

@@ -1,0 +1,46 @@
+"""Run directories for the CompLaB.xml cases of tests/golden/cases: the XML copied beside an
+input/ folder holding its geometry file, written from a seeded map in the reference's .dat order
+(interior x-planes, x slowest, z fastest, one integer per line)."""
+import os
+import shutil
+
+import numpy as np
+
+HERE = os.path.join(os.path.dirname(__file__), "golden", "cases")
+
+
+def write_dat(path, inner):
+    with open(path, "w") as f:
+        f.write("\n".join(str(int(v)) for v in np.asarray(inner).ravel()))
+        f.write("\n")
+
+
+def carbonate_duct_map():
+    nx, ny, nz = 20, 12, 10
+    m = np.full((nx, ny, nz), 2, np.int8)
+    m[:, 0, :] = m[:, -1, :] = 1
+    m[:, :, 0] = m[:, :, -1] = 1
+    m[6:9, 4:8, 3:6] = 1
+    m[13:15, 2:5, 5:9] = 0
+    return m
+
+
+def biofilm_flow_map(clb):
+    nx, ny, nz = 22, 12, 11
+    m = clb.sphere_pack(nx, ny, nz, 0.55, 2.0, 3.0, 33, "yz").reshape(nx, ny, nz)
+    rng = np.random.default_rng(33)
+    pore = np.argwhere(m == 2)
+    pore = pore[(pore[:, 0] > 2) & (pore[:, 0] < nx - 3)]
+    pick = pore[rng.choice(len(pore), size=40, replace=False)]
+    for k, (x, y, z) in enumerate(pick):
+        m[x, y, z] = 3 if k % 2 == 0 else 4
+    return m
+
+
+def run_dir(tmp, name, inner):
+    d = os.path.join(str(tmp), name)
+    os.makedirs(os.path.join(d, "input"), exist_ok=True)
+    shutil.copy(os.path.join(HERE, name + ".xml"), os.path.join(d, "CompLaB.xml"))
+    fname = {"carbonate_duct": "duct.dat", "biofilm_flow": "pack.dat"}[name]
+    write_dat(os.path.join(d, "input", fname), inner)
+    return os.path.join(d, "CompLaB.xml")
