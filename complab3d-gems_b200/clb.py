@@ -156,6 +156,8 @@ SIGNATURES = {
     "clb_set_kinetics": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double],
     "clb_set_biomass": [C.c_void_p, C.c_int, C.c_void_p],
     "clb_set_thermo_gate": [C.c_void_p, C.POINTER(ThermoDesc)],
+    "clb_set_symbolic_kinetics": [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int, C.c_char_p],
+    "clb_symbolic_eval": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)],
     "clb_write_vti": [C.c_void_p, C.c_int, C.c_int, C.c_char_p],
     "clb_checkpoint_save": [C.c_void_p, C.c_char_p, C.c_int],
     "clb_checkpoint_load": [C.c_void_p, C.c_char_p],
@@ -488,6 +490,24 @@ class Domain:
         d.dG0, d.atp, d.dGatp, d.chi, d.cmin, d.dGloss = dG0, atp, dGatp, chi, cmin, dGloss
         d.temperature, d.gas_constant, d.conc_scale = temperature, gas_constant, conc_scale
         self._check(lib().clb_set_thermo_gate(self.h, C.byref(d)))
+
+    def set_symbolic_kinetics(self, path, species_names, microbe=-1, microbe_name=""):
+        """A rate law read from a .sym file: microbe m's law (its biomass variable named
+        microbe_name in the file), or the abiotic law for microbe = -1; species_names name the
+        handle's species in user order."""
+        arr = (C.c_char_p * len(species_names))(*[n.encode() for n in species_names])
+        self._check(lib().clb_set_symbolic_kinetics(self.h, os.fsencode(path), C.cast(arr, C.c_void_p), int(microbe),
+                                                    microbe_name.encode()))
+
+    def symbolic_eval(self, microbe, X):
+        """The bound law's rates on the rows of X (its variables in file order), by the device
+        interpreter."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        nr = C.c_int()
+        self._check(lib().clb_symbolic_eval(self.h, int(microbe), None, 0, None, C.byref(nr)))
+        out = np.zeros((X.shape[0], nr.value))
+        self._check(lib().clb_symbolic_eval(self.h, int(microbe), _ptr(X), X.shape[0], _ptr(out), C.byref(nr)))
+        return out
 
     def checkpoint_save(self, path, flow=True, transport=True):
         """A restart file of the flow and/or transport lattices (FP64, exact)."""

@@ -39,7 +39,72 @@ constexpr int ADE_THREADS = 128;
 // the increments of the mobile species in dC (internal species m = slot m); immobile species and
 // biomass are updated in place. `bc` holds the biomass of the first `bn` microbes as staged with
 // the node's gathers (stride ADE_THREADS).
-template <typename TC, int NM, bool EXT>
+// The organisms' rate laws read from .sym files (CLB_LAW_SYMBOLIC), as run_symbolic3D applies them
+// (complab3d_processors_symbolic.hh:100-200), in FP64: concentrations at or below 1e-12 read as 0;
+// every organism whose biomass exceeds 1e-12 evaluates its program on them (its own biomass as
+// its variable), requests rate x F_T x dt of each substrate and grows by growth x F_T x biomass x
+// dt (never below zero); the requests of all organisms then share each substrate's headroom: a draw
+// larger than what the voxel holds takes what it holds. F_T is the gate of microbe 0's block.
+template <typename TC, int NM>
+__device__ __noinline__ void sym_biotic(const AdeParams& P, int n_mobile, const TC* rb, double* __restrict__ imm,
+                                        double* __restrict__ bio, int64_t nd, TC* dC) {
+    const int64_t N = P.g.N;
+    double C[NM], req[NM];
+#pragma unroll
+    for (int s = 0; s < NM; ++s) {
+        double c = 0.0;
+        if (s < n_mobile) c = (double)rb[s] + 1.0;
+        else if (s < P.S) c = imm[(int64_t)s * N + nd];
+        C[s] = c > THRD ? c : 0.0;
+        req[s] = 0.0;
+    }
+    for (int m = 0; m < P.M; ++m) {
+        if (!((P.sym_mask >> m) & 1u)) continue;
+        const double b = bio[(int64_t)m * N + nd];
+        const double bm = b > THRD ? b : 0.0;
+        if (!(bm > THRD)) continue;
+        const SymProg& S = P.sym[m];
+        double x[SYM_MAX_VARS], y[SYM_MAX_RATES];
+        for (int v = 0; v < S.n_vars; ++v) {
+            const int src = S.var_src[v];
+            double xv = bm;
+            if (src >= 0) {
+#pragma unroll
+                for (int s = 0; s < NM; ++s)
+                    if (s == src) xv = C[s];
+            }
+            x[v] = xv;
+        }
+        sym_eval(S, x, y);
+        const double ft = (m == 0 && P.gate_on) ? thermo_gate<double, NM>(P, C) : 1.0;
+        double dB = 0.0;
+        for (int r = 0; r < S.n_rates; ++r) {
+            const int dst = S.rate_dst[r];
+            if (dst >= 0) {
+#pragma unroll
+                for (int s = 0; s < NM; ++s)
+                    if (s == dst) req[s] += y[r] * ft * P.dt;
+            } else {
+                dB += y[r] * ft * bm * P.dt;
+            }
+        }
+        if (dB > THRD || dB < -THRD) {
+            if (dB + bm < 0.0) dB = -bm;
+            bio[(int64_t)m * N + nd] += dB;
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NM; ++s) {
+        if (s >= P.S) continue;
+        double draw = req[s];
+        if (!(draw > THRD || draw < -THRD)) continue;
+        if (draw + C[s] < 0.0) draw = -C[s];
+        if (s < n_mobile) dC[s] = (TC)draw;
+        else imm[(int64_t)s * N + nd] += draw;
+    }
+}
+
+template <typename TC, int NM, int EXT>
 __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra& X, int64_t k, int64_t nd, int code,
                                               bool west, bool east, int n_mobile, const TC (&rb)[NM],
                                               double* __restrict__ imm, double* __restrict__ bio,
@@ -47,7 +112,14 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra
     const Geom G = P.g;
 #pragma unroll
     for (int s = 0; s < NM; ++s) dC[s] = 0;
-    if (P.law != CLB_LAW_NONE && !west && !east && P.react[code]) {
+    bool sym_done = false;
+    if constexpr (EXT == 2) {
+        if (P.law == CLB_LAW_SYMBOLIC && !west && !east && P.react[code]) {
+            sym_biotic<TC, NM>(P, n_mobile, rb, imm, bio, nd, dC);
+            sym_done = true;
+        }
+    }
+    if (!sym_done && P.law != CLB_LAW_NONE && P.law != CLB_LAW_SYMBOLIC && !west && !east && P.react[code]) {
         // biotic block in the lattice's arithmetic type (FP64 lattices: FP64 throughout)
         const TC thr = (TC)THRD;
         TC C[NM], R[NM];
@@ -93,7 +165,7 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra
                 else if (s < P.S) c = imm[(int64_t)s * G.N + nd];
                 C[s] = c < THRD ? 0.0 : c;
             }
-            eval_rates2<NM>(P, C, R);
+            eval_rates2<NM, EXT == 2>(P, C, R);
 #pragma unroll
             for (int s = 0; s < NM; ++s) {
                 if (s >= P.S) continue;
@@ -288,7 +360,7 @@ __device__ __forceinline__ uint32_t ade_gather(TS* __restrict__ g, const TC* __r
 
 // The second half, once the staged values are in the frame: boundary completion, sums, kinetics,
 // collision with the deposit, scatter back to the node's slots.
-template <typename TS, typename TC, bool ODD, int NM, bool EXT, typename AP>
+template <typename TS, typename TC, bool ODD, int NM, int EXT, typename AP>
 __device__ __forceinline__ void ade_finish(TS* __restrict__ g, double* __restrict__ imm, double* __restrict__ bio,
                                            const TC* __restrict__ u, const SparseView& S, const double* __restrict__ neu, const AP& P,
                                            int n_mobile, const int* __restrict__ mob_species, int64_t k_west_end,
@@ -384,7 +456,7 @@ __device__ __forceinline__ void ade_finish(TS* __restrict__ g, double* __restric
     }
 }
 
-template <typename TS, typename TC, bool ODD, int NM, bool EXT, typename AP>
+template <typename TS, typename TC, bool ODD, int NM, int EXT, typename AP>
 __device__ __forceinline__ void ade_node(TS* __restrict__ g, double* __restrict__ imm, double* __restrict__ bio,
                                          const TC* __restrict__ u, const SparseView& S,
                                          const double* __restrict__ neu, const AP& P, int n_mobile,
@@ -398,7 +470,7 @@ __device__ __forceinline__ void ade_node(TS* __restrict__ g, double* __restrict_
                                      F, k, M, actm);
 }
 
-template <typename TS, typename TC, bool ODD, int NM, bool EXT>
+template <typename TS, typename TC, bool ODD, int NM, int EXT>
 __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>()))
     k_ade_aa(TS* __restrict__ g, double* __restrict__ imm, double* __restrict__ bio, const TC* __restrict__ u,
              const SparseView S, const double* __restrict__ neu, const AdeParams P, int n_mobile,
@@ -423,7 +495,7 @@ constexpr int ade_pipe_minb() {
 // finished from the other, and the metadata of the node after that is loading. Same arithmetic
 // and memory traffic as k_ade_aa. For 4- and 8-byte storage where two slot sets leave at least
 // two resident blocks per SM.
-template <typename TS, typename TC, bool ODD, int NM, bool EXT>
+template <typename TS, typename TC, bool ODD, int NM, int EXT>
 __global__ void __launch_bounds__(ADE_THREADS, (ade_pipe_minb<TC, NM>() < 1 ? 1 : ade_pipe_minb<TC, NM>()))
     k_ade_pipe(TS* __restrict__ g, double* __restrict__ imm, double* __restrict__ bio, const TC* __restrict__ u,
                const SparseView S, const double* __restrict__ neu, const AdeParams P, int n_mobile,
@@ -530,6 +602,37 @@ __global__ void k_ade_get_pops(const TS* __restrict__ g, const TS* __restrict__ 
         double v[7];
         natural<TS, double, 7>(S, G, g, glink, n, odd, init, v);
         for (int i = 0; i < 7; ++i) out[(int64_t)i * G.N + n] = v[i];
+    }
+}
+
+// computeDensity of species s (internal index) at every voxel: BGK nodes of a Dirichlet / Neumann
+// plane report the stored value; every other voxel 1 + the sum of its incoming populations (a voxel
+// that is not a node holds the initial equilibrium at c0).
+template <typename TS>
+__global__ void k_ade_density(const TS* __restrict__ g, const TS* __restrict__ glink, const SparseView S,
+                              const int8_t* __restrict__ mat, const AdeParams P, int s, int odd,
+                              const double* __restrict__ neu, double* __restrict__ out) {
+    const Geom G = P.g;
+    double init[7];
+    for (int i = 0; i < 7; ++i) init[i] = q7w(i) * (P.c0[s] - 1.0);
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(n / G.plane);
+        const int p = (int)(n - (int64_t)x * G.plane);
+        const int dyn = P.dyn[(uint8_t)mat[n]];
+        const bool bgk = dyn == ADE_PORE || dyn == ADE_BIO;
+        if (bgk && x == 0 && P.ltype[s] != CLB_CLOSED) {
+            out[n] = P.ltype[s] == CLB_DIRICHLET ? P.lbc[s] : neu[p];
+            continue;
+        }
+        if (bgk && x == G.nx - 1 && P.rtype[s] != CLB_CLOSED) {
+            out[n] = P.rtype[s] == CLB_DIRICHLET ? P.rbc[s] : neu[G.plane + p];
+            continue;
+        }
+        double v[7];
+        natural<TS, double, 7>(S, G, g, glink, n, odd, init, v);
+        double r = 1.0;
+        for (int i = 0; i < 7; ++i) r += v[i];
+        out[n] = r;
     }
 }
 
@@ -692,6 +795,7 @@ void ade_free(clb_handle* h) {
     cudaFree(h->d_u); h->d_u = nullptr;
     cudaFree(h->d_neu); h->d_neu = nullptr;
     cudaFree(h->d_red); h->d_red = nullptr;
+    cudaFree(h->d_stage); h->d_stage = nullptr;
     precip_free(h);
     ca_free(h);
     sparse_free(h->ade_sp);
@@ -842,6 +946,7 @@ clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm,
     AdeParams& P = h->ap;
     const int S = h->S;
     P.law = law;
+    P.sym_mask = 0;  // a compiled law replaces the organisms' rate-law files
     std::memset(P.prm, 0, sizeof(P.prm));
     switch (law) {
         case CLB_LAW_DECAY:
@@ -1022,7 +1127,7 @@ static void launch_ade_t(clb_handle* h) {
     const TC* u = (const TC*)h->d_u;
     int* mt = mob_table(h);
     const SparseView S = view_of(h->ade_sp);
-    const bool ext = h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on || h->ap.gate_on;
+    const bool ext = h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on || h->ap.gate_on || h->ap.law == CLB_LAW_SYMBOLIC;
     const AdeExtra X = ade_extra(h);
 #define CLB_ADE(NM, EXT)                                                                                          \
     do {                                                                                                          \
@@ -1042,15 +1147,23 @@ static void launch_ade_t(clb_handle* h) {
         kern<<<gr, ADE_THREADS, sm, h->stream>>>(g, h->d_imm, h->d_bio, u, S, h->d_neu, h->ap, nm, mt,            \
                                                  h->ade_west_end, h->ade_east_begin, X);                          \
     } while (0)
-    if (ext) {
-        if (nb <= 4) CLB_ADE(4, true);
-        else if (nb <= 8) CLB_ADE(8, true);
-        else CLB_ADE(16, true);
-    } else if (nb <= 1) CLB_ADE(1, false);
-    else if (nb <= 2) CLB_ADE(2, false);
-    else if (nb <= 4) CLB_ADE(4, false);
-    else if (nb <= 8) CLB_ADE(8, false);
-    else CLB_ADE(16, false);
+    // EXT: 0 the compiled biotic laws alone; 1 with the abiotic block, dissolution and the
+    // thermodynamic gate; 2 also the rate-law files (their interpreter's registers and stack stay
+    // out of the other instantiations)
+    const bool sym = h->ap.law == CLB_LAW_SYMBOLIC || h->ap.law2 == CLB_LAW_SYMBOLIC;
+    if (sym) {
+        if (nb <= 4) CLB_ADE(4, 2);
+        else if (nb <= 8) CLB_ADE(8, 2);
+        else CLB_ADE(16, 2);
+    } else if (ext) {
+        if (nb <= 4) CLB_ADE(4, 1);
+        else if (nb <= 8) CLB_ADE(8, 1);
+        else CLB_ADE(16, 1);
+    } else if (nb <= 1) CLB_ADE(1, 0);
+    else if (nb <= 2) CLB_ADE(2, 0);
+    else if (nb <= 4) CLB_ADE(4, 0);
+    else if (nb <= 8) CLB_ADE(8, 0);
+    else CLB_ADE(16, 0);
 #undef CLB_ADE
 }
 
@@ -1123,7 +1236,7 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>() > 6 ? 6 : ade
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int di = batch_find(soff, B.ndom, t);
         const BatchDomain& d = B.dom[di];
-        ade_node<TS, TC, ODD, NM, false>((TS*)d.g, d.imm, d.bio, (const TC*)d.u, d.as, d.neu, d.ap, d.n_mobile,
+        ade_node<TS, TC, ODD, NM, 0>((TS*)d.g, d.imm, d.bio, (const TC*)d.u, d.as, d.neu, d.ap, d.n_mobile,
                                          d.mob, d.akw, d.ake, X, F, t - soff[di]);
     }
 }
@@ -1298,30 +1411,28 @@ clb_status ade_density(clb_handle* h, int s, double* host) {
         return cuda_check(h, cudaMemcpy(host, h->d_imm + (size_t)s * N, sizeof(double) * N, cudaMemcpyDeviceToHost), "immobile copy");
     // the Neumann planes' stored values as the reference holds them after the last stream
     refresh_neumann(h);
-    std::vector<double> pops(7 * N);
-    clb_status st = ade_populations_i(h, s, pops.data());
-    if (st != CLB_OK) return st;
-    std::vector<double> neu((size_t)2 * h->g.plane);
-    cudaMemcpy(neu.data(), h->d_neu + (size_t)s * 2 * h->g.plane, sizeof(double) * neu.size(), cudaMemcpyDeviceToHost);
-    const AdeParams& P = h->ap;
-    for (size_t n = 0; n < N; ++n) {
-        const int x = (int)(n / h->g.plane);
-        const int p = (int)(n - (size_t)x * h->g.plane);
-        const int dyn = P.dyn[(uint8_t)h->h_mat[n]];
-        const bool bgk = dyn == ADE_PORE || dyn == ADE_BIO;
-        if (bgk && x == 0 && P.ltype[s] != CLB_CLOSED) {
-            host[n] = P.ltype[s] == CLB_DIRICHLET ? P.lbc[s] : neu[p];
-            continue;
-        }
-        if (bgk && x == h->g.nx - 1 && P.rtype[s] != CLB_CLOSED) {
-            host[n] = P.rtype[s] == CLB_DIRICHLET ? P.rbc[s] : neu[h->g.plane + p];
-            continue;
-        }
-        double r = 1.0;
-        for (int i = 0; i < 7; ++i) r += pops[(size_t)i * N + n];
-        host[n] = r;
+    if (!h->d_stage) {
+        cudaError_t e = cudaMalloc(&h->d_stage, sizeof(double) * N);
+        if (e != cudaSuccess) return cuda_check(h, e, "field staging buffer");
     }
-    return CLB_OK;
+    const int m = h->ap.slot[s];
+    const int odd = (int)(h->ade_iters & 1);
+    const size_t off = (size_t)m * h->ade_sp.SS;
+    const SparseView Sv = view_of(h->ade_sp);
+    const double* neu = h->d_neu + (size_t)s * 2 * h->g.plane;
+    const int grid = h->num_sms * 8;
+#define CLB_DENS(TS)                                                                                              \
+    k_ade_density<TS><<<grid, 256, 0, h->stream>>>((const TS*)h->d_g + off, (const TS*)h->d_glink + off, Sv, h->d_mat, \
+                                                   h->ap, s, odd, neu, h->d_stage)
+    switch (h->ade_prec) {
+        case CLB_F64: CLB_DENS(double); break;
+        case CLB_F32: CLB_DENS(float); break;
+        default: CLB_DENS(__half); break;
+    }
+#undef CLB_DENS
+    cudaError_t e = cudaMemcpyAsync(host, h->d_stage, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return cuda_check(h, e, "concentration copy");
 }
 
 clb_status ade_biomass(clb_handle* h, int m, double* host) {

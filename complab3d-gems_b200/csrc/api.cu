@@ -104,6 +104,7 @@ clb_status clb_destroy(clb_handle* h) {
     cudaFree(h->d_spec_stats);
     cudaFree(h->d_mlp);
     cudaFree(h->d_mlp_bf16);
+    cudaFree(h->d_sym);
     if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -261,6 +262,19 @@ clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass)
     if (!h || (n_microbes > 0 && !biomass)) return fail(h, CLB_INVALID_ARG, "null argument");
     CLB_ON_DEVICE(h);
     return ade_set_biomass(h, n_microbes, biomass);
+}
+
+clb_status clb_set_symbolic_kinetics(clb_handle* h, const char* sym_path, const char* const* species_names,
+                                     int microbe, const char* microbe_name) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    return symbolic_set(h, sym_path, species_names, microbe, microbe_name);
+}
+
+clb_status clb_symbolic_eval(clb_handle* h, int microbe, const double* vars, int n, double* rates, int* n_rates) {
+    if (!h || (n > 0 && (!vars || !rates))) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return symbolic_eval(h, microbe, vars, n, rates, n_rates);
 }
 
 clb_status clb_ade_step(clb_handle* h, int n) {

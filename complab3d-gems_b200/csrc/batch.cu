@@ -73,7 +73,8 @@ clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out) {
             delete b;
             return fail(nullptr, CLB_INVALID_ARG, "batch handles must share their storage precisions");
         }
-        if (b->has_ade && (h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on || h->ap.gate_on || h->spec_mode != CLB_SPEC_OFF)) {
+        if (b->has_ade && (h->ap.law2 != CLB_LAW_NONE || h->ap.dis_on || h->ap.gate_on || h->ap.law == CLB_LAW_SYMBOLIC ||
+                           h->spec_mode != CLB_SPEC_OFF)) {
             delete b;
             return fail(nullptr, CLB_INVALID_ARG,
                         "batched transport has no abiotic law, dissolution, thermodynamic gate or speciation");

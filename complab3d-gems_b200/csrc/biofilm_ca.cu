@@ -90,6 +90,7 @@ struct CaScalars {
     unsigned int changed;  // ages changed by a sweep
     unsigned int overflow; // active voxels beyond the capacity
     unsigned int nonfinite; // biomass values that are NaN or infinite (mask pass)
+    unsigned int moved;     // voxels whose material the mask pass changed
 };
 
 // ------------------------------------------------------------------ set-up and mask update
@@ -152,7 +153,10 @@ __global__ void k_ca_mask_total(const CaView C, int8_t* __restrict__ mat, const 
             } else if (poreflag && bmass >= C.thr && newmask > 0) {
                 out = newmask;
             }
-            if (out != mk) mat[n] = (int8_t)out;
+            if (out != mk) {
+                mat[n] = (int8_t)out;
+                atomicAdd(&sc->moved, 1u);
+            }
             msum += out;
         } else {
             msum += mk;
@@ -548,7 +552,7 @@ static clb_status ca_scalars(clb_handle* h, CaScalars& s) {
 }
 
 // mask / total pass; returns max(total) and the mask sum
-static clb_status ca_mask_pass(clb_handle* h, const CaView& C, double& gmax, long long& msum) {
+static clb_status ca_mask_pass(clb_handle* h, const CaView& C, double& gmax, long long& msum, unsigned int* moved) {
     // non-finite biomass stops the run cleanly, as the reference does after this pass
     // (complab.cpp:2794-2796)
     CaScalars s;
@@ -563,6 +567,7 @@ static clb_status ca_mask_pass(clb_handle* h, const CaView& C, double& gmax, lon
     if (st != CLB_OK) return st;
     gmax = unordered(s.gmax);
     msum = s.mask_sum;
+    if (moved) *moved += s.moved;
     if (s.nonfinite || !std::isfinite(gmax))
         return fail(h, CLB_NONFINITE, "non-finite biomass (NaN or Inf) in the biofilm fields");
     return CLB_OK;
@@ -662,7 +667,8 @@ clb_status ca_step(clb_handle* h, int* sweeps_out, int* mask_changed) {
     const CaView C = ca_view(h);
     double gmax;
     long long msum;
-    clb_status st = ca_mask_pass(h, C, gmax, msum);
+    unsigned int moved = 0;  // voxels the mask passes of this call changed
+    clb_status st = ca_mask_pass(h, C, gmax, msum, &moved);
     if (st != CLB_OK) return st;
     int whilecount = 0;
     clb_status rc = CLB_OK;
@@ -671,7 +677,7 @@ clb_status ca_step(clb_handle* h, int* sweeps_out, int* mask_changed) {
         int stall = 0;
         while (gmax - h->ca_bmax > THRD) {
             if ((st = ca_push_sweep(h, C)) != CLB_OK) return st;
-            if ((st = ca_mask_pass(h, C, gmax, msum)) != CLB_OK) return st;
+            if ((st = ca_mask_pass(h, C, gmax, msum, &moved)) != CLB_OK) return st;
             if (gmax > prev - THRD) {
                 if (++stall >= 100) { rc = fail(h, CLB_NOT_CONVERGED, "biofilm push stalled: excess biomass cannot spread"); break; }
             } else {
@@ -692,9 +698,13 @@ clb_status ca_step(clb_handle* h, int* sweeps_out, int* mask_changed) {
         h->ca_mask_sum = msum;
         ca_age_sweep_inplace(h, C);
     }
-    cudaError_t e = cudaMemcpy(h->h_mat.data(), h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_check(h, e, "mask copy");
-    if (changed) {
+    // the host copy of the map follows the device only when a voxel changed (an unchanged mask sum
+    // can hide changes that cancel, so the passes count changed voxels themselves)
+    if (moved) {
+        cudaError_t e = cudaMemcpy(h->h_mat.data(), h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_check(h, e, "mask copy");
+    }
+    if (moved) {
         st = geometry_refresh(h);
         if (st != CLB_OK) return st;
     }

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/clb.h"
+#include "symbolic.cuh"
 
 namespace clb {
 
@@ -132,6 +133,10 @@ struct AdeParams {
     double gate_dG0, gate_dGloss, gate_atp, gate_dGatp, gate_chi, gate_cmin, gate_RT, gate_cscale;
     double gate_x0, gate_inv_chi;   // (dG0 + dGloss + atp dGatp) / (chi RT) and 1 / chi
     int* nonfinite;                 // host-mapped flag a transport step sets on a NaN / Inf density
+    // rate laws read from .sym files (law / law2 CLB_LAW_SYMBOLIC): programs [microbe], then the
+    // abiotic one at [CLB_MAX_MICROBES]; sym_mask: the microbes that have one
+    const SymProg* sym;
+    uint32_t sym_mask;
 };
 
 // Per-node state of the precipitation / dissolution machinery (geometry_update.cu), passed to the
@@ -180,6 +185,8 @@ struct clb_handle_s {
     int num_sms = 148;
     std::string err;
     int64_t launches = 0;             // kernels this handle enqueued on the coupled step's path
+    void* d_sym = nullptr;            // SymProg[SYM_MAX_PROGS] on the device
+    clb::SymProg sym_host[clb::SYM_MAX_PROGS];
     std::vector<int8_t> h_mat;
     int8_t* d_mat = nullptr;
 
@@ -223,6 +230,7 @@ struct clb_handle_s {
     void* d_u = nullptr;              // [3][K] advection velocity (arithmetic type)
     double* d_neu = nullptr;          // [S][2][ny*nz] stored boundary densities
     double* d_red = nullptr;          // scratch of clb_reduce (partials, then the result)
+    double* d_stage = nullptr;        // [N] staging of a field read back to the host
     clb::AdeParams ap;
     int64_t ade_iters = 0;
     int64_t neu_iter = -1;            // iteration whose stream the Neumann store reflects
@@ -343,6 +351,12 @@ void ca_free(clb_handle* h);
 
 // driver.cu
 clb_status run(clb_handle* h, const clb_run_desc* d, clb_run_report* r);
+
+// symbolic.cu
+clb_status symbolic_set(clb_handle* h, const char* path, const char* const* species_names, int microbe,
+                        const char* microbe_name);
+clb_status symbolic_eval(clb_handle* h, int which, const double* vars, int n, double* rates, int* n_rates);
+void sym_eval_batch(clb_handle* h, int slot, const double* dvars, int n, double* drates);
 
 // speciation.cu
 clb_status speciation_setup(clb_handle* h, const clb_speciation_desc* d);

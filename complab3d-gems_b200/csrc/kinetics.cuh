@@ -119,7 +119,9 @@ __device__ __forceinline__ KT thermo_gate(const AdeParams& P, const KT (&C)[NB])
 // Abiotic laws (clb_law CLB_LAW_PRECIP / CLB_LAW_MINERAL) over internal species indices, evaluated
 // on the concentrations the biotic law left (run_abiotic_kinetics, complab3d_processors_part1.hh:
 // 199-297, with the rate law of the reference's defineAbioticRxnKinetics).
-template <int NB>
+// SYM: also the abiotic rate-law file (CLB_LAW_SYMBOLIC); the instantiations without it keep their
+// registers.
+template <int NB, bool SYM = true>
 __device__ __forceinline__ void eval_rates2(const AdeParams& P, const double (&C)[NB], double (&R)[NB]) {
 #pragma unroll
     for (int s = 0; s < NB; ++s) R[s] = 0.0;
@@ -137,6 +139,24 @@ __device__ __forceinline__ void eval_rates2(const AdeParams& P, const double (&C
             if (s == a) R[s] -= r;
             if (s == b) R[s] -= r;
             if (s == q) R[s] += r;
+        }
+    } else if (SYM && P.law2 == CLB_LAW_SYMBOLIC) {
+        // an abiotic rate-law file: the extent and the species rates it derives, on the floored
+        // concentrations (complab3d_processors_abiotic_learned.hh reads the same values)
+        const SymProg& S = P.sym[CLB_MAX_MICROBES];
+        double x[SYM_MAX_VARS], y[SYM_MAX_RATES];
+        for (int v = 0; v < S.n_vars; ++v) {
+            double xv = 0.0;
+#pragma unroll
+            for (int s = 0; s < NB; ++s)
+                if (s == S.var_src[v]) xv = C[s];
+            x[v] = xv;
+        }
+        sym_eval(S, x, y);
+        for (int r = 0; r < S.n_rates; ++r) {
+#pragma unroll
+            for (int s = 0; s < NB; ++s)
+                if (s == S.rate_dst[r]) R[s] += y[r];
         }
     } else if (P.law2 == CLB_LAW_MINERAL) {
         const int q = (int)P.prm2[2];

@@ -57,6 +57,8 @@ typedef enum clb_law {
     /* abiotic laws (clb_set_abiotic_kinetics; defineAbioticRxnKinetics of the reference) */
     CLB_LAW_PRECIP = 4,     /* params kp, a, b, p: A + B -> P(s), R = kp max(C_a,0) max(C_b,0),
                                R_a = R_b = -R, R_p = +R (examples/13_precipitation)          */
+    CLB_LAW_SYMBOLIC = 6,   /* a rate-law file read at run time (clb_set_symbolic_kinetics);
+                               not selected through clb_set_kinetics / clb_set_abiotic_kinetics */
     CLB_LAW_MINERAL = 5     /* params k, log10 Ksp, p, nu[S]: saturation
                                Omega = 10^(sum_{j != p} nu_j log10 C_j - log10 Ksp),
                                R_p = k (Omega - 1), R_j = -nu_j R_p: the mineral p grows when the
@@ -259,6 +261,31 @@ typedef struct clb_thermo_desc {
  * Replaces: complab_thermo::gateFor (complab3d_thermo.hh:215-258, 669-692) in run_kinetics
  * (complab3d_processors_part1.hh:134-141) with one reaction block. */
 clb_status clb_set_thermo_gate(clb_handle* h, const clb_thermo_desc* desc);
+
+/* A rate law read at run time from a .sym file (the reference's complab3d_symbolic.hh format:
+ * units / vars / range / rate / reaction / yield / biomass lines; expressions with + - * / ^,
+ * exp log log10 sqrt abs tanh min max pow, pi, e; rate lines may use earlier ones; a 'reaction'
+ * line derives the species lines), compiled on the host and evaluated per voxel in FP64 inside the
+ * fused transport step. species_names[S] names the handle's species (user order) for the file's
+ * variables and rate outputs.
+ *   microbe >= 0: the law of the organism whose biomass field is `microbe` (a 'growth' line;
+ *     microbe_name is its variable in the file): where its biomass exceeds 1e-12, the substrate
+ *     rates are requested and the growth rate times the biomass grows it; the requests of all
+ *     organisms of a voxel share each substrate's headroom (a draw never takes more than the
+ *     voxel holds), as run_symbolic3D does (complab3d_processors_symbolic.hh:100-200).
+ *   microbe = -1: an abiotic law (an 'extent' line), in place of clb_set_abiotic_kinetics, in every
+ *     reacting voxel, each increment clamped at what the voxel holds.
+ * Variables are clamped to the file's ranges; per_hour rates are divided by 3600; the time step is
+ * clb_set_kinetics's dt. Replaces: complab_sym::load / evaluate (complab3d_symbolic.hh:420-1063)
+ * and run_symbolic3D. */
+clb_status clb_set_symbolic_kinetics(clb_handle* h, const char* sym_path, const char* const* species_names,
+                                     int microbe, const char* microbe_name);
+
+/* The bound law of `microbe` (-1: the abiotic one) on n rows of its variables in file order
+ * (vars [n][n_vars], host) into rates [n][n_rates] (host; rate lines in file order, derived lines
+ * last, units applied), evaluated by the device interpreter; *n_rates receives the rate count
+ * (may be NULL). */
+clb_status clb_symbolic_eval(clb_handle* h, int microbe, const double* vars, int n, double* rates, int* n_rates);
 
 /* Biomass fields of the CA microbes, [n_microbes][N] float64. */
 clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass);

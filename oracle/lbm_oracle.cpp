@@ -50,9 +50,13 @@
  *       (complab3d_processors_symbolic.hh:165-180); applied only if |dC| > 1e-12;
  *       biomass never negative (ibid. :193).
  */
+#include <cctype>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
+#include <sstream>
 #include <string>
 #include <vector>
 #include <algorithm>
@@ -350,8 +354,25 @@ void orc_flow_set_populations(OrcFlow* F, const double* in) {
 // =====================================================================================
 enum { ADE_BB = 0, ADE_NONE = 1, ADE_PORE = 2, ADE_BIO = 3 };
 enum { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_CLOSED = 2 };
-enum { LAW_NONE = 0, LAW_DECAY = 1, LAW_MONOD = 2, LAW_DUAL_MONOD = 3, LAW_PRECIP = 4, LAW_MINERAL = 5 };
+enum { LAW_NONE = 0, LAW_DECAY = 1, LAW_MONOD = 2, LAW_DUAL_MONOD = 3, LAW_PRECIP = 4, LAW_MINERAL = 5, LAW_SYMBOLIC = 6 };
 enum { DISSOL_NONE = 0, DISSOL_FIRST_ORDER = 1, DISSOL_MINERAL = 2 };
+
+// ---- rate laws read from a .sym file (complab3d_symbolic.hh restated; see the section below)
+struct SymNode {
+    int kind;         // 0 const, 1 var, 2 neg, 3 add, 4 sub, 5 mul, 6 div, 7 pow, 8 exp, 9 log, 10 log10,
+                      // 11 sqrt, 12 abs, 13 tanh, 14 min, 15 max
+    double value;
+    int a, b;
+};
+struct SymLaw {
+    std::vector<std::string> vars, rates;
+    std::vector<SymNode> nodes;
+    std::vector<int> roots;
+    std::vector<double> lo, hi;
+    double unit = 1.0;
+    bool extent = false;
+    std::vector<int> var_src, rate_dst;  // binding: species index (-1 biomass / growth / extent)
+};
 
 struct OrcAde {
     int nx, ny, nz, S, M;
@@ -379,6 +400,8 @@ struct OrcAde {
     void* spec = nullptr;  // EqTableau of the speciation step, or none
     // abiotic rate law (run_abiotic_kinetics / surfaceAbioticKinetics3D)
     int law2 = LAW_NONE;
+    std::vector<SymLaw> sym;             // [microbe] then the abiotic law at index 8
+    unsigned sym_mask = 0;
     std::vector<double> prm2;
     int surf = 0;
     // precipitation sealing and dissolution (precipitationVOP.hh, dissolutionVOP.hh)
@@ -488,6 +511,280 @@ void orc_ade_set_biomass(OrcAde* A, int M, const double* b) {
     A->bio.assign(b, b + (size_t)M * A->N);
 }
 
+
+// =====================================================================================
+//          RATE LAWS READ FROM A .sym FILE (complab3d_symbolic.hh, restated)
+// =====================================================================================
+// The file's keywords, the expression grammar and the evaluation rules of the reference's run-time
+// rate laws: a tree per rate line evaluated recursively; division by a number below 1e-300 gives 0,
+// a negative base to a fractional power 0, log / log10 / sqrt of a non-positive number 0; a NaN rate
+// is 0 and a rate is held within +-1e300; variables are clamped to their ranges; rates are scaled
+// by the unit (per_hour / 3600) but later lines see the unscaled values; a 'reaction' line derives
+// the species lines (nu / |nu_key| / Y * growth * biomass, or nu * extent, coefficients written with
+// 10 significant digits).
+namespace {
+struct SymParser {
+    const std::vector<std::string>& scope;
+    std::vector<SymNode>& nodes;
+    std::string s;
+    size_t p = 0;
+    bool ok = true;
+    SymParser(const std::vector<std::string>& sc, std::vector<SymNode>& n) : scope(sc), nodes(n) {}
+    int mk(int k, int a = -1, int b = -1, double v = 0.0) {
+        nodes.push_back(SymNode{k, v, a, b});
+        return (int)nodes.size() - 1;
+    }
+    void sk() {
+        while (p < s.size() && (s[p] == ' ' || s[p] == '\t')) ++p;
+    }
+    int expr() {
+        int l = term();
+        for (;;) {
+            sk();
+            if (!ok || p >= s.size()) return l;
+            if (s[p] == '+') { ++p; l = mk(3, l, term()); }
+            else if (s[p] == '-') { ++p; l = mk(4, l, term()); }
+            else return l;
+        }
+    }
+    int term() {
+        int l = unary();
+        for (;;) {
+            sk();
+            if (!ok || p >= s.size()) return l;
+            if (s[p] == '*') { ++p; l = mk(5, l, unary()); }
+            else if (s[p] == '/') { ++p; l = mk(6, l, unary()); }
+            else return l;
+        }
+    }
+    int unary() {
+        sk();
+        if (p < s.size() && s[p] == '-') { ++p; return mk(2, unary()); }
+        if (p < s.size() && s[p] == '+') { ++p; return unary(); }
+        int b = atom();
+        sk();
+        if (p < s.size() && s[p] == '^') { ++p; return mk(7, b, unary()); }
+        return b;
+    }
+    int atom() {
+        sk();
+        if (p >= s.size()) { ok = false; return mk(0); }
+        if (s[p] == '(') {
+            ++p;
+            int e = expr();
+            sk();
+            if (p < s.size() && s[p] == ')') ++p; else ok = false;
+            return e;
+        }
+        if (std::isdigit((unsigned char)s[p]) || s[p] == '.') {
+            char* e = nullptr;
+            const double v = std::strtod(s.c_str() + p, &e);
+            if (e == s.c_str() + p) { ok = false; return mk(0); }
+            p = (size_t)(e - s.c_str());
+            return mk(0, -1, -1, v);
+        }
+        if (std::isalpha((unsigned char)s[p]) || s[p] == '_') {
+            size_t q = p;
+            while (p < s.size() && (std::isalnum((unsigned char)s[p]) || s[p] == '_')) ++p;
+            const std::string id = s.substr(q, p - q);
+            sk();
+            if (p < s.size() && s[p] == '(') {
+                ++p;
+                int a = expr(), b = -1;
+                const bool two = id == "min" || id == "max" || id == "pow";
+                sk();
+                if (two) { if (p < s.size() && s[p] == ',') { ++p; b = expr(); } else ok = false; }
+                sk();
+                if (p < s.size() && s[p] == ')') ++p; else ok = false;
+                static const char* f1[] = {"exp", "log", "log10", "sqrt", "abs", "tanh"};
+                for (int k = 0; k < 6; ++k) if (id == f1[k]) return mk(8 + k, a);
+                if (id == "min") return mk(14, a, b);
+                if (id == "max") return mk(15, a, b);
+                if (id == "pow") return mk(7, a, b);
+                ok = false;
+                return mk(0);
+            }
+            if (id == "pi") return mk(0, -1, -1, 3.14159265358979323846);
+            if (id == "e") return mk(0, -1, -1, 2.71828182845904523536);
+            for (size_t i = 0; i < scope.size(); ++i) if (scope[i] == id) return mk(1, (int)i);
+            ok = false;
+            return mk(0);
+        }
+        ok = false;
+        return mk(0);
+    }
+};
+
+double sym_node(const std::vector<SymNode>& n, int i, const std::vector<double>& v) {
+    const SymNode& d = n[(size_t)i];
+    switch (d.kind) {
+        case 0: return d.value;
+        case 1: return v[(size_t)d.a];
+        case 2: return -sym_node(n, d.a, v);
+        case 3: return sym_node(n, d.a, v) + sym_node(n, d.b, v);
+        case 4: return sym_node(n, d.a, v) - sym_node(n, d.b, v);
+        case 5: return sym_node(n, d.a, v) * sym_node(n, d.b, v);
+        case 6: { const double q = sym_node(n, d.b, v); return std::fabs(q) < 1e-300 ? 0.0 : sym_node(n, d.a, v) / q; }
+        case 7: { const double b = sym_node(n, d.a, v), e = sym_node(n, d.b, v);
+                  return (b < 0.0 && e != std::floor(e)) ? 0.0 : std::pow(b, e); }
+        case 8: return std::exp(sym_node(n, d.a, v));
+        case 9: { const double x = sym_node(n, d.a, v); return x > 0.0 ? std::log(x) : 0.0; }
+        case 10: { const double x = sym_node(n, d.a, v); return x > 0.0 ? std::log10(x) : 0.0; }
+        case 11: { const double x = sym_node(n, d.a, v); return x > 0.0 ? std::sqrt(x) : 0.0; }
+        case 12: return std::fabs(sym_node(n, d.a, v));
+        case 13: return std::tanh(sym_node(n, d.a, v));
+        case 14: { const double x = sym_node(n, d.a, v), y = sym_node(n, d.b, v); return x < y ? x : y; }
+        case 15: { const double x = sym_node(n, d.a, v), y = sym_node(n, d.b, v); return x > y ? x : y; }
+    }
+    return 0.0;
+}
+
+bool sym_add(SymLaw& L, const std::string& name, const std::string& ex) {
+    std::vector<std::string> scope = L.vars;
+    scope.insert(scope.end(), L.rates.begin(), L.rates.end());
+    SymParser P(scope, L.nodes);
+    P.s = ex;
+    const int root = P.expr();
+    P.sk();
+    if (!P.ok || P.p != P.s.size()) return false;
+    L.rates.push_back(name);
+    L.roots.push_back(root);
+    return true;
+}
+
+bool sym_load(const char* path, SymLaw& L) {
+    L = SymLaw();
+    FILE* f = std::fopen(path, "r");
+    if (!f) return false;
+    char buf[4096];
+    std::vector<std::pair<std::string, double>> st;
+    std::string yof, bio;
+    double y = 0;
+    bool ok = true;
+    while (ok && std::fgets(buf, sizeof buf, f)) {
+        std::string l(buf);
+        const size_t h = l.find('#');
+        if (h != std::string::npos) l = l.substr(0, h);
+        while (!l.empty() && (l.back() == '\n' || l.back() == '\r')) l.pop_back();
+        std::istringstream in(l);
+        std::string key;
+        if (!(in >> key)) continue;
+        const std::string rest = l.substr(l.find(key) + key.size());
+        if (key == "version") continue;
+        if (key == "units") {
+            std::string u;
+            in >> u;
+            for (char& c : u) c = (char)std::tolower((unsigned char)c);
+            if (u == "per_hour" || u == "per_hr" || u == "h") L.unit = 1.0 / 3600.0;
+        } else if (key == "vars") {
+            std::string w;
+            while (in >> w) L.vars.push_back(w);
+            L.lo.assign(L.vars.size(), 0.0);
+            L.hi.assign(L.vars.size(), -1.0);
+        } else if (key == "range") {
+            std::string nm;
+            double a, b;
+            in >> nm >> a >> b;
+            for (size_t i = 0; i < L.vars.size(); ++i) if (L.vars[i] == nm) { L.lo[i] = a; L.hi[i] = b; }
+        } else if (key == "rate") {
+            const size_t eq = rest.find('=');
+            std::istringstream nn(rest.substr(0, eq));
+            std::string nm;
+            nn >> nm;
+            ok = sym_add(L, nm, rest.substr(eq + 1));
+        } else if (key == "reaction") {
+            std::string nm;
+            double nu;
+            while (in >> nm >> nu) st.push_back({nm, nu});
+        } else if (key == "yield") {
+            in >> yof >> y;
+        } else if (key == "biomass") {
+            in >> bio;
+        }
+    }
+    std::fclose(f);
+    if (!ok) return false;
+    for (const std::string& r : L.rates) L.extent |= r == "extent";
+    char b2[256];
+    if (!st.empty() && L.extent) {
+        for (const auto& t : st) { std::snprintf(b2, sizeof b2, "%.10g * extent", t.second); if (!sym_add(L, t.first, b2)) return false; }
+    } else if (!st.empty()) {
+        double key = 0;
+        for (const auto& t : st) if (t.first == yof) key = t.second;
+        const double mag = key < 0 ? -key : key;
+        for (const auto& t : st) {
+            std::snprintf(b2, sizeof b2, "%.10g * growth * %s", (t.second / mag) / y, bio.c_str());
+            if (!sym_add(L, t.first, b2)) return false;
+        }
+    }
+    return !L.rates.empty();
+}
+
+void sym_rates(const SymLaw& L, const double* x, double* out) {
+    const size_t nv = L.vars.size();
+    std::vector<double> v(nv + L.rates.size(), 0.0);
+    for (size_t i = 0; i < nv; ++i) {
+        double a = x[i];
+        if (L.hi[i] > L.lo[i]) a = a < L.lo[i] ? L.lo[i] : (a > L.hi[i] ? L.hi[i] : a);
+        v[i] = a;
+    }
+    for (size_t r = 0; r < L.rates.size(); ++r) {
+        double y = sym_node(L.nodes, L.roots[r], v);
+        if (y != y) y = 0.0;
+        if (y > 1e300) y = 1e300; else if (y < -1e300) y = -1e300;
+        v[nv + r] = y;
+        out[r] = y * L.unit;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+// standalone evaluation of a file on n rows of its variables (the pinning test's entry point)
+int orc_sym_eval(const char* path, int n, const double* vars, double* out, int* n_rates) {
+    SymLaw L;
+    if (!sym_load(path, L)) return -1;
+    const size_t nv = L.vars.size(), nr = L.rates.size();
+    *n_rates = (int)nr;
+    for (int i = 0; i < n; ++i) sym_rates(L, vars + (size_t)i * nv, out + (size_t)i * nr);
+    return 0;
+}
+
+// binds a file to the species (names: S newline-separated names) as microbe m's law (m >= 0) or the
+// abiotic law (m = -1)
+int orc_ade_set_symbolic(OrcAde* A, const char* path, const char* names, int m, const char* microbe_name) {
+    SymLaw L;
+    if (!sym_load(path, L)) return -1;
+    std::vector<std::string> sp;
+    std::istringstream in(names);
+    std::string w;
+    while (std::getline(in, w)) sp.push_back(w);
+    for (const std::string& v : L.vars) {
+        int hit = -2;
+        for (size_t s = 0; s < sp.size(); ++s) if (sp[s] == v) hit = (int)s;
+        if (hit == -2 && m >= 0 && v == microbe_name) hit = -1;
+        if (hit == -2) return -2;
+        L.var_src.push_back(hit);
+    }
+    for (const std::string& r : L.rates) {
+        int hit = -1;
+        for (size_t s = 0; s < sp.size(); ++s) if (sp[s] == r) hit = (int)s;
+        L.rate_dst.push_back(hit);
+    }
+    if (A->sym.size() < 9) A->sym.resize(9);
+    if (m >= 0) {
+        A->sym[(size_t)m] = L;
+        A->sym_mask |= 1u << m;
+        A->law = LAW_SYMBOLIC;
+    } else {
+        A->sym[8] = L;
+        A->law2 = LAW_SYMBOLIC;
+    }
+    return 0;
+}
+
+}  // extern "C"
+
 static void rates(const OrcAde* A, const double* C, const double* B, double* R, double* RB) {
     const int S = A->S;
     for (int s = 0; s < S; ++s) R[s] = 0;
@@ -533,6 +830,13 @@ static void rates2(const OrcAde* A, const double* C, double* R) {
         R[a] -= r;
         R[b] -= r;
         R[q] += r;
+    } else if (A->law2 == LAW_SYMBOLIC) {
+        const SymLaw& L = A->sym[8];
+        std::vector<double> x(L.vars.size()), y(L.rates.size());
+        for (size_t v = 0; v < x.size(); ++v) x[v] = C[L.var_src[v]];
+        sym_rates(L, x.data(), y.data());
+        for (size_t r = 0; r < y.size(); ++r)
+            if (L.rate_dst[r] >= 0) R[L.rate_dst[r]] += y[r];
     } else if (A->law2 == LAW_MINERAL) {
         const int q = (int)p[2];
         double la = 0;
@@ -704,8 +1008,47 @@ static double thermo_factor(const OrcAde* A, const double* C) {
     return F < 0.0 ? 0.0 : (F > 1.0 ? 1.0 : F);
 }
 
+// the organisms' .sym laws in one voxel (run_symbolic3D, complab3d_processors_symbolic.hh:100-200)
+static void symbolic_voxel(const OrcAde* A, const double* C, const double* B, double* dC, double* dB) {
+    const int S = A->S;
+    std::vector<double> req(S, 0.0), x, y;
+    for (int m = 0; m < A->M; ++m) {
+        dB[m] = 0.0;
+        if (!((A->sym_mask >> m) & 1u)) continue;
+        const double bm = B[m] > THRD ? B[m] : 0.0;
+        if (!(bm > THRD)) continue;
+        const SymLaw& L = A->sym[(size_t)m];
+        x.resize(L.vars.size());
+        y.resize(L.rates.size());
+        for (size_t v = 0; v < L.vars.size(); ++v) x[v] = L.var_src[v] >= 0 ? C[L.var_src[v]] : bm;
+        sym_rates(L, x.data(), y.data());
+        const double ft = (m == 0 && A->gate_on) ? thermo_factor(A, C) : 1.0;
+        double d = 0.0;
+        for (size_t r = 0; r < y.size(); ++r) {
+            if (L.rate_dst[r] >= 0) req[(size_t)L.rate_dst[r]] += y[r] * ft * A->dt;
+            else d += y[r] * ft * bm * A->dt;
+        }
+        if (d > THRD || d < -THRD) {
+            if (d + bm < 0.0) d = -bm;
+            dB[m] = d;
+        }
+    }
+    for (int s = 0; s < S; ++s) {
+        dC[s] = 0.0;
+        double draw = req[s];
+        if (!(draw > THRD || draw < -THRD)) continue;
+        if (draw + C[s] < 0.0) draw = -C[s];
+        dC[s] = draw;
+    }
+}
+
 static void biotic_voxel(const OrcAde* A, double* C, double* B, double* R, double* RB, double* dC, double* dB) {
     const int S = A->S;
+    if (A->law == LAW_SYMBOLIC) {
+        for (int s = 0; s < S; ++s) C[s] = C[s] > THRD ? C[s] : 0.0;
+        symbolic_voxel(A, C, B, dC, dB);
+        return;
+    }
     for (int s = 0; s < S; ++s)
         if (C[s] < THRD) C[s] = 0;
     for (int m = 0; m < A->M; ++m)

@@ -72,6 +72,8 @@ def lib():
             "orc_ca_age_flags": ([vp, vp], None),
             "orc_dissolution_increments": ([ip, ip, ip, ip, ip, dp, ip, vp, ip, vp, ip, ip, vp, vp, vp], None),
             "orc_sphere_pack": ([ip, ip, ip, dp, dp, dp, C.c_uint64, C.c_char_p, ip, ip, ip, vp], ip),
+            "orc_sym_eval": ([C.c_char_p, ip, vp, vp, C.POINTER(C.c_int)], ip),
+            "orc_ade_set_symbolic": ([vp, C.c_char_p, C.c_char_p, ip, C.c_char_p], ip),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -92,6 +94,16 @@ def sphere_pack(nx, ny, nz, porosity, rmin, rmax, seed, walls="yz", grain=1, wal
     if lib().orc_sphere_pack(nx, ny, nz, porosity, rmin, rmax, seed, walls.encode(), grain, wall, pore, _p(out)):
         raise ValueError("bad sphere-pack arguments")
     return out
+
+
+def sym_eval(path, X, n_rates_max=16):
+    """The oracle's evaluation of a .sym rate-law file on the rows of X (its variables in file order)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.zeros(X.shape[0] * n_rates_max)
+    nr = C.c_int()
+    if lib().orc_sym_eval(os.fsencode(path), X.shape[0], _p(X), _p(out), C.byref(nr)) != 0:
+        raise ValueError(f"cannot load {path}")
+    return out[:X.shape[0] * nr.value].reshape(X.shape[0], nr.value)
 
 
 def set_threads(n):
@@ -228,6 +240,13 @@ class OracleAde:
         self._spec = [S, np.ascontiguousarray(logK, dtype=np.float64), np.ascontiguousarray(comp, dtype=np.int32)]
         lib().orc_ade_set_speciation(self.h, S.shape[0], S.shape[1], _p(self._spec[0]), _p(self._spec[1]),
                                      _p(self._spec[2]), tol, max_it)
+
+    def set_symbolic(self, path, names, microbe=-1, microbe_name=""):
+        """A .sym rate law bound to the species `names` (microbe m's law, or abiotic for -1)."""
+        rc = lib().orc_ade_set_symbolic(self.h, os.fsencode(path), "\n".join(names).encode(), int(microbe),
+                                        microbe_name.encode())
+        if rc != 0:
+            raise ValueError(f"cannot bind {path}")
 
     def set_abiotic(self, law, params, surface_only=0):
         p = np.ascontiguousarray(params, dtype=np.float64)

@@ -32,7 +32,7 @@ def test_combinations_equal_unreacting_tracers_at_every_step(clb):
         got = cc.combinations(c)
         for k, name in enumerate(("A - B", "A + C", "B + C")):
             np.testing.assert_allclose(got[name], c[3 + k], rtol=0, atol=1e-13, err_msg=name)
-        assert np.max(c[2]) > 1e-3  # the reaction is running
+    assert np.max(c[2]) > 1e-3  # the reaction is running once A and B meet
 
 
 def test_pe0_steady_profiles_are_the_reference_straight_lines(clb):
