@@ -580,13 +580,13 @@ __global__ void k_ade_init(TS* __restrict__ g, TS* __restrict__ glink, int64_t K
             if (k < K)
                 for (int i = 0; i < 7; ++i) {
                     double v = q7w(i) * (c - 1.0);
-                    if constexpr (std::is_same<TS, __half>::value) g[(int64_t)m * SS + (int64_t)i * K + k] = __double2half(v);
+                    if constexpr (std::is_same<TS, __half>::value) g[(int64_t)m * SS + (int64_t)i * K + k] = to_half(v);
                     else g[(int64_t)m * SS + (int64_t)i * K + k] = (TS)v;
                 }
             if (k < L) {
                 // a wall slot holds population j of the wall node; every j != 0 has weight 1/8
                 double v = 0.125 * (c - 1.0);
-                if constexpr (std::is_same<TS, __half>::value) glink[(int64_t)m * SS + k] = __double2half(v);
+                if constexpr (std::is_same<TS, __half>::value) glink[(int64_t)m * SS + k] = to_half(v);
                 else glink[(int64_t)m * SS + k] = (TS)v;
             }
         }

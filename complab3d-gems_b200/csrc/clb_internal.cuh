@@ -47,18 +47,27 @@ constexpr int MAX_CODES = 128;  // material codes 0..127 (int8, non-negative)
 constexpr double THRD = 1e-12;  // complab3d_processors.hh:60
 
 // ------------------------------------------------------------------ storage conversion
+// FP16 storage holds the shifted populations f - t_i times 2^10: the small deviations of a flow
+// lattice (1e-6 .. 1e-4) stay in half's normal range (subnormal below 6.1e-5 unscaled, below
+// 6.0e-8 scaled), which keeps their 11 significant bits; the scaled range ends at |f - t_i| = 64.
+// Scaling by a power of two is exact both ways, so only the rounding to 11 bits remains.
+constexpr float HALF_SCALE = 1024.0f, HALF_INV = 1.0f / 1024.0f;
 template <typename TS, typename TC>
 __device__ __forceinline__ TC ld(const TS* p) { return (TC)(*p); }
 template <>
-__device__ __forceinline__ float ld<__half, float>(const __half* p) { return __half2float(*p); }
+__device__ __forceinline__ float ld<__half, float>(const __half* p) { return __half2float(*p) * HALF_INV; }
+template <>
+__device__ __forceinline__ double ld<__half, double>(const __half* p) { return (double)(__half2float(*p) * HALF_INV); }
 template <typename TS>
 __device__ __forceinline__ double ldd(const TS* p) { return (double)(*p); }
 template <>
-__device__ __forceinline__ double ldd<__half>(const __half* p) { return (double)__half2float(*p); }
+__device__ __forceinline__ double ldd<__half>(const __half* p) { return (double)(__half2float(*p) * HALF_INV); }
 template <typename TS, typename TC>
 __device__ __forceinline__ void st(TS* p, TC v) { *p = (TS)v; }
 template <>
-__device__ __forceinline__ void st<__half, float>(__half* p, float v) { *p = __float2half_rn(v); }
+__device__ __forceinline__ void st<__half, float>(__half* p, float v) { *p = __float2half_rn(v * HALF_SCALE); }
+// a double into FP16 storage (set-up and host writes)
+__device__ __forceinline__ __half to_half(double v) { return __double2half(v * (double)HALF_SCALE); }
 
 // ------------------------------------------------------------------ geometry of a domain
 struct Geom {

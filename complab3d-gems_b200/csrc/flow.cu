@@ -599,11 +599,11 @@ __global__ void k_flow_init(TS* __restrict__ f, TS* __restrict__ link, const Spa
             const double eq = bgk ? q19w(i) * (rho - 1.0) : 0.0;
             const bool wall_src = i != 0 && ((wm >> q19opp(i)) & 1u);
             const double v = wall_src ? 0.0 : eq;
-            if constexpr (std::is_same<TS, __half>::value) f[(int64_t)i * S.KS + k] = __double2half(v);
+            if constexpr (std::is_same<TS, __half>::value) f[(int64_t)i * S.KS + k] = to_half(v);
             else f[(int64_t)i * S.KS + k] = (TS)v;
             if (wall_src) {
                 TS* x_ = link_slot(S, link, (int)k, q19opp(i));
-                if constexpr (std::is_same<TS, __half>::value) *x_ = __double2half(eq);
+                if constexpr (std::is_same<TS, __half>::value) *x_ = to_half(eq);
                 else *x_ = (TS)eq;
             }
         }

@@ -150,7 +150,7 @@ __device__ __forceinline__ void put_natural(const SparseView& S, const Geom& G, 
     for (int i = 0; i < Q; ++i) {
         TS* p = natural_slot<TS, Q>(S, G, f, link, n, x, y, z, i, odd);
         if (!p) continue;
-        if constexpr (std::is_same<TS, __half>::value) *p = __double2half(in[i]);
+        if constexpr (std::is_same<TS, __half>::value) *p = to_half(in[i]);
         else *p = (TS)in[i];
     }
 }

@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
                 for (int q = 0; q < 7; ++q) {
                     TS* p = out_slot7(S, f, lk, (int)k, q, odd);
                     const double v = ldd(p) + q7w(q) * dC;
-                    if constexpr (std::is_same<TS, __half>::value) *p = __double2half(v);
+                    if constexpr (std::is_same<TS, __half>::value) *p = to_half(v);
                     else *p = (TS)v;
                 }
             } else {
