@@ -433,11 +433,14 @@ def bench_speciation(clb, workloads, torch, local, steps=10):
                          "n_train": rep["n_train"], "source": "the run's own voxel states, jitter 0.6 decades"}}
 
 
-def bench_ensemble(clb, workloads, torch, local, steps=200):
+def bench_ensemble(clb, workloads, torch, local, peak, steps=5000):
     """96 independent uneven domains (the parameter-sweep configuration), FP32, each with a D3Q19
-    flow and 3 D3Q7 species with Monod kinetics, advanced by the batched steps (one launch per
-    lattice and step for all domains, pairs of steps replayed from a CUDA graph) after the
-    batch autotuner, against the same domains stepped one after another."""
+    flow and 3 D3Q7 species with Monod kinetics, advanced `steps` steps by the batch after its
+    autotuner (persistent item tables against per-lattice launches), timed with CUDA events on
+    the batch's stream. Roofline: algorithmic bytes per step = flow nodes x 2 x 19 x 4 B + transport
+    nodes x (3 species x 2 x 7 x 4 B + 3 x 4 B velocity + 1 B material), over the measured copy
+    bandwidth. Also timed: the per-lattice schedule (1000 steps) and the domains stepped one after
+    another through their own handles (20 steps)."""
     cfg = workloads.ensemble_uneven_packs()
     doms = []
     for d in cfg["domains"]:
@@ -449,16 +452,22 @@ def bench_ensemble(clb, workloads, torch, local, steps=200):
         D.couple_velocity()
         D.set_kinetics(d["law"], d["params"], d["dt"])
         doms.append(D)
+    stream = torch.cuda.Stream()
     B = clb.Batch(doms)
-    tuned = B.autotune(10)
+    B.set_stream(stream.cuda_stream)
+    tuned = B.autotune(16)
+    sched = B.get_schedule()
     nf, nt = B.counts()
-    B.step(4)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    B.step(steps)
-    dt = time.perf_counter() - t0
+    step_bytes = nf * 2 * 19 * 4 + nt * (3 * 2 * 7 * 4 + 3 * 4 + 1)
+    ms = timed_steps(torch, stream, B.step, steps, 8) / steps
+    # the per-lattice schedule on the same domains
+    B.schedule(persistent=False)
+    ms_lattice = timed_steps(torch, stream, B.step, 1000, 4) / 1000
+    if sched["persistent"]:
+        B.schedule(persistent=True, tile=sched["tile"], lag=sched["lag"], steps_per_launch=sched["steps_per_launch"])
     # the same domains one by one (each call enqueues its own launches)
     k = 20
+    torch.cuda.synchronize()
     t1 = time.perf_counter()
     for D in doms:
         D.flow_step(k)
@@ -470,13 +479,19 @@ def bench_ensemble(clb, workloads, torch, local, steps=200):
     for D in doms:
         D.close()
     n = len(doms)
-    upd = nf + 3 * nt
+    achieved = step_bytes / (ms * 1e-3) / 1e9
     return {"workload": cfg["name"] + ", FP32", "domains": n, "flow_nodes": nf, "transport_nodes": nt,
-            "steps": steps, "ms_per_step": dt / steps * 1e3, "domain_steps_per_s": n * steps / dt,
-            "aggregate_mlups": upd * steps / dt / 1e6,
+            "steps": steps, "ms_per_step": ms, "domain_steps_per_s": n / (ms * 1e-3),
+            "aggregate_mlups": (nf + 3 * nt) / (ms * 1e-3) / 1e6,
             "unit": "domain-steps / s; MLUPS = flow node + species x transport node updates / s (1e6)",
-            "one_by_one_ms_per_step": dt1 * 1e3, "speedup_vs_one_by_one": dt1 / (dt / steps),
-            "autotune": tuned, "timing": "host clock around the batched steps (one synchronisation)"}
+            "schedule": sched, "per_lattice_ms_per_step": ms_lattice,
+            "speedup_vs_per_lattice": ms_lattice / ms,
+            "one_by_one_ms_per_step": dt1 * 1e3, "speedup_vs_one_by_one": dt1 / (ms * 1e-3),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "bytes_per_step": step_bytes},
+            "autotune": tuned,
+            "timing": f"CUDA events on the batch stream around {steps} steps (graph-replayed launches); "
+                      "one-by-one: host clock, 20 steps"}
 
 
 def bench_flow(clb, workloads, torch, local, peak, steps=200, warmup=20, precision="f32", autotune=True):
@@ -568,7 +583,7 @@ def main():
               "flow": lambda: bench_flow(clb, workloads, torch, local, peak, autotune=not a.no_autotune),
               "precision": lambda: bench_precision(clb, workloads, torch, local),
               "speciation": lambda: bench_speciation(clb, workloads, torch, local),
-              "ensemble": lambda: bench_ensemble(clb, workloads, torch, local)}.get(a.leg)
+              "ensemble": lambda: bench_ensemble(clb, workloads, torch, local, peak)}.get(a.leg)
         if fn is not None:
             print(json.dumps({"leg": a.leg, "scale": a.scale, a.leg: fn()}))
             return
@@ -668,7 +683,7 @@ def main():
                         ("d3q7", lambda: bench_d3q7(clb, workloads, torch, local, peak)),
                         ("precision", lambda: bench_precision(clb, workloads, torch, local)),
                         ("speciation", lambda: bench_speciation(clb, workloads, torch, local)),
-                        ("ensemble", lambda: bench_ensemble(clb, workloads, torch, local))):
+                        ("ensemble", lambda: bench_ensemble(clb, workloads, torch, local, peak))):
             try:
                 extra[key] = fn()
             except Exception as exc:  # a failed side measurement must not hide the headline line

@@ -174,6 +174,10 @@ SIGNATURES = {
     "clb_batch_autotune": [C.c_void_p, C.c_int, C.c_char_p, C.c_int],
     "clb_batch_counts": [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "clb_batch_destroy": [C.c_void_p],
+    "clb_batch_schedule": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int],
+    "clb_batch_get_schedule": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                               C.POINTER(C.c_int)],
+    "clb_batch_set_stream": [C.c_void_p, C.c_void_p],
     "clb_ca_step": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "clb_refresh_dynamics": [C.c_void_p, C.c_int, C.c_int],
     "clb_precip_setup": [C.c_void_p, C.POINTER(PrecipDesc)],
@@ -314,6 +318,19 @@ class Domain:
 
     def tune(self, key, value):
         self._check(lib().clb_tune(self.h, key.encode(), int(value)))
+
+    def schedule(self, persistent=True, tile=2048, lag=8, steps_per_launch=2):
+        _check_global(lib().clb_batch_schedule(self.b, int(bool(persistent)), int(tile), int(lag),
+                                               int(steps_per_launch)))
+
+    def get_schedule(self):
+        v = [C.c_int() for _ in range(4)]
+        _check_global(lib().clb_batch_get_schedule(self.b, *[C.byref(x) for x in v]))
+        return dict(persistent=bool(v[0].value), tile=v[1].value, lag=v[2].value, steps_per_launch=v[3].value)
+
+    def set_stream(self, stream):
+        """stream: a cudaStream_t as an integer (torch.cuda.Stream().cuda_stream), or None."""
+        _check_global(lib().clb_batch_set_stream(self.b, C.c_void_p(stream) if stream else None))
 
     def autotune(self, steps=20):
         buf = C.create_string_buffer(512)
@@ -717,9 +734,11 @@ class Case:
 
 
 class Batch:
-    """An ensemble of Domains advanced together (clb_batch_*): one launch per lattice and step for
-    all of them, pairs of steps replayed from a CUDA graph. Results equal stepping each domain
-    on its own. The domains must stay alive and unchanged while the batch exists."""
+    """An ensemble of Domains advanced together (clb_batch_*): by default one persistent launch
+    runs several steps of every lattice of every domain (a table of tiles with per-domain
+    dependencies), launches replayed from a CUDA graph; or one launch per lattice and step.
+    Results equal stepping each domain on its own. The domains must stay alive and unchanged
+    while the batch exists."""
 
     def __init__(self, domains):
         self.domains = list(domains)
@@ -730,6 +749,19 @@ class Batch:
 
     def step(self, n=1, flow=True, transport=True):
         _check_global(lib().clb_batch_step(self.b, int(n), int(flow), int(transport)))
+
+    def schedule(self, persistent=True, tile=2048, lag=8, steps_per_launch=2):
+        _check_global(lib().clb_batch_schedule(self.b, int(bool(persistent)), int(tile), int(lag),
+                                               int(steps_per_launch)))
+
+    def get_schedule(self):
+        v = [C.c_int() for _ in range(4)]
+        _check_global(lib().clb_batch_get_schedule(self.b, *[C.byref(x) for x in v]))
+        return dict(persistent=bool(v[0].value), tile=v[1].value, lag=v[2].value, steps_per_launch=v[3].value)
+
+    def set_stream(self, stream):
+        """stream: a cudaStream_t as an integer (torch.cuda.Stream().cuda_stream), or None."""
+        _check_global(lib().clb_batch_set_stream(self.b, C.c_void_p(stream) if stream else None))
 
     def autotune(self, steps=20):
         buf = C.create_string_buffer(512)

@@ -21,6 +21,7 @@
 // Algorithmic bytes per node update: 2*7*sizeof(storage) per mobile species, plus the velocity
 // (3*sizeof(arith)) and the material byte shared by all species.
 #include "batch.cuh"
+#include "flow_node.cuh"
 #include "kinetics.cuh"
 #include "tma.cuh"
 
@@ -1299,6 +1300,202 @@ void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_m
         default: if (odd) launch_ade_batch_p<__half, float, true>(B, nm, grid_mult, num_sms, st); else launch_ade_batch_p<__half, float, false>(B, nm, grid_mult, num_sms, st); break;
     }
 }
+
+// ------------------------------------------------------------------ persistent batched steps
+// One launch advances every domain of a batch by several steps. The work is a table of items,
+// each a tile of one lattice of one domain at one step of the launch (flow nodes, the Neumann
+// planes of the domain's species, transport nodes). CTAs take items in table order from one
+// ticket counter; an item starts once the items it depends on are done: the same lattice of the
+// same domain at the previous step (an AA step reads what the neighbours wrote), and, for the
+// transport tiles, the Neumann planes of their own step. Finished items are counted per (step,
+// lattice, domain). The table orders step s of domain d by d + W s (W, the lag, a schedule
+// parameter), so step s + 1 of a domain follows step s of it while its populations are still in
+// L2, and every item depends only on items earlier in the table. Tickets are taken in order, so
+// an awaited item is held by a CTA that is running: the schedule cannot deadlock. Each wait is
+// still bounded (wait_ns) and gives up with a status rather than spin for ever.
+//
+// Visibility across CTAs: the finishing CTA's threads store, meet at a barrier, and one thread
+// fences and increments the counter; the waiting CTA's thread reads the counter, fences, and
+// meets its threads at a barrier before any of them reads -- the pattern of a grid-wide barrier.
+// No pointer of the launch is a read-only kernel argument, so no load goes through the
+// non-coherent read-only path.
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// waits until *c >= target; false when the wait gave up (limit reached or another wait gave up)
+__device__ __forceinline__ bool persist_wait(const int* c, int target, const int* status, int64_t limit_ns) {
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0; it < (1u << 26); ++it) {
+        if (*(const volatile int*)c >= target) {
+            __threadfence();
+            return true;
+        }
+        if (*(const volatile int*)status) return false;
+        if ((it & 31u) == 31u && (int64_t)(global_ns() - t0) > limit_ns) return false;
+        __nanosleep(64);
+    }
+    return false;
+}
+
+// coherent (L2) read of one stored population
+template <typename TS, typename TC>
+__device__ __forceinline__ TC ld_cg(const TS* p) {
+    if constexpr (std::is_same<TS, __half>::value) return (TC)(__half2float(__ldcg(p)) * HALF_INV);
+    else return (TC)__ldcg(p);
+}
+
+// k_neumann_batch's value for plane pixel p of job J, with coherent reads
+template <typename TS, typename TC>
+__device__ __forceinline__ void persist_neumann_pixel(const BatchDomain& d, const NeumannJob& J, int p, int odd) {
+    const Geom G = d.ap.g;
+    const int xb = J.side == 0 ? 0 : G.nx - 1, xi = J.side == 0 ? 1 : G.nx - 2;
+    const int64_t nb = (int64_t)xb * G.plane + p, ni = (int64_t)xi * G.plane + p;
+    const int db = d.ap.dyn[d.mat[nb]], di = d.ap.dyn[d.mat[ni]];
+    if (!(db == ADE_PORE || db == ADE_BIO) || !(di == ADE_PORE || di == ADE_BIO)) return;
+    const double c0 = d.ap.c0[J.s];
+    const TS* f = (const TS*)d.g + (int64_t)J.m * d.as.SS;
+    const TS* link = (const TS*)d.glink + (int64_t)J.m * d.as.SS;
+    int x, y, z;
+    decode(G, ni, x, y, z);
+    double r = 1.0;
+    for (int i = 0; i < 7; ++i) {
+        const TS* q = natural_slot<const TS, 7>(d.as, G, f, link, ni, x, y, z, i, odd);
+        const TC v = q ? ld_cg<TS, TC>(q) : (TC)(q7w(i) * (c0 - 1.0));
+        r += (double)v;
+    }
+    d.neu[((int64_t)J.s * 2 + J.side) * G.plane + p] = r;
+}
+
+template <typename TS, typename TC, int NM>
+#ifndef PERSIST_MINB
+#define PERSIST_MINB 4
+#endif
+__global__ void __launch_bounds__(ADE_THREADS, PERSIST_MINB) k_batch_persistent(const PersistView V) {
+    extern __shared__ __align__(16) unsigned char ade_smem[];
+    const AdeFrame<TC> F = ade_frame<TC, NM>(ade_smem, 0);
+    __shared__ __align__(16) BatchDomain sd;
+    __shared__ int s_next, s_abort;
+    const int tid = threadIdx.x;
+    const int ndom = V.B.ndom;
+    AdeExtra X;
+    X.iface = nullptr;
+    X.xidx = nullptr;
+    X.xdc = nullptr;
+    X.ng = 0;
+    if (tid == 0) s_next = atomicAdd(V.ticket, 1);
+    __syncthreads();
+    int t = s_next;
+    while (t < V.n_items) {
+        const BatchItem it = V.items[t];
+        if (tid == 0) {
+            const int s = it.step, d = it.d;
+            const int* w = nullptr;
+            int target = 0;
+            if (it.kind == BI_FLOW) {
+                if (s > 0) { w = V.done + ((s - 1) * 3 + BI_FLOW) * ndom + d; target = V.need[BI_FLOW * ndom + d]; }
+            } else if (it.kind == BI_NEUMANN) {
+                if (s > 0) { w = V.done + ((s - 1) * 3 + BI_TRANSPORT) * ndom + d; target = V.need[BI_TRANSPORT * ndom + d]; }
+            } else if (V.need[BI_NEUMANN * ndom + d] > 0) {
+                w = V.done + (s * 3 + BI_NEUMANN) * ndom + d;
+                target = V.need[BI_NEUMANN * ndom + d];
+            } else if (s > 0) {
+                w = V.done + ((s - 1) * 3 + BI_TRANSPORT) * ndom + d;
+                target = V.need[BI_TRANSPORT * ndom + d];
+            }
+            bool ok = w ? persist_wait(w, target, V.status, V.wait_ns) : (*(const volatile int*)V.status == 0);
+            if (!ok) atomicExch(V.status, 1);
+            s_abort = ok ? 0 : 1;
+            s_next = atomicAdd(V.ticket, 1);
+        }
+        // the item's domain into shared memory
+        {
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(V.B.dom + it.d);
+            uint64_t* dst = reinterpret_cast<uint64_t*>(&sd);
+            for (int q = tid; q < (int)(sizeof(BatchDomain) / 8); q += ADE_THREADS) dst[q] = src[q];
+        }
+        __syncthreads();
+        const int tn = s_next;
+        if (s_abort) break;
+        const int64_t k0 = it.first, k1 = it.first + it.count;
+        if (it.kind == BI_FLOW) {
+            TS* f = (TS*)sd.f;
+            TS* fl = (TS*)sd.flink;
+            if ((V.fodd ^ it.step) & 1) {
+                for (int64_t k = k0 + tid; k < k1; k += ADE_THREADS)
+                    flow_node<TS, TC, true>(f, fl, sd.fs, sd.fp, k, sd.fkw, sd.fke);
+            } else {
+                for (int64_t k = k0 + tid; k < k1; k += ADE_THREADS)
+                    flow_node<TS, TC, false>(f, fl, sd.fs, sd.fp, k, sd.fkw, sd.fke);
+            }
+        } else if (it.kind == BI_NEUMANN) {
+            const int odd = (V.aodd ^ it.step) & 1;
+            for (int j = V.jbeg[it.d]; j < V.jbeg[it.d + 1]; ++j) {
+                const NeumannJob J = V.B.jobs[j];
+                for (int p = tid; p < sd.ap.g.plane; p += ADE_THREADS) persist_neumann_pixel<TS, TC>(sd, J, p, odd);
+            }
+        } else {
+            TS* g = (TS*)sd.g;
+            if ((V.aodd ^ it.step) & 1) {
+                for (int64_t k = k0 + tid; k < k1; k += ADE_THREADS)
+                    ade_node<TS, TC, true, NM, 0>(g, sd.imm, sd.bio, (const TC*)sd.u, sd.as, sd.neu, sd.ap, sd.n_mobile,
+                                                  sd.mob, sd.akw, sd.ake, X, F, k);
+            } else {
+                for (int64_t k = k0 + tid; k < k1; k += ADE_THREADS)
+                    ade_node<TS, TC, false, NM, 0>(g, sd.imm, sd.bio, (const TC*)sd.u, sd.as, sd.neu, sd.ap, sd.n_mobile,
+                                                   sd.mob, sd.akw, sd.ake, X, F, k);
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicAdd(V.done + (it.step * 3 + it.kind) * ndom + it.d, 1);
+        }
+        t = tn;
+    }
+}
+
+template <typename TS, typename TC, int NM>
+static void persist_launch_t(const PersistView& V, int blocks_per_sm, int num_sms, cudaStream_t st) {
+    // the shared-memory attribute was set on this device by batch_persistent_resident (batch set-up)
+    k_batch_persistent<TS, TC, NM><<<blocks_per_sm * num_sms, ADE_THREADS, ade_slot_bytes<TC, NM>(), st>>>(V);
+}
+
+template <typename TS, typename TC, int NM>
+static int persist_resident_t() {
+    auto kern = k_batch_persistent<TS, TC, NM>;
+    const int sm = ade_slot_bytes<TC, NM>();
+    cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)kern, ADE_THREADS, sm) != cudaSuccess) b = 1;
+    return std::max(1, b);
+}
+
+#define CLB_PERSIST_NM(F, TS, TC, ...)                      \
+    (nm <= 1 ? F<TS, TC, 1>(__VA_ARGS__)                     \
+     : nm <= 2 ? F<TS, TC, 2>(__VA_ARGS__)                   \
+     : nm <= 4 ? F<TS, TC, 4>(__VA_ARGS__)                   \
+     : nm <= 8 ? F<TS, TC, 8>(__VA_ARGS__) : F<TS, TC, 16>(__VA_ARGS__))
+
+void launch_batch_persistent(const PersistView& V, int prec, int nm, int blocks_per_sm, int num_sms, cudaStream_t st) {
+    switch (prec) {
+        case CLB_F64: CLB_PERSIST_NM(persist_launch_t, double, double, V, blocks_per_sm, num_sms, st); break;
+        case CLB_F32: CLB_PERSIST_NM(persist_launch_t, float, float, V, blocks_per_sm, num_sms, st); break;
+        default: CLB_PERSIST_NM(persist_launch_t, __half, float, V, blocks_per_sm, num_sms, st); break;
+    }
+}
+
+int batch_persistent_resident(int prec, int nm) {
+    switch (prec) {
+        case CLB_F64: return CLB_PERSIST_NM(persist_resident_t, double, double);
+        case CLB_F32: return CLB_PERSIST_NM(persist_resident_t, float, float);
+        default: return CLB_PERSIST_NM(persist_resident_t, __half, float);
+    }
+}
+#undef CLB_PERSIST_NM
 
 void ade_refresh_neumann(clb_handle* h) { refresh_neumann(h); }
 

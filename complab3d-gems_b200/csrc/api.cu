@@ -355,6 +355,21 @@ clb_status clb_batch_counts(clb_batch* batch, int64_t* flow_nodes, int64_t* tran
     return batch_counts(batch, flow_nodes, transport_nodes);
 }
 
+clb_status clb_batch_schedule(clb_batch* batch, int persistent, int tile, int lag, int steps_per_launch) {
+    if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
+    return batch_schedule(batch, persistent, tile, lag, steps_per_launch);
+}
+
+clb_status clb_batch_get_schedule(clb_batch* batch, int* persistent, int* tile, int* lag, int* steps_per_launch) {
+    if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
+    return batch_get_schedule(batch, persistent, tile, lag, steps_per_launch);
+}
+
+clb_status clb_batch_set_stream(clb_batch* batch, void* stream) {
+    if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
+    return batch_set_stream(batch, stream);
+}
+
 clb_status clb_batch_destroy(clb_batch* batch) { return batch_destroy(batch); }
 
 clb_status clb_reduce_noalloc(clb_handle* h, clb_stats* out) {

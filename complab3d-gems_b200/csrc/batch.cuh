@@ -45,10 +45,39 @@ struct BatchView {
 
 constexpr int BATCH_MAX_DOMAINS = 2048;
 
+// One entry of the persistent schedule: a tile of one lattice of one domain at one step of the
+// launch (or the Neumann planes of the domain's species at that step).
+constexpr int BI_FLOW = 0, BI_NEUMANN = 1, BI_TRANSPORT = 2;
+struct BatchItem {
+    int d;
+    int16_t kind;   // BI_FLOW, BI_NEUMANN or BI_TRANSPORT
+    int16_t step;   // step within the launch
+    int64_t first;  // first compact node of the tile
+    int count;      // nodes in the tile
+    int pad;
+};
+constexpr int PERSIST_MAX_STEPS = 8;
+
+struct PersistView {
+    BatchView B;
+    const BatchItem* items;
+    int n_items;
+    const int* need;  // [3][ndom]: items of each kind per domain and step
+    const int* jbeg;  // [ndom + 1]: the Neumann jobs of domain d are jobs[jbeg[d] .. jbeg[d + 1])
+    int* done;        // [steps][3][ndom]: items finished, zero when the launch starts
+    int* ticket;      // next item to take, zero when the launch starts
+    int* status;      // nonzero: a wait gave up (the launch's remaining items were skipped)
+    int fodd, aodd;   // parities of the launch's first step
+    int64_t wait_ns;  // limit of one wait
+};
+
 // flow.cu
 void launch_flow_batch(const BatchView& B, int prec, bool odd, int grid, int threads, cudaStream_t st);
 // ade.cu (nm: species register bucket 1, 2, 4, 8 or 16)
 void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_mult, int num_sms, cudaStream_t st);
 void launch_neumann_batch(const BatchView& B, int prec, bool odd, int grid, cudaStream_t st);
+// the persistent schedule: one launch runs the whole item table
+void launch_batch_persistent(const PersistView& V, int prec, int nm, int blocks_per_sm, int num_sms, cudaStream_t st);
+int batch_persistent_resident(int prec, int nm);  // resident CTAs per SM of that launch
 
 }  // namespace clb

@@ -350,6 +350,9 @@ clb_status batch_step(clb_batch* b, int n, int flow, int ade);
 clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len);
 clb_status batch_destroy(clb_batch* b);
 clb_status batch_counts(clb_batch* b, int64_t* flow_nodes, int64_t* ade_nodes);
+clb_status batch_schedule(clb_batch* b, int persistent, int tile, int lag, int steps_per_launch);
+clb_status batch_set_stream(clb_batch* b, void* stream);
+clb_status batch_get_schedule(clb_batch* b, int* persistent, int* tile, int* lag, int* steps_per_launch);
 
 // biofilm_ca.cu
 clb_status ca_setup(clb_handle* h, const clb_ca_desc* d);

@@ -69,18 +69,34 @@ def pack256x128x128(scale=1, gen=None):
                 eps=1e-7, peclet=10.0, char_length=8.0, tau_ade_fixed=0.8)
 
 
+def inlet_connected(mat, shape, open_codes=(2,)):
+    """Mask of the open voxels (materials in open_codes) that face-connected open paths join to
+    the first interior plane x = 1."""
+    from scipy import ndimage
+
+    m = np.isin(mat.reshape(shape), open_codes)
+    lab, _ = ndimage.label(m)
+    keep = np.unique(lab[1][lab[1] > 0])
+    return np.isin(lab, keep).ravel()
+
+
 def pack256cube_8species(scale=1, seed=1003, gen=None):
     """256^3 sphere pack (porosity 0.40), 8 species with D_pore ~ U[0.02, 0.2] and
-    D_biofilm = D_pore / 2, two microbes (materials 3 and 4) seeded on 2 % of pore voxels,
-    dual-Monod kinetics mu_max 1e-4, Ks 0.1, Y 0.4, decay 1e-6; the biofilm automaton ('fraction'
-    push, max density 100, biofilm threshold 0.1 of it) every iteration; the flow (tau 0.8,
-    pressure drop 1e-4, FP32) solved to 1e-6 first and re-solved every 500 iterations; 10,000
-    iterations."""
+    D_biofilm = D_pore / 2, two microbes (materials 3 and 4) seeded on as many voxels as 2 % of the
+    pore voxels, drawn from the pore space that open paths join to the inlet plane; dual-Monod
+    kinetics mu_max 1e-4, Ks 0.1, Y 0.4, decay 1e-6; the biofilm automaton ('fraction' push, max
+    density 100, biofilm threshold 0.1 of it) every iteration; the flow (tau 0.8, pressure drop
+    1e-4, FP32) solved to 1e-6 first and re-solved every 500 iterations; 10,000 iterations.
+
+    Seeds stay out of isolated pore pockets: a colony that fills a pocket with no open neighbour
+    below the maximum density leaves the automaton's age wavefront without a fixed point (every
+    sweep deepens it), which ends the reference's run (complab.cpp:3039-3046) as it ends ours."""
     nxi, ny, nz = max(8, int(256 * scale)), max(8, int(256 * scale)), max(8, int(256 * scale))
     mat, shape = sphere_pack_domain(nxi, ny, nz, 0.40, 3.0, 8.0, seed=seed, gen=gen)
     rng = np.random.default_rng(seed)
     pore = np.flatnonzero(mat == 2)
-    seeded = rng.choice(pore, size=max(2, int(0.02 * pore.size)), replace=False)
+    joined = np.flatnonzero(inlet_connected(mat, shape))
+    seeded = rng.choice(joined, size=max(2, min(joined.size, int(0.02 * pore.size))), replace=False)
     seeded.sort()
     half = seeded.size // 2
     mat = mat.copy()

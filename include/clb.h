@@ -459,23 +459,41 @@ clb_status clb_run(clb_handle* h, const clb_run_desc* d, clb_run_report* report)
 /* ---------------------------------------------------------------- ensembles of domains */
 
 /* A parameter sweep: many independent domains (each its own handle, with its own size, geometry,
- * relaxation times and species) advanced together. Every step of the batch is one launch per
- * lattice covering the nodes of all domains, and pairs of steps are replayed from a captured CUDA
- * graph, so many small uneven domains are not bound by launch overhead. Results are those of
- * stepping each domain on its own, bit for bit. No counterpart in the reference (one domain per
- * run there). The handles must share a device and storage precisions, be at the same step
- * parity, and have no abiotic law, dissolution or speciation; they must stay unchanged (no
- * re-initialisation) while the batch exists. */
+ * relaxation times and species) advanced together, so many small uneven domains are not bound by
+ * launch overhead. Two schedules:
+ *   persistent (the default): one launch runs several steps of every lattice of every domain,
+ *     walking a table of (step, domain, lattice, tile) items in which an item waits only for the
+ *     same lattice of the same domain at the previous step; launches are replayed from a captured
+ *     CUDA graph;
+ *   per lattice: one launch per lattice and step covering the nodes of all domains, pairs of
+ *     steps replayed from a captured CUDA graph.
+ * Results are those of stepping each domain on its own, bit for bit, on either schedule. No
+ * counterpart in the reference (one domain per run there). The handles must share a device and
+ * storage precisions, be at the same step parity, and have no abiotic law, dissolution or
+ * speciation; they must stay unchanged (no re-initialisation) while the batch exists. */
 typedef struct clb_batch_s clb_batch;
 clb_status clb_batch_create(clb_handle* const* handles, int n, clb_batch** out);
 
 /* n steps of the flow lattices (flow != 0) and/or the species lattices (transport != 0) of every
- * domain; returns once they are done. Each handle's iteration counters advance by n. */
+ * domain; returns once they are done. Each handle's iteration counters advance by n. CLB_TIMEOUT:
+ * a dependency wait of the persistent schedule gave up (bounded at two seconds; the domains'
+ * state is then undefined). */
 clb_status clb_batch_step(clb_batch* batch, int n, int flow, int transport);
 
-/* Times the launch shapes of the batched steps over `steps` steps per shape and keeps the
- * fastest; the timed steps are real steps (the handles' counters show them). */
+/* Times the schedules and launch shapes of the batched steps over `steps` steps each (rounded up
+ * to a multiple of 8) and keeps the fastest; the timed steps are real steps (the handles'
+ * counters show them). */
 clb_status clb_batch_autotune(clb_batch* batch, int steps, char* report, int report_len);
+
+/* Sets the schedule: persistent != 0 with `tile` nodes per item (a multiple of 256), a lag of
+ * `lag` >= 1 domains between a domain's successive steps in the item table, and an even 2..8
+ * steps per launch; persistent == 0: one launch per lattice and step (the other arguments are
+ * ignored). The persistent schedule needs one storage type for flow and transport. */
+clb_status clb_batch_schedule(clb_batch* batch, int persistent, int tile, int lag, int steps_per_launch);
+clb_status clb_batch_get_schedule(clb_batch* batch, int* persistent, int* tile, int* lag, int* steps_per_launch);
+
+/* Enqueue the batch's work on `stream` (a cudaStream_t; NULL: the batch's own stream). */
+clb_status clb_batch_set_stream(clb_batch* batch, void* stream);
 
 /* Open (collide / stream) nodes of the flow and species lattices over all domains. */
 clb_status clb_batch_counts(clb_batch* batch, int64_t* flow_nodes, int64_t* transport_nodes);

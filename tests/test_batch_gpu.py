@@ -1,6 +1,7 @@
-"""Ensembles of uneven domains advanced by the batched steps (one launch per lattice and step for
-all domains, pairs of steps replayed from a CUDA graph) against the same domains stepped one by
-one: the populations must agree bit for bit, in FP64 and FP32."""
+"""Ensembles of uneven domains advanced by the batched steps (the persistent schedule: a table of
+(step, domain, lattice, tile) items walked by one launch per few steps; or one launch per lattice
+and step; launches replayed from CUDA graphs) against the same domains stepped one by one: the
+populations must agree bit for bit, in FP64, FP32 and FP16-shifted storage."""
 import numpy as np
 import pytest
 
@@ -78,4 +79,45 @@ def test_batch_rejects_mixed_parity(clb):
     batch = clb.Batch(B)
     with pytest.raises(clb.ClbError):
         batch.step(2)
+    batch.close()
+
+
+@pytest.mark.parametrize("prec,sched", [
+    ("F32", dict(persistent=False)),
+    ("F32", dict(tile=256, lag=1, steps_per_launch=2)),
+    ("F32", dict(tile=1024, lag=3, steps_per_launch=8)),
+    ("F64", dict(tile=512, lag=2, steps_per_launch=4)),
+    ("F16S", dict(tile=4096, lag=100, steps_per_launch=6)),
+])
+def test_batch_schedules_match_single_domains(clb, prec, sched):
+    """Every schedule of the batched steps (per-lattice launches; persistent item tables with tiles
+    of 256 to 4096 nodes, lags from 1 domain (a domain's next step right behind its last) to more
+    than the ensemble, 2 to 8 steps per launch, graph replays and remainder launches) gives the
+    populations of stepping each domain on its own, bit for bit."""
+    cfg = workloads.ensemble_uneven_packs(n_domains=9, seed=21, scale=0.5)
+    p = getattr(clb, prec)
+    A = build(clb, cfg, p)
+    B = build(clb, cfg, p)
+    batch = clb.Batch(B)
+    batch.schedule(**sched)
+    got = batch.get_schedule()
+    assert got["persistent"] == sched.get("persistent", True)
+    for n, flow, tr in ((17, True, True), (9, True, False), (6, False, True), (3, True, True)):
+        for D in A:
+            if flow:
+                D.flow_step(n)
+            if tr:
+                D.ade_step(n)
+        batch.step(n, flow=flow, transport=tr)
+    assert_same(A, B)
+    batch.close()
+
+
+def test_batch_schedule_rejects_bad_settings(clb):
+    cfg = workloads.ensemble_uneven_packs(n_domains=2, seed=22, scale=0.5)
+    B = build(clb, cfg, clb.F32)
+    batch = clb.Batch(B)
+    for bad in (dict(tile=300), dict(lag=0), dict(steps_per_launch=3), dict(steps_per_launch=10)):
+        with pytest.raises(clb.ClbError):
+            batch.schedule(**bad)
     batch.close()

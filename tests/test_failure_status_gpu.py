@@ -82,13 +82,19 @@ def sealed_duct(nx=40, ny=8, nz=8, seal_at=20):
     return m.ravel()
 
 
-@pytest.mark.parametrize("prec", ["F64", "F32"])
-def test_sealed_path_loses_percolation(clb, prec):
+@pytest.mark.parametrize("prec,cap", [("F64", 800), ("F32", 8000)])
+def test_sealed_path_loses_percolation(clb, prec, cap):
+    """The reference flags a lost percolation path only when the re-solve stops at its cap with
+    the outlet plane's mean u_x at or below 1e-12 (complab.cpp:3092-3113); a sealed duct whose
+    energy settles (FP64 reaches a constant round-off energy after about 1000 iterations) counts as
+    converged there and the run goes on. So the FP64 case stops at 800 iterations, while the
+    energy still falls by orders of magnitude per window and the outlet's mean u_x is near 4e-15
+    (the oracle's values); FP32 never settles below its round-off noise."""
     shape = (40, 8, 8)
     D = clb.Domain(sealed_duct(), *shape, 0.8, flow_precision=getattr(clb, prec))
     D.flow_init(1e-4)
     with pytest.raises(clb.ClbError) as e:
-        D.flow_solve(8000, 1e-9)
+        D.flow_solve(cap, 1e-9)
     assert e.value.status == PERCOLATION_LOST
     # the same duct open: the solve converges and the outlet flows
     open_duct = sealed_duct()

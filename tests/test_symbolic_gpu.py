@@ -55,8 +55,11 @@ def test_refusals(clb, tmp_path):
     bad.write_text("vars a b\nrate growth = a * (b + 1\n")
     with pytest.raises(clb.ClbError, match="missing"):
         D.set_symbolic_kinetics(str(bad), ["a", "b", "c"], 0, "")
+    # a refused file leaves no law behind; with one installed the batch refuses the domain (the
+    # batched kernels carry no rate-law interpreter)
+    D.set_symbolic_kinetics(os.path.join(SYM, "monod_pair.sym"), names, 0, "cells")
     with pytest.raises(clb.ClbError):
-        clb.Batch([D])  # the batched kernels carry no rate-law interpreter
+        clb.Batch([D])
 
 
 def test_transport_with_file_laws_matches_the_oracle(clb, oracle):
