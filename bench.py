@@ -372,65 +372,105 @@ def bench_precision(clb, workloads, torch, local, steps=300, warmup=20):
 
 
 def bench_speciation(clb, workloads, torch, local, steps=10):
-    """Equilibrium speciation of the 5-component, 12-species tableau inside the transport step on a
-    96^3 pack: Newton-Raphson (FP64) against the BF16 surrogate with a two-step Newton polish and
-    Newton-Raphson fallback. The surrogate is trained on the GPU from Newton-Raphson solves of the
-    states the run itself generates (1e6 samples of the domain's voxels after 20 steps, each
-    species scaled by 10^U(-0.6, 0.6)). Speciation time = step time with it minus step time
-    without; error = max relative species difference after one step from the same state (open
-    voxels), against Newton-Raphson. The component H+ (species 0) is kept dominant so every
-    component total is positive (the reference clamps non-positive totals to 1e-30)."""
-    S, logK, comp = workloads.tableau_5x12()
+    """Equilibrium speciation of the 5-component, 12-species tableau inside the transport step of the
+    precipitation configuration (192^3 rough fracture, FP32 transport, FP64 speciation, the mineral
+    law): Newton-Raphson against the BF16 surrogate. The surrogate is trained on the GPU from
+    Newton-Raphson solves of states of this run (1e6 samples of its voxels after 100 coupled steps
+    with precipitation, each species scaled by 10^U(-0.6, 0.6)). Timed per transport step with CUDA
+    events: speciation off, Newton-Raphson, the surrogate alone (newton_polish 0, every in-range
+    answer kept) and the surrogate with a two-step Newton polish and residual check (fallback to
+    Newton-Raphson). Errors: relative species difference against Newton-Raphson on 100k held-out
+    states drawn like the training set (another seed), for the network alone and polished; and after
+    one transport step from the same state (open voxels)."""
+    cfg = workloads.fracture192_carbonate(
+        lambda nx, ny, nz: clb.geom_generate("fracture", nx, ny, nz, aperture=12.0, roughness=0.3, seed=1004,
+                                             walls="none"))
+    S, logK, comp = cfg["S"], cfg["logK"], cfg["comp"]
     ns = S.shape[0]
-    mat, shape = workloads.sphere_pack_domain(96, 96, 96, 0.40, 3.0, 6.0, seed=1004)
-    rng = np.random.default_rng(1004)
-    sp = [dict(omega_pore=1 / 0.9, left_type=clb.DIRICHLET, right_type=clb.NEUMANN,
-               left_bc=float(10 ** rng.uniform(-6, -4)), c0=float(10 ** rng.uniform(-6, -4))) for _ in range(ns)]
-    sp[0]["c0"], sp[0]["left_bc"] = 3e-3, 2e-3
-    D = clb.Domain(mat, *shape, 0.8, ade_precision=clb.F32, device=local)
+    nx, ny, nz = cfg["shape"]
+    mat = cfg["mat"]
+    D = clb.Domain(mat, nx, ny, nz, cfg["tau"], flow_precision=clb.F32, ade_precision=clb.F32, device=local)
     stream = torch.cuda.Stream()
     D.set_stream(stream.cuda_stream)
-    D.ade_init(sp)
+    D.flow_init(cfg["delta_p"])
+    D.flow_solve(20000, 1e-6, allow_unconverged=True)
+    D.ade_init(cfg["species"])
+    D.couple_velocity()
     D.speciation_setup(S, logK, comp, tol=1e-10)
     D.set_speciation_mode(clb.SPEC_NR)
-    D.ade_step(20)
+    D.set_abiotic_kinetics(clb.LAW_MINERAL, cfg["mineral"], 0)
+    D.set_concentration(cfg["mineral_species"], cfg["deposit"])
+    D.precip_setup(cfg["mineral_species"], cfg["full"], seal_flow=1, flow_max_iterations=2000, flow_eps=1e-6)
+    sealed = 0
+    for _ in range(10):
+        D.ade_step(10)
+        sealed += D.geometry_update(allow_unconverged=True)[0]
     t_train = time.perf_counter()
     rep = D.surrogate_train([-6.0] * ns, [-2.5] * ns, n_samples=1000000, epochs=60, batch=1024, patience=8,
                             learning_rate=3e-3, seed=1004, from_domain=True, jitter=0.6)
     t_train = time.perf_counter() - t_train
+    open_ = (D.material() == 2)
+    n_open = int(np.count_nonzero(open_))
+    # held-out states: the run's voxel states, jittered like the training set (another seed)
+    conc = np.stack([D.concentration(s)[open_] for s in range(ns)], axis=1)
+    rng = np.random.default_rng(77)
+    pick = rng.choice(conc.shape[0], size=min(100000, conc.shape[0]), replace=False)
+    states = np.maximum(conc[pick], 1e-30) * 10.0 ** rng.uniform(-0.6, 0.6, size=(pick.size, ns))
+    states = states[(states @ S > 0).all(axis=1)]
+    nr, _ = D.speciation_solve(states)
+    D.surrogate_set_check(0.02, 0, 1e30)
+    raw, acc_raw = D.surrogate_predict(states, residual_check=False)
     D.surrogate_set_check(0.02, 2, 1e-6)
-    n_open = int(np.count_nonzero(mat == 2))
+    pol, acc_pol = D.surrogate_predict(states, residual_check=True)
+    r_raw = np.abs(raw / nr - 1)[acc_raw]
+    r_pol = np.abs(pol / nr - 1)[acc_pol]
     times = {}
-    used = 0.0
-    for mode in (clb.SPEC_OFF, clb.SPEC_NR, clb.SPEC_MLP_NR):
+    used = {}
+    modes = (("off", clb.SPEC_OFF, None), ("nr", clb.SPEC_NR, None), ("raw", clb.SPEC_MLP_NR, (0.02, 0, 1e30)),
+             ("polished", clb.SPEC_MLP_NR, (0.02, 2, 1e-6)))
+    for key, mode, chk in modes:
+        if chk:
+            D.surrogate_set_check(*chk)
         D.set_speciation_mode(mode)
         s0 = D.speciation_stats()
-        times[mode] = timed_steps(torch, stream, D.ade_step, steps, 2) / steps
+        times[key] = timed_steps(torch, stream, D.ade_step, steps, 2) / steps
         s1 = D.speciation_stats()
-        if mode == clb.SPEC_MLP_NR:
-            used = (s1["surrogate_used"] - s0["surrogate_used"]) / max(1, s1["solves"] - s0["solves"])
-    # accuracy: one step from the same state under each mode
-    conc0 = [D.ade_populations(s) for s in range(ns)]
+        used[key] = (s1["surrogate_used"] - s0["surrogate_used"]) / max(1, s1["solves"] - s0["solves"])
+    # one transport step from the same state under each mode
+    pops0 = [D.ade_populations(s) for s in range(ns)]
+    mineral0 = D.concentration(cfg["mineral_species"])
     res = {}
-    for mode in (clb.SPEC_NR, clb.SPEC_MLP_NR):
+    for key, mode, chk in modes[1:]:
         for s in range(ns):
-            D.set_ade_populations(s, conc0[s])
+            D.set_ade_populations(s, pops0[s])
+        D.set_concentration(cfg["mineral_species"], mineral0)
+        if chk:
+            D.surrogate_set_check(*chk)
         D.set_speciation_mode(mode)
         D.ade_step(1)
-        res[mode] = np.array([D.concentration(s) for s in range(ns)])
-    open_ = (mat == 2)
-    a, b = res[clb.SPEC_MLP_NR][:, open_], res[clb.SPEC_NR][:, open_]
-    rel = np.abs(a / np.where(b == 0, 1, b) - 1)
+        res[key] = np.array([D.concentration(s)[open_] for s in range(ns)])
+    step_err = {}
+    for key in ("raw", "polished"):
+        a, b = res[key], res["nr"]
+        step_err[key] = float(np.max(np.abs(a / np.where(b == 0, 1, b) - 1)))
     D.close()
-    t_nr = times[clb.SPEC_NR] - times[clb.SPEC_OFF]
-    t_ml = times[clb.SPEC_MLP_NR] - times[clb.SPEC_OFF]
-    return {"workload": "96^3 sphere pack, 5 components x 12 species tableau, FP32 transport, FP64 speciation",
-            "open_voxels": n_open, "nr_ms_per_step": t_nr, "surrogate_ms_per_step": t_ml,
-            "nr_solves_per_s": n_open / (t_nr * 1e-3), "surrogate_solves_per_s": n_open / (t_ml * 1e-3),
-            "speedup": t_nr / t_ml, "max_rel_err_vs_nr": float(rel.max()), "p99_rel_err_vs_nr": float(np.percentile(rel, 99)),
-            "surrogate_used_fraction": used,
-            "training": {"seconds": t_train, "val_mse": rep["val_mse"], "epochs": rep["epochs"],
-                         "n_train": rep["n_train"], "source": "the run's own voxel states, jitter 0.6 decades"}}
+    t_nr = times["nr"] - times["off"]
+    out = {"workload": cfg["name"] + ", FP32 transport, FP64 speciation", "open_voxels": n_open,
+           "voxels_sealed_before_training": sealed, "nr_ms_per_step": t_nr,
+           "nr_solves_per_s": n_open / (t_nr * 1e-3)}
+    for key in ("raw", "polished"):
+        t = times[key] - times["off"]
+        r = r_raw if key == "raw" else r_pol
+        out[key] = {"ms_per_step": t, "solves_per_s": n_open / (t * 1e-3), "speedup_vs_nr": t_nr / t,
+                    "kept_fraction_in_step": used[key],
+                    "heldout_max_rel_err": float(r.max()), "heldout_p99_rel_err": float(np.percentile(r, 99)),
+                    "heldout_median_rel_err": float(np.median(r)),
+                    "heldout_in_range": float((acc_raw if key == "raw" else acc_pol).mean()),
+                    "one_step_max_rel_err": step_err[key]}
+    out["training"] = {"seconds": t_train, "val_mse": rep["val_mse"], "epochs": rep["epochs"], "steps": rep["steps"],
+                       "ms_per_minibatch": t_train * 1e3 / max(1, rep["steps"]), "n_train": rep["n_train"],
+                       "source": "states of this run after 100 coupled steps, jitter 0.6 decades"}
+    return out
 
 
 def bench_ensemble(clb, workloads, torch, local, peak, steps=5000):

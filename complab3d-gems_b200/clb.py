@@ -764,8 +764,8 @@ class Batch:
         _check_global(lib().clb_batch_set_stream(self.b, C.c_void_p(stream) if stream else None))
 
     def autotune(self, steps=20):
-        buf = C.create_string_buffer(512)
-        _check_global(lib().clb_batch_autotune(self.b, int(steps), buf, 512))
+        buf = C.create_string_buffer(4096)
+        _check_global(lib().clb_batch_autotune(self.b, int(steps), buf, 4096))
         return buf.value.decode()
 
     def counts(self):

@@ -54,7 +54,7 @@ __device__ __noinline__ void sym_biotic(const AdeParams& P, int n_mobile, const 
 #pragma unroll
     for (int s = 0; s < NM; ++s) {
         double c = 0.0;
-        if (s < n_mobile) c = (double)rb[s] + 1.0;
+        if (s < n_mobile) c = (double)rb[s] + ade_sigma<TC>();
         else if (s < P.S) c = imm[(int64_t)s * N + nd];
         C[s] = c > THRD ? c : 0.0;
         req[s] = 0.0;
@@ -127,7 +127,7 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra
 #pragma unroll
         for (int s = 0; s < NM; ++s) {
             TC c = 0;
-            if (s < n_mobile) c = rb[s] + (TC)1;
+            if (s < n_mobile) c = rb[s] + (TC)ade_sigma<TC>();
             else if (s < P.S) c = (TC)imm[(int64_t)s * G.N + nd];
             C[s] = c < thr ? (TC)0 : c;
         }
@@ -162,7 +162,7 @@ __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra
 #pragma unroll
             for (int s = 0; s < NM; ++s) {
                 double c = 0.0;
-                if (s < n_mobile) c = (double)rb[s] + 1.0 + (double)dC[s];
+                if (s < n_mobile) c = (double)rb[s] + ade_sigma<TC>() + (double)dC[s];
                 else if (s < P.S) c = imm[(int64_t)s * G.N + nd];
                 C[s] = c < THRD ? 0.0 : c;
             }
@@ -394,7 +394,7 @@ __device__ __forceinline__ void ade_finish(TS* __restrict__ g, double* __restric
 #pragma unroll
             for (int i = 0; i < 7; ++i)
                 if (i != miss) sum += slot[i * T];
-            slot[miss * T] = (TC)(rs - 1.0) - sum;
+            slot[miss * T] = (TC)(rs - ade_sigma<TC>()) - sum;
         }
         TC r = 0;
 #pragma unroll
@@ -438,7 +438,7 @@ __device__ __forceinline__ void ade_finish(TS* __restrict__ g, double* __restric
         } else {
             const TC w = (TC)(dyn == ADE_BIO ? P.wbio[s] : P.wpore[s]);
             const TC omw = (TC)1 - w;
-            const TC rho = rb[m] + (TC)1;
+            const TC rho = rb[m] + (TC)ade_sigma<TC>();
             const TC jx = rho * ux, jy = rho * uy, jz = rho * uz;
             const TC d = dC[m];
             // feq_i = t_i (rb + 4 c_i . j), in opposite-pair form (no zero products)
@@ -556,14 +556,14 @@ __global__ void k_ade_neumann(const TS* __restrict__ g, const TS* __restrict__ g
     const double c0 = P.c0[s];
     const int xb = side == 0 ? 0 : G.nx - 1, xi = side == 0 ? 1 : G.nx - 2;
     TC init[7];
-    for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - 1.0));
+    for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - ade_sigma<TC>()));
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < G.plane; p += gridDim.x * blockDim.x) {
         const int64_t nb = (int64_t)xb * G.plane + p, ni = (int64_t)xi * G.plane + p;
         const int db = P.dyn[mat[nb]], di = P.dyn[mat[ni]];
         if (!(db == ADE_PORE || db == ADE_BIO) || !(di == ADE_PORE || di == ADE_BIO)) continue;
         TC pop[7];
         natural<TS, TC, 7>(S, G, g + (int64_t)m * S.SS, glink + (int64_t)m * S.SS, ni, odd, init, pop);
-        double r = 1.0;
+        double r = ade_sigma<TC>();
         for (int i = 0; i < 7; ++i) r += (double)pop[i];
         neu[((int64_t)s * 2 + side) * G.plane + p] = r;
     }
@@ -580,13 +580,13 @@ __global__ void k_ade_init(TS* __restrict__ g, TS* __restrict__ glink, int64_t K
             if (c < THRD && c > -THRD) c = 0.0;
             if (k < K)
                 for (int i = 0; i < 7; ++i) {
-                    double v = q7w(i) * (c - 1.0);
+                    double v = q7w(i) * (c - ade_sigma<TS>());
                     if constexpr (std::is_same<TS, __half>::value) g[(int64_t)m * SS + (int64_t)i * K + k] = to_half(v);
                     else g[(int64_t)m * SS + (int64_t)i * K + k] = (TS)v;
                 }
             if (k < L) {
                 // a wall slot holds population j of the wall node; every j != 0 has weight 1/8
-                double v = 0.125 * (c - 1.0);
+                double v = 0.125 * (c - ade_sigma<TS>());
                 if constexpr (std::is_same<TS, __half>::value) glink[(int64_t)m * SS + k] = to_half(v);
                 else glink[(int64_t)m * SS + k] = (TS)v;
             }
@@ -597,12 +597,14 @@ __global__ void k_ade_init(TS* __restrict__ g, TS* __restrict__ glink, int64_t K
 template <typename TS>
 __global__ void k_ade_get_pops(const TS* __restrict__ g, const TS* __restrict__ glink, const SparseView S,
                                const Geom G, int odd, double c0, double* __restrict__ out) {
+    // stored values g_i - sigma t_i; the shifted populations g_i - t_i go out
+    constexpr double sig = ade_sigma<TS>();
     double init[7];
-    for (int i = 0; i < 7; ++i) init[i] = q7w(i) * (c0 - 1.0);
+    for (int i = 0; i < 7; ++i) init[i] = q7w(i) * (c0 - sig);
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
         double v[7];
         natural<TS, double, 7>(S, G, g, glink, n, odd, init, v);
-        for (int i = 0; i < 7; ++i) out[(int64_t)i * G.N + n] = v[i];
+        for (int i = 0; i < 7; ++i) out[(int64_t)i * G.N + n] = sig == 1.0 ? v[i] : v[i] - q7w(i) * (1.0 - sig);
     }
 }
 
@@ -615,7 +617,7 @@ __global__ void k_ade_density(const TS* __restrict__ g, const TS* __restrict__ g
                               const double* __restrict__ neu, double* __restrict__ out) {
     const Geom G = P.g;
     double init[7];
-    for (int i = 0; i < 7; ++i) init[i] = q7w(i) * (P.c0[s] - 1.0);
+    for (int i = 0; i < 7; ++i) init[i] = q7w(i) * (P.c0[s] - ade_sigma<TS>());
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(n / G.plane);
         const int p = (int)(n - (int64_t)x * G.plane);
@@ -631,7 +633,7 @@ __global__ void k_ade_density(const TS* __restrict__ g, const TS* __restrict__ g
         }
         double v[7];
         natural<TS, double, 7>(S, G, g, glink, n, odd, init, v);
-        double r = 1.0;
+        double r = ade_sigma<TS>();
         for (int i = 0; i < 7; ++i) r += v[i];
         out[n] = r;
     }
@@ -642,7 +644,7 @@ __global__ void k_ade_set_pops(TS* __restrict__ g, TS* __restrict__ glink, const
                                const double* __restrict__ in) {
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
         double v[7];
-        for (int i = 0; i < 7; ++i) v[i] = in[(int64_t)i * G.N + n];
+        for (int i = 0; i < 7; ++i) v[i] = in[(int64_t)i * G.N + n] + q7w(i) * (1.0 - ade_sigma<TS>());
         put_natural<TS, 7>(S, G, g, glink, n, odd, v);
     }
 }
@@ -696,26 +698,30 @@ __global__ void __launch_bounds__(RED_THREADS)
     if (row < S_) {
         const int s = row, m = P.slot[s];
         double tot = 0.0, cont = 0.0, mn = 1e300, mx = -1e300, nonf = 0.0;
+        // content in the shifted convention whatever the storage: a link slot holds a population of
+        // weight 1/8
+        constexpr double sig = ade_sigma<TS>();
         if (m >= 0)
-            for (int64_t k = k0; k < S.L; k += stride) cont += ldd(glink + (int64_t)m * S.SS + k);
+            for (int64_t k = k0; k < S.L; k += stride) cont += ldd(glink + (int64_t)m * S.SS + k) - 0.125 * (1.0 - sig);
         for (int64_t k = k0; k < K; k += stride) {
             const int code = S.code[k];
             const bool open = k >= k_west_end && k < k_east_begin && P.react[code];
             double c = 0.0;
             if (m >= 0) {
                 // content: the node's own slots (every slot of the lattice counted once)
-                double sum = 1.0;
+                double sum = sig;
 #pragma unroll
                 for (int i = 0; i < 7; ++i) sum += ldd(g + (int64_t)m * S.SS + (int64_t)i * S.KS + k);
                 cont += sum;
                 if (open) {
                     // concentration: the node's incoming populations wherever the step parity keeps
                     // them (computeDensity after the stream)
-                    const double zero[7] = {0, 0, 0, 0, 0, 0, 0};
+                    double zero[7];  // an untouched slot: the equilibrium at 1
+                    for (int i = 0; i < 7; ++i) zero[i] = q7w(i) * (1.0 - sig);
                     double pop[7];
                     natural<TS, double, 7>(S, P.g, g + (int64_t)m * S.SS, glink + (int64_t)m * S.SS, S.node[k], odd,
                                            zero, pop);
-                    c = 1.0;
+                    c = sig;
 #pragma unroll
                     for (int i = 0; i < 7; ++i) c += pop[i];
                 }
@@ -1258,10 +1264,10 @@ __global__ void k_neumann_batch(const BatchView B, int odd) {
         if (!(db == ADE_PORE || db == ADE_BIO) || !(di == ADE_PORE || di == ADE_BIO)) continue;
         const double c0 = d.ap.c0[J.s];
         TC init[7], pop[7];
-        for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - 1.0));
+        for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - ade_sigma<TC>()));
         natural<TS, TC, 7>(d.as, G, (const TS*)d.g + (int64_t)J.m * d.as.SS, (const TS*)d.glink + (int64_t)J.m * d.as.SS,
                            ni, odd, init, pop);
-        double r = 1.0;
+        double r = ade_sigma<TC>();
         for (int i = 0; i < 7; ++i) r += (double)pop[i];
         d.neu[((int64_t)J.s * 2 + J.side) * G.plane + p] = r;
     }
@@ -1361,10 +1367,10 @@ __device__ __forceinline__ void persist_neumann_pixel(const BatchDomain& d, cons
     const TS* link = (const TS*)d.glink + (int64_t)J.m * d.as.SS;
     int x, y, z;
     decode(G, ni, x, y, z);
-    double r = 1.0;
+    double r = ade_sigma<TC>();
     for (int i = 0; i < 7; ++i) {
         const TS* q = natural_slot<const TS, 7>(d.as, G, f, link, ni, x, y, z, i, odd);
-        const TC v = q ? ld_cg<TS, TC>(q) : (TC)(q7w(i) * (c0 - 1.0));
+        const TC v = q ? ld_cg<TS, TC>(q) : (TC)(q7w(i) * (c0 - ade_sigma<TC>()));
         r += (double)v;
     }
     d.neu[((int64_t)J.s * 2 + J.side) * G.plane + p] = r;

@@ -69,6 +69,16 @@ __device__ __forceinline__ void st<__half, float>(__half* p, float v) { *p = __f
 // a double into FP16 storage (set-up and host writes)
 __device__ __forceinline__ __half to_half(double v) { return __double2half(v * (double)HALF_SCALE); }
 
+// Transport populations are stored as g_i - sigma t_i. Lattices computed in FP64 keep the
+// reference's shifted form (sigma = 1: Palabos stores f_i - t_i and a density is 1 + the sum), so
+// FP64 runs repeat the reference's rounding; lattices computed in FP32 (FP32 and FP16 storage) keep
+// g_i itself (sigma = 0), so a concentration far below 1 keeps its relative precision instead of
+// being the small difference of two numbers near t_i. The collision has the same form in both:
+// with rb = the sum of the stored values, C = rb + sigma and g^eq_i - sigma t_i = t_i (rb + 4 c_i.j).
+// The populations the C ABI exchanges are always the shifted ones, g_i - t_i.
+template <typename T>
+__host__ __device__ constexpr double ade_sigma() { return sizeof(T) == 8 ? 1.0 : 0.0; }
+
 // ------------------------------------------------------------------ geometry of a domain
 struct Geom {
     int nx, ny, nz;

@@ -207,7 +207,8 @@ __device__ void post_biotic(const AdeParams& P, const SparseView& S, const TS* g
                             const double* imm, const double* bio, int n_mobile, int64_t n, int odd,
                             double* Craw) {
     const Geom G = P.g;
-    TC init[7] = {};
+    TC init[7];  // an untouched slot: the equilibrium at 1
+    for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (1.0 - ade_sigma<TC>()));
     TC rsum[CLB_MAX_SPECIES] = {};
     for (int s = 0; s < P.S; ++s) {
         if (s < n_mobile) {
@@ -216,7 +217,7 @@ __device__ void post_biotic(const AdeParams& P, const SparseView& S, const TS* g
             TC r = 0;
             for (int i = 0; i < 7; ++i) r += pop[i];
             rsum[s] = r;
-            Craw[s] = (double)r + 1.0;
+            Craw[s] = (double)r + ade_sigma<TC>();
         } else {
             Craw[s] = imm[(int64_t)s * G.N + n];
         }
@@ -228,7 +229,7 @@ __device__ void post_biotic(const AdeParams& P, const SparseView& S, const TS* g
 #pragma unroll
     for (int s = 0; s < CLB_MAX_SPECIES; ++s) {
         TC c = 0;
-        if (s < n_mobile) c = rsum[s] + (TC)1;
+        if (s < n_mobile) c = rsum[s] + (TC)ade_sigma<TC>();
         else if (s < P.S) c = (TC)Craw[s];
         C[s] = c < thr ? (TC)0 : c;
     }

@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
                     const int m = A.slot[si];
                     TS* f = g + (int64_t)m * S.SS;
                     TS* lk = glink + (int64_t)m * S.SS;
-                    v = 1.0;
+                    v = ade_sigma<TS>();
                     for (int q = 0; q < 7; ++q) v += ldd(out_slot7(S, f, lk, (int)k, q, odd));
                 } else {
                     v = imm[(int64_t)si * A.g.N + S.node[k]];
@@ -451,6 +451,11 @@ clb_status speciation_stats(clb_handle* h, clb_speciation_stats* out) {
 //   W1 [64][16], b1 [64], W2 [64][64], b2 [64], W3 [16][64], b3 [16]
 constexpr int P_W1 = 0, P_B1 = P_W1 + MLP_H * MLP_IN, P_W2 = P_B1 + MLP_H, P_B2 = P_W2 + MLP_H * MLP_H,
               P_W3 = P_B2 + MLP_H, P_B3 = P_W3 + MLP_OUT * MLP_H, P_N = P_B3 + MLP_OUT;
+// BF16 operand copies: W1, W2, W3 as stored (forward), then W2 and W3 transposed (backward)
+constexpr int BF_W1 = 0, BF_W2 = BF_W1 + MLP_H * MLP_IN, BF_W3 = BF_W2 + MLP_H * MLP_H,
+              BF_W2T = BF_W3 + MLP_OUT * MLP_H, BF_W3T = BF_W2T + MLP_H * MLP_H, BF_N = BF_W3T + MLP_H * MLP_OUT;
+// per-block partial gradients of a training launch: P_N values then the block's squared error
+constexpr int PART_STRIDE = P_N + 1;
 
 MlpView mlp_view(clb_handle* h) {
     MlpView M;
@@ -461,6 +466,8 @@ MlpView mlp_view(clb_handle* h) {
     M.w1b = pb;
     M.w2b = pb + MLP_H * MLP_IN;
     M.w3b = pb + MLP_H * MLP_IN + MLP_H * MLP_H;
+    M.w2t = pb + BF_W2T;
+    M.w3t = pb + BF_W3T;
     M.b1 = pf + P_B1;
     M.b2 = pf + P_B2;
     M.b3 = pf + P_B3;
@@ -502,7 +509,8 @@ __global__ void k_mlp_sample_field(const TS* __restrict__ g, const TS* __restric
                                    const SpecParams P, int odd, int64_t k_lo, int64_t k_hi, int n, uint64_t seed,
                                    double jitter, double* __restrict__ c) {
     const Geom G = A.g;
-    const double init[7] = {0, 0, 0, 0, 0, 0, 0};
+    double init[7];  // an untouched slot: the equilibrium at 1
+    for (int i = 0; i < 7; ++i) init[i] = q7w(i) * (1.0 - ade_sigma<TS>());
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         uint64_t hsh = mix64(seed ^ mix64(0x5DEECE66DULL + (uint64_t)t));
         int64_t k = k_lo + (int64_t)(hsh % (uint64_t)(k_hi - k_lo));
@@ -518,7 +526,7 @@ __global__ void k_mlp_sample_field(const TS* __restrict__ g, const TS* __restric
                 const int m = A.slot[si];
                 double pop[7];
                 natural<TS, double, 7>(S, G, g + (int64_t)m * S.SS, glink + (int64_t)m * S.SS, nd, odd, init, pop);
-                v = 1.0;
+                v = ade_sigma<TS>();
                 for (int q = 0; q < 7; ++q) v += pop[q];
             } else {
                 v = imm[(int64_t)si * G.N + nd];
@@ -559,28 +567,67 @@ __global__ void k_mlp_scale(int n, int width, int used, float* __restrict__ Z, c
     }
 }
 
-__global__ void k_mlp_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ b) {
-    // BF16 operand copies of W1, W2, W3 (biases stay FP32)
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < MLP_H * MLP_IN + MLP_H * MLP_H + MLP_OUT * MLP_H;
-         t += gridDim.x * blockDim.x) {
-        float v;
-        if (t < MLP_H * MLP_IN) v = p[P_W1 + t];
-        else if (t < MLP_H * MLP_IN + MLP_H * MLP_H) v = p[P_W2 + t - MLP_H * MLP_IN];
-        else v = p[P_W3 + t - MLP_H * MLP_IN - MLP_H * MLP_H];
-        b[t] = __float2bfloat16_rn(v);
+// the BF16 operand copy of FP32 parameter q (a weight), plain and, for W2 and W3, transposed
+__device__ __forceinline__ void mlp_bf16_store(__nv_bfloat16* b, int q, float v) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    if (q < P_B1) {
+        b[BF_W1 + q - P_W1] = h;
+    } else if (q >= P_W2 && q < P_B2) {
+        const int jj = (q - P_W2) / MLP_H, ii = (q - P_W2) % MLP_H;  // W2[j][i]
+        b[BF_W2 + q - P_W2] = h;
+        b[BF_W2T + ii * MLP_H + jj] = h;
+    } else if (q >= P_W3 && q < P_B3) {
+        const int o = (q - P_W3) / MLP_H, jj = (q - P_W3) % MLP_H;   // W3[o][j]
+        b[BF_W3 + q - P_W3] = h;
+        b[BF_W3T + jj * MLP_OUT + o] = h;
     }
 }
 
-// One minibatch chunk of 128 samples per block: forward on the tensor cores (BF16 operands,
-// FP32 accumulation), mean-squared error on the scaled outputs, backward in FP32 on the CUDA
-// cores from the stored activations, gradients summed into `grad` (FP32 atomics).
-// rows[] selects the samples (a shuffled index list); count = samples in the minibatch.
+__global__ void k_mlp_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ b) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < P_N; q += gridDim.x * blockDim.x) mlp_bf16_store(b, q, p[q]);
+}
+
+// One minibatch chunk of 128 samples per block (4 warps, 32 rows each): forward on the tensor
+// cores, mean-squared error on the scaled outputs, backward on the tensor cores too -- every GEMM
+// of the backward pass (dH2 = dY W3, dH1 = dZ2 W2 per warp's rows; dW3 = dY^T H2, dW2 = dZ2^T H1,
+// dW1 = dZ1^T X over the block's 128 rows) as mma.sync m16n8k16 with BF16 operands and FP32
+// accumulation; bias gradients as FP32 column sums. The block writes its gradient and its squared
+// error to its own row of `part` (PART_STRIDE floats); the optimiser kernel sums the rows in
+// block order, so training is deterministic. rows[] selects the samples (a shuffled index list);
+// count = samples in the minibatch.
 constexpr int TR_ROWS = 128;
 
-__global__ void __launch_bounds__(128) k_mlp_train(const MlpView M, const float* __restrict__ params,
-                                                   const float* __restrict__ X, const float* __restrict__ Y,
-                                                   const int* __restrict__ rows, int count, float inv_norm,
-                                                   float* __restrict__ grad, float* __restrict__ loss_acc) {
+// A fragment (m16 x k16) of the transpose of a row-major [rows][ld] float matrix Z: rows of the
+// fragment are Z's columns c0.., its k are Z's rows k0.. (BF16 pairs along k)
+__device__ __forceinline__ void load_at(const float* Z, int ld, int k0, int c0, int lane, uint32_t (&A)[4]) {
+    const int g = lane >> 2, t = lane & 3;
+    const float* p = Z + (k0 + 2 * t) * ld + c0 + g;
+    A[0] = pack_bf16(p[0], p[ld]);
+    A[1] = pack_bf16(p[8], p[ld + 8]);
+    A[2] = pack_bf16(p[8 * ld], p[9 * ld]);
+    A[3] = pack_bf16(p[8 * ld + 8], p[9 * ld + 8]);
+}
+
+// B fragment (k16 x n8) of a row-major [rows][ld] float matrix Z read as B[k][n] = Z[k0 + k][n0 + n]
+__device__ __forceinline__ void load_bz(const float* Z, int ld, int k0, int n0, int lane, uint32_t& b0, uint32_t& b1) {
+    const int g = lane >> 2, t = lane & 3;
+    const float* p = Z + (k0 + 2 * t) * ld + n0 + g;
+    b0 = pack_bf16(p[0], p[ld]);
+    b1 = pack_bf16(p[8 * ld], p[9 * ld]);
+}
+
+// D fragment of an m16 x n8 tile (rows m0.., cols n0..) into out[row * ld + col]
+__device__ __forceinline__ void store_d(float* out, int ld, int m0, int n0, int lane, const float (&d)[4]) {
+    const int g = lane >> 2, t = lane & 3;
+    out[(m0 + g) * ld + n0 + 2 * t] = d[0];
+    out[(m0 + g) * ld + n0 + 2 * t + 1] = d[1];
+    out[(m0 + g + 8) * ld + n0 + 2 * t] = d[2];
+    out[(m0 + g + 8) * ld + n0 + 2 * t + 1] = d[3];
+}
+
+__global__ void __launch_bounds__(128) k_mlp_train(const MlpView M, const float* __restrict__ X,
+                                                   const float* __restrict__ Y, const int* __restrict__ rows,
+                                                   int count, float inv_norm, float* __restrict__ part) {
     extern __shared__ float tsm[];
     float* xs = tsm;                          // [128][16]
     float* h1 = xs + TR_ROWS * 16;            // [128][64]
@@ -588,6 +635,7 @@ __global__ void __launch_bounds__(128) k_mlp_train(const MlpView M, const float*
     float* dy = h2 + TR_ROWS * 64;            // [128][16]
     float* d2 = dy + TR_ROWS * 16;            // [128][64]  dL/d(pre-activation of layer 2)
     float* d1 = d2 + TR_ROWS * 64;            // [128][64]  dL/d(pre-activation of layer 1)
+    __shared__ float wsum[4];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int r0 = blockIdx.x * TR_ROWS;
     for (int q = tid; q < TR_ROWS * 16; q += blockDim.x) {
@@ -605,12 +653,10 @@ __global__ void __launch_bounds__(128) k_mlp_train(const MlpView M, const float*
         mlp_tile_forward(M, A, lane, y, a1, a2);
 #pragma unroll
         for (int nt = 0; nt < 8; ++nt) {
-            const int c = nt * 8 + 2 * t;
-            h1[(tr + g) * 64 + c] = a1[nt][0]; h1[(tr + g) * 64 + c + 1] = a1[nt][1];
-            h1[(tr + g + 8) * 64 + c] = a1[nt][2]; h1[(tr + g + 8) * 64 + c + 1] = a1[nt][3];
-            h2[(tr + g) * 64 + c] = a2[nt][0]; h2[(tr + g) * 64 + c + 1] = a2[nt][1];
-            h2[(tr + g + 8) * 64 + c] = a2[nt][2]; h2[(tr + g + 8) * 64 + c + 1] = a2[nt][3];
+            store_d(h1, 64, tr, nt * 8, lane, a1[nt]);
+            store_d(h2, 64, tr, nt * 8, lane, a2[nt]);
         }
+        float dyv[2][4];
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
@@ -620,75 +666,154 @@ __global__ void __launch_bounds__(128) k_mlp_train(const MlpView M, const float*
                 const float target = live ? Y[(int64_t)rows[r0 + row] * MLP_OUT + col] : 0.f;
                 const float diff = live ? (y[nt][q] - target) : 0.f;
                 lsum += diff * diff;
-                dy[row * 16 + col] = 2.f * diff * inv_norm;
+                dyv[nt][q] = 2.f * diff * inv_norm;
             }
-    }
-    __syncthreads();
-    // backward: d2 = (dy W3) (1 - h2^2); d1 = (d2 W2) (1 - h1^2)
-    const float* W2 = params + P_W2;
-    const float* W3 = params + P_W3;
-    for (int q = tid; q < TR_ROWS * 64; q += blockDim.x) {
-        const int r = q >> 6, j = q & 63;
-        float s = 0.f;
-        for (int o = 0; o < M.ns; ++o) s = fmaf(dy[r * 16 + o], W3[o * 64 + j], s);
-        const float hv = h2[q];
-        d2[q] = s * (1.f - hv * hv);
-    }
-    __syncthreads();
-    for (int q = tid; q < TR_ROWS * 64; q += blockDim.x) {
-        const int r = q >> 6, i = q & 63;
-        float s = 0.f;
-        for (int j = 0; j < 64; ++j) s = fmaf(d2[r * 64 + j], W2[j * 64 + i], s);
-        const float hv = h1[q];
-        d1[q] = s * (1.f - hv * hv);
-    }
-    __syncthreads();
-    // weight gradients summed over the block's rows
-    for (int q = tid; q < P_N; q += blockDim.x) {
-        float s = 0.f;
-        if (q < P_B1) {                       // W1[i][k] += d1[r][i] x[r][k]
-            const int i = q / MLP_IN, kk = q % MLP_IN;
-            if (kk < M.nc) for (int r = 0; r < TR_ROWS; ++r) s = fmaf(d1[r * 64 + i], xs[r * 16 + kk], s);
-        } else if (q < P_W2) {                // b1
-            const int i = q - P_B1;
-            for (int r = 0; r < TR_ROWS; ++r) s += d1[r * 64 + i];
-        } else if (q < P_B2) {                // W2[j][i] += d2[r][j] h1[r][i]
-            const int j = (q - P_W2) / 64, i = (q - P_W2) % 64;
-            for (int r = 0; r < TR_ROWS; ++r) s = fmaf(d2[r * 64 + j], h1[r * 64 + i], s);
-        } else if (q < P_W3) {                // b2
-            const int j = q - P_B2;
-            for (int r = 0; r < TR_ROWS; ++r) s += d2[r * 64 + j];
-        } else if (q < P_B3) {                // W3[o][j] += dy[r][o] h2[r][j]
-            const int o = (q - P_W3) / 64, j = (q - P_W3) % 64;
-            if (o < M.ns) for (int r = 0; r < TR_ROWS; ++r) s = fmaf(dy[r * 16 + o], h2[r * 64 + j], s);
-        } else {                              // b3
-            const int o = q - P_B3;
-            if (o < M.ns) for (int r = 0; r < TR_ROWS; ++r) s += dy[r * 16 + o];
+        store_d(dy, 16, tr, 0, lane, dyv[0]);
+        store_d(dy, 16, tr, 8, lane, dyv[1]);
+        __syncwarp();
+        // dH2 = dY (16 x 16) W3 (16 x 64); dZ2 = dH2 (1 - h2^2), kept as the next GEMM's A
+        load_a_tile(dy + tr * 16, lane, A);
+        uint32_t A2[4][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+            uint32_t b0, b1;
+            load_b(M.w3t, MLP_OUT, nt, 0, lane, b0, b1);
+            mma_bf16(d, A, b0, b1);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) d[q] *= 1.f - a2[nt][q] * a2[nt][q];
+            store_d(d2, 64, tr, nt * 8, lane, d);
+            const int kt = nt >> 1, hi = nt & 1;
+            A2[kt][0 + 2 * hi] = pack_bf16(d[0], d[1]);
+            A2[kt][1 + 2 * hi] = pack_bf16(d[2], d[3]);
         }
-        if (s != 0.f) atomicAdd(&grad[q], s);
+        // dH1 = dZ2 (16 x 64) W2 (64 x 64); dZ1 = dH1 (1 - h1^2)
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kt = 0; kt < 4; ++kt) {
+                uint32_t b0, b1;
+                load_b(M.w2t, MLP_H, nt, kt, lane, b0, b1);
+                mma_bf16(d, A2[kt], b0, b1);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) d[q] *= 1.f - a1[nt][q] * a1[nt][q];
+            store_d(d1, 64, tr, nt * 8, lane, d);
+        }
+    }
+    __syncthreads();
+    float* out = part + (int64_t)blockIdx.x * PART_STRIDE;
+    // weight gradients over the block's 128 rows (K = 128: 8 k-steps). Warp w: rows w*16.. of
+    // dW2 (64 x 64) and dW1 (64 x 16), columns w*16.. of dW3 (16 x 64).
+    {
+        float acc[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+        for (int kt = 0; kt < TR_ROWS / 16; ++kt) {
+            uint32_t A[4];
+            load_at(d2, 64, kt * 16, w * 16, lane, A);
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                uint32_t b0, b1;
+                load_bz(h1, 64, kt * 16, nt * 8, lane, b0, b1);
+                mma_bf16(acc[nt], A, b0, b1);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) store_d(out + P_W2, 64, w * 16, nt * 8, lane, acc[nt]);
+    }
+    {
+        float acc[2][4];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+        for (int kt = 0; kt < TR_ROWS / 16; ++kt) {
+            uint32_t A[4];
+            load_at(d1, 64, kt * 16, w * 16, lane, A);
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                uint32_t b0, b1;
+                load_bz(xs, 16, kt * 16, nt * 8, lane, b0, b1);
+                mma_bf16(acc[nt], A, b0, b1);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) store_d(out + P_W1, 16, w * 16, nt * 8, lane, acc[nt]);
+    }
+    {
+        float acc[2][4];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+        for (int kt = 0; kt < TR_ROWS / 16; ++kt) {
+            uint32_t A[4];
+            load_at(dy, 16, kt * 16, 0, lane, A);
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                uint32_t b0, b1;
+                load_bz(h2, 64, kt * 16, w * 16 + nt * 8, lane, b0, b1);
+                mma_bf16(acc[nt], A, b0, b1);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) store_d(out + P_W3, 64, 0, w * 16 + nt * 8, lane, acc[nt]);
+    }
+    // bias gradients: column sums in row order
+    for (int c = tid; c < 2 * MLP_H + MLP_OUT; c += blockDim.x) {
+        float sum = 0.f;
+        if (c < MLP_H) {
+            for (int r = 0; r < TR_ROWS; ++r) sum += d1[r * 64 + c];
+            out[P_B1 + c] = sum;
+        } else if (c < 2 * MLP_H) {
+            for (int r = 0; r < TR_ROWS; ++r) sum += d2[r * 64 + c - MLP_H];
+            out[P_B2 + c - MLP_H] = sum;
+        } else {
+            for (int r = 0; r < TR_ROWS; ++r) sum += dy[r * 16 + c - 2 * MLP_H];
+            out[P_B3 + c - 2 * MLP_H] = sum;
+        }
     }
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
-    if (lane == 0) atomicAdd(loss_acc, lsum);
+    if (lane == 0) wsum[w] = lsum;
+    __syncthreads();
+    if (tid == 0) out[P_N] = (wsum[0] + wsum[1]) + (wsum[2] + wsum[3]);
 }
 
+// Adam on the block-order sum of the partial gradients, with the BF16 operand copies refreshed;
+// one thread adds the launch's squared errors to loss_acc[0] in block order.
 __global__ void k_mlp_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
-                           float* __restrict__ grad, float lr, float b1, float b2, float eps, float c1, float c2) {
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < P_N; q += gridDim.x * blockDim.x) {
-        const float gq = grad[q];
+                           const float* __restrict__ part, int nb, float lr, float b1, float b2, float eps, float c1,
+                           float c2, __nv_bfloat16* __restrict__ bf, float* __restrict__ loss_acc) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= P_N; q += gridDim.x * blockDim.x) {
+        float gq = 0.f;
+        for (int b = 0; b < nb; ++b) gq += part[(int64_t)b * PART_STRIDE + q];
+        if (q == P_N) {
+            loss_acc[0] += gq;
+            continue;
+        }
         const float mq = b1 * m[q] + (1.f - b1) * gq;
         const float vq = b2 * v[q] + (1.f - b2) * gq * gq;
         m[q] = mq;
         v[q] = vq;
-        p[q] -= lr * (mq / c1) / (sqrtf(vq / c2) + eps);
-        grad[q] = 0.f;
+        const float pq = p[q] - lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+        p[q] = pq;
+        mlp_bf16_store(bf, q, pq);
+    }
+}
+
+// the block-order sum of the partial gradients (the gradient check's view)
+__global__ void k_mlp_grad_sum(const float* __restrict__ part, int nb, float* __restrict__ grad) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= P_N; q += gridDim.x * blockDim.x) {
+        float gq = 0.f;
+        for (int b = 0; b < nb; ++b) gq += part[(int64_t)b * PART_STRIDE + q];
+        grad[q] = gq;
     }
 }
 
 // forward only: squared error on scaled outputs, summed
 __global__ void __launch_bounds__(128) k_mlp_eval(const MlpView M, const float* __restrict__ X,
                                                   const float* __restrict__ Y, int first, int count,
-                                                  float* __restrict__ loss_acc) {
+                                                  float* __restrict__ block_loss) {
     __shared__ float xs[4][32 * 16];
+    __shared__ float wsum[4];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
     float lsum = 0.f;
@@ -715,7 +840,9 @@ __global__ void __launch_bounds__(128) k_mlp_eval(const MlpView M, const float* 
         __syncwarp();
     }
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
-    if (lane == 0) atomicAdd(loss_acc, lsum);
+    if (lane == 0) wsum[w] = lsum;
+    __syncthreads();
+    if (threadIdx.x == 0) block_loss[blockIdx.x] = (wsum[0] + wsum[1]) + (wsum[2] + wsum[3]);
 }
 
 // surrogate prediction of species for raw concentration inputs (the speciation step's view)
@@ -745,14 +872,14 @@ __global__ void __launch_bounds__(128) k_mlp_predict(const MlpView M, const Spec
 static clb_status mlp_alloc(clb_handle* h) {
     if (h->d_mlp) return CLB_OK;
     cudaError_t e = cudaMalloc(&h->d_mlp, sizeof(float) * (4 * P_N + 64));
-    if (e == cudaSuccess) e = cudaMalloc(&h->d_mlp_bf16, sizeof(__nv_bfloat16) * (MLP_H * MLP_IN + MLP_H * MLP_H + MLP_OUT * MLP_H));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_mlp_bf16, sizeof(__nv_bfloat16) * BF_N);
     if (e != cudaSuccess) return cuda_check(h, e, "surrogate parameters");
     cudaMemsetAsync(h->d_mlp, 0, sizeof(float) * (4 * P_N + 64), h->stream);
     return CLB_OK;
 }
 
 static void mlp_refresh_bf16(clb_handle* h) {
-    k_mlp_to_bf16<<<32, 256, 0, h->stream>>>(h->d_mlp, static_cast<__nv_bfloat16*>(h->d_mlp_bf16));
+    k_mlp_to_bf16<<<(P_N + 255) / 256, 256, 0, h->stream>>>(h->d_mlp, static_cast<__nv_bfloat16*>(h->d_mlp_bf16));
 }
 
 // Glorot-uniform initial weights from a seeded xorshift64* stream, zero biases
@@ -795,10 +922,14 @@ clb_status surrogate_train(clb_handle* h, const clb_surrogate_train_desc* d, clb
     if (e == cudaSuccess) e = cudaMalloc(&X, sizeof(float) * (size_t)n * MLP_IN);
     if (e == cudaSuccess) e = cudaMalloc(&Y, sizeof(float) * (size_t)n * MLP_OUT);
     if (e == cudaSuccess) e = cudaMalloc(&loss, sizeof(float) * 4);
+    const int part_blocks = (d->batch + TR_ROWS - 1) / TR_ROWS, eval_blocks = h->num_sms * 2;
+    float *part = nullptr, *eval_part = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&part, sizeof(float) * (size_t)part_blocks * PART_STRIDE);
+    if (e == cudaSuccess) e = cudaMalloc(&eval_part, sizeof(float) * eval_blocks);
     if (e == cudaSuccess) e = cudaMalloc(&rows, sizeof(int) * (size_t)n);
     auto cleanup = [&]() {
         cudaFree(dlo); cudaFree(dhi); cudaFree(cin); cudaFree(ceq); cudaFree(X); cudaFree(Y);
-        cudaFree(loss); cudaFree(rows); cudaFree(rng);
+        cudaFree(loss); cudaFree(rows); cudaFree(rng); cudaFree(part); cudaFree(eval_part);
         cudaEventDestroy(t0); cudaEventDestroy(t1);
     };
     if (e != cudaSuccess) { cleanup(); return cuda_check(h, e, "training buffers"); }
@@ -861,7 +992,6 @@ clb_status surrogate_train(clb_handle* h, const clb_surrogate_train_desc* d, clb
     float* P = h->d_mlp;
     float* Mm = P + P_N;
     float* V = P + 2 * P_N;
-    float* G = P + 3 * P_N;
     cudaMemcpyAsync(P, p0.data(), sizeof(float) * P_N, cudaMemcpyHostToDevice, h->stream);
     cudaMemsetAsync(Mm, 0, sizeof(float) * 3 * P_N, h->stream);
     mlp_refresh_bf16(h);
@@ -886,22 +1016,26 @@ clb_status surrogate_train(clb_handle* h, const clb_surrogate_train_desc* d, clb
         for (int s0 = 0; s0 < n_tr; s0 += d->batch) {
             const int cnt = std::min(d->batch, n_tr - s0);
             const MlpView Mv = mlp_view(h);
-            k_mlp_train<<<(cnt + TR_ROWS - 1) / TR_ROWS, 128, smem, h->stream>>>(Mv, P, X, Y, rows + s0, cnt,
-                                                                                1.f / (float)(cnt * ns), G, loss);
+            const int nb = (cnt + TR_ROWS - 1) / TR_ROWS;
+            k_mlp_train<<<nb, 128, smem, h->stream>>>(Mv, X, Y, rows + s0, cnt, 1.f / (float)(cnt * ns), part);
             ++step;
             const float c1 = 1.f - std::pow(b1, (float)step), c2 = 1.f - std::pow(b2, (float)step);
             // learning rate decays by 5 % per epoch
             const float lr = (float)d->learning_rate * std::pow(0.95f, (float)epoch);
-            k_mlp_adam<<<(P_N + 255) / 256, 256, 0, h->stream>>>(P, Mm, V, G, lr, b1, b2, 1e-8f, c1, c2);
-            mlp_refresh_bf16(h);
+            k_mlp_adam<<<(P_N + 256) / 256, 256, 0, h->stream>>>(P, Mm, V, part, nb, lr, b1, b2, 1e-8f, c1, c2,
+                                                                   static_cast<__nv_bfloat16*>(h->d_mlp_bf16), loss);
         }
-        k_mlp_eval<<<h->num_sms * 2, 128, 0, h->stream>>>(mlp_view(h), X, Y, n_tr, n_val, loss + 1);
+        k_mlp_eval<<<eval_blocks, 128, 0, h->stream>>>(mlp_view(h), X, Y, n_tr, n_val, eval_part);
         float l[4];
+        std::vector<float> ev((size_t)eval_blocks);
         cudaMemcpyAsync(l, loss, sizeof(l), cudaMemcpyDeviceToHost, h->stream);
+        cudaMemcpyAsync(ev.data(), eval_part, sizeof(float) * eval_blocks, cudaMemcpyDeviceToHost, h->stream);
         e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) { cleanup(); return cuda_check(h, e, "training"); }
+        double vsum = 0;
+        for (float x : ev) vsum += x;  // block order: deterministic
         last_train = l[0] / (float)((size_t)n_tr * ns);
-        const float val = l[1] / (float)((size_t)n_val * ns);
+        const float val = (float)(vsum / (double)((size_t)n_val * ns));
         if (val < best_val) {
             best_val = val;
             since = 0;
@@ -955,12 +1089,14 @@ clb_status surrogate_predict(clb_handle* h, const double* cin, int n, double* co
 // Loss and gradient of the current network on given scaled samples (for the gradient check).
 clb_status surrogate_gradient(clb_handle* h, const float* X, const float* Y, int n, float* grad, float* loss) {
     if (!h->mlp_ready) return fail(h, CLB_NOT_INITIALIZED, "no surrogate parameters");
-    float *dx = nullptr, *dy = nullptr, *dl = nullptr, *dg = nullptr;
+    if (n < 1) return fail(h, CLB_INVALID_ARG, "no samples");
+    const int nb = (n + TR_ROWS - 1) / TR_ROWS;
+    float *dx = nullptr, *dy = nullptr, *dp = nullptr, *dg = nullptr;
     int* dr = nullptr;
     cudaError_t e = cudaMalloc(&dx, sizeof(float) * (size_t)n * MLP_IN);
     if (e == cudaSuccess) e = cudaMalloc(&dy, sizeof(float) * (size_t)n * MLP_OUT);
-    if (e == cudaSuccess) e = cudaMalloc(&dl, sizeof(float) * 4);
-    if (e == cudaSuccess) e = cudaMalloc(&dg, sizeof(float) * P_N);
+    if (e == cudaSuccess) e = cudaMalloc(&dp, sizeof(float) * (size_t)nb * PART_STRIDE);
+    if (e == cudaSuccess) e = cudaMalloc(&dg, sizeof(float) * PART_STRIDE);
     if (e == cudaSuccess) e = cudaMalloc(&dr, sizeof(int) * n);
     std::vector<int> r(n);
     for (int q = 0; q < n; ++q) r[q] = q;
@@ -968,17 +1104,15 @@ clb_status surrogate_gradient(clb_handle* h, const float* X, const float* Y, int
     if (e == cudaSuccess) e = cudaMemcpyAsync(dy, Y, sizeof(float) * (size_t)n * MLP_OUT, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dr, r.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) {
-        cudaMemsetAsync(dl, 0, sizeof(float) * 4, h->stream);
-        cudaMemsetAsync(dg, 0, sizeof(float) * P_N, h->stream);
         const size_t smem = sizeof(float) * TR_ROWS * (16 + 64 + 64 + 16 + 64 + 64);
         cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_mlp_train<<<(n + TR_ROWS - 1) / TR_ROWS, 128, smem, h->stream>>>(mlp_view(h), h->d_mlp, dx, dy, dr, n,
-                                                                            1.f / (float)(n * CLB_SP(h).ns), dg, dl);
+        k_mlp_train<<<nb, 128, smem, h->stream>>>(mlp_view(h), dx, dy, dr, n, 1.f / (float)(n * CLB_SP(h).ns), dp);
+        k_mlp_grad_sum<<<(P_N + 256) / 256, 256, 0, h->stream>>>(dp, nb, dg);
         e = cudaMemcpyAsync(grad, dg, sizeof(float) * P_N, cudaMemcpyDeviceToHost, h->stream);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(loss, dl, sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(loss, dg + P_N, sizeof(float), cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     }
-    cudaFree(dx); cudaFree(dy); cudaFree(dl); cudaFree(dg); cudaFree(dr);
+    cudaFree(dx); cudaFree(dy); cudaFree(dp); cudaFree(dg); cudaFree(dr);
     return cuda_check(h, e, "surrogate gradient");
 }
 

@@ -20,6 +20,8 @@ struct MlpView {
     const __nv_bfloat16* w1b;  // [64][16]
     const __nv_bfloat16* w2b;  // [64][64]
     const __nv_bfloat16* w3b;  // [16][64]
+    const __nv_bfloat16* w2t;  // [64][64] W2 transposed (backward operand)
+    const __nv_bfloat16* w3t;  // [64][16] W3 transposed (backward operand)
     const float* b1;           // [64]
     const float* b2;           // [64]
     const float* b3;           // [16]

@@ -69,33 +69,36 @@ def pack256x128x128(scale=1, gen=None):
                 eps=1e-7, peclet=10.0, char_length=8.0, tau_ade_fixed=0.8)
 
 
-def inlet_connected(mat, shape, open_codes=(2,)):
-    """Mask of the open voxels (materials in open_codes) that face-connected open paths join to
-    the first interior plane x = 1."""
+def percolating_pores(mat, shape, open_codes=(2,)):
+    """Mask of the open voxels (materials in open_codes) of the interior planes x = 1..nx-2 that
+    face-connected open paths inside those planes join to both x = 1 and x = nx-2."""
     from scipy import ndimage
 
     m = np.isin(mat.reshape(shape), open_codes)
+    m[0] = m[-1] = False
     lab, _ = ndimage.label(m)
-    keep = np.unique(lab[1][lab[1] > 0])
+    keep = np.intersect1d(np.unique(lab[1][lab[1] > 0]), np.unique(lab[-2][lab[-2] > 0]))
     return np.isin(lab, keep).ravel()
 
 
 def pack256cube_8species(scale=1, seed=1003, gen=None):
     """256^3 sphere pack (porosity 0.40), 8 species with D_pore ~ U[0.02, 0.2] and
     D_biofilm = D_pore / 2, two microbes (materials 3 and 4) seeded on as many voxels as 2 % of the
-    pore voxels, drawn from the pore space that open paths join to the inlet plane; dual-Monod
+    pore voxels, drawn from the percolating pore cluster of the interior planes; dual-Monod
     kinetics mu_max 1e-4, Ks 0.1, Y 0.4, decay 1e-6; the biofilm automaton ('fraction' push, max
     density 100, biofilm threshold 0.1 of it) every iteration; the flow (tau 0.8, pressure drop
     1e-4, FP32) solved to 1e-6 first and re-solved every 500 iterations; 10,000 iterations.
 
-    Seeds stay out of isolated pore pockets: a colony that fills a pocket with no open neighbour
-    below the maximum density leaves the automaton's age wavefront without a fixed point (every
-    sweep deepens it), which ends the reference's run (complab.cpp:3039-3046) as it ends ours."""
+    Seeds stay out of pockets the percolating cluster does not reach: the automaton pushes only
+    between voxels of x = 1..nx-2 (the reference's bdryGap of 1), so a colony in a pocket with no
+    open face neighbour there (a pore at x = 1 walled in by grains except toward the inlet plane)
+    cannot shed its excess, or fills the pocket and leaves the age wavefront without a fixed
+    point; either ends the reference's run (complab.cpp:3030-3046) as it ends ours."""
     nxi, ny, nz = max(8, int(256 * scale)), max(8, int(256 * scale)), max(8, int(256 * scale))
     mat, shape = sphere_pack_domain(nxi, ny, nz, 0.40, 3.0, 8.0, seed=seed, gen=gen)
     rng = np.random.default_rng(seed)
     pore = np.flatnonzero(mat == 2)
-    joined = np.flatnonzero(inlet_connected(mat, shape))
+    joined = np.flatnonzero(percolating_pores(mat, shape))
     seeded = rng.choice(joined, size=max(2, min(joined.size, int(0.02 * pore.size))), replace=False)
     seeded.sort()
     half = seeded.size // 2
@@ -124,6 +127,35 @@ def pack256cube_8species(scale=1, seed=1003, gen=None):
 # headline reports the run's own figure). The CPU baseline weights its flow and transport samples
 # by it so that both arms time the same mix of work.
 FLOW_PER_TRANSPORT_CONFIG3 = 2.0
+
+
+def fracture192_carbonate(gen, scale=1.0, seed=1004):
+    """Precipitation with equilibrium chemistry: a 192^3 rough fracture (aperture 12, roughness 0.3;
+    `gen(nx_inner, ny, nz)` returns the generator's map, 0 rock and 2 pore), the 5-component
+    12-species tableau (tableau_5x12) solved per voxel, species fed at the inlet and initially
+    present at log-uniform levels in [1e-6, 1e-4] (H+ dominant so every component total is
+    positive), two components supersaturated with an immobile mineral (k 2e-6, log10 Ksp -6) that
+    seals a voxel at density 1e-3 (the deposit starts uniform in [0, 1e-3)), flow tau 0.8 at
+    pressure drop 1e-4 re-solved every 200 steps."""
+    S, logK, comp = tableau_5x12(seed)
+    ns = S.shape[0]
+    nxi, ny, nz = (max(8, int(192 * scale)),) * 3
+    mat = add_ghost_planes(gen(nxi, ny, nz), nxi, ny, nz)
+    shape = (nxi + 2, ny, nz)
+    rng = np.random.default_rng(seed)
+    sp = [dict(omega_pore=1 / 0.9, left_type=DIRICHLET, right_type=NEUMANN, left_bc=float(10 ** rng.uniform(-5, -3.5)),
+               c0=float(10 ** rng.uniform(-6, -4))) for _ in range(ns)]
+    sp[0]["c0"], sp[0]["left_bc"] = 3e-3, 2e-3
+    for s in (1, 2):
+        sp[s]["c0"], sp[s]["left_bc"] = 2e-3, 2e-3
+    sp.append(dict(omega_pore=1.0, mobile=0, left_type=NEUMANN, right_type=NEUMANN, c0=0.0))
+    nu = [0.0] * (ns + 1)
+    nu[1], nu[2] = 1.0, 1.0
+    full = 1e-3
+    m0 = np.random.default_rng(seed + 1).uniform(0.0, full, mat.size) * (mat == 2)
+    return dict(name="rough fracture 192^3, 5 components x 12 species, mineral", mat=mat, shape=shape, S=S,
+                logK=logK, comp=comp, species=sp, mineral=[2e-6, -6.0, ns] + nu, mineral_species=ns, full=full,
+                deposit=m0, tau=0.8, delta_p=1e-4, resolve_every=200)
 
 
 def ensemble_uneven_packs(n_domains=96, seed=1005, scale=1.0):

@@ -71,8 +71,9 @@ def bf16(a):
 
 
 def cpu_loss_grad(p, X, Y, ns):
-    """The network's loss and parameter gradient in FP64, with the forward GEMM operands rounded
-    to BF16 as the tensor cores see them and the backward pass in full precision."""
+    """The network's loss and parameter gradient in FP64, with every GEMM operand of the forward and
+    the backward pass rounded to BF16 as the tensor cores see them (FP32 accumulation on the GPU)
+    and the bias gradients from unrounded values."""
     W1 = p[:1024].reshape(64, 16); b1 = p[1024:1088]
     W2 = p[1088:5184].reshape(64, 64); b2 = p[5184:5248]
     W3 = p[5248:6272].reshape(16, 64); b3 = p[6272:6288]
@@ -84,9 +85,10 @@ def cpu_loss_grad(p, X, Y, ns):
     diff[:, :ns] = y[:, :ns] - Y[:, :ns]
     loss = np.sum(diff ** 2)
     dy = 2 * diff / (n * ns)
-    d2 = (dy @ W3) * (1 - h2 ** 2)
-    d1 = (d2 @ W2) * (1 - h1 ** 2)
-    g = np.concatenate([(d1.T @ X).ravel(), d1.sum(0), (d2.T @ h1).ravel(), d2.sum(0), (dy.T @ h2).ravel(), dy.sum(0)])
+    d2 = (bf16(dy) @ bf16(W3)) * (1 - h2 ** 2)
+    d1 = (bf16(d2) @ bf16(W2)) * (1 - h1 ** 2)
+    g = np.concatenate([(bf16(d1).T @ bf16(X)).ravel(), d1.sum(0), (bf16(d2).T @ bf16(h1)).ravel(), d2.sum(0),
+                        (bf16(dy).T @ bf16(h2)).ravel(), dy.sum(0)])
     return loss, g
 
 
@@ -110,6 +112,21 @@ def test_surrogate_gradient_matches_cpu(clb):
     scale = np.abs(g_c).max()
     assert np.max(np.abs(g - g_c)) < 2e-3 * scale
     assert np.dot(g, g_c) / (np.linalg.norm(g) * np.linalg.norm(g_c)) > 0.99999
+
+
+def test_surrogate_training_is_deterministic(clb):
+    """Gradients are summed per block and then across blocks in a fixed order (no atomics), and the
+    validation loss likewise, so two trainings from the same seed give the same parameters bit for
+    bit."""
+    S, logK, comp = workloads.carbonate_tableau()
+    out = []
+    for _ in range(2):
+        D = handle(clb, S, logK, comp)
+        D.surrogate_train([-5, -9, -8, -6], [-2, -5, -4, -3], n_samples=20000, epochs=3, batch=1024, patience=8,
+                          learning_rate=3e-3, seed=5)
+        out.append(D.surrogate_params()[0])
+        D.close()
+    np.testing.assert_array_equal(out[0], out[1])
 
 
 @pytest.fixture(scope="module")
