@@ -174,9 +174,9 @@ SIGNATURES = {
     "clb_batch_autotune": [C.c_void_p, C.c_int, C.c_char_p, C.c_int],
     "clb_batch_counts": [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "clb_batch_destroy": [C.c_void_p],
-    "clb_batch_schedule": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int],
+    "clb_batch_schedule": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
     "clb_batch_get_schedule": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
-                               C.POINTER(C.c_int)],
+                               C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "clb_batch_set_stream": [C.c_void_p, C.c_void_p],
     "clb_ca_step": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "clb_refresh_dynamics": [C.c_void_p, C.c_int, C.c_int],
@@ -319,14 +319,15 @@ class Domain:
     def tune(self, key, value):
         self._check(lib().clb_tune(self.h, key.encode(), int(value)))
 
-    def schedule(self, persistent=True, tile=2048, lag=8, steps_per_launch=2):
+    def schedule(self, persistent=True, tile=2048, lag=8, steps_per_launch=2, ctas_per_sm=4):
         _check_global(lib().clb_batch_schedule(self.b, int(bool(persistent)), int(tile), int(lag),
-                                               int(steps_per_launch)))
+                                               int(steps_per_launch), int(ctas_per_sm)))
 
     def get_schedule(self):
-        v = [C.c_int() for _ in range(4)]
+        v = [C.c_int() for _ in range(5)]
         _check_global(lib().clb_batch_get_schedule(self.b, *[C.byref(x) for x in v]))
-        return dict(persistent=bool(v[0].value), tile=v[1].value, lag=v[2].value, steps_per_launch=v[3].value)
+        return dict(persistent=bool(v[0].value), tile=v[1].value, lag=v[2].value, steps_per_launch=v[3].value,
+                    ctas_per_sm=v[4].value)
 
     def set_stream(self, stream):
         """stream: a cudaStream_t as an integer (torch.cuda.Stream().cuda_stream), or None."""
@@ -750,14 +751,15 @@ class Batch:
     def step(self, n=1, flow=True, transport=True):
         _check_global(lib().clb_batch_step(self.b, int(n), int(flow), int(transport)))
 
-    def schedule(self, persistent=True, tile=2048, lag=8, steps_per_launch=2):
+    def schedule(self, persistent=True, tile=2048, lag=8, steps_per_launch=2, ctas_per_sm=4):
         _check_global(lib().clb_batch_schedule(self.b, int(bool(persistent)), int(tile), int(lag),
-                                               int(steps_per_launch)))
+                                               int(steps_per_launch), int(ctas_per_sm)))
 
     def get_schedule(self):
-        v = [C.c_int() for _ in range(4)]
+        v = [C.c_int() for _ in range(5)]
         _check_global(lib().clb_batch_get_schedule(self.b, *[C.byref(x) for x in v]))
-        return dict(persistent=bool(v[0].value), tile=v[1].value, lag=v[2].value, steps_per_launch=v[3].value)
+        return dict(persistent=bool(v[0].value), tile=v[1].value, lag=v[2].value, steps_per_launch=v[3].value,
+                    ctas_per_sm=v[4].value)
 
     def set_stream(self, stream):
         """stream: a cudaStream_t as an integer (torch.cuda.Stream().cuda_stream), or None."""

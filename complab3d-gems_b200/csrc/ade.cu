@@ -594,17 +594,17 @@ __global__ void k_ade_init(TS* __restrict__ g, TS* __restrict__ glink, int64_t K
     }
 }
 
+// shifted != 0: the populations g_i - t_i go out; 0: the stored values g_i - sigma t_i as they are
 template <typename TS>
 __global__ void k_ade_get_pops(const TS* __restrict__ g, const TS* __restrict__ glink, const SparseView S,
-                               const Geom G, int odd, double c0, double* __restrict__ out) {
-    // stored values g_i - sigma t_i; the shifted populations g_i - t_i go out
+                               const Geom G, int odd, double c0, int shifted, double* __restrict__ out) {
     constexpr double sig = ade_sigma<TS>();
     double init[7];
     for (int i = 0; i < 7; ++i) init[i] = q7w(i) * (c0 - sig);
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
         double v[7];
         natural<TS, double, 7>(S, G, g, glink, n, odd, init, v);
-        for (int i = 0; i < 7; ++i) out[(int64_t)i * G.N + n] = sig == 1.0 ? v[i] : v[i] - q7w(i) * (1.0 - sig);
+        for (int i = 0; i < 7; ++i) out[(int64_t)i * G.N + n] = (sig == 1.0 || !shifted) ? v[i] : v[i] - q7w(i) * (1.0 - sig);
     }
 }
 
@@ -639,12 +639,14 @@ __global__ void k_ade_density(const TS* __restrict__ g, const TS* __restrict__ g
     }
 }
 
+// shifted != 0: `in` holds g_i - t_i; 0: the stored values g_i - sigma t_i
 template <typename TS>
 __global__ void k_ade_set_pops(TS* __restrict__ g, TS* __restrict__ glink, const SparseView S, const Geom G, int odd,
-                               const double* __restrict__ in) {
+                               int shifted, const double* __restrict__ in) {
+    const double add = shifted ? 1.0 - ade_sigma<TS>() : 0.0;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
         double v[7];
-        for (int i = 0; i < 7; ++i) v[i] = in[(int64_t)i * G.N + n] + q7w(i) * (1.0 - ade_sigma<TS>());
+        for (int i = 0; i < 7; ++i) v[i] = in[(int64_t)i * G.N + n] + q7w(i) * add;
         put_natural<TS, 7>(S, G, g, glink, n, odd, v);
     }
 }
@@ -1042,12 +1044,14 @@ clb_status ade_set_concentration(clb_handle* h, int s, const double* host) {
     if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
     if (h->ap.slot[h->u2i[s]] < 0) return ade_set_immobile(h, s, host);
     const size_t N = (size_t)h->g.N;
+    // in the storage's own convention, so a small concentration is not rounded through C - 1
+    const double sig = h->ade_prec == CLB_F64 ? 1.0 : 0.0;
     std::vector<double> pops(7 * N);
     for (int i = 0; i < 7; ++i) {
         const double w = q7w(i);
-        for (size_t n = 0; n < N; ++n) pops[(size_t)i * N + n] = w * (host[n] - 1.0);
+        for (size_t n = 0; n < N; ++n) pops[(size_t)i * N + n] = w * (host[n] - sig);
     }
-    return ade_set_populations(h, s, pops.data());
+    return ade_set_populations(h, s, pops.data(), 0);
 }
 
 clb_status ade_set_thermo(clb_handle* h, const clb_thermo_desc* d) {
@@ -1376,11 +1380,10 @@ __device__ __forceinline__ void persist_neumann_pixel(const BatchDomain& d, cons
     d.neu[((int64_t)J.s * 2 + J.side) * G.plane + p] = r;
 }
 
-template <typename TS, typename TC, int NM>
-#ifndef PERSIST_MINB
-#define PERSIST_MINB 4
-#endif
-__global__ void __launch_bounds__(ADE_THREADS, PERSIST_MINB) k_batch_persistent(const PersistView V) {
+// MINB: resident CTAs per SM the registers are budgeted for (4: no spills; 6 and 8 trade some
+// spilled registers for more warps to hide memory latency)
+template <typename TS, typename TC, int NM, int MINB>
+__global__ void __launch_bounds__(ADE_THREADS, MINB) k_batch_persistent(const PersistView V) {
     extern __shared__ __align__(16) unsigned char ade_smem[];
     const AdeFrame<TC> F = ade_frame<TC, NM>(ade_smem, 0);
     __shared__ __align__(16) BatchDomain sd;
@@ -1464,15 +1467,15 @@ __global__ void __launch_bounds__(ADE_THREADS, PERSIST_MINB) k_batch_persistent(
     }
 }
 
-template <typename TS, typename TC, int NM>
+template <typename TS, typename TC, int NM, int MINB>
 static void persist_launch_t(const PersistView& V, int blocks_per_sm, int num_sms, cudaStream_t st) {
     // the shared-memory attribute was set on this device by batch_persistent_resident (batch set-up)
-    k_batch_persistent<TS, TC, NM><<<blocks_per_sm * num_sms, ADE_THREADS, ade_slot_bytes<TC, NM>(), st>>>(V);
+    k_batch_persistent<TS, TC, NM, MINB><<<blocks_per_sm * num_sms, ADE_THREADS, ade_slot_bytes<TC, NM>(), st>>>(V);
 }
 
-template <typename TS, typename TC, int NM>
+template <typename TS, typename TC, int NM, int MINB>
 static int persist_resident_t() {
-    auto kern = k_batch_persistent<TS, TC, NM>;
+    auto kern = k_batch_persistent<TS, TC, NM, MINB>;
     const int sm = ade_slot_bytes<TC, NM>();
     cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     int b = 0;
@@ -1480,28 +1483,50 @@ static int persist_resident_t() {
     return std::max(1, b);
 }
 
-#define CLB_PERSIST_NM(F, TS, TC, ...)                      \
-    (nm <= 1 ? F<TS, TC, 1>(__VA_ARGS__)                     \
-     : nm <= 2 ? F<TS, TC, 2>(__VA_ARGS__)                   \
-     : nm <= 4 ? F<TS, TC, 4>(__VA_ARGS__)                   \
-     : nm <= 8 ? F<TS, TC, 8>(__VA_ARGS__) : F<TS, TC, 16>(__VA_ARGS__))
+// register budgets built: 4 for every lattice; 6 and 8 also for FP32 arithmetic with up to 4
+// mobile species (the ensemble sweeps)
+int persist_minb(int prec, int nm, int minb) {
+    if (prec != CLB_F64 && nm <= 4 && (minb == 6 || minb == 8)) return minb;
+    return 4;
+}
 
-void launch_batch_persistent(const PersistView& V, int prec, int nm, int blocks_per_sm, int num_sms, cudaStream_t st) {
+#define CLB_PERSIST_M(F, TS, TC, NMV, ...)                                                                     \
+    (mb == 8 ? F<TS, TC, NMV, 8>(__VA_ARGS__) : mb == 6 ? F<TS, TC, NMV, 6>(__VA_ARGS__) : F<TS, TC, NMV, 4>(__VA_ARGS__))
+#define CLB_PERSIST_NM(F, TS, TC, ...)                                                                         \
+    (nm <= 1 ? CLB_PERSIST_M(F, TS, TC, 1, __VA_ARGS__)                                                       \
+     : nm <= 2 ? CLB_PERSIST_M(F, TS, TC, 2, __VA_ARGS__)                                                     \
+     : nm <= 4 ? CLB_PERSIST_M(F, TS, TC, 4, __VA_ARGS__)                                                     \
+     : nm <= 8 ? F<TS, TC, 8, 4>(__VA_ARGS__) : F<TS, TC, 16, 4>(__VA_ARGS__))
+
+void launch_batch_persistent(const PersistView& V, int prec, int nm, int minb, int blocks_per_sm, int num_sms,
+                             cudaStream_t st) {
+    const int mb = persist_minb(prec, nm, minb);
     switch (prec) {
-        case CLB_F64: CLB_PERSIST_NM(persist_launch_t, double, double, V, blocks_per_sm, num_sms, st); break;
+        case CLB_F64: nm <= 1 ? persist_launch_t<double, double, 1, 4>(V, blocks_per_sm, num_sms, st)
+                      : nm <= 2 ? persist_launch_t<double, double, 2, 4>(V, blocks_per_sm, num_sms, st)
+                      : nm <= 4 ? persist_launch_t<double, double, 4, 4>(V, blocks_per_sm, num_sms, st)
+                      : nm <= 8 ? persist_launch_t<double, double, 8, 4>(V, blocks_per_sm, num_sms, st)
+                                : persist_launch_t<double, double, 16, 4>(V, blocks_per_sm, num_sms, st);
+                      break;
         case CLB_F32: CLB_PERSIST_NM(persist_launch_t, float, float, V, blocks_per_sm, num_sms, st); break;
         default: CLB_PERSIST_NM(persist_launch_t, __half, float, V, blocks_per_sm, num_sms, st); break;
     }
 }
 
-int batch_persistent_resident(int prec, int nm) {
+int batch_persistent_resident(int prec, int nm, int minb) {
+    const int mb = persist_minb(prec, nm, minb);
     switch (prec) {
-        case CLB_F64: return CLB_PERSIST_NM(persist_resident_t, double, double);
+        case CLB_F64: return nm <= 1 ? persist_resident_t<double, double, 1, 4>()
+                           : nm <= 2 ? persist_resident_t<double, double, 2, 4>()
+                           : nm <= 4 ? persist_resident_t<double, double, 4, 4>()
+                           : nm <= 8 ? persist_resident_t<double, double, 8, 4>()
+                                     : persist_resident_t<double, double, 16, 4>();
         case CLB_F32: return CLB_PERSIST_NM(persist_resident_t, float, float);
         default: return CLB_PERSIST_NM(persist_resident_t, __half, float);
     }
 }
 #undef CLB_PERSIST_NM
+#undef CLB_PERSIST_M
 
 void ade_refresh_neumann(clb_handle* h) { refresh_neumann(h); }
 
@@ -1546,7 +1571,7 @@ clb_status ade_couple(clb_handle* h) {
     return flow_velocity_at(h, h->ade_sp.node, h->ade_sp.K, h->d_u, h->ade_sp.K, h->ade_prec == CLB_F64 ? 0 : 1);
 }
 
-static clb_status ade_populations_i(clb_handle* h, int s, double* host) {
+static clb_status ade_populations_i(clb_handle* h, int s, double* host, int shifted = 1) {
     if (h->ap.slot[s] < 0) return fail(h, CLB_INVALID_ARG, "not a mobile species");
     const int m = h->ap.slot[s];
     double* buf = nullptr;
@@ -1558,9 +1583,9 @@ static clb_status ade_populations_i(clb_handle* h, int s, double* host) {
     const SparseView S = view_of(h->ade_sp);
     const double c0 = h->ap.c0[s];
     switch (h->ade_prec) {
-        case CLB_F64: k_ade_get_pops<double><<<grid, 256, 0, h->stream>>>((const double*)h->d_g + off, (const double*)h->d_glink + loff, S, h->g, odd, c0, buf); break;
-        case CLB_F32: k_ade_get_pops<float><<<grid, 256, 0, h->stream>>>((const float*)h->d_g + off, (const float*)h->d_glink + loff, S, h->g, odd, c0, buf); break;
-        default: k_ade_get_pops<__half><<<grid, 256, 0, h->stream>>>((const __half*)h->d_g + off, (const __half*)h->d_glink + loff, S, h->g, odd, c0, buf); break;
+        case CLB_F64: k_ade_get_pops<double><<<grid, 256, 0, h->stream>>>((const double*)h->d_g + off, (const double*)h->d_glink + loff, S, h->g, odd, c0, shifted, buf); break;
+        case CLB_F32: k_ade_get_pops<float><<<grid, 256, 0, h->stream>>>((const float*)h->d_g + off, (const float*)h->d_glink + loff, S, h->g, odd, c0, shifted, buf); break;
+        default: k_ade_get_pops<__half><<<grid, 256, 0, h->stream>>>((const __half*)h->d_g + off, (const __half*)h->d_glink + loff, S, h->g, odd, c0, shifted, buf); break;
     }
     e = cudaMemcpyAsync(host, buf, sizeof(double) * 7 * (size_t)h->g.N, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -1568,13 +1593,13 @@ static clb_status ade_populations_i(clb_handle* h, int s, double* host) {
     return cuda_check(h, e, "population copy");
 }
 
-clb_status ade_populations(clb_handle* h, int s, double* host) {
+clb_status ade_populations(clb_handle* h, int s, double* host, int shifted) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
-    return ade_populations_i(h, h->u2i[s], host);
+    return ade_populations_i(h, h->u2i[s], host, shifted);
 }
 
-clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
+clb_status ade_set_populations(clb_handle* h, int s, const double* host, int shifted) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (s < 0 || s >= h->S) return fail(h, CLB_INVALID_ARG, "species index out of range");
     if (h->h_flags) {
@@ -1593,9 +1618,9 @@ clb_status ade_set_populations(clb_handle* h, int s, const double* host) {
     const size_t off = (size_t)m * h->ade_sp.SS, loff = off;
     const SparseView S = view_of(h->ade_sp);
     switch (h->ade_prec) {
-        case CLB_F64: k_ade_set_pops<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g + off, (double*)h->d_glink + loff, S, h->g, odd, buf); break;
-        case CLB_F32: k_ade_set_pops<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g + off, (float*)h->d_glink + loff, S, h->g, odd, buf); break;
-        default: k_ade_set_pops<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g + off, (__half*)h->d_glink + loff, S, h->g, odd, buf); break;
+        case CLB_F64: k_ade_set_pops<double><<<grid, 256, 0, h->stream>>>((double*)h->d_g + off, (double*)h->d_glink + loff, S, h->g, odd, shifted, buf); break;
+        case CLB_F32: k_ade_set_pops<float><<<grid, 256, 0, h->stream>>>((float*)h->d_g + off, (float*)h->d_glink + loff, S, h->g, odd, shifted, buf); break;
+        default: k_ade_set_pops<__half><<<grid, 256, 0, h->stream>>>((__half*)h->d_g + off, (__half*)h->d_glink + loff, S, h->g, odd, shifted, buf); break;
     }
     e = cudaStreamSynchronize(h->stream);
     cudaFree(buf);

@@ -26,6 +26,17 @@ clb_status cuda_check(clb_handle* h, cudaError_t e, const char* what) {
     return fail(h, e == cudaErrorMemoryAllocation ? CLB_OUT_OF_MEMORY : CLB_CUDA_ERROR, m);
 }
 
+// The host copy of the material map follows the device's lazily: a mask pass of the automaton that
+// changes voxels marks it stale, and the readers of h_mat refresh it here first, so the automaton
+// moves no map to the host in iterations where nobody reads it.
+clb_status host_mat_sync(clb_handle* h) {
+    if (!h->h_mat_stale) return CLB_OK;
+    cudaError_t e = cudaMemcpy(h->h_mat.data(), h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_check(h, e, "material copy");
+    h->h_mat_stale = false;
+    return CLB_OK;
+}
+
 // Compacted list of nodes whose class (by material code) is nonzero, in lexicographic order.
 std::vector<int32_t> build_list(const clb_handle* h, const int8_t* cls_by_code) {
     std::vector<int32_t> list;
@@ -355,14 +366,16 @@ clb_status clb_batch_counts(clb_batch* batch, int64_t* flow_nodes, int64_t* tran
     return batch_counts(batch, flow_nodes, transport_nodes);
 }
 
-clb_status clb_batch_schedule(clb_batch* batch, int persistent, int tile, int lag, int steps_per_launch) {
+clb_status clb_batch_schedule(clb_batch* batch, int persistent, int tile, int lag, int steps_per_launch,
+                              int ctas_per_sm) {
     if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
-    return batch_schedule(batch, persistent, tile, lag, steps_per_launch);
+    return batch_schedule(batch, persistent, tile, lag, steps_per_launch, ctas_per_sm);
 }
 
-clb_status clb_batch_get_schedule(clb_batch* batch, int* persistent, int* tile, int* lag, int* steps_per_launch) {
+clb_status clb_batch_get_schedule(clb_batch* batch, int* persistent, int* tile, int* lag, int* steps_per_launch,
+                                  int* ctas_per_sm) {
     if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
-    return batch_get_schedule(batch, persistent, tile, lag, steps_per_launch);
+    return batch_get_schedule(batch, persistent, tile, lag, steps_per_launch, ctas_per_sm);
 }
 
 clb_status clb_batch_set_stream(clb_batch* batch, void* stream) {
@@ -451,6 +464,8 @@ clb_status clb_get_field(clb_handle* h, int field, int index, void* host, int dt
     const size_t N = (size_t)h->g.N;
     if (field == CLB_FIELD_MATERIAL) {
         if (dtype != 2) return fail(h, CLB_INVALID_ARG, "material is int8");
+        clb_status st = host_mat_sync(h);
+        if (st != CLB_OK) return st;
         std::memcpy(host, h->h_mat.data(), N);
         return CLB_OK;
     }

@@ -33,7 +33,7 @@ struct clb_batch_s {
     std::map<std::tuple<int, int, int, int, int, int, int>, cudaGraphExec_t> graphs;
     // persistent schedule
     bool persistent = true;
-    int tile = 2048, lag = 8, per_launch = 2, resident = 0;
+    int tile = 2048, lag = 8, per_launch = 2, minb = 4, resident = 0;
     int64_t wait_ns = 2000000000;
     std::vector<int64_t> kf, ka;  // flow and transport nodes of each domain
     std::vector<int> jbeg;        // Neumann jobs of domain d: [jbeg[d], jbeg[d + 1])
@@ -196,7 +196,7 @@ clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out) {
     b->view.joff = b->d_joff;
     b->view.njobs = (int)jobs.size();
     b->neu_grid = std::max<int64_t>(1, std::min<int64_t>((joff.back() + 255) / 256, b->num_sms * 4));
-    b->resident = batch_persistent_resident(b->has_ade ? b->ade_prec : b->flow_prec, b->nm);
+    b->resident = batch_persistent_resident(b->has_ade ? b->ade_prec : b->flow_prec, b->nm, b->minb);
     if (b->has_flow && b->has_ade && b->flow_prec != b->ade_prec) b->persistent = false;  // one storage type per launch
     *out = b;
     return CLB_OK;
@@ -271,7 +271,7 @@ static clb_status persist_launch(clb_batch* b, int steps, int fodd, int aodd, bo
     V.aodd = aodd;
     V.wait_ns = b->wait_ns;
     cudaMemsetAsync(b->d_sync + 1, 0, sizeof(int) * (1 + (size_t)steps * 3 * nd), bstream(b));
-    launch_batch_persistent(V, ade ? b->ade_prec : b->flow_prec, b->nm, b->resident, b->num_sms, bstream(b));
+    launch_batch_persistent(V, ade ? b->ade_prec : b->flow_prec, b->nm, b->minb, b->resident, b->num_sms, bstream(b));
     return CLB_OK;
 }
 
@@ -407,7 +407,8 @@ clb_status batch_step(clb_batch* b, int n, int flow_on, int ade_on) {
 // Times the schedules of the batched steps and keeps the fastest. Per-lattice launches: flow with
 // 128 or 256 threads per block and 2, 4 or 8 blocks per SM, transport with 1 or 2 times the
 // resident grid. Persistent launches (when the lattices share one storage type): tiles of 1024,
-// 2048 or 4096 nodes, lags of 2, 8 or 32 domains, 2 or 8 steps per launch. Every timed step is a
+// 2048 or 4096 nodes, lags of 2, 8 or 32 domains, 2 or 8 steps per launch, registers budgeted for
+// 4, 6 or 8 resident CTAs per SM where those kernels are built. Every timed step is a
 // real step of the domains: their iteration counters show the advance.
 clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len) {
     cudaSetDevice(b->device);
@@ -490,27 +491,37 @@ clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len)
     float best = legacy;
     const bool can_persist = !(b->has_flow && b->has_ade && b->flow_prec != b->ade_prec);
     if (can_persist) {
-        int bt = b->tile, bw = b->lag, bs = b->per_launch;
-        for (int tile : {1024, 2048, 4096})
-            for (int lag : {2, 8, 32})
-                for (int S : {2, 8}) {
-                    b->tile = tile;
-                    b->lag = lag;
-                    b->per_launch = S;
-                    const float ms = time_persist();
-                    char buf[96];
-                    std::snprintf(buf, sizeof buf, "persistent %d/%d/%d:%.1fus ", tile, lag, S, ms * 1e3f);
-                    rep += buf;
-                    if (ms < best) { best = ms; bt = tile; bw = lag; bs = S; b->persistent = true; }
-                }
+        const int prec = b->has_ade ? b->ade_prec : b->flow_prec;
+        int bt = b->tile, bw = b->lag, bs = b->per_launch, bb = b->minb;
+        for (int mb : {4, 6, 8}) {
+            if (persist_minb(prec, b->nm, mb) != mb) continue;
+            b->minb = mb;
+            b->resident = batch_persistent_resident(prec, b->nm, mb);
+            for (int tile : {1024, 2048, 4096})
+                for (int lag : {2, 8, 32})
+                    for (int S : {2, 8}) {
+                        b->tile = tile;
+                        b->lag = lag;
+                        b->per_launch = S;
+                        const float ms = time_persist();
+                        char buf[96];
+                        std::snprintf(buf, sizeof buf, "persistent %d/%d/%d/%dx%d:%.1fus ", tile, lag, S, mb, b->resident,
+                                      ms * 1e3f);
+                        rep += buf;
+                        if (ms < best) { best = ms; bt = tile; bw = lag; bs = S; bb = mb; b->persistent = true; }
+                    }
+        }
         b->tile = bt;
         b->lag = bw;
         b->per_launch = bs;
+        b->minb = bb;
+        b->resident = batch_persistent_resident(prec, b->nm, bb);
     }
     {
         char buf[128];
         if (b->persistent)
-            std::snprintf(buf, sizeof buf, "-> persistent tile %d lag %d steps/launch %d", b->tile, b->lag, b->per_launch);
+            std::snprintf(buf, sizeof buf, "-> persistent tile %d lag %d steps/launch %d ctas/SM %d", b->tile, b->lag,
+                          b->per_launch, b->minb);
         else
             std::snprintf(buf, sizeof buf, "-> per-lattice launches");
         rep += buf;
@@ -541,17 +552,23 @@ clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len)
 }
 
 // Sets the schedule: persistent (tile nodes per item, lag in domains, steps per launch: even, at
-// most PERSIST_MAX_STEPS) or, persistent == 0, one launch per lattice and step.
-clb_status batch_schedule(clb_batch* b, int persistent, int tile, int lag, int steps_per_launch) {
+// most PERSIST_MAX_STEPS, the register budget in resident CTAs per SM) or, persistent == 0, one
+// launch per lattice and step.
+clb_status batch_schedule(clb_batch* b, int persistent, int tile, int lag, int steps_per_launch, int ctas_per_sm) {
     if (persistent) {
         if (b->has_flow && b->has_ade && b->flow_prec != b->ade_prec)
             return bfail(b, CLB_INVALID_ARG, "the persistent schedule needs one storage type for flow and transport");
         if (tile < 256 || tile % 256 || tile > (1 << 20) || lag < 1 || steps_per_launch < 2 ||
             steps_per_launch > PERSIST_MAX_STEPS || steps_per_launch % 2)
             return bfail(b, CLB_INVALID_ARG, "schedule: tile a multiple of 256, lag >= 1, an even 2..8 steps per launch");
+        const int prec = b->has_ade ? b->ade_prec : b->flow_prec;
+        if (ctas_per_sm != 4 && persist_minb(prec, b->nm, ctas_per_sm) != ctas_per_sm)
+            return bfail(b, CLB_INVALID_ARG, "schedule: no persistent kernel built for that number of CTAs per SM");
         b->tile = tile;
         b->lag = lag;
         b->per_launch = steps_per_launch;
+        b->minb = ctas_per_sm;
+        b->resident = batch_persistent_resident(prec, b->nm, ctas_per_sm);
     }
     b->persistent = persistent != 0;
     drop_graphs(b);
@@ -568,8 +585,10 @@ clb_status batch_set_stream(clb_batch* b, void* stream) {
 }
 
 // The schedule in force (for reports).
-clb_status batch_get_schedule(clb_batch* b, int* persistent, int* tile, int* lag, int* steps_per_launch) {
+clb_status batch_get_schedule(clb_batch* b, int* persistent, int* tile, int* lag, int* steps_per_launch,
+                              int* ctas_per_sm) {
     if (persistent) *persistent = b->persistent ? 1 : 0;
+    if (ctas_per_sm) *ctas_per_sm = b->minb;
     if (tile) *tile = b->tile;
     if (lag) *lag = b->lag;
     if (steps_per_launch) *steps_per_launch = b->per_launch;

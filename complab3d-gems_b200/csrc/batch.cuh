@@ -77,7 +77,9 @@ void launch_flow_batch(const BatchView& B, int prec, bool odd, int grid, int thr
 void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_mult, int num_sms, cudaStream_t st);
 void launch_neumann_batch(const BatchView& B, int prec, bool odd, int grid, cudaStream_t st);
 // the persistent schedule: one launch runs the whole item table
-void launch_batch_persistent(const PersistView& V, int prec, int nm, int blocks_per_sm, int num_sms, cudaStream_t st);
-int batch_persistent_resident(int prec, int nm);  // resident CTAs per SM of that launch
+void launch_batch_persistent(const PersistView& V, int prec, int nm, int minb, int blocks_per_sm, int num_sms,
+                             cudaStream_t st);
+int batch_persistent_resident(int prec, int nm, int minb);  // resident CTAs per SM of that launch
+int persist_minb(int prec, int nm, int minb);                // the register budget built for that request
 
 }  // namespace clb

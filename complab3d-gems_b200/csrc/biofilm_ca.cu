@@ -34,8 +34,10 @@
 //
 // The age sweep after a mask change is one in-place lexicographic sweep: it runs as wavefronts
 // over x + y + z, each voxel seeing its earlier neighbours updated and its later ones not. The
-// relaxation to convergence runs as Jacobi sweeps: the update is monotone and only ever raises an
-// age, so Jacobi and the in-place sweeps reach the same least fixed point.
+// relaxation to convergence runs as unordered in-place sweeps over the voxels that hold biomass
+// (the only ones the rule changes; the mask pass lists them): the update is monotone and only ever
+// raises an age, so any order of updates reaches the same least fixed point as the reference's
+// lexicographic in-place sweeps. Counters cross to the host through pinned memory.
 #include "sparse.cuh"
 
 #include <algorithm>
@@ -91,6 +93,7 @@ struct CaScalars {
     unsigned int overflow; // active voxels beyond the capacity
     unsigned int nonfinite; // biomass values that are NaN or infinite (mask pass)
     unsigned int moved;     // voxels whose material the mask pass changed
+    unsigned int nbio;      // voxels in the biomass list the mask pass writes
 };
 
 // ------------------------------------------------------------------ set-up and mask update
@@ -117,11 +120,19 @@ __global__ void k_ca_init(const CaView C, const int8_t* __restrict__ mat, const 
 
 // updateLocalMaskNtotalLattices3D; with several pore codes a reopened voxel copies the first
 // pore neighbour found in `mask_before` (the mask as it stood before the pass).
+// Also lists the voxels whose total biomass exceeds 1e-14 afterwards (in no particular order): the
+// only voxels the age wavefront and the push can touch.
 __global__ void k_ca_mask_total(const CaView C, int8_t* __restrict__ mat, const int8_t* __restrict__ mask_before,
-                                const double* __restrict__ bio, double* __restrict__ total, CaScalars* sc) {
+                                const double* __restrict__ bio, double* __restrict__ total, int32_t* __restrict__ blist,
+                                CaScalars* sc) {
     const Geom G = C.g;
     long long best = LLONG_MIN, msum = 0;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.N; n += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    // whole warps run the loop together, so the list append below is warp-wide
+    const int64_t span = (G.N + 31) / 32 * 32;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < span; n += (int64_t)gridDim.x * blockDim.x) {
+        bool listed = false;
+        if (n < G.N) {
         const int mk = mat[n];
         if (ca_open(C, mk)) {
             double bmass = 0.0;
@@ -161,7 +172,17 @@ __global__ void k_ca_mask_total(const CaView C, int8_t* __restrict__ mat, const 
         } else {
             msum += mk;
         }
-        best = max(best, ordered(total[n]));
+        const double tn = total[n];
+        best = max(best, ordered(tn));
+        listed = tn > 1e-14;
+        }
+        const unsigned int bal = __ballot_sync(0xffffffffu, listed);
+        if (bal) {
+            unsigned int base = 0;
+            if (lane == 0) base = atomicAdd(&sc->nbio, (unsigned int)__popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (listed) blist[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)n;
+        }
     }
     // block reduction, then one atomic per warp
     for (int o = 16; o > 0; o >>= 1) {
@@ -176,13 +197,16 @@ __global__ void k_ca_mask_total(const CaView C, int8_t* __restrict__ mat, const 
 
 // ------------------------------------------------------------------ push sweep
 
+// the voxels of x = 1..nx-2 that push, from the biomass list (any voxel above the maximum is on it)
 __global__ void k_ca_collect(const CaView C, const int8_t* __restrict__ mat, const double* __restrict__ total,
-                             int* __restrict__ aidx, int* __restrict__ act, int* __restrict__ done, int cap,
-                             CaScalars* sc) {
+                             const int32_t* __restrict__ blist, int* __restrict__ aidx, int* __restrict__ act,
+                             int* __restrict__ done, int cap, CaScalars* sc) {
     const Geom G = C.g;
     const int64_t lo = G.plane, hi = G.N - G.plane;  // x = 1..nx-2
-    for (int64_t n = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += (int64_t)gridDim.x * blockDim.x) {
-        if (!ca_open(C, mat[n])) continue;
+    const int nb = (int)sc->nbio;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb; j += gridDim.x * blockDim.x) {
+        const int64_t n = blist[j];
+        if (n < lo || n >= hi || !ca_open(C, mat[n])) continue;
         const double t = total[n];
         if (C.half) {
             // 'half': only biofilm voxels push, any total above the maximum
@@ -379,13 +403,23 @@ __device__ __forceinline__ int age_rule(const CaView& C, int64_t n, const int* _
     return cnt == nd ? a + 1 : a;
 }
 
-__global__ void k_age_jacobi(const CaView C, const int* __restrict__ in, int* __restrict__ out,
-                             const int8_t* __restrict__ distp, const double* __restrict__ total, CaScalars* sc) {
+// One relaxation sweep over the biomass list, in place (the rule leaves every other voxel as it
+// is). A voxel may read a neighbour's age before or after that neighbour's update in the same
+// sweep: both are iterates of the same monotone, inflationary rule, so the sweeps still reach the
+// least fixed point above the start, the one the reference's in-place sweeps reach, and a sweep
+// that changes nothing has read only final values.
+__global__ void k_age_relax(const CaView C, int* age, const int8_t* __restrict__ distp,
+                            const double* __restrict__ total, const int32_t* __restrict__ blist, CaScalars* sc) {
     unsigned int ch = 0;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < C.g.N; n += (int64_t)gridDim.x * blockDim.x) {
-        const int v = age_rule(C, n, in, distp, total);
-        out[n] = v;
-        ch += v != in[n];
+    const int nb = (int)sc->nbio;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb; j += gridDim.x * blockDim.x) {
+        const int64_t n = blist[j];
+        const int old = age[n];
+        const int v = age_rule(C, n, age, distp, total);
+        if (v != old) {
+            age[n] = v;
+            ++ch;
+        }
     }
     for (int o = 16; o > 0; o >>= 1) ch += __shfl_down_sync(0xffffffffu, ch, o);
     if ((threadIdx.x & 31) == 0 && ch) atomicAdd(&sc->changed, ch);
@@ -467,7 +501,9 @@ static CaView ca_view(const clb_handle* h) {
 void ca_free(clb_handle* h) {
     cudaFree(h->d_ca_total); h->d_ca_total = nullptr;
     cudaFree(h->d_ca_age); h->d_ca_age = nullptr;
-    cudaFree(h->d_ca_age2); h->d_ca_age2 = nullptr;
+    cudaFree(h->d_ca_blist); h->d_ca_blist = nullptr;
+    if (h->h_ca_pin) cudaFreeHost(h->h_ca_pin);
+    h->h_ca_pin = nullptr;
     cudaFree(h->d_ca_distp); h->d_ca_distp = nullptr;
     cudaFree(h->d_ca_aidx); h->d_ca_aidx = nullptr;
     cudaFree(h->d_ca_act); h->d_ca_act = nullptr;
@@ -510,7 +546,8 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
     const size_t N = (size_t)h->g.N;
     cudaError_t e = cudaMalloc(&h->d_ca_total, sizeof(double) * N);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_age, sizeof(int) * N);
-    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_age2, sizeof(int) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_blist, sizeof(int32_t) * N);
+    if (e == cudaSuccess) e = cudaHostAlloc(&h->h_ca_pin, 3 * sizeof(CaScalars), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_distp, N);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_aidx, sizeof(int) * N);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_sc, sizeof(CaScalars));
@@ -530,9 +567,11 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
     h->ca_half = d->push_mode;
     h->ca_seed = d->seed;
     h->ca_sweeps = 0;
-    CaScalars zero;
-    std::memset(&zero, 0, sizeof zero);
-    cudaMemcpyAsync(SC(h), &zero, sizeof zero, cudaMemcpyHostToDevice, h->stream);
+    // pinned copies: [0] the mask pass's starting value (max at its least), [1] read back, [2] scratch
+    CaScalars* pin = static_cast<CaScalars*>(h->h_ca_pin);
+    std::memset(pin, 0, 3 * sizeof(CaScalars));
+    pin[0].gmax = LLONG_MIN;
+    cudaMemsetAsync(SC(h), 0, sizeof(CaScalars), h->stream);
     const CaView C = ca_view(h);
     k_ca_init<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_bio, h->d_ca_total, h->d_ca_age,
                                                              h->d_ca_distp, h->d_ca_aidx, SC(h));
@@ -546,8 +585,10 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
 }
 
 static clb_status ca_scalars(clb_handle* h, CaScalars& s) {
-    cudaError_t e = cudaMemcpyAsync(&s, SC(h), sizeof s, cudaMemcpyDeviceToHost, h->stream);
+    CaScalars* pin = static_cast<CaScalars*>(h->h_ca_pin);
+    cudaError_t e = cudaMemcpyAsync(&pin[1], SC(h), sizeof s, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    s = pin[1];
     return e == cudaSuccess ? CLB_OK : cuda_check(h, e, "cellular automaton counters");
 }
 
@@ -556,13 +597,11 @@ static clb_status ca_mask_pass(clb_handle* h, const CaView& C, double& gmax, lon
     // non-finite biomass stops the run cleanly, as the reference does after this pass
     // (complab.cpp:2794-2796)
     CaScalars s;
-    std::memset(&s, 0, sizeof s);
-    s.gmax = LLONG_MIN;
-    cudaMemcpyAsync(SC(h), &s, sizeof s, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(SC(h), h->h_ca_pin, sizeof s, cudaMemcpyHostToDevice, h->stream);  // pinned: no staging
     if (h->d_ca_mask0) cudaMemcpyAsync(h->d_ca_mask0, h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToDevice, h->stream);
     ++h->launches;
     k_ca_mask_total<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_ca_mask0, h->d_bio,
-                                                                   h->d_ca_total, SC(h));
+                                                                   h->d_ca_total, h->d_ca_blist, SC(h));
     clb_status st = ca_scalars(h, s);
     if (st != CLB_OK) return st;
     gmax = unordered(s.gmax);
@@ -577,11 +616,11 @@ static clb_status ca_push_sweep(clb_handle* h, const CaView& C) {
     const int grid = h->num_sms * 8;
     for (;;) {
         CaScalars s;
-        std::memset(&s, 0, sizeof s);
-        cudaMemcpyAsync(SC(h), &s, sizeof s, cudaMemcpyHostToDevice, h->stream);
+        // active, remaining, changed, overflow to zero; the mask pass's results (the biomass list) stay
+        cudaMemsetAsync(&SC(h)->active, 0, 4 * sizeof(unsigned int), h->stream);
         h->launches += 1;
-        k_ca_collect<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_ca_total, h->d_ca_aidx, h->d_ca_act,
-                                                         h->d_ca_done, h->ca_cap, SC(h));
+        k_ca_collect<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_ca_total, h->d_ca_blist, h->d_ca_aidx,
+                                                         h->d_ca_act, h->d_ca_done, h->ca_cap, SC(h));
         clb_status st = ca_scalars(h, s);
         if (st != CLB_OK) return st;
         const int count = (int)std::min<unsigned int>(s.active, (unsigned int)h->ca_cap);
@@ -593,8 +632,9 @@ static clb_status ca_push_sweep(clb_handle* h, const CaView& C) {
             continue;
         }
         if (count == 0) { ++h->ca_sweeps; return CLB_OK; }
-        s.remaining = (unsigned int)count;
-        cudaMemcpyAsync(&SC(h)->remaining, &s.remaining, sizeof(unsigned int), cudaMemcpyHostToDevice, h->stream);
+        CaScalars* pin = static_cast<CaScalars*>(h->h_ca_pin);
+        pin[2].remaining = (unsigned int)count;  // pinned scratch: untouched until the next synchronisation
+        cudaMemcpyAsync(&SC(h)->remaining, &pin[2].remaining, sizeof(unsigned int), cudaMemcpyHostToDevice, h->stream);
         // every round completes at least the lexicographically first unfinished voxel, so `count`
         // rounds always suffice. Rounds go out in batches and the host reads the remaining count once
         // per batch: a round after the last voxel finished finds every voxel done and changes nothing,
@@ -622,33 +662,32 @@ static clb_status ca_push_sweep(clb_handle* h, const CaView& C) {
     }
 }
 
-// Jacobi sweeps of the age field until one changes nothing, at most 1001 sweeps (the reference's
-// limit of 1000 after the first). Sweeps go out in batches; the change counter is cleared before
-// the last sweep of a batch and read after it. A sweep of a settled field changes nothing, so a
-// batch that continues past the settling sweep leaves the same field, and the total number of
-// sweeps never exceeds the sequential loop's, so an unsettled field ends the same too.
+// Relaxation sweeps of the age field (in place, over the biomass list) until one changes nothing,
+// at most 1001 sweeps (the reference's limit of 1000 after the first). Sweeps go out in batches; the
+// change counter is cleared before the last sweep of a batch and read after it. A sweep of a settled
+// field changes nothing, so a batch that continues past the settling sweep leaves the same field.
+// The unordered in-place sweeps settle in no more sweeps than Jacobi sweeps would, and every
+// ordering reaches the same fixed point, so the field is the reference's; only how close a field
+// that never settles comes to the limit may differ.
 static clb_status ca_age_converge(clb_handle* h, const CaView& C, bool& settled) {
     settled = false;
     constexpr int SWEEP_BATCH = 8, MAX_SWEEPS = 1001;
     int done = 0;
+    CaScalars* pin = static_cast<CaScalars*>(h->h_ca_pin);
     while (done < MAX_SWEEPS) {
         const int b = std::min(SWEEP_BATCH, MAX_SWEEPS - done);
         for (int k = 0; k < b; ++k) {
-            if (k == b - 1) {
-                unsigned int zero = 0;
-                cudaMemcpyAsync(&SC(h)->changed, &zero, sizeof zero, cudaMemcpyHostToDevice, h->stream);
-            }
+            if (k == b - 1) cudaMemsetAsync(&SC(h)->changed, 0, sizeof(unsigned int), h->stream);
             ++h->launches;
-            k_age_jacobi<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_ca_age, h->d_ca_age2, h->d_ca_distp,
-                                                                        h->d_ca_total, SC(h));
-            std::swap(h->d_ca_age, h->d_ca_age2);
+            k_age_relax<<<h->num_sms * 4, CA_THREADS, 0, h->stream>>>(C, h->d_ca_age, h->d_ca_distp, h->d_ca_total,
+                                                                       h->d_ca_blist, SC(h));
         }
         done += b;
-        unsigned int ch = 0;
-        cudaError_t e = cudaMemcpyAsync(&ch, &SC(h)->changed, sizeof ch, cudaMemcpyDeviceToHost, h->stream);
+        cudaError_t e = cudaMemcpyAsync(&pin[1].changed, &SC(h)->changed, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                        h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) return cuda_check(h, e, "age relaxation");
-        if (ch == 0) { settled = true; return CLB_OK; }
+        if (pin[1].changed == 0) { settled = true; return CLB_OK; }
     }
     return CLB_OK;
 }
@@ -701,10 +740,7 @@ clb_status ca_step(clb_handle* h, int* sweeps_out, int* mask_changed) {
     // the host copy of the map follows the device only when a voxel changed (an unchanged mask sum
     // can hide changes that cancel, so the passes count changed voxels themselves)
     if (moved) {
-        cudaError_t e = cudaMemcpy(h->h_mat.data(), h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) return cuda_check(h, e, "mask copy");
-    }
-    if (moved) {
+        h->h_mat_stale = true;
         st = geometry_refresh(h);
         if (st != CLB_OK) return st;
     }

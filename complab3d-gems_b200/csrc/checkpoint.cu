@@ -1,10 +1,11 @@
 // checkpoint.cu -- restart files of a domain's lattices (the reference's .chk checkpoints:
 // saveBinaryBlock of the flow lattice, complab.cpp:2004, and of every substrate and biomass
 // lattice, :2292-2302; loadBinaryBlock at :1106-1108 and :2044-2055). One file per call holds the
-// flow lattice's incoming populations, and/or every species (mobile: incoming populations,
-// immobile: concentration), the biomass fields and the advection velocity, in FP64 (exact for
-// every storage precision), with the step counters; loading it into a handle set up on the same
-// material map continues the run exactly as the saved handle would.
+// flow lattice's incoming populations, and/or every species (mobile: incoming populations in the
+// storage's own convention, g_i - t_i for FP64 lattices and g_i for FP32 / FP16 ones; immobile:
+// concentration), the biomass fields and the advection velocity, in FP64 (exact for every storage
+// precision), with the step counters; loading it into a handle set up on the same material map and
+// precisions continues the run exactly as the saved handle would.
 //
 // The header records which species are mobile and the biofilm material codes, because a species'
 // block size follows from its mobility: a handle whose mobile set differs would otherwise read
@@ -24,7 +25,7 @@ using namespace clb;
 namespace {
 
 const char MAGIC[8] = {'C', 'L', 'B', 'C', 'K', 'P', 'T', '1'};
-constexpr int32_t VERSION = 2;
+constexpr int32_t VERSION = 3;
 
 struct Header {
     char magic[8];
@@ -76,6 +77,10 @@ clb_status clb_checkpoint_save(clb_handle* h, const char* path, int what) {
     hd.mobile_mask = (what & CLB_CKPT_TRANSPORT) ? mobile_mask(h) : 0;
     hd.n_microbes = h->d.n_microbes;
     for (int m = 0; m < h->d.n_microbes && m < CLB_MAX_MICROBES; ++m) hd.bio_codes[m] = h->d.bio_codes[m];
+    {
+        clb_status hs = host_mat_sync(h);
+        if (hs != CLB_OK) return hs;
+    }
     const std::string tmp = std::string(path) + ".tmp";
     std::FILE* f = std::fopen(tmp.c_str(), "wb");
     if (!f) return fail(h, CLB_INVALID_ARG, "cannot open " + tmp);
@@ -91,7 +96,7 @@ clb_status clb_checkpoint_save(clb_handle* h, const char* path, int what) {
         for (int s = 0; ok && s < h->S; ++s) {
             const bool mob = mobile(h, s);
             buf.resize((mob ? 7 : 1) * N);
-            st = clb_get_field(h, mob ? CLB_FIELD_ADE_POPULATIONS : CLB_FIELD_CONCENTRATION, s, buf.data(), 0);
+            st = mob ? ade_populations(h, s, buf.data(), 0) : clb_get_field(h, CLB_FIELD_CONCENTRATION, s, buf.data(), 0);
             ok = st == CLB_OK && put(f, buf.data(), sizeof(double) * buf.size());
         }
         for (int m = 0; ok && m < h->M; ++m) {
@@ -135,6 +140,7 @@ clb_status clb_checkpoint_load(clb_handle* h, const char* path) {
         return bad("not a checkpoint of this library version");
     if (hd.nx != h->g.nx || hd.ny != h->g.ny || hd.nz != h->g.nz) return bad("lattice size differs");
     if (!get(f, mat.data(), N)) return bad("truncated");
+    if (host_mat_sync(h) != CLB_OK) return bad("cannot read the handle's material map");
     if (std::memcmp(mat.data(), h->h_mat.data(), N) != 0) return bad("saved on a different material map");
     if (hd.n_microbes != h->d.n_microbes) return bad("biofilm materials differ");
     for (int m = 0; m < hd.n_microbes && m < CLB_MAX_MICROBES; ++m)
@@ -188,8 +194,7 @@ clb_status clb_checkpoint_load(clb_handle* h, const char* path) {
     if (hd.what & CLB_CKPT_TRANSPORT) {
         h->ade_iters = hd.ade_iters;
         for (int s = 0; s < h->S; ++s) {
-            st = mobile(h, s) ? clb_set_field(h, CLB_FIELD_ADE_POPULATIONS, s, spec[s].data(), 0)
-                              : ade_set_immobile(h, s, spec[s].data());
+            st = mobile(h, s) ? ade_set_populations(h, s, spec[s].data(), 0) : ade_set_immobile(h, s, spec[s].data());
             if (st != CLB_OK) { h->ade_iters = save_ade; return st; }
         }
         for (int m = 0; m < h->M; ++m)

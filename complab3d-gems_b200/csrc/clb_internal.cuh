@@ -292,7 +292,9 @@ struct clb_handle_s {
     long long ca_mask_sum = 0;
     double* d_ca_total = nullptr;     // [N] total biomass as the automaton tracks it
     int* d_ca_age = nullptr;          // [N] age wavefront
-    int* d_ca_age2 = nullptr;
+    int32_t* d_ca_blist = nullptr;    // [N] voxels whose total biomass exceeds 1e-14 (last mask pass)
+    bool h_mat_stale = false;         // the automaton changed the device map since h_mat was copied
+    void* h_ca_pin = nullptr;         // pinned host copies of the counters: [0] reset value, [1] read back, [2] scratch
     int8_t* d_ca_distp = nullptr;     // [N] 1 where the distance-from-wall field is positive
     int* d_ca_aidx = nullptr;         // [N] row of an active voxel in the sweep, -1
     int* d_ca_act = nullptr;          // [cap] active voxels of a sweep
@@ -308,6 +310,8 @@ struct clb_handle_s {
 namespace clb {
 // error helpers (api.cu)
 clb_status fail(clb_handle* h, clb_status s, const std::string& msg);
+// brings h_mat up to date with the device map after automaton passes changed it (api.cu)
+clb_status host_mat_sync(clb_handle* h);
 clb_status cuda_check(clb_handle* h, cudaError_t e, const char* what);
 
 // flow.cu
@@ -330,8 +334,10 @@ clb_status ade_couple(clb_handle* h);
 clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm, double dt);
 clb_status ade_set_biomass(clb_handle* h, int M, const double* b);
 clb_status ade_density(clb_handle* h, int s, double* host);
-clb_status ade_populations(clb_handle* h, int s, double* host);
-clb_status ade_set_populations(clb_handle* h, int s, const double* host);
+// shifted != 0: the C ABI's populations g_i - t_i; 0: the storage's own g_i - sigma t_i (exact round
+// trips for restart files)
+clb_status ade_populations(clb_handle* h, int s, double* host, int shifted = 1);
+clb_status ade_set_populations(clb_handle* h, int s, const double* host, int shifted = 1);
 clb_status ade_biomass(clb_handle* h, int m, double* host);
 clb_status ade_velocity(clb_handle* h, double* host);
 clb_status ade_set_velocity(clb_handle* h, const double* host);
@@ -360,9 +366,10 @@ clb_status batch_step(clb_batch* b, int n, int flow, int ade);
 clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len);
 clb_status batch_destroy(clb_batch* b);
 clb_status batch_counts(clb_batch* b, int64_t* flow_nodes, int64_t* ade_nodes);
-clb_status batch_schedule(clb_batch* b, int persistent, int tile, int lag, int steps_per_launch);
+clb_status batch_schedule(clb_batch* b, int persistent, int tile, int lag, int steps_per_launch, int ctas_per_sm);
 clb_status batch_set_stream(clb_batch* b, void* stream);
-clb_status batch_get_schedule(clb_batch* b, int* persistent, int* tile, int* lag, int* steps_per_launch);
+clb_status batch_get_schedule(clb_batch* b, int* persistent, int* tile, int* lag, int* steps_per_launch,
+                              int* ctas_per_sm);
 
 // biofilm_ca.cu
 clb_status ca_setup(clb_handle* h, const clb_ca_desc* d);

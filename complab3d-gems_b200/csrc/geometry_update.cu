@@ -230,6 +230,10 @@ static clb_status grow(clb_handle* h, void** p, size_t bytes, const char* what) 
 // host material map and the stamp field.
 clb_status geometry_refresh(clb_handle* h) {
     if (!h->ade_ready) return CLB_OK;
+    {
+        clb_status st = host_mat_sync(h);
+        if (st != CLB_OK) return st;
+    }
     const AdeParams& P = h->ap;
     const Geom G = h->g;
     const int64_t K = h->ade_sp.K;
@@ -362,6 +366,8 @@ clb_status precip_setup(clb_handle* h, const clb_precip_desc* d) {
             return fail(h, CLB_INVALID_ARG, "unknown dissolution law");
     }
     if (d->seal_flow) {
+        clb_status hs = host_mat_sync(h);
+        if (hs != CLB_OK) return hs;
         for (int64_t n = 0; n < h->g.N; ++n)
             if ((uint8_t)h->h_mat[n] == SEALED_FLOW_CODE)
                 return fail(h, CLB_INVALID_ARG, "seal_flow reserves material code 127");
@@ -463,6 +469,7 @@ clb_status geometry_update(clb_handle* h, int* sealed, int* reopened) {
     }
     e = cudaMemcpy(h->h_mat.data(), h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_check(h, e, "material copy");
+    h->h_mat_stale = false;
     clb_status st = geometry_refresh(h);
     if (st != CLB_OK) return st;
     if (h->prc.seal_flow && h->flow_ready) {

@@ -240,6 +240,10 @@ static unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, (n
 clb_status sparse_build(clb_handle* h, const int8_t* stored_by_code, int q, SparseBuffers& out,
                         const std::vector<int8_t>* map) {
     sparse_free(out);
+    if (!map) {
+        clb_status st = host_mat_sync(h);
+        if (st != CLB_OK) return st;
+    }
     const std::vector<int8_t>& mat = map ? *map : h->h_mat;
     const Geom& G = h->g;
     const int nx = G.nx, ny = G.ny, nz = G.nz;

@@ -130,6 +130,8 @@ clb_status clb_write_vti(clb_handle* h, int field, int index, const char* path) 
         const void* data[2] = {norm.data(), vel.data()};
         st = clb_vti_write(path, nx, ny, nz, 2, names, comps, types, data);
     } else if (field == CLB_FIELD_MATERIAL) {
+        st = host_mat_sync(h);
+        if (st != CLB_OK) return st;
         std::vector<float> tag(N);
         for (size_t n = 0; n < N; ++n) tag[n] = (float)h->h_mat[n];
         const char* names[1] = {"tag"};

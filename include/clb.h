@@ -486,11 +486,15 @@ clb_status clb_batch_step(clb_batch* batch, int n, int flow, int transport);
 clb_status clb_batch_autotune(clb_batch* batch, int steps, char* report, int report_len);
 
 /* Sets the schedule: persistent != 0 with `tile` nodes per item (a multiple of 256), a lag of
- * `lag` >= 1 domains between a domain's successive steps in the item table, and an even 2..8
- * steps per launch; persistent == 0: one launch per lattice and step (the other arguments are
- * ignored). The persistent schedule needs one storage type for flow and transport. */
-clb_status clb_batch_schedule(clb_batch* batch, int persistent, int tile, int lag, int steps_per_launch);
-clb_status clb_batch_get_schedule(clb_batch* batch, int* persistent, int* tile, int* lag, int* steps_per_launch);
+ * `lag` >= 1 domains between a domain's successive steps in the item table, an even 2..8 steps
+ * per launch, and registers budgeted for `ctas_per_sm` resident CTAs per SM (4 always; 6 and 8
+ * for FP32 / FP16 storage with up to 4 mobile species); persistent == 0: one launch per lattice
+ * and step (the other arguments are ignored). The persistent schedule needs one storage type for
+ * flow and transport. */
+clb_status clb_batch_schedule(clb_batch* batch, int persistent, int tile, int lag, int steps_per_launch,
+                              int ctas_per_sm);
+clb_status clb_batch_get_schedule(clb_batch* batch, int* persistent, int* tile, int* lag, int* steps_per_launch,
+                                  int* ctas_per_sm);
 
 /* Enqueue the batch's work on `stream` (a cudaStream_t; NULL: the batch's own stream). */
 clb_status clb_batch_set_stream(clb_batch* batch, void* stream);

@@ -85,7 +85,8 @@ def test_batch_rejects_mixed_parity(clb):
 @pytest.mark.parametrize("prec,sched", [
     ("F32", dict(persistent=False)),
     ("F32", dict(tile=256, lag=1, steps_per_launch=2)),
-    ("F32", dict(tile=1024, lag=3, steps_per_launch=8)),
+    ("F32", dict(tile=1024, lag=3, steps_per_launch=8, ctas_per_sm=8)),
+    ("F32", dict(tile=2048, lag=8, steps_per_launch=2, ctas_per_sm=6)),
     ("F64", dict(tile=512, lag=2, steps_per_launch=4)),
     ("F16S", dict(tile=4096, lag=100, steps_per_launch=6)),
 ])
@@ -117,7 +118,7 @@ def test_batch_schedule_rejects_bad_settings(clb):
     cfg = workloads.ensemble_uneven_packs(n_domains=2, seed=22, scale=0.5)
     B = build(clb, cfg, clb.F32)
     batch = clb.Batch(B)
-    for bad in (dict(tile=300), dict(lag=0), dict(steps_per_launch=3), dict(steps_per_launch=10)):
+    for bad in (dict(tile=300), dict(lag=0), dict(steps_per_launch=3), dict(steps_per_launch=10), dict(ctas_per_sm=5)):
         with pytest.raises(clb.ClbError):
             batch.schedule(**bad)
     batch.close()
