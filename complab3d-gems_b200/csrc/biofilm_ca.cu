@@ -40,6 +40,8 @@
 // lexicographic in-place sweeps. Counters cross to the host through pinned memory.
 #include "sparse.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -77,13 +79,9 @@ __device__ __forceinline__ long long ordered(double v) {
     long long i = __double_as_longlong(v);
     return i < 0 ? i ^ 0x7FFFFFFFFFFFFFFFLL : i;
 }
-static double unordered(long long i) {
-    if (i < 0) i ^= 0x7FFFFFFFFFFFFFFFLL;
-    double v;
-    std::memcpy(&v, &i, sizeof v);
-    return v;
-}
 
+// Counters and control state of the automaton in device memory. The pass counters are cleared
+// and read inside one step; the step results and the totals are what the host reads back.
 struct CaScalars {
     long long gmax;        // ordered bits of max(total)
     long long mask_sum;
@@ -92,8 +90,37 @@ struct CaScalars {
     unsigned int changed;  // ages changed by a sweep
     unsigned int overflow; // active voxels beyond the capacity
     unsigned int nonfinite; // biomass values that are NaN or infinite (mask pass)
-    unsigned int moved;     // voxels whose material the mask pass changed
+    unsigned int moved;     // voxels whose material the passes of the step changed
     unsigned int nbio;      // voxels in the biomass list the mask pass writes
+    int status;             // CA_OK, or why a step stopped (kept until the host reads it)
+    int fail_iter;          // the iteration whose step set `status`
+    int step_sweeps;        // push sweeps of the last step
+    int step_changed;       // 1: the last step changed the mask sum
+    unsigned int moved_any; // a step changed voxels since the host last looked
+    long long ca_mask_sum;  // the mask sum after the last step
+    unsigned long long sweep_counter;  // push sweeps since set-up: the random streams' sweep number
+    long long total_sweeps, total_changes;  // over all steps since set-up
+};
+
+enum : int { CA_OK = 0, CA_NONFINITE = 1, CA_STALL = 2, CA_AGE = 3, CA_SWEEPS = 4, CA_CAPACITY = 5, CA_ROUNDS = 6 };
+
+// the device buffers one step of the automaton works on
+struct CaBufs {
+    int8_t* mat;
+    int8_t* mask0;  // the mask before a pass (several pore codes), else null
+    double* bio;
+    double* total;
+    int* age;
+    const int8_t* distp;
+    int* aidx;
+    int* act;
+    int* done;
+    int* tgt;
+    double* amt;
+    double* own;
+    int32_t* blist;
+    int cap;
+    uint64_t seed;
 };
 
 // ------------------------------------------------------------------ set-up and mask update
@@ -122,10 +149,13 @@ __global__ void k_ca_init(const CaView C, const int8_t* __restrict__ mat, const 
 // pore neighbour found in `mask_before` (the mask as it stood before the pass).
 // Also lists the voxels whose total biomass exceeds 1e-14 afterwards (in no particular order): the
 // only voxels the age wavefront and the push can touch.
-__global__ void k_ca_mask_total(const CaView C, int8_t* __restrict__ mat, const int8_t* __restrict__ mask_before,
-                                const double* __restrict__ bio, double* __restrict__ total, int32_t* __restrict__ blist,
-                                CaScalars* sc) {
+__device__ void ca_mask_total(const CaView& C, const CaBufs& B, CaScalars* sc) {
     const Geom G = C.g;
+    int8_t* __restrict__ mat = B.mat;
+    const int8_t* __restrict__ mask_before = B.mask0;
+    const double* __restrict__ bio = B.bio;
+    double* __restrict__ total = B.total;
+    int32_t* __restrict__ blist = B.blist;
     long long best = LLONG_MIN, msum = 0;
     const int lane = threadIdx.x & 31;
     // whole warps run the loop together, so the list append below is warp-wide
@@ -198,10 +228,15 @@ __global__ void k_ca_mask_total(const CaView C, int8_t* __restrict__ mat, const 
 // ------------------------------------------------------------------ push sweep
 
 // the voxels of x = 1..nx-2 that push, from the biomass list (any voxel above the maximum is on it)
-__global__ void k_ca_collect(const CaView C, const int8_t* __restrict__ mat, const double* __restrict__ total,
-                             const int32_t* __restrict__ blist, int* __restrict__ aidx, int* __restrict__ act,
-                             int* __restrict__ done, int cap, CaScalars* sc) {
+__device__ void ca_collect(const CaView& C, const CaBufs& B, CaScalars* sc) {
     const Geom G = C.g;
+    const int8_t* __restrict__ mat = B.mat;
+    const double* __restrict__ total = B.total;
+    const int32_t* __restrict__ blist = B.blist;
+    int* __restrict__ aidx = B.aidx;
+    int* __restrict__ act = B.act;
+    int* __restrict__ done = B.done;
+    const int cap = B.cap;
     const int64_t lo = G.plane, hi = G.N - G.plane;  // x = 1..nx-2
     const int nb = (int)sc->nbio;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb; j += gridDim.x * blockDim.x) {
@@ -231,12 +266,19 @@ __device__ __forceinline__ void add_records(const CaView& C, int j, int64_t n, c
     }
 }
 
-__global__ void k_ca_round(const CaView C, const int8_t* __restrict__ mat, const double* __restrict__ total,
-                           const int* __restrict__ age, const double* __restrict__ bio, const int* __restrict__ aidx,
-                           const int* __restrict__ act, int* __restrict__ done, int* __restrict__ tgt,
-                           double* __restrict__ amt, double* __restrict__ own, int count, int round, uint64_t seed,
-                           uint64_t sweep, CaScalars* sc) {
+__device__ void ca_round(const CaView& C, const CaBufs& B, int count, int round, uint64_t sweep, CaScalars* sc) {
     const Geom G = C.g;
+    const int8_t* __restrict__ mat = B.mat;
+    const double* __restrict__ total = B.total;
+    const int* __restrict__ age = B.age;
+    const double* __restrict__ bio = B.bio;
+    const int* __restrict__ aidx = B.aidx;
+    const int* __restrict__ act = B.act;
+    int* __restrict__ done = B.done;
+    int* __restrict__ tgt = B.tgt;
+    double* __restrict__ amt = B.amt;
+    double* __restrict__ own = B.own;
+    const uint64_t seed = B.seed;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         if (done[i]) continue;
         const int64_t n = act[i];
@@ -337,9 +379,13 @@ __global__ void k_ca_round(const CaView C, const int8_t* __restrict__ mat, const
 }
 
 // every voxel takes the pushes it received, in the order the sequential sweep adds them
-__global__ void k_ca_apply(const CaView C, double* __restrict__ bio, const int* __restrict__ aidx,
-                           const int* __restrict__ tgt, const double* __restrict__ amt, const double* __restrict__ own) {
+__device__ void ca_apply(const CaView& C, const CaBufs& B) {
     const Geom G = C.g;
+    double* __restrict__ bio = B.bio;
+    const int* __restrict__ aidx = B.aidx;
+    const int* __restrict__ tgt = B.tgt;
+    const double* __restrict__ amt = B.amt;
+    const double* __restrict__ own = B.own;
     const int64_t lo = G.plane, hi = G.N - G.plane;
     for (int64_t n = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += (int64_t)gridDim.x * blockDim.x) {
         int x, y, z;
@@ -367,14 +413,14 @@ __global__ void k_ca_apply(const CaView C, double* __restrict__ bio, const int* 
     }
 }
 
-__global__ void k_ca_clear(int* __restrict__ aidx, const int* __restrict__ act, int count) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) aidx[act[i]] = -1;
+__device__ void ca_clear(const CaBufs& B, int count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) B.aidx[B.act[i]] = -1;
 }
 
 // ------------------------------------------------------------------ age wavefront
 
 // new age of voxel n from the ages it sees (updateAgeDistance3D); returns the old age when unchanged
-__device__ __forceinline__ int age_rule(const CaView& C, int64_t n, const int* __restrict__ age,
+__device__ __forceinline__ int age_rule(const CaView& C, int64_t n, const int* age,
                                         const int8_t* __restrict__ distp, const double* __restrict__ total) {
     const Geom G = C.g;
     const int a = age[n];
@@ -408,8 +454,11 @@ __device__ __forceinline__ int age_rule(const CaView& C, int64_t n, const int* _
 // sweep: both are iterates of the same monotone, inflationary rule, so the sweeps still reach the
 // least fixed point above the start, the one the reference's in-place sweeps reach, and a sweep
 // that changes nothing has read only final values.
-__global__ void k_age_relax(const CaView C, int* age, const int8_t* __restrict__ distp,
-                            const double* __restrict__ total, const int32_t* __restrict__ blist, CaScalars* sc) {
+__device__ void ca_age_relax(const CaView& C, const CaBufs& B, CaScalars* sc) {
+    int* age = B.age;
+    const int8_t* __restrict__ distp = B.distp;
+    const double* __restrict__ total = B.total;
+    const int32_t* __restrict__ blist = B.blist;
     unsigned int ch = 0;
     const int nb = (int)sc->nbio;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb; j += gridDim.x * blockDim.x) {
@@ -426,9 +475,11 @@ __global__ void k_age_relax(const CaView C, int* age, const int8_t* __restrict__
 }
 
 // voxels with x + y + z = level, in place
-__global__ void k_age_level(const CaView C, int* __restrict__ age, const int8_t* __restrict__ distp,
-                            const double* __restrict__ total, int level) {
+__device__ void ca_age_level(const CaView& C, const CaBufs& B, int level) {
     const Geom G = C.g;
+    int* age = B.age;
+    const int8_t* __restrict__ distp = B.distp;
+    const double* __restrict__ total = B.total;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)G.nx * G.ny;
          t += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(t / G.ny), y = (int)(t - (int64_t)x * G.ny);
@@ -439,11 +490,156 @@ __global__ void k_age_level(const CaView C, int* __restrict__ age, const int8_t*
     }
 }
 
+// ------------------------------------------------------------------ one step, on the device
+
+// the mask as it stands before a pass, for the reopening rule with several pore codes
+__device__ __forceinline__ void ca_snapshot_mask(const CaView& C, const CaBufs& B) {
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < C.g.N; n += (int64_t)gridDim.x * blockDim.x)
+        B.mask0[n] = B.mat[n];
+}
+
+__device__ __forceinline__ double unordered_dev(long long i) {
+    if (i < 0) i ^= 0x7FFFFFFFFFFFFFFFLL;
+    return __longlong_as_double(i);
+}
+
+// One step of the automaton (ca_step's sequence: mask pass; while max(total) exceeds Bmax, push
+// sweeps with their mask passes, the stall and sweep limits and, every 50 sweeps, the age
+// relaxation; the in-place age sweep after a mask change) in one cooperative launch, with grid-wide
+// barriers between the phases, so no phase waits for the host. Every block makes the same decisions
+// from values it reads after a barrier; a value is changed again only after a further barrier, so no
+// block can read a later value than another. Every loop is bounded: rounds by the active count
+// (each round finishes at least the lexicographically first unfinished voxel), sweeps by 1001, age
+// sweeps by 1001 per relaxation. A failure is recorded in `status` with the iteration and later
+// steps do nothing until the host has read it.
+__global__ void __launch_bounds__(CA_THREADS) k_ca_step(const CaView C, const CaBufs B, CaScalars* sc, int iter) {
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    // `status` is written only after the last barrier of a step, so every block reads the same value
+    if (sc->status != CA_OK) return;
+    if (lead) {
+        sc->gmax = LLONG_MIN;
+        sc->mask_sum = 0;
+        sc->nbio = 0;
+        sc->nonfinite = 0;
+        sc->moved = 0;
+    }
+    if (B.mask0) ca_snapshot_mask(C, B);
+    grid.sync();
+    ca_mask_total(C, B, sc);
+    grid.sync();
+    double gmax = unordered_dev(sc->gmax);
+    long long msum = sc->mask_sum;
+    int status = (sc->nonfinite || !isfinite(gmax)) ? CA_NONFINITE : CA_OK;
+    uint64_t sweep = sc->sweep_counter;
+    const long long mask_sum0 = sc->ca_mask_sum;
+    grid.sync();
+    int whilecount = 0, stall = 0;
+    double prev = gmax;
+    if (status == CA_OK && gmax - C.bmax > THRD) {
+        while (gmax - C.bmax > THRD) {
+            // ---- push sweep: the voxels above the maximum, their rounds, the pushes applied
+            if (lead) {
+                sc->active = 0;
+                sc->overflow = 0;
+            }
+            grid.sync();
+            ca_collect(C, B, sc);
+            grid.sync();
+            const int count = (int)sc->active;
+            const bool over = sc->overflow != 0;
+            grid.sync();
+            if (over) { status = CA_CAPACITY; break; }
+            if (count > 0) {
+                if (lead) sc->remaining = (unsigned int)count;
+                grid.sync();
+                for (int round = 1;; ++round) {
+                    ca_round(C, B, count, round, sweep, sc);
+                    grid.sync();
+                    const unsigned int rem = sc->remaining;
+                    grid.sync();
+                    if (rem == 0) break;
+                    if (round >= count) { status = CA_ROUNDS; break; }
+                }
+                if (status != CA_OK) break;
+                ca_apply(C, B);
+                grid.sync();
+                ca_clear(B, count);
+            }
+            ++sweep;
+            // ---- mask pass after the sweep
+            if (lead) {
+                sc->gmax = LLONG_MIN;
+                sc->mask_sum = 0;
+                sc->nbio = 0;
+                sc->nonfinite = 0;
+            }
+            if (B.mask0) ca_snapshot_mask(C, B);
+            grid.sync();
+            ca_mask_total(C, B, sc);
+            grid.sync();
+            gmax = unordered_dev(sc->gmax);
+            msum = sc->mask_sum;
+            const bool nonf = sc->nonfinite != 0;
+            grid.sync();
+            if (nonf || !isfinite(gmax)) { status = CA_NONFINITE; break; }
+            if (gmax > prev - THRD) {
+                if (++stall >= 100) { status = CA_STALL; break; }
+            } else {
+                stall = 0;
+            }
+            prev = gmax;
+            if (whilecount % 50 == 0) {
+                bool settled = false;
+                for (int k = 0; k < 1001 && !settled; ++k) {
+                    if (lead) sc->changed = 0;
+                    grid.sync();
+                    ca_age_relax(C, B, sc);
+                    grid.sync();
+                    settled = sc->changed == 0;
+                    grid.sync();
+                }
+                if (!settled) { status = CA_AGE; break; }
+            }
+            if (whilecount > 1000) { status = CA_SWEEPS; break; }
+            ++whilecount;
+        }
+    }
+    bool changed = false;
+    if (status != CA_NONFINITE) {
+        // after the block, a changed mask takes one in-place age sweep (wavefronts over x + y + z)
+        changed = msum != mask_sum0;
+        if (changed) {
+            const int levels = C.g.nx + C.g.ny + C.g.nz - 2;
+            for (int l = 0; l < levels; ++l) {
+                ca_age_level(C, B, l);
+                grid.sync();
+            }
+        }
+    }
+    if (lead) {
+        sc->step_sweeps = whilecount;
+        sc->step_changed = changed ? 1 : 0;
+        if (changed) sc->ca_mask_sum = msum;
+        sc->sweep_counter = sweep;
+        sc->total_sweeps += whilecount;
+        sc->total_changes += changed ? 1 : 0;
+        if (sc->moved) sc->moved_any = 1;
+        if (status != CA_OK) {
+            sc->status = status;
+            sc->fail_iter = iter;
+        }
+    }
+}
+
 // ------------------------------------------------------------------ dynamics refresh
 
 // updateSoluteDynamics3D: open voxels take the pore or the biofilm dynamics from the mask
+// guard: when given, the pass acts only if the automaton's last step changed the mask
 __global__ void k_refresh_species(int8_t* __restrict__ code, const int32_t* __restrict__ node, int64_t K,
-                                  const int8_t* __restrict__ mat, const CaView C, int bio0) {
+                                  const int8_t* __restrict__ mat, const CaView C, int bio0, const int* guard) {
+    if (guard && *guard == 0) return;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
         const int m = mat[node[k]];
         if (!ca_open(C, m)) continue;
@@ -553,7 +749,16 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_sc, sizeof(CaScalars));
     if (e == cudaSuccess && h->d.n_pore_codes > 1) e = cudaMalloc(&h->d_ca_mask0, N);
     if (e != cudaSuccess) return cuda_check(h, e, "cellular automaton fields");
-    clb_status st = ca_reserve(h, (int)std::max<size_t>(4096, N / 64));
+    // room for every voxel that can push (open voxels of x = 1..nx-2), so a sweep never overflows
+    int open_inner = 0;
+    {
+        clb_status hs = host_mat_sync(h);
+        if (hs != CLB_OK) return hs;
+        const CaView C0 = ca_view(h);
+        auto open_code = [&](int m) { return m != C0.bb && m != C0.solid; };  // ca_open
+        for (int64_t n = h->g.plane; n < h->g.N - h->g.plane; ++n) open_inner += open_code(h->h_mat[n]) ? 1 : 0;
+    }
+    clb_status st = ca_reserve(h, std::max(1024, open_inner));
     if (st != CLB_OK) return st;
     if (!h->d_mat_flow) {
         // from now on the mask moves with the automaton; the flow keeps its own map until a refresh
@@ -575,11 +780,17 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
     const CaView C = ca_view(h);
     k_ca_init<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_bio, h->d_ca_total, h->d_ca_age,
                                                              h->d_ca_distp, h->d_ca_aidx, SC(h));
+    // the mask sum the steps compare against
+    cudaMemcpyAsync(&SC(h)->ca_mask_sum, &SC(h)->mask_sum, sizeof(long long), cudaMemcpyDeviceToDevice, h->stream);
     CaScalars s;
     e = cudaMemcpyAsync(&s, SC(h), sizeof s, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_check(h, e, "cellular automaton set-up");
     h->ca_mask_sum = s.mask_sum;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_ca_step, CA_THREADS, 0);
+    if (e != cudaSuccess || per_sm < 1) return cuda_check(h, e == cudaSuccess ? cudaErrorLaunchOutOfResources : e, "automaton step");
+    h->ca_grid = h->num_sms * std::min(per_sm, 2);
     h->ca_ready = true;
     return CLB_OK;
 }
@@ -593,160 +804,74 @@ static clb_status ca_scalars(clb_handle* h, CaScalars& s) {
 }
 
 // mask / total pass; returns max(total) and the mask sum
-static clb_status ca_mask_pass(clb_handle* h, const CaView& C, double& gmax, long long& msum, unsigned int* moved) {
-    // non-finite biomass stops the run cleanly, as the reference does after this pass
-    // (complab.cpp:2794-2796)
-    CaScalars s;
-    cudaMemcpyAsync(SC(h), h->h_ca_pin, sizeof s, cudaMemcpyHostToDevice, h->stream);  // pinned: no staging
-    if (h->d_ca_mask0) cudaMemcpyAsync(h->d_ca_mask0, h->d_mat, (size_t)h->g.N, cudaMemcpyDeviceToDevice, h->stream);
+static CaBufs ca_bufs(clb_handle* h) {
+    CaBufs B;
+    B.mat = h->d_mat;
+    B.mask0 = h->d_ca_mask0;
+    B.bio = h->d_bio;
+    B.total = h->d_ca_total;
+    B.age = h->d_ca_age;
+    B.distp = h->d_ca_distp;
+    B.aidx = h->d_ca_aidx;
+    B.act = h->d_ca_act;
+    B.done = h->d_ca_done;
+    B.tgt = h->d_ca_tgt;
+    B.amt = h->d_ca_amt;
+    B.own = h->d_ca_own;
+    B.blist = h->d_ca_blist;
+    B.cap = h->ca_cap;
+    B.seed = h->ca_seed;
+    return B;
+}
+
+// Enqueues one step of the automaton (k_ca_step); `iter` is the iteration a failure is recorded with.
+clb_status ca_step_async(clb_handle* h, int64_t iter) {
+    if (!h->ca_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ca_setup first");
+    CaView C = ca_view(h);
+    CaBufs B = ca_bufs(h);
+    CaScalars* sc = SC(h);
+    int it = (int)std::min<int64_t>(iter, INT32_MAX);
+    void* args[] = {&C, &B, &sc, &it};
     ++h->launches;
-    k_ca_mask_total<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_ca_mask0, h->d_bio,
-                                                                   h->d_ca_total, h->d_ca_blist, SC(h));
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_ca_step, dim3(h->ca_grid), dim3(CA_THREADS), args, 0,
+                                                h->stream);
+    return cuda_check(h, e, "automaton step");
+}
+
+// Reads the automaton's results back (synchronises): the last step's sweeps and mask change, the
+// totals, and a failure a step recorded (cleared once read, so the handle can step again).
+clb_status ca_read(clb_handle* h, int* step_sweeps, int* step_changed, int64_t* total_sweeps, int64_t* total_changes) {
+    CaScalars s;
     clb_status st = ca_scalars(h, s);
     if (st != CLB_OK) return st;
-    gmax = unordered(s.gmax);
-    msum = s.mask_sum;
-    if (moved) *moved += s.moved;
-    if (s.nonfinite || !std::isfinite(gmax))
-        return fail(h, CLB_NONFINITE, "non-finite biomass (NaN or Inf) in the biofilm fields");
-    return CLB_OK;
-}
-
-static clb_status ca_push_sweep(clb_handle* h, const CaView& C) {
-    const int grid = h->num_sms * 8;
-    for (;;) {
-        CaScalars s;
-        // active, remaining, changed, overflow to zero; the mask pass's results (the biomass list) stay
-        cudaMemsetAsync(&SC(h)->active, 0, 4 * sizeof(unsigned int), h->stream);
-        h->launches += 1;
-        k_ca_collect<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_ca_total, h->d_ca_blist, h->d_ca_aidx,
-                                                         h->d_ca_act, h->d_ca_done, h->ca_cap, SC(h));
-        clb_status st = ca_scalars(h, s);
-        if (st != CLB_OK) return st;
-        const int count = (int)std::min<unsigned int>(s.active, (unsigned int)h->ca_cap);
-        if (s.overflow) {
-            ++h->launches;
-            k_ca_clear<<<grid, CA_THREADS, 0, h->stream>>>(h->d_ca_aidx, h->d_ca_act, count);
-            st = ca_reserve(h, (int)s.active * 2);
-            if (st != CLB_OK) return st;
-            continue;
-        }
-        if (count == 0) { ++h->ca_sweeps; return CLB_OK; }
-        CaScalars* pin = static_cast<CaScalars*>(h->h_ca_pin);
-        pin[2].remaining = (unsigned int)count;  // pinned scratch: untouched until the next synchronisation
-        cudaMemcpyAsync(&SC(h)->remaining, &pin[2].remaining, sizeof(unsigned int), cudaMemcpyHostToDevice, h->stream);
-        // every round completes at least the lexicographically first unfinished voxel, so `count`
-        // rounds always suffice. Rounds go out in batches and the host reads the remaining count once
-        // per batch: a round after the last voxel finished finds every voxel done and changes nothing,
-        // so the batching leaves the result bit for bit the same.
-        constexpr int ROUND_BATCH = 16;
-        for (int round = 1; round <= count; round += ROUND_BATCH) {
-            const int last = std::min(count, round + ROUND_BATCH - 1);
-            for (int r = round; r <= last; ++r) {
-                ++h->launches;
-                k_ca_round<<<(count + CA_THREADS - 1) / CA_THREADS, CA_THREADS, 0, h->stream>>>(
-                    C, h->d_mat, h->d_ca_total, h->d_ca_age, h->d_bio, h->d_ca_aidx, h->d_ca_act, h->d_ca_done,
-                    h->d_ca_tgt, h->d_ca_amt, h->d_ca_own, count, r, h->ca_seed, h->ca_sweeps, SC(h));
-            }
-            unsigned int rem = 0;
-            cudaError_t e = cudaMemcpyAsync(&rem, &SC(h)->remaining, sizeof rem, cudaMemcpyDeviceToHost, h->stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-            if (e != cudaSuccess) return cuda_check(h, e, "push round");
-            if (rem == 0) break;
-        }
-        h->launches += 2;  // apply + clear
-        k_ca_apply<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_bio, h->d_ca_aidx, h->d_ca_tgt, h->d_ca_amt, h->d_ca_own);
-        k_ca_clear<<<grid, CA_THREADS, 0, h->stream>>>(h->d_ca_aidx, h->d_ca_act, count);
-        ++h->ca_sweeps;
-        return cuda_check(h, cudaGetLastError(), "push sweep");
+    if (step_sweeps) *step_sweeps = s.step_sweeps;
+    if (step_changed) *step_changed = s.step_changed;
+    if (total_sweeps) *total_sweeps = s.total_sweeps;
+    if (total_changes) *total_changes = s.total_changes;
+    h->ca_sweeps = s.sweep_counter;
+    if (s.moved_any) {
+        cudaMemsetAsync(&SC(h)->moved_any, 0, sizeof(unsigned int), h->stream);
+        h->h_mat_stale = true;
+        if ((st = geometry_refresh(h)) != CLB_OK) return st;
+    }
+    if (s.status == CA_OK) return CLB_OK;
+    cudaMemsetAsync(&SC(h)->status, 0, sizeof(int), h->stream);
+    const std::string at = " (iteration " + std::to_string(s.fail_iter) + ")";
+    switch (s.status) {
+        case CA_NONFINITE: return fail(h, CLB_NONFINITE, "non-finite biomass (NaN or Inf) in the biofilm fields" + at);
+        case CA_STALL: return fail(h, CLB_NOT_CONVERGED, "biofilm push stalled: excess biomass cannot spread" + at);
+        case CA_AGE: return fail(h, CLB_NOT_CONVERGED, "age relaxation did not settle in 1000 sweeps" + at);
+        case CA_SWEEPS: return fail(h, CLB_NOT_CONVERGED, "biofilm push did not settle in 1000 sweeps" + at);
+        default: return fail(h, CLB_CUDA_ERROR, "automaton step: active voxels beyond the sweep's bounds" + at);
     }
 }
 
-// Relaxation sweeps of the age field (in place, over the biomass list) until one changes nothing,
-// at most 1001 sweeps (the reference's limit of 1000 after the first). Sweeps go out in batches; the
-// change counter is cleared before the last sweep of a batch and read after it. A sweep of a settled
-// field changes nothing, so a batch that continues past the settling sweep leaves the same field.
-// The unordered in-place sweeps settle in no more sweeps than Jacobi sweeps would, and every
-// ordering reaches the same fixed point, so the field is the reference's; only how close a field
-// that never settles comes to the limit may differ.
-static clb_status ca_age_converge(clb_handle* h, const CaView& C, bool& settled) {
-    settled = false;
-    constexpr int SWEEP_BATCH = 8, MAX_SWEEPS = 1001;
-    int done = 0;
-    CaScalars* pin = static_cast<CaScalars*>(h->h_ca_pin);
-    while (done < MAX_SWEEPS) {
-        const int b = std::min(SWEEP_BATCH, MAX_SWEEPS - done);
-        for (int k = 0; k < b; ++k) {
-            if (k == b - 1) cudaMemsetAsync(&SC(h)->changed, 0, sizeof(unsigned int), h->stream);
-            ++h->launches;
-            k_age_relax<<<h->num_sms * 4, CA_THREADS, 0, h->stream>>>(C, h->d_ca_age, h->d_ca_distp, h->d_ca_total,
-                                                                       h->d_ca_blist, SC(h));
-        }
-        done += b;
-        cudaError_t e = cudaMemcpyAsync(&pin[1].changed, &SC(h)->changed, sizeof(unsigned int), cudaMemcpyDeviceToHost,
-                                        h->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-        if (e != cudaSuccess) return cuda_check(h, e, "age relaxation");
-        if (pin[1].changed == 0) { settled = true; return CLB_OK; }
-    }
-    return CLB_OK;
-}
-
-static void ca_age_sweep_inplace(clb_handle* h, const CaView& C) {
-    const int levels = h->g.nx + h->g.ny + h->g.nz - 2;
-    const int64_t cols = (int64_t)h->g.nx * h->g.ny;
-    const int grid = (int)std::min<int64_t>((cols + CA_THREADS - 1) / CA_THREADS, h->num_sms * 8);
-    h->launches += levels;
-    for (int l = 0; l < levels; ++l)
-        k_age_level<<<grid, CA_THREADS, 0, h->stream>>>(C, h->d_ca_age, h->d_ca_distp, h->d_ca_total, l);
-}
-
+// One step of the automaton, synchronously (clb_ca_step): the results are read back at once.
 clb_status ca_step(clb_handle* h, int* sweeps_out, int* mask_changed) {
     if (!h->ca_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ca_setup first");
-    const CaView C = ca_view(h);
-    double gmax;
-    long long msum;
-    unsigned int moved = 0;  // voxels the mask passes of this call changed
-    clb_status st = ca_mask_pass(h, C, gmax, msum, &moved);
-    if (st != CLB_OK) return st;
-    int whilecount = 0;
-    clb_status rc = CLB_OK;
-    if (gmax - h->ca_bmax > THRD) {
-        double prev = gmax;
-        int stall = 0;
-        while (gmax - h->ca_bmax > THRD) {
-            if ((st = ca_push_sweep(h, C)) != CLB_OK) return st;
-            if ((st = ca_mask_pass(h, C, gmax, msum, &moved)) != CLB_OK) return st;
-            if (gmax > prev - THRD) {
-                if (++stall >= 100) { rc = fail(h, CLB_NOT_CONVERGED, "biofilm push stalled: excess biomass cannot spread"); break; }
-            } else {
-                stall = 0;
-            }
-            prev = gmax;
-            if (whilecount % 50 == 0) {
-                bool settled;
-                if ((st = ca_age_converge(h, C, settled)) != CLB_OK) return st;
-                if (!settled) { rc = fail(h, CLB_NOT_CONVERGED, "age relaxation did not settle in 1000 sweeps"); break; }
-            }
-            if (whilecount > 1000) { rc = fail(h, CLB_NOT_CONVERGED, "biofilm push did not settle in 1000 sweeps"); break; }
-            ++whilecount;
-        }
-    }
-    const bool changed = msum != h->ca_mask_sum;
-    if (changed) {
-        h->ca_mask_sum = msum;
-        ca_age_sweep_inplace(h, C);
-    }
-    // the host copy of the map follows the device only when a voxel changed (an unchanged mask sum
-    // can hide changes that cancel, so the passes count changed voxels themselves)
-    if (moved) {
-        h->h_mat_stale = true;
-        st = geometry_refresh(h);
-        if (st != CLB_OK) return st;
-    }
-    if (sweeps_out) *sweeps_out = whilecount;
-    if (mask_changed) *mask_changed = changed ? 1 : 0;
-    return rc;
+    clb_status st = ca_step_async(h, h->ade_iters);
+    if (st == CLB_OK) st = ca_read(h, sweeps_out, mask_changed, nullptr, nullptr);
+    return st;
 }
 
 clb_status refresh_dynamics(clb_handle* h, int species, int flow) {
@@ -756,7 +881,7 @@ clb_status refresh_dynamics(clb_handle* h, int species, int flow) {
     if (species && h->ade_ready) ++h->launches;
     if (species && h->ade_ready)
         k_refresh_species<<<grid, CA_THREADS, 0, h->stream>>>(h->ade_sp.code, h->ade_sp.node, h->ade_sp.K, h->d_mat, C,
-                                                              bio0);
+                                                              bio0, nullptr);
     if (flow && h->flow_ready) {
         const int64_t N = h->g.N;
         cudaError_t e = cudaSuccess;
@@ -778,6 +903,16 @@ clb_status refresh_dynamics(clb_handle* h, int species, int flow) {
         for (int64_t n = 0; n < N; ++n) nbgk += h->fp.dyn[(uint8_t)h->h_mat_flow[n] & 127] == DYN_BGK;
         h->fp.n_bgk = nbgk;
     }
+    return cuda_check(h, cudaGetLastError(), "dynamics refresh");
+}
+
+// updateSoluteDynamics3D enqueued after an automaton step, acting only if that step changed the mask
+clb_status refresh_species_if_changed(clb_handle* h) {
+    const CaView C = ca_view(h);
+    const int bio0 = h->d.n_microbes > 0 ? h->d.bio_codes[0] : -1;
+    ++h->launches;
+    k_refresh_species<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(h->ade_sp.code, h->ade_sp.node, h->ade_sp.K,
+                                                                     h->d_mat, C, bio0, &SC(h)->step_changed);
     return cuda_check(h, cudaGetLastError(), "dynamics refresh");
 }
 

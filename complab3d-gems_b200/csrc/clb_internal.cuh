@@ -305,6 +305,7 @@ struct clb_handle_s {
     void* d_ca_sc = nullptr;          // device counters of the automaton
     int8_t* d_ca_mask0 = nullptr;     // mask before a pass (several pore codes)
     int ca_cap = 0;
+    int ca_grid = 0;                  // blocks of the cooperative automaton step (all resident)
 };
 
 namespace clb {
@@ -374,6 +375,10 @@ clb_status batch_get_schedule(clb_batch* b, int* persistent, int* tile, int* lag
 // biofilm_ca.cu
 clb_status ca_setup(clb_handle* h, const clb_ca_desc* d);
 clb_status ca_step(clb_handle* h, int* sweeps, int* mask_changed);
+// the step enqueued only, and the results read back later (clb_run's loop)
+clb_status ca_step_async(clb_handle* h, int64_t iter);
+clb_status ca_read(clb_handle* h, int* step_sweeps, int* step_changed, int64_t* total_sweeps, int64_t* total_changes);
+clb_status refresh_species_if_changed(clb_handle* h);
 clb_status refresh_dynamics(clb_handle* h, int species, int flow);
 clb_status ca_fields(clb_handle* h, int which, double* host);
 void ca_free(clb_handle* h);

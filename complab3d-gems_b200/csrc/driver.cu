@@ -113,6 +113,30 @@ clb_status run(clb_handle* h, const clb_run_desc* d, clb_run_report* r) {
     PhaseTimer tt(h->stream), tc(h->stream), tf(h->stream), tg(h->stream);
     bool moved_since_resolve = false;
     clb_status st = CLB_OK;
+    // The automaton's steps run on the device without the host in the loop unless a schedule needs
+    // each step's outcome on the host at once (a re-solve on a mask change, abiotic laws whose lists
+    // follow the map): the dynamics refresh after a mask change is enqueued every update interval
+    // and acts only when the step changed the mask, and the results (failures, counts) are read
+    // back every POLL iterations, at each re-solve and at the end.
+    const bool ca_async = d->ca && d->ns_update_interval == 0 && h->ap.law2 == CLB_LAW_NONE && !h->ap.dis_on;
+    constexpr int POLL = 64;
+    int64_t ca_sweeps0 = 0, ca_changes0 = 0, ca_changes_at_resolve = 0;
+    if (ca_async) {
+        st = ca_read(h, nullptr, nullptr, &ca_sweeps0, &ca_changes0);
+        ca_changes_at_resolve = ca_changes0;
+    }
+    auto ca_poll = [&](bool for_resolve) {
+        int64_t sw = 0, ch = 0;
+        clb_status ps = ca_read(h, nullptr, nullptr, &sw, &ch);
+        r->ca_sweeps = (int)(sw - ca_sweeps0);
+        r->mask_changes = (int)(ch - ca_changes0);
+        if (for_resolve) {
+            if (ch != ca_changes_at_resolve) moved_since_resolve = true;
+            ca_changes_at_resolve = ch;
+        }
+        if (ps == CLB_OK) ps = ade_nonfinite_check(h);
+        return ps;
+    };
     for (int k = 0; k < d->iterations && st == CLB_OK; ++k) {
         const int64_t iT = h->ade_iters;  // the reference's iteration counter at this step
         tt.start();
@@ -120,7 +144,15 @@ clb_status run(clb_handle* h, const clb_run_desc* d, clb_run_report* r) {
         tt.stop();
         if (st != CLB_OK) break;
         r->iterations += 1;
-        if (d->ca) {
+        if (ca_async) {
+            tc.start();
+            st = ca_step_async(h, iT);
+            if (st == CLB_OK && d->ade_update_interval > 0 && iT % d->ade_update_interval == 0)
+                st = refresh_species_if_changed(h);  // updateSoluteDynamics3D after a mask change
+            tc.stop();
+            if (st != CLB_OK) break;
+            if ((k + 1) % POLL == 0 && (st = ca_poll(false)) != CLB_OK) break;
+        } else if (d->ca) {
             int sweeps = 0, changed = 0;
             tc.start();
             st = ca_step(h, &sweeps, &changed);  // synchronises: its mask pass reads counters back
@@ -145,6 +177,7 @@ clb_status run(clb_handle* h, const clb_run_desc* d, clb_run_report* r) {
             }
         }
         if (d->resolve_every > 0 && (iT + 1) % d->resolve_every == 0) {
+            if (ca_async && (st = ca_poll(true)) != CLB_OK) break;
             if ((st = ade_nonfinite_check(h)) != CLB_OK) break;
             st = resolve_flow(h, d, moved_since_resolve, r, tf);
             moved_since_resolve = false;
@@ -168,6 +201,10 @@ clb_status run(clb_handle* h, const clb_run_desc* d, clb_run_report* r) {
     tc.stop();
     tg.stop();
     tf.stop();
+    if (ca_async) {
+        const clb_status ps = ca_poll(false);
+        if (st == CLB_OK) st = ps;
+    }
     const cudaError_t e = cudaStreamSynchronize(h->stream);
     r->ms_transport = tt.total();
     r->ms_ca = tc.total();
