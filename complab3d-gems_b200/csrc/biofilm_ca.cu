@@ -149,69 +149,116 @@ __global__ void k_ca_init(const CaView C, const int8_t* __restrict__ mat, const 
 // pore neighbour found in `mask_before` (the mask as it stood before the pass).
 // Also lists the voxels whose total biomass exceeds 1e-14 afterwards (in no particular order): the
 // only voxels the age wavefront and the push can touch.
+// One voxel of the pass, from its loaded material, previous total and biomass; returns whether it
+// goes on the biomass list.
+__device__ __forceinline__ bool ca_mask_voxel(const CaView& C, const CaBufs& B, CaScalars* sc, int64_t n, int mk,
+                                              double told, const double* bm, long long& best, long long& msum) {
+    const Geom G = C.g;
+    double tn = told;
+    if (ca_open(C, mk)) {
+        double bmass = 0.0;
+        int newmask = 0;
+        for (int m = 0; m < C.M; ++m) {
+            if (!isfinite(bm[m])) atomicAdd(&sc->nonfinite, 1u);  // the run stops (complab.cpp:2796)
+            if (bm[m] > 1e-14) {
+                bmass += bm[m];
+                newmask += C.bio_code[m];
+            }
+        }
+        if (fabs(bmass - told) > 1e-14) {
+            B.total[n] = bmass;
+            tn = bmass;
+        }
+        const bool poreflag = ca_pore(C, mk);
+        int out = mk;
+        if (!poreflag && bmass < C.thr) {
+            out = C.pore[0];
+            if (C.n_pore > 1) {
+                int x, y, z;
+                decode(G, n, x, y, z);
+                const int d6[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+                for (int d = 0; d < 6; ++d) {
+                    const int X = x + d6[d][0], Y = y + d6[d][1], Z = z + d6[d][2];
+                    if (X < 0 || Y < 0 || Z < 0 || X >= G.nx || Y >= G.ny || Z >= G.nz) continue;
+                    const int nm = B.mask0[(int64_t)X * G.plane + (int64_t)Y * G.nz + Z];
+                    if (ca_open(C, nm) && ca_pore(C, nm)) { out = nm; break; }
+                }
+            }
+        } else if (poreflag && bmass >= C.thr && newmask > 0) {
+            out = newmask;
+        }
+        if (out != mk) {
+            B.mat[n] = (int8_t)out;
+            atomicAdd(&sc->moved, 1u);
+        }
+        msum += out;
+    } else {
+        msum += mk;
+    }
+    best = max(best, ordered(tn));
+    return tn > 1e-14;
+}
+
+// appends n (where `listed`) to the biomass list, one atomic per warp; the whole warp calls it
+__device__ __forceinline__ void ca_list_append(const CaBufs& B, CaScalars* sc, int64_t n, bool listed) {
+    const int lane = threadIdx.x & 31;
+    const unsigned int bal = __ballot_sync(0xffffffffu, listed);
+    if (!bal) return;
+    unsigned int base = 0;
+    if (lane == 0) base = atomicAdd(&sc->nbio, (unsigned int)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (listed) B.blist[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)n;
+}
+
+// updateLocalMaskNtotalLattices3D over every voxel. Each thread takes UNR voxels a grid stride
+// apart per round and issues their loads together, so the pass is not bound by one voxel's latency.
 __device__ void ca_mask_total(const CaView& C, const CaBufs& B, CaScalars* sc) {
     const Geom G = C.g;
-    int8_t* __restrict__ mat = B.mat;
-    const int8_t* __restrict__ mask_before = B.mask0;
-    const double* __restrict__ bio = B.bio;
-    double* __restrict__ total = B.total;
-    int32_t* __restrict__ blist = B.blist;
     long long best = LLONG_MIN, msum = 0;
-    const int lane = threadIdx.x & 31;
-    // whole warps run the loop together, so the list append below is warp-wide
+    constexpr int UNR = 4;
+    const int64_t S = (int64_t)gridDim.x * blockDim.x;
+    // whole warps run the loop together, so the list append is warp-wide
     const int64_t span = (G.N + 31) / 32 * 32;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < span; n += (int64_t)gridDim.x * blockDim.x) {
-        bool listed = false;
-        if (n < G.N) {
-        const int mk = mat[n];
-        if (ca_open(C, mk)) {
-            double bmass = 0.0;
-            int newmask = 0;
-            for (int m = 0; m < C.M; ++m) {
-                const double bm = bio[(int64_t)m * G.N + n];
-                if (!isfinite(bm)) atomicAdd(&sc->nonfinite, 1u);  // the run stops (complab.cpp:2796)
-                if (bm > 1e-14) {
-                    bmass += bm;
-                    newmask += C.bio_code[m];
+    if (C.M <= 2) {
+        for (int64_t n0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n0 < span; n0 += UNR * S) {
+            int mk[UNR];
+            double told[UNR], b0[UNR], b1[UNR];
+#pragma unroll
+            for (int j = 0; j < UNR; ++j) {
+                const int64_t n = n0 + j * S;
+                const bool in = n < G.N;
+                mk[j] = in ? (int)B.mat[n] : C.bb;
+                told[j] = in ? B.total[n] : 0.0;
+            }
+            // biomass only where the voxel is open (most voxels of a pack are not)
+#pragma unroll
+            for (int j = 0; j < UNR; ++j) {
+                const int64_t n = n0 + j * S;
+                const bool op = n < G.N && ca_open(C, mk[j]);
+                b0[j] = op ? B.bio[n] : 0.0;
+                b1[j] = (op && C.M > 1) ? B.bio[G.N + n] : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < UNR; ++j) {
+                const int64_t n = n0 + j * S;
+                if (n >= span) break;  // uniform per warp: span and S are multiples of 32
+                bool listed = false;
+                if (n < G.N) {
+                    const double bm[2] = {b0[j], b1[j]};
+                    listed = ca_mask_voxel(C, B, sc, n, mk[j], told[j], bm, best, msum);
                 }
+                ca_list_append(B, sc, n, listed);
             }
-            if (fabs(bmass - total[n]) > 1e-14) total[n] = bmass;
-            const bool poreflag = ca_pore(C, mk);
-            int out = mk;
-            if (!poreflag && bmass < C.thr) {
-                out = C.pore[0];
-                if (C.n_pore > 1) {
-                    int x, y, z;
-                    decode(G, n, x, y, z);
-                    const int d6[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-                    for (int d = 0; d < 6; ++d) {
-                        const int X = x + d6[d][0], Y = y + d6[d][1], Z = z + d6[d][2];
-                        if (X < 0 || Y < 0 || Z < 0 || X >= G.nx || Y >= G.ny || Z >= G.nz) continue;
-                        const int nm = mask_before[(int64_t)X * G.plane + (int64_t)Y * G.nz + Z];
-                        if (ca_open(C, nm) && ca_pore(C, nm)) { out = nm; break; }
-                    }
-                }
-            } else if (poreflag && bmass >= C.thr && newmask > 0) {
-                out = newmask;
-            }
-            if (out != mk) {
-                mat[n] = (int8_t)out;
-                atomicAdd(&sc->moved, 1u);
-            }
-            msum += out;
-        } else {
-            msum += mk;
         }
-        const double tn = total[n];
-        best = max(best, ordered(tn));
-        listed = tn > 1e-14;
-        }
-        const unsigned int bal = __ballot_sync(0xffffffffu, listed);
-        if (bal) {
-            unsigned int base = 0;
-            if (lane == 0) base = atomicAdd(&sc->nbio, (unsigned int)__popc(bal));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (listed) blist[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)n;
+    } else {
+        for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < span; n += S) {
+            bool listed = false;
+            if (n < G.N) {
+                double bm[CLB_MAX_MICROBES];
+                for (int m = 0; m < C.M; ++m) bm[m] = B.bio[(int64_t)m * G.N + n];
+                listed = ca_mask_voxel(C, B, sc, n, B.mat[n], B.total[n], bm, best, msum);
+            }
+            ca_list_append(B, sc, n, listed);
         }
     }
     // block reduction, then one atomic per warp
@@ -512,7 +559,7 @@ __device__ __forceinline__ double unordered_dev(long long i) {
 // (each round finishes at least the lexicographically first unfinished voxel), sweeps by 1001, age
 // sweeps by 1001 per relaxation. A failure is recorded in `status` with the iteration and later
 // steps do nothing until the host has read it.
-__global__ void __launch_bounds__(CA_THREADS) k_ca_step(const CaView C, const CaBufs B, CaScalars* sc, int iter) {
+__global__ void __launch_bounds__(CA_THREADS, 4) k_ca_step(const CaView C, const CaBufs B, CaScalars* sc, int iter) {
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
@@ -790,7 +837,7 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_ca_step, CA_THREADS, 0);
     if (e != cudaSuccess || per_sm < 1) return cuda_check(h, e == cudaSuccess ? cudaErrorLaunchOutOfResources : e, "automaton step");
-    h->ca_grid = h->num_sms * std::min(per_sm, 2);
+    h->ca_grid = h->num_sms * per_sm;  // every resident block: the full-box passes are latency-bound
     h->ca_ready = true;
     return CLB_OK;
 }
