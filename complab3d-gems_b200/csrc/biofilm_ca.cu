@@ -539,6 +539,14 @@ __device__ void ca_age_level(const CaView& C, const CaBufs& B, int level) {
 
 // ------------------------------------------------------------------ one step, on the device
 
+// The step's first mask pass as an ordinary launch over every resident thread the pass can use
+// (many more than the cooperative step keeps resident); its counters were reset before it.
+__global__ void __launch_bounds__(CA_THREADS) k_ca_mask_first(const CaView C, const CaBufs B, CaScalars* sc) {
+    if (sc->status != CA_OK) return;
+    if (B.mask0) return;  // several pore codes: the cooperative step snapshots the mask and runs this pass
+    ca_mask_total(C, B, sc);
+}
+
 // the mask as it stands before a pass, for the reopening rule with several pore codes
 __device__ __forceinline__ void ca_snapshot_mask(const CaView& C, const CaBufs& B) {
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < C.g.N; n += (int64_t)gridDim.x * blockDim.x)
@@ -565,16 +573,19 @@ __global__ void __launch_bounds__(CA_THREADS, 4) k_ca_step(const CaView C, const
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
     // `status` is written only after the last barrier of a step, so every block reads the same value
     if (sc->status != CA_OK) return;
-    if (lead) {
-        sc->gmax = LLONG_MIN;
-        sc->mask_sum = 0;
-        sc->nbio = 0;
-        sc->nonfinite = 0;
-        sc->moved = 0;
+    if (B.mask0) {
+        // the first pass, which k_ca_mask_first leaves to this launch with several pore codes
+        if (lead) {
+            sc->gmax = LLONG_MIN;
+            sc->mask_sum = 0;
+            sc->nbio = 0;
+            sc->nonfinite = 0;
+            sc->moved = 0;
+        }
+        ca_snapshot_mask(C, B);
+        grid.sync();
+        ca_mask_total(C, B, sc);
     }
-    if (B.mask0) ca_snapshot_mask(C, B);
-    grid.sync();
-    ca_mask_total(C, B, sc);
     grid.sync();
     double gmax = unordered_dev(sc->gmax);
     long long msum = sc->mask_sum;
@@ -879,7 +890,10 @@ clb_status ca_step_async(clb_handle* h, int64_t iter) {
     CaScalars* sc = SC(h);
     int it = (int)std::min<int64_t>(iter, INT32_MAX);
     void* args[] = {&C, &B, &sc, &it};
-    ++h->launches;
+    // the pass counters (everything before `status`) from the pinned reset value, then the first pass
+    cudaMemcpyAsync(sc, h->h_ca_pin, offsetof(CaScalars, status), cudaMemcpyHostToDevice, h->stream);
+    h->launches += 2;
+    k_ca_mask_first<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, B, sc);
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_ca_step, dim3(h->ca_grid), dim3(CA_THREADS), args, 0,
                                                 h->stream);
     return cuda_check(h, e, "automaton step");
