@@ -306,6 +306,9 @@ struct clb_handle_s {
     int8_t* d_ca_mask0 = nullptr;     // mask before a pass (several pore codes)
     int ca_cap = 0;
     int ca_grid = 0;                  // blocks of the cooperative automaton step (all resident)
+    // the window of the in-loop re-solves' tracer between re-solves (valid after the first)
+    clb::Tracer resolve_tracer{};
+    bool resolve_tracer_valid = false;
 };
 
 namespace clb {
@@ -318,7 +321,9 @@ clb_status cuda_check(clb_handle* h, cudaError_t e, const char* what);
 // flow.cu
 clb_status flow_init(clb_handle* h, double delta_p);
 clb_status flow_step(clb_handle* h, int n, bool trace, double eps);
-clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations);
+// keep_window: the in-loop re-solves' ValueTracer (complab.cpp:2166, ns_convg2) is one object for
+// the whole run, never reset, so each re-solve starts with the window the previous one left
+clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations, bool keep_window = false);
 clb_status flow_autotune(clb_handle* h, int steps, char* report, int report_len);
 clb_status flow_stats(clb_handle* h, double char_length, clb_flow_stats* out);
 clb_status flow_velocity(clb_handle* h, void* dst, int dtype_device, bool to_host);

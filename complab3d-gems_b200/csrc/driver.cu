@@ -84,7 +84,7 @@ static clb_status resolve_flow(clb_handle* h, const clb_run_desc* d, bool mask_m
     clb_status st = CLB_OK;
     if (mask_moved && h->ca_ready) st = refresh_dynamics(h, 0, 1);  // updateNsLatticesDynamics3D
     int it = 0;
-    if (st == CLB_OK) st = flow_solve(h, d->flow_max_iterations, d->flow_eps, &it);
+    if (st == CLB_OK) st = flow_solve(h, d->flow_max_iterations, d->flow_eps, &it, true);
     r->flow_resolves += 1;
     r->flow_iterations += it;
     if (st == CLB_NOT_CONVERGED) {

@@ -538,6 +538,7 @@ static int flow_gather_grid(clb_handle* h) {
 }
 
 clb_status flow_init(clb_handle* h, double delta_p) {
+    h->resolve_tracer_valid = false;  // a new flow: the in-loop tracer starts empty again
     const clb_domain_desc& d = h->d;
     FlowParams& P = h->fp;
     std::memset(&P, 0, sizeof(P));
@@ -722,10 +723,16 @@ clb_status flow_step(clb_handle* h, int n, bool trace, double eps) {
     return cuda_check(h, cudaGetLastError(), "flow step");
 }
 
-clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations) {
-    // a fresh util::ValueTracer: empty window, new epsilon
+clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations, bool keep_window) {
+    // a fresh util::ValueTracer (empty window, new epsilon), or the in-loop one as the previous
+    // re-solve left it
     Tracer t0;
     std::memset(&t0, 0, sizeof(t0));
+    if (keep_window && h->resolve_tracer_valid) {
+        std::memcpy(t0.ring, h->resolve_tracer.ring, sizeof(t0.ring));
+        t0.count = h->resolve_tracer.count;
+        t0.head = h->resolve_tracer.head;
+    }
     Tracer cur;
     cudaError_t e = cudaMemcpyAsync(&cur, h->d_tracer, sizeof(Tracer), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -751,6 +758,10 @@ clb_status flow_solve(clb_handle* h, int max_it, double eps, int* iterations) {
     }
     h->flow_iters = cur.iterations;  // steps after convergence were no-ops
     if (iterations) *iterations = (int)(cur.iterations - start);
+    if (keep_window) {
+        h->resolve_tracer = cur;
+        h->resolve_tracer_valid = true;
+    }
     // leave the tracer disabled for plain steps
     int zero = 0;
     cudaMemcpyAsync(&h->d_tracer->converged, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream);

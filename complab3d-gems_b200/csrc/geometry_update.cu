@@ -476,7 +476,7 @@ clb_status geometry_update(clb_handle* h, int* sealed, int* reopened) {
         st = flow_follow(h);
         if (st != CLB_OK) return st;
         int it = 0;
-        st = flow_solve(h, h->prc.flow_max_iterations, h->prc.flow_eps, &it);
+        st = flow_solve(h, h->prc.flow_max_iterations, h->prc.flow_eps, &it, true);
         if (st != CLB_OK && st != CLB_NOT_CONVERGED) return st;
         const clb_status cs = ade_couple(h);
         if (cs != CLB_OK) return cs;
