@@ -1094,6 +1094,7 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
     h->d_bio = nullptr;
     h->M = M;
     h->ap.M = M;
+    h->ca_full = true;  // the automaton's next mask pass looks at every voxel's new biomass
     if (M == 0) return CLB_OK;
     cudaError_t e = cudaMalloc(&h->d_bio, sizeof(double) * M * (size_t)h->g.N);
     if (e != cudaSuccess) return cuda_check(h, e, "biomass");
@@ -1665,11 +1666,13 @@ clb_status ade_density(clb_handle* h, int s, double* host) {
 
 clb_status ade_biomass(clb_handle* h, int m, double* host) {
     if (!h->ade_ready || m < 0 || m >= h->M) return fail(h, CLB_INVALID_ARG, "no such biomass field");
+    h->ca_full = true;
     return cuda_check(h, cudaMemcpy(host, h->d_bio + (size_t)m * h->g.N, sizeof(double) * h->g.N, cudaMemcpyDeviceToHost), "biomass copy");
 }
 
 clb_status ade_set_biomass_field(clb_handle* h, int m, const double* host) {
     if (!h->ade_ready || m < 0 || m >= h->M) return fail(h, CLB_INVALID_ARG, "no such biomass field");
+    h->ca_full = true;
     return cuda_check(h, cudaMemcpy(h->d_bio + (size_t)m * h->g.N, host, sizeof(double) * h->g.N, cudaMemcpyHostToDevice), "biomass copy");
 }
 

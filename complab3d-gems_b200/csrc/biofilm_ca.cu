@@ -38,6 +38,17 @@
 // (the only ones the rule changes; the mask pass lists them): the update is monotone and only ever
 // raises an age, so any order of updates reaches the same least fixed point as the reference's
 // lexicographic in-place sweeps. Counters cross to the host through pinned memory.
+//
+// Passes over the biomass list, not the box. A mask pass lists the voxels whose total exceeds
+// 1e-14 afterwards. A voxel off that list holds every microbe below 1e-12 (a microbe at or above
+// it makes the sum differ from a stored total at or below 1e-14 by more than 1e-14, so the pass
+// stores the new total and lists the voxel) and a pore or closed code (a biofilm code below the
+// biofilm threshold reverts). The rate laws leave biomass below 1e-12 as it is, and such a voxel
+// is a fixed point of the mask rule, so the next pass needs only the listed voxels plus those a
+// push sweep deposited into. The mask sum is carried along by the changes each pass makes. The
+// pushes of a sweep likewise change only the active voxels and the voxels their records name, so
+// the apply pass walks those two lists. A pass over the whole box runs after set-up and after
+// the host or a geometry update wrote biomass or the material map (`full`).
 #include "sparse.cuh"
 
 #include <cooperative_groups.h>
@@ -80,18 +91,24 @@ __device__ __forceinline__ long long ordered(double v) {
     return i < 0 ? i ^ 0x7FFFFFFFFFFFFFFFLL : i;
 }
 
-// Counters and control state of the automaton in device memory. The pass counters are cleared
-// and read inside one step; the step results and the totals are what the host reads back.
+// Counters and control state of the automaton in device memory. The pass and sweep counters are
+// cleared and read inside one step (the first pass's by the step before, or at set-up); the step
+// results and the totals are what the host reads back.
 struct CaScalars {
-    long long gmax;        // ordered bits of max(total)
-    long long mask_sum;
-    unsigned int active;   // voxels collected for the sweep
-    unsigned int remaining;
-    unsigned int changed;  // ages changed by a sweep
-    unsigned int overflow; // active voxels beyond the capacity
+    long long gmax;         // ordered bits of max(total) over the voxels the pass visits, at least 0
+    long long msum;         // whole-box pass: the mask sum; list pass: the change it made to it
     unsigned int nonfinite; // biomass values that are NaN or infinite (mask pass)
+    unsigned int nout;      // voxels the mask pass lists
     unsigned int moved;     // voxels whose material the passes of the step changed
-    unsigned int nbio;      // voxels in the biomass list the mask pass writes
+    unsigned int active;    // voxels collected for the sweep
+    unsigned int remaining;
+    unsigned int changed;   // ages changed by a sweep
+    unsigned int overflow;  // active voxels beyond the capacity
+    unsigned int next;      // voxels the sweep pushed into that are not active themselves
+    unsigned int next2;     // of those, the ones not on the biomass list
+    unsigned int nlist;     // voxels on the current biomass list
+    int list;               // which of the two list buffers holds it
+    long long mask_run;     // the mask sum as it stands
     int status;             // CA_OK, or why a step stopped (kept until the host reads it)
     int fail_iter;          // the iteration whose step set `status`
     int step_sweeps;        // push sweeps of the last step
@@ -118,7 +135,10 @@ struct CaBufs {
     int* tgt;
     double* amt;
     double* own;
-    int32_t* blist;
+    int32_t* list[2];  // the biomass list and the one the next mask pass writes
+    int32_t* ext;      // voxels a sweep pushed into that are not active
+    int32_t* ext2;     // of those, the ones off the biomass list
+    int* tmark;        // 1 while a voxel is on ext (cleared after the sweep)
     int cap;
     uint64_t seed;
 };
@@ -142,15 +162,15 @@ __global__ void k_ca_init(const CaView C, const int8_t* __restrict__ mat, const 
         distp[n] = (ca_open(C, mk) && x < G.nx - 1 && y < G.ny - 1 && z < G.nz - 1) ? 1 : 0;
         aidx[n] = -1;
     }
-    atomicAdd((unsigned long long*)&sc->mask_sum, (unsigned long long)msum);
+    atomicAdd((unsigned long long*)&sc->mask_run, (unsigned long long)msum);
 }
 
 // updateLocalMaskNtotalLattices3D; with several pore codes a reopened voxel copies the first
-// pore neighbour found in `mask_before` (the mask as it stood before the pass).
-// Also lists the voxels whose total biomass exceeds 1e-14 afterwards (in no particular order): the
-// only voxels the age wavefront and the push can touch.
+// pore neighbour found in `mask0` (the mask as it stood before the pass).
 // One voxel of the pass, from its loaded material, previous total and biomass; returns whether it
-// goes on the biomass list.
+// goes on the biomass list. `msum` takes the voxel's code (DELTA false: a whole-box pass sums the
+// mask) or the change the pass made to it (DELTA true: a list pass carries the sum along).
+template <bool DELTA>
 __device__ __forceinline__ bool ca_mask_voxel(const CaView& C, const CaBufs& B, CaScalars* sc, int64_t n, int mk,
                                               double told, const double* bm, long long& best, long long& msum) {
     const Geom G = C.g;
@@ -191,74 +211,99 @@ __device__ __forceinline__ bool ca_mask_voxel(const CaView& C, const CaBufs& B, 
             B.mat[n] = (int8_t)out;
             atomicAdd(&sc->moved, 1u);
         }
-        msum += out;
-    } else {
+        msum += DELTA ? out - mk : out;
+    } else if (!DELTA) {
         msum += mk;
     }
     best = max(best, ordered(tn));
     return tn > 1e-14;
 }
 
-// appends n (where `listed`) to the biomass list, one atomic per warp; the whole warp calls it
-__device__ __forceinline__ void ca_list_append(const CaBufs& B, CaScalars* sc, int64_t n, bool listed) {
+// appends n (where `listed`) to `out` (count in *nout), one atomic per warp; the whole warp calls it
+__device__ __forceinline__ void ca_list_append(int32_t* __restrict__ out, unsigned int* nout, int64_t n, bool listed) {
     const int lane = threadIdx.x & 31;
     const unsigned int bal = __ballot_sync(0xffffffffu, listed);
     if (!bal) return;
     unsigned int base = 0;
-    if (lane == 0) base = atomicAdd(&sc->nbio, (unsigned int)__popc(bal));
+    if (lane == 0) base = atomicAdd(nout, (unsigned int)__popc(bal));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (listed) B.blist[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)n;
+    if (listed) out[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)n;
 }
 
-// updateLocalMaskNtotalLattices3D over every voxel. Each thread takes UNR voxels a grid stride
-// apart per round and issues their loads together, so the pass is not bound by one voxel's latency.
-__device__ void ca_mask_total(const CaView& C, const CaBufs& B, CaScalars* sc) {
+// updateLocalMaskNtotalLattices3D. FULL: over every voxel; each thread takes UNR voxels a grid
+// stride apart per round and issues their loads together, so the pass is not bound by one voxel's
+// latency. Otherwise over the voxels of in[0, n_in) and in2[0, n_in2) (disjoint lists), every other
+// voxel being a fixed point of the rule. The voxels whose total exceeds 1e-14 afterwards go to
+// `out` (count in sc->nout); max(total), the mask sum (FULL) or its change, and the counts go to
+// the pass counters.
+template <bool FULL>
+__device__ void ca_mask_pass(const CaView& C, const CaBufs& B, CaScalars* sc, const int32_t* __restrict__ in,
+                             int n_in, const int32_t* __restrict__ in2, int n_in2, int32_t* __restrict__ out) {
     const Geom G = C.g;
-    long long best = LLONG_MIN, msum = 0;
-    constexpr int UNR = 4;
+    long long best = 0, msum = 0;  // ordered(+0.0) == 0: totals are never below zero
     const int64_t S = (int64_t)gridDim.x * blockDim.x;
-    // whole warps run the loop together, so the list append is warp-wide
-    const int64_t span = (G.N + 31) / 32 * 32;
-    if (C.M <= 2) {
-        for (int64_t n0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n0 < span; n0 += UNR * S) {
-            int mk[UNR];
-            double told[UNR], b0[UNR], b1[UNR];
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (FULL) {
+        constexpr int UNR = 4;
+        // whole warps run the loop together, so the list append is warp-wide
+        const int64_t span = (G.N + 31) / 32 * 32;
+        if (C.M <= 2) {
+            for (int64_t n0 = t0; n0 < span; n0 += UNR * S) {
+                int mk[UNR];
+                double told[UNR], b0[UNR], b1[UNR];
 #pragma unroll
-            for (int j = 0; j < UNR; ++j) {
-                const int64_t n = n0 + j * S;
-                const bool in = n < G.N;
-                mk[j] = in ? (int)B.mat[n] : C.bb;
-                told[j] = in ? B.total[n] : 0.0;
+                for (int j = 0; j < UNR; ++j) {
+                    const int64_t n = n0 + j * S;
+                    const bool inb = n < G.N;
+                    mk[j] = inb ? (int)B.mat[n] : C.bb;
+                    told[j] = inb ? B.total[n] : 0.0;
+                }
+                // biomass only where the voxel is open (most voxels of a pack are not)
+#pragma unroll
+                for (int j = 0; j < UNR; ++j) {
+                    const int64_t n = n0 + j * S;
+                    const bool op = n < G.N && ca_open(C, mk[j]);
+                    b0[j] = op ? B.bio[n] : 0.0;
+                    b1[j] = (op && C.M > 1) ? B.bio[G.N + n] : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < UNR; ++j) {
+                    const int64_t n = n0 + j * S;
+                    if (n >= span) break;  // uniform per warp: span and S are multiples of 32
+                    bool listed = false;
+                    if (n < G.N) {
+                        const double bm[2] = {b0[j], b1[j]};
+                        listed = ca_mask_voxel<false>(C, B, sc, n, mk[j], told[j], bm, best, msum);
+                    }
+                    ca_list_append(out, &sc->nout, n, listed);
+                }
             }
-            // biomass only where the voxel is open (most voxels of a pack are not)
-#pragma unroll
-            for (int j = 0; j < UNR; ++j) {
-                const int64_t n = n0 + j * S;
-                const bool op = n < G.N && ca_open(C, mk[j]);
-                b0[j] = op ? B.bio[n] : 0.0;
-                b1[j] = (op && C.M > 1) ? B.bio[G.N + n] : 0.0;
-            }
-#pragma unroll
-            for (int j = 0; j < UNR; ++j) {
-                const int64_t n = n0 + j * S;
-                if (n >= span) break;  // uniform per warp: span and S are multiples of 32
+        } else {
+            for (int64_t n = t0; n < span; n += S) {
                 bool listed = false;
                 if (n < G.N) {
-                    const double bm[2] = {b0[j], b1[j]};
-                    listed = ca_mask_voxel(C, B, sc, n, mk[j], told[j], bm, best, msum);
+                    double bm[CLB_MAX_MICROBES];
+                    for (int m = 0; m < C.M; ++m) bm[m] = B.bio[(int64_t)m * G.N + n];
+                    listed = ca_mask_voxel<false>(C, B, sc, n, B.mat[n], B.total[n], bm, best, msum);
                 }
-                ca_list_append(B, sc, n, listed);
+                ca_list_append(out, &sc->nout, n, listed);
             }
         }
     } else {
-        for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < span; n += S) {
+        const int64_t n_all = (int64_t)n_in + n_in2;
+        const int64_t span = (n_all + 31) / 32 * 32;
+        for (int64_t j = t0; j < span; j += S) {
             bool listed = false;
-            if (n < G.N) {
+            int64_t n = 0;
+            if (j < n_all) {
+                n = j < n_in ? in[j] : in2[j - n_in];
+                const int mk = B.mat[n];
                 double bm[CLB_MAX_MICROBES];
-                for (int m = 0; m < C.M; ++m) bm[m] = B.bio[(int64_t)m * G.N + n];
-                listed = ca_mask_voxel(C, B, sc, n, B.mat[n], B.total[n], bm, best, msum);
+                const bool op = ca_open(C, mk);
+                for (int m = 0; m < C.M; ++m) bm[m] = op ? B.bio[(int64_t)m * G.N + n] : 0.0;
+                listed = ca_mask_voxel<true>(C, B, sc, n, mk, B.total[n], bm, best, msum);
             }
-            ca_list_append(B, sc, n, listed);
+            ca_list_append(out, &sc->nout, n, listed);
         }
     }
     // block reduction, then one atomic per warp
@@ -268,24 +313,23 @@ __device__ void ca_mask_total(const CaView& C, const CaBufs& B, CaScalars* sc) {
     }
     if ((threadIdx.x & 31) == 0) {
         atomicMax(&sc->gmax, best);
-        atomicAdd((unsigned long long*)&sc->mask_sum, (unsigned long long)msum);
+        atomicAdd((unsigned long long*)&sc->msum, (unsigned long long)msum);
     }
 }
 
 // ------------------------------------------------------------------ push sweep
 
 // the voxels of x = 1..nx-2 that push, from the biomass list (any voxel above the maximum is on it)
-__device__ void ca_collect(const CaView& C, const CaBufs& B, CaScalars* sc) {
+__device__ void ca_collect(const CaView& C, const CaBufs& B, CaScalars* sc, const int32_t* __restrict__ blist,
+                           int nb) {
     const Geom G = C.g;
     const int8_t* __restrict__ mat = B.mat;
     const double* __restrict__ total = B.total;
-    const int32_t* __restrict__ blist = B.blist;
     int* __restrict__ aidx = B.aidx;
     int* __restrict__ act = B.act;
     int* __restrict__ done = B.done;
     const int cap = B.cap;
     const int64_t lo = G.plane, hi = G.N - G.plane;  // x = 1..nx-2
-    const int nb = (int)sc->nbio;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb; j += gridDim.x * blockDim.x) {
         const int64_t n = blist[j];
         if (n < lo || n >= hi || !ca_open(C, mat[n])) continue;
@@ -425,16 +469,37 @@ __device__ void ca_round(const CaView& C, const CaBufs& B, int count, int round,
     }
 }
 
-// every voxel takes the pushes it received, in the order the sequential sweep adds them
-__device__ void ca_apply(const CaView& C, const CaBufs& B) {
+// The voxels a sweep pushed into that are not active themselves, each once (ext), and of those the
+// ones off the biomass list (ext2: their total is at most 1e-14, which is the list's criterion;
+// the total changes only in mask passes). Every voxel whose biomass the sweep changes is active
+// or on ext.
+__device__ void ca_targets(const CaBufs& B, CaScalars* sc, int count) {
+    const int* __restrict__ tgt = B.tgt;
+    const int* __restrict__ aidx = B.aidx;
+    const double* __restrict__ total = B.total;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        for (int t = 0; t < CA_REC; ++t) {
+            const int m = tgt[i * CA_REC + t];
+            if (m < 0 || aidx[m] >= 0) continue;
+            if (atomicExch(&B.tmark[m], 1) != 0) continue;
+            B.ext[atomicAdd(&sc->next, 1u)] = m;
+            if (!(total[m] > 1e-14)) B.ext2[atomicAdd(&sc->next2, 1u)] = m;
+        }
+    }
+}
+
+// every voxel takes the pushes it received, in the order the sequential sweep adds them: the
+// active voxels (act[0, count)) and the voxels they pushed into (ext[0, next)); no other voxel's
+// biomass changes
+__device__ void ca_apply(const CaView& C, const CaBufs& B, int count, int next) {
     const Geom G = C.g;
     double* __restrict__ bio = B.bio;
     const int* __restrict__ aidx = B.aidx;
     const int* __restrict__ tgt = B.tgt;
     const double* __restrict__ amt = B.amt;
     const double* __restrict__ own = B.own;
-    const int64_t lo = G.plane, hi = G.N - G.plane;
-    for (int64_t n = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += (int64_t)gridDim.x * blockDim.x) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < count + next; j += gridDim.x * blockDim.x) {
+        const int64_t n = j < count ? B.act[j] : B.ext[j - count];
         int x, y, z;
         decode(G, n, x, y, z);
         const int a = aidx[n];
@@ -460,8 +525,11 @@ __device__ void ca_apply(const CaView& C, const CaBufs& B) {
     }
 }
 
-__device__ void ca_clear(const CaBufs& B, int count) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) B.aidx[B.act[i]] = -1;
+__device__ void ca_clear(const CaBufs& B, int count, int next) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count + next; i += gridDim.x * blockDim.x) {
+        if (i < count) B.aidx[B.act[i]] = -1;
+        else B.tmark[B.ext[i - count]] = 0;
+    }
 }
 
 // ------------------------------------------------------------------ age wavefront
@@ -501,13 +569,12 @@ __device__ __forceinline__ int age_rule(const CaView& C, int64_t n, const int* a
 // sweep: both are iterates of the same monotone, inflationary rule, so the sweeps still reach the
 // least fixed point above the start, the one the reference's in-place sweeps reach, and a sweep
 // that changes nothing has read only final values.
-__device__ void ca_age_relax(const CaView& C, const CaBufs& B, CaScalars* sc) {
+__device__ void ca_age_relax(const CaView& C, const CaBufs& B, CaScalars* sc, const int32_t* __restrict__ blist,
+                             int nb) {
     int* age = B.age;
     const int8_t* __restrict__ distp = B.distp;
     const double* __restrict__ total = B.total;
-    const int32_t* __restrict__ blist = B.blist;
     unsigned int ch = 0;
-    const int nb = (int)sc->nbio;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb; j += gridDim.x * blockDim.x) {
         const int64_t n = blist[j];
         const int old = age[n];
@@ -540,11 +607,14 @@ __device__ void ca_age_level(const CaView& C, const CaBufs& B, int level) {
 // ------------------------------------------------------------------ one step, on the device
 
 // The step's first mask pass as an ordinary launch over every resident thread the pass can use
-// (many more than the cooperative step keeps resident); its counters were reset before it.
-__global__ void __launch_bounds__(CA_THREADS) k_ca_mask_first(const CaView C, const CaBufs B, CaScalars* sc) {
+// (many more than the cooperative step keeps resident): over the whole box when `full`, else over
+// the biomass list; it writes the other list buffer. The step before cleared its counters.
+__global__ void __launch_bounds__(CA_THREADS) k_ca_mask_first(const CaView C, const CaBufs B, CaScalars* sc, int full) {
     if (sc->status != CA_OK) return;
     if (B.mask0) return;  // several pore codes: the cooperative step snapshots the mask and runs this pass
-    ca_mask_total(C, B, sc);
+    const int cur = sc->list;
+    if (full) ca_mask_pass<true>(C, B, sc, nullptr, 0, nullptr, 0, B.list[cur ^ 1]);
+    else ca_mask_pass<false>(C, B, sc, B.list[cur], (int)sc->nlist, nullptr, 0, B.list[cur ^ 1]);
 }
 
 // the mask as it stands before a pass, for the reopening rule with several pore codes
@@ -558,6 +628,14 @@ __device__ __forceinline__ double unordered_dev(long long i) {
     return __longlong_as_double(i);
 }
 
+// the counters of a mask pass, cleared by one thread ahead of a barrier
+__device__ __forceinline__ void ca_pass_reset(CaScalars* sc) {
+    sc->gmax = 0;  // ordered(+0.0)
+    sc->msum = 0;
+    sc->nonfinite = 0;
+    sc->nout = 0;
+}
+
 // One step of the automaton (ca_step's sequence: mask pass; while max(total) exceeds Bmax, push
 // sweeps with their mask passes, the stall and sweep limits and, every 50 sweeps, the age
 // relaxation; the in-place age sweep after a mask change) in one cooperative launch, with grid-wide
@@ -566,34 +644,35 @@ __device__ __forceinline__ double unordered_dev(long long i) {
 // block can read a later value than another. Every loop is bounded: rounds by the active count
 // (each round finishes at least the lexicographically first unfinished voxel), sweeps by 1001, age
 // sweeps by 1001 per relaxation. A failure is recorded in `status` with the iteration and later
-// steps do nothing until the host has read it.
-__global__ void __launch_bounds__(CA_THREADS, 4) k_ca_step(const CaView C, const CaBufs B, CaScalars* sc, int iter) {
+// steps do nothing until the host has read it. The biomass list alternates between two buffers:
+// every block tracks which one is current and its length, and the step leaves both for the next.
+__global__ void __launch_bounds__(CA_THREADS, 4) k_ca_step(const CaView C, const CaBufs B, CaScalars* sc, int iter,
+                                                            int full) {
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
-    // `status` is written only after the last barrier of a step, so every block reads the same value
+    // `status`, `list`, `nlist` and `mask_run` are written only after the last barrier of a step, so
+    // every block reads the same values
     if (sc->status != CA_OK) return;
+    int cur = sc->list;
+    int nlist = (int)sc->nlist;
     if (B.mask0) {
         // the first pass, which k_ca_mask_first leaves to this launch with several pore codes
-        if (lead) {
-            sc->gmax = LLONG_MIN;
-            sc->mask_sum = 0;
-            sc->nbio = 0;
-            sc->nonfinite = 0;
-            sc->moved = 0;
-        }
         ca_snapshot_mask(C, B);
         grid.sync();
-        ca_mask_total(C, B, sc);
+        if (full) ca_mask_pass<true>(C, B, sc, nullptr, 0, nullptr, 0, B.list[cur ^ 1]);
+        else ca_mask_pass<false>(C, B, sc, B.list[cur], nlist, nullptr, 0, B.list[cur ^ 1]);
     }
     grid.sync();
     double gmax = unordered_dev(sc->gmax);
-    long long msum = sc->mask_sum;
+    long long msum = full ? sc->msum : sc->mask_run + sc->msum;  // the mask sum now
     int status = (sc->nonfinite || !isfinite(gmax)) ? CA_NONFINITE : CA_OK;
+    cur ^= 1;
+    nlist = (int)sc->nout;
     uint64_t sweep = sc->sweep_counter;
     const long long mask_sum0 = sc->ca_mask_sum;
     grid.sync();
-    int whilecount = 0, stall = 0;
+    int whilecount = 0, stall = 0, count = 0, next = 0;
     double prev = gmax;
     if (status == CA_OK && gmax - C.bmax > THRD) {
         while (gmax - C.bmax > THRD) {
@@ -601,14 +680,22 @@ __global__ void __launch_bounds__(CA_THREADS, 4) k_ca_step(const CaView C, const
             if (lead) {
                 sc->active = 0;
                 sc->overflow = 0;
+                sc->next = 0;
+                sc->next2 = 0;
             }
             grid.sync();
-            ca_collect(C, B, sc);
+            ca_collect(C, B, sc, B.list[cur], nlist);
             grid.sync();
-            const int count = (int)sc->active;
+            count = (int)sc->active;
             const bool over = sc->overflow != 0;
             grid.sync();
-            if (over) { status = CA_CAPACITY; break; }
+            if (over) {
+                count = count < B.cap ? count : B.cap;  // the rows written; cleared below
+                status = CA_CAPACITY;
+                break;
+            }
+            int next2 = 0;
+            next = 0;
             if (count > 0) {
                 if (lead) sc->remaining = (unsigned int)count;
                 grid.sync();
@@ -621,24 +708,26 @@ __global__ void __launch_bounds__(CA_THREADS, 4) k_ca_step(const CaView C, const
                     if (round >= count) { status = CA_ROUNDS; break; }
                 }
                 if (status != CA_OK) break;
-                ca_apply(C, B);
+                ca_targets(B, sc, count);
                 grid.sync();
-                ca_clear(B, count);
+                next = (int)sc->next;
+                next2 = (int)sc->next2;
+                ca_apply(C, B, count, next);
+                grid.sync();
+                ca_clear(B, count, next);
+                count = next = 0;
             }
             ++sweep;
-            // ---- mask pass after the sweep
-            if (lead) {
-                sc->gmax = LLONG_MIN;
-                sc->mask_sum = 0;
-                sc->nbio = 0;
-                sc->nonfinite = 0;
-            }
+            // ---- mask pass after the sweep: the list and the voxels pushed into off it
+            if (lead) ca_pass_reset(sc);
             if (B.mask0) ca_snapshot_mask(C, B);
             grid.sync();
-            ca_mask_total(C, B, sc);
+            ca_mask_pass<false>(C, B, sc, B.list[cur], nlist, B.ext2, next2, B.list[cur ^ 1]);
             grid.sync();
             gmax = unordered_dev(sc->gmax);
-            msum = sc->mask_sum;
+            msum += sc->msum;
+            cur ^= 1;
+            nlist = (int)sc->nout;
             const bool nonf = sc->nonfinite != 0;
             grid.sync();
             if (nonf || !isfinite(gmax)) { status = CA_NONFINITE; break; }
@@ -653,7 +742,7 @@ __global__ void __launch_bounds__(CA_THREADS, 4) k_ca_step(const CaView C, const
                 for (int k = 0; k < 1001 && !settled; ++k) {
                     if (lead) sc->changed = 0;
                     grid.sync();
-                    ca_age_relax(C, B, sc);
+                    ca_age_relax(C, B, sc, B.list[cur], nlist);
                     grid.sync();
                     settled = sc->changed == 0;
                     grid.sync();
@@ -664,6 +753,10 @@ __global__ void __launch_bounds__(CA_THREADS, 4) k_ca_step(const CaView C, const
             ++whilecount;
         }
     }
+    // a sweep that stopped before its pushes were applied leaves its active voxels marked: unmark
+    // them (after the barrier the break followed), so the handle can step again once the host has
+    // read the failure
+    if (count > 0) ca_clear(B, count, 0);
     bool changed = false;
     if (status != CA_NONFINITE) {
         // after the block, a changed mask takes one in-place age sweep (wavefronts over x + y + z)
@@ -676,14 +769,20 @@ __global__ void __launch_bounds__(CA_THREADS, 4) k_ca_step(const CaView C, const
             }
         }
     }
+    // every block read the counters before a barrier it has passed, so the lead may reset them
     if (lead) {
         sc->step_sweeps = whilecount;
         sc->step_changed = changed ? 1 : 0;
         if (changed) sc->ca_mask_sum = msum;
+        sc->mask_run = msum;
+        sc->list = cur;
+        sc->nlist = (unsigned int)nlist;
         sc->sweep_counter = sweep;
         sc->total_sweeps += whilecount;
         sc->total_changes += changed ? 1 : 0;
         if (sc->moved) sc->moved_any = 1;
+        sc->moved = 0;
+        ca_pass_reset(sc);  // for the next step's first pass
         if (status != CA_OK) {
             sc->status = status;
             sc->fail_iter = iter;
@@ -755,7 +854,13 @@ static CaView ca_view(const clb_handle* h) {
 void ca_free(clb_handle* h) {
     cudaFree(h->d_ca_total); h->d_ca_total = nullptr;
     cudaFree(h->d_ca_age); h->d_ca_age = nullptr;
-    cudaFree(h->d_ca_blist); h->d_ca_blist = nullptr;
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(h->d_ca_list[i]);
+        h->d_ca_list[i] = nullptr;
+    }
+    cudaFree(h->d_ca_ext); h->d_ca_ext = nullptr;
+    cudaFree(h->d_ca_ext2); h->d_ca_ext2 = nullptr;
+    cudaFree(h->d_ca_tmark); h->d_ca_tmark = nullptr;
     if (h->h_ca_pin) cudaFreeHost(h->h_ca_pin);
     h->h_ca_pin = nullptr;
     cudaFree(h->d_ca_distp); h->d_ca_distp = nullptr;
@@ -800,7 +905,12 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
     const size_t N = (size_t)h->g.N;
     cudaError_t e = cudaMalloc(&h->d_ca_total, sizeof(double) * N);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_age, sizeof(int) * N);
-    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_blist, sizeof(int32_t) * N);
+    for (int i = 0; i < 2; ++i)
+        if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_list[i], sizeof(int32_t) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_ext, sizeof(int32_t) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_ext2, sizeof(int32_t) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_tmark, sizeof(int) * N);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_ca_tmark, 0, sizeof(int) * N, h->stream);
     if (e == cudaSuccess) e = cudaHostAlloc(&h->h_ca_pin, 3 * sizeof(CaScalars), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_distp, N);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ca_aidx, sizeof(int) * N);
@@ -830,21 +940,23 @@ clb_status ca_setup(clb_handle* h, const clb_ca_desc* d) {
     h->ca_half = d->push_mode;
     h->ca_seed = d->seed;
     h->ca_sweeps = 0;
-    // pinned copies: [0] the mask pass's starting value (max at its least), [1] read back, [2] scratch
+    // pinned copies: [1] read back ([0] and [2] unused)
     CaScalars* pin = static_cast<CaScalars*>(h->h_ca_pin);
     std::memset(pin, 0, 3 * sizeof(CaScalars));
-    pin[0].gmax = LLONG_MIN;
+    // all counters zero: the first pass's are cleared (gmax 0 is ordered(+0.0)), the list is empty,
+    // and the first step's pass runs over the whole box
     cudaMemsetAsync(SC(h), 0, sizeof(CaScalars), h->stream);
+    h->ca_full = true;
     const CaView C = ca_view(h);
     k_ca_init<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, h->d_mat, h->d_bio, h->d_ca_total, h->d_ca_age,
                                                              h->d_ca_distp, h->d_ca_aidx, SC(h));
     // the mask sum the steps compare against
-    cudaMemcpyAsync(&SC(h)->ca_mask_sum, &SC(h)->mask_sum, sizeof(long long), cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(&SC(h)->ca_mask_sum, &SC(h)->mask_run, sizeof(long long), cudaMemcpyDeviceToDevice, h->stream);
     CaScalars s;
     e = cudaMemcpyAsync(&s, SC(h), sizeof s, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_check(h, e, "cellular automaton set-up");
-    h->ca_mask_sum = s.mask_sum;
+    h->ca_mask_sum = s.mask_run;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_ca_step, CA_THREADS, 0);
     if (e != cudaSuccess || per_sm < 1) return cuda_check(h, e == cudaSuccess ? cudaErrorLaunchOutOfResources : e, "automaton step");
@@ -876,7 +988,11 @@ static CaBufs ca_bufs(clb_handle* h) {
     B.tgt = h->d_ca_tgt;
     B.amt = h->d_ca_amt;
     B.own = h->d_ca_own;
-    B.blist = h->d_ca_blist;
+    B.list[0] = h->d_ca_list[0];
+    B.list[1] = h->d_ca_list[1];
+    B.ext = h->d_ca_ext;
+    B.ext2 = h->d_ca_ext2;
+    B.tmark = h->d_ca_tmark;
     B.cap = h->ca_cap;
     B.seed = h->ca_seed;
     return B;
@@ -889,13 +1005,14 @@ clb_status ca_step_async(clb_handle* h, int64_t iter) {
     CaBufs B = ca_bufs(h);
     CaScalars* sc = SC(h);
     int it = (int)std::min<int64_t>(iter, INT32_MAX);
-    void* args[] = {&C, &B, &sc, &it};
-    // the pass counters (everything before `status`) from the pinned reset value, then the first pass
-    cudaMemcpyAsync(sc, h->h_ca_pin, offsetof(CaScalars, status), cudaMemcpyHostToDevice, h->stream);
+    int full = h->ca_full ? 1 : 0;  // biomass or the map written outside the automaton: whole box
+    void* args[] = {&C, &B, &sc, &it, &full};
+    // the first pass (its counters were cleared by the step before), then the rest of the step
     h->launches += 2;
-    k_ca_mask_first<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, B, sc);
+    k_ca_mask_first<<<h->num_sms * 8, CA_THREADS, 0, h->stream>>>(C, B, sc, full);
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_ca_step, dim3(h->ca_grid), dim3(CA_THREADS), args, 0,
                                                 h->stream);
+    if (e == cudaSuccess) h->ca_full = false;
     return cuda_check(h, e, "automaton step");
 }
 

@@ -292,9 +292,14 @@ struct clb_handle_s {
     long long ca_mask_sum = 0;
     double* d_ca_total = nullptr;     // [N] total biomass as the automaton tracks it
     int* d_ca_age = nullptr;          // [N] age wavefront
-    int32_t* d_ca_blist = nullptr;    // [N] voxels whose total biomass exceeds 1e-14 (last mask pass)
+    int32_t* d_ca_list[2] = {nullptr, nullptr};  // [N] each: voxels whose total biomass exceeds 1e-14
+                                      // (the last mask pass's list and the one the next pass writes)
+    int32_t* d_ca_ext = nullptr;      // [N] voxels a push sweep deposited into that are not active
+    int32_t* d_ca_ext2 = nullptr;     // [N] of those, the ones off the biomass list
+    int* d_ca_tmark = nullptr;        // [N] 1 while a voxel is on d_ca_ext
+    bool ca_full = true;              // the next automaton step's first pass covers the whole box
     bool h_mat_stale = false;         // the automaton changed the device map since h_mat was copied
-    void* h_ca_pin = nullptr;         // pinned host copies of the counters: [0] reset value, [1] read back, [2] scratch
+    void* h_ca_pin = nullptr;         // pinned host copies of the counters: [1] read back
     int8_t* d_ca_distp = nullptr;     // [N] 1 where the distance-from-wall field is positive
     int* d_ca_aidx = nullptr;         // [N] row of an active voxel in the sweep, -1
     int* d_ca_act = nullptr;          // [cap] active voxels of a sweep

@@ -459,6 +459,7 @@ clb_status geometry_update(clb_handle* h, int* sealed, int* reopened) {
     if (sealed) *sealed = (int)cnt[0];
     if (reopened) *reopened = (int)cnt[1];
     if (cnt[0] == 0 && cnt[1] == 0) return CLB_OK;
+    h->ca_full = true;  // the automaton's next mask pass looks at the whole changed map
     if (!h->d_mat_flow) {
         // from now on the flow lattice has a map of its own: the one before the first change
         h->h_mat_flow = h->h_mat;
