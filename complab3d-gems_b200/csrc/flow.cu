@@ -308,9 +308,9 @@ __global__ void __launch_bounds__(TILE, sizeof(TS) == 8 ? 2 : 4)
                 r += wl;
             }
         }
+        fence_async_smem();  // this thread's writes to the tile, ordered before the bulk stores read it
         __syncthreads();
         if (tid == 0) {
-            fence_async_smem();
             for (int i = 0; i < 19; ++i) bulk_s2g(f + (int64_t)i * KS + (int64_t)t * TILE, buf + i * TILE, row_bytes);
             bulk_commit();
         }

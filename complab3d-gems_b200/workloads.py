@@ -122,12 +122,12 @@ def pack256cube_8species(scale=1, seed=1003, gen=None):
                 flow_max_iterations=100000)
 
 
-# Flow iterations per transport iteration of the 256^3 coupled configuration: the re-solve's
-# collide-and-stream calls over its 500-iteration interval, as measured on one B200 over the
-# configuration's 10,000 iterations (10,255 flow iterations; bench.py's headline reports the run's
-# own figure). The CPU baseline weights its flow and transport samples by it so that both arms
-# time the same mix of work.
-FLOW_PER_TRANSPORT_CONFIG3 = 1.03
+# Flow iterations per transport iteration of the 256^3 coupled configuration: the re-solves'
+# collide-and-stream calls over the configuration's 10,000 iterations, as measured on one B200
+# (7,106 flow iterations: the first in-loop re-solve fills the tracer's window, the later ones
+# find the flow settled; bench.py's headline reports the run's own figure). The CPU baseline weights
+# its flow and transport samples by it so that both arms time the same mix of work.
+FLOW_PER_TRANSPORT_CONFIG3 = 0.711
 
 
 def fracture192_carbonate(gen, scale=1.0, seed=1004):
