@@ -158,6 +158,9 @@ SIGNATURES = {
     "clb_set_thermo_gate": [C.c_void_p, C.POINTER(ThermoDesc)],
     "clb_set_symbolic_kinetics": [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int, C.c_char_p],
     "clb_symbolic_eval": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)],
+    "clb_set_graph_network": [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int],
+    "clb_graph_network_eval": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int),
+                               C.POINTER(C.c_long)],
     "clb_write_vti": [C.c_void_p, C.c_int, C.c_int, C.c_char_p],
     "clb_checkpoint_save": [C.c_void_p, C.c_char_p, C.c_int],
     "clb_checkpoint_load": [C.c_void_p, C.c_char_p],
@@ -526,6 +529,23 @@ class Domain:
         out = np.zeros((X.shape[0], nr.value))
         self._check(lib().clb_symbolic_eval(self.h, int(microbe), _ptr(X), X.shape[0], _ptr(out), C.byref(nr)))
         return out
+
+    def set_graph_network(self, path, species_names, microbe=-1):
+        """A rate law given as a .gnn graph network: microbe m's law, or the abiotic law for
+        microbe = -1; species_names name the handle's species in user order."""
+        arr = (C.c_char_p * len(species_names))(*[n.encode() for n in species_names])
+        self._check(lib().clb_set_graph_network(self.h, os.fsencode(path), C.cast(arr, C.c_void_p), int(microbe)))
+
+    def graph_network_eval(self, microbe, X):
+        """The bound network's outputs on the rows of X (concentrations in the file's species
+        order), evaluated on the device; returns (out [n][n_out], rows clamped to the training box)."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        no, nc = C.c_int(), C.c_long()
+        self._check(lib().clb_graph_network_eval(self.h, int(microbe), None, 0, None, C.byref(no), None))
+        out = np.zeros((X.shape[0], no.value))
+        self._check(lib().clb_graph_network_eval(self.h, int(microbe), _ptr(X), X.shape[0], _ptr(out), C.byref(no),
+                                                 C.byref(nc)))
+        return out, nc.value
 
     def checkpoint_save(self, path, flow=True, transport=True):
         """A restart file of the flow and/or transport lattices (FP64, exact)."""

@@ -60,10 +60,40 @@ __device__ __noinline__ void sym_biotic(const AdeParams& P, int n_mobile, const 
         req[s] = 0.0;
     }
     for (int m = 0; m < P.M; ++m) {
-        if (!((P.sym_mask >> m) & 1u)) continue;
+        const bool net = (P.gnn_mask >> m) & 1u;
+        if (!net && !((P.sym_mask >> m) & 1u)) continue;
         const double b = bio[(int64_t)m * N + nd];
         const double bm = b > THRD ? b : 0.0;
         if (!(bm > THRD)) continue;
+        if (net) {
+            // a graph network (run_graphnet3D, complab3d_processors_graphnet.hh:120-170): the
+            // concentrations of the species it was trained on in, a signed rate per species and
+            // a growth rate out; the same budget as a rate-law file
+            const GnnNet& G = P.gnn[m];
+            double x[GNN_MAX_S], y[GNN_MAX_S + 1];
+            for (int i = 0; i < G.nS; ++i) {
+                double xv = 0.0;
+#pragma unroll
+                for (int s = 0; s < NM; ++s)
+                    if (s == G.sp[i]) xv = C[s];
+                x[i] = xv;
+            }
+            gnn_eval(G, x, y);
+            const double ft = (m == 0 && P.gate_on) ? thermo_gate<double, NM>(P, C) : 1.0;
+            for (int i = 0; i < G.nS; ++i) {
+#pragma unroll
+                for (int s = 0; s < NM; ++s)
+                    if (s == G.sp[i]) req[s] += y[i] * ft * P.dt;
+            }
+            if (G.growth) {
+                double dB = y[G.nS] * ft * bm * P.dt;
+                if (dB > THRD || dB < -THRD) {
+                    if (dB + bm < 0.0) dB = -bm;
+                    bio[(int64_t)m * N + nd] += dB;
+                }
+            }
+            continue;
+        }
         const SymProg& S = P.sym[m];
         double x[SYM_MAX_VARS], y[SYM_MAX_RATES];
         for (int v = 0; v < S.n_vars; ++v) {
@@ -955,7 +985,8 @@ clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm,
     AdeParams& P = h->ap;
     const int S = h->S;
     P.law = law;
-    P.sym_mask = 0;  // a compiled law replaces the organisms' rate-law files
+    P.sym_mask = 0;  // a compiled law replaces the organisms' rate-law files and networks
+    P.gnn_mask = 0;
     std::memset(P.prm, 0, sizeof(P.prm));
     switch (law) {
         case CLB_LAW_DECAY:
@@ -1021,6 +1052,7 @@ clb_status ade_set_abiotic(clb_handle* h, int law, const double* prm, int nprm, 
             return fail(h, CLB_INVALID_ARG, "not an abiotic rate law");
     }
     P.law2 = law;
+    P.gnn_abiotic = 0;
     P.surf = surface_only ? 1 : 0;
     return geometry_refresh(h);
 }

@@ -116,6 +116,8 @@ clb_status clb_destroy(clb_handle* h) {
     cudaFree(h->d_mlp);
     cudaFree(h->d_mlp_bf16);
     cudaFree(h->d_sym);
+    cudaFree(h->d_gnn);
+    delete[] h->gnn_host;
     if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -286,6 +288,20 @@ clb_status clb_symbolic_eval(clb_handle* h, int microbe, const double* vars, int
     if (!h || (n > 0 && (!vars || !rates))) return fail(h, CLB_INVALID_ARG, "null argument");
     CLB_ON_DEVICE(h);
     return symbolic_eval(h, microbe, vars, n, rates, n_rates);
+}
+
+clb_status clb_set_graph_network(clb_handle* h, const char* gnn_path, const char* const* species_names,
+                                 int microbe) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    return graphnet_set(h, gnn_path, species_names, microbe);
+}
+
+clb_status clb_graph_network_eval(clb_handle* h, int microbe, const double* conc, int n, double* out, int* n_out,
+                                  long* n_clamped) {
+    if (!h || (n > 0 && (!conc || !out))) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return graphnet_eval(h, microbe, conc, n, out, n_out, n_clamped);
 }
 
 clb_status clb_ade_step(clb_handle* h, int n) {

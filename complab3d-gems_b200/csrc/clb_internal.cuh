@@ -10,6 +10,7 @@
 
 #include "../../include/clb.h"
 #include "symbolic.cuh"
+#include "graphnet.cuh"
 
 namespace clb {
 
@@ -156,6 +157,12 @@ struct AdeParams {
     // abiotic one at [CLB_MAX_MICROBES]; sym_mask: the microbes that have one
     const SymProg* sym;
     uint32_t sym_mask;
+    // graph networks read from .gnn files, in the same slots ([microbe], then the abiotic one);
+    // gnn_mask: the microbes whose law is a network (law CLB_LAW_SYMBOLIC), gnn_abiotic: the abiotic
+    // law (law2 CLB_LAW_SYMBOLIC) is a network
+    const GnnNet* gnn;
+    uint32_t gnn_mask;
+    int gnn_abiotic;
 };
 
 // Per-node state of the precipitation / dissolution machinery (geometry_update.cu), passed to the
@@ -206,6 +213,8 @@ struct clb_handle_s {
     int64_t launches = 0;             // kernels this handle enqueued on the coupled step's path
     void* d_sym = nullptr;            // SymProg[SYM_MAX_PROGS] on the device
     clb::SymProg sym_host[clb::SYM_MAX_PROGS];
+    void* d_gnn = nullptr;            // GnnNet[SYM_MAX_PROGS] on the device
+    clb::GnnNet* gnn_host = nullptr;  // host copies of the bound networks (SYM_MAX_PROGS, allocated on first use)
     std::vector<int8_t> h_mat;
     int8_t* d_mat = nullptr;
 
@@ -401,6 +410,9 @@ clb_status symbolic_set(clb_handle* h, const char* path, const char* const* spec
                         const char* microbe_name);
 clb_status symbolic_eval(clb_handle* h, int which, const double* vars, int n, double* rates, int* n_rates);
 void sym_eval_batch(clb_handle* h, int slot, const double* dvars, int n, double* drates);
+clb_status graphnet_set(clb_handle* h, const char* path, const char* const* species_names, int microbe);
+clb_status graphnet_eval(clb_handle* h, int which, const double* conc, int n, double* out, int* n_out,
+                         long* n_clamped);
 
 // speciation.cu
 clb_status speciation_setup(clb_handle* h, const clb_speciation_desc* d);

@@ -140,6 +140,24 @@ __device__ __forceinline__ void eval_rates2(const AdeParams& P, const double (&C
             if (s == b) R[s] -= r;
             if (s == q) R[s] += r;
         }
+    } else if (SYM && P.law2 == CLB_LAW_SYMBOLIC && P.gnn_abiotic) {
+        // an abiotic graph network (run_graphnet_abiotic3D, complab3d_processors_abiotic_learned.hh:
+        // 200-235): a rate per species it was trained on, no growth
+        const GnnNet& G = P.gnn[CLB_MAX_MICROBES];
+        double x[GNN_MAX_S], y[GNN_MAX_S + 1];
+        for (int i = 0; i < G.nS; ++i) {
+            double xv = 0.0;
+#pragma unroll
+            for (int s = 0; s < NB; ++s)
+                if (s == G.sp[i]) xv = C[s];
+            x[i] = xv;
+        }
+        gnn_eval(G, x, y);
+        for (int i = 0; i < G.nS; ++i) {
+#pragma unroll
+            for (int s = 0; s < NB; ++s)
+                if (s == G.sp[i]) R[s] += y[i];
+        }
     } else if (SYM && P.law2 == CLB_LAW_SYMBOLIC) {
         // an abiotic rate-law file: the extent and the species rates it derives, on the floored
         // concentrations (complab3d_processors_abiotic_learned.hh reads the same values)

@@ -403,9 +403,11 @@ clb_status symbolic_set(clb_handle* h, const char* path, const char* const* spec
     A.sym = static_cast<const SymProg*>(h->d_sym);
     if (abiotic) {
         A.law2 = CLB_LAW_SYMBOLIC;
+        A.gnn_abiotic = 0;
     } else {
         A.law = CLB_LAW_SYMBOLIC;
         A.sym_mask |= 1u << microbe;
+        A.gnn_mask &= ~(1u << microbe);  // an organism has one run-time law
     }
     return geometry_refresh(h);
 }
@@ -413,7 +415,7 @@ clb_status symbolic_set(clb_handle* h, const char* path, const char* const* spec
 clb_status symbolic_eval(clb_handle* h, int which, const double* vars, int n, double* rates, int* n_rates) {
     const int slot = which < 0 ? CLB_MAX_MICROBES : which;
     if (which >= CLB_MAX_MICROBES || (which >= 0 && !(h->ap.sym_mask >> which & 1u)) ||
-        (which < 0 && h->ap.law2 != CLB_LAW_SYMBOLIC))
+        (which < 0 && (h->ap.law2 != CLB_LAW_SYMBOLIC || h->ap.gnn_abiotic)))
         return fail(h, CLB_INVALID_ARG, "no rate-law file is bound there");
     const SymProg& P = h->sym_host[slot];
     if (n_rates) *n_rates = P.n_rates;

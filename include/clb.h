@@ -287,6 +287,35 @@ clb_status clb_set_symbolic_kinetics(clb_handle* h, const char* sym_path, const 
  * (may be NULL). */
 clb_status clb_symbolic_eval(clb_handle* h, int microbe, const double* vars, int n, double* rates, int* n_rates);
 
+/* A rate law given as a graph network read at run time from a .gnn file (the reference's
+ * complab3d_graphnet.hh format: a bipartite network over the species and reactions of the file's
+ * stoichiometric matrix, `rounds` rounds of message passing of width `width` with tanh layers,
+ * readout `species` or `extent`, an optional growth output, inputs clamped to trainmin..trainmax,
+ * per_hour rates divided by 3600), evaluated per voxel in FP64 inside the fused transport step.
+ * The file's species names are matched against species_names[S] (the handle's species, user
+ * order).
+ *   microbe >= 0: the law of the organism whose biomass field is `microbe`: where its biomass
+ *     exceeds 1e-12 the network's species rates are requested and its growth rate times the
+ *     biomass grows it; the requests of all organisms of a voxel (networks and .sym laws alike)
+ *     share each substrate's headroom, a draw never taking more than the voxel holds, and
+ *     production passing through (run_graphnet3D, complab3d_processors_graphnet.hh:70-200).
+ *   microbe = -1: an abiotic network (no growth output) in every reacting voxel, each increment
+ *     clamped at what the voxel holds (run_graphnet_abiotic3D,
+ *     complab3d_processors_abiotic_learned.hh:163-250).
+ * The time step is clb_set_kinetics's dt; a network replaces a .sym law bound to the same slot
+ * and the other way round. Networks of up to 8 species, 8 reactions, width 16 and 4 rounds.
+ * Replaces: complab_gnn::load / Network::eval / bindToSubstrates (complab3d_graphnet.hh:84-330,
+ * 402-600). */
+clb_status clb_set_graph_network(clb_handle* h, const char* gnn_path, const char* const* species_names,
+                                 int microbe);
+
+/* The bound network of `microbe` (-1: the abiotic one) on n rows of concentrations in the file's
+ * species order (conc [n][nS], host) into out [n][n_out] (host; the species rates, then growth when
+ * the file has it; units applied), evaluated on the device; *n_out receives the output count and
+ * *n_clamped the rows the training-box clamp changed (either may be NULL). */
+clb_status clb_graph_network_eval(clb_handle* h, int microbe, const double* conc, int n, double* out, int* n_out,
+                                  long* n_clamped);
+
 /* Biomass fields of the CA microbes, [n_microbes][N] float64. */
 clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass);
 

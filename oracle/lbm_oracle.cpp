@@ -374,6 +374,18 @@ struct SymLaw {
     std::vector<int> var_src, rate_dst;  // binding: species index (-1 biomass / growth / extent)
 };
 
+// ---- graph networks read from a .gnn file (complab3d_graphnet.hh restated; section below)
+struct GnnLaw {
+    int nS = 0, nR = 0, W = 0, rounds = 0;
+    bool extent = false, growth = false;
+    double unit = 1.0, xymin = -1.0, yymin = -1.0;
+    std::vector<std::string> species;
+    std::vector<double> S;  // nS x nR
+    std::vector<double> da, xiscale, xoff, xgain, yoff, ygain, tmin, tmax, Wenc, benc, Wout, bout;
+    std::vector<std::vector<double>> Wsr, Wss, Wrs, Wda, bR, bS;  // per round
+    std::vector<int> sp;  // binding: species index of each network species
+};
+
 struct OrcAde {
     int nx, ny, nz, S, M;
     size_t N;
@@ -402,6 +414,9 @@ struct OrcAde {
     int law2 = LAW_NONE;
     std::vector<SymLaw> sym;             // [microbe] then the abiotic law at index 8
     unsigned sym_mask = 0;
+    std::vector<GnnLaw> gnn;             // graph networks in the same slots
+    unsigned gnn_mask = 0;
+    int gnn_abiotic = 0;
     std::vector<double> prm2;
     int surf = 0;
     // precipitation sealing and dissolution (precipitationVOP.hh, dissolutionVOP.hh)
@@ -738,6 +753,233 @@ void sym_rates(const SymLaw& L, const double* x, double* out) {
 }
 }  // namespace
 
+// Reads a .gnn file: keywords then their numbers; '#' comments and `provenance` to the end of the
+// line; `species` / `reactions` with their names on the rest of the line; the per-round arrays
+// after `layer l`. False on anything missing or unknown.
+bool gnn_load(const char* path, GnnLaw& G) {
+    G = GnnLaw();
+    std::FILE* f = std::fopen(path, "r");
+    if (!f) return false;
+    std::string text;
+    char buf[4096];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
+    std::fclose(f);
+    std::istringstream in(text);
+    auto read_n = [&](std::vector<double>& v, int n) {
+        v.assign((size_t)std::max(n, 0), 0.0);
+        for (auto& x : v)
+            if (!(in >> x)) return false;
+        return true;
+    };
+    int cur = -1;
+    bool stoich = false;
+    std::string k;
+    while (in >> k) {
+        if (k[0] == '#' || k == "provenance") {
+            std::string rest;
+            std::getline(in, rest);
+        } else if (k == "species" || k == "reactions") {
+            std::string rest, w;
+            std::getline(in, rest);
+            if (k == "species") {
+                std::istringstream ws(rest);
+                while (ws >> w) G.species.push_back(w);
+            }
+        } else if (k == "version") {
+            int v;
+            if (!(in >> v)) return false;
+        } else if (k == "units") {
+            std::string u;
+            in >> u;
+            for (auto& c : u) c = (char)std::tolower((unsigned char)c);
+            if (u == "per_hour") G.unit = 1.0 / 3600.0;
+            else if (u != "per_second") return false;
+        } else if (k == "rounds") {
+            if (!(in >> G.rounds)) return false;
+        } else if (k == "width") {
+            if (!(in >> G.W)) return false;
+        } else if (k == "growth") {
+            int v;
+            if (!(in >> v)) return false;
+            G.growth = v != 0;
+        } else if (k == "readout") {
+            std::string m;
+            in >> m;
+            for (auto& c : m) c = (char)std::tolower((unsigned char)c);
+            if (m == "extent") G.extent = true;
+            else if (m != "species") return false;
+        } else if (k == "stoich") {
+            if (!(in >> G.nS >> G.nR) || !read_n(G.S, G.nS * G.nR)) return false;
+            stoich = true;
+        } else if (!stoich) {
+            return false;
+        } else {
+            const int nys = G.extent ? (G.growth ? 1 : 0) : G.nS + (G.growth ? 1 : 0);
+            const int nh = G.growth ? 2 : 1;
+            bool ok = true;
+            if (k == "da") ok = read_n(G.da, G.nR);
+            else if (k == "xoffset") ok = read_n(G.xoff, G.nS);
+            else if (k == "xgain") ok = read_n(G.xgain, G.nS);
+            else if (k == "xymin") ok = (bool)(in >> G.xymin);
+            else if (k == "yoffset") ok = read_n(G.yoff, nys);
+            else if (k == "ygain") ok = read_n(G.ygain, nys);
+            else if (k == "xiscale") ok = read_n(G.xiscale, G.nR);
+            else if (k == "yymin") ok = (bool)(in >> G.yymin);
+            else if (k == "trainmin") ok = read_n(G.tmin, G.nS);
+            else if (k == "trainmax") ok = read_n(G.tmax, G.nS);
+            else if (k == "Wenc") ok = read_n(G.Wenc, G.W);
+            else if (k == "benc") ok = read_n(G.benc, G.W);
+            else if (k == "Wout") ok = read_n(G.Wout, nh * G.W);
+            else if (k == "bout") ok = read_n(G.bout, nh);
+            else if (k == "layer") {
+                ok = (bool)(in >> cur) && cur >= 0 && cur < G.rounds;
+                if (ok && G.Wsr.size() < (size_t)G.rounds) {
+                    G.Wsr.resize(G.rounds); G.Wss.resize(G.rounds); G.Wrs.resize(G.rounds);
+                    G.Wda.resize(G.rounds); G.bR.resize(G.rounds); G.bS.resize(G.rounds);
+                }
+            } else if (cur >= 0 && k == "Wsr") ok = read_n(G.Wsr[cur], G.W * G.W);
+            else if (cur >= 0 && k == "Wss") ok = read_n(G.Wss[cur], G.W * G.W);
+            else if (cur >= 0 && k == "Wrs") ok = read_n(G.Wrs[cur], G.W * G.W);
+            else if (cur >= 0 && k == "Wda") ok = read_n(G.Wda[cur], G.W);
+            else if (cur >= 0 && k == "bR") ok = read_n(G.bR[cur], G.W);
+            else if (cur >= 0 && k == "bS") ok = read_n(G.bS[cur], G.W);
+            else return false;
+            if (!ok) return false;
+        }
+    }
+    if (!stoich || G.W < 1 || G.rounds < 1 || (int)G.species.size() != G.nS) return false;
+    if ((int)G.Wsr.size() != G.rounds) return false;
+    for (int l = 0; l < G.rounds; ++l)
+        if (G.Wsr[l].empty() || G.Wss[l].empty() || G.Wrs[l].empty() || G.Wda[l].empty() || G.bR[l].empty() ||
+            G.bS[l].empty())
+            return false;
+    return (int)G.da.size() == G.nR && (int)G.tmin.size() == G.nS && (int)G.tmax.size() == G.nS &&
+           !G.Wenc.empty() && !G.bout.empty() && (!G.extent || (int)G.xiscale.size() == G.nR);
+}
+
+// The forward pass of complab_gnn::Network::eval (complab3d_graphnet.hh:215-332), restated: encode
+// each species node from its clamped, scaled concentration; per round, reaction nodes from the
+// stoichiometry-weighted species states, then species nodes from their own state and the weighted
+// reaction states; read the rates off the species nodes (SPECIES) or as extents off the reaction
+// nodes (EXTENT), and growth off the mean species node. Returns whether the clamp acted.
+bool gnn_rates(const GnnLaw& G, const double* c, double* out) {
+    const int W = G.W, nS = G.nS, nR = G.nR;
+    auto S = [&](int i, int r) { return G.S[(size_t)i * nR + r]; };
+    std::vector<std::vector<double>> hs(nS, std::vector<double>(W)), hr(nR, std::vector<double>(W));
+    bool clamped = false;
+    for (int i = 0; i < nS; ++i) {
+        const double ci = c[i] < G.tmin[i] ? G.tmin[i] : (c[i] > G.tmax[i] ? G.tmax[i] : c[i]);
+        clamped = clamped || ci != c[i];
+        const double x = (ci - G.xoff[i]) * G.xgain[i] + G.xymin;
+        for (int h = 0; h < W; ++h) hs[i][h] = std::tanh(x * G.Wenc[h] + G.benc[h]);
+    }
+    std::vector<double> msg(W);
+    for (int l = 0; l < G.rounds; ++l) {
+        for (int r = 0; r < nR; ++r) {
+            std::fill(msg.begin(), msg.end(), 0.0);
+            for (int i = 0; i < nS; ++i)
+                if (S(i, r) != 0.0)
+                    for (int k = 0; k < W; ++k) msg[k] += S(i, r) * hs[i][k];
+            for (int h = 0; h < W; ++h) {
+                double a = G.bR[l][h] + G.da[r] * G.Wda[l][h];
+                for (int k = 0; k < W; ++k) a += G.Wsr[l][(size_t)h * W + k] * msg[k];
+                hr[r][h] = std::tanh(a);
+            }
+        }
+        std::vector<std::vector<double>> next(nS, std::vector<double>(W));
+        for (int i = 0; i < nS; ++i) {
+            std::fill(msg.begin(), msg.end(), 0.0);
+            for (int r = 0; r < nR; ++r)
+                if (S(i, r) != 0.0)
+                    for (int k = 0; k < W; ++k) msg[k] += S(i, r) * hr[r][k];
+            for (int h = 0; h < W; ++h) {
+                double a = G.bS[l][h];
+                for (int k = 0; k < W; ++k)
+                    a += G.Wss[l][(size_t)h * W + k] * hs[i][k] + G.Wrs[l][(size_t)h * W + k] * msg[k];
+                next[i][h] = std::tanh(a);
+            }
+        }
+        hs.swap(next);
+    }
+    if (G.extent) {
+        std::vector<double> xi(nR);
+        for (int r = 0; r < nR; ++r) {
+            double y = G.bout[0];
+            for (int h = 0; h < W; ++h) y += G.Wout[h] * hr[r][h];
+            xi[r] = (y == y ? y : 0.0) * G.xiscale[r];
+        }
+        for (int i = 0; i < nS; ++i) {
+            double v = 0.0;
+            for (int r = 0; r < nR; ++r) v += S(i, r) * xi[r];
+            out[i] = v * G.unit;
+        }
+    } else {
+        for (int i = 0; i < nS; ++i) {
+            double y = G.bout[0];
+            for (int h = 0; h < W; ++h) y += G.Wout[h] * hs[i][h];
+            const double v = (y - G.yymin) / G.ygain[i] + G.yoff[i];
+            out[i] = (v == v ? v : 0.0) * G.unit;
+        }
+    }
+    if (G.growth) {
+        const int gs = G.extent ? 0 : nS;
+        double y = G.bout[1];
+        for (int h = 0; h < W; ++h) {
+            double sum = 0.0;
+            for (int i = 0; i < nS; ++i) sum += hs[i][h];
+            y += G.Wout[(size_t)W + h] * (sum / (double)nS);
+        }
+        const double v = (y - G.yymin) / G.ygain[gs] + G.yoff[gs];
+        out[nS] = (v == v ? v : 0.0) * G.unit;
+    }
+    return clamped;
+}
+
+extern "C" {
+
+// standalone evaluation of a .gnn file on n rows of concentrations (the pinning test's entry point)
+int orc_gnn_eval(const char* path, int n, const double* conc, double* out, int* n_out) {
+    GnnLaw G;
+    if (!gnn_load(path, G)) return -1;
+    const int no = G.nS + (G.growth ? 1 : 0);
+    *n_out = no;
+    for (int i = 0; i < n; ++i) gnn_rates(G, conc + (size_t)i * G.nS, out + (size_t)i * no);
+    return 0;
+}
+
+// binds a .gnn file to the species (names: S newline-separated names) as microbe m's law (m >= 0)
+// or the abiotic law (m = -1)
+int orc_ade_set_graph_network(OrcAde* A, const char* path, const char* names, int m) {
+    GnnLaw G;
+    if (!gnn_load(path, G)) return -1;
+    std::vector<std::string> sp;
+    std::istringstream in(names);
+    std::string w;
+    while (std::getline(in, w)) sp.push_back(w);
+    for (const std::string& v : G.species) {
+        int hit = -1;
+        for (size_t s = 0; s < sp.size(); ++s) if (sp[s] == v) hit = (int)s;
+        if (hit < 0) return -2;
+        G.sp.push_back(hit);
+    }
+    if (m < 0 && G.growth) return -3;
+    if (A->gnn.size() < 9) A->gnn.resize(9);
+    if (m >= 0) {
+        A->gnn[(size_t)m] = G;
+        A->gnn_mask |= 1u << m;
+        A->sym_mask &= ~(1u << m);
+        A->law = LAW_SYMBOLIC;
+    } else {
+        A->gnn[8] = G;
+        A->gnn_abiotic = 1;
+        A->law2 = LAW_SYMBOLIC;
+    }
+    return 0;
+}
+
+}  // extern "C"
+
 extern "C" {
 
 // standalone evaluation of a file on n rows of its variables (the pinning test's entry point)
@@ -775,9 +1017,11 @@ int orc_ade_set_symbolic(OrcAde* A, const char* path, const char* names, int m, 
     if (m >= 0) {
         A->sym[(size_t)m] = L;
         A->sym_mask |= 1u << m;
+        A->gnn_mask &= ~(1u << m);
         A->law = LAW_SYMBOLIC;
     } else {
         A->sym[8] = L;
+        A->gnn_abiotic = 0;
         A->law2 = LAW_SYMBOLIC;
     }
     return 0;
@@ -830,6 +1074,13 @@ static void rates2(const OrcAde* A, const double* C, double* R) {
         R[a] -= r;
         R[b] -= r;
         R[q] += r;
+    } else if (A->law2 == LAW_SYMBOLIC && A->gnn_abiotic) {
+        // run_graphnet_abiotic3D (complab3d_processors_abiotic_learned.hh:200-235)
+        const GnnLaw& G = A->gnn[8];
+        std::vector<double> x((size_t)G.nS), y((size_t)G.nS + 1);
+        for (int i = 0; i < G.nS; ++i) x[(size_t)i] = C[G.sp[(size_t)i]];
+        gnn_rates(G, x.data(), y.data());
+        for (int i = 0; i < G.nS; ++i) R[G.sp[(size_t)i]] += y[(size_t)i];
     } else if (A->law2 == LAW_SYMBOLIC) {
         const SymLaw& L = A->sym[8];
         std::vector<double> x(L.vars.size()), y(L.rates.size());
@@ -1014,9 +1265,27 @@ static void symbolic_voxel(const OrcAde* A, const double* C, const double* B, do
     std::vector<double> req(S, 0.0), x, y;
     for (int m = 0; m < A->M; ++m) {
         dB[m] = 0.0;
-        if (!((A->sym_mask >> m) & 1u)) continue;
+        const bool net = (A->gnn_mask >> m) & 1u;
+        if (!net && !((A->sym_mask >> m) & 1u)) continue;
         const double bm = B[m] > THRD ? B[m] : 0.0;
         if (!(bm > THRD)) continue;
+        if (net) {
+            // run_graphnet3D (complab3d_processors_graphnet.hh:120-200): the same budget
+            const GnnLaw& G = A->gnn[(size_t)m];
+            std::vector<double> xg((size_t)G.nS), yg((size_t)G.nS + 1);
+            for (int i = 0; i < G.nS; ++i) xg[(size_t)i] = C[G.sp[(size_t)i]];
+            gnn_rates(G, xg.data(), yg.data());
+            const double ft = (m == 0 && A->gate_on) ? thermo_factor(A, C) : 1.0;
+            for (int i = 0; i < G.nS; ++i) req[(size_t)G.sp[(size_t)i]] += yg[(size_t)i] * ft * A->dt;
+            if (G.growth) {
+                double d = yg[(size_t)G.nS] * ft * bm * A->dt;
+                if (d > THRD || d < -THRD) {
+                    if (d + bm < 0.0) d = -bm;
+                    dB[m] = d;
+                }
+            }
+            continue;
+        }
         const SymLaw& L = A->sym[(size_t)m];
         x.resize(L.vars.size());
         y.resize(L.rates.size());

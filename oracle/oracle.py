@@ -74,6 +74,8 @@ def lib():
             "orc_sphere_pack": ([ip, ip, ip, dp, dp, dp, C.c_uint64, C.c_char_p, ip, ip, ip, vp], ip),
             "orc_sym_eval": ([C.c_char_p, ip, vp, vp, C.POINTER(C.c_int)], ip),
             "orc_ade_set_symbolic": ([vp, C.c_char_p, C.c_char_p, ip, C.c_char_p], ip),
+            "orc_gnn_eval": ([C.c_char_p, ip, vp, vp, C.POINTER(C.c_int)], ip),
+            "orc_ade_set_graph_network": ([vp, C.c_char_p, C.c_char_p, ip], ip),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -104,6 +106,17 @@ def sym_eval(path, X, n_rates_max=16):
     if lib().orc_sym_eval(os.fsencode(path), X.shape[0], _p(X), _p(out), C.byref(nr)) != 0:
         raise ValueError(f"cannot load {path}")
     return out[:X.shape[0] * nr.value].reshape(X.shape[0], nr.value)
+
+
+def gnn_eval(path, X, n_out_max=17):
+    """The oracle's evaluation of a .gnn graph network on the rows of X (concentrations in the
+    file's species order): the species rates, then growth when the file has it."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.zeros(X.shape[0] * n_out_max)
+    no = C.c_int()
+    if lib().orc_gnn_eval(os.fsencode(path), X.shape[0], _p(X), _p(out), C.byref(no)) != 0:
+        raise ValueError(f"cannot load {path}")
+    return out[:X.shape[0] * no.value].reshape(X.shape[0], no.value)
 
 
 def set_threads(n):
@@ -247,6 +260,12 @@ class OracleAde:
                                         microbe_name.encode())
         if rc != 0:
             raise ValueError(f"cannot bind {path}")
+
+    def set_graph_network(self, path, names, microbe=-1):
+        """A .gnn graph network bound to the species `names` (microbe m's law, or abiotic for -1)."""
+        rc = lib().orc_ade_set_graph_network(self.h, os.fsencode(path), "\n".join(names).encode(), int(microbe))
+        if rc != 0:
+            raise ValueError(f"cannot bind {path} ({rc})")
 
     def set_abiotic(self, law, params, surface_only=0):
         p = np.ascontiguousarray(params, dtype=np.float64)
