@@ -9,8 +9,9 @@
 // (tau 0.8, ns_max_iT 100000, ns_converge_iT1 1e-8 / iT2 1e-6, update intervals 1, unit um), the
 // boundary-type words (Dirichlet, Neumann, closed / noflux / no_flux / wall, any case), nx counting
 // interior planes (two ghost planes are added), Pe = 0 when delta_P is below 1e-14, a biofilm
-// viscosity ratio n giving the permeability ratio 1/n. Rate laws are compiled code in the reference
-// (defineRxnKinetics); here they are chosen after set-up with clb_set_kinetics.
+// viscosity ratio n giving the permeability ratio 1/n. Compiled rate laws (the reference's
+// defineRxnKinetics) are chosen after set-up with clb_set_kinetics; the run-time ones the file names
+// (<symbolic> .sym laws, <graphnet> networks, per the organisms' reaction_type) are bound at set-up.
 #include "../../include/clb.h"
 
 #include <algorithm>
@@ -144,6 +145,9 @@ struct Microbe {
     std::vector<int> codes;               // biofilm material numbers
     std::vector<double> b0;               // initial density per material number
     double visc_ratio = 0;                // viscosity_ratio_in_biofilm (permeability ratio 1/n)
+    int rxn = 1;                          // reaction_type: 0 none, 1 kinetics (a compiled law the host
+                                          // chooses), 8 a .sym law, 9 a .gnn network
+    std::string sym_file;                 // <microbeN><expressions_file>: its own .sym law
 };
 
 }  // namespace
@@ -173,6 +177,9 @@ struct clb_case_s {
     std::vector<std::string> components;
     std::vector<std::vector<double>> stoich;
     std::vector<double> logk;
+    // run-time rate laws: <symbolic> (.sym files) and <graphnet> (.gnn networks)
+    bool sym_on = false, gnn_on = false;
+    std::string sym_file, sym_abiotic, gnn_file, gnn_abiotic;
     // precipitation (one phase)
     bool prc_on = false;
     int prc_sub = -1, prc_interval = 1, prc_surface = 1;
@@ -364,6 +371,28 @@ void parse(clb_case_s& c, const XNode& root) {
             throw std::runtime_error("the material numbers and initial_densities of " + bn + " differ in length");
         if (!read_num(n->child("viscosity_ratio_in_biofilm"), M.visc_ratio))
             throw std::runtime_error("<" + bn + "> needs viscosity_ratio_in_biofilm (a cellular-automaton microbe)");
+        // reaction_type (rxntype::parse, complab3d_metabolic.hh:207-236; kinetics when absent)
+        std::string rt;
+        if (read_str(n->child("reaction_type"), rt)) {
+            const std::string r = lower(rt);
+            if (r == "none" || r == "no" || r == "0") M.rxn = 0;
+            else if (r == "kinetics" || r == "kns" || r == "1") M.rxn = 1;
+            else if (r == "symbolic" || r == "sym" || r == "sym_law" || r == "rate_law" || r == "8") M.rxn = 8;
+            else if (r == "graphnet" || r == "gnn" || r == "graph_network" || r == "graph" || r == "9") M.rxn = 9;
+            else if (r == "symbolic_and_kinetics" || r == "symbolic+kinetics" || r == "10" ||
+                     r == "graphnet_and_kinetics" || r == "graphnet+kinetics" || r == "11")
+                throw std::runtime_error("<" + bn + ">: reaction_type " + rt +
+                                         " (a run-time law and a compiled one on the same organism) is not on this path");
+            else if (r == "glpk" || r == "fba" || r == "fba_glpk" || r == "cobrapy" || r == "cpy" ||
+                     r == "fba_cobrapy" || r == "surrogate" || r == "srg" || r == "ann" || r == "2" || r == "3" ||
+                     r == "4" || r == "5" || r == "6" || r == "7" || r.find("_and_kinetics") != std::string::npos ||
+                     r.find("+kinetics") != std::string::npos)
+                throw std::runtime_error("<" + bn + ">: reaction_type " + rt +
+                                         " (flux balance or its surrogate) is not on this path");
+            else
+                throw std::runtime_error("<" + bn + ">: reaction_type " + rt + " is not defined");
+        }
+        read_str(n->child("expressions_file"), M.sym_file);
         c.mic.push_back(M);
     }
     if (nm > 0) {
@@ -380,6 +409,37 @@ void parse(clb_case_s& c, const XNode& root) {
         }
     }
     // equilibrium (complab.cpp:614-723)
+    // run-time rate laws (complab3d_integration.hh:263-313): one .sym file for every symbolic
+    // organism unless the organism names its own, one .gnn network for every graphnet organism, and
+    // an abiotic file of either kind
+    read_bool(at(root, {"symbolic", "enabled"}), c.sym_on);
+    if (c.sym_on) {
+        read_str(at(root, {"symbolic", "expressions_file"}), c.sym_file);
+        read_str(at(root, {"symbolic", "abiotic_file"}), c.sym_abiotic);
+    }
+    read_bool(at(root, {"graphnet", "enabled"}), c.gnn_on);
+    if (c.gnn_on) {
+        read_str(at(root, {"graphnet", "network_file"}), c.gnn_file);
+        read_str(at(root, {"graphnet", "abiotic_file"}), c.gnn_abiotic);
+        if (c.gnn_file.empty() && c.gnn_abiotic.empty())
+            throw std::runtime_error("<graphnet> is enabled but neither <network_file> nor <abiotic_file> is set");
+    }
+    for (size_t m = 0; m < c.mic.size(); ++m) {
+        const Microbe& M = c.mic[m];
+        if (M.rxn == 8 && (!c.sym_on || (c.sym_file.empty() && M.sym_file.empty())))
+            throw std::runtime_error("microbe" + std::to_string(m) +
+                                     " has reaction_type symbolic but <symbolic> names no file for it");
+        if (M.rxn == 9 && (!c.gnn_on || c.gnn_file.empty()))
+            throw std::runtime_error("microbe" + std::to_string(m) +
+                                     " has reaction_type graphnet but <graphnet> names no network_file");
+    }
+    if (c.sym_on && c.sym_file.empty() && c.sym_abiotic.empty()) {
+        bool any = false;
+        for (const Microbe& M : c.mic) any = any || !M.sym_file.empty();
+        if (!any) throw std::runtime_error("<symbolic> is enabled but neither <expressions_file> nor <abiotic_file> is set");
+    }
+    if (c.sym_on && !c.sym_abiotic.empty() && c.gnn_on && !c.gnn_abiotic.empty())
+        throw std::runtime_error("<symbolic> and <graphnet> both name an abiotic file; a run has one abiotic law");
     read_bool(at(root, {"equilibrium", "enabled"}), c.eq_on);
     if (c.eq_on) {
         std::string comp;
@@ -427,7 +487,10 @@ void parse(clb_case_s& c, const XNode& root) {
         const std::string p = "microbe." + std::to_string(m) + ".";
         v[p + "code"] = c.mic[m].codes[0];
         v[p + "perm_ratio"] = c.mic[m].visc_ratio > 1e-14 ? 1.0 / c.mic[m].visc_ratio : 0.0;
+        v[p + "reaction_type"] = c.mic[m].rxn;
     }
+    v["symbolic"] = c.sym_on;
+    v["graphnet"] = c.gnn_on;
 }
 
 // The relaxation rates and the time step (complab.cpp:1221-1253). Substrate 0's pore diffusivity is
@@ -653,6 +716,31 @@ clb_status clb_case_setup(clb_case* c, int flow_precision, int ade_precision, cl
         cd.seed = 1;
         cd.push_mode = c->ca_half ? CLB_PUSH_HALF : CLB_PUSH_FRACTION;
         if ((st = clb_ca_setup(h, &cd)) != CLB_OK) return bad(st);
+    }
+    // run-time rate laws, bound to the substrates by name (files beside the XML): every symbolic
+    // organism its .sym law, every graphnet organism the network, then the abiotic law
+    if (!sd.empty() && (c->sym_on || c->gnn_on)) {
+        std::vector<const char*> names;
+        for (const Species& S : c->sp) names.push_back(S.name.c_str());
+        for (size_t m = 0; m < c->mic.size(); ++m) {
+            const Microbe& M = c->mic[m];
+            if (M.rxn == 8) {
+                const std::string f = join_path(c->xml_dir, M.sym_file.empty() ? c->sym_file : M.sym_file);
+                if ((st = clb_set_symbolic_kinetics(h, f.c_str(), names.data(), (int)m, M.name.c_str())) != CLB_OK)
+                    return bad(st);
+            } else if (M.rxn == 9) {
+                const std::string f = join_path(c->xml_dir, c->gnn_file);
+                if ((st = clb_set_graph_network(h, f.c_str(), names.data(), (int)m)) != CLB_OK) return bad(st);
+            }
+        }
+        if (c->sym_on && !c->sym_abiotic.empty()) {
+            const std::string f = join_path(c->xml_dir, c->sym_abiotic);
+            if ((st = clb_set_symbolic_kinetics(h, f.c_str(), names.data(), -1, "")) != CLB_OK) return bad(st);
+        }
+        if (c->gnn_on && !c->gnn_abiotic.empty()) {
+            const std::string f = join_path(c->xml_dir, c->gnn_abiotic);
+            if ((st = clb_set_graph_network(h, f.c_str(), names.data(), -1)) != CLB_OK) return bad(st);
+        }
     }
     // equilibrium chemistry: rows are the substrates, columns the named components
     if (c->eq_on) {

@@ -37,10 +37,25 @@ def biofilm_flow_map(clb):
     return m
 
 
+def graphnet_duct_map():
+    nx, ny, nz = 18, 10, 9
+    m = np.full((nx, ny, nz), 2, np.int8)
+    m[:, 0, :] = m[:, -1, :] = 1
+    m[:, :, 0] = m[:, :, -1] = 1
+    m[5:7, 3:6, 2:5] = 1
+    m[11:13, 5:8, 4:7] = 0
+    m[8:11, 2:5, 3:7] = 3  # the biofilm patch
+    return m
+
+
 def run_dir(tmp, name, inner):
     d = os.path.join(str(tmp), name)
     os.makedirs(os.path.join(d, "input"), exist_ok=True)
     shutil.copy(os.path.join(HERE, name + ".xml"), os.path.join(d, "CompLaB.xml"))
-    fname = {"carbonate_duct": "duct.dat", "biofilm_flow": "pack.dat"}[name]
+    fname = {"carbonate_duct": "duct.dat", "biofilm_flow": "pack.dat", "graphnet_duct": "duct.dat"}[name]
     write_dat(os.path.join(d, "input", fname), inner)
+    if name == "graphnet_duct":
+        gnn = os.path.join(os.path.dirname(HERE), "gnn")
+        shutil.copy(os.path.join(gnn, "extent_growth.gnn"), os.path.join(d, "input", "organism.gnn"))
+        shutil.copy(os.path.join(gnn, "abiotic_extent.gnn"), os.path.join(d, "input", "abiotic.gnn"))
     return os.path.join(d, "CompLaB.xml")

@@ -77,6 +77,29 @@ def test_errors_are_reported(clb, tmp_path, old, new, msg):
         clb.Case(xml)
 
 
+@pytest.mark.parametrize("old,new,msg", [
+    ("<reaction_type>graphnet</reaction_type>", "<reaction_type>glpk</reaction_type>", "flux balance"),
+    ("<reaction_type>graphnet</reaction_type>", "<reaction_type>graphnet_and_kinetics</reaction_type>",
+     "a run-time law and a compiled one"),
+    ("<reaction_type>graphnet</reaction_type>", "<reaction_type>quantum</reaction_type>", "is not defined"),
+    ("<network_file>input/organism.gnn</network_file>", "", "names no network_file"),
+    ("<enabled>true</enabled>", "<enabled>false</enabled>", "names no network_file"),
+])
+def test_rate_law_errors_are_reported(clb, tmp_path, old, new, msg):
+    xml = case_files.run_dir(tmp_path, "graphnet_duct", case_files.graphnet_duct_map())
+    text = open(xml).read()
+    assert old in text
+    open(xml, "w").write(text.replace(old, new))
+    with pytest.raises(clb.ClbError, match=msg):
+        clb.Case(xml)
+
+
+def test_rate_law_blocks_parse(clb, tmp_path):
+    xml = case_files.run_dir(tmp_path, "graphnet_duct", case_files.graphnet_duct_map())
+    c = clb.Case(xml)
+    assert c.get("graphnet") == 1 and c.get("symbolic") == 0 and c.get("microbe.0.reaction_type") == 9
+
+
 def test_reference_examples_parse(clb):
     """Every CompLaB.xml the reference ships whose run lies on this path parses with its own
     values (checked when the reference checkout is named by CLB_REFERENCE_SRC)."""
@@ -91,7 +114,8 @@ def test_reference_examples_parse(clb):
         except clb.ClbError as e:
             # microbes solved by finite differences or LBM are not on this path, nor are files
             # that leave out what a run off this path does not need
-            assert "cellular-automaton" in str(e) or "FD" in str(e) or "missing" in str(e) or "needs" in str(e), (f, e)
+            assert "cellular-automaton" in str(e) or "FD" in str(e) or "missing" in str(e) or "needs" in str(e) \
+                or "flux balance" in str(e), (f, e)
             continue
         assert c.get("nx") >= 3 and c.get("n_substrates") >= 0
         parsed += 1

@@ -86,3 +86,35 @@ def test_biofilm_flow_case_sets_up_like_the_reference(clb, oracle, tmp_path):
     rep = c.run(D)
     assert rep["iterations"] == 60 and rep["flow_resolves"] >= 0
     assert np.isfinite(D.concentration(0)).all() and D.biomass(0).sum() > b0
+
+
+def test_graphnet_case_binds_its_networks(clb, tmp_path):
+    """reaction_type graphnet and the <graphnet> block: the case binds the organism's network and
+    the abiotic one at set-up (files beside the XML), and its run equals a run of the same case
+    with the block switched off and the two networks bound by hand, bit for bit."""
+    import os
+    xml = case_files.run_dir(tmp_path, "graphnet_duct", case_files.graphnet_duct_map())
+    c = clb.Case(xml)
+    assert c.get("graphnet") == 1 and c.get("microbe.0.reaction_type") == 9
+    D = c.setup(clb.F64, clb.F64)
+    out, _ = D.graph_network_eval(0, np.full((1, 4), 0.3))
+    assert out.shape == (1, 5)
+    rep = c.run(D)
+    assert rep["iterations"] == 80
+    # the same description with the block off, networks bound through the library's entry points
+    text = open(xml).read().replace("<enabled>true</enabled>", "<enabled>false</enabled>").replace(
+        "<reaction_type>graphnet</reaction_type>", "<reaction_type>kinetics</reaction_type>")
+    xml2 = os.path.join(os.path.dirname(xml), "manual.xml")
+    open(xml2, "w").write(text)
+    c2 = clb.Case(xml2)
+    assert c2.get("graphnet") == 0
+    D2 = c2.setup(clb.F64, clb.F64)
+    inp = os.path.join(os.path.dirname(xml), "input")
+    D2.set_graph_network(os.path.join(inp, "organism.gnn"), ["A", "B", "C", "D"], 0)
+    D2.set_graph_network(os.path.join(inp, "abiotic.gnn"), ["A", "B", "C", "D"], -1)
+    c2.run(D2)
+    for s in range(4):
+        np.testing.assert_array_equal(D.concentration(s), D2.concentration(s))
+    np.testing.assert_array_equal(D.biomass(0), D2.biomass(0))
+    b0 = case_files.graphnet_duct_map()
+    assert np.abs(D.biomass(0)).sum() != 60.0 * (b0 == 3).sum()  # the network grew or decayed it
