@@ -89,6 +89,11 @@ class ThermoDesc(C.Structure):
                 ("gas_constant", C.c_double), ("conc_scale", C.c_double)]
 
 
+class SurrogateDesc(C.Structure):
+    _fields_ = [("half_saturation", C.c_double * MAX_SPECIES), ("max_uptake_flux", C.c_double * MAX_SPECIES),
+                ("biomass_molar_mass", C.c_double), ("decay", C.c_double)]
+
+
 class PrecipDesc(C.Structure):
     _fields_ = [("mineral_species", C.c_int32), ("full_density", C.c_double), ("precip_code", C.c_int32),
                 ("seal_flow", C.c_int32), ("seal_perm_ratio", C.c_double), ("flow_max_iterations", C.c_int32),
@@ -159,6 +164,9 @@ SIGNATURES = {
     "clb_set_symbolic_kinetics": [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int, C.c_char_p],
     "clb_symbolic_eval": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)],
     "clb_set_graph_network": [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int],
+    "clb_set_surrogate_organism": [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int, C.c_void_p],
+    "clb_surrogate_eval": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int),
+                           C.POINTER(C.c_long)],
     "clb_graph_network_eval": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int),
                                C.POINTER(C.c_long)],
     "clb_write_vti": [C.c_void_p, C.c_int, C.c_int, C.c_char_p],
@@ -545,6 +553,32 @@ class Domain:
         out = np.zeros((X.shape[0], no.value))
         self._check(lib().clb_graph_network_eval(self.h, int(microbe), _ptr(X), X.shape[0], _ptr(out), C.byref(no),
                                                  C.byref(nc)))
+        return out, nc.value
+
+    def set_surrogate_organism(self, path, species_names, microbe, half_saturation, max_uptake_flux,
+                               biomass_molar_mass, decay):
+        """Microbe `microbe` as a surrogate organism: a .srg network fed with its Michaelis-Menten
+        uptake estimates (half_saturation, max_uptake_flux per species in user order)."""
+        S = len(species_names)
+        d = SurrogateDesc()
+        for s in range(S):
+            d.half_saturation[s] = float(half_saturation[s])
+            d.max_uptake_flux[s] = float(max_uptake_flux[s])
+        d.biomass_molar_mass = float(biomass_molar_mass)
+        d.decay = float(decay)
+        arr = (C.c_char_p * S)(*[n.encode() for n in species_names])
+        self._check(lib().clb_set_surrogate_organism(self.h, os.fsencode(path), C.cast(arr, C.c_void_p),
+                                                     int(microbe), C.cast(C.byref(d), C.c_void_p)))
+
+    def surrogate_eval(self, microbe, X):
+        """Every output of the bound surrogate network on the rows of X (its inputs), by the device;
+        returns (out [n][n_out], rows clamped to the training box)."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        no, nc = C.c_int(), C.c_long()
+        self._check(lib().clb_surrogate_eval(self.h, int(microbe), None, 0, None, C.byref(no), None))
+        out = np.zeros((X.shape[0], no.value))
+        self._check(lib().clb_surrogate_eval(self.h, int(microbe), _ptr(X), X.shape[0], _ptr(out), C.byref(no),
+                                             C.byref(nc)))
         return out, nc.value
 
     def checkpoint_save(self, path, flow=True, transport=True):

@@ -61,10 +61,52 @@ __device__ __noinline__ void sym_biotic(const AdeParams& P, int n_mobile, const 
     }
     for (int m = 0; m < P.M; ++m) {
         const bool net = (P.gnn_mask >> m) & 1u;
-        if (!net && !((P.sym_mask >> m) & 1u)) continue;
+        const bool srg = (P.srg_mask >> m) & 1u;
+        if (!net && !srg && !((P.sym_mask >> m) & 1u)) continue;
         const double b = bio[(int64_t)m * N + nd];
         const double bm = b > THRD ? b : 0.0;
         if (!(bm > THRD)) continue;
+        if (srg) {
+            // a surrogate organism (run_surrogate3D, complab3d_processors_surrogate.hh:155-250, with
+            // the run-time network of surrogateModel.hh): Michaelis-Menten uptake estimates in, the
+            // growth rate out; the estimates are what it draws
+            const SrgNet& Q = P.srg[m];
+            double fin[NM];
+#pragma unroll
+            for (int s = 0; s < NM; ++s) {
+                fin[s] = 0.0;
+                if (s >= P.S) continue;
+                const double av = C[s];
+                const double mm = (Q.kc[s] + av > 0.0) ? av / (Q.kc[s] + av) : 0.0;
+                const double cap = -srg_exhaustion(av, bm, Q.mw, P.dt);  // >= 0
+                double v = Q.vmax[s] > THRD ? Q.vmax[s] * mm : cap * mm;
+                if (cap > 0.0 && v > cap) v = cap;
+                fin[s] = v;
+            }
+            double x[SRG_MAX_IN], y[SRG_MAX_W];
+            for (int i = 0; i < Q.nIn; ++i) {
+                double xv = 0.0;
+#pragma unroll
+                for (int s = 0; s < NM; ++s)
+                    if (s == Q.subs[i]) xv = fin[s];
+                x[i] = xv;
+            }
+            srg_eval(Q, x, y);
+            double mu = y[0];
+            const double ft = (m == 0 && P.gate_on) ? thermo_gate<double, NM>(P, C) : 1.0;
+            if (ft < 1.0) {
+#pragma unroll
+                for (int s = 0; s < NM; ++s) fin[s] *= ft;
+                mu *= ft;
+            }
+            double dB = (fabs(mu) < THRD) ? -Q.kd * bm * P.dt : mu * bm * P.dt / 3600.0;
+            if (dB + bm < 0.0) dB = -bm;
+            if (dB > THRD || dB < -THRD) bio[(int64_t)m * N + nd] += dB;
+#pragma unroll
+            for (int s = 0; s < NM; ++s)
+                if (s < P.S) req[s] += -(fin[s] * (bm * Q.mw) * P.dt / 3.6e6);
+            continue;
+        }
         if (net) {
             // a graph network (run_graphnet3D, complab3d_processors_graphnet.hh:120-170): the
             // concentrations of the species it was trained on in, a signed rate per species and
@@ -987,6 +1029,7 @@ clb_status ade_set_kinetics(clb_handle* h, int law, const double* prm, int nprm,
     P.law = law;
     P.sym_mask = 0;  // a compiled law replaces the organisms' rate-law files and networks
     P.gnn_mask = 0;
+    P.srg_mask = 0;
     std::memset(P.prm, 0, sizeof(P.prm));
     switch (law) {
         case CLB_LAW_DECAY:

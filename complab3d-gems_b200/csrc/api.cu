@@ -118,6 +118,8 @@ clb_status clb_destroy(clb_handle* h) {
     cudaFree(h->d_sym);
     cudaFree(h->d_gnn);
     delete[] h->gnn_host;
+    cudaFree(h->d_srg);
+    delete[] h->srg_host;
     if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -302,6 +304,20 @@ clb_status clb_graph_network_eval(clb_handle* h, int microbe, const double* conc
     if (!h || (n > 0 && (!conc || !out))) return fail(h, CLB_INVALID_ARG, "null argument");
     CLB_ON_DEVICE(h);
     return graphnet_eval(h, microbe, conc, n, out, n_out, n_clamped);
+}
+
+clb_status clb_set_surrogate_organism(clb_handle* h, const char* srg_path, const char* const* species_names,
+                                      int microbe, const clb_surrogate_desc* desc) {
+    if (!h) return fail(nullptr, CLB_INVALID_ARG, "null handle");
+    CLB_ON_DEVICE(h);
+    return srg_set(h, srg_path, species_names, microbe, desc);
+}
+
+clb_status clb_surrogate_eval(clb_handle* h, int microbe, const double* x, int n, double* out, int* n_out,
+                              long* n_clamped) {
+    if (!h || (n > 0 && (!x || !out))) return fail(h, CLB_INVALID_ARG, "null argument");
+    CLB_ON_DEVICE(h);
+    return srg_eval_host(h, microbe, x, n, out, n_out, n_clamped);
 }
 
 clb_status clb_ade_step(clb_handle* h, int n) {

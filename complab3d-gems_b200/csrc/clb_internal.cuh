@@ -11,6 +11,7 @@
 #include "../../include/clb.h"
 #include "symbolic.cuh"
 #include "graphnet.cuh"
+#include "srgnet.cuh"
 
 namespace clb {
 
@@ -163,6 +164,10 @@ struct AdeParams {
     const GnnNet* gnn;
     uint32_t gnn_mask;
     int gnn_abiotic;
+    // surrogate organisms (.srg networks with their uptake parameters, [microbe]); srg_mask: the
+    // microbes that are one (law CLB_LAW_SYMBOLIC)
+    const SrgNet* srg;
+    uint32_t srg_mask;
 };
 
 // Per-node state of the precipitation / dissolution machinery (geometry_update.cu), passed to the
@@ -215,6 +220,8 @@ struct clb_handle_s {
     clb::SymProg sym_host[clb::SYM_MAX_PROGS];
     void* d_gnn = nullptr;            // GnnNet[SYM_MAX_PROGS] on the device
     clb::GnnNet* gnn_host = nullptr;  // host copies of the bound networks (SYM_MAX_PROGS, allocated on first use)
+    void* d_srg = nullptr;            // SrgNet[CLB_MAX_MICROBES] on the device
+    clb::SrgNet* srg_host = nullptr;  // host copies of the bound surrogates (CLB_MAX_MICROBES, on first use)
     std::vector<int8_t> h_mat;
     int8_t* d_mat = nullptr;
 
@@ -412,6 +419,10 @@ clb_status symbolic_eval(clb_handle* h, int which, const double* vars, int n, do
 void sym_eval_batch(clb_handle* h, int slot, const double* dvars, int n, double* drates);
 clb_status graphnet_set(clb_handle* h, const char* path, const char* const* species_names, int microbe);
 clb_status graphnet_eval(clb_handle* h, int which, const double* conc, int n, double* out, int* n_out,
+                         long* n_clamped);
+clb_status srg_set(clb_handle* h, const char* path, const char* const* species_names, int microbe,
+                   const clb_surrogate_desc* d);
+clb_status srg_eval_host(clb_handle* h, int microbe, const double* x, int n, double* out, int* n_out,
                          long* n_clamped);
 
 // speciation.cu

@@ -268,6 +268,7 @@ clb_status graphnet_set(clb_handle* h, const char* path, const char* const* spec
         A.law = CLB_LAW_SYMBOLIC;
         A.gnn_mask |= 1u << microbe;
         A.sym_mask &= ~(1u << microbe);  // an organism has one run-time law
+        A.srg_mask &= ~(1u << microbe);
     }
     return geometry_refresh(h);
 }

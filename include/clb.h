@@ -316,6 +316,43 @@ clb_status clb_set_graph_network(clb_handle* h, const char* gnn_path, const char
 clb_status clb_graph_network_eval(clb_handle* h, int microbe, const double* conc, int n, double* out, int* n_out,
                                   long* n_clamped);
 
+/* The uptake parameters of a surrogate organism, per species in user order: half-saturation
+ * constants Kc (mol/L) and maximum uptake fluxes (mmol/gDW/h; 0: none, the flux that would exhaust
+ * the voxel in one step stands in), the biomass molar mass (gDW/mol) and the decay coefficient
+ * (1/s) that acts where the network predicts no growth. */
+typedef struct {
+    double half_saturation[CLB_MAX_SPECIES];
+    double max_uptake_flux[CLB_MAX_SPECIES];
+    double biomass_molar_mass;
+    double decay;
+} clb_surrogate_desc;
+
+/* A surrogate organism: the growth rate of the organism whose biomass field is `microbe` from a
+ * feed-forward network read at run time from a .srg file (the reference's complab3d_surrogate.hh
+ * format: mapminmax scaling, tansig hidden layers, a linear output layer, output 0 the growth rate
+ * in 1/h, optionally as log10; inputs clamped to trainmin..trainmax), fed, as the reference's
+ * default surrogate model feeds it, with the organism's Michaelis-Menten uptake estimates of the
+ * substrates the file names (inputnames matched against species_names[S], user order; a file
+ * without names takes the substrates in order). Where its biomass B exceeds 1e-12: every
+ * substrate's estimate v = vmax C/(Kc + C) (without vmax the one-step exhaustion flux
+ * C 3.6e6/(B MW dt), capped at 1e4, times C/(Kc + C)), never above that exhaustion flux; growth
+ * mu B dt/3600, or decay kd B dt where |mu| < 1e-12; the substrates drawn by v B MW dt/3.6e6 under
+ * the shared headroom budget of the voxel's run-time organisms. The time step (seconds) is
+ * clb_set_kinetics's dt. A surrogate replaces a .sym law or a network bound to the same organism.
+ * Networks of up to 8 inputs, 4 layers and 32 units a layer.
+ * Replaces: run_surrogate3D (complab3d_processors_surrogate.hh:96-293) with surrogateModel.hh's
+ * run-time network (complab_srg::load / Network::eval / evalBound, complab3d_surrogate.hh:117-258,
+ * 380-470, 1029-1049) and MetabolicConfig's unit chain (complab3d_metabolic.hh:554-595). */
+clb_status clb_set_surrogate_organism(clb_handle* h, const char* srg_path, const char* const* species_names,
+                                      int microbe, const clb_surrogate_desc* desc);
+
+/* The bound surrogate network of `microbe` on n rows of its inputs (x [n][n_inputs], host) into
+ * out [n][n_out] (host; every output, output 0 the growth rate with its log and floor), after the
+ * training-box clamp, evaluated on the device; *n_out receives the output count and *n_clamped the
+ * rows the clamp changed (either may be NULL). */
+clb_status clb_surrogate_eval(clb_handle* h, int microbe, const double* x, int n, double* out, int* n_out,
+                              long* n_clamped);
+
 /* Biomass fields of the CA microbes, [n_microbes][N] float64. */
 clb_status clb_set_biomass(clb_handle* h, int n_microbes, const double* biomass);
 

@@ -386,6 +386,20 @@ struct GnnLaw {
     std::vector<int> sp;  // binding: species index of each network species
 };
 
+// ---- surrogate organisms: .srg networks (complab3d_surrogate.hh restated; section below)
+struct SrgLaw {
+    int nIn = 0;
+    std::vector<int> sizes;
+    std::vector<std::vector<double>> W, B;
+    std::vector<double> xoff, xgain, tmin, tmax, yoff, ygain;
+    double xymin = -1.0, yymin = -1.0;
+    bool logout = false;
+    std::vector<std::string> inputs;
+    std::vector<int> subs;            // binding: species index of each input
+    std::vector<double> kc, vmax;     // per species
+    double mw = 1.0, kd = 0.0;
+};
+
 struct OrcAde {
     int nx, ny, nz, S, M;
     size_t N;
@@ -417,6 +431,8 @@ struct OrcAde {
     std::vector<GnnLaw> gnn;             // graph networks in the same slots
     unsigned gnn_mask = 0;
     int gnn_abiotic = 0;
+    std::vector<SrgLaw> srg;             // surrogate organisms [microbe]
+    unsigned srg_mask = 0;
     std::vector<double> prm2;
     int surf = 0;
     // precipitation sealing and dissolution (precipitationVOP.hh, dissolutionVOP.hh)
@@ -936,6 +952,152 @@ bool gnn_rates(const GnnLaw& G, const double* c, double* out) {
     return clamped;
 }
 
+// Reads a .srg file (keywords, '#' comments, `layers` / `inputnames` / `outputnames` / `yoffset` /
+// `ygain` / `outrange` on the rest of their line, `W l` and `B l` blocks); false on anything
+// missing.
+bool srg_load(const char* path, SrgLaw& Q) {
+    Q = SrgLaw();
+    std::FILE* f = std::fopen(path, "r");
+    if (!f) return false;
+    std::string text;
+    char buf[4096];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
+    std::fclose(f);
+    std::istringstream in(text);
+    auto rest = [&]() {
+        std::string r;
+        std::getline(in, r);
+        std::istringstream ws(r);
+        std::vector<std::string> w;
+        std::string t;
+        while (ws >> t) w.push_back(t);
+        return w;
+    };
+    auto nums = [&](std::vector<double>& v, int n) {
+        v.assign((size_t)std::max(n, 0), 0.0);
+        for (auto& x : v)
+            if (!(in >> x)) return false;
+        return true;
+    };
+    std::string k;
+    while (in >> k) {
+        if (k[0] == '#') { rest(); continue; }
+        if (k == "version") { int v; if (!(in >> v)) return false; }
+        else if (k == "inputs") { if (!(in >> Q.nIn)) return false; }
+        else if (k == "layers") { Q.sizes.clear(); for (auto& w : rest()) Q.sizes.push_back(std::atoi(w.c_str())); }
+        else if (k == "logoutput") { int v; if (!(in >> v)) return false; Q.logout = v != 0; }
+        else if (k == "inputnames") Q.inputs = rest();
+        else if (k == "outputnames" || k == "outrange") rest();
+        else if (k == "xoffset") { if (!nums(Q.xoff, Q.nIn)) return false; }
+        else if (k == "xgain") { if (!nums(Q.xgain, Q.nIn)) return false; }
+        else if (k == "trainmin") { if (!nums(Q.tmin, Q.nIn)) return false; }
+        else if (k == "trainmax") { if (!nums(Q.tmax, Q.nIn)) return false; }
+        else if (k == "xymin") { if (!(in >> Q.xymin)) return false; }
+        else if (k == "yymin") { if (!(in >> Q.yymin)) return false; }
+        else if (k == "outputs") { int v; if (!(in >> v)) return false; }
+        else if (k == "yoffset" || k == "ygain") {
+            std::vector<double>& v = k == "yoffset" ? Q.yoff : Q.ygain;
+            v.clear();
+            for (auto& w : rest()) v.push_back(std::atof(w.c_str()));
+        } else if (k == "W" || k == "B") {
+            int L;
+            if (!(in >> L) || L < 0 || L + 1 >= (int)Q.sizes.size()) return false;
+            if ((int)Q.W.size() < L + 1) { Q.W.resize(L + 1); Q.B.resize(L + 1); }
+            const int rows = Q.sizes[L + 1], cols = Q.sizes[L];
+            if (!nums(k == "W" ? Q.W[L] : Q.B[L], k == "W" ? rows * cols : rows)) return false;
+        } else return false;
+    }
+    const int nL = (int)Q.sizes.size() - 1;
+    if (Q.nIn <= 0 || nL < 1 || (int)Q.W.size() != nL || (int)Q.B.size() != nL) return false;
+    for (int l = 0; l < nL; ++l)
+        if ((int)Q.W[l].size() != Q.sizes[l + 1] * Q.sizes[l] || (int)Q.B[l].size() != Q.sizes[l + 1]) return false;
+    if ((int)Q.tmin.size() < Q.nIn || (int)Q.tmax.size() < Q.nIn) return false;
+    const int nO = Q.sizes.back();
+    Q.yoff.resize((size_t)nO, 0.0);
+    if ((int)Q.ygain.size() < nO) Q.ygain.resize((size_t)nO, 1.0);
+    return true;
+}
+
+// Network::evalAll (complab3d_surrogate.hh:200-235) after evalBound's clamp (:1029-1049), restated:
+// every output; returns whether the clamp acted
+bool srg_outputs(const SrgLaw& Q, const double* x, double* out) {
+    std::vector<double> a((size_t)Q.nIn);
+    bool clamped = false;
+    for (int i = 0; i < Q.nIn; ++i) {
+        double v = x[i];
+        if (v < Q.tmin[i]) { v = Q.tmin[i]; clamped = true; }
+        else if (v > Q.tmax[i]) { v = Q.tmax[i]; clamped = true; }
+        a[(size_t)i] = (v - Q.xoff[i]) * Q.xgain[i] + Q.xymin;
+    }
+    const size_t nL = Q.W.size();
+    for (size_t l = 0; l < nL; ++l) {
+        const int rows = Q.sizes[l + 1], cols = Q.sizes[l];
+        std::vector<double> o((size_t)rows);
+        for (int r = 0; r < rows; ++r) {
+            double t = Q.B[l][(size_t)r];
+            for (int c = 0; c < cols; ++c) t += Q.W[l][(size_t)r * cols + c] * a[(size_t)c];
+            o[(size_t)r] = (l + 1 == nL) ? t : 2.0 / (1.0 + std::exp(-2.0 * t)) - 1.0;
+        }
+        a.swap(o);
+    }
+    const int nO = Q.sizes.back();
+    for (int k = 0; k < nO; ++k) {
+        const double gain = Q.ygain[k] != 0.0 ? Q.ygain[k] : 1.0;
+        out[k] = (a[(size_t)k] - Q.yymin) / gain + Q.yoff[k];
+    }
+    if (Q.logout) out[0] = std::pow(10.0, out[0]);
+    if (!(out[0] > 1e-8)) out[0] = 0.0;
+    for (int k = 1; k < nO; ++k)
+        if (out[k] != out[k]) out[k] = 0.0;
+    return clamped;
+}
+
+extern "C" {
+
+// standalone evaluation of a .srg file on n rows of its inputs, clamped to its training box
+int orc_srg_eval(const char* path, int n, const double* x, double* out, int* n_out) {
+    SrgLaw Q;
+    if (!srg_load(path, Q)) return -1;
+    const int no = Q.sizes.back();
+    *n_out = no;
+    for (int i = 0; i < n; ++i) srg_outputs(Q, x + (size_t)i * Q.nIn, out + (size_t)i * no);
+    return 0;
+}
+
+// binds a .srg file to the species (names: S newline-separated) as microbe m's surrogate, with its
+// uptake parameters per species (kc, vmax), biomass molar mass and decay coefficient
+int orc_ade_set_surrogate(OrcAde* A, const char* path, const char* names, int m, const double* kc,
+                          const double* vmax, double mw, double kd) {
+    SrgLaw Q;
+    if (!srg_load(path, Q) || m < 0) return -1;
+    std::vector<std::string> sp;
+    std::istringstream in(names);
+    std::string w;
+    while (std::getline(in, w)) sp.push_back(w);
+    for (int i = 0; i < Q.nIn; ++i) {
+        int hit = -1;
+        if (Q.inputs.empty()) hit = i < (int)sp.size() ? i : -1;
+        else
+            for (size_t s = 0; s < sp.size(); ++s) if (sp[s] == Q.inputs[(size_t)i]) hit = (int)s;
+        if (hit < 0) return -2;
+        Q.subs.push_back(hit);
+    }
+    Q.kc.assign(kc, kc + A->S);
+    Q.vmax.assign(vmax, vmax + A->S);
+    Q.mw = mw;
+    Q.kd = kd;
+    if ((int)A->srg.size() < 8) A->srg.resize(8);
+    A->srg[(size_t)m] = Q;
+    A->srg_mask |= 1u << m;
+    A->sym_mask &= ~(1u << m);
+    A->gnn_mask &= ~(1u << m);
+    A->law = LAW_SYMBOLIC;
+    return 0;
+}
+
+}  // extern "C"
+
 extern "C" {
 
 // standalone evaluation of a .gnn file on n rows of concentrations (the pinning test's entry point)
@@ -969,6 +1131,7 @@ int orc_ade_set_graph_network(OrcAde* A, const char* path, const char* names, in
         A->gnn[(size_t)m] = G;
         A->gnn_mask |= 1u << m;
         A->sym_mask &= ~(1u << m);
+        A->srg_mask &= ~(1u << m);
         A->law = LAW_SYMBOLIC;
     } else {
         A->gnn[8] = G;
@@ -1018,6 +1181,7 @@ int orc_ade_set_symbolic(OrcAde* A, const char* path, const char* names, int m, 
         A->sym[(size_t)m] = L;
         A->sym_mask |= 1u << m;
         A->gnn_mask &= ~(1u << m);
+        A->srg_mask &= ~(1u << m);
         A->law = LAW_SYMBOLIC;
     } else {
         A->sym[8] = L;
@@ -1266,9 +1430,46 @@ static void symbolic_voxel(const OrcAde* A, const double* C, const double* B, do
     for (int m = 0; m < A->M; ++m) {
         dB[m] = 0.0;
         const bool net = (A->gnn_mask >> m) & 1u;
-        if (!net && !((A->sym_mask >> m) & 1u)) continue;
+        const bool srg = (A->srg_mask >> m) & 1u;
+        if (!net && !srg && !((A->sym_mask >> m) & 1u)) continue;
         const double bm = B[m] > THRD ? B[m] : 0.0;
         if (!(bm > THRD)) continue;
+        if (srg) {
+            // run_surrogate3D (complab3d_processors_surrogate.hh:155-250) with the run-time network:
+            // Michaelis-Menten uptake estimates (MetabolicConfig's unit chain,
+            // complab3d_metabolic.hh:554-595) feed the network; its growth rate (or decay) moves the
+            // biomass; the estimates are drawn from the substrates
+            const SrgLaw& Q = A->srg[(size_t)m];
+            std::vector<double> fin((size_t)S, 0.0);
+            for (int s = 0; s < S; ++s) {
+                const double av = C[s];
+                const double mm = (Q.kc[(size_t)s] + av > 0.0) ? av / (Q.kc[(size_t)s] + av) : 0.0;
+                double exh = 0.0;
+                const double denom = bm * Q.mw * A->dt;
+                if (denom > 1e-30) {
+                    exh = -av * 3.6e6 / denom;
+                    if (exh < -1e4) exh = -1e4;
+                }
+                double v = Q.vmax[(size_t)s] > THRD ? Q.vmax[(size_t)s] * mm : -exh * mm;
+                const double cap = -exh;
+                if (cap > 0.0 && v > cap) v = cap;
+                fin[(size_t)s] = v;
+            }
+            std::vector<double> xs((size_t)Q.nIn), ys((size_t)Q.sizes.back());
+            for (int i = 0; i < Q.nIn; ++i) xs[(size_t)i] = fin[(size_t)Q.subs[(size_t)i]];
+            srg_outputs(Q, xs.data(), ys.data());
+            double mu = ys[0];
+            const double ft = (m == 0 && A->gate_on) ? thermo_factor(A, C) : 1.0;
+            if (ft < 1.0) {
+                for (auto& v : fin) v *= ft;
+                mu *= ft;
+            }
+            double d = (std::fabs(mu) < THRD) ? -Q.kd * bm * A->dt : mu * bm * A->dt / 3600.0;
+            if (d + bm < 0.0) d = -bm;
+            if (d > THRD || d < -THRD) dB[m] = d;
+            for (int s = 0; s < S; ++s) req[(size_t)s] += -(fin[(size_t)s] * (bm * Q.mw) * A->dt / 3.6e6);
+            continue;
+        }
         if (net) {
             // run_graphnet3D (complab3d_processors_graphnet.hh:120-200): the same budget
             const GnnLaw& G = A->gnn[(size_t)m];

@@ -76,6 +76,8 @@ def lib():
             "orc_ade_set_symbolic": ([vp, C.c_char_p, C.c_char_p, ip, C.c_char_p], ip),
             "orc_gnn_eval": ([C.c_char_p, ip, vp, vp, C.POINTER(C.c_int)], ip),
             "orc_ade_set_graph_network": ([vp, C.c_char_p, C.c_char_p, ip], ip),
+            "orc_srg_eval": ([C.c_char_p, ip, vp, vp, C.POINTER(C.c_int)], ip),
+            "orc_ade_set_surrogate": ([vp, C.c_char_p, C.c_char_p, ip, vp, vp, dp, dp], ip),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -115,6 +117,17 @@ def gnn_eval(path, X, n_out_max=17):
     out = np.zeros(X.shape[0] * n_out_max)
     no = C.c_int()
     if lib().orc_gnn_eval(os.fsencode(path), X.shape[0], _p(X), _p(out), C.byref(no)) != 0:
+        raise ValueError(f"cannot load {path}")
+    return out[:X.shape[0] * no.value].reshape(X.shape[0], no.value)
+
+
+def srg_eval(path, X, n_out_max=32):
+    """The oracle's evaluation of a .srg surrogate network on the rows of X (its inputs), clamped to
+    its training box: every output, output 0 the growth rate."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.zeros(X.shape[0] * n_out_max)
+    no = C.c_int()
+    if lib().orc_srg_eval(os.fsencode(path), X.shape[0], _p(X), _p(out), C.byref(no)) != 0:
         raise ValueError(f"cannot load {path}")
     return out[:X.shape[0] * no.value].reshape(X.shape[0], no.value)
 
@@ -264,6 +277,15 @@ class OracleAde:
     def set_graph_network(self, path, names, microbe=-1):
         """A .gnn graph network bound to the species `names` (microbe m's law, or abiotic for -1)."""
         rc = lib().orc_ade_set_graph_network(self.h, os.fsencode(path), "\n".join(names).encode(), int(microbe))
+        if rc != 0:
+            raise ValueError(f"cannot bind {path} ({rc})")
+
+    def set_surrogate(self, path, names, microbe, half_saturation, max_uptake_flux, biomass_molar_mass, decay):
+        """Microbe `microbe` as a surrogate organism (.srg network, uptake parameters per species)."""
+        self._srg = [np.ascontiguousarray(half_saturation, dtype=np.float64),
+                     np.ascontiguousarray(max_uptake_flux, dtype=np.float64)]
+        rc = lib().orc_ade_set_surrogate(self.h, os.fsencode(path), "\n".join(names).encode(), int(microbe),
+                                         _p(self._srg[0]), _p(self._srg[1]), float(biomass_molar_mass), float(decay))
         if rc != 0:
             raise ValueError(f"cannot bind {path} ({rc})")
 
