@@ -146,8 +146,11 @@ struct Microbe {
     std::vector<double> b0;               // initial density per material number
     double visc_ratio = 0;                // viscosity_ratio_in_biofilm (permeability ratio 1/n)
     int rxn = 1;                          // reaction_type: 0 none, 1 kinetics (a compiled law the host
-                                          // chooses), 8 a .sym law, 9 a .gnn network
+                                          // chooses), 3 a .srg surrogate, 8 a .sym law, 9 a .gnn network
     std::string sym_file;                 // <microbeN><expressions_file>: its own .sym law
+    // a surrogate organism's uptake parameters (complab3d_metabolic.hh:814-960)
+    std::vector<double> kc, vmax;         // half_saturation_constants, (fba_)maximum_uptake_flux
+    double mw = 24.6, kd = 0.0;           // biomass_molar_mass (default 24.6), decay_coefficient (1/s)
 };
 
 }  // namespace
@@ -178,8 +181,9 @@ struct clb_case_s {
     std::vector<std::vector<double>> stoich;
     std::vector<double> logk;
     // run-time rate laws: <symbolic> (.sym files) and <graphnet> (.gnn networks)
-    bool sym_on = false, gnn_on = false;
-    std::string sym_file, sym_abiotic, gnn_file, gnn_abiotic;
+    bool sym_on = false, gnn_on = false, srg_on = false;
+    std::string sym_file, sym_abiotic, gnn_file, gnn_abiotic, srg_file;
+    int srg_microbe = -1;                 // <surrogate><microbe>: the one organism, -1 every surrogate one
     // precipitation (one phase)
     bool prc_on = false;
     int prc_sub = -1, prc_interval = 1, prc_surface = 1;
@@ -383,16 +387,24 @@ void parse(clb_case_s& c, const XNode& root) {
                      r == "graphnet_and_kinetics" || r == "graphnet+kinetics" || r == "11")
                 throw std::runtime_error("<" + bn + ">: reaction_type " + rt +
                                          " (a run-time law and a compiled one on the same organism) is not on this path");
+            else if (r == "surrogate" || r == "srg" || r == "ann" || r == "3") M.rxn = 3;
             else if (r == "glpk" || r == "fba" || r == "fba_glpk" || r == "cobrapy" || r == "cpy" ||
-                     r == "fba_cobrapy" || r == "surrogate" || r == "srg" || r == "ann" || r == "2" || r == "3" ||
-                     r == "4" || r == "5" || r == "6" || r == "7" || r.find("_and_kinetics") != std::string::npos ||
-                     r.find("+kinetics") != std::string::npos)
+                     r == "fba_cobrapy" || r == "2" || r == "4" || r == "5" || r == "6" || r == "7" ||
+                     r.find("_and_kinetics") != std::string::npos || r.find("+kinetics") != std::string::npos)
                 throw std::runtime_error("<" + bn + ">: reaction_type " + rt +
-                                         " (flux balance or its surrogate) is not on this path");
+                                         " (a flux-balance linear program, or one with a compiled law) is not on this path");
             else
                 throw std::runtime_error("<" + bn + ">: reaction_type " + rt + " is not defined");
         }
         read_str(n->child("expressions_file"), M.sym_file);
+        if (M.rxn == 3) {
+            read_vec(n->child("half_saturation_constants"), M.kc);
+            if (!read_vec(n->child("fba_maximum_uptake_flux"), M.vmax)) read_vec(n->child("maximum_uptake_flux"), M.vmax);
+            for (double& v : M.vmax) v = std::fabs(v);
+            read_num(n->child("biomass_molar_mass"), M.mw);
+            read_num(n->child("decay_coefficient"), M.kd);
+            if (!(M.mw > 0)) throw std::runtime_error("<" + bn + "> needs a positive biomass_molar_mass");
+        }
         c.mic.push_back(M);
     }
     if (nm > 0) {
@@ -417,6 +429,12 @@ void parse(clb_case_s& c, const XNode& root) {
         read_str(at(root, {"symbolic", "expressions_file"}), c.sym_file);
         read_str(at(root, {"symbolic", "abiotic_file"}), c.sym_abiotic);
     }
+    read_bool(at(root, {"surrogate", "enabled"}), c.srg_on);
+    if (c.srg_on) {
+        read_str(at(root, {"surrogate", "weights_file"}), c.srg_file);
+        read_int(at(root, {"surrogate", "microbe"}), c.srg_microbe);
+        if (c.srg_file.empty()) throw std::runtime_error("<surrogate> is enabled but <weights_file> is not set");
+    }
     read_bool(at(root, {"graphnet", "enabled"}), c.gnn_on);
     if (c.gnn_on) {
         read_str(at(root, {"graphnet", "network_file"}), c.gnn_file);
@@ -429,6 +447,12 @@ void parse(clb_case_s& c, const XNode& root) {
         if (M.rxn == 8 && (!c.sym_on || (c.sym_file.empty() && M.sym_file.empty())))
             throw std::runtime_error("microbe" + std::to_string(m) +
                                      " has reaction_type symbolic but <symbolic> names no file for it");
+        if (M.rxn == 3 && (!c.srg_on || (c.srg_microbe >= 0 && c.srg_microbe != (int)m)))
+            throw std::runtime_error("microbe" + std::to_string(m) +
+                                     " has reaction_type surrogate but <surrogate> names no weights_file for it");
+        if (M.rxn == 3 && (M.kc.size() != c.sp.size() || (!M.vmax.empty() && M.vmax.size() != c.sp.size())))
+            throw std::runtime_error("microbe" + std::to_string(m) +
+                                     ": half_saturation_constants and maximum_uptake_flux need one value per substrate");
         if (M.rxn == 9 && (!c.gnn_on || c.gnn_file.empty()))
             throw std::runtime_error("microbe" + std::to_string(m) +
                                      " has reaction_type graphnet but <graphnet> names no network_file");
@@ -491,6 +515,7 @@ void parse(clb_case_s& c, const XNode& root) {
     }
     v["symbolic"] = c.sym_on;
     v["graphnet"] = c.gnn_on;
+    v["surrogate"] = c.srg_on;
 }
 
 // The relaxation rates and the time step (complab.cpp:1221-1253). Substrate 0's pore diffusivity is
@@ -719,7 +744,7 @@ clb_status clb_case_setup(clb_case* c, int flow_precision, int ade_precision, cl
     }
     // run-time rate laws, bound to the substrates by name (files beside the XML): every symbolic
     // organism its .sym law, every graphnet organism the network, then the abiotic law
-    if (!sd.empty() && (c->sym_on || c->gnn_on)) {
+    if (!sd.empty() && (c->sym_on || c->gnn_on || c->srg_on)) {
         std::vector<const char*> names;
         for (const Species& S : c->sp) names.push_back(S.name.c_str());
         for (size_t m = 0; m < c->mic.size(); ++m) {
@@ -728,6 +753,17 @@ clb_status clb_case_setup(clb_case* c, int flow_precision, int ade_precision, cl
                 const std::string f = join_path(c->xml_dir, M.sym_file.empty() ? c->sym_file : M.sym_file);
                 if ((st = clb_set_symbolic_kinetics(h, f.c_str(), names.data(), (int)m, M.name.c_str())) != CLB_OK)
                     return bad(st);
+            } else if (M.rxn == 3) {
+                const std::string f = join_path(c->xml_dir, c->srg_file);
+                clb_surrogate_desc q;
+                std::memset(&q, 0, sizeof q);
+                for (size_t s = 0; s < c->sp.size(); ++s) {
+                    q.half_saturation[s] = M.kc[s];
+                    q.max_uptake_flux[s] = M.vmax.empty() ? 0.0 : M.vmax[s];
+                }
+                q.biomass_molar_mass = M.mw;
+                q.decay = M.kd;
+                if ((st = clb_set_surrogate_organism(h, f.c_str(), names.data(), (int)m, &q)) != CLB_OK) return bad(st);
             } else if (M.rxn == 9) {
                 const std::string f = join_path(c->xml_dir, c->gnn_file);
                 if ((st = clb_set_graph_network(h, f.c_str(), names.data(), (int)m)) != CLB_OK) return bad(st);

@@ -55,7 +55,29 @@ def run_dir(tmp, name, inner):
     fname = {"carbonate_duct": "duct.dat", "biofilm_flow": "pack.dat", "graphnet_duct": "duct.dat"}[name]
     write_dat(os.path.join(d, "input", fname), inner)
     if name == "graphnet_duct":
+        shutil.copy(os.path.join(os.path.dirname(HERE), "srg", "uptake_growth.srg"), os.path.join(d, "input", "organism.srg"))
         gnn = os.path.join(os.path.dirname(HERE), "gnn")
         shutil.copy(os.path.join(gnn, "extent_growth.gnn"), os.path.join(d, "input", "organism.gnn"))
         shutil.copy(os.path.join(gnn, "abiotic_extent.gnn"), os.path.join(d, "input", "abiotic.gnn"))
     return os.path.join(d, "CompLaB.xml")
+
+
+def surrogate_case(tmp, inner):
+    """The graph-network duct with its organism turned into a surrogate organism: reaction_type
+    surrogate, a <surrogate> block naming input/organism.srg, the uptake parameters in the microbe
+    block; the abiotic network stays."""
+    xml = run_dir(tmp, "graphnet_duct", inner)
+    text = open(xml).read()
+    text = text.replace("<network_file>input/organism.gnn</network_file>", "")
+    text = text.replace("<graphnet>", "<surrogate>\n        <enabled>true</enabled>\n"
+                        "        <weights_file>input/organism.srg</weights_file>\n    </surrogate>\n    <graphnet>")
+    text = text.replace("<reaction_type>graphnet</reaction_type>",
+                        "<reaction_type>surrogate</reaction_type>\n"
+                        "            <half_saturation_constants>0.05 0.1 0.02 0.2</half_saturation_constants>\n"
+                        "            <fba_maximum_uptake_flux>10 5 0 0</fba_maximum_uptake_flux>\n"
+                        "            <biomass_molar_mass>24.6</biomass_molar_mass>\n"
+                        "            <decay_coefficient>2e-6</decay_coefficient>")
+    text = text.replace("<initial_densities>60</initial_densities>", "<initial_densities>0.03</initial_densities>")
+    out = os.path.join(os.path.dirname(xml), "surrogate.xml")
+    open(out, "w").write(text)
+    return out

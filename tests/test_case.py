@@ -78,7 +78,8 @@ def test_errors_are_reported(clb, tmp_path, old, new, msg):
 
 
 @pytest.mark.parametrize("old,new,msg", [
-    ("<reaction_type>graphnet</reaction_type>", "<reaction_type>glpk</reaction_type>", "flux balance"),
+    ("<reaction_type>graphnet</reaction_type>", "<reaction_type>glpk</reaction_type>", "linear program"),
+    ("<reaction_type>graphnet</reaction_type>", "<reaction_type>surrogate</reaction_type>", "no weights_file"),
     ("<reaction_type>graphnet</reaction_type>", "<reaction_type>graphnet_and_kinetics</reaction_type>",
      "a run-time law and a compiled one"),
     ("<reaction_type>graphnet</reaction_type>", "<reaction_type>quantum</reaction_type>", "is not defined"),
@@ -100,6 +101,11 @@ def test_rate_law_blocks_parse(clb, tmp_path):
     assert c.get("graphnet") == 1 and c.get("symbolic") == 0 and c.get("microbe.0.reaction_type") == 9
 
 
+def test_surrogate_case_parses(clb, tmp_path):
+    c = clb.Case(case_files.surrogate_case(tmp_path, case_files.graphnet_duct_map()))
+    assert c.get("surrogate") == 1 and c.get("microbe.0.reaction_type") == 3
+
+
 def test_reference_examples_parse(clb):
     """Every CompLaB.xml the reference ships whose run lies on this path parses with its own
     values (checked when the reference checkout is named by CLB_REFERENCE_SRC)."""
@@ -115,7 +121,7 @@ def test_reference_examples_parse(clb):
             # microbes solved by finite differences or LBM are not on this path, nor are files
             # that leave out what a run off this path does not need
             assert "cellular-automaton" in str(e) or "FD" in str(e) or "missing" in str(e) or "needs" in str(e) \
-                or "flux balance" in str(e), (f, e)
+                or "linear program" in str(e), (f, e)
             continue
         assert c.get("nx") >= 3 and c.get("n_substrates") >= 0
         parsed += 1

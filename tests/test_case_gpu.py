@@ -118,3 +118,34 @@ def test_graphnet_case_binds_its_networks(clb, tmp_path):
     np.testing.assert_array_equal(D.biomass(0), D2.biomass(0))
     b0 = case_files.graphnet_duct_map()
     assert np.abs(D.biomass(0)).sum() != 60.0 * (b0 == 3).sum()  # the network grew or decayed it
+
+
+def test_surrogate_case_binds_its_network(clb, tmp_path):
+    """reaction_type surrogate and the <surrogate> block: the case binds the organism's .srg network
+    with the microbe block's uptake parameters (half-saturation constants, fba_maximum_uptake_flux,
+    biomass_molar_mass, decay_coefficient), and its run equals the same case with the organism bound
+    by hand, bit for bit."""
+    import os
+    xml = case_files.surrogate_case(tmp_path, case_files.graphnet_duct_map())
+    c = clb.Case(xml)
+    D = c.setup(clb.F64, clb.F64)
+    out, _ = D.surrogate_eval(0, np.full((1, 2), 5.0))
+    assert out.shape == (1, 3)
+    b0 = D.biomass(0).copy()
+    c.run(D)
+    text = open(xml).read().replace("<reaction_type>surrogate</reaction_type>", "<reaction_type>kinetics</reaction_type>")
+    text = text.replace("<surrogate>\n        <enabled>true</enabled>", "<surrogate>\n        <enabled>false</enabled>")
+    xml2 = os.path.join(os.path.dirname(xml), "manual_srg.xml")
+    open(xml2, "w").write(text)
+    c2 = clb.Case(xml2)
+    assert c2.get("surrogate") == 0
+    D2 = c2.setup(clb.F64, clb.F64)
+    inp = os.path.join(os.path.dirname(xml), "input")
+    D2.set_surrogate_organism(os.path.join(inp, "organism.srg"), ["A", "B", "C", "D"], 0, [0.05, 0.1, 0.02, 0.2],
+                              [10, 5, 0, 0], 24.6, 2e-6)
+    D2.set_graph_network(os.path.join(inp, "abiotic.gnn"), ["A", "B", "C", "D"], -1)
+    c2.run(D2)
+    for s in range(4):
+        np.testing.assert_array_equal(D.concentration(s), D2.concentration(s))
+    np.testing.assert_array_equal(D.biomass(0), D2.biomass(0))
+    assert np.abs(D.biomass(0) - b0).max() > 1e-9
