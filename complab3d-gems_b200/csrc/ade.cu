@@ -181,18 +181,21 @@ template <typename TC, int NM, int EXT>
 __device__ __forceinline__ void node_kinetics(const AdeParams& P, const AdeExtra& X, int64_t k, int64_t nd, int code,
                                               bool west, bool east, int n_mobile, const TC (&rb)[NM],
                                               double* __restrict__ imm, double* __restrict__ bio,
-                                              const double* bc, int bn, TC (&dC)[NM]) {
+                                              const double* bc, int bn, bool hb, TC (&dC)[NM]) {
     const Geom G = P.g;
 #pragma unroll
     for (int s = 0; s < NM; ++s) dC[s] = 0;
     bool sym_done = false;
     if constexpr (EXT == 2) {
         if (P.law == CLB_LAW_SYMBOLIC && !west && !east && P.react[code]) {
-            sym_biotic<TC, NM>(P, n_mobile, rb, imm, bio, nd, dC);
+            // no organism acts where no biomass reaches 1e-12: every request would be zero
+            if (hb) sym_biotic<TC, NM>(P, n_mobile, rb, imm, bio, nd, dC);
             sym_done = true;
         }
     }
-    if (!sym_done && P.law != CLB_LAW_NONE && P.law != CLB_LAW_SYMBOLIC && !west && !east && P.react[code]) {
+    // dual Monod without biomass: every rate is zero, so the block is skipped (same increments)
+    if (!sym_done && P.law != CLB_LAW_NONE && P.law != CLB_LAW_SYMBOLIC && (hb || P.law != CLB_LAW_DUAL_MONOD) &&
+        !west && !east && P.react[code]) {
         // biotic block in the lattice's arithmetic type (FP64 lattices: FP64 throughout)
         const TC thr = (TC)THRD;
         TC C[NM], R[NM];
@@ -268,15 +271,17 @@ struct AdeMeta {
     uint32_t mt;
     int2 dv;
     int nd;  // dense index of the voxel (per-voxel fields, boundary planes)
+    int hb;  // 1: biomass may act at the node (AdeParams::bflag)
 };
 
 template <bool ODD>
-__device__ __forceinline__ AdeMeta ade_meta(const SparseView& S, int64_t k) {
+__device__ __forceinline__ AdeMeta ade_meta(const SparseView& S, int64_t k, const uint8_t* __restrict__ bflag) {
     AdeMeta M;
     M.code = S.code[k];
     M.mt = S.meta[k];
     M.dv = ODD ? *reinterpret_cast<const int2*>(S.dres + 4 * k) : make_int2(0, 0);
     M.nd = S.node[k];
+    M.hb = bflag ? bflag[k] : 1;
     return M;
 }
 
@@ -424,7 +429,10 @@ __device__ __forceinline__ uint32_t ade_gather(TS* __restrict__ g, const TC* __r
         cp_async<sizeof(TC)>(F.u + T, u + K + k);
         cp_async<sizeof(TC)>(F.u + 2 * T, u + 2 * K + k);
     }
-    if (P.law == CLB_LAW_DUAL_MONOD && !west && !east && P.react[M.code]) {
+    // biomass where it can act (bit 31 of the returned mask tells ade_finish)
+    const bool hb = M.hb != 0;
+    if (hb) actm |= 1u << 31;
+    if (hb && P.law == CLB_LAW_DUAL_MONOD && !west && !east && P.react[M.code]) {
         const int bn = P.M < ade_bio_cache<TC>() ? P.M : ade_bio_cache<TC>();
         for (int mb = 0; mb < bn; ++mb) cp_async<8>(F.bio + mb * T, bio + (int64_t)mb * P.g.N + M.nd);
     }
@@ -482,7 +490,7 @@ __device__ __forceinline__ void ade_finish(TS* __restrict__ g, double* __restric
     }
     TC dC[NM];  // increments of the mobile species, in the arithmetic type of the deposit
     node_kinetics<TC, NM, EXT>(P, X, k, M.nd, code, west, east, n_mobile, rb, imm, bio, F.bio,
-                               P.M < ade_bio_cache<TC>() ? P.M : ade_bio_cache<TC>(), dC);
+                               P.M < ade_bio_cache<TC>() ? P.M : ade_bio_cache<TC>(), (actm >> 31) & 1u, dC);
     // ---- phase 2: collide, deposit, stream, species by species from the shared slots
     uint32_t off2[7];  // read back rather than kept live through the kinetics
 #pragma unroll
@@ -535,7 +543,7 @@ __device__ __forceinline__ void ade_node(TS* __restrict__ g, double* __restrict_
                                          const double* __restrict__ neu, const AP& P, int n_mobile,
                                          const int* __restrict__ mob_species, int64_t k_west_end,
                                          int64_t k_east_begin, const AdeExtra& X, const AdeFrame<TC>& F, int64_t k) {
-    const AdeMeta M = ade_meta<ODD>(S, k);
+    const AdeMeta M = ade_meta<ODD>(S, k, P.bflag);
     const uint32_t actm = ade_gather<TS, TC, ODD, NM>(g, u, bio, S, P, n_mobile, mob_species, k_west_end,
                                                       k_east_begin, F, k, M);
     cp_async_wait_all();  // each thread reads only its own slots
@@ -581,13 +589,13 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_pipe_minb<TC, NM>() < 1 ? 1 
     AdeMeta cur, nxt;
     uint32_t acur = 0, anxt = 0;
     if (k < K) {
-        cur = ade_meta<ODD>(S, k);
+        cur = ade_meta<ODD>(S, k, P.bflag);
         acur = ade_gather<TS, TC, ODD, NM>(g, u, bio, S, P, n_mobile, mob_species, k_west_end, k_east_begin, F0, k,
                                            cur);
     }
     cp_async_commit();
     int64_t kn = k + sk;
-    if (kn < K) nxt = ade_meta<ODD>(S, kn);
+    if (kn < K) nxt = ade_meta<ODD>(S, kn, P.bflag);
     int q = 0;
     while (k < K) {
         if (kn < K)
@@ -596,7 +604,7 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_pipe_minb<TC, NM>() < 1 ? 1 
         cp_async_commit();
         const int64_t knn = kn + sk;
         AdeMeta nn;
-        if (knn < K) nn = ade_meta<ODD>(S, knn);
+        if (knn < K) nn = ade_meta<ODD>(S, knn, P.bflag);
         cp_async_wait_group<1>();  // node k's values have landed
         ade_finish<TS, TC, ODD, NM, EXT>(g, imm, bio, u, S, neu, P, n_mobile, mob_species, k_west_end, k_east_begin, X,
                                          q ? F1 : F0, k, cur, acur);
@@ -873,6 +881,7 @@ void ade_free(clb_handle* h) {
     h->d_glink = nullptr;  // inside d_g
     cudaFree(h->d_imm); h->d_imm = nullptr;
     cudaFree(h->d_bio); h->d_bio = nullptr;
+    cudaFree(h->d_bflag); h->d_bflag = nullptr;
     cudaFree(h->d_u); h->d_u = nullptr;
     cudaFree(h->d_neu); h->d_neu = nullptr;
     cudaFree(h->d_red); h->d_red = nullptr;
@@ -976,6 +985,9 @@ clb_status ade_init(clb_handle* h, const clb_species_desc* sp, int S) {
     }
     if ((e = cudaMalloc(&h->d_red, sizeof(double) * reduce_scratch_doubles(S, CLB_MAX_MICROBES, reduce_blocks(h)))) != cudaSuccess)
         return cuda_check(h, e, "reduction scratch");
+    if ((e = cudaMalloc(&h->d_bflag, K1)) != cudaSuccess) return cuda_check(h, e, "biomass flags");
+    cudaMemsetAsync(h->d_bflag, 1, K1, h->stream);  // until biomass is set, every node may hold some
+    h->ap.bflag = h->d_bflag;
     cudaMemsetAsync(h->d_u, 0, usize(h->ade_prec) * 3 * K1, h->stream);
     // immobile species: uniform c0 (initial_concentration applies to the whole domain)
     std::vector<double> immh(N1);
@@ -1162,6 +1174,25 @@ clb_status ade_set_thermo(clb_handle* h, const clb_thermo_desc* d) {
     return CLB_OK;
 }
 
+// the biomass flag of every species-lattice node: 1 where some microbe's biomass is not below 1e-12
+// (NaN included, so a non-finite field still reaches the kinetics and is reported)
+__global__ void k_bflag(uint8_t* __restrict__ flag, const int32_t* __restrict__ node, int64_t K,
+                        const double* __restrict__ bio, int M, int64_t N) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t nd = node[k];
+        uint8_t f = 0;
+        for (int m = 0; m < M; ++m) f |= !(bio[(int64_t)m * N + nd] < THRD);
+        flag[k] = f;
+    }
+}
+
+static clb_status refresh_bflag(clb_handle* h) {
+    if (!h->d_bflag || h->M < 1 || !h->d_bio) return CLB_OK;
+    ++h->launches;
+    k_bflag<<<h->num_sms * 4, 256, 0, h->stream>>>(h->d_bflag, h->ade_sp.node, h->ade_sp.K, h->d_bio, h->M, h->g.N);
+    return cuda_check(h, cudaGetLastError(), "biomass flags");
+}
+
 clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
     if (!h->ade_ready) return fail(h, CLB_NOT_INITIALIZED, "clb_ade_init first");
     if (M < 0 || M > CLB_MAX_MICROBES) return fail(h, CLB_INVALID_ARG, "microbe count out of range");
@@ -1173,7 +1204,9 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
     if (M == 0) return CLB_OK;
     cudaError_t e = cudaMalloc(&h->d_bio, sizeof(double) * M * (size_t)h->g.N);
     if (e != cudaSuccess) return cuda_check(h, e, "biomass");
-    return cuda_check(h, cudaMemcpy(h->d_bio, b, sizeof(double) * M * (size_t)h->g.N, cudaMemcpyHostToDevice), "biomass copy");
+    clb_status st = cuda_check(h, cudaMemcpy(h->d_bio, b, sizeof(double) * M * (size_t)h->g.N, cudaMemcpyHostToDevice),
+                               "biomass copy");
+    return st == CLB_OK ? refresh_bflag(h) : st;
 }
 
 // Resident blocks per SM of a transport-step instantiation with `smem` bytes of shared memory
@@ -1748,7 +1781,9 @@ clb_status ade_biomass(clb_handle* h, int m, double* host) {
 clb_status ade_set_biomass_field(clb_handle* h, int m, const double* host) {
     if (!h->ade_ready || m < 0 || m >= h->M) return fail(h, CLB_INVALID_ARG, "no such biomass field");
     h->ca_full = true;
-    return cuda_check(h, cudaMemcpy(h->d_bio + (size_t)m * h->g.N, host, sizeof(double) * h->g.N, cudaMemcpyHostToDevice), "biomass copy");
+    clb_status st = cuda_check(
+        h, cudaMemcpy(h->d_bio + (size_t)m * h->g.N, host, sizeof(double) * h->g.N, cudaMemcpyHostToDevice), "biomass copy");
+    return st == CLB_OK ? refresh_bflag(h) : st;
 }
 
 __global__ void k_u_to_dense(const void* __restrict__ u, int f64, const int32_t* __restrict__ node, int64_t K,

@@ -139,6 +139,8 @@ struct CaBufs {
     int32_t* ext;      // voxels a sweep pushed into that are not active
     int32_t* ext2;     // of those, the ones off the biomass list
     int* tmark;        // 1 while a voxel is on ext (cleared after the sweep)
+    uint8_t* bflag;    // the transport step's biomass flags per species node (see below), or null
+    const int32_t* sidx;  // species-lattice node of each voxel, -1
     int cap;
     uint64_t seed;
 };
@@ -216,6 +218,12 @@ __device__ __forceinline__ bool ca_mask_voxel(const CaView& C, const CaBufs& B, 
         msum += mk;
     }
     best = max(best, ordered(tn));
+    // the transport step reads this voxel's biomass only when it is listed (a voxel off the list
+    // holds every microbe below 1e-12, where no rate law acts); a NaN total stays flagged
+    if (B.bflag) {
+        const int32_t k = B.sidx[n];
+        if (k >= 0) B.bflag[k] = !(tn <= 1e-14);
+    }
     return tn > 1e-14;
 }
 
@@ -993,6 +1001,8 @@ static CaBufs ca_bufs(clb_handle* h) {
     B.ext = h->d_ca_ext;
     B.ext2 = h->d_ca_ext2;
     B.tmark = h->d_ca_tmark;
+    B.bflag = h->d_bflag;
+    B.sidx = h->ade_sp.idx_of;
     B.cap = h->ca_cap;
     B.seed = h->ca_seed;
     return B;

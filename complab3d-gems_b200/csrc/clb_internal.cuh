@@ -168,6 +168,10 @@ struct AdeParams {
     // microbes that are one (law CLB_LAW_SYMBOLIC)
     const SrgNet* srg;
     uint32_t srg_mask;
+    // [K] per species-lattice node: 0 where no microbe's biomass reaches 1e-12 (so no organism
+    // grows, decays or draws there), 1 where one may; kept by clb_set_biomass / clb_set_field and
+    // by the automaton's mask passes, so the transport step reads biomass only where it can act
+    const uint8_t* bflag;
 };
 
 // Per-node state of the precipitation / dissolution machinery (geometry_update.cu), passed to the
@@ -243,6 +247,7 @@ struct clb_handle_s {
     int flow_odd_pipe = 1;            // odd step pipelined through shared memory (4- and 8-byte storage)
     int flow_pipe_grid = 0;           // its resident-CTA grid; 0 where it is not available
     int* d_err = nullptr;             // device error flag (bounded waits that gave up)
+    uint8_t* d_bflag = nullptr;       // [K] species-lattice nodes where biomass may act (AdeParams::bflag)
     int* h_flags = nullptr;           // host-mapped pinned flags: [0] a transport step met a non-finite
     int* d_flags = nullptr;           // density (its device alias)
     int64_t flow_iters = 0;           // host mirror of the device iteration count

@@ -68,7 +68,10 @@ __device__ __forceinline__ void biotic_rates(const AdeParams& P, const KT (&C)[N
                     KT d = rbm * (KT)P.dt;
                     if (d > thr || d < -thr) {
                         if (d + Bm < (KT)0) d = -Bm;
-                        *const_cast<double*>(bp) += (double)d;
+                        // braw is the value in memory (staged or read above; only this thread writes
+                        // this voxel's biomass in a step): the same sum as `*bp += d`, without
+                        // reading the field again inside the kinetics
+                        *const_cast<double*>(bp) = braw + (double)d;
                     }
                 }
             }
