@@ -761,6 +761,13 @@ def main():
                "sample": f"2 coupled iterations (8 species + automaton, {tt:.2f} s each) and 2 flow iterations "
                          f"({tf:.2f} s each) of the full map, FP64, weighted by this run's {mix:.3f} flow "
                          "iterations per transport iteration"}
+        # the same code on one thread: one coupled and one flow iteration
+        oracle.set_threads(1)
+        t1 = O.transport_iteration()
+        f1 = O.flow_iteration()
+        cpu["single_thread"] = {"value": O.mixed_mlups(t1, f1, mix), "unit": "MLUPS", "cores": 1,
+                                "sample": f"1 coupled iteration ({t1:.2f} s) and 1 flow iteration ({f1:.2f} s) of "
+                                          "the full map, weighted the same way"}
         del O
 
     if rank == 0:

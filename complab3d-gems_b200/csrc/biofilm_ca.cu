@@ -319,9 +319,11 @@ __device__ void ca_mask_pass(const CaView& C, const CaBufs& B, CaScalars* sc, co
         best = max(best, __shfl_down_sync(0xffffffffu, best, o));
         msum += __shfl_down_sync(0xffffffffu, msum, o);
     }
+    // warps whose values are the identity (most of a list pass's warps have no voxel) leave the
+    // two contended counters alone
     if ((threadIdx.x & 31) == 0) {
-        atomicMax(&sc->gmax, best);
-        atomicAdd((unsigned long long*)&sc->msum, (unsigned long long)msum);
+        if (best > 0) atomicMax(&sc->gmax, best);
+        if (msum != 0) atomicAdd((unsigned long long*)&sc->msum, (unsigned long long)msum);
     }
 }
 
