@@ -340,17 +340,27 @@ __device__ void ca_collect(const CaView& C, const CaBufs& B, CaScalars* sc, cons
     int* __restrict__ done = B.done;
     const int cap = B.cap;
     const int64_t lo = G.plane, hi = G.N - G.plane;  // x = 1..nx-2
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb; j += gridDim.x * blockDim.x) {
-        const int64_t n = blist[j];
-        if (n < lo || n >= hi || !ca_open(C, mat[n])) continue;
-        const double t = total[n];
-        if (C.half) {
-            // 'half': only biofilm voxels push, any total above the maximum
-            if (ca_pore(C, mat[n]) || !(t > C.bmax)) continue;
-        } else if (!(t > C.bmax) || !(t - C.bmax > THRD)) {
-            continue;
+    // whole warps run the loop together: one atomic per warp takes the rows of its active voxels
+    const int span = (nb + 31) / 32 * 32;
+    const int lane = threadIdx.x & 31;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < span; j += gridDim.x * blockDim.x) {
+        bool take = false;
+        int64_t n = 0;
+        if (j < nb) {
+            n = blist[j];
+            if (n >= lo && n < hi && ca_open(C, mat[n])) {
+                const double t = total[n];
+                if (C.half) take = !ca_pore(C, mat[n]) && t > C.bmax;  // 'half': biofilm voxels, any excess
+                else take = t > C.bmax && t - C.bmax > THRD;
+            }
         }
-        const unsigned int i = atomicAdd(&sc->active, 1u);
+        const unsigned int bal = __ballot_sync(0xffffffffu, take);
+        if (!bal) continue;
+        unsigned int base = 0;
+        if (lane == 0) base = atomicAdd(&sc->active, (unsigned int)__popc(bal));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (!take) continue;
+        const unsigned int i = base + __popc(bal & ((1u << lane) - 1u));
         if ((int)i >= cap) { atomicAdd(&sc->overflow, 1u); continue; }
         act[i] = (int)n;
         aidx[n] = (int)i;
@@ -380,6 +390,7 @@ __device__ void ca_round(const CaView& C, const CaBufs& B, int count, int round,
     double* __restrict__ amt = B.amt;
     double* __restrict__ own = B.own;
     const uint64_t seed = B.seed;
+    unsigned int fin = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         if (done[i]) continue;
         const int64_t n = act[i];
@@ -475,8 +486,11 @@ __device__ void ca_round(const CaView& C, const CaBufs& B, int count, int round,
         }
         for (int m = 0; m < C.M; ++m) own[(int64_t)i * C.M + m] = b[m];
         done[i] = round;
-        atomicSub(&sc->remaining, 1u);
+        ++fin;
     }
+    // the voxels this round finished, one atomic per warp (every lane reaches this point)
+    for (int o = 16; o > 0; o >>= 1) fin += __shfl_down_sync(0xffffffffu, fin, o);
+    if ((threadIdx.x & 31) == 0 && fin) atomicSub(&sc->remaining, fin);
 }
 
 // The voxels a sweep pushed into that are not active themselves, each once (ext), and of those the
@@ -487,13 +501,21 @@ __device__ void ca_targets(const CaBufs& B, CaScalars* sc, int count) {
     const int* __restrict__ tgt = B.tgt;
     const int* __restrict__ aidx = B.aidx;
     const double* __restrict__ total = B.total;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    // whole warps run the loop together, so the appends take one atomic per warp
+    const int span = (count + 31) / 32 * 32;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < span; i += gridDim.x * blockDim.x) {
         for (int t = 0; t < CA_REC; ++t) {
-            const int m = tgt[i * CA_REC + t];
-            if (m < 0 || aidx[m] >= 0) continue;
-            if (atomicExch(&B.tmark[m], 1) != 0) continue;
-            B.ext[atomicAdd(&sc->next, 1u)] = m;
-            if (!(total[m] > 1e-14)) B.ext2[atomicAdd(&sc->next2, 1u)] = m;
+            bool take = false, off_list = false;
+            int m = 0;
+            if (i < count) {
+                m = tgt[i * CA_REC + t];
+                if (m >= 0 && aidx[m] < 0 && atomicExch(&B.tmark[m], 1) == 0) {
+                    take = true;
+                    off_list = !(total[m] > 1e-14);
+                }
+            }
+            ca_list_append(B.ext, &sc->next, m, take);
+            ca_list_append(B.ext2, &sc->next2, m, off_list);
         }
     }
 }
