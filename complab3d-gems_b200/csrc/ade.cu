@@ -621,31 +621,47 @@ __global__ void __launch_bounds__(ADE_THREADS, (ade_pipe_minb<TC, NM>() < 1 ? 1 
 // The stored density of every Neumann plane node: the density of its inner neighbour as it
 // stands before the step (FlatAdiabaticBoundaryFunctional3D after the previous stream). A node
 // whose inner neighbour is not a fluid node keeps its previous value.
-// The Neumann planes of one step (one grid row per species and side).
+// The Neumann planes of one step, by side (0: x = 0, 1: x = nx - 1): species and mobile slot.
 struct NeumannPlanes {
-    int n;
-    int s[2 * CLB_MAX_SPECIES], m[2 * CLB_MAX_SPECIES], side[2 * CLB_MAX_SPECIES];
+    int n[2];
+    int s[2][CLB_MAX_SPECIES], m[2][CLB_MAX_SPECIES];
 };
 
+// One thread per plane pixel and side: the inner neighbour's 7 storage locations are found once
+// (they are the same in every species' buffer, a species stride apart) and serve every species
+// with a Neumann face on that side, whose loads are then all independent.
 template <typename TS, typename TC>
 __global__ void k_ade_neumann(const TS* __restrict__ g, const TS* __restrict__ glink, const SparseView S,
                               const int8_t* __restrict__ mat, double* __restrict__ neu, const AdeParams P,
                               const NeumannPlanes J, int odd) {
     const Geom G = P.g;
-    const int s = J.s[blockIdx.y], m = J.m[blockIdx.y], side = J.side[blockIdx.y];
-    const double c0 = P.c0[s];
+    const int side = blockIdx.y;
+    const int ns = J.n[side];
+    if (ns == 0) return;
     const int xb = side == 0 ? 0 : G.nx - 1, xi = side == 0 ? 1 : G.nx - 2;
-    TC init[7];
-    for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - ade_sigma<TC>()));
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < G.plane; p += gridDim.x * blockDim.x) {
         const int64_t nb = (int64_t)xb * G.plane + p, ni = (int64_t)xi * G.plane + p;
         const int db = P.dyn[mat[nb]], di = P.dyn[mat[ni]];
         if (!(db == ADE_PORE || db == ADE_BIO) || !(di == ADE_PORE || di == ADE_BIO)) continue;
-        TC pop[7];
-        natural<TS, TC, 7>(S, G, g + (int64_t)m * S.SS, glink + (int64_t)m * S.SS, ni, odd, init, pop);
-        double r = ade_sigma<TC>();
-        for (int i = 0; i < 7; ++i) r += (double)pop[i];
-        neu[((int64_t)s * 2 + side) * G.plane + p] = r;
+        int x, y, z;
+        decode(G, ni, x, y, z);
+        const TS* loc[7];  // in species 0's buffer; nullptr: never written, the initial value
+#pragma unroll
+        for (int i = 0; i < 7; ++i) loc[i] = natural_slot<const TS, 7>(S, G, g, glink, ni, x, y, z, i, odd);
+#pragma unroll 2
+        for (int j = 0; j < ns; ++j) {
+            const int s = J.s[side][j];
+            const int64_t sh = (int64_t)J.m[side][j] * S.SS;
+            const double c0 = P.c0[s];
+            TC pop[7];
+#pragma unroll
+            for (int i = 0; i < 7; ++i)
+                pop[i] = loc[i] ? ld<TS, TC>(loc[i] + sh) : (TC)(q7w(i) * (c0 - ade_sigma<TC>()));
+            double r = ade_sigma<TC>();
+#pragma unroll
+            for (int i = 0; i < 7; ++i) r += (double)pop[i];
+            neu[((int64_t)s * 2 + side) * G.plane + p] = r;
+        }
     }
 }
 
@@ -1291,23 +1307,22 @@ template <typename TS, typename TC>
 static void launch_neumann(clb_handle* h, int odd) {
     const SparseView S = view_of(h->ade_sp);
     NeumannPlanes J;
-    J.n = 0;
+    J.n[0] = J.n[1] = 0;
     for (int s = 0; s < h->S; ++s) {
         const int m = h->ap.slot[s];
         if (m < 0) continue;
         for (int side = 0; side < 2; ++side) {
             const int t = side == 0 ? h->ap.ltype[s] : h->ap.rtype[s];
             if (t != CLB_NEUMANN) continue;
-            J.s[J.n] = s;
-            J.m[J.n] = m;
-            J.side[J.n] = side;
-            ++J.n;
+            J.s[side][J.n[side]] = s;
+            J.m[side][J.n[side]] = m;
+            ++J.n[side];
         }
     }
-    if (J.n == 0) return;
-    const dim3 grid(std::max(1, std::min(h->num_sms * 2, (h->g.plane + 255) / 256)), J.n);
+    if (J.n[0] + J.n[1] == 0) return;
+    const dim3 grid(std::max(1, std::min(h->num_sms * 4, (h->g.plane + 127) / 128)), 2);
     ++h->launches;
-    k_ade_neumann<TS, TC><<<grid, 256, 0, h->stream>>>((const TS*)h->d_g, (const TS*)h->d_glink, S, h->d_mat,
+    k_ade_neumann<TS, TC><<<grid, 128, 0, h->stream>>>((const TS*)h->d_g, (const TS*)h->d_glink, S, h->d_mat,
                                                        h->d_neu, h->ap, J, odd);
 }
 
