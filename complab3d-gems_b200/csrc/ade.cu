@@ -1227,7 +1227,8 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
 
 // Resident blocks per SM of a transport-step instantiation with `smem` bytes of shared memory
 // (set up once per instantiation), times the SM count: the persistent grid.
-static int ade_grid_for(const void* kern, int smem, int num_sms, int threads, int resident = ADE_RESIDENT) {
+static int ade_grid_for(const void* kern, int smem, int num_sms, int threads, int resident = ADE_RESIDENT,
+                        int static_smem = 0) {
     struct Known { const void* kern; int smem, threads, blocks; };
     static std::mutex mu;
     static std::vector<Known> known;
@@ -1242,7 +1243,7 @@ static int ade_grid_for(const void* kern, int smem, int num_sms, int threads, in
     // cache, which the odd step's neighbour gathers reuse (five resident blocks with less L1 ran
     // the odd step slower on B200; the even step, which reads only its own slots, gained from five).
     {
-        const int per_block = smem + 1024;  // the runtime reserves 1 KB per block
+        const int per_block = smem + static_smem + 1024;  // the runtime reserves 1 KB per block
         const int fit = std::max(1, (228 * 1024) / per_block);
         const int res = std::min(resident, fit);
         const int pct = (int)((100LL * res * per_block + 228 * 1024 - 1) / (228 * 1024));
@@ -1352,57 +1353,82 @@ __device__ __forceinline__ int batch_find(const int64_t* off, int n, int64_t t) 
     return lo;
 }
 
-// One transport step of every domain (no abiotic law, no dissolution): the species nodes of all
-// domains form one index range; shared memory holds the slots, then the domain offsets.
+// One transport step of every domain (no abiotic law, no dissolution). Each CTA takes a
+// contiguous run of the tile table (tiles are in domain order) and copies a tile's domain
+// description into shared memory when it differs from the previous tile's; the per-node code is
+// the single-domain step's, its parameters read from that copy.
 template <typename TS, typename TC, bool ODD, int NM>
 __global__ void __launch_bounds__(ADE_THREADS, (ade_minb<TC, NM>() > 6 ? 6 : ade_minb<TC, NM>()))
     k_ade_batch(const BatchView B) {
     extern __shared__ __align__(16) unsigned char ade_smem[];
+    __shared__ __align__(16) BatchDomain sd;
     const AdeFrame<TC> F = ade_frame<TC, NM>(ade_smem, 0);
-    int64_t* soff = reinterpret_cast<int64_t*>(ade_smem + ade_slot_bytes<TC, NM>());
-    for (int i = threadIdx.x; i <= B.ndom; i += blockDim.x) soff[i] = B.aoff[i];
-    __syncthreads();
-    const int64_t total = soff[B.ndom];
+    const int tid = threadIdx.x;
     AdeExtra X;
     X.iface = nullptr;
     X.xidx = nullptr;
     X.xdc = nullptr;
     X.ng = 0;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-        const int di = batch_find(soff, B.ndom, t);
-        const BatchDomain& d = B.dom[di];
-        ade_node<TS, TC, ODD, NM, 0>((TS*)d.g, d.imm, d.bio, (const TC*)d.u, d.as, d.neu, d.ap, d.n_mobile,
-                                         d.mob, d.akw, d.ake, X, F, t - soff[di]);
+    const int per = (B.nat + gridDim.x - 1) / gridDim.x;
+    const int t0 = blockIdx.x * per, t1 = min(B.nat, t0 + per);
+    int cur = -1;
+    for (int t = t0; t < t1; ++t) {
+        const BatchTile T = B.atiles[t];
+        if (T.d != cur) {
+            __syncthreads();  // every thread is done with the previous domain
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(B.dom + T.d);
+            uint64_t* dst = reinterpret_cast<uint64_t*>(&sd);
+            for (int q = tid; q < (int)(sizeof(BatchDomain) / 8); q += ADE_THREADS) dst[q] = src[q];
+            __syncthreads();
+            cur = T.d;
+        }
+        for (int64_t k = T.first + tid; k < T.first + T.count; k += ADE_THREADS)
+            ade_node<TS, TC, ODD, NM, 0>((TS*)sd.g, sd.imm, sd.bio, (const TC*)sd.u, sd.as, sd.neu, sd.ap, sd.n_mobile,
+                                         sd.mob, sd.akw, sd.ake, X, F, k);
     }
 }
 
-// the Neumann planes of every domain (as k_ade_neumann, over a list of planes)
+// the Neumann planes of every domain (as k_ade_neumann): one thread per pixel of a face that some
+// species treats as Neumann; the inner neighbour's storage locations serve all those species
 template <typename TS, typename TC>
 __global__ void k_neumann_batch(const BatchView B, int odd) {
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < B.joff[B.njobs];
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int j = batch_find(B.joff, B.njobs, t);
-        const NeumannJob J = B.jobs[j];
+    const int64_t total = B.foff_faces[B.nfaces];
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int j = batch_find(B.foff_faces, B.nfaces, t);
+        const NeumannFace J = B.faces[j];
         const BatchDomain& d = B.dom[J.d];
         const Geom G = d.ap.g;
-        const int p = (int)(t - B.joff[j]);
+        const int p = (int)(t - B.foff_faces[j]);
         const int xb = J.side == 0 ? 0 : G.nx - 1, xi = J.side == 0 ? 1 : G.nx - 2;
         const int64_t nb = (int64_t)xb * G.plane + p, ni = (int64_t)xi * G.plane + p;
         const int db = d.ap.dyn[d.mat[nb]], di = d.ap.dyn[d.mat[ni]];
         if (!(db == ADE_PORE || db == ADE_BIO) || !(di == ADE_PORE || di == ADE_BIO)) continue;
-        const double c0 = d.ap.c0[J.s];
-        TC init[7], pop[7];
-        for (int i = 0; i < 7; ++i) init[i] = (TC)(q7w(i) * (c0 - ade_sigma<TC>()));
-        natural<TS, TC, 7>(d.as, G, (const TS*)d.g + (int64_t)J.m * d.as.SS, (const TS*)d.glink + (int64_t)J.m * d.as.SS,
-                           ni, odd, init, pop);
-        double r = ade_sigma<TC>();
-        for (int i = 0; i < 7; ++i) r += (double)pop[i];
-        d.neu[((int64_t)J.s * 2 + J.side) * G.plane + p] = r;
+        int x, y, z;
+        decode(G, ni, x, y, z);
+        const TS* g0 = (const TS*)d.g;
+        const TS* loc[7];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) loc[i] = natural_slot<const TS, 7>(d.as, G, g0, (const TS*)d.glink, ni, x, y, z, i, odd);
+        const int S = d.ap.S;
+        for (int s = 0; s < S; ++s) {
+            const int m = d.ap.slot[s];
+            if (m < 0 || (J.side == 0 ? d.ap.ltype[s] : d.ap.rtype[s]) != CLB_NEUMANN) continue;
+            const int64_t sh = (int64_t)m * d.as.SS;
+            const double c0 = d.ap.c0[s];
+            TC pop[7];
+#pragma unroll
+            for (int i = 0; i < 7; ++i)
+                pop[i] = loc[i] ? ld<TS, TC>(loc[i] + sh) : (TC)(q7w(i) * (c0 - ade_sigma<TC>()));
+            double r = ade_sigma<TC>();
+#pragma unroll
+            for (int i = 0; i < 7; ++i) r += (double)pop[i];
+            d.neu[((int64_t)s * 2 + J.side) * G.plane + p] = r;
+        }
     }
 }
 
 void launch_neumann_batch(const BatchView& B, int prec, bool odd, int grid, cudaStream_t st) {
-    if (B.njobs == 0) return;
+    if (B.nfaces == 0) return;
     switch (prec) {
         case CLB_F64: k_neumann_batch<double, double><<<grid, 256, 0, st>>>(B, odd ? 1 : 0); break;
         case CLB_F32: k_neumann_batch<float, float><<<grid, 256, 0, st>>>(B, odd ? 1 : 0); break;
@@ -1413,9 +1439,10 @@ void launch_neumann_batch(const BatchView& B, int prec, bool odd, int grid, cuda
 template <typename TS, typename TC, bool ODD, int NM>
 static void launch_ade_batch_t(const BatchView& B, int grid_mult, int num_sms, cudaStream_t st) {
     auto kern = k_ade_batch<TS, TC, ODD, NM>;
-    const int sm = ade_slot_bytes<TC, NM>() + (int)sizeof(int64_t) * (B.ndom + 1);
-    const int per_sm = ade_grid_for((const void*)kern, sm, 1, ADE_THREADS);
-    kern<<<per_sm * num_sms * grid_mult, ADE_THREADS, sm, st>>>(B);
+    const int sm = ade_slot_bytes<TC, NM>();
+    const int per_sm = ade_grid_for((const void*)kern, sm, 1, ADE_THREADS, ADE_RESIDENT, (int)sizeof(BatchDomain));
+    const int grid = std::max(1, std::min(per_sm * num_sms * grid_mult, B.nat));
+    kern<<<grid, ADE_THREADS, sm, st>>>(B);
 }
 
 template <typename TS, typename TC, bool ODD>

@@ -24,8 +24,10 @@ struct clb_batch_s {
     int flow_prec = 0, ade_prec = 0, nm = 1;
     bool has_flow = false, has_ade = false;
     clb::BatchDomain* d_dom = nullptr;
-    int64_t *d_foff = nullptr, *d_aoff = nullptr, *d_joff = nullptr;
+    int64_t *d_foff = nullptr, *d_aoff = nullptr, *d_joff = nullptr, *d_face_off = nullptr;
     clb::NeumannJob* d_jobs = nullptr;
+    clb::BatchTile *d_ftiles = nullptr, *d_atiles = nullptr;
+    clb::NeumannFace* d_faces = nullptr;
     clb::BatchView view{};
     int64_t flow_nodes = 0, ade_nodes = 0;
     int flow_threads = 256, flow_mult = 4, ade_mult = 1, neu_grid = 148;
@@ -79,6 +81,10 @@ static void batch_free(clb_batch* b) {
     cudaFree(b->d_aoff);
     cudaFree(b->d_jobs);
     cudaFree(b->d_joff);
+    cudaFree(b->d_ftiles);
+    cudaFree(b->d_atiles);
+    cudaFree(b->d_faces);
+    cudaFree(b->d_face_off);
     if (b->stream) cudaStreamDestroy(b->stream);
 }
 
@@ -119,6 +125,9 @@ clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out) {
     std::vector<BatchDomain> dom((size_t)n);
     std::vector<int64_t> foff((size_t)n + 1, 0), aoff((size_t)n + 1, 0), joff(1, 0);
     std::vector<NeumannJob> jobs;
+    std::vector<BatchTile> ftiles, atiles;
+    std::vector<NeumannFace> faces;
+    std::vector<int64_t> face_off(1, 0);
     b->kf.assign((size_t)n, 0);
     b->ka.assign((size_t)n, 0);
     b->jbeg.assign((size_t)n + 1, 0);
@@ -136,6 +145,8 @@ clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out) {
             d.fp = h->fp;
             foff[(size_t)i + 1] = foff[(size_t)i] + h->flow_sp.K;
             b->kf[(size_t)i] = h->flow_sp.K;
+            for (int64_t k = 0; k < h->flow_sp.K; k += BATCH_FLOW_TILE)
+                ftiles.push_back({i, (int)std::min<int64_t>(BATCH_FLOW_TILE, h->flow_sp.K - k), k});
         }
         if (b->has_ade) {
             d.g = h->d_g;
@@ -153,6 +164,16 @@ clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out) {
             d.n_mobile = h->n_mobile;
             aoff[(size_t)i + 1] = aoff[(size_t)i] + h->ade_sp.K;
             b->ka[(size_t)i] = h->ade_sp.K;
+            for (int64_t k = 0; k < h->ade_sp.K; k += BATCH_ADE_TILE)
+                atiles.push_back({i, (int)std::min<int64_t>(BATCH_ADE_TILE, h->ade_sp.K - k), k});
+            for (int side = 0; side < 2; ++side) {
+                bool any = false;
+                for (int s = 0; s < h->S; ++s)
+                    any = any || (h->ap.slot[s] >= 0 && (side == 0 ? h->ap.ltype[s] : h->ap.rtype[s]) == CLB_NEUMANN);
+                if (!any) continue;
+                faces.push_back({i, side});
+                face_off.push_back(face_off.back() + h->g.plane);
+            }
             for (int s = 0; s < h->S; ++s) {
                 const int m = h->ap.slot[s];
                 if (m < 0) continue;
@@ -174,6 +195,18 @@ clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->d_jobs, sizeof(NeumannJob) * std::max<size_t>(1, jobs.size()));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_joff, sizeof(int64_t) * joff.size());
     if (e == cudaSuccess) e = cudaMalloc(&b->d_jbeg, sizeof(int) * (n + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ftiles, sizeof(BatchTile) * std::max<size_t>(1, ftiles.size()));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_atiles, sizeof(BatchTile) * std::max<size_t>(1, atiles.size()));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_faces, sizeof(NeumannFace) * std::max<size_t>(1, faces.size()));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_face_off, sizeof(int64_t) * face_off.size());
+    if (e == cudaSuccess && !ftiles.empty())
+        e = cudaMemcpy(b->d_ftiles, ftiles.data(), sizeof(BatchTile) * ftiles.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !atiles.empty())
+        e = cudaMemcpy(b->d_atiles, atiles.data(), sizeof(BatchTile) * atiles.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !faces.empty())
+        e = cudaMemcpy(b->d_faces, faces.data(), sizeof(NeumannFace) * faces.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_face_off, face_off.data(), sizeof(int64_t) * face_off.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_sync, sizeof(int) * (2 + (size_t)PERSIST_MAX_STEPS * 3 * n));
     if (e == cudaSuccess) e = cudaMemset(b->d_sync, 0, sizeof(int) * (2 + (size_t)PERSIST_MAX_STEPS * 3 * n));
     if (e == cudaSuccess) e = cudaMemcpy(b->d_jbeg, b->jbeg.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice);
@@ -195,7 +228,14 @@ clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out) {
     b->view.jobs = b->d_jobs;
     b->view.joff = b->d_joff;
     b->view.njobs = (int)jobs.size();
-    b->neu_grid = std::max<int64_t>(1, std::min<int64_t>((joff.back() + 255) / 256, b->num_sms * 4));
+    b->view.ftiles = b->d_ftiles;
+    b->view.nft = (int)ftiles.size();
+    b->view.atiles = b->d_atiles;
+    b->view.nat = (int)atiles.size();
+    b->view.faces = b->d_faces;
+    b->view.foff_faces = b->d_face_off;
+    b->view.nfaces = (int)faces.size();
+    b->neu_grid = std::max<int64_t>(1, std::min<int64_t>((face_off.back() + 255) / 256, b->num_sms * 4));
     b->resident = batch_persistent_resident(b->has_ade ? b->ade_prec : b->flow_prec, b->nm, b->minb);
     if (b->has_flow && b->has_ade && b->flow_prec != b->ade_prec) b->persistent = false;  // one storage type per launch
     *out = b;

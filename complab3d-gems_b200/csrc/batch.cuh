@@ -33,6 +33,21 @@ struct NeumannJob {
     int d, s, m, side;
 };
 
+// A run of consecutive compact nodes of one domain's lattice: the unit the per-lattice batched
+// launches hand to a CTA, which holds the domain's description in shared memory while it works.
+struct BatchTile {
+    int d;
+    int count;
+    int64_t first;
+};
+constexpr int BATCH_FLOW_TILE = 1024;  // flow nodes per tile
+constexpr int BATCH_ADE_TILE = 512;    // transport nodes per tile
+
+// One x-face of one domain that at least one mobile species treats as Neumann
+struct NeumannFace {
+    int d, side;
+};
+
 struct BatchView {
     const BatchDomain* dom;
     const int64_t* foff;  // [ndom + 1] prefix sums of the flow node counts
@@ -41,6 +56,13 @@ struct BatchView {
     const NeumannJob* jobs;
     const int64_t* joff;  // [njobs + 1] prefix sums of the plane sizes
     int njobs;
+    const BatchTile* ftiles;  // flow tiles, domain by domain
+    int nft;
+    const BatchTile* atiles;  // transport tiles, domain by domain
+    int nat;
+    const NeumannFace* faces;
+    const int64_t* foff_faces;  // [nfaces + 1] prefix sums of the face sizes
+    int nfaces;
 };
 
 constexpr int BATCH_MAX_DOMAINS = 2048;

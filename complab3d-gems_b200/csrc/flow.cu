@@ -323,36 +323,39 @@ __global__ void __launch_bounds__(TILE, sizeof(TS) == 8 ? 2 : 4)
 
 // ------------------------------------------------------------------ batched step of many domains
 
-// largest d with off[d] <= t (off ascending, off[0] = 0)
-__device__ __forceinline__ int batch_domain(const int64_t* off, int ndom, int64_t t) {
-    int lo = 0, hi = ndom - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (off[mid] <= t) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-// One AA step of every domain's flow lattice: the nodes of all domains form one index range.
+// One AA step of every domain's flow lattice. Each CTA takes a contiguous run of the tile table
+// (tiles are in domain order) and copies a tile's domain description into shared memory when it
+// differs from the previous tile's, so the node loop reads the layout and the parameters from
+// shared memory with the very same per-node code as the single-domain step.
 template <typename TS, typename TC, bool ODD>
 __global__ void __launch_bounds__(256) k_flow_batch(const BatchView B) {
-    extern __shared__ int64_t soff[];
-    for (int i = threadIdx.x; i <= B.ndom; i += blockDim.x) soff[i] = B.foff[i];
-    __syncthreads();
-    const int64_t total = soff[B.ndom];
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-        const int di = batch_domain(soff, B.ndom, t);
-        const BatchDomain& d = B.dom[di];
-        flow_node<TS, TC, ODD>((TS*)d.f, (TS*)d.flink, d.fs, d.fp, t - soff[di], d.fkw, d.fke);
+    __shared__ __align__(16) BatchDomain sd;
+    const int tid = threadIdx.x;
+    const int per = (B.nft + gridDim.x - 1) / gridDim.x;
+    const int t0 = blockIdx.x * per, t1 = min(B.nft, t0 + per);
+    int cur = -1;
+    for (int t = t0; t < t1; ++t) {
+        const BatchTile T = B.ftiles[t];
+        if (T.d != cur) {
+            __syncthreads();  // every thread is done with the previous domain
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(B.dom + T.d);
+            uint64_t* dst = reinterpret_cast<uint64_t*>(&sd);
+            for (int q = tid; q < (int)(sizeof(BatchDomain) / 8); q += blockDim.x) dst[q] = src[q];
+            __syncthreads();
+            cur = T.d;
+        }
+        TS* f = (TS*)sd.f;
+        TS* fl = (TS*)sd.flink;
+        for (int64_t k = T.first + tid; k < T.first + T.count; k += blockDim.x)
+            flow_node<TS, TC, ODD>(f, fl, sd.fs, sd.fp, k, sd.fkw, sd.fke);
     }
 }
 
 void launch_flow_batch(const BatchView& B, int prec, bool odd, int grid, int threads, cudaStream_t st) {
-    const size_t sm = sizeof(int64_t) * (B.ndom + 1);
+    grid = std::max(1, std::min(grid, B.nft));
 #define CLB_FB(TS, TC)                                                                      \
-    if (odd) k_flow_batch<TS, TC, true><<<grid, threads, sm, st>>>(B);                     \
-    else k_flow_batch<TS, TC, false><<<grid, threads, sm, st>>>(B);
+    if (odd) k_flow_batch<TS, TC, true><<<grid, threads, 0, st>>>(B);                      \
+    else k_flow_batch<TS, TC, false><<<grid, threads, 0, st>>>(B);
     switch (prec) {
         case CLB_F64: CLB_FB(double, double); break;
         case CLB_F32: CLB_FB(float, float); break;
