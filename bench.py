@@ -281,6 +281,16 @@ def timed_steps(torch, stream, step, steps, warmup):
     return e0.elapsed_time(e1)
 
 
+def biomass_bytes(bio, open_mask):
+    """Biomass bytes per open voxel of one transport step: the 1-byte per-voxel flag; every
+    microbe's value read where the flag is set (some microbe holds at least 1e-14); a microbe's
+    value written back where it holds biomass (its growth or decay passes the threshold)."""
+    b = np.asarray(bio).reshape(len(bio), -1)[:, open_mask.ravel()]
+    flag = float(np.mean(np.any(b >= 1e-14, axis=0)))
+    held = float(np.sum(np.mean(b >= 1e-14, axis=1)))
+    return 1.0 + 8.0 * len(bio) * flag + 8.0 * held, flag
+
+
 def bench_d3q7(clb, workloads, torch, local, peak, steps=60, warmup=5, scale=1.0):
     """Fused transport of the 256^3 sphere pack with 8 species and 2 biofilm microbes (dual Monod),
     FP32 populations; the lattice (1.5 GB) is far larger than L2, so no flush is needed."""
@@ -305,8 +315,10 @@ def bench_d3q7(clb, workloads, torch, local, peak, steps=60, warmup=5, scale=1.0
     S = len(cfg["species"])
     n_open = int(np.count_nonzero((mat != 0) & (mat != 1)))
     per = ms / steps
-    M = cfg["biomass"].shape[0]
-    alg_node = S * 2 * 7 * 4 + 3 * 4 + 1 + M * 8
+    open_mask = (mat != 0) & (mat != 1)
+    bio_b, flagged = biomass_bytes([D.biomass(m) for m in range(cfg["biomass"].shape[0])], open_mask)
+    # S x 2 x 7 x 4 B populations + 12 B velocity + 1 B material + the biomass bytes
+    alg_node = S * 2 * 7 * 4 + 3 * 4 + 1 + bio_b
     achieved = alg_node * n_open / (per * 1e-3) / 1e9
     D.close()
     return {"workload": cfg["name"] + ", FP32 populations, dual-Monod kinetics fused",
@@ -314,7 +326,8 @@ def bench_d3q7(clb, workloads, torch, local, peak, steps=60, warmup=5, scale=1.0
             "ms_per_step": per, "thermo_gate_ms_per_step": ms_gate / steps, "open_voxels": n_open, "species": S,
             "steps": steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "algorithmic_bytes_per_node": alg_node, "kernel": "k_ade_aa (all species fused)"}}
+                         "algorithmic_bytes_per_node": alg_node, "biomass_flagged_fraction": flagged,
+                         "kernel": "k_ade_aa (all species fused)"}}
 
 
 def bench_precision(clb, workloads, torch, local, steps=300, warmup=20):
@@ -673,6 +686,8 @@ def main():
     torch.cuda.synchronize()
     barrier()
     final = D.reduce()
+    open_mask = (cfg["mat"] != 0) & (cfg["mat"] != 1)
+    bio_end = biomass_bytes([D.biomass(m) for m in range(M)], open_mask)
     D.close()
     del D
     ms = max_over_ranks(torch, sum(ms_blocks), world, "cuda")
@@ -684,13 +699,17 @@ def main():
     launches = sum(r["launches"] for r in reps)
 
     # roofline of the dominant kernel, the fused transport step: algorithmic bytes per open node =
-    # S x 2 x 7 x 4 B populations + 12 B velocity + 1 B material + M x 8 B biomass
-    alg_node = S * 2 * 7 * 4 + 3 * 4 + 1 + M * 8
+    # S x 2 x 7 x 4 B populations + 12 B velocity + 1 B material + the biomass bytes (flag, reads
+    # where it is set, writes where a microbe holds biomass), the mean of the timed region's first
+    # and last states (the biofilm grows in between)
+    bio_start = biomass_bytes(cfg["biomass"], open_mask)
+    alg_node = S * 2 * 7 * 4 + 3 * 4 + 1 + 0.5 * (bio_start[0] + bio_end[0])
     per_launch = ms_transport / max(1, iters)
     achieved = alg_node * n_open / (per_launch * 1e-3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic_per_launch("k_ade_aa_f32_pack256cube_8species"), "peak_source": peak_kind,
             "algorithmic_bytes_per_launch": alg_node * n_open, "algorithmic_bytes_per_node": alg_node,
+            "biomass_flagged_fraction": [bio_start[1], bio_end[1]],
             "kernel": "k_ade_aa (all 8 species fused, even/odd AA steps) + k_ade_neumann, the fused transport "
                       "step; mean device time per iteration from CUDA events on the handle's stream",
             "share_of_step": ms_transport / sum(ms_blocks)}
