@@ -489,11 +489,11 @@ def bench_speciation(clb, workloads, torch, local, steps=10):
 def bench_ensemble(clb, workloads, torch, local, peak, steps=5000):
     """96 independent uneven domains (the parameter-sweep configuration), FP32, each with a D3Q19
     flow and 3 D3Q7 species with Monod kinetics, advanced `steps` steps by the batch after its
-    autotuner (persistent item tables against per-lattice launches), timed with CUDA events on
-    the batch's stream. Roofline: algorithmic bytes per step = flow nodes x 2 x 19 x 4 B + transport
+    autotuner (persistent item tables against per-lattice launches, the flow step plain or staged),
+    timed with CUDA events on the batch's stream. Roofline: algorithmic bytes per step = flow nodes x 2 x 19 x 4 B + transport
     nodes x (3 species x 2 x 7 x 4 B + 3 x 4 B velocity + 1 B material), over the measured copy
-    bandwidth. Also timed: the per-lattice schedule (1000 steps) and the domains stepped one after
-    another through their own handles (20 steps)."""
+    bandwidth. Also timed: the per-lattice schedule with the plain per-node flow step (1000 steps)
+    and the domains stepped one after another through their own handles (20 steps)."""
     cfg = workloads.ensemble_uneven_packs()
     doms = []
     for d in cfg["domains"]:
@@ -513,12 +513,10 @@ def bench_ensemble(clb, workloads, torch, local, peak, steps=5000):
     nf, nt = B.counts()
     step_bytes = nf * 2 * 19 * 4 + nt * (3 * 2 * 7 * 4 + 3 * 4 + 1)
     ms = timed_steps(torch, stream, B.step, steps, 8) / steps
-    # the per-lattice schedule on the same domains
+    # the per-lattice schedule with the plain flow step on the same domains
     B.schedule(persistent=False)
     ms_lattice = timed_steps(torch, stream, B.step, 1000, 4) / 1000
-    if sched["persistent"]:
-        B.schedule(persistent=True, tile=sched["tile"], lag=sched["lag"], steps_per_launch=sched["steps_per_launch"],
-                   ctas_per_sm=sched["ctas_per_sm"])
+    B.schedule(**sched)
     # the same domains one by one (each call enqueues its own launches)
     k = 20
     torch.cuda.synchronize()
@@ -538,8 +536,8 @@ def bench_ensemble(clb, workloads, torch, local, peak, steps=5000):
             "steps": steps, "ms_per_step": ms, "domain_steps_per_s": n / (ms * 1e-3),
             "aggregate_mlups": (nf + 3 * nt) / (ms * 1e-3) / 1e6,
             "unit": "domain-steps / s; MLUPS = flow node + species x transport node updates / s (1e6)",
-            "schedule": sched, "per_lattice_ms_per_step": ms_lattice,
-            "speedup_vs_per_lattice": ms_lattice / ms,
+            "schedule": sched, "per_lattice_plain_ms_per_step": ms_lattice,
+            "speedup_vs_per_lattice_plain": ms_lattice / ms,
             "one_by_one_ms_per_step": dt1 * 1e3, "speedup_vs_one_by_one": dt1 / (ms * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "bytes_per_step": step_bytes},

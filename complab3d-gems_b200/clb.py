@@ -330,20 +330,6 @@ class Domain:
     def tune(self, key, value):
         self._check(lib().clb_tune(self.h, key.encode(), int(value)))
 
-    def schedule(self, persistent=True, tile=2048, lag=8, steps_per_launch=2, ctas_per_sm=4):
-        _check_global(lib().clb_batch_schedule(self.b, int(bool(persistent)), int(tile), int(lag),
-                                               int(steps_per_launch), int(ctas_per_sm)))
-
-    def get_schedule(self):
-        v = [C.c_int() for _ in range(5)]
-        _check_global(lib().clb_batch_get_schedule(self.b, *[C.byref(x) for x in v]))
-        return dict(persistent=bool(v[0].value), tile=v[1].value, lag=v[2].value, steps_per_launch=v[3].value,
-                    ctas_per_sm=v[4].value)
-
-    def set_stream(self, stream):
-        """stream: a cudaStream_t as an integer (torch.cuda.Stream().cuda_stream), or None."""
-        _check_global(lib().clb_batch_set_stream(self.b, C.c_void_p(stream) if stream else None))
-
     def autotune(self, steps=20):
         buf = C.create_string_buffer(512)
         self._check(lib().clb_autotune(self.h, steps, buf, 512))
@@ -805,15 +791,18 @@ class Batch:
     def step(self, n=1, flow=True, transport=True):
         _check_global(lib().clb_batch_step(self.b, int(n), int(flow), int(transport)))
 
-    def schedule(self, persistent=True, tile=2048, lag=8, steps_per_launch=2, ctas_per_sm=4):
-        _check_global(lib().clb_batch_schedule(self.b, int(bool(persistent)), int(tile), int(lag),
-                                               int(steps_per_launch), int(ctas_per_sm)))
+    def schedule(self, persistent=True, tile=2048, lag=8, steps_per_launch=2, ctas_per_sm=4, staged_flow=False):
+        """persistent: the item-table schedule; else one launch per lattice and step, the flow step
+        through the staged kernels when staged_flow (4- and 8-byte storage)."""
+        mode = 1 if persistent else (2 if staged_flow else 0)
+        _check_global(lib().clb_batch_schedule(self.b, mode, int(tile), int(lag), int(steps_per_launch),
+                                               int(ctas_per_sm)))
 
     def get_schedule(self):
         v = [C.c_int() for _ in range(5)]
         _check_global(lib().clb_batch_get_schedule(self.b, *[C.byref(x) for x in v]))
-        return dict(persistent=bool(v[0].value), tile=v[1].value, lag=v[2].value, steps_per_launch=v[3].value,
-                    ctas_per_sm=v[4].value)
+        return dict(persistent=v[0].value == 1, staged_flow=v[0].value == 2, tile=v[1].value, lag=v[2].value,
+                    steps_per_launch=v[3].value, ctas_per_sm=v[4].value)
 
     def set_stream(self, stream):
         """stream: a cudaStream_t as an integer (torch.cuda.Stream().cuda_stream), or None."""

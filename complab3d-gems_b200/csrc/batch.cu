@@ -31,6 +31,7 @@ struct clb_batch_s {
     clb::BatchView view{};
     int64_t flow_nodes = 0, ade_nodes = 0;
     int flow_threads = 256, flow_mult = 4, ade_mult = 1, neu_grid = 148;
+    bool flow_staged = false;  // the flow step through the staged kernels (4- and 8-byte storage)
     // graphs by (flow parity, ade parity, flow, ade, steps per launch (0: per lattice), tile, lag)
     std::map<std::tuple<int, int, int, int, int, int, int>, cudaGraphExec_t> graphs;
     // persistent schedule
@@ -235,6 +236,7 @@ clb_status batch_create(clb_handle* const* hs, int n, clb_batch** out) {
     b->view.faces = b->d_faces;
     b->view.foff_faces = b->d_face_off;
     b->view.nfaces = (int)faces.size();
+    b->view.status = b->d_sync;
     b->neu_grid = std::max<int64_t>(1, std::min<int64_t>((face_off.back() + 255) / 256, b->num_sms * 4));
     b->resident = batch_persistent_resident(b->has_ade ? b->ade_prec : b->flow_prec, b->nm, b->minb);
     if (b->has_flow && b->has_ade && b->flow_prec != b->ade_prec) b->persistent = false;  // one storage type per launch
@@ -318,8 +320,12 @@ static clb_status persist_launch(clb_batch* b, int steps, int fodd, int aodd, bo
 // one step of the requested lattices at the given parities, on the batch stream
 static void batch_launch_step(clb_batch* b, int fodd, int aodd, bool flow, bool ade) {
     if (flow) {
-        const int grid = b->num_sms * b->flow_mult;
-        launch_flow_batch(b->view, b->flow_prec, fodd != 0, grid, b->flow_threads, bstream(b));
+        if (b->flow_staged) {
+            launch_flow_batch_staged(b->view, b->flow_prec, fodd != 0, b->num_sms, bstream(b));
+        } else {
+            const int grid = b->num_sms * b->flow_mult;
+            launch_flow_batch(b->view, b->flow_prec, fodd != 0, grid, b->flow_threads, bstream(b));
+        }
     }
     if (ade) {
         launch_neumann_batch(b->view, b->ade_prec, aodd != 0, b->neu_grid, bstream(b));
@@ -498,6 +504,7 @@ clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len)
     if (b->has_flow) {
         float best = 1e30f;
         int bt = 256, bm = 4;
+        b->flow_staged = false;
         for (int threads : {128, 256})
             for (int mult : {2, 4, 8}) {
                 b->flow_threads = threads;
@@ -508,6 +515,16 @@ clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len)
                 rep += buf;
                 if (ms < best) { best = ms; bt = threads; bm = b->flow_mult; }
             }
+        bool staged = false;
+        if (flow_batch_staged_available(b->flow_prec)) {
+            b->flow_staged = true;
+            const float ms = time_steps(true, false);
+            char buf[96];
+            std::snprintf(buf, sizeof buf, "flow staged:%.1fus ", ms * 1e3f);
+            rep += buf;
+            if (ms < best) { best = ms; staged = true; }
+        }
+        b->flow_staged = staged;
         b->flow_threads = bt;
         b->flow_mult = bm;
         legacy += best;
@@ -595,7 +612,8 @@ clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len)
 // most PERSIST_MAX_STEPS, the register budget in resident CTAs per SM) or, persistent == 0, one
 // launch per lattice and step.
 clb_status batch_schedule(clb_batch* b, int persistent, int tile, int lag, int steps_per_launch, int ctas_per_sm) {
-    if (persistent) {
+    if (persistent < 0 || persistent > 2) return bfail(b, CLB_INVALID_ARG, "schedule: persistent is 0, 1 or 2");
+    if (persistent == 1) {
         if (b->has_flow && b->has_ade && b->flow_prec != b->ade_prec)
             return bfail(b, CLB_INVALID_ARG, "the persistent schedule needs one storage type for flow and transport");
         if (tile < 256 || tile % 256 || tile > (1 << 20) || lag < 1 || steps_per_launch < 2 ||
@@ -610,7 +628,10 @@ clb_status batch_schedule(clb_batch* b, int persistent, int tile, int lag, int s
         b->minb = ctas_per_sm;
         b->resident = batch_persistent_resident(prec, b->nm, ctas_per_sm);
     }
-    b->persistent = persistent != 0;
+    if (persistent == 2 && b->has_flow && !flow_batch_staged_available(b->flow_prec))
+        return bfail(b, CLB_INVALID_ARG, "schedule: the staged flow step needs 4- or 8-byte flow storage");
+    b->persistent = persistent == 1;
+    b->flow_staged = persistent == 2;
     drop_graphs(b);
     return CLB_OK;
 }
@@ -627,7 +648,7 @@ clb_status batch_set_stream(clb_batch* b, void* stream) {
 // The schedule in force (for reports).
 clb_status batch_get_schedule(clb_batch* b, int* persistent, int* tile, int* lag, int* steps_per_launch,
                               int* ctas_per_sm) {
-    if (persistent) *persistent = b->persistent ? 1 : 0;
+    if (persistent) *persistent = b->persistent ? 1 : (b->flow_staged ? 2 : 0);
     if (ctas_per_sm) *ctas_per_sm = b->minb;
     if (tile) *tile = b->tile;
     if (lag) *lag = b->lag;

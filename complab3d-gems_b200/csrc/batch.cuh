@@ -63,6 +63,7 @@ struct BatchView {
     const NeumannFace* faces;
     const int64_t* foff_faces;  // [nfaces + 1] prefix sums of the face sizes
     int nfaces;
+    int* status;  // nonzero: a bounded wait of a staged step gave up
 };
 
 constexpr int BATCH_MAX_DOMAINS = 2048;
@@ -93,8 +94,11 @@ struct PersistView {
     int64_t wait_ns;  // limit of one wait
 };
 
-// flow.cu
+// flow.cu (staged: the even step through bulk-copied tiles, the odd step with the next node's
+// gathers in flight, 4- and 8-byte storage; else the plain per-node step)
 void launch_flow_batch(const BatchView& B, int prec, bool odd, int grid, int threads, cudaStream_t st);
+bool flow_batch_staged_available(int prec);
+void launch_flow_batch_staged(const BatchView& B, int prec, bool odd, int num_sms, cudaStream_t st);
 // ade.cu (nm: species register bucket 1, 2, 4, 8 or 16)
 void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_mult, int num_sms, cudaStream_t st);
 void launch_neumann_batch(const BatchView& B, int prec, bool odd, int grid, cudaStream_t st);

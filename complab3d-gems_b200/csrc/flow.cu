@@ -31,6 +31,8 @@
 #include "tma.cuh"
 
 #include <algorithm>
+#include <mutex>
+#include <vector>
 #include <cmath>
 #include <cstring>
 
@@ -362,6 +364,220 @@ void launch_flow_batch(const BatchView& B, int prec, bool odd, int grid, int thr
         default: CLB_FB(__half, float); break;
     }
 #undef CLB_FB
+}
+
+// The staged batched steps: a CTA's run of the tile table is cut into segments of consecutive
+// tiles of one domain; for each segment the domain's description goes to shared memory and the
+// segment's nodes are stepped as the single-domain staged kernels step a lattice (the even step
+// through bulk-copied 256-node tiles, the odd step with each thread's next node's gathers in
+// flight). Tile-table runs start on 1024-node boundaries, so no two CTAs share a 256-node tile.
+
+// the segment of a CTA's run that starts at tile t (t < t1): tiles [t, returned) of one domain,
+// compact nodes [kb, ke)
+__device__ __forceinline__ int batch_segment(const BatchTile* __restrict__ tiles, int t, int t1, int64_t& kb,
+                                             int64_t& ke) {
+    const int d = tiles[t].d;
+    kb = tiles[t].first;
+    ke = kb;
+    int te = t;
+    while (te < t1 && tiles[te].d == d) {
+        ke = tiles[te].first + tiles[te].count;
+        ++te;
+    }
+    return te;
+}
+
+__device__ __forceinline__ void batch_load_domain(BatchDomain& sd, const BatchDomain* src, int tid, int nt) {
+    const uint64_t* a = reinterpret_cast<const uint64_t*>(src);
+    uint64_t* b = reinterpret_cast<uint64_t*>(&sd);
+    for (int q = tid; q < (int)(sizeof(BatchDomain) / 8); q += nt) b[q] = a[q];
+}
+
+template <typename TS, typename TC>
+__global__ void __launch_bounds__(PIPE_THREADS, 2) k_flow_batch_odd(const BatchView B) {
+    extern __shared__ __align__(16) unsigned char flow_smem[];
+    __shared__ __align__(16) BatchDomain sd;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    TS* buf = reinterpret_cast<TS*>(flow_smem);  // [2][19][nt]
+    const int per = (B.nft + gridDim.x - 1) / gridDim.x;
+    int t = blockIdx.x * per;
+    const int t1 = min(B.nft, t + per);
+    while (t < t1) {
+        int64_t kb, ke;
+        const int d = B.ftiles[t].d;
+        t = batch_segment(B.ftiles, t, t1, kb, ke);
+        __syncthreads();  // every thread is done with the previous domain
+        batch_load_domain(sd, B.dom + d, tid, nt);
+        __syncthreads();
+        TS* f = (TS*)sd.f;
+        const SparseView& S = sd.fs;
+        const FlowParams& P = sd.fp;
+        const uint32_t K32 = (uint32_t)S.KS;
+        const int64_t kw = sd.fkw, kE = sd.fke;
+        uint32_t A[19], C[19];
+        auto issue = [&](int64_t kk, const FlowMeta& M, int q, uint32_t (&ad)[19]) {
+            const OddRows R = odd_rows(S, kk, M);
+            TS* dst = buf + (q * 19) * nt + tid;
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                ad[i] = odd_src(i, kk, R, K32);
+                cp_async<sizeof(TS)>(dst + i * nt, f + ad[i]);
+            }
+        };
+        int64_t k = kb + tid;
+        FlowMeta cur, nxt;
+        if (k < ke) {
+            cur = flow_meta<true>(S, k);
+            issue(k, cur, 0, A);
+        }
+        cp_async_commit();
+        int64_t kn = k + nt;
+        if (kn < ke) nxt = flow_meta<true>(S, kn);
+        auto node = [&](int q, uint32_t (&ac)[19], uint32_t (&an)[19]) {
+            if (kn < ke) issue(kn, nxt, q ^ 1, an);
+            cp_async_commit();
+            const int64_t knn = kn + nt;
+            FlowMeta nn;
+            if (knn < ke) nn = flow_meta<true>(S, knn);
+            cp_async_wait_group<1>();  // this node's populations have landed
+            const int code = cur.code;
+            if (P.dyn[code] != DYN_BB) {
+                TC g[19];
+                const TS* src = buf + (q * 19) * nt + tid;
+#pragma unroll
+                for (int i = 0; i < 19; ++i) g[i] = ld<TS, TC>(src + i * nt);
+                if (P.dyn[code] == DYN_BGK) {
+                    if (k < kw) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
+                    else if (k >= kE) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
+                    bgk19<TC>(g, (TC)P.omega[code]);
+                }
+#pragma unroll
+                for (int i = 0; i < 19; ++i) st<TS, TC>(f + ac[q19opp(i)], g[i]);
+            }
+            k = kn;
+            kn = knn;
+            cur = nxt;
+            nxt = nn;
+        };
+        while (k < ke) {
+            node(0, A, C);
+            if (k >= ke) break;
+            node(1, C, A);
+        }
+        cp_async_wait_group<0>();
+    }
+}
+
+template <typename TS, typename TC>
+__global__ void __launch_bounds__(TILE, sizeof(TS) == 8 ? 2 : 4) k_flow_batch_even(const BatchView B) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    TS* stages = reinterpret_cast<TS*>(smem_raw);
+    __shared__ __align__(8) uint64_t full[NSTAGE];
+    __shared__ __align__(16) BatchDomain sd;
+    __shared__ int s_abort;
+    const int tid = threadIdx.x;
+    const uint32_t row_bytes = TILE * sizeof(TS);
+    if (tid == 0) {
+        for (int q = 0; q < NSTAGE; ++q) mbar_init(&full[q], 1);
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+    const int per = (B.nft + gridDim.x - 1) / gridDim.x;
+    int t = blockIdx.x * per;
+    const int t1 = min(B.nft, t + per);
+    int j = 0;  // tiles stepped by this CTA: stage j % NSTAGE, its phase (j / NSTAGE) & 1
+    while (t < t1) {
+        int64_t kb, ke;
+        const int d = B.ftiles[t].d;
+        t = batch_segment(B.ftiles, t, t1, kb, ke);
+        __syncthreads();  // every thread is done with the previous domain
+        batch_load_domain(sd, B.dom + d, tid, TILE);
+        __syncthreads();
+        TS* f = (TS*)sd.f;
+        TS* link = (TS*)sd.flink;
+        const SparseView& S = sd.fs;
+        const FlowParams& P = sd.fp;
+        const int64_t K = S.K, KS = S.KS;
+        const int tb = (int)(kb / TILE), te = (int)((ke + TILE - 1) / TILE);
+        auto issue_load = [&](int tt, int q) {
+            TS* dst = stages + (size_t)q * 19 * TILE;
+            mbar_expect_tx(&full[q], 19 * row_bytes);
+            for (int i = 0; i < 19; ++i)
+                bulk_g2s(dst + i * TILE, f + (int64_t)i * KS + (int64_t)tt * TILE, row_bytes, &full[q]);
+        };
+        if (tid == 0) {
+            bulk_wait_read_all();  // the stages' earlier bulk stores have read them
+            for (int q = 0; q < NSTAGE - 1; ++q)
+                if (tb + q < te) issue_load(tb + q, (j + q) % NSTAGE);
+        }
+        for (int tt = tb; tt < te; ++tt, ++j) {
+            const int q = j % NSTAGE;
+            TS* buf = stages + (size_t)q * 19 * TILE;
+            const int tn = tt + NSTAGE - 1;
+            if (tid == 0 && tn < te) {
+                bulk_wait_read_all();
+                issue_load(tn, (j + NSTAGE - 1) % NSTAGE);
+            }
+            const int64_t k = (int64_t)tt * TILE + tid;
+            int code = 0;
+            if (k < K) code = S.code[k];
+            const bool live = k < K && P.dyn[code] != DYN_BB;
+            uint32_t wm = 0;
+            int lb = 0;
+            TC xv[19];
+            if (live) {
+                const uint32_t m0 = S.meta[2 * k];
+                wm = m0 & 0x7FFFFu;
+                lb = S.tlb[tt] + (int)(m0 >> 19);
+                int r = 0;
+#pragma unroll
+                for (int i = 1; i < 19; ++i) {
+                    const bool wl = (wm >> i) & 1u;
+                    xv[q19opp(i)] = wl ? ld<TS, TC>(link + lb + r) : (TC)0;
+                    r += wl;
+                }
+            }
+            if (!mbar_wait(&full[q], (uint32_t)((j / NSTAGE) & 1))) {
+                if (tid == 0) {
+                    atomicExch(B.status, 1);
+                    s_abort = 1;
+                }
+            }
+            __syncthreads();
+            if (s_abort) break;
+            if (live) {
+                TC g[19];
+#pragma unroll
+                for (int i = 0; i < 19; ++i) {
+                    const bool wsrc = i != 0 && ((wm >> q19opp(i)) & 1u);
+                    g[i] = wsrc ? xv[i] : ld<TS, TC>(buf + i * TILE + tid);
+                }
+                if (P.dyn[code] == DYN_BGK) {
+                    if (k < sd.fkw) regularize19<TC>(g, -1, (TC)(P.rho_w - 1.0));
+                    else if (k >= sd.fke) regularize19<TC>(g, 1, (TC)(P.rho_e - 1.0));
+                    bgk19<TC>(g, (TC)P.omega[code]);
+                }
+                int r = 0;
+#pragma unroll
+                for (int i = 0; i < 19; ++i) {
+                    const bool wl = (wm >> i) & 1u;
+                    if (wl) st<TS, TC>(link + lb + r, g[i]);
+                    else st<TS, TC>(buf + q19opp(i) * TILE + tid, g[i]);
+                    r += wl;
+                }
+            }
+            fence_async_smem();  // this thread's writes to the tile, ordered before the bulk stores read it
+            __syncthreads();
+            if (tid == 0) {
+                for (int i = 0; i < 19; ++i)
+                    bulk_s2g(f + (int64_t)i * KS + (int64_t)tt * TILE, buf + i * TILE, row_bytes);
+                bulk_commit();
+            }
+        }
+        if (s_abort) break;
+    }
+    if (tid == 0) bulk_wait_all();
 }
 
 // PressureGradient equilibrium (complab_functions.hh:82-94): BGK nodes t_i (rho(x) - 1),
@@ -973,6 +1189,43 @@ clb_status flow_autotune(clb_handle* h, int steps, char* report, int report_len)
         report[report_len - 1] = 0;
     }
     return cuda_check(h, e, "autotune");
+}
+
+bool flow_batch_staged_available(int prec) { return prec == CLB_F64 || prec == CLB_F32; }
+
+// resident CTAs of a staged batched kernel times the SM count (set up once per kernel)
+static int batch_staged_grid(const void* kern, int threads, size_t smem, int num_sms) {
+    struct Known { const void* kern; int blocks; };
+    static std::mutex mu;
+    static std::vector<Known> known;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto& kv : known)
+        if (kv.kern == kern) return kv.blocks * num_sms;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, smem) != cudaSuccess || nb < 1) nb = 1;
+    known.push_back({kern, nb});
+    return nb * num_sms;
+}
+
+template <typename TS, typename TC>
+static void launch_flow_batch_staged_t(const BatchView& B, bool odd, int num_sms, cudaStream_t st) {
+    if (odd) {
+        auto kern = k_flow_batch_odd<TS, TC>;
+        const size_t sm = pipe_smem<TS>();
+        const int grid = std::max(1, std::min(batch_staged_grid((const void*)kern, PIPE_THREADS, sm, num_sms), B.nft));
+        kern<<<grid, PIPE_THREADS, sm, st>>>(B);
+    } else {
+        auto kern = k_flow_batch_even<TS, TC>;
+        const size_t sm = even_smem<TS>();
+        const int grid = std::max(1, std::min(batch_staged_grid((const void*)kern, TILE, sm, num_sms), B.nft));
+        kern<<<grid, TILE, sm, st>>>(B);
+    }
+}
+
+void launch_flow_batch_staged(const BatchView& B, int prec, bool odd, int num_sms, cudaStream_t st) {
+    if (prec == CLB_F64) launch_flow_batch_staged_t<double, double>(B, odd, num_sms, st);
+    else launch_flow_batch_staged_t<float, float>(B, odd, num_sms, st);
 }
 
 }  // namespace clb

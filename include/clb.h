@@ -551,12 +551,14 @@ clb_status clb_batch_step(clb_batch* batch, int n, int flow, int transport);
  * counters show them). */
 clb_status clb_batch_autotune(clb_batch* batch, int steps, char* report, int report_len);
 
-/* Sets the schedule: persistent != 0 with `tile` nodes per item (a multiple of 256), a lag of
+/* Sets the schedule: persistent == 1 with `tile` nodes per item (a multiple of 256), a lag of
  * `lag` >= 1 domains between a domain's successive steps in the item table, an even 2..8 steps
  * per launch, and registers budgeted for `ctas_per_sm` resident CTAs per SM (4 always; 6 and 8
  * for FP32 / FP16 storage with up to 4 mobile species); persistent == 0: one launch per lattice
- * and step (the other arguments are ignored). The persistent schedule needs one storage type for
- * flow and transport. */
+ * and step (the other arguments are ignored); persistent == 2: the same with the flow step
+ * through the staged kernels (bulk-copied tiles on even steps, the next node's gathers in flight
+ * on odd steps; FP32 / FP64 flow storage). The persistent schedule needs one storage type for
+ * flow and transport. clb_batch_get_schedule reports the same three values. */
 clb_status clb_batch_schedule(clb_batch* batch, int persistent, int tile, int lag, int steps_per_launch,
                               int ctas_per_sm);
 clb_status clb_batch_get_schedule(clb_batch* batch, int* persistent, int* tile, int* lag, int* steps_per_launch,

@@ -84,6 +84,8 @@ def test_batch_rejects_mixed_parity(clb):
 
 @pytest.mark.parametrize("prec,sched", [
     ("F32", dict(persistent=False)),
+    ("F32", dict(persistent=False, staged_flow=True)),
+    ("F64", dict(persistent=False, staged_flow=True)),
     ("F32", dict(tile=256, lag=1, steps_per_launch=2)),
     ("F32", dict(tile=1024, lag=3, steps_per_launch=8, ctas_per_sm=8)),
     ("F32", dict(tile=2048, lag=8, steps_per_launch=2, ctas_per_sm=6)),
@@ -103,6 +105,7 @@ def test_batch_schedules_match_single_domains(clb, prec, sched):
     batch.schedule(**sched)
     got = batch.get_schedule()
     assert got["persistent"] == sched.get("persistent", True)
+    assert got["staged_flow"] == sched.get("staged_flow", False)
     for n, flow, tr in ((17, True, True), (9, True, False), (6, False, True), (3, True, True)):
         for D in A:
             if flow:
@@ -121,4 +124,14 @@ def test_batch_schedule_rejects_bad_settings(clb):
     for bad in (dict(tile=300), dict(lag=0), dict(steps_per_launch=3), dict(steps_per_launch=10), dict(ctas_per_sm=5)):
         with pytest.raises(clb.ClbError):
             batch.schedule(**bad)
+    batch.close()
+
+
+def test_batch_staged_flow_needs_four_byte_storage(clb):
+    cfg = workloads.ensemble_uneven_packs(n_domains=2, seed=23, scale=0.5)
+    B = build(clb, cfg, clb.F16S)
+    batch = clb.Batch(B)
+    with pytest.raises(clb.ClbError):
+        batch.schedule(persistent=False, staged_flow=True)
+    assert batch.get_schedule()["staged_flow"] is False
     batch.close()
