@@ -684,8 +684,6 @@ def main():
     torch.cuda.synchronize()
     barrier()
     final = D.reduce()
-    open_mask = (cfg["mat"] != 0) & (cfg["mat"] != 1)
-    bio_end = biomass_bytes([D.biomass(m) for m in range(M)], open_mask)
     D.close()
     del D
     ms = max_over_ranks(torch, sum(ms_blocks), world, "cuda")
@@ -695,22 +693,6 @@ def main():
     value = world * upd / (ms * 1e-3) / 1e6
     ms_transport = sum(r["ms_transport"] for r in reps)
     launches = sum(r["launches"] for r in reps)
-
-    # roofline of the dominant kernel, the fused transport step: algorithmic bytes per open node =
-    # S x 2 x 7 x 4 B populations + 12 B velocity + 1 B material + the biomass bytes (flag, reads
-    # where it is set, writes where a microbe holds biomass), the mean of the timed region's first
-    # and last states (the biofilm grows in between)
-    bio_start = biomass_bytes(cfg["biomass"], open_mask)
-    alg_node = S * 2 * 7 * 4 + 3 * 4 + 1 + 0.5 * (bio_start[0] + bio_end[0])
-    per_launch = ms_transport / max(1, iters)
-    achieved = alg_node * n_open / (per_launch * 1e-3) / 1e9
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic_per_launch("k_ade_aa_f32_pack256cube_8species"), "peak_source": peak_kind,
-            "algorithmic_bytes_per_launch": alg_node * n_open, "algorithmic_bytes_per_node": alg_node,
-            "biomass_flagged_fraction": [bio_start[1], bio_end[1]],
-            "kernel": "k_ade_aa (all 8 species fused, even/odd AA steps) + k_ade_neumann, the fused transport "
-                      "step; mean device time per iteration from CUDA events on the handle's stream",
-            "share_of_step": ms_transport / sum(ms_blocks)}
 
     # end to end through the C ABI with host buffers: the material map and the biomass fields go in
     # from pinned host memory; create, flow solve from rest, species set-up, the same K update
@@ -746,6 +728,26 @@ def main():
         e2e_val = world * e_upd / t_e2e / 1e6
         h2d = mat_host.nbytes + bio_host.nbytes
         d2h = out_host.nbytes
+
+    # roofline of the dominant kernel, the fused transport step: algorithmic bytes per open node =
+    # S x 2 x 7 x 4 B populations + 12 B velocity + 1 B material + the biomass bytes (flag, reads
+    # where it is set, writes where a microbe holds biomass), the mean of the first and last states
+    # of the K intervals (the biofilm grows in between)
+    # (the last state from the end-to-end job, which runs the same intervals from the same start and
+    # reads its biomass back anyway)
+    open_mask = (cfg["mat"] != 0) & (cfg["mat"] != 1)
+    bio_start = biomass_bytes(cfg["biomass"], open_mask)
+    bio_end = biomass_bytes(out_host[S:S + M], open_mask) if t_e2e is not None else bio_start
+    alg_node = S * 2 * 7 * 4 + 3 * 4 + 1 + 0.5 * (bio_start[0] + bio_end[0])
+    per_launch = ms_transport / max(1, iters)
+    achieved = alg_node * n_open / (per_launch * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic_per_launch("k_ade_aa_f32_pack256cube_8species"), "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": alg_node * n_open, "algorithmic_bytes_per_node": alg_node,
+            "biomass_flagged_fraction": [bio_start[1], bio_end[1]],
+            "kernel": "k_ade_aa (all 8 species fused, even/odd AA steps) + k_ade_neumann, the fused transport "
+                      "step; mean device time per iteration from CUDA events on the handle's stream",
+            "share_of_step": ms_transport / sum(ms_blocks)}
 
     extra = {}
     if rank == 0 and world == 1 and not a.no_extra and a.scale == 1.0:
