@@ -1436,29 +1436,49 @@ void launch_neumann_batch(const BatchView& B, int prec, bool odd, int grid, cuda
     }
 }
 
+// `resident` blocks per SM the shared-memory carveout is sized for (the rest of the SM stays L1,
+// which the odd step's neighbour gathers reuse); set on every launch, since the batch's autotuner
+// tries several
 template <typename TS, typename TC, bool ODD, int NM>
-static void launch_ade_batch_t(const BatchView& B, int grid_mult, int num_sms, cudaStream_t st) {
+static void launch_ade_batch_t(const BatchView& B, int grid_mult, int resident, int num_sms, cudaStream_t st) {
     auto kern = k_ade_batch<TS, TC, ODD, NM>;
     const int sm = ade_slot_bytes<TC, NM>();
-    const int per_sm = ade_grid_for((const void*)kern, sm, 1, ADE_THREADS, ADE_RESIDENT, (int)sizeof(BatchDomain));
-    const int grid = std::max(1, std::min(per_sm * num_sms * grid_mult, B.nat));
+    const int per_block = sm + (int)sizeof(BatchDomain) + 1024;  // the runtime reserves 1 KB per block
+    const int fit = std::max(1, std::min(resident, (228 * 1024) / per_block));
+    const int pct = std::min(100, (int)((100LL * fit * per_block + 228 * 1024 - 1) / (228 * 1024)));
+    if (sm > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, ADE_THREADS, sm) != cudaSuccess || nb < 1) nb = 1;
+    nb = std::min(nb, fit);
+    const int grid = std::max(1, std::min(nb * num_sms * grid_mult, B.nat));
     kern<<<grid, ADE_THREADS, sm, st>>>(B);
 }
 
 template <typename TS, typename TC, bool ODD>
-static void launch_ade_batch_p(const BatchView& B, int nm, int grid_mult, int num_sms, cudaStream_t st) {
-    if (nm <= 1) launch_ade_batch_t<TS, TC, ODD, 1>(B, grid_mult, num_sms, st);
-    else if (nm <= 2) launch_ade_batch_t<TS, TC, ODD, 2>(B, grid_mult, num_sms, st);
-    else if (nm <= 4) launch_ade_batch_t<TS, TC, ODD, 4>(B, grid_mult, num_sms, st);
-    else if (nm <= 8) launch_ade_batch_t<TS, TC, ODD, 8>(B, grid_mult, num_sms, st);
-    else launch_ade_batch_t<TS, TC, ODD, 16>(B, grid_mult, num_sms, st);
+static void launch_ade_batch_p(const BatchView& B, int nm, int grid_mult, int resident, int num_sms, cudaStream_t st) {
+    if (nm <= 1) launch_ade_batch_t<TS, TC, ODD, 1>(B, grid_mult, resident, num_sms, st);
+    else if (nm <= 2) launch_ade_batch_t<TS, TC, ODD, 2>(B, grid_mult, resident, num_sms, st);
+    else if (nm <= 4) launch_ade_batch_t<TS, TC, ODD, 4>(B, grid_mult, resident, num_sms, st);
+    else if (nm <= 8) launch_ade_batch_t<TS, TC, ODD, 8>(B, grid_mult, resident, num_sms, st);
+    else launch_ade_batch_t<TS, TC, ODD, 16>(B, grid_mult, resident, num_sms, st);
 }
 
-void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_mult, int num_sms, cudaStream_t st) {
+void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_mult, int resident, int num_sms,
+                      cudaStream_t st) {
     switch (prec) {
-        case CLB_F64: if (odd) launch_ade_batch_p<double, double, true>(B, nm, grid_mult, num_sms, st); else launch_ade_batch_p<double, double, false>(B, nm, grid_mult, num_sms, st); break;
-        case CLB_F32: if (odd) launch_ade_batch_p<float, float, true>(B, nm, grid_mult, num_sms, st); else launch_ade_batch_p<float, float, false>(B, nm, grid_mult, num_sms, st); break;
-        default: if (odd) launch_ade_batch_p<__half, float, true>(B, nm, grid_mult, num_sms, st); else launch_ade_batch_p<__half, float, false>(B, nm, grid_mult, num_sms, st); break;
+        case CLB_F64:
+            if (odd) launch_ade_batch_p<double, double, true>(B, nm, grid_mult, resident, num_sms, st);
+            else launch_ade_batch_p<double, double, false>(B, nm, grid_mult, resident, num_sms, st);
+            break;
+        case CLB_F32:
+            if (odd) launch_ade_batch_p<float, float, true>(B, nm, grid_mult, resident, num_sms, st);
+            else launch_ade_batch_p<float, float, false>(B, nm, grid_mult, resident, num_sms, st);
+            break;
+        default:
+            if (odd) launch_ade_batch_p<__half, float, true>(B, nm, grid_mult, resident, num_sms, st);
+            else launch_ade_batch_p<__half, float, false>(B, nm, grid_mult, resident, num_sms, st);
+            break;
     }
 }
 

@@ -30,7 +30,7 @@ struct clb_batch_s {
     clb::NeumannFace* d_faces = nullptr;
     clb::BatchView view{};
     int64_t flow_nodes = 0, ade_nodes = 0;
-    int flow_threads = 256, flow_mult = 4, ade_mult = 1, neu_grid = 148;
+    int flow_threads = 256, flow_mult = 4, ade_mult = 1, ade_resident = 4, neu_grid = 148;
     bool flow_staged = false;  // the flow step through the staged kernels (4- and 8-byte storage)
     // graphs by (flow parity, ade parity, flow, ade, steps per launch (0: per lattice), tile, lag)
     std::map<std::tuple<int, int, int, int, int, int, int>, cudaGraphExec_t> graphs;
@@ -329,7 +329,7 @@ static void batch_launch_step(clb_batch* b, int fodd, int aodd, bool flow, bool 
     }
     if (ade) {
         launch_neumann_batch(b->view, b->ade_prec, aodd != 0, b->neu_grid, bstream(b));
-        launch_ade_batch(b->view, b->ade_prec, aodd != 0, b->nm, b->ade_mult, b->num_sms, bstream(b));
+        launch_ade_batch(b->view, b->ade_prec, aodd != 0, b->nm, b->ade_mult, b->ade_resident, b->num_sms, bstream(b));
     }
 }
 
@@ -451,8 +451,8 @@ clb_status batch_step(clb_batch* b, int n, int flow_on, int ade_on) {
 }
 
 // Times the schedules of the batched steps and keeps the fastest. Per-lattice launches: flow with
-// 128 or 256 threads per block and 2, 4 or 8 blocks per SM, transport with 1 or 2 times the
-// resident grid. Persistent launches (when the lattices share one storage type): tiles of 1024,
+// 128 or 256 threads per block and 2, 4 or 8 blocks per SM, or the staged flow kernels; transport
+// with shared memory for 4 or 6 resident blocks per SM and 1 or 2 times the resident grid. Persistent launches (when the lattices share one storage type): tiles of 1024,
 // 2048 or 4096 nodes, lags of 2, 8 or 32 domains, 2 or 8 steps per launch, registers budgeted for
 // 4, 6 or 8 resident CTAs per SM where those kernels are built. Every timed step is a
 // real step of the domains: their iteration counters show the advance.
@@ -531,16 +531,19 @@ clb_status batch_autotune(clb_batch* b, int steps, char* report, int report_len)
     }
     if (b->has_ade) {
         float best = 1e30f;
-        int bm = 1;
-        for (int mult : {1, 2}) {
-            b->ade_mult = mult;
-            const float ms = time_steps(false, true);
-            char buf[96];
-            std::snprintf(buf, sizeof buf, "transport x%d:%.1fus ", mult, ms * 1e3f);
-            rep += buf;
-            if (ms < best) { best = ms; bm = mult; }
-        }
+        int bm = 1, br = 4;
+        for (int resident : {4, 6})
+            for (int mult : {1, 2}) {
+                b->ade_mult = mult;
+                b->ade_resident = resident;
+                const float ms = time_steps(false, true);
+                char buf[96];
+                std::snprintf(buf, sizeof buf, "transport %dx%d:%.1fus ", resident, mult, ms * 1e3f);
+                rep += buf;
+                if (ms < best) { best = ms; bm = mult; br = resident; }
+            }
         b->ade_mult = bm;
+        b->ade_resident = br;
         legacy += best;
     }
     // the flow and transport steps of the per-lattice schedule run one after the other

@@ -100,7 +100,8 @@ void launch_flow_batch(const BatchView& B, int prec, bool odd, int grid, int thr
 bool flow_batch_staged_available(int prec);
 void launch_flow_batch_staged(const BatchView& B, int prec, bool odd, int num_sms, cudaStream_t st);
 // ade.cu (nm: species register bucket 1, 2, 4, 8 or 16)
-void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_mult, int num_sms, cudaStream_t st);
+void launch_ade_batch(const BatchView& B, int prec, bool odd, int nm, int grid_mult, int resident, int num_sms,
+                      cudaStream_t st);
 void launch_neumann_batch(const BatchView& B, int prec, bool odd, int grid, cudaStream_t st);
 // the persistent schedule: one launch runs the whole item table
 void launch_batch_persistent(const PersistView& V, int prec, int nm, int minb, int blocks_per_sm, int num_sms,
