@@ -238,6 +238,30 @@ __device__ __forceinline__ void ca_list_append(int32_t* __restrict__ out, unsign
     if (listed) out[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)n;
 }
 
+// appends n (where `listed`) to `out` (count in *nout) with one atomic per block: a pass over a
+// list runs with whole blocks in step, and one counter taken by every warp of the grid would
+// serialise thousands of atomics on one address. Every thread of the block calls it; s_cnt holds
+// blockDim.x / 32 + 1 counts.
+__device__ __forceinline__ void ca_list_append_block(int32_t* __restrict__ out, unsigned int* nout, int64_t n,
+                                                     bool listed, unsigned int* s_cnt) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned int bal = __ballot_sync(0xffffffffu, listed);
+    if (lane == 0) s_cnt[w] = (unsigned int)__popc(bal);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int tot = 0;
+        for (int i = 0; i < nw; ++i) {
+            const unsigned int c = s_cnt[i];
+            s_cnt[i] = tot;
+            tot += c;
+        }
+        s_cnt[nw] = tot ? atomicAdd(nout, tot) : 0u;
+    }
+    __syncthreads();
+    if (listed) out[s_cnt[nw] + s_cnt[w] + (unsigned int)__popc(bal & ((1u << lane) - 1u))] = (int32_t)n;
+    __syncthreads();  // the counts are reused by the next call
+}
+
 // updateLocalMaskNtotalLattices3D. FULL: over every voxel; each thread takes UNR voxels a grid
 // stride apart per round and issues their loads together, so the pass is not bound by one voxel's
 // latency. Otherwise over the voxels of in[0, n_in) and in2[0, n_in2) (disjoint lists), every other
@@ -299,8 +323,10 @@ __device__ void ca_mask_pass(const CaView& C, const CaBufs& B, CaScalars* sc, co
         }
     } else {
         const int64_t n_all = (int64_t)n_in + n_in2;
-        const int64_t span = (n_all + 31) / 32 * 32;
-        for (int64_t j = t0; j < span; j += S) {
+        __shared__ unsigned int s_cnt[CA_THREADS / 32 + 1];
+        // whole blocks run the loop together (the list append is block-wide)
+        for (int64_t jb = (int64_t)blockIdx.x * blockDim.x; jb < n_all; jb += S) {
+            const int64_t j = jb + threadIdx.x;
             bool listed = false;
             int64_t n = 0;
             if (j < n_all) {
@@ -311,20 +337,30 @@ __device__ void ca_mask_pass(const CaView& C, const CaBufs& B, CaScalars* sc, co
                 for (int m = 0; m < C.M; ++m) bm[m] = op ? B.bio[(int64_t)m * G.N + n] : 0.0;
                 listed = ca_mask_voxel<true>(C, B, sc, n, mk, B.total[n], bm, best, msum);
             }
-            ca_list_append(out, &sc->nout, n, listed);
+            ca_list_append_block(out, &sc->nout, n, listed, s_cnt);
         }
     }
-    // block reduction, then one atomic per warp
+    // warp, then block reduction; one atomic per block, and none where the value is the identity
     for (int o = 16; o > 0; o >>= 1) {
         best = max(best, __shfl_down_sync(0xffffffffu, best, o));
         msum += __shfl_down_sync(0xffffffffu, msum, o);
     }
-    // warps whose values are the identity (most of a list pass's warps have no voxel) leave the
-    // two contended counters alone
+    __shared__ long long s_best[CA_THREADS / 32], s_msum[CA_THREADS / 32];
     if ((threadIdx.x & 31) == 0) {
-        if (best > 0) atomicMax(&sc->gmax, best);
-        if (msum != 0) atomicAdd((unsigned long long*)&sc->msum, (unsigned long long)msum);
+        s_best[threadIdx.x >> 5] = best;
+        s_msum[threadIdx.x >> 5] = msum;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long b = 0, m = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            b = max(b, s_best[i]);
+            m += s_msum[i];
+        }
+        if (b > 0) atomicMax(&sc->gmax, b);
+        if (m != 0) atomicAdd((unsigned long long*)&sc->msum, (unsigned long long)m);
+    }
+    __syncthreads();  // the block's partials are reused by the next pass of a cooperative step
 }
 
 // ------------------------------------------------------------------ push sweep
