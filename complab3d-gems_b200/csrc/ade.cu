@@ -1227,8 +1227,7 @@ clb_status ade_set_biomass(clb_handle* h, int M, const double* b) {
 
 // Resident blocks per SM of a transport-step instantiation with `smem` bytes of shared memory
 // (set up once per instantiation), times the SM count: the persistent grid.
-static int ade_grid_for(const void* kern, int smem, int num_sms, int threads, int resident = ADE_RESIDENT,
-                        int static_smem = 0) {
+static int ade_grid_for(const void* kern, int smem, int num_sms, int threads, int resident = ADE_RESIDENT) {
     struct Known { const void* kern; int smem, threads, blocks; };
     static std::mutex mu;
     static std::vector<Known> known;
@@ -1243,7 +1242,7 @@ static int ade_grid_for(const void* kern, int smem, int num_sms, int threads, in
     // cache, which the odd step's neighbour gathers reuse (five resident blocks with less L1 ran
     // the odd step slower on B200; the even step, which reads only its own slots, gained from five).
     {
-        const int per_block = smem + static_smem + 1024;  // the runtime reserves 1 KB per block
+        const int per_block = smem + 1024;  // the runtime reserves 1 KB per block
         const int fit = std::max(1, (228 * 1024) / per_block);
         const int res = std::min(resident, fit);
         const int pct = (int)((100LL * res * per_block + 228 * 1024 - 1) / (228 * 1024));
