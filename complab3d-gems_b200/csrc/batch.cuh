@@ -42,6 +42,9 @@ struct BatchTile {
 };
 constexpr int BATCH_FLOW_TILE = 1024;  // flow nodes per tile
 constexpr int BATCH_ADE_TILE = 512;    // transport nodes per tile
+// the staged flow kernels step whole 256-node tiles of the layout: a run of the tile table must not
+// split one
+static_assert(BATCH_FLOW_TILE % TILE == 0, "flow tiles are whole layout tiles");
 
 // One x-face of one domain that at least one mobile species treats as Neumann
 struct NeumannFace {
