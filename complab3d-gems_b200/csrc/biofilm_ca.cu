@@ -1,6 +1,6 @@
 // biofilm_ca.cu -- the biofilm cellular automaton: excess biomass pushed to face neighbours
-// ('fraction' mode), the mask / total-biomass update and the age wavefront, on the GPU with the
-// same results as the sequential lexicographic algorithm.
+// ('fraction' and 'half' modes), the mask / total-biomass update and the age wavefront, on the
+// GPU with the same results as the sequential lexicographic algorithm.
 //
 // Reference behaviour (complab.cpp:2792-3055 and :3074-3079):
 //   updateLocalMaskNtotalLattices3D (complab3d_processors_part2.hh:71-259): the total biomass of
