@@ -22,14 +22,25 @@
 
 namespace clb {
 
+// The solver is built for tableau shapes fixed at compile time (NC components, NS species; the
+// loops unroll and the per-voxel arrays live in registers) and for any shape (NC = NS = 0: sizes
+// from the parameters, arrays of the largest size in local memory). The arithmetic and its order
+// are the same in every build.
+#define EQ_NC(NC) ((NC) > 0 ? (NC) : CLB_MAX_COMPONENTS)
+#define EQ_NS(NS) ((NS) > 0 ? (NS) : CLB_MAX_EQ_SPECIES)
+
+template <int NC, int NS>
 __device__ __forceinline__ void eq_species(const SpecParams& P, const double* x, const double* init, double* c) {
-    for (int i = 0; i < P.ns; ++i) {
+    const int nc = NC > 0 ? NC : P.nc, ns = NS > 0 ? NS : P.ns;
+#pragma unroll (NS > 0 ? NS : 1)
+    for (int i = 0; i < ns; ++i) {
         if (!P.eq[i]) {
             c[i] = init[i] > EQ_MIN_C ? fmin(init[i], EQ_MAX_C) : EQ_MIN_C;
             continue;
         }
         double lc = P.logK[i];
-        for (int j = 0; j < P.nc; ++j) lc = fma(P.S[i * CLB_MAX_COMPONENTS + j], x[j], lc);
+#pragma unroll (NC > 0 ? NC : 1)
+        for (int j = 0; j < nc; ++j) lc = fma(P.S[i * CLB_MAX_COMPONENTS + j], x[j], lc);
         lc = fmax(fmin(lc, EQ_MAX_LOG), EQ_MIN_LOG);
         double v = exp10(lc);
         if (isnan(v) || isinf(v)) v = init[i] > EQ_MIN_C ? init[i] : EQ_MIN_C;
@@ -40,27 +51,35 @@ __device__ __forceinline__ void eq_species(const SpecParams& P, const double* x,
 // Inside the Newton loop the species follow mass action without the [1e-30, 10] clamps (a
 // species saturated at a clamp has a zero derivative the Jacobian does not see, and the iteration
 // stalls from a far initial guess); the clamps apply to the answer only.
+template <int NC, int NS>
 __device__ __forceinline__ void eq_species_free(const SpecParams& P, const double* x, const double* init, double* c) {
-    for (int i = 0; i < P.ns; ++i) {
+    const int nc = NC > 0 ? NC : P.nc, ns = NS > 0 ? NS : P.ns;
+#pragma unroll (NS > 0 ? NS : 1)
+    for (int i = 0; i < ns; ++i) {
         if (!P.eq[i]) {
             c[i] = init[i] > EQ_MIN_C ? fmin(init[i], EQ_MAX_C) : EQ_MIN_C;
             continue;
         }
         double lc = P.logK[i];
-        for (int j = 0; j < P.nc; ++j) lc = fma(P.S[i * CLB_MAX_COMPONENTS + j], x[j], lc);
+#pragma unroll (NC > 0 ? NC : 1)
+        for (int j = 0; j < nc; ++j) lc = fma(P.S[i * CLB_MAX_COMPONENTS + j], x[j], lc);
         c[i] = exp10(fmax(fmin(lc, 300.0), -300.0));
     }
 }
 
 constexpr double EQ_MAX_STEP = 2.0;  // largest log10 change of a component in one Newton step
 
+template <int NC, int NS>
 __device__ __forceinline__ double eq_residual(const SpecParams& P, const double* x, const double* T,
                                               const double* init, double* c, double* F) {
-    eq_species_free(P, x, init, c);
+    const int nc = NC > 0 ? NC : P.nc, ns = NS > 0 ? NS : P.ns;
+    eq_species_free<NC, NS>(P, x, init, c);
     double s = 0;
-    for (int j = 0; j < P.nc; ++j) {
+#pragma unroll (NC > 0 ? NC : 1)
+    for (int j = 0; j < nc; ++j) {
         double v = -T[j];
-        for (int i = 0; i < P.ns; ++i)
+#pragma unroll (NS > 0 ? NS : 1)
+        for (int i = 0; i < ns; ++i)
             if (P.eq[i]) v = fma(P.S[i * CLB_MAX_COMPONENTS + j], c[i], v);
         F[j] = v;
         s = fma(v, v, s);
@@ -68,30 +87,63 @@ __device__ __forceinline__ double eq_residual(const SpecParams& P, const double*
     return sqrt(s);
 }
 
+template <int NC, int NS>
 __device__ __forceinline__ void eq_totals(const SpecParams& P, const double* cin, double* T) {
-    for (int j = 0; j < P.nc; ++j) {
+    const int nc = NC > 0 ? NC : P.nc, ns = NS > 0 ? NS : P.ns;
+#pragma unroll (NC > 0 ? NC : 1)
+    for (int j = 0; j < nc; ++j) {
         double v = 0;
-        for (int i = 0; i < P.ns; ++i)
+#pragma unroll (NS > 0 ? NS : 1)
+        for (int i = 0; i < ns; ++i)
             if (P.eq[i]) v = fma(P.S[i * CLB_MAX_COMPONENTS + j], fmax(fmin(cin[i], EQ_MAX_C), EQ_MIN_C), v);
         T[j] = fmax(v, EQ_MIN_C);
     }
 }
 
+// v[i] for a run-time i < n; in a fixed-shape build a select over every i, so v stays in registers
+template <int NS>
+__device__ __forceinline__ double eq_pick(const double* v, int i, int n) {
+    if constexpr (NS > 0) {
+        double r = 0.0;
+#pragma unroll
+        for (int q = 0; q < NS; ++q)
+            if (q == i) r = v[q];
+        return r;
+    } else {
+        return i < n ? v[i] : 0.0;
+    }
+}
+
+// v[i] = x for a run-time i; in a fixed-shape build a predicated store to every slot
+template <int NS>
+__device__ __forceinline__ void eq_put(double* v, int i, double x) {
+    if constexpr (NS > 0) {
+#pragma unroll
+        for (int q = 0; q < NS; ++q)
+            if (q == i) v[q] = x;
+    } else {
+        v[i] = x;
+    }
+}
+
 // x0: optional starting log10 component concentrations (else the reference's guess from the
 // component species, 1e-7 for a component that is not a species); max_it < 0: the tableau's cap.
+template <int NC, int NS>
 __device__ __forceinline__ bool eq_solve_nr(const SpecParams& P, const double* cin, double* cout, int* iters,
                                             const double* x0, int max_it) {
-    const int nc = P.nc;
-    double T[CLB_MAX_COMPONENTS], x[CLB_MAX_COMPONENTS], F[CLB_MAX_COMPONENTS], xn[CLB_MAX_COMPONENTS],
-        d[CLB_MAX_COMPONENTS];
-    double A[CLB_MAX_COMPONENTS][CLB_MAX_COMPONENTS + 1];
-    double c[CLB_MAX_EQ_SPECIES];
-    eq_totals(P, cin, T);
+    constexpr int MC = EQ_NC(NC), MS = EQ_NS(NS);
+    const int nc = NC > 0 ? NC : P.nc, ns = NS > 0 ? NS : P.ns;
+    double T[MC], x[MC], F[MC], xn[MC], d[MC];
+    double A[MC][MC + 1];
+    double c[MS];
+    eq_totals<NC, NS>(P, cin, T);
+#pragma unroll (NC > 0 ? NC : 1)
     for (int j = 0; j < nc; ++j) {
         if (x0) {
             x[j] = fmax(fmin(x0[j], EQ_MAX_LOG), EQ_MIN_LOG);
         } else {
-            const double cc = P.comp[j] >= 0 ? cin[P.comp[j]] : 1e-7;
+            double cc = 1e-7;  // the component's species (selected, not indexed: see eq_pick)
+            if (P.comp[j] >= 0) cc = eq_pick<NS>(cin, P.comp[j], ns);
             x[j] = log10(fmax(fmin(cc, EQ_MAX_C), EQ_MIN_C));
         }
     }
@@ -100,73 +152,117 @@ __device__ __forceinline__ bool eq_solve_nr(const SpecParams& P, const double* c
     const double ln10 = 2.302585092994045684;
     const int cap = max_it < 0 ? P.max_it : max_it;
     for (; it < cap; ++it) {
-        const double fn = eq_residual(P, x, T, cin, c, F);
+        const double fn = eq_residual<NC, NS>(P, x, T, cin, c, F);
         if (fn < P.tol) { conv = true; ++it; break; }
+#pragma unroll (NC > 0 ? NC : 1)
         for (int j = 0; j < nc; ++j) {
+#pragma unroll (NC > 0 ? NC : 1)
             for (int k = 0; k < nc; ++k) {
                 double v = 0;
-                for (int i = 0; i < P.ns; ++i)
+#pragma unroll (NS > 0 ? NS : 1)
+                for (int i = 0; i < ns; ++i)
                     if (P.eq[i]) v = fma(ln10 * P.S[i * CLB_MAX_COMPONENTS + j] * P.S[i * CLB_MAX_COMPONENTS + k], c[i], v);
                 A[j][k] = v;
             }
             A[j][nc] = -F[j];
         }
         bool ok = true;
+#pragma unroll (NC > 0 ? NC : 1)
         for (int p = 0; p < nc; ++p) {
             int r = p;
             double mv = fabs(A[p][p]);
+#pragma unroll (NC > 0 ? NC : 1)
             for (int q = p + 1; q < nc; ++q)
                 if (fabs(A[q][p]) > mv) { mv = fabs(A[q][p]); r = q; }
             if (mv < 1e-30) { ok = false; break; }
-            if (r != p)
-                for (int q = 0; q <= nc; ++q) { const double t = A[p][q]; A[p][q] = A[r][q]; A[r][q] = t; }
+            if (r != p) {
+                // row swap by predicated selects, so a fixed-shape build keeps A in registers
+#pragma unroll (NC > 0 ? NC : 1)
+                for (int q = p + 1; q < nc; ++q) {
+                    if (q != r) continue;
+#pragma unroll (NC > 0 ? NC + 1 : 1)
+                    for (int m = 0; m <= nc; ++m) { const double t = A[p][m]; A[p][m] = A[q][m]; A[q][m] = t; }
+                }
+            }
+#pragma unroll (NC > 0 ? NC : 1)
             for (int q = p + 1; q < nc; ++q) {
                 const double fct = A[q][p] / A[p][p];
+#pragma unroll (NC > 0 ? NC + 1 : 1)
                 for (int m = p; m <= nc; ++m) A[q][m] -= fct * A[p][m];
             }
         }
         if (!ok) { ++it; break; }
+#pragma unroll (NC > 0 ? NC : 1)
         for (int p = nc - 1; p >= 0; --p) {
             double v = A[p][nc];
+#pragma unroll (NC > 0 ? NC : 1)
             for (int q = p + 1; q < nc; ++q) v -= A[p][q] * d[q];
             d[p] = v / A[p][p];
         }
         double dmax = 0;
+#pragma unroll (NC > 0 ? NC : 1)
         for (int j = 0; j < nc; ++j) dmax = fmax(dmax, fabs(d[j]));
-        if (dmax > EQ_MAX_STEP)
+        if (dmax > EQ_MAX_STEP) {
+#pragma unroll (NC > 0 ? NC : 1)
             for (int j = 0; j < nc; ++j) d[j] *= EQ_MAX_STEP / dmax;
+        }
         double alpha = 1.0, fnew = 0;
         for (int ls = 0; ls < 40; ++ls) {
+#pragma unroll (NC > 0 ? NC : 1)
             for (int j = 0; j < nc; ++j) xn[j] = fmax(fmin(x[j] + alpha * d[j], EQ_MAX_LOG), EQ_MIN_LOG);
-            fnew = eq_residual(P, xn, T, cin, c, F);
+            fnew = eq_residual<NC, NS>(P, xn, T, cin, c, F);
             if (fnew < fn * (1.0 - 0.0001 * alpha) || alpha < 1e-15) break;
             alpha *= 0.5;
         }
         double dn = 0;
+#pragma unroll (NC > 0 ? NC : 1)
         for (int j = 0; j < nc; ++j) { x[j] = xn[j]; dn = fma(d[j], d[j], dn); }
         if (alpha * sqrt(dn) < P.tol * 1e-3 && fnew < P.tol * 100) { conv = true; ++it; break; }
     }
-    eq_species(P, x, cin, cout);
-    for (int i = 0; i < P.ns; ++i) {
+    eq_species<NC, NS>(P, x, cin, cout);
+#pragma unroll (NS > 0 ? NS : 1)
+    for (int i = 0; i < ns; ++i) {
         double v = cout[i];
         if (isnan(v) || isinf(v)) v = cin[i] > EQ_MIN_C ? fmin(cin[i], EQ_MAX_C) : EQ_MIN_C;
         cout[i] = fmax(fmin(v, EQ_MAX_C), EQ_MIN_C);
     }
-    if (x0) for (int j = 0; j < nc; ++j) const_cast<double*>(x0)[j] = x[j];  // hand back where it stopped
+    if (x0) {
+#pragma unroll (NC > 0 ? NC : 1)
+        for (int j = 0; j < nc; ++j) const_cast<double*>(x0)[j] = x[j];  // hand back where it stopped
+    }
     *iters = it;
     return conv;
 }
 
+template <int NC, int NS>
 __global__ void k_eq_batch(const SpecParams P, const double* __restrict__ cin, double* __restrict__ cout,
                            int* __restrict__ iters, int n) {
+    const int ns = NS > 0 ? NS : P.ns;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        double ci[CLB_MAX_EQ_SPECIES], co[CLB_MAX_EQ_SPECIES];
-        for (int i = 0; i < P.ns; ++i) ci[i] = cin[(int64_t)t * P.ns + i];
+        double ci[EQ_NS(NS)], co[EQ_NS(NS)];
+#pragma unroll (NS > 0 ? NS : 1)
+        for (int i = 0; i < ns; ++i) ci[i] = cin[(int64_t)t * ns + i];
         int it = 0;
-        eq_solve_nr(P, ci, co, &it, nullptr, -1);
-        for (int i = 0; i < P.ns; ++i) cout[(int64_t)t * P.ns + i] = co[i];
+        eq_solve_nr<NC, NS>(P, ci, co, &it, nullptr, -1);
+#pragma unroll (NS > 0 ? NS : 1)
+        for (int i = 0; i < ns; ++i) cout[(int64_t)t * ns + i] = co[i];
         if (iters) iters[t] = it;
     }
+}
+
+// the tableau shapes with a build of their own: the 5 x 12 tableau of the fracture configuration
+// and the two-component carbonate system; any other shape runs the general build
+#define CLB_EQ_SHAPES(P, X)                                      \
+    do {                                                         \
+        if ((P).nc == 5 && (P).ns == 12) X(5, 12);               \
+        else if ((P).nc == 2 && (P).ns == 4) X(2, 4);            \
+        else X(0, 0);                                            \
+    } while (0)
+
+template <int NC, int NS>
+static void launch_eq_batch(const SpecParams& P, const double* cin, double* cout, int* iters, int n, int num_sms,
+                            cudaStream_t st) {
+    k_eq_batch<NC, NS><<<std::max(1, std::min(num_sms * 8, (n + 127) / 128)), 128, 0, st>>>(P, cin, cout, iters, n);
 }
 
 // Where outgoing population i of node k sits after a step of parity `odd` (AA pattern,
@@ -199,17 +295,20 @@ __device__ __forceinline__ TS* out_slot7(const SparseView& S, TS* f, TS* link, i
 // start from the surrogate's component values. Accepted (true) when the input lies inside the
 // trained range and, when `check`, the polished answer has converged; x0_out returns where the
 // polish stopped so a fallback can continue from there.
+template <int NC, int NS>
 __device__ __forceinline__ bool mlp_warp_speciate(const MlpView& M, const SpecParams& P, bool active,
                                                   const double* c, double* e, bool check, float* ws,
                                                   double* x0_out, int* it_used) {
     const int lane = threadIdx.x & 31;
-    double T[CLB_MAX_COMPONENTS];
+    double T[EQ_NC(NC)];
     bool in_range = active;
     float* row = ws + lane * 16;
     for (int q = 0; q < 16; ++q) row[q] = 0.f;
+    const int nc = NC > 0 ? NC : P.nc, ns = NS > 0 ? NS : P.ns;
     if (active) {
-        eq_totals(P, c, T);
-        for (int j = 0; j < P.nc; ++j) {
+        eq_totals<NC, NS>(P, c, T);
+#pragma unroll (NC > 0 ? NC : 1)
+        for (int j = 0; j < nc; ++j) {
             const float x = (float)log10(T[j]);
             const float lo = M.in_lo[j], hi = M.in_hi[j];
             const float sx = 2.f * (x - lo) / (hi - lo) - 1.f;
@@ -230,24 +329,30 @@ __device__ __forceinline__ bool mlp_warp_speciate(const MlpView& M, const SpecPa
     }
     if (!active) return false;
     // the surrogate's log10 species; its components' values start a short Newton polish
-    double x[CLB_MAX_COMPONENTS];
-    for (int i = 0; i < P.ns; ++i) {
+    double x[EQ_NC(NC)];
+#pragma unroll (NS > 0 ? NS : 1)
+    for (int i = 0; i < ns; ++i) {
         const float lo = M.out_lo[i], hi = M.out_hi[i];
         e[i] = (double)lo + ((double)row[i] + 1.0) * 0.5 * (double)(hi - lo);
     }
-    for (int j = 0; j < P.nc; ++j) x[j] = P.comp[j] >= 0 ? e[P.comp[j]] : -7.0;
+#pragma unroll (NC > 0 ? NC : 1)
+    for (int j = 0; j < nc; ++j) x[j] = P.comp[j] >= 0 ? eq_pick<NS>(e, P.comp[j], ns) : -7.0;
     *it_used = 0;
     if (!in_range) {
-        for (int j = 0; j < P.nc; ++j) x0_out[j] = x[j];
+#pragma unroll (NC > 0 ? NC : 1)
+        for (int j = 0; j < nc; ++j) x0_out[j] = x[j];
         return false;
     }
-    eq_solve_nr(P, c, e, it_used, x, M.polish);
-    for (int j = 0; j < P.nc; ++j) x0_out[j] = x[j];
+    eq_solve_nr<NC, NS>(P, c, e, it_used, x, M.polish);
+#pragma unroll (NC > 0 ? NC : 1)
+    for (int j = 0; j < nc; ++j) x0_out[j] = x[j];
     if (!check) return true;
     double worst = 0;
-    for (int j = 0; j < P.nc; ++j) {
+#pragma unroll (NC > 0 ? NC : 1)
+    for (int j = 0; j < nc; ++j) {
         double v = -T[j];
-        for (int i = 0; i < P.ns; ++i)
+#pragma unroll (NS > 0 ? NS : 1)
+        for (int i = 0; i < ns; ++i)
             if (P.eq[i]) v = fma(P.S[i * CLB_MAX_COMPONENTS + j], e[i], v);
         worst = fmax(worst, fabs(v) / fmax(T[j], EQ_MIN_C));
     }
@@ -256,7 +361,7 @@ __device__ __forceinline__ bool mlp_warp_speciate(const MlpView& M, const SpecPa
 
 // The speciation step on the populations the last transport step wrote. Warps walk 32
 // consecutive nodes at a time so the surrogate's tensor-core tiles see converged warps.
-template <typename TS>
+template <typename TS, int NC, int NS>
 __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* __restrict__ glink,
                                                        double* __restrict__ imm, const SparseView S, const AdeParams A,
                                                        const SpecParams P, int odd, int64_t k_west_end,
@@ -270,9 +375,12 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
     for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + wib) * 32; base < S.K; base += nwarps * 32) {
         const int64_t k = base + lane;
         const bool active = k < S.K && k >= k_west_end && k < k_east_begin && A.react[S.code[k]];
-        double c[CLB_MAX_EQ_SPECIES], e[CLB_MAX_EQ_SPECIES];
+        double c[EQ_NS(NS)], e[EQ_NS(NS)];
+        const int ns = NS > 0 ? NS : P.ns;
         if (active) {
-            for (int i = 0; i < P.ns; ++i) {
+            // species by species (the gathers stay a loop; the values go to c by selects)
+#pragma unroll 1
+            for (int i = 0; i < ns; ++i) {
                 const int si = P.ispec[i];
                 double v;
                 if (A.slot[si] >= 0) {
@@ -284,14 +392,14 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
                 } else {
                     v = imm[(int64_t)si * A.g.N + S.node[k]];
                 }
-                c[i] = fmax(v, EQ_MIN_C);
+                eq_put<NS>(c, i, fmax(v, EQ_MIN_C));
             }
         }
         bool done = false;
-        double xs[CLB_MAX_COMPONENTS];
+        double xs[EQ_NC(NC)];
         int pit = 0;
         if (use_mlp) {  // warp-uniform
-            done = mlp_warp_speciate(M, P, active, c, e, mode == CLB_SPEC_MLP_NR, wsm[wib], xs, &pit);
+            done = mlp_warp_speciate<NC, NS>(M, P, active, c, e, mode == CLB_SPEC_MLP_NR, wsm[wib], xs, &pit);
             if (active) { if (done) ++n_sur; else ++n_fb; }
         }
         if (!active) continue;
@@ -302,14 +410,16 @@ __global__ void __launch_bounds__(128) k_speciate_step(TS* __restrict__ g, TS* _
         } else {
             // Newton-Raphson fallback, from where the surrogate's polish stopped when there was one
             int it = 0;
-            if (eq_solve_nr(P, c, e, &it, (use_mlp && pit > 0) ? xs : nullptr, -1)) ++n_conv;
+            if (eq_solve_nr<NC, NS>(P, c, e, &it, (use_mlp && pit > 0) ? xs : nullptr, -1)) ++n_conv;
             n_it += it;
         }
-        for (int i = 0; i < P.ns; ++i) {
-            double dC = e[i] - c[i];
-            const double cap = fmax(1e-9, 0.1 * fabs(c[i]));
+#pragma unroll 1
+        for (int i = 0; i < ns; ++i) {
+            const double ci = eq_pick<NS>(c, i, ns);
+            double dC = eq_pick<NS>(e, i, ns) - ci;
+            const double cap = fmax(1e-9, 0.1 * fabs(ci));
             if (fabs(dC) > cap) dC = dC > 0 ? cap : -cap;
-            if (c[i] + dC < 1e-20) dC = 1e-20 - c[i];
+            if (ci + dC < 1e-20) dC = 1e-20 - ci;
             if (!(fabs(dC) > THRD)) continue;
             const int si = P.ispec[i];
             if (A.slot[si] >= 0) {
@@ -383,6 +493,14 @@ clb_status speciation_setup(clb_handle* h, const clb_speciation_desc* d) {
     return cuda_check(h, cudaGetLastError(), "speciation setup");
 }
 
+template <typename TS, int NC, int NS>
+static int launch_speciate(clb_handle* h, int grid, const SparseView& S, const MlpView& M, int odd) {
+    k_speciate_step<TS, NC, NS><<<grid, 128, 0, h->stream>>>((TS*)h->d_g, (TS*)h->d_glink, h->d_imm, S, h->ap,
+                                                            CLB_SP(h), odd, h->ade_west_end, h->ade_east_begin, M,
+                                                            h->spec_mode, h->d_spec_stats);
+    return 0;
+}
+
 clb_status speciation_step(clb_handle* h) {
     if (!h->spec_ready || h->spec_mode == CLB_SPEC_OFF) return CLB_OK;
     if ((h->spec_mode == CLB_SPEC_MLP || h->spec_mode == CLB_SPEC_MLP_NR) && !h->mlp_ready)
@@ -393,9 +511,15 @@ clb_status speciation_step(clb_handle* h) {
     const MlpView M = mlp_view(h);
     ++h->launches;
     switch (h->ade_prec) {
-        case CLB_F64: k_speciate_step<double><<<grid, 128, 0, h->stream>>>((double*)h->d_g, (double*)h->d_glink, h->d_imm, S, h->ap, CLB_SP(h), odd, h->ade_west_end, h->ade_east_begin, M, h->spec_mode, h->d_spec_stats); break;
-        case CLB_F32: k_speciate_step<float><<<grid, 128, 0, h->stream>>>((float*)h->d_g, (float*)h->d_glink, h->d_imm, S, h->ap, CLB_SP(h), odd, h->ade_west_end, h->ade_east_begin, M, h->spec_mode, h->d_spec_stats); break;
-        default: k_speciate_step<__half><<<grid, 128, 0, h->stream>>>((__half*)h->d_g, (__half*)h->d_glink, h->d_imm, S, h->ap, CLB_SP(h), odd, h->ade_west_end, h->ade_east_begin, M, h->spec_mode, h->d_spec_stats); break;
+#define CLB_SPEC_F64(NC, NS) launch_speciate<double, NC, NS>(h, grid, S, M, odd)
+#define CLB_SPEC_F32(NC, NS) launch_speciate<float, NC, NS>(h, grid, S, M, odd)
+#define CLB_SPEC_F16(NC, NS) launch_speciate<__half, NC, NS>(h, grid, S, M, odd)
+        case CLB_F64: CLB_EQ_SHAPES(CLB_SP(h), CLB_SPEC_F64); break;
+        case CLB_F32: CLB_EQ_SHAPES(CLB_SP(h), CLB_SPEC_F32); break;
+        default: CLB_EQ_SHAPES(CLB_SP(h), CLB_SPEC_F16); break;
+#undef CLB_SPEC_F64
+#undef CLB_SPEC_F32
+#undef CLB_SPEC_F16
     }
     return cuda_check(h, cudaGetLastError(), "speciation step");
 }
@@ -411,7 +535,9 @@ clb_status speciation_solve(clb_handle* h, const double* cin, int n, double* cou
     if (e == cudaSuccess && iters) e = cudaMalloc(&dit, sizeof(int) * n);
     if (e == cudaSuccess) e = cudaMemcpyAsync(di, cin, bytes, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) {
-        k_eq_batch<<<std::max(1, std::min(h->num_sms * 8, (n + 127) / 128)), 128, 0, h->stream>>>(CLB_SP(h), di, dout, dit, n);
+#define CLB_EQB(NC, NS) launch_eq_batch<NC, NS>(CLB_SP(h), di, dout, dit, n, h->num_sms, h->stream)
+        CLB_EQ_SHAPES(CLB_SP(h), CLB_EQB);
+#undef CLB_EQB
         e = cudaMemcpyAsync(cout, dout, bytes, cudaMemcpyDeviceToHost, h->stream);
     }
     if (e == cudaSuccess && iters) e = cudaMemcpyAsync(iters, dit, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream);
@@ -424,7 +550,9 @@ clb_status speciation_solve(clb_handle* h, const double* cin, int n, double* cou
 
 // device-resident batch solve (used by the surrogate's training-data generator)
 clb_status speciation_solve_device(clb_handle* h, const double* d_in, int n, double* d_out) {
-    k_eq_batch<<<std::max(1, std::min(h->num_sms * 8, (n + 127) / 128)), 128, 0, h->stream>>>(CLB_SP(h), d_in, d_out, nullptr, n);
+#define CLB_EQB(NC, NS) launch_eq_batch<NC, NS>(CLB_SP(h), d_in, d_out, nullptr, n, h->num_sms, h->stream)
+    CLB_EQ_SHAPES(CLB_SP(h), CLB_EQB);
+#undef CLB_EQB
     return cuda_check(h, cudaGetLastError(), "speciation batch");
 }
 
@@ -552,7 +680,7 @@ __global__ void k_mlp_xy(const SpecParams P, int n, const double* __restrict__ c
             for (int i = 0; i < P.ns; ++i) if (P.eq[i]) raw += P.S[i * CLB_MAX_COMPONENTS + j] * ci[i];
             if (!(raw > 0)) valid = false;
         }
-        eq_totals(P, ci, T);
+        eq_totals<0, 0>(P, ci, T);
         for (int q = 0; q < MLP_IN; ++q) X[(int64_t)t * MLP_IN + q] = q < P.nc ? (float)log10(T[q]) : 0.f;
         if (!valid) X[(int64_t)t * MLP_IN] = __int_as_float(0x7fc00000);
         for (int q = 0; q < MLP_OUT; ++q) Y[(int64_t)t * MLP_OUT + q] = q < P.ns ? (float)log10(ceq[(int64_t)t * P.ns + q]) : 0.f;
@@ -859,7 +987,7 @@ __global__ void __launch_bounds__(128) k_mlp_predict(const MlpView M, const Spec
             for (int i = 0; i < P.ns; ++i) c[i] = fmax(cin[(int64_t)tix * P.ns + i], EQ_MIN_C);
         double xs[CLB_MAX_COMPONENTS];
         int pit = 0;
-        const bool ok = mlp_warp_speciate(M, P, active, c, e, check != 0, wsm[w], xs, &pit);
+        const bool ok = mlp_warp_speciate<0, 0>(M, P, active, c, e, check != 0, wsm[w], xs, &pit);
         if (active) {
             for (int i = 0; i < P.ns; ++i) cout[(int64_t)tix * P.ns + i] = e[i];
             if (accepted) accepted[tix] = ok ? 1 : 0;
