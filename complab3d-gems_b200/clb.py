@@ -189,6 +189,7 @@ SIGNATURES = {
     "clb_batch_get_schedule": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "clb_batch_set_stream": [C.c_void_p, C.c_void_p],
+    "clb_batch_set_wait_limit": [C.c_void_p, C.c_int64],
     "clb_ca_step": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "clb_refresh_dynamics": [C.c_void_p, C.c_int, C.c_int],
     "clb_precip_setup": [C.c_void_p, C.POINTER(PrecipDesc)],
@@ -807,6 +808,10 @@ class Batch:
     def set_stream(self, stream):
         """stream: a cudaStream_t as an integer (torch.cuda.Stream().cuda_stream), or None."""
         _check_global(lib().clb_batch_set_stream(self.b, C.c_void_p(stream) if stream else None))
+
+    def set_wait_limit(self, ns):
+        """Limit of one dependency wait of the persistent schedule, in nanoseconds."""
+        _check_global(lib().clb_batch_set_wait_limit(self.b, int(ns)))
 
     def autotune(self, steps=20):
         buf = C.create_string_buffer(4096)

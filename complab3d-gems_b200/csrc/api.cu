@@ -410,6 +410,11 @@ clb_status clb_batch_get_schedule(clb_batch* batch, int* persistent, int* tile, 
     return batch_get_schedule(batch, persistent, tile, lag, steps_per_launch, ctas_per_sm);
 }
 
+clb_status clb_batch_set_wait_limit(clb_batch* batch, int64_t ns) {
+    if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
+    return batch_set_wait_limit(batch, ns);
+}
+
 clb_status clb_batch_set_stream(clb_batch* batch, void* stream) {
     if (!batch) return fail(nullptr, CLB_INVALID_ARG, "null batch");
     return batch_set_stream(batch, stream);

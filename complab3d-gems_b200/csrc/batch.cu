@@ -639,6 +639,16 @@ clb_status batch_schedule(clb_batch* b, int persistent, int tile, int lag, int s
     return CLB_OK;
 }
 
+// The limit of one dependency wait of the persistent schedule (nanoseconds); a wait that reaches
+// it gives up, the launch skips its remaining items and the step returns CLB_TIMEOUT.
+clb_status batch_set_wait_limit(clb_batch* b, int64_t ns) {
+    if (ns < 0) return bfail(b, CLB_INVALID_ARG, "wait limit must not be negative");
+    cudaStreamSynchronize(bstream(b));
+    b->wait_ns = ns;
+    drop_graphs(b);  // the limit is a parameter of the captured launches
+    return CLB_OK;
+}
+
 // The stream the batch's work is enqueued on (nullptr: the batch's own); the steps still return
 // once their work is done.
 clb_status batch_set_stream(clb_batch* b, void* stream) {

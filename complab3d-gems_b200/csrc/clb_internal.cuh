@@ -400,6 +400,7 @@ clb_status batch_destroy(clb_batch* b);
 clb_status batch_counts(clb_batch* b, int64_t* flow_nodes, int64_t* ade_nodes);
 clb_status batch_schedule(clb_batch* b, int persistent, int tile, int lag, int steps_per_launch, int ctas_per_sm);
 clb_status batch_set_stream(clb_batch* b, void* stream);
+clb_status batch_set_wait_limit(clb_batch* b, int64_t ns);
 clb_status batch_get_schedule(clb_batch* b, int* persistent, int* tile, int* lag, int* steps_per_launch,
                               int* ctas_per_sm);
 

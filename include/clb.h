@@ -567,6 +567,11 @@ clb_status clb_batch_get_schedule(clb_batch* batch, int* persistent, int* tile, 
 /* Enqueue the batch's work on `stream` (a cudaStream_t; NULL: the batch's own stream). */
 clb_status clb_batch_set_stream(clb_batch* batch, void* stream);
 
+/* The limit of one dependency wait of the persistent schedule, in nanoseconds (default 2 s). A
+ * wait that reaches it gives up: the launch skips its remaining items, the step returns
+ * CLB_TIMEOUT and the domains' state is undefined; the device stays usable. */
+clb_status clb_batch_set_wait_limit(clb_batch* batch, int64_t ns);
+
 /* Open (collide / stream) nodes of the flow and species lattices over all domains. */
 clb_status clb_batch_counts(clb_batch* batch, int64_t* flow_nodes, int64_t* transport_nodes);
 clb_status clb_batch_destroy(clb_batch* batch);

@@ -135,3 +135,23 @@ def test_batch_staged_flow_needs_four_byte_storage(clb):
         batch.schedule(persistent=False, staged_flow=True)
     assert batch.get_schedule()["staged_flow"] is False
     batch.close()
+
+
+def test_persistent_wait_limit_reports_timeout(clb):
+    """A dependency wait of the persistent schedule that reaches its limit gives up on the device:
+    with a limit far below a step's duration, waits that find their dependency still in progress
+    give up, the launch skips its remaining items, the step returns CLB_TIMEOUT and the device
+    stays usable (the same batch steps again once the limit is back)."""
+    cfg = workloads.ensemble_uneven_packs(n_domains=9, seed=24, scale=0.5)
+    B = build(clb, cfg, clb.F32)
+    batch = clb.Batch(B)
+    batch.schedule(tile=256, lag=1, steps_per_launch=8)
+    batch.set_wait_limit(1)
+    with pytest.raises(clb.ClbError) as err:
+        batch.step(8)
+    assert clb.STATUS[err.value.status] == "TIMEOUT" and "wait" in str(err.value)
+    batch.set_wait_limit(2_000_000_000)
+    batch.step(8)
+    batch.close()
+    for D in B:
+        D.close()
